@@ -1,0 +1,359 @@
+"""Case writer: grids, boundary files, parameter files and initial states in
+the reference's on-disk formats, so that the reference driver and this
+library read identical inputs.
+
+Formats written (all under ``<dir>/CASE``):
+
+* ``setup/filenames`` and the four parameter files, in the key/value + LIST
+  syntax parsed by src/0_basic/1_MPCNS_Parameter.cpp:4-66 (the shipped
+  Z4_Lunar/9999setup/* files are the template).
+* ``geometry/grid   0.grd``: binary grid, Read_Method 2
+  (src/1_grid/1_MPCNS_Grid.cpp:125-230): int32 nblock, per block an int32
+  byte count plus NUL-terminated name, per block int32 imax/jmax/kmax (node
+  counts), then per block x, y, z as float64 with i fastest.
+* ``geometry/boundary_condition/boundary   0.txt``: per block the number of
+  physical faces, then "ist ied jst jed kst ked bctype" with 0-based node
+  indices (src/1_grid/1_MPCNS_Grid.cpp:232-296).
+* ``geometry/boundary_condition/boundary_name.fvbnd``: header line, name of
+  type 0, further names from type 2 on, terminated by BOUNDARIES
+  (src/1_grid/1_MPCNS_Grid.cpp:298-334).
+* ``geometry/boundary_condition/inner   0.txt``: total count, per-block
+  counts, a comment line, then one line per interface with 1-based node
+  ranges whose signs encode the in-plane axis pairing, the signed 1-based
+  block number (negative = periodic) and block name for both sides
+  (src/1_grid/1_MPCNS_Grid.cpp:413-520, include/1_grid/Grid_Boundary.h:236-330).
+* ``geometry/boundary_condition/parallel   0.txt``: no inter-rank faces.
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+
+from . import rst
+
+# Physical constants of the shipped Lunar setup (Z4_Lunar/9999setup/0_General_Setting.txt:23-28)
+GAMMA = 1.6667
+NA = 6.02e23
+R_UNI = 8.314
+MU0 = 1.256637061e-6
+Q_E = 1.602e-19
+
+BC_NAMES = ["Solid_Surface", "Farfield", "Pole", "Outflow"]  # types 2, 3, 4, 5
+
+
+@dataclass
+class BlockGrid:
+    name: str
+    x: np.ndarray  # (imax, jmax, kmax) node coordinates
+    y: np.ndarray
+    z: np.ndarray
+    physical: List[Tuple[Tuple[int, int, int, int, int, int], str]] = field(default_factory=list)
+
+    @property
+    def ncell(self):
+        return tuple(s - 1 for s in self.x.shape)
+
+
+@dataclass
+class InnerFace:
+    """One side of a block interface in the inner-file convention: 1-based
+    node ranges (ist, ied, jst, jed, kst, ked) whose signs/order encode the
+    axis pairing, plus the 1-based block number (negative for periodic)."""
+    this_range: Tuple[int, int, int, int, int, int]
+    this_block: int
+    tar_range: Tuple[int, int, int, int, int, int]
+    tar_block: int
+
+
+@dataclass
+class CaseSpec:
+    blocks: List[BlockGrid]
+    inner: List[List[InnerFace]]  # per block
+    params: Dict[str, object]
+
+
+def ref_scales(U=4.61e5, n=7.0e6, M=0.001, T=1.2e5, L=1.7374e6):
+    """Reference scales chosen so that inver_MA2 = momentum_hall_coeff = 1
+    (Z4_Lunar/src/physics/LunarSolver_Tools.cpp:37-39): B_ref = U*sqrt(mu0*rho_ref)."""
+    rho_ref = M * n / NA
+    B = U * math.sqrt(MU0 * rho_ref)
+    return dict(U=U, T=T, n=n, Molecular_mass=M, B_ref=B, L_ref=L)
+
+
+def default_params(**over):
+    p = dict(
+        CFL=0.4, max_Time=0.0, max_Nstep=100000000, output_step=0, output_residual=0,
+        Archive_Output_Time=0.0, continue_calc=0, dimension=3, ngg=4, Read_Method=2,
+        corner_treat=2, scale=1.0, mole_mass1=0.001, eta_max_lunar=1.25e7,
+        REF=ref_scales(),
+        INITIAL=None,  # dict(U, T, n, Molecular_mass, c_y, c_z, Bx, By, Bz)
+        num_of_dipole=0, is_Lunar_resistance=0, use_implicit_lunar_resistance=0,
+        n_resistive_subcycles=1, implicit_resistive_ksp_rtol=1e-10,
+        implicit_resistive_ksp_atol=1e-30, implicit_resistive_ksp_max_it=200,
+        arti_eta_max=0.0, J_range_start=800.0, J_range_on=3000.0,
+    )
+    p.update(over)
+    if p["INITIAL"] is None:
+        r = p["REF"]
+        p["INITIAL"] = dict(U=r["U"], T=r["T"], n=r["n"], Molecular_mass=r["Molecular_mass"],
+                            c_y=0.0, c_z=0.0, Bx=0.0, By=0.0, Bz=0.0)
+    return p
+
+
+def _num(v) -> str:
+    if isinstance(v, bool):
+        return "1" if v else "0"
+    if isinstance(v, int):
+        return str(v)
+    return repr(float(v))
+
+
+def write_setup(case_dir: str, p: Dict[str, object]) -> None:
+    d = os.path.join(case_dir, "CASE", "setup")
+    os.makedirs(d, exist_ok=True)
+    with open(os.path.join(d, "filenames"), "w") as f:
+        f.write("0_General_Setting.txt\n1_Initial_condition.txt\n2_Boundary_Condition.txt\n3_MHD_Control.txt\n###END###\n")
+    g = []
+    g.append(f"double  CFL                     {_num(p['CFL'])}")
+    g.append(f"double  max_Time                {_num(p['max_Time'])}")
+    g.append(f"int     max_Nstep               {_num(p['max_Nstep'])}")
+    g.append(f"int     output_step             {_num(p['output_step'])}")
+    g.append(f"int     output_residual         {_num(p['output_residual'])}")
+    g.append(f"double  Archive_Output_Time     {_num(p['Archive_Output_Time'])}")
+    g.append(f"bool    continue_calc           {_num(p['continue_calc'])}")
+    g.append(f"int     dimension               {_num(p['dimension'])}")
+    g.append(f"int     ngg                     {_num(p['ngg'])}")
+    g.append(f"int     Read_Method             {_num(p['Read_Method'])}")
+    g.append(f"int     corner_treat            {_num(p['corner_treat'])}")
+    g.append(f"double  scale                   {_num(p['scale'])}")
+    g.append(f"double  mole_mass1              {_num(p['mole_mass1'])}")
+    g.append(f"double  eta_max_lunar           {_num(p['eta_max_lunar'])}")
+    g.append("")
+    g.append("LIST==================================================================")
+    g.append("constant        5")
+    g.append("(double)")
+    g.append("gamma           NA              R_uni       mu_mag             q_e")
+    g.append(f"{_num(GAMMA)} {_num(NA)} {_num(R_UNI)} {_num(MU0)} {_num(Q_E)}")
+    g.append("LIST==================================================================")
+    g.append("")
+    g.append("END_OF_FILE")
+    with open(os.path.join(d, "0_General_Setting.txt"), "w") as f:
+        f.write("\n".join(g) + "\n")
+    r = p["REF"]
+    ini = p["INITIAL"]
+    s = []
+    s.append("LIST==================================================================")
+    s.append("REF             6")
+    s.append("(double)")
+    s.append("U               T               n           Molecular_mass  B_ref   L_ref")
+    s.append(" ".join(_num(r[k]) for k in ["U", "T", "n", "Molecular_mass", "B_ref", "L_ref"]))
+    s.append("LIST==================================================================")
+    s.append("")
+    s.append("LIST==================================================================")
+    s.append("INITIAL         9")
+    s.append("(double)")
+    s.append("U               T               n           Molecular_mass  c_y     c_z     Bx      By      Bz")
+    s.append(" ".join(_num(ini[k]) for k in ["U", "T", "n", "Molecular_mass", "c_y", "c_z", "Bx", "By", "Bz"]))
+    s.append("LIST==================================================================")
+    s.append("")
+    s.append("END_OF_FILE")
+    with open(os.path.join(d, "1_Initial_condition.txt"), "w") as f:
+        f.write("\n".join(s) + "\n")
+    with open(os.path.join(d, "2_Boundary_Condition.txt"), "w") as f:
+        f.write("LIST==================================================================\n"
+                "Boundary_Priority      5\n(int)\n"
+                "Pole                   Outflow     Absorbing   Solid_Surface   Farfield\n"
+                "0                      4           2           3               1\n"
+                "LIST==================================================================\n\nEND_OF_FILE\n")
+    m = []
+    m.append(f"int     num_of_dipole                   {_num(p['num_of_dipole'])}")
+    m.append(f"bool    is_Lunar_resistance           {_num(p['is_Lunar_resistance'])}")
+    m.append(f"bool    use_implicit_lunar_resistance {_num(p['use_implicit_lunar_resistance'])}")
+    m.append(f"int     n_resistive_subcycles           {_num(p['n_resistive_subcycles'])}")
+    m.append(f"double  implicit_resistive_ksp_rtol     {_num(p['implicit_resistive_ksp_rtol'])}")
+    m.append(f"double  implicit_resistive_ksp_atol     {_num(p['implicit_resistive_ksp_atol'])}")
+    m.append(f"int     implicit_resistive_ksp_max_it   {_num(p['implicit_resistive_ksp_max_it'])}")
+    m.append(f"double  arti_eta_max                    {_num(p['arti_eta_max'])}")
+    m.append(f"double  J_range_start                   {_num(p['J_range_start'])}")
+    m.append(f"double  J_range_on                      {_num(p['J_range_on'])}")
+    m.append("")
+    m.append("END_OF_FILE")
+    with open(os.path.join(d, "3_MHD_Control.txt"), "w") as f:
+        f.write("\n".join(m) + "\n")
+
+
+def write_geometry(case_dir: str, spec: CaseSpec) -> None:
+    gdir = os.path.join(case_dir, "CASE", "geometry")
+    bdir = os.path.join(gdir, "boundary_condition")
+    os.makedirs(bdir, exist_ok=True)
+    rank = "   0"
+    with open(os.path.join(gdir, f"grid{rank}.grd"), "wb") as f:
+        f.write(np.int32(len(spec.blocks)).tobytes())
+        for b in spec.blocks:
+            nm = b.name.encode() + b"\0"
+            f.write(np.int32(len(nm)).tobytes())
+            f.write(nm)
+        for b in spec.blocks:
+            f.write(np.array(b.x.shape, dtype="<i4").tobytes())
+        for b in spec.blocks:
+            for c in (b.x, b.y, b.z):
+                # stored with i fastest, then j, then k
+                f.write(np.ascontiguousarray(np.transpose(c, (2, 1, 0)), dtype="<f8").tobytes())
+    with open(os.path.join(bdir, f"boundary{rank}.txt"), "w") as f:
+        for b in spec.blocks:
+            f.write(f"{len(b.physical)}\n")
+            for rng, name in b.physical:
+                f.write(" ".join(str(v) for v in rng) + f" {2 + BC_NAMES.index(name)}\n")
+    with open(os.path.join(bdir, "boundary_name.fvbnd"), "w") as f:
+        f.write("FVBND 1 4\nUnspecified\n")
+        for n in BC_NAMES:
+            f.write(n + "\n")
+        f.write("BOUNDARIES\n")
+    total = sum(len(x) for x in spec.inner)
+    with open(os.path.join(bdir, f"inner{rank}.txt"), "w") as f:
+        f.write(f"{total}\n")
+        f.write(" ".join(str(len(x)) for x in spec.inner) + "\n")
+        f.write("imin imax jmin jmax kmin kmax block name | target imin imax jmin jmax kmin kmax block name\n")
+        for ib, faces in enumerate(spec.inner):
+            for fc in faces:
+                f.write(" ".join(str(v) for v in fc.this_range) + f" {fc.this_block} {spec.blocks[ib].name} "
+                        + " ".join(str(v) for v in fc.tar_range)
+                        + f" {fc.tar_block} {spec.blocks[abs(fc.tar_block) - 1].name}\n")
+    with open(os.path.join(bdir, f"parallel{rank}.txt"), "w") as f:
+        f.write(f"{len(spec.blocks)}\n0\n" + " ".join("0" for _ in spec.blocks) + "\nno inter-rank faces\n")
+
+
+def write_case(case_dir: str, spec: CaseSpec) -> None:
+    write_setup(case_dir, spec.params)
+    write_geometry(case_dir, spec)
+
+
+# --------------------------------------------------------------------------
+# Grids
+# --------------------------------------------------------------------------
+
+def periodic_box(n: Tuple[int, int, int], amp: float = 0.05) -> BlockGrid:
+    """Unit cube with the sinusoidal map x = xi + a sin(2 pi eta),
+    y = eta + a sin(2 pi zeta), z = zeta + a sin(2 pi xi), nodes at xi = i/n."""
+    ni, nj, nk = n
+    xi = np.arange(ni + 1) / ni
+    et = np.arange(nj + 1) / nj
+    ze = np.arange(nk + 1) / nk
+    XI, ET, ZE = np.meshgrid(xi, et, ze, indexing="ij")
+    x = XI + amp * np.sin(2.0 * np.pi * ET)
+    y = ET + amp * np.sin(2.0 * np.pi * ZE)
+    z = ZE + amp * np.sin(2.0 * np.pi * XI)
+    return BlockGrid("Fluid", x, y, z)
+
+
+def periodic_inner(n: Tuple[int, int, int]) -> List[InnerFace]:
+    """Self-periodic interfaces of one block (block number -1 = periodic).
+    In-plane pairing convention: the second tangential axis carries negative
+    indices on both sides, so the transform is the identity up to the normal
+    offset (include/1_grid/Grid_Boundary.h:274-299)."""
+    I, J, K = n[0] + 1, n[1] + 1, n[2] + 1
+    faces = []
+    # i faces: tangential j (primary), k (secondary, negative)
+    lo_i = (1, 1, 1, J, -1, -K)
+    hi_i = (I, I, 1, J, -1, -K)
+    lo_j = (1, I, 1, 1, -1, -K)
+    hi_j = (1, I, J, J, -1, -K)
+    lo_k = (1, I, -1, -J, 1, 1)
+    hi_k = (1, I, -1, -J, K, K)
+    for a, b in ((lo_i, hi_i), (lo_j, hi_j), (lo_k, hi_k)):
+        faces.append(InnerFace(a, -1, b, -1))
+        faces.append(InnerFace(b, -1, a, -1))
+    return faces
+
+
+def periodic_box_case(n=(64, 64, 64), **param_over) -> CaseSpec:
+    blk = periodic_box(n)
+    return CaseSpec([blk], [periodic_inner(n)], default_params(**param_over))
+
+
+# --------------------------------------------------------------------------
+# Initial states
+# --------------------------------------------------------------------------
+
+def _face_area_vectors(x, y, z):
+    """Face area vectors S = 0.5 * (d1 x d2) of the bilinear faces spanned by
+    node arrays (same construction as the reference's JDxi/JDet/JDze,
+    src/3_field/4_MPCNS_Geometry.cpp:98-197).  Returns three arrays of shape
+    (ni+1, nj, nk, 3), (ni, nj+1, nk, 3), (ni, nj, nk+1, 3) over interior faces."""
+    P = np.stack([x, y, z], axis=-1)
+
+    def quad(p0, pa, pb, pab):
+        rx = pa - p0
+        ry = pb - p0
+        rx_ = pb - pab
+        ry_ = pa - pab
+        return 0.5 * (np.cross(rx, ry) + np.cross(rx_, ry_))
+
+    Sxi = quad(P[:, :-1, :-1], P[:, 1:, :-1], P[:, :-1, 1:], P[:, 1:, 1:])
+    Set = quad(P[:-1, :, :-1], P[:-1, :, 1:], P[1:, :, :-1], P[1:, :, 1:])
+    Sze = quad(P[:-1, :-1, :], P[1:, :-1, :], P[:-1, 1:, :], P[1:, 1:, :])
+    return Sxi, Set, Sze
+
+
+def _curl_edge_to_face(axi, aet, aze):
+    """Face circulation of edge 1-forms with the reference's orientation
+    (Z4_Lunar/src/operators/CTOperators.cpp:6-56, multiplier +1).  Edge arrays
+    cover interior edges: axi (ni, nj+1, nk+1), aet (ni+1, nj, nk+1),
+    aze (ni+1, nj+1, nk)."""
+    bxi = (aet[:, :, :-1] - aet[:, :, 1:]) + (aze[:, 1:, :] - aze[:, :-1, :])
+    bet = (axi[:, :, 1:] - axi[:, :, :-1]) + (aze[:-1, :, :] - aze[1:, :, :])
+    bze = (axi[:, :-1, :] - axi[:, 1:, :]) + (aet[1:, :, :] - aet[:-1, :, :])
+    return bxi, bet, bze
+
+
+def _embed(interior: np.ndarray, loc: int, ncell, nghost: int, ncomp: int) -> rst.FieldArray:
+    lo, hi = rst.extent(loc, ncell, nghost)
+    shape = (hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], ncomp)
+    a = np.zeros(shape)
+    g = nghost
+    s = interior.shape
+    a[g:g + s[0], g:g + s[1], g:g + s[2], :] = interior.reshape(s[0], s[1], s[2], ncomp)
+    return rst.FieldArray(lo, hi, a)
+
+
+def initial_state(spec: CaseSpec, rho0=1.0, p0=0.1, v0=(0.1, 0.0, 0.0), B0=(1.0, 0.0, 0.0),
+                  sigma=1e-3, seed=20261203, periodic=True, gamma=GAMMA) -> rst.RestartFile:
+    """Uniform state plus seeded Gaussian noise (numpy PCG64): rho and the
+    three velocity components per cell, then a random edge potential whose
+    face circulation is added to B, so div B stays at round-off.  U_H holds
+    (rho, rho u, rho v, rho w, E) with E = p/(gamma-1) + rho|u|^2/2 (the fluid
+    energy excludes the magnetic energy, Z4_Lunar/src/boundary/Boundary_Condition_Fluid.cpp:179).
+    Ghost layers are left at zero; the reader fills them by a Sync."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ng = spec.params["ngg"]
+    fields = {nm: rst.FieldRecord(nm, loc, nc, ng) for nm, loc, nc in
+              (("U_H", rst.CELL, 5), ("B_xi", rst.FACE_XI, 1), ("B_eta", rst.FACE_ET, 1), ("B_zeta", rst.FACE_ZE, 1))}
+    for blk in spec.blocks:
+        ni, nj, nk = blk.ncell
+        rho = rho0 + sigma * rng.standard_normal((ni, nj, nk))
+        vel = [v0[c] + sigma * rng.standard_normal((ni, nj, nk)) for c in range(3)]
+        E = p0 / (gamma - 1.0) + 0.5 * rho * (vel[0] ** 2 + vel[1] ** 2 + vel[2] ** 2)
+        U = np.stack([rho, rho * vel[0], rho * vel[1], rho * vel[2], E], axis=-1)
+        fields["U_H"].blocks.append(_embed(U, rst.CELL, (ni, nj, nk), ng, 5))
+        Sxi, Set, Sze = _face_area_vectors(blk.x, blk.y, blk.z)
+        b = np.asarray(B0, dtype=float)
+        bxi, bet, bze = Sxi @ b, Set @ b, Sze @ b
+        h2 = float(np.mean(np.linalg.norm(Sxi, axis=-1)))
+        if periodic:
+            a_u = [sigma * h2 * rng.standard_normal((ni, nj, nk)) for _ in range(3)]
+            axi = np.pad(a_u[0], ((0, 0), (0, 1), (0, 1)), mode="wrap")
+            aet = np.pad(a_u[1], ((0, 1), (0, 0), (0, 1)), mode="wrap")
+            aze = np.pad(a_u[2], ((0, 1), (0, 1), (0, 0)), mode="wrap")
+        else:
+            axi = sigma * h2 * rng.standard_normal((ni, nj + 1, nk + 1))
+            aet = sigma * h2 * rng.standard_normal((ni + 1, nj, nk + 1))
+            aze = sigma * h2 * rng.standard_normal((ni + 1, nj + 1, nk))
+        dxi, det, dze = _curl_edge_to_face(axi, aet, aze)
+        fields["B_xi"].blocks.append(_embed(bxi + dxi, rst.FACE_XI, (ni, nj, nk), ng, 1))
+        fields["B_eta"].blocks.append(_embed(bet + det, rst.FACE_ET, (ni, nj, nk), ng, 1))
+        fields["B_zeta"].blocks.append(_embed(bze + dze, rst.FACE_ZE, (ni, nj, nk), ng, 1))
+    return rst.RestartFile(0, 0.0, len(spec.blocks), fields)

@@ -1,0 +1,480 @@
+// Oracle harness around the reference Lunar solver (test infrastructure).
+//
+// Runs the reference's own set-up exactly as Z4_Lunar/main.cpp:23-212 does
+// (Param, Grid_Preprocess, build_topology, Field + the same field
+// registrations, Halo + the same halo registrations, LunarSolver), then,
+// instead of LunarSolver::Advance(), drives the solver's own member
+// functions and dumps fields in the MPCNSRST v1 layout
+// (src/5_io/IOModule_Bin.cpp:168-233) so the Python side reads one format.
+//
+// Usage (run inside a case directory holding ./CASE):
+//   ref_lunar geom  <out.bin>                      geometry + node coordinates
+//   ref_lunar run   <state.rst> <nsteps> <prefix>  state after each StepOnce
+//   ref_lunar probe <state.rst> <group> <out.bin>  index-encoded Sync(group)
+//   ref_lunar time  <state.rst> <nsteps>           wall time of the step loop
+//
+// The member functions are private in the reference; this translation unit
+// alone widens access to call them (the class layout is unchanged).
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <compare>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <functional>
+#include <iomanip>
+#include <iostream>
+#include <limits>
+#include <map>
+#include <memory>
+#include <set>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <unordered_map>
+#include <unordered_set>
+#include <utility>
+#include <vector>
+
+#include <mpi.h>
+#include <petscksp.h>
+#include <petscsnes.h>
+
+#define private public
+#define protected public
+#include "1_grid/1_MPCNS_Grid.h"
+#include "0_basic/MPI_WRAPPER.h"
+#include "2_topology/2_MPCNS_Topology.h"
+#include "3_field/2_MPCNS_Field.h"
+#include "4_halo/1_MPCNS_Halo.h"
+#include "LunarSolver.h"
+#include "2_topology/2_MPCNS_Topology_Equiv.h"
+#include "4_halo/1_MPCNS_Halo_EdgeOwner.h"
+#undef private
+#undef protected
+
+namespace
+{
+
+void wr_i32(std::ofstream &o, int32_t v) { o.write(reinterpret_cast<const char *>(&v), 4); }
+void wr_f64(std::ofstream &o, double v) { o.write(reinterpret_cast<const char *>(&v), 8); }
+void wr_str(std::ofstream &o, const std::string &s)
+{
+    wr_i32(o, int32_t(s.size()));
+    o.write(s.data(), std::streamsize(s.size()));
+}
+
+// location code as the restart writer stores it (src/5_io/IOModule_Bin.cpp:62-85)
+int loc_code(StaggerLocation l)
+{
+    switch (l)
+    {
+    case StaggerLocation::Cell:
+        return 0;
+    case StaggerLocation::FaceXi:
+        return 1;
+    case StaggerLocation::FaceEt:
+        return 2;
+    case StaggerLocation::FaceZe:
+        return 3;
+    case StaggerLocation::EdgeXi:
+        return 4;
+    case StaggerLocation::EdgeEt:
+        return 5;
+    case StaggerLocation::EdgeZe:
+        return 6;
+    default:
+        return 7;
+    }
+}
+
+// One dump entry: either a registered field or a node-coordinate array.
+struct DumpItem
+{
+    std::string name;
+    int loc;
+    int ncomp;
+    int nghost;
+    std::function<void(int ib, Int3 &lo, Int3 &hi, bool &active)> extent;
+    std::function<double(int ib, int i, int j, int k, int m)> value;
+};
+
+void write_dump(const std::string &path, int step, double time, int nblock, const std::vector<DumpItem> &items)
+{
+    std::ofstream out(path, std::ios::binary);
+    if (!out)
+    {
+        std::fprintf(stderr, "cannot open %s\n", path.c_str());
+        std::exit(2);
+    }
+    const char magic[8] = {'M', 'P', 'C', 'N', 'S', 'R', 'S', 'T'};
+    out.write(magic, 8);
+    wr_i32(out, 1);
+    wr_i32(out, step);
+    wr_f64(out, time);
+    wr_i32(out, nblock);
+    wr_i32(out, int32_t(items.size()));
+    for (const auto &it : items)
+    {
+        wr_str(out, it.name);
+        wr_i32(out, it.loc);
+        wr_i32(out, it.ncomp);
+        wr_i32(out, it.nghost);
+        for (int ib = 0; ib < nblock; ++ib)
+        {
+            Int3 lo{}, hi{};
+            bool active = false;
+            it.extent(ib, lo, hi, active);
+            wr_i32(out, lo.i);
+            wr_i32(out, lo.j);
+            wr_i32(out, lo.k);
+            wr_i32(out, hi.i);
+            wr_i32(out, hi.j);
+            wr_i32(out, hi.k);
+            wr_i32(out, active ? 1 : 0);
+            if (!active)
+                continue;
+            for (int i = lo.i; i < hi.i; ++i)
+                for (int j = lo.j; j < hi.j; ++j)
+                    for (int k = lo.k; k < hi.k; ++k)
+                        for (int m = 0; m < it.ncomp; ++m)
+                            wr_f64(out, it.value(ib, i, j, k, m));
+        }
+    }
+}
+
+DumpItem field_item(Field *fld, const std::string &name)
+{
+    const int fid = fld->field_id(name);
+    const FieldDescriptor &d = fld->descriptor(fid);
+    DumpItem it;
+    it.name = name;
+    it.loc = loc_code(d.location);
+    it.ncomp = d.ncomp;
+    it.nghost = d.nghost;
+    it.extent = [fld, fid](int ib, Int3 &lo, Int3 &hi, bool &active)
+    {
+        FieldBlock &fb = fld->field(fid, ib);
+        lo = fb.get_lo();
+        hi = fb.get_hi();
+        active = fb.is_allocated();
+    };
+    it.value = [fld, fid](int ib, int i, int j, int k, int m) { return fld->field(fid, ib)(i, j, k, m); };
+    return it;
+}
+
+// Node coordinates with the reference's ghost nodes (ngg+1 layers), as a
+// pseudo-field with location code 1 (Node) and 3 components (x, y, z).
+DumpItem node_item(Grid *grd)
+{
+    DumpItem it;
+    it.name = "X_node";
+    it.loc = loc_code(StaggerLocation::Node);
+    it.ncomp = 3;
+    it.nghost = grd->ngg + 1;
+    it.extent = [grd](int ib, Int3 &lo, Int3 &hi, bool &active)
+    {
+        const Block &b = grd->grids(ib);
+        const int g = grd->ngg + 1;
+        lo = Int3{-g, -g, -g};
+        hi = Int3{b.mx + 1 + g, b.my + 1 + g, b.mz + 1 + g};
+        active = true;
+    };
+    it.value = [grd](int ib, int i, int j, int k, int m)
+    {
+        Block &b = grd->grids(ib);
+        if (m == 0)
+            return b.x(i, j, k);
+        if (m == 1)
+            return b.y(i, j, k);
+        return b.z(i, j, k);
+    };
+    return it;
+}
+
+struct Harness
+{
+    Param *par = nullptr;
+    Grid *grd = nullptr;
+    TOPO::Topology topology;
+    TOPO::TopologyEquiv topo_equiv;
+    Field *fld = nullptr;
+    Halo *hal = nullptr;
+    HALO_OWNER::EdgeOwnerSyncPattern edge_owner_pattern;
+    std::unique_ptr<LunarSolver> solver;
+
+    // Z4_Lunar/main.cpp:43-212, unchanged in substance.
+    void setup()
+    {
+        int myid = 0;
+        par = new Param;
+        par->ReadParam(myid);
+        grd = new Grid;
+        grd->Grid_Preprocess(par);
+        topology = TOPO::build_topology(*grd, myid, par->GetInt("dimension"));
+        TOPO::build_topology_equiv(topology, *grd, myid, par->GetInt("dimension"), topo_equiv);
+        const int ngg = par->GetInt("ngg");
+        fld = new Field(grd, par, ngg);
+        fld->register_field({"U_H", StaggerLocation::Cell, 5, ngg, "Fluid"});
+        fld->register_field({"B_xi", StaggerLocation::FaceXi, 1, ngg});
+        fld->register_field({"B_eta", StaggerLocation::FaceEt, 1, ngg});
+        fld->register_field({"B_zeta", StaggerLocation::FaceZe, 1, ngg});
+        fld->register_field({"E_xi", StaggerLocation::EdgeXi, 1, ngg});
+        fld->register_field({"E_eta", StaggerLocation::EdgeEt, 1, ngg});
+        fld->register_field({"E_zeta", StaggerLocation::EdgeZe, 1, ngg});
+        fld->register_field({"Ehall_xi", StaggerLocation::EdgeXi, 1, ngg});
+        fld->register_field({"Ehall_eta", StaggerLocation::EdgeEt, 1, ngg});
+        fld->register_field({"Ehall_zeta", StaggerLocation::EdgeZe, 1, ngg});
+        fld->register_field({"Eres_xi", StaggerLocation::EdgeXi, 1, ngg});
+        fld->register_field({"Eres_eta", StaggerLocation::EdgeEt, 1, ngg});
+        fld->register_field({"Eres_zeta", StaggerLocation::EdgeZe, 1, ngg});
+        fld->register_field({"Eface_xi", StaggerLocation::FaceXi, 3, ngg});
+        fld->register_field({"Eface_eta", StaggerLocation::FaceEt, 3, ngg});
+        fld->register_field({"Eface_zeta", StaggerLocation::FaceZe, 3, ngg});
+        fld->register_field({"J_xi", StaggerLocation::EdgeXi, 1, ngg});
+        fld->register_field({"J_eta", StaggerLocation::EdgeEt, 1, ngg});
+        fld->register_field({"J_zeta", StaggerLocation::EdgeZe, 1, ngg});
+        fld->register_field({"J_cell", StaggerLocation::Cell, 3, ngg});
+        fld->register_field({"dE_xi", StaggerLocation::EdgeXi, 1, ngg});
+        fld->register_field({"dE_eta", StaggerLocation::EdgeEt, 1, ngg});
+        fld->register_field({"dE_zeta", StaggerLocation::EdgeZe, 1, ngg});
+        fld->register_field({"dB_xi", StaggerLocation::FaceXi, 1, ngg});
+        fld->register_field({"dB_eta", StaggerLocation::FaceEt, 1, ngg});
+        fld->register_field({"dB_zeta", StaggerLocation::FaceZe, 1, ngg});
+        fld->register_field({"dJ_xi", StaggerLocation::EdgeXi, 1, ngg});
+        fld->register_field({"dJ_eta", StaggerLocation::EdgeEt, 1, ngg});
+        fld->register_field({"dJ_zeta", StaggerLocation::EdgeZe, 1, ngg});
+        fld->register_field({"dJ_cell", StaggerLocation::Cell, 3, ngg});
+        fld->register_field({"dEpre_xi", StaggerLocation::EdgeXi, 1, ngg});
+        fld->register_field({"dEpre_eta", StaggerLocation::EdgeEt, 1, ngg});
+        fld->register_field({"dEpre_zeta", StaggerLocation::EdgeZe, 1, ngg});
+        fld->register_field({"Badd_xi", StaggerLocation::FaceXi, 1, ngg});
+        fld->register_field({"Badd_eta", StaggerLocation::FaceEt, 1, ngg});
+        fld->register_field({"Badd_zeta", StaggerLocation::FaceZe, 1, ngg});
+        fld->register_field({"B_cell", StaggerLocation::Cell, 3, ngg});
+        fld->register_field({"Bind_cell", StaggerLocation::Cell, 3, ngg});
+        fld->register_field({"U_plus", StaggerLocation::Cell, 3, ngg});
+        fld->register_field(FieldDescriptor{"PV_H", StaggerLocation::Cell, 5, ngg, "Fluid"});
+        fld->register_field({"F_xi", StaggerLocation::FaceXi, 5, 0, "Fluid"});
+        fld->register_field({"F_eta", StaggerLocation::FaceEt, 5, 0, "Fluid"});
+        fld->register_field({"F_zeta", StaggerLocation::FaceZe, 5, 0, "Fluid"});
+        fld->register_field(FieldDescriptor{"divB", StaggerLocation::Cell, 1, 1});
+        fld->register_field(FieldDescriptor{"RHS_H", StaggerLocation::Cell, 5, 0, "Fluid"});
+        fld->register_field(FieldDescriptor{"RHS_B_xi", StaggerLocation::FaceXi, 1, 0});
+        fld->register_field(FieldDescriptor{"RHS_B_eta", StaggerLocation::FaceEt, 1, 0});
+        fld->register_field(FieldDescriptor{"RHS_B_zeta", StaggerLocation::FaceZe, 1, 0});
+        fld->register_field(FieldDescriptor{"RHS_Bres_xi", StaggerLocation::FaceXi, 1, 0});
+        fld->register_field(FieldDescriptor{"RHS_Bres_eta", StaggerLocation::FaceEt, 1, 0});
+        fld->register_field(FieldDescriptor{"RHS_Bres_zeta", StaggerLocation::FaceZe, 1, 0});
+
+        hal = new Halo(fld, &topology);
+        for (const char *fn : {"U_H", "U_plus", "B_xi", "B_eta", "B_zeta", "Badd_xi", "Badd_eta", "Badd_zeta",
+                               "E_xi", "E_eta", "E_zeta", "J_xi", "J_eta", "J_zeta", "Ehall_xi", "Ehall_eta",
+                               "Ehall_zeta", "Eres_xi", "Eres_eta", "Eres_zeta", "dB_xi", "dB_eta", "dB_zeta",
+                               "dE_xi", "dE_eta", "dE_zeta", "dJ_xi", "dJ_eta", "dJ_zeta", "dJ_cell"})
+        {
+            std::string s(fn);
+            hal->register_halo_field(s, HaloLevel::Vertex);
+        }
+        hal->build_registered_patterns();
+        HALO_OWNER::build_edge_owner_sync_pattern(topo_equiv, edge_owner_pattern);
+
+        solver = std::make_unique<LunarSolver>(grd, &topology, fld, hal, par, &topo_equiv, &edge_owner_pattern);
+    }
+
+    // Load U_H and B_xi/B_eta/B_zeta from an MPCNSRST file, then fill their
+    // ghosts with the reference's own Sync so every derived field starts
+    // from a consistent state.
+    void load_state(const std::string &path)
+    {
+        solver->io_.Change_RestartPath(path);
+        solver->io_.ReadRestartBinFile();
+        solver->lunar_bound_.Sync("Ucell");
+        solver->lunar_bound_.Sync("Bface");
+    }
+};
+
+const std::vector<std::string> &geom_fields()
+{
+    static const std::vector<std::string> v = {
+        "Jac", "JDxi", "JDet", "JDze", "beta_xi", "beta_eta", "beta_zeta", "alpha_xi", "alpha_eta",
+        "alpha_zeta", "dr_xi", "dr_eta", "dr_zeta", "Area_xi", "Area_eta", "Area_zeta", "dl_xi", "dl_eta",
+        "dl_zeta", "Bcell_from_Bface_w", "Jcell_from_Jedge_w", "Badd_xi", "Badd_eta", "Badd_zeta"};
+    return v;
+}
+
+const std::vector<std::string> &state_fields()
+{
+    static const std::vector<std::string> v = {
+        "U_H", "B_xi", "B_eta", "B_zeta", "PV_H", "U_plus", "B_cell", "Bind_cell", "J_xi", "J_eta", "J_zeta",
+        "J_cell", "E_xi", "E_eta", "E_zeta", "Eface_xi", "Eface_eta", "Eface_zeta", "RHS_H", "RHS_B_xi",
+        "RHS_B_eta", "RHS_B_zeta", "divB", "Eres_xi", "Eres_eta", "Eres_zeta"};
+    return v;
+}
+
+int cmd_geom(Harness &h, const std::string &out)
+{
+    std::vector<DumpItem> items;
+    for (const auto &n : geom_fields())
+        items.push_back(field_item(h.fld, n));
+    items.push_back(node_item(h.grd));
+    write_dump(out, 0, 0.0, h.fld->num_blocks(), items);
+    return 0;
+}
+
+void dump_state(Harness &h, const std::string &path)
+{
+    std::vector<DumpItem> items;
+    for (const auto &n : state_fields())
+        items.push_back(field_item(h.fld, n));
+    // dt of the step just taken, as a 1x1x1 pseudo-field
+    DumpItem dti;
+    dti.name = "dt";
+    dti.loc = -1;
+    dti.ncomp = 1;
+    dti.nghost = 0;
+    LunarSolver *s = h.solver.get();
+    dti.extent = [](int, Int3 &lo, Int3 &hi, bool &active)
+    {
+        lo = Int3{0, 0, 0};
+        hi = Int3{1, 1, 1};
+        active = true;
+    };
+    dti.value = [s](int, int, int, int, int) { return s->dt; };
+    items.push_back(dti);
+    write_dump(path, s->run_data_->step, s->run_data_->time, h.fld->num_blocks(), items);
+}
+
+int cmd_run(Harness &h, const std::string &state, int nsteps, const std::string &prefix)
+{
+    h.load_state(state);
+    LunarSolver &s = *h.solver;
+    s.UpdateDerivedFields_();
+    dump_state(h, prefix + "_0000.bin");
+    for (int n = 1; n <= nsteps; ++n)
+    {
+        s.StepOnce();
+        char buf[32];
+        std::snprintf(buf, sizeof(buf), "_%04d.bin", n);
+        dump_state(h, prefix + buf);
+    }
+    return 0;
+}
+
+// Every field of the group is overwritten with value = block*2^32 + AoS
+// offset + 1 (exact in a double), then the reference Sync(group) runs; the
+// dump therefore records, for every point, which original point it was copied
+// from (or a non-integer value where a handler computed it).
+int cmd_probe(Harness &h, const std::string &state, const std::string &group, const std::string &out)
+{
+    h.load_state(state);
+    LunarSolver &s = *h.solver;
+    s.UpdateDerivedFields_();
+    auto git = s.lunar_bound_.groups_.find(group);
+    if (git == s.lunar_bound_.groups_.end())
+    {
+        std::fprintf(stderr, "unknown group %s\n", group.c_str());
+        return 2;
+    }
+    std::vector<DumpItem> items;
+    for (const auto &fn : git->second.fields)
+    {
+        const int fid = h.fld->field_id(fn);
+        const int ncomp = h.fld->descriptor(fid).ncomp;
+        for (int ib = 0; ib < h.fld->num_blocks(); ++ib)
+        {
+            FieldBlock &fb = h.fld->field(fid, ib);
+            if (!fb.is_allocated())
+                continue;
+            const Int3 lo = fb.get_lo(), hi = fb.get_hi();
+            const int64_t nj = hi.j - lo.j, nk = hi.k - lo.k;
+            for (int i = lo.i; i < hi.i; ++i)
+                for (int j = lo.j; j < hi.j; ++j)
+                    for (int k = lo.k; k < hi.k; ++k)
+                        for (int m = 0; m < ncomp; ++m)
+                        {
+                            const int64_t off = (((int64_t(i - lo.i) * nj + (j - lo.j)) * nk + (k - lo.k)) * ncomp + m);
+                            fb(i, j, k, m) = double(int64_t(ib) * (int64_t(1) << 32) + off + 1);
+                        }
+        }
+        items.push_back(field_item(h.fld, fn));
+    }
+    s.lunar_bound_.Sync(group);
+    write_dump(out, 0, 0.0, h.fld->num_blocks(), items);
+    return 0;
+}
+
+int cmd_time(Harness &h, const std::string &state, int nsteps)
+{
+    h.load_state(state);
+    LunarSolver &s = *h.solver;
+    s.UpdateDerivedFields_();
+    int64_t cells = 0;
+    for (int ib = 0; ib < h.fld->num_blocks(); ++ib)
+    {
+        FieldBlock &U = h.fld->field(s.fid_.fid_U_H, ib);
+        const Int3 lo = U.inner_lo(), hi = U.inner_hi();
+        cells += int64_t(hi.i - lo.i) * (hi.j - lo.j) * (hi.k - lo.k);
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int n = 0; n < nsteps; ++n)
+        s.StepOnce();
+    const auto t1 = std::chrono::steady_clock::now();
+    const double sec = std::chrono::duration<double>(t1 - t0).count();
+    std::printf("{\"cells\": %lld, \"steps\": %d, \"seconds\": %.9f, \"cell_updates_per_s\": %.6e}\n",
+                (long long)cells, nsteps, sec, double(cells) * nsteps / sec);
+    return 0;
+}
+
+} // namespace
+
+int main(int argc, char **argv)
+{
+    if (argc < 3)
+    {
+        std::fprintf(stderr, "usage: ref_lunar geom|run|probe|time ...\n");
+        return 2;
+    }
+    PARALLEL::mpi_initial(argc, argv);
+    PetscInitialize(&argc, &argv, nullptr, nullptr);
+    int rc = 0;
+    {
+        // the reference prints progress on stdout; keep stdout for results
+        std::streambuf *saved = std::cout.rdbuf();
+        std::ofstream sink("ref_harness.log");
+        std::cout.rdbuf(sink.rdbuf());
+        Harness h;
+        h.setup();
+        const std::string cmd = argv[1];
+        if (cmd == "geom")
+            rc = cmd_geom(h, argv[2]);
+        else if (cmd == "run" && argc >= 5)
+            rc = cmd_run(h, argv[2], std::atoi(argv[3]), argv[4]);
+        else if (cmd == "probe" && argc >= 5)
+            rc = cmd_probe(h, argv[2], argv[3], argv[4]);
+        else if (cmd == "time" && argc >= 4)
+        {
+            std::cout.rdbuf(saved);
+            std::streambuf *s2 = std::cout.rdbuf();
+            // timing result goes to stdout via printf; solver chatter to the log
+            std::cout.rdbuf(sink.rdbuf());
+            rc = cmd_time(h, argv[2], std::atoi(argv[3]));
+            (void)s2;
+        }
+        else
+        {
+            std::fprintf(stderr, "bad command\n");
+            rc = 2;
+        }
+        std::cout.rdbuf(saved);
+    }
+    PetscFinalize();
+    PARALLEL::mpi_finalize();
+    return rc;
+}
