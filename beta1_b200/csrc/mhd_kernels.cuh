@@ -1,0 +1,43 @@
+// Kernel declarations shared by the C-ABI implementation.
+#pragma once
+
+#include "mhd_layout.cuh"
+#include "../../include/beta1_mhd.h"
+
+namespace mhd
+{
+
+// Nondimensional constants passed by value to the kernels.
+struct Consts
+{
+    double gamma;
+    double cfl;
+    double inver_MA2;
+    double mom_hall;
+    double state_coeff;
+    double M_H, M_ref;
+    double ne_floor;
+};
+
+__global__ void k_fluid_rhs(const BlockView *bvs, Consts c, int64_t maxpts);
+__global__ void k_eface(const BlockView *bvs);
+__global__ void k_eedge(const BlockView *bvs, int G);
+__global__ void k_curl_e2f(const BlockView *bvs, int fE0, int fR0, int fB0, double mult, const double *dtp,
+                           double dtdiv);
+__global__ void k_update_u(const BlockView *bvs, const double *dtp);
+__global__ void k_bcell(const BlockView *bvs);
+__global__ void k_jedge(const BlockView *bvs, int fB0, int fJ0, double mult);
+__global__ void k_jcell(const BlockView *bvs);
+__global__ void k_pv_uplus_dt(const BlockView *bvs, Consts c, unsigned long long *dt_key);
+__global__ void k_begin_step(const unsigned long long *dt_key, double *dt, int *err, double dt_abort);
+__global__ void k_arm_dt(unsigned long long *dt_key);
+__global__ void k_end_step(const double *dt, double *time, long long *step);
+__global__ void k_gather(double *pool, const uint64_t *dst, const uint64_t *src, int64_t n);
+__global__ void k_gather_stage(double *tmp, const double *pool, const uint64_t *src, int64_t n);
+__global__ void k_scatter_stage(double *pool, const double *tmp, const uint64_t *dst, int64_t n);
+__global__ void k_aos_to_soa(const BlockView *bvs, int blk, int fid, int ncomp, int lo0, int lo1, int lo2, int n0,
+                             int n1, int n2, const double *aos);
+__global__ void k_soa_to_aos(const BlockView *bvs, int blk, int fid, int ncomp, int lo0, int lo1, int lo2, int n0,
+                             int n1, int n2, double *aos);
+
+} // namespace mhd

@@ -1,0 +1,734 @@
+// FP64 hot-path kernels for sm_100a.
+//
+// Each kernel evaluates one stage of LunarSolver::StepOnce with the same
+// floating-point operation order as the reference's loops; this translation
+// unit is compiled with -fmad=false so that no multiply-add is contracted,
+// and the results agree with the reference bit for bit.  The stencils are
+// HBM-bound (about 1-3 flop per byte), so they run on the CUDA cores with
+// coalesced k-fastest accesses; no tensor cores are involved.
+#include "mhd_kernels.cuh"
+
+#include <cfloat>
+#include <cmath>
+
+namespace mhd
+{
+
+// std::max / std::min semantics (return the first argument unless the
+// second compares greater / smaller), which differ from fmax on NaN.
+__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
+
+__device__ __forceinline__ double at(const BlockView &b, int f, int m, int i, int j, int k)
+{
+    return b.f[f][m * b.vol + pidx(b, i, j, k)];
+}
+
+// Thread -> (block, i, j, k) over a box [lo, lo + n) with k fastest.
+__device__ __forceinline__ bool box_point(const int lo[3], const int n[3], int64_t t, int &i, int &j, int &k)
+{
+    const int64_t tot = int64_t(n[0]) * n[1] * n[2];
+    if (t >= tot)
+        return false;
+    k = lo[2] + int(t % n[2]);
+    t /= n[2];
+    j = lo[1] + int(t % n[1]);
+    i = lo[0] + int(t / n[1]);
+    return true;
+}
+
+// Box of a location on block b: inner range [0, n + plus) widened by g.
+__device__ __forceinline__ void loc_box(const BlockView &b, int loc, int g, int lo[3], int n[3])
+{
+    int pi, pj, pk;
+    loc_plus(loc, pi, pj, pk);
+    lo[0] = lo[1] = lo[2] = -g;
+    n[0] = b.ni + pi + 2 * g;
+    n[1] = b.nj + pj + 2 * g;
+    n[2] = b.nk + pk + 2 * g;
+}
+
+// ---------------------------------------------------------------------------
+// Scheme_U_ + AddSourceToRHS_Fluid
+// (Z4_Lunar/src/physics/LunarSolver_FluidRHS.cpp:3-201, :528-568)
+// ---------------------------------------------------------------------------
+
+// One Rusanov face flux (Reconstruction_Rusanov, piecewise-constant states)
+__device__ __forceinline__ void rusanov_face(const BlockView &b, const Consts &c, int dir, int i, int j, int k,
+                                             double out[5])
+{
+    const int JD = (dir == 0) ? F_JDxi : (dir == 1) ? F_JDeta : F_JDzeta;
+    const int64_t p = pidx(b, i, j, k);
+    const double k1 = b.f[JD][p];
+    const double k2 = b.f[JD][b.vol + p];
+    const double k3 = b.f[JD][2 * b.vol + p];
+    const int iL = i - (dir == 0), jL = j - (dir == 1), kL = k - (dir == 2);
+    const int64_t pL = pidx(b, iL, jL, kL);
+    const double *U = b.f[F_U];
+    const double *PV = b.f[F_PV];
+    const int64_t v = b.vol;
+
+    const double rhoL = U[pL], uL = PV[pL], vL = PV[v + pL], wL = PV[2 * v + pL], pLp = PV[3 * v + pL];
+    const double rhoR = U[p], uR = PV[p], vR = PV[v + p], wR = PV[2 * v + p], pR = PV[3 * v + p];
+    const double g = c.gamma;
+
+    double UL[5], UR[5];
+    UL[0] = rhoL;
+    UL[1] = rhoL * uL;
+    UL[2] = rhoL * vL;
+    UL[3] = rhoL * wL;
+    UL[4] = pLp / (g - 1.0) + 0.5 * rhoL * (uL * uL + vL * vL + wL * wL);
+    UR[0] = rhoR;
+    UR[1] = rhoR * uR;
+    UR[2] = rhoR * vR;
+    UR[3] = rhoR * wR;
+    UR[4] = pR / (g - 1.0) + 0.5 * rhoR * (uR * uR + vR * vR + wR * wR);
+
+    const double kk = (k1 * k1 + k2 * k2 + k3 * k3);
+    const double uvwL = k1 * uL + k2 * vL + k3 * wL;
+    const double uvwR = k1 * uR + k2 * vR + k3 * wR;
+    const double cL = sqrt(smax(0.0, g * pLp / smax(rhoL, 1e-30)));
+    const double cR = sqrt(smax(0.0, g * pR / smax(rhoR, 1e-30)));
+    const double radL = fabs(uvwL) + cL * sqrt(kk);
+    const double radR = fabs(uvwR) + cR * sqrt(kk);
+    const double rad = smax(radL, radR);
+
+    const double rhoeL = pLp / (g - 1.0) + 0.5 * rhoL * (uL * uL + vL * vL + wL * wL);
+    const double rhoeR = pR / (g - 1.0) + 0.5 * rhoR * (uR * uR + vR * vR + wR * wR);
+    double FL[5], FR[5];
+    FL[0] = rhoL * uvwL;
+    FL[1] = rhoL * uvwL * uL + k1 * pLp;
+    FL[2] = rhoL * uvwL * vL + k2 * pLp;
+    FL[3] = rhoL * uvwL * wL + k3 * pLp;
+    FL[4] = uvwL * (rhoeL + pLp);
+    FR[0] = rhoR * uvwR;
+    FR[1] = rhoR * uvwR * uR + k1 * pR;
+    FR[2] = rhoR * uvwR * vR + k2 * pR;
+    FR[3] = rhoR * uvwR * wR + k3 * pR;
+    FR[4] = uvwR * (rhoeR + pR);
+#pragma unroll
+    for (int m = 0; m < 5; ++m)
+        out[m] = 0.5 * (FL[m] + FR[m]) - 0.5 * rad * (UR[m] - UL[m]);
+}
+
+__global__ void k_fluid_rhs(const BlockView *__restrict__ bvs, Consts c, int64_t /*maxpts*/)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    int lo[3], n[3];
+    loc_box(b, LOC_CELL, 0, lo, n);
+    int i, j, k;
+    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+        return;
+    const int64_t p = pidx(b, i, j, k);
+    const int64_t v = b.vol;
+    double Fm[5], Fp[5];
+    double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const double invJ = 1.0 / b.f[F_Jac][p];
+
+    rusanov_face(b, c, 0, i, j, k, Fm);
+    rusanov_face(b, c, 0, i + 1, j, k, Fp);
+    double dx[5];
+#pragma unroll
+    for (int m = 0; m < 5; ++m)
+        dx[m] = Fp[m] - Fm[m];
+    rusanov_face(b, c, 1, i, j, k, Fm);
+    rusanov_face(b, c, 1, i, j + 1, k, Fp);
+    double dy[5];
+#pragma unroll
+    for (int m = 0; m < 5; ++m)
+        dy[m] = Fp[m] - Fm[m];
+    rusanov_face(b, c, 2, i, j, k, Fm);
+    rusanov_face(b, c, 2, i, j, k + 1, Fp);
+#pragma unroll
+    for (int m = 0; m < 5; ++m)
+    {
+        r[m] -= dx[m] * invJ;
+        r[m] -= dy[m] * invJ;
+        r[m] -= (Fp[m] - Fm[m]) * invJ;
+    }
+
+    // J x B force with the Hall_Num_Limiter weight (LunarSolver_Tools.cpp:47-56)
+    const double rho = b.f[F_U][p];
+    const double n_true = smax(rho, 0.0) / c.M_H * c.M_ref;
+    const double ne_eff = sqrt(n_true * n_true + c.ne_floor * c.ne_floor);
+    const double w = n_true / ne_eff;
+    const double fc = c.mom_hall * w;
+    const double *J = b.f[F_Jcell];
+    const double *B = b.f[F_Bcell];
+    const double jx = J[p], jy = J[v + p], jz = J[2 * v + p];
+    const double bx = B[p], by = B[v + p], bz = B[2 * v + p];
+    const double jxb_x = jy * bz - jz * by;
+    const double jxb_y = jz * bx - jx * bz;
+    const double jxb_z = jx * by - jy * bx;
+    const double *PV = b.f[F_PV];
+    r[1] += fc * jxb_x;
+    r[2] += fc * jxb_y;
+    r[3] += fc * jxb_z;
+    r[4] += fc * (jxb_x * PV[p] + jxb_y * PV[v + p] + jxb_z * PV[2 * v + p]);
+
+    double *R = b.f[F_RHS];
+#pragma unroll
+    for (int m = 0; m < 5; ++m)
+        R[m * v + p] = r[m];
+}
+
+// ---------------------------------------------------------------------------
+// AssembleOneDirectionEMF_ (Z4_Lunar/src/physics/LunarSolver_MagExplicit_Ideal.cpp:348-496)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ double face_ind(const BlockView &b, int axis, int i, int j, int k)
+{
+    const int F = (axis == 0) ? F_Bxi : (axis == 1) ? F_Beta : F_Bzeta;
+    return b.f[F][pidx(b, i, j, k)];
+}
+__device__ __forceinline__ double face_tot(const BlockView &b, int axis, int i, int j, int k)
+{
+    const int F = (axis == 0) ? F_Bxi : (axis == 1) ? F_Beta : F_Bzeta;
+    const int A = (axis == 0) ? F_Baddxi : (axis == 1) ? F_Baddeta : F_Baddzeta;
+    const int64_t p = pidx(b, i, j, k);
+    return b.f[F][p] + b.f[A][p];
+}
+// contravariant velocity of a cell along `axis` (cell_u_contra)
+__device__ __forceinline__ double u_contra(const BlockView &b, int axis, int i, int j, int k)
+{
+    const int JD = (axis == 0) ? F_JDxi : (axis == 1) ? F_JDeta : F_JDzeta;
+    const int64_t p = pidx(b, i, j, k);
+    const int64_t q = pidx(b, i + (axis == 0), j + (axis == 1), k + (axis == 2));
+    const int64_t v = b.vol;
+    const double *M = b.f[JD];
+    const double kx = 0.5 * (M[p] + M[q]);
+    const double ky = 0.5 * (M[v + p] + M[v + q]);
+    const double kz = 0.5 * (M[2 * v + p] + M[2 * v + q]);
+    const double inv_jac = 1.0 / (fabs(b.f[F_Jac][p]) + 1.0e-30);
+    const double *Up = b.f[F_Uplus];
+    return (kx * Up[p] + ky * Up[v + p] + kz * Up[2 * v + p]) * inv_jac;
+}
+
+__device__ __forceinline__ double emf_flux(const BlockView &b, int ba, int fa, int iL, int jL, int kL, int iR, int jR,
+                                           int kR, double bff)
+{
+    const int sa = (ba == 0), sb = (ba == 1), sc = (ba == 2);
+    const double btL = 0.5 * (face_tot(b, ba, iL, jL, kL) + face_tot(b, ba, iL + sa, jL + sb, kL + sc));
+    const double btR = 0.5 * (face_tot(b, ba, iR, jR, kR) + face_tot(b, ba, iR + sa, jR + sb, kR + sc));
+    const double biL = 0.5 * (face_ind(b, ba, iL, jL, kL) + face_ind(b, ba, iL + sa, jL + sb, kL + sc));
+    const double biR = 0.5 * (face_ind(b, ba, iR, jR, kR) + face_ind(b, ba, iR + sa, jR + sb, kR + sc));
+    const double ufL = u_contra(b, fa, iL, jL, kL);
+    const double ufR = u_contra(b, fa, iR, jR, kR);
+    const double ubL = u_contra(b, ba, iL, jL, kL);
+    const double ubR = u_contra(b, ba, iR, jR, kR);
+    const double GL = ufL * btL - ubL * bff;
+    const double GR = ufR * btR - ubR * bff;
+    const double radius = smax(fabs(ufL), fabs(ufR));
+    return 0.5 * (GL + GR) - 0.5 * radius * (biR - biL);
+}
+
+// blockIdx.z = flux axis
+__global__ void k_eface(const BlockView *__restrict__ bvs)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    const int fa = blockIdx.z;
+    int lo[3], n[3];
+    loc_box(b, LOC_FXI + fa, 0, lo, n);
+    int i, j, k;
+    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+        return;
+    const int iL = i - (fa == 0), jL = j - (fa == 1), kL = k - (fa == 2);
+    const double bff = face_tot(b, fa, i, j, k);
+    double e0 = 0.0, e1 = 0.0, e2 = 0.0;
+    if (fa == 0)
+    {
+        const double G_eta_xi = emf_flux(b, 1, 0, iL, jL, kL, i, j, k, bff);
+        const double G_zeta_xi = emf_flux(b, 2, 0, iL, jL, kL, i, j, k, bff);
+        e1 = G_zeta_xi;
+        e2 = -G_eta_xi;
+    }
+    else if (fa == 1)
+    {
+        const double G_xi_eta = emf_flux(b, 0, 1, iL, jL, kL, i, j, k, bff);
+        const double G_zeta_eta = emf_flux(b, 2, 1, iL, jL, kL, i, j, k, bff);
+        e0 = -G_zeta_eta;
+        e2 = G_xi_eta;
+    }
+    else
+    {
+        const double G_xi_zeta = emf_flux(b, 0, 2, iL, jL, kL, i, j, k, bff);
+        const double G_eta_zeta = emf_flux(b, 1, 2, iL, jL, kL, i, j, k, bff);
+        e0 = G_eta_zeta;
+        e1 = -G_xi_zeta;
+    }
+    const int F = F_Efxi + fa;
+    const int64_t p = pidx(b, i, j, k);
+    b.f[F][p] = e0;
+    b.f[F][b.vol + p] = e1;
+    b.f[F][2 * b.vol + p] = e2;
+}
+
+// ---------------------------------------------------------------------------
+// AssembleEdgeEMF_FromFaceE_Ideal_ (LunarSolver_MagExplicit_Ideal.cpp:53-287)
+// with the zeroing of E_edge over the whole array (LunarSolver_MagneticRHS.cpp:9-28)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ double max_abs_u4(const BlockView &b, int axis, int i0, int j0, int k0, int i1, int j1,
+                                             int k1, int i2, int j2, int k2, int i3, int j3, int k3)
+{
+    double a = 0.0;
+    a = smax(a, fabs(u_contra(b, axis, i0, j0, k0)));
+    a = smax(a, fabs(u_contra(b, axis, i1, j1, k1)));
+    a = smax(a, fabs(u_contra(b, axis, i2, j2, k2)));
+    a = smax(a, fabs(u_contra(b, axis, i3, j3, k3)));
+    return a;
+}
+
+// blockIdx.z = edge axis; covers the full array (ghost edges are zeroed)
+__global__ void k_eedge(const BlockView *__restrict__ bvs, int G)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    const int ea = blockIdx.z;
+    int lo[3], n[3];
+    loc_box(b, LOC_EXI + ea, G, lo, n);
+    int i, j, k;
+    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+        return;
+    int pi, pj, pk;
+    loc_plus(LOC_EXI + ea, pi, pj, pk);
+    const bool inner = (i >= 0 && j >= 0 && k >= 0 && i < b.ni + pi && j < b.nj + pj && k < b.nk + pk);
+    const double Cuct = 0.5;
+    double E = 0.0;
+    if (inner)
+    {
+        if (ea == 0)
+        {
+            const double *Fe = b.f[F_Efeta];
+            const double *Fz = b.f[F_Efzeta];
+            const double Ec = 0.25 * (Fe[pidx(b, i, j, k)] + Fe[pidx(b, i, j, k - 1)] + Fz[pidx(b, i, j, k)] +
+                                      Fz[pidx(b, i, j - 1, k)]);
+            const double a_eta = max_abs_u4(b, 1, i, j, k, i, j - 1, k, i, j, k - 1, i, j - 1, k - 1);
+            const double a_zeta = max_abs_u4(b, 2, i, j, k, i, j - 1, k, i, j, k - 1, i, j - 1, k - 1);
+            const double dBzeta_eta = face_ind(b, 2, i, j, k) - face_ind(b, 2, i, j - 1, k);
+            const double dBeta_zeta = face_ind(b, 1, i, j, k) - face_ind(b, 1, i, j, k - 1);
+            E = Ec + Cuct * (0.5 * a_eta * dBzeta_eta - 0.5 * a_zeta * dBeta_zeta);
+        }
+        else if (ea == 1)
+        {
+            const double *Fx = b.f[F_Efxi];
+            const double *Fz = b.f[F_Efzeta];
+            const int64_t v = b.vol;
+            const double Ec = 0.25 * (Fx[v + pidx(b, i, j, k)] + Fx[v + pidx(b, i, j, k - 1)] +
+                                      Fz[v + pidx(b, i, j, k)] + Fz[v + pidx(b, i - 1, j, k)]);
+            const double a_zeta = max_abs_u4(b, 2, i, j, k, i - 1, j, k, i, j, k - 1, i - 1, j, k - 1);
+            const double a_xi = max_abs_u4(b, 0, i, j, k, i - 1, j, k, i, j, k - 1, i - 1, j, k - 1);
+            const double dBxi_zeta = face_ind(b, 0, i, j, k) - face_ind(b, 0, i, j, k - 1);
+            const double dBzeta_xi = face_ind(b, 2, i, j, k) - face_ind(b, 2, i - 1, j, k);
+            E = Ec + Cuct * (0.5 * a_zeta * dBxi_zeta - 0.5 * a_xi * dBzeta_xi);
+        }
+        else
+        {
+            const double *Fx = b.f[F_Efxi];
+            const double *Fe = b.f[F_Efeta];
+            const int64_t v2 = 2 * b.vol;
+            const double Ec = 0.25 * (Fx[v2 + pidx(b, i, j, k)] + Fx[v2 + pidx(b, i, j - 1, k)] +
+                                      Fe[v2 + pidx(b, i, j, k)] + Fe[v2 + pidx(b, i - 1, j, k)]);
+            const double a_xi = max_abs_u4(b, 0, i, j, k, i - 1, j, k, i, j - 1, k, i - 1, j - 1, k);
+            const double a_eta = max_abs_u4(b, 1, i, j, k, i - 1, j, k, i, j - 1, k, i - 1, j - 1, k);
+            const double dBeta_xi = face_ind(b, 1, i, j, k) - face_ind(b, 1, i - 1, j, k);
+            const double dBxi_eta = face_ind(b, 0, i, j, k) - face_ind(b, 0, i, j - 1, k);
+            E = Ec + Cuct * (0.5 * a_xi * dBeta_xi - 0.5 * a_eta * dBxi_eta);
+        }
+    }
+    b.f[F_Exi + ea][pidx(b, i, j, k)] = E;
+}
+
+// ---------------------------------------------------------------------------
+// CTOperators::CurlEdgeToFace (Z4_Lunar/src/operators/CTOperators.cpp:6-56)
+// with multiplier `mult`, written to RHS_B, optionally followed by the face
+// part of ApplyUpdate_Euler_ (LunarSolver_Advance.cpp:95-121): B += dt*RHS_B.
+// blockIdx.z = face axis.
+// ---------------------------------------------------------------------------
+__global__ void k_curl_e2f(const BlockView *__restrict__ bvs, int fE0, int fR0, int fB0, double mult,
+                           const double *__restrict__ dtp, double dtdiv)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    const int fa = blockIdx.z;
+    int lo[3], n[3];
+    loc_box(b, LOC_FXI + fa, 0, lo, n);
+    int i, j, k;
+    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+        return;
+    const double *Ex = b.f[fE0], *Ee = b.f[fE0 + 1], *Ez = b.f[fE0 + 2];
+    double curl;
+    if (fa == 0)
+        curl = (Ee[pidx(b, i, j, k)] - Ee[pidx(b, i, j, k + 1)]) + (Ez[pidx(b, i, j + 1, k)] - Ez[pidx(b, i, j, k)]);
+    else if (fa == 1)
+        curl = (Ex[pidx(b, i, j, k + 1)] - Ex[pidx(b, i, j, k)]) + (Ez[pidx(b, i, j, k)] - Ez[pidx(b, i + 1, j, k)]);
+    else
+        curl = (Ex[pidx(b, i, j, k)] - Ex[pidx(b, i, j + 1, k)]) + (Ee[pidx(b, i + 1, j, k)] - Ee[pidx(b, i, j, k)]);
+    const int64_t p = pidx(b, i, j, k);
+    const double rhs = mult * curl;
+    if (fR0 >= 0)
+        b.f[fR0 + fa][p] = rhs;
+    if (fB0 >= 0)
+    {
+        const double dt = dtp[0] / dtdiv;
+        b.f[fB0 + fa][p] += dt * rhs;
+    }
+}
+
+// cell part of ApplyUpdate_Euler_ (LunarSolver_Advance.cpp:82-93): U += dt*RHS_H
+__global__ void k_update_u(const BlockView *__restrict__ bvs, const double *__restrict__ dtp)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    int lo[3], n[3];
+    loc_box(b, LOC_CELL, 0, lo, n);
+    int i, j, k;
+    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+        return;
+    const double dt = dtp[0];
+    const int64_t p = pidx(b, i, j, k);
+#pragma unroll
+    for (int m = 0; m < 5; ++m)
+        b.f[F_U][m * b.vol + p] += dt * b.f[F_RHS][m * b.vol + p];
+}
+
+// ---------------------------------------------------------------------------
+// calc_Bcell (Z4_Lunar/src/physics/LunarSolver_Tools.cpp:163-241)
+// ---------------------------------------------------------------------------
+__global__ void k_bcell(const BlockView *__restrict__ bvs)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    int lo[3], n[3];
+    loc_box(b, LOC_CELL, 0, lo, n);
+    int i, j, k;
+    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+        return;
+    const double *Bx = b.f[F_Bxi], *Be = b.f[F_Beta], *Bz = b.f[F_Bzeta];
+    const double *Ax = b.f[F_Baddxi], *Ae = b.f[F_Baddeta], *Az = b.f[F_Baddzeta];
+    const int64_t p = pidx(b, i, j, k);
+    const int64_t pi1 = pidx(b, i + 1, j, k), pj1 = pidx(b, i, j + 1, k), pk1 = pidx(b, i, j, k + 1);
+    const double phi_tot[6] = {-Bx[p] - Ax[p], Bx[pi1] + Ax[pi1], -Be[p] - Ae[p],
+                               Be[pj1] + Ae[pj1], -Bz[p] - Az[p], Bz[pk1] + Az[pk1]};
+    const double phi_ind[6] = {-Bx[p], Bx[pi1], -Be[p], Be[pj1], -Bz[p], Bz[pk1]};
+    const double *W = b.f[F_WB];
+    const int64_t v = b.vol;
+    double bxt = 0.0, byt = 0.0, bzt = 0.0, bxi = 0.0, byi = 0.0, bzi = 0.0;
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+    {
+        const double wx = W[q * v + p];
+        const double wy = W[(6 + q) * v + p];
+        const double wz = W[(12 + q) * v + p];
+        bxt += wx * phi_tot[q];
+        byt += wy * phi_tot[q];
+        bzt += wz * phi_tot[q];
+        bxi += wx * phi_ind[q];
+        byi += wy * phi_ind[q];
+        bzi += wz * phi_ind[q];
+    }
+    double *Bc = b.f[F_Bcell], *Bi = b.f[F_Bind];
+    Bc[p] = bxt;
+    Bc[v + p] = byt;
+    Bc[2 * v + p] = bzt;
+    Bi[p] = bxi;
+    Bi[v + p] = byi;
+    Bi[2 * v + p] = bzi;
+}
+
+// ---------------------------------------------------------------------------
+// Calc_J_Edge: CTOperators::CurlAdjFaceToEdge (CTOperators.cpp:58-110) with
+// the face Hodge scale beta, times the edge scale alpha
+// (LunarSolver_Tools.cpp:777-835).  blockIdx.z = edge axis.
+// ---------------------------------------------------------------------------
+__global__ void k_jedge(const BlockView *__restrict__ bvs, int fB0, int fJ0, double mult)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    const int ea = blockIdx.z;
+    int lo[3], n[3];
+    loc_box(b, LOC_EXI + ea, 0, lo, n);
+    int i, j, k;
+    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+        return;
+    const double *Fx = b.f[fB0], *Fe = b.f[fB0 + 1], *Fz = b.f[fB0 + 2];
+    const double *bx = b.f[F_betaxi], *be = b.f[F_betaeta], *bz = b.f[F_betazeta];
+    double val;
+    if (ea == 0)
+    {
+        const int64_t a = pidx(b, i, j, k - 1), c0 = pidx(b, i, j, k), d = pidx(b, i, j - 1, k);
+        val = (be[a] * Fe[a] - be[c0] * Fe[c0]) + (bz[c0] * Fz[c0] - bz[d] * Fz[d]);
+    }
+    else if (ea == 1)
+    {
+        const int64_t c0 = pidx(b, i, j, k), a = pidx(b, i, j, k - 1), d = pidx(b, i - 1, j, k);
+        val = (bx[c0] * Fx[c0] - bx[a] * Fx[a]) + (bz[d] * Fz[d] - bz[c0] * Fz[c0]);
+    }
+    else
+    {
+        const int64_t a = pidx(b, i, j - 1, k), c0 = pidx(b, i, j, k), d = pidx(b, i - 1, j, k);
+        val = (bx[a] * Fx[a] - bx[c0] * Fx[c0]) + (be[c0] * Fe[c0] - be[d] * Fe[d]);
+    }
+    const int64_t p = pidx(b, i, j, k);
+    const double J = mult * val;
+    b.f[fJ0 + ea][p] = J * b.f[F_alphaxi + ea][p];
+}
+
+// ---------------------------------------------------------------------------
+// calc_Jcell (LunarSolver_Tools.cpp:837-892)
+// ---------------------------------------------------------------------------
+__global__ void k_jcell(const BlockView *__restrict__ bvs)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    int lo[3], n[3];
+    loc_box(b, LOC_CELL, 0, lo, n);
+    int i, j, k;
+    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+        return;
+    const double *Jx = b.f[F_Jxi], *Je = b.f[F_Jeta], *Jz = b.f[F_Jzeta];
+    const double s[12] = {Jx[pidx(b, i, j, k)],         Jx[pidx(b, i, j + 1, k)],     Jx[pidx(b, i, j, k + 1)],
+                          Jx[pidx(b, i, j + 1, k + 1)], Je[pidx(b, i, j, k)],         Je[pidx(b, i + 1, j, k)],
+                          Je[pidx(b, i, j, k + 1)],     Je[pidx(b, i + 1, j, k + 1)], Jz[pidx(b, i, j, k)],
+                          Jz[pidx(b, i + 1, j, k)],     Jz[pidx(b, i, j + 1, k)],     Jz[pidx(b, i + 1, j + 1, k)]};
+    const double *W = b.f[F_WJ];
+    const int64_t p = pidx(b, i, j, k);
+    const int64_t v = b.vol;
+    double jx = 0.0, jy = 0.0, jz = 0.0;
+#pragma unroll
+    for (int q = 0; q < 12; ++q)
+    {
+        jx += W[q * v + p] * s[q];
+        jy += W[(12 + q) * v + p] * s[q];
+        jz += W[(24 + q) * v + p] * s[q];
+    }
+    double *Jc = b.f[F_Jcell];
+    Jc[p] = jx;
+    Jc[v + p] = jy;
+    Jc[2 * v + p] = jz;
+}
+
+// ---------------------------------------------------------------------------
+// calc_PV + calc_Uplus over the whole array (LunarSolver_Tools.cpp:58-141)
+// and, on inner cells, the CFL time-step bound of the next
+// Compute_Timestep (LunarSolver_Timestep.cpp:8-140) reduced with warp
+// shuffles and one atomicMin per thread block.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ double cfl_face_term(double ax, double ay, double az, bool outward_plus, double ux,
+                                                double uy, double uz, double Bx, double By, double Bz, double B2,
+                                                double rho, double cs2, double inver_MA2)
+{
+    const double A = sqrt(ax * ax + ay * ay + az * az);
+    if (A <= 0.0)
+        return 0.0;
+    double nx = ax / A, ny = ay / A, nz = az / A;
+    if (!outward_plus)
+    {
+        nx = -nx;
+        ny = -ny;
+        nz = -nz;
+    }
+    const double un = ux * nx + uy * ny + uz * nz;
+    const double Bn = Bx * nx + By * ny + Bz * nz;
+    const double vA2 = inver_MA2 * B2 / rho;
+    const double vAn2 = inver_MA2 * (Bn * Bn) / rho;
+    const double term = cs2 + vA2;
+    double disc = term * term - 4.0 * cs2 * vAn2;
+    if (disc < 0.0)
+        disc = 0.0;
+    const double cf = sqrt(0.5 * (term + sqrt(disc)));
+    return (fabs(un) + cf) * A;
+}
+
+__device__ __forceinline__ unsigned long long dbl_key(double x)
+{
+    // order-preserving key for non-negative doubles (NaN maps above +inf)
+    return (unsigned long long)__double_as_longlong(x);
+}
+
+__global__ void k_pv_uplus_dt(const BlockView *__restrict__ bvs, Consts c, unsigned long long *dt_key)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    int lo[3], n[3];
+    loc_box(b, LOC_CELL, b.G, lo, n);
+    int i, j, k;
+    double dtc = 1e100;
+    bool any = false;
+    if (box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+    {
+        any = true;
+        const int64_t p = pidx(b, i, j, k);
+        const int64_t v = b.vol;
+        const double *U = b.f[F_U];
+        const double U0 = U[p], U1 = U[v + p], U2 = U[2 * v + p], U3 = U[3 * v + p], U4 = U[4 * v + p];
+        {
+            const double rho = smax(U0, 1e-12);
+            const double u = U1 / rho, vv = U2 / rho, w = U3 / rho;
+            const double ke = 0.5 * rho * (u * u + vv * vv + w * w);
+            double eint = U4 - ke;
+            if (eint < 0.0)
+                eint = 0.0;
+            double pr = (c.gamma - 1.0) * eint;
+            pr = smax(pr, 1e-12);
+            const double T = pr / (rho * c.state_coeff);
+            double *PV = b.f[F_PV];
+            PV[p] = u;
+            PV[v + p] = vv;
+            PV[2 * v + p] = w;
+            PV[3 * v + p] = pr;
+            PV[4 * v + p] = T;
+            const bool has_plasma = U0 > 1e-20;
+            double *Up = b.f[F_Uplus];
+            Up[p] = has_plasma ? u : 0.0;
+            Up[v + p] = has_plasma ? vv : 0.0;
+            Up[2 * v + p] = has_plasma ? w : 0.0;
+        }
+        const bool inner = (i >= 0 && j >= 0 && k >= 0 && i < b.ni && j < b.nj && k < b.nk);
+        if (inner && dt_key)
+        {
+            const double V = fabs(b.f[F_Jac][p]);
+            if (V > 0.0)
+            {
+                const double rho = smax(U0, 1e-2);
+                const double ux = U1 / rho, uy = U2 / rho, uz = U3 / rho;
+                const double ke = 0.5 * rho * (ux * ux + uy * uy + uz * uz);
+                const double eint = U4 - ke;
+                const double pr = (c.gamma - 1.0) * eint;
+                const double cs2 = c.gamma * pr / rho;
+                const double *Bc = b.f[F_Bcell];
+                const double Bx = Bc[p], By = Bc[v + p], Bz = Bc[2 * v + p];
+                const double B2 = Bx * Bx + By * By + Bz * Bz;
+                const double *X = b.f[F_JDxi], *Y = b.f[F_JDeta], *Z = b.f[F_JDzeta];
+                const int64_t pi1 = pidx(b, i + 1, j, k), pj1 = pidx(b, i, j + 1, k), pk1 = pidx(b, i, j, k + 1);
+                double denom = 0.0;
+                denom += cfl_face_term(X[p], X[v + p], X[2 * v + p], false, ux, uy, uz, Bx, By, Bz, B2, rho, cs2,
+                                       c.inver_MA2);
+                denom += cfl_face_term(X[pi1], X[v + pi1], X[2 * v + pi1], true, ux, uy, uz, Bx, By, Bz, B2, rho,
+                                       cs2, c.inver_MA2);
+                denom += cfl_face_term(Y[p], Y[v + p], Y[2 * v + p], false, ux, uy, uz, Bx, By, Bz, B2, rho, cs2,
+                                       c.inver_MA2);
+                denom += cfl_face_term(Y[pj1], Y[v + pj1], Y[2 * v + pj1], true, ux, uy, uz, Bx, By, Bz, B2, rho,
+                                       cs2, c.inver_MA2);
+                denom += cfl_face_term(Z[p], Z[v + p], Z[2 * v + p], false, ux, uy, uz, Bx, By, Bz, B2, rho, cs2,
+                                       c.inver_MA2);
+                denom += cfl_face_term(Z[pk1], Z[v + pk1], Z[2 * v + pk1], true, ux, uy, uz, Bx, By, Bz, B2, rho,
+                                       cs2, c.inver_MA2);
+                // cells with denom <= 0 (or NaN) do not bound dt, as in the reference
+                if (denom > 0.0)
+                    dtc = c.cfl * V / denom;
+            }
+        }
+    }
+    (void)any;
+    if (!dt_key)
+        return;
+    // block-wide minimum of the order-preserving keys
+    unsigned long long key = dbl_key(dtc);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, off);
+        key = (o < key) ? o : key;
+    }
+    __shared__ unsigned long long wmin[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+        wmin[warp] = key;
+    __syncthreads();
+    if (warp == 0)
+    {
+        const int nw = (blockDim.x + 31) >> 5;
+        key = (lane < nw) ? wmin[lane] : ~0ull;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, off);
+            key = (o < key) ? o : key;
+        }
+        if (lane == 0)
+            atomicMin(dt_key, key);
+    }
+}
+
+// Start of StepOnce: dt = global minimum of the CFL bounds, abort check
+// (dt < dt_abort or NaN sets the error word, LunarSolver_Timestep.cpp:128-139).
+__global__ void k_begin_step(const unsigned long long *dt_key, double *dt, int *err, double dt_abort)
+{
+    const double d = __longlong_as_double((long long)dt_key[0]);
+    dt[0] = d;
+    if (!isfinite(d) || d < dt_abort)
+        err[0] = MHD_EDT;
+}
+
+// Arms the dt reduction with the reference's initial bound (dt_local = 1e100).
+__global__ void k_arm_dt(unsigned long long *dt_key) { dt_key[0] = dbl_key(1e100); }
+
+// End of StepOnce: run-data counters (Z4_Lunar/src/LunarSolver_Driver.cpp:75-79)
+__global__ void k_end_step(const double *dt, double *time, long long *step)
+{
+    time[0] += dt[0];
+    step[0] += 1;
+}
+
+// ---------------------------------------------------------------------------
+// compiled Sync: dst <- src over the field pool
+// ---------------------------------------------------------------------------
+__global__ void k_gather(double *__restrict__ pool, const uint64_t *__restrict__ dst, const uint64_t *__restrict__ src,
+                         int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        pool[dst[t]] = pool[src[t]];
+}
+
+// two-phase variant when a source is also a destination
+__global__ void k_gather_stage(double *__restrict__ tmp, const double *__restrict__ pool,
+                               const uint64_t *__restrict__ src, int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        tmp[t] = pool[src[t]];
+}
+__global__ void k_scatter_stage(double *__restrict__ pool, const double *__restrict__ tmp,
+                                const uint64_t *__restrict__ dst, int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        pool[dst[t]] = tmp[t];
+}
+
+// ---------------------------------------------------------------------------
+// AoS (reference host layout) <-> padded SoA, on the device
+// ---------------------------------------------------------------------------
+__global__ void k_aos_to_soa(const BlockView *__restrict__ bvs, int blk, int fid, int ncomp, int lo0, int lo1,
+                             int lo2, int n0, int n1, int n2, const double *__restrict__ aos)
+{
+    const BlockView &b = bvs[blk];
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t tot = int64_t(n0) * n1 * n2 * ncomp;
+    if (t >= tot)
+        return;
+    int64_t r = t;
+    const int m = int(r % ncomp);
+    r /= ncomp;
+    const int k = lo2 + int(r % n2);
+    r /= n2;
+    const int j = lo1 + int(r % n1);
+    const int i = lo0 + int(r / n1);
+    b.f[fid][m * b.vol + pidx(b, i, j, k)] = aos[t];
+}
+
+__global__ void k_soa_to_aos(const BlockView *__restrict__ bvs, int blk, int fid, int ncomp, int lo0, int lo1,
+                             int lo2, int n0, int n1, int n2, double *__restrict__ aos)
+{
+    const BlockView &b = bvs[blk];
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t tot = int64_t(n0) * n1 * n2 * ncomp;
+    if (t >= tot)
+        return;
+    int64_t r = t;
+    const int m = int(r % ncomp);
+    r /= ncomp;
+    const int k = lo2 + int(r % n2);
+    r /= n2;
+    const int j = lo1 + int(r % n1);
+    const int i = lo0 + int(r / n1);
+    aos[t] = b.f[fid][m * b.vol + pidx(b, i, j, k)];
+}
+
+} // namespace mhd

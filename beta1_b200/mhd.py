@@ -1,0 +1,207 @@
+"""ctypes binding of the C ABI in include/beta1_mhd.h, plus a small solver
+facade that sets a case up the way the reference's LunarSolver constructor
+does (geometry, boundary tables, constants, restart state) and then steps it
+on the GPU.
+
+The compiled library is required: importing works without a GPU, but every
+call that touches the device fails with an error naming the cause; there is
+no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict, Iterable, List, Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbeta1_mhd.so")
+
+MHD_OK = 0
+ERRORS = {1: "EINVAL", 2: "ECUDA", 3: "ENOMEM", 4: "EDT", 5: "ESTATE", 6: "EKRYLOV"}
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+STAGE_TIMESTEP, STAGE_FLUID_RHS, STAGE_INDUCTION, STAGE_UPDATE = 1, 2, 3, 4
+
+
+class BlockDesc(C.Structure):
+    _fields_ = [("ni", C.c_int32), ("nj", C.c_int32), ("nk", C.c_int32)]
+
+
+class Params(C.Structure):
+    _fields_ = [("gamma", C.c_double), ("cfl", C.c_double), ("inver_MA2", C.c_double),
+                ("momentum_hall_coeff", C.c_double), ("state_coeff", C.c_double), ("M_H", C.c_double),
+                ("M_ref", C.c_double), ("ne_hall_floor", C.c_double), ("dt_abort", C.c_double),
+                ("ngg", C.c_int32), ("precision", C.c_int32)]
+
+
+# every symbol the header declares, with its signature
+_SIGS = {
+    "mhd_ctx_create": (C.c_int, [C.POINTER(BlockDesc), C.c_int32, C.POINTER(Params), C.POINTER(C.c_void_p)]),
+    "mhd_ctx_destroy": (C.c_int, [C.c_void_p]),
+    "mhd_last_error": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),
+    "mhd_field_info": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                 C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "mhd_upload_field": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_void_p, C.c_int64]),
+    "mhd_download_field": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_void_p, C.c_int64]),
+    "mhd_point_id": (C.c_int64, [C.c_void_p, C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "mhd_set_sync_map": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64]),
+    "mhd_sync": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "mhd_update_derived": (C.c_int, [C.c_void_p]),
+    "mhd_step": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "mhd_step_host": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_double)]),
+    "mhd_state_count": (C.c_int64, [C.c_void_p]),
+    "mhd_host_alloc": (C.c_int, [C.c_int64, C.POINTER(C.c_void_p)]),
+    "mhd_host_free": (C.c_int, [C.c_void_p]),
+    "mhd_stage": (C.c_int, [C.c_void_p, C.c_int32]),
+    "mhd_get_time": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    "mhd_set_time": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_int64]),
+    "mhd_kernel_launches": (C.c_int64, [C.c_void_p]),
+    "mhd_stream": (C.c_void_p, [C.c_void_p]),
+}
+
+_lib: Optional[C.CDLL] = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Loads the CUDA library (built by beta1_b200.build); raises if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with beta1_b200.build.build_library()")
+    lib = C.CDLL(path)
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def exported_symbols() -> List[str]:
+    return list(_SIGS)
+
+
+class MHDError(RuntimeError):
+    pass
+
+
+class Context:
+    """One device context (all blocks of one grid on the current GPU)."""
+
+    def __init__(self, ncells: Sequence[Sequence[int]], params: Params):
+        self.lib = load()
+        arr = (BlockDesc * len(ncells))(*[BlockDesc(*map(int, n)) for n in ncells])
+        h = C.c_void_p()
+        rc = self.lib.mhd_ctx_create(arr, len(ncells), C.byref(params), C.byref(h))
+        if rc != MHD_OK:
+            raise MHDError(f"mhd_ctx_create failed: {ERRORS.get(rc, rc)}")
+        self.h = h
+        self.ncells = [tuple(map(int, n)) for n in ncells]
+        self.params = params
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mhd_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != MHD_OK:
+            buf = C.create_string_buffer(512)
+            self.lib.mhd_last_error(self.h, buf, 512)
+            raise MHDError(f"{what}: {ERRORS.get(rc, rc)}: {buf.value.decode(errors='replace')}")
+
+    def field_info(self, name: str, block: int = 0):
+        loc, nc, ng = C.c_int32(), C.c_int32(), C.c_int32()
+        lo, hi = (C.c_int32 * 3)(), (C.c_int32 * 3)()
+        self._check(self.lib.mhd_field_info(self.h, name.encode(), block, C.byref(loc), C.byref(nc), C.byref(ng),
+                                            lo, hi), f"field_info {name}")
+        return dict(loc=loc.value, ncomp=nc.value, nghost=ng.value, lo=tuple(lo), hi=tuple(hi))
+
+    def upload(self, name: str, block: int, data: np.ndarray):
+        a = np.ascontiguousarray(data, dtype=np.float64)
+        self._check(self.lib.mhd_upload_field(self.h, name.encode(), block, a.ctypes.data, a.size), f"upload {name}")
+
+    def download(self, name: str, block: int = 0) -> np.ndarray:
+        inf = self.field_info(name, block)
+        shape = tuple(h - l for l, h in zip(inf["lo"], inf["hi"])) + (inf["ncomp"],)
+        out = np.empty(shape, dtype=np.float64)
+        self._check(self.lib.mhd_download_field(self.h, name.encode(), block, out.ctypes.data, out.size),
+                    f"download {name}")
+        return out
+
+    def point_base(self, name: str, block: int) -> int:
+        inf = self.field_info(name, block)
+        pid = self.lib.mhd_point_id(self.h, name.encode(), block, *inf["lo"], 0)
+        if pid < 0:
+            raise MHDError(f"point id of {name}")
+        return int(pid)
+
+    def set_sync_map(self, group: str, dst: np.ndarray, src: np.ndarray):
+        d = np.ascontiguousarray(dst, dtype=np.int64)
+        s = np.ascontiguousarray(src, dtype=np.int64)
+        assert d.shape == s.shape
+        self._check(self.lib.mhd_set_sync_map(self.h, group.encode(), d.ctypes.data, s.ctypes.data, d.size),
+                    f"set_sync_map {group}")
+
+    def sync(self, group: str):
+        self._check(self.lib.mhd_sync(self.h, group.encode()), f"sync {group}")
+
+    def update_derived(self):
+        self._check(self.lib.mhd_update_derived(self.h), "update_derived")
+
+    def step(self, n: int = 1):
+        dt, t = C.c_double(), C.c_double()
+        self._check(self.lib.mhd_step(self.h, n, C.byref(dt), C.byref(t)), "step")
+        return dt.value, t.value
+
+    def stage(self, sid: int):
+        self._check(self.lib.mhd_stage(self.h, sid), f"stage {sid}")
+
+    def get_time(self):
+        dt, t, s = C.c_double(), C.c_double(), C.c_int64()
+        self._check(self.lib.mhd_get_time(self.h, C.byref(dt), C.byref(t), C.byref(s)), "get_time")
+        return dt.value, t.value, s.value
+
+    def state_count(self) -> int:
+        return int(self.lib.mhd_state_count(self.h))
+
+    def step_host(self, nsteps: int, state_in: np.ndarray, state_out: np.ndarray) -> float:
+        dt = C.c_double()
+        self._check(self.lib.mhd_step_host(self.h, nsteps, state_in.ctypes.data, state_out.ctypes.data,
+                                           state_in.size, C.byref(dt)), "step_host")
+        return dt.value
+
+    def launches(self) -> int:
+        return int(self.lib.mhd_kernel_launches(self.h))
+
+    def stream(self) -> int:
+        return int(self.lib.mhd_stream(self.h) or 0)
+
+
+class PinnedArray:
+    """Page-locked float64 host buffer from mhd_host_alloc, viewed as numpy."""
+
+    def __init__(self, n: int):
+        self.lib = load()
+        p = C.c_void_p()
+        rc = self.lib.mhd_host_alloc(int(n) * 8, C.byref(p))
+        if rc != MHD_OK:
+            raise MHDError("mhd_host_alloc failed")
+        self.p = p
+        self.a = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double)), shape=(int(n),))
+
+    def free(self):
+        if self.p:
+            self.lib.mhd_host_free(self.p)
+            self.p = None

@@ -1,0 +1,60 @@
+"""Solver facade: sets a case up on the device the way the reference's
+LunarSolver constructor prepares its fields (Z4_Lunar/src/LunarSolver.cpp:12-235),
+then steps it with the CUDA library."""
+from __future__ import annotations
+
+from typing import Optional
+
+import numpy as np
+
+from . import case as case_mod
+from . import geometry, mhd, physics, rst, syncmap
+
+GEOM_FIELDS = ["Jac", "JDxi", "JDet", "JDze", "beta_xi", "beta_eta", "beta_zeta", "alpha_xi", "alpha_eta",
+               "alpha_zeta", "dr_xi", "dr_eta", "dr_zeta", "Bcell_from_Bface_w", "Jcell_from_Jedge_w"]
+STATE_FIELDS = ["U_H", "B_xi", "B_eta", "B_zeta"]
+
+
+def make_params(p, precision=mhd.PREC_FP64) -> mhd.Params:
+    c = physics.constants(p)
+    return mhd.Params(gamma=c["gamma"], cfl=c["cfl"], inver_MA2=c["inver_MA2"],
+                      momentum_hall_coeff=c["momentum_hall_coeff"], state_coeff=c["state_coeff"], M_H=c["M_H"],
+                      M_ref=c["M_ref"], ne_hall_floor=c["ne_hall_floor"], dt_abort=1e-7, ngg=int(p["ngg"]),
+                      precision=int(precision))
+
+
+class Solver:
+    def __init__(self, spec: case_mod.CaseSpec, topology: str = "periodic", precision=mhd.PREC_FP64):
+        self.spec = spec
+        ngg = int(spec.params["ngg"])
+        self.ctx = mhd.Context([b.ncell for b in spec.blocks], make_params(spec.params, precision))
+        self.geom = []
+        for ib, b in enumerate(spec.blocks):
+            X = geometry.ghost_mesh(b.x, b.y, b.z, ngg)
+            g = geometry.build(X, b.ncell, ngg)
+            for name in GEOM_FIELDS:
+                lo, hi, a = g[name]
+                self.ctx.upload(name, ib, a)
+            self.geom.append(g)
+        if topology == "periodic":
+            assert len(spec.blocks) == 1
+            self.sync_sizes = syncmap.install_periodic(self.ctx, spec.blocks[0].ncell)
+        else:
+            raise ValueError(f"unknown topology {topology}")
+
+    def load_state(self, state: rst.RestartFile):
+        """Restart load + the syncs that make ghosts consistent, then
+        UpdateDerivedFields_ (the state the first StepOnce starts from)."""
+        for name in STATE_FIELDS:
+            rec = state.fields[name]
+            for ib, fa in enumerate(rec.blocks):
+                self.ctx.upload(name, ib, fa.data)
+        self.ctx.sync("Ucell")
+        self.ctx.sync("Bface")
+        self.ctx.update_derived()
+
+    def step(self, n=1):
+        return self.ctx.step(n)
+
+    def field(self, name, block=0) -> np.ndarray:
+        return self.ctx.download(name, block)

@@ -1,0 +1,163 @@
+/*
+ * beta1_mhd.h -- C ABI of the B200 (sm_100a) per-timestep MHD hot path.
+ *
+ * One context holds every block of a multi-block structured grid on one GPU,
+ * one CUDA stream, the device copies of the solver's fields and the gather
+ * tables of its boundary/halo synchronisations.  All entry points return 0 on
+ * success and a positive MHD_E* code otherwise; nothing here exits or throws.
+ * A context is not thread-safe; different contexts are independent.
+ *
+ * Field data cross this boundary in the reference's own host layout: a field
+ * on block b is the half-open logical box [lo, hi) of its stagger location
+ * (include/3_field/1_Field_Block.h:29-35, src/3_field/1_Field_Block.cpp:51-131),
+ * stored as float64 in (i, j, k, m) order with the component m fastest
+ * (include/3_field/Field_Array.h:177).  Field names are the reference's
+ * (Z4_Lunar/main.cpp:61-123, src/3_field/4_MPCNS_Geometry.cpp:4-69).
+ *
+ * Each entry point below names the reference interface it replaces.
+ */
+#ifndef BETA1_MHD_H
+#define BETA1_MHD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define MHD_OK 0
+#define MHD_EINVAL 1      /* bad argument (unknown name, size mismatch, null) */
+#define MHD_ECUDA 2       /* a CUDA runtime call failed */
+#define MHD_ENOMEM 3      /* device or host allocation failed */
+#define MHD_EDT 4         /* time step underflow or NaN (dt < dt_abort) */
+#define MHD_ESTATE 5      /* call out of order (e.g. step before set-up) */
+#define MHD_EKRYLOV 6     /* implicit solve did not converge */
+
+/* stagger locations, numbered as the reference's restart writer does
+   (src/5_io/IOModule_Bin.cpp:62-85) */
+#define MHD_LOC_CELL 0
+#define MHD_LOC_FACE_XI 1
+#define MHD_LOC_FACE_ETA 2
+#define MHD_LOC_FACE_ZETA 3
+#define MHD_LOC_EDGE_XI 4
+#define MHD_LOC_EDGE_ETA 5
+#define MHD_LOC_EDGE_ZETA 6
+
+/* precision of the flux / EMF / Krylov-operator arithmetic */
+#define MHD_PREC_FP64 0   /* FP64 throughout, operation order of the reference */
+#define MHD_PREC_MIXED 1  /* FP32 face fluxes, FP64 CT, state and residuals */
+
+typedef struct mhd_ctx mhd_ctx;
+
+/* Cell counts of one block (Block::mx/my/mz, include/1_grid/1_MPCNS_Grid.h:34-44). */
+typedef struct
+{
+    int32_t ni, nj, nk;
+} mhd_block_desc;
+
+/* Nondimensional constants of the solver, as LunarSolver::calc_physical_constant
+   computes them (Z4_Lunar/src/physics/LunarSolver_Tools.cpp:3-45). */
+typedef struct
+{
+    double gamma;               /* ratio of specific heats */
+    double cfl;                 /* CFL number of Compute_Timestep */
+    double inver_MA2;           /* 1 / Alfven Mach^2 scale of v_A^2 */
+    double momentum_hall_coeff; /* J x B force coefficient */
+    double state_coeff;         /* p = rho T state_coeff */
+    double M_H, M_ref;          /* molar masses in Hall_Num_Limiter */
+    double ne_hall_floor;       /* electron-density floor of Hall_Num_Limiter */
+    double dt_abort;            /* abort threshold of Compute_Timestep (1e-7) */
+    int32_t ngg;                /* ghost layers of the state fields (4) */
+    int32_t precision;          /* MHD_PREC_* */
+} mhd_params;
+
+/* LunarSolver ctor + Field registration (Z4_Lunar/src/LunarSolver.cpp:12-235,
+   Z4_Lunar/main.cpp:57-123): allocates every hot-path field of every block
+   on the current CUDA device, zero-filled. */
+int mhd_ctx_create(const mhd_block_desc *blocks, int32_t nblocks, const mhd_params *params, mhd_ctx **out);
+
+/* ~LunarSolver / delete fld (Z4_Lunar/main.cpp:216-222). */
+int mhd_ctx_destroy(mhd_ctx *ctx);
+
+/* Message of the last failing call on this context (NUL-terminated). */
+int mhd_last_error(const mhd_ctx *ctx, char *buf, int32_t buflen);
+
+/* Descriptor of a named field: location, components, ghost layers and the
+   logical box [lo, hi) on block `block` (FieldBlock::get_lo/get_hi,
+   include/3_field/1_Field_Block.h:29-35). */
+int mhd_field_info(const mhd_ctx *ctx, const char *name, int32_t block, int32_t *loc, int32_t *ncomp,
+                   int32_t *nghost, int32_t lo[3], int32_t hi[3]);
+
+/* FieldBlock host storage <-> device (the reference reads/writes FieldBlock
+   storage directly, src/3_field/1_Field_Block.cpp:3-25).  `data` holds the
+   field's full logical box in AoS order; `count` must equal its size. */
+int mhd_upload_field(mhd_ctx *ctx, const char *name, int32_t block, const double *data, int64_t count);
+int mhd_download_field(mhd_ctx *ctx, const char *name, int32_t block, double *data, int64_t count);
+
+/* Point id of (field, block, i, j, k, m) for the gather tables below. */
+int64_t mhd_point_id(const mhd_ctx *ctx, const char *name, int32_t block, int32_t i, int32_t j, int32_t k,
+                     int32_t m);
+
+/* Compiled boundary synchronisation of one group (LunarBoundary::Sync,
+   Z4_Lunar/src/boundary/Boundary.cpp:30-40 and Boundary_Sync_.cpp:4-65:
+   physical handlers, corner defaults, face/edge/vertex halos of
+   src/4_halo/1_MPCNS_Halo_Inner.cpp:3-217).  The group's whole ordered
+   sequence of copies is given as its composition: after the sync, point
+   dst[n] holds the value point src[n] had before it.  Groups: "Ucell",
+   "Bface", "Eface", "Eedge", "B_cell", "Jedge", "J_cell", "Uplus",
+   "Eres", "Eres1form", "dB". */
+int mhd_set_sync_map(mhd_ctx *ctx, const char *group, const int64_t *dst, const int64_t *src, int64_t n);
+
+/* LunarBoundary::Sync(group) on the device. */
+int mhd_sync(mhd_ctx *ctx, const char *group);
+
+/* LunarSolver::UpdateDerivedFields_ (Z4_Lunar/src/physics/LunarSolver_Tools.cpp:157-161):
+   B_cell, J_edge, J_cell, PV, U_plus with their syncs; also the CFL time step
+   of the next StepOnce (LunarSolver::Compute_Timestep,
+   Z4_Lunar/src/physics/LunarSolver_Timestep.cpp:8-140). */
+int mhd_update_derived(mhd_ctx *ctx);
+
+/* `nsteps` x LunarSolver::StepOnce (Z4_Lunar/src/LunarSolver_Driver.cpp:21-92),
+   replayed as one CUDA graph per step.  dt_out / time_out (may be NULL)
+   receive the last step's dt and the accumulated time. */
+int mhd_step(mhd_ctx *ctx, int32_t nsteps, double *dt_out, double *time_out);
+
+/* End-to-end step through host buffers: uploads U_H and B_xi/B_eta/B_zeta of
+   every block from host AoS arrays (concatenated block after block), runs
+   Sync("Ucell"), Sync("Bface"), UpdateDerivedFields_ and `nsteps` StepOnce,
+   downloads the same fields back.  The host arrays may be pinned (see
+   mhd_host_alloc) for full copy bandwidth. */
+int mhd_step_host(mhd_ctx *ctx, int32_t nsteps, const double *state_in, double *state_out, int64_t count,
+                  double *dt_out);
+
+/* Size in doubles of the concatenated host state used by mhd_step_host. */
+int64_t mhd_state_count(const mhd_ctx *ctx);
+
+/* Page-locked host memory for the state buffers (cudaHostAlloc). */
+int mhd_host_alloc(int64_t bytes, void **ptr);
+int mhd_host_free(void *ptr);
+
+/* Individual stages, for stage-level parity checks and for drivers that keep
+   their own step loop.  Stage ids: */
+#define MHD_STAGE_TIMESTEP 1   /* Compute_Timestep (dt of the current state) */
+#define MHD_STAGE_FLUID_RHS 2  /* ZeroRHS_ + Scheme_U_ + AddSourceToRHS_Fluid -> RHS_H */
+#define MHD_STAGE_INDUCTION 3  /* AssembleRHS_Induction_CT_ -> Eface, E, RHS_B */
+#define MHD_STAGE_UPDATE 4     /* ApplyUpdate_Euler_ with the current dt */
+int mhd_stage(mhd_ctx *ctx, int32_t stage_id);
+
+/* Current dt / time / step counters (device -> host). */
+int mhd_get_time(mhd_ctx *ctx, double *dt, double *time, int64_t *step);
+int mhd_set_time(mhd_ctx *ctx, double dt, double time, int64_t step);
+
+/* Launch statistics: number of kernels this library launched since creation. */
+int64_t mhd_kernel_launches(const mhd_ctx *ctx);
+
+/* CUDA stream of the context (cudaStream_t), for callers that time with events. */
+void *mhd_stream(const mhd_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BETA1_MHD_H */

@@ -1,0 +1,92 @@
+"""Generates the committed golden fixtures from the reference itself.
+
+Runs the reference Lunar solver, compiled from its own sources against the
+single-rank MPI / PETSc-subset shims (oracle/Makefile -> oracle/_ref/ref_lunar),
+on small seeded cases written in the reference's own input formats, and
+stores its outputs as compressed numpy archives:
+
+* periodic_<n>_geom.npz    every geometry field and the ghost node coordinates
+* periodic_<n>_probe.npz   for each Sync group, the point each ghost is copied from
+* periodic_<n>_steps.npz   state + derived + intermediate fields after 0..S StepOnce
+
+Needs the reference tree (default /root/reference) and a built oracle; run
+    make -C oracle -j8 && python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from beta1_b200 import case, rst  # noqa: E402
+
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "ref_lunar")
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+STEP_FIELDS = ["U_H", "B_xi", "B_eta", "B_zeta", "PV_H", "U_plus", "B_cell", "Bind_cell", "J_xi", "J_eta", "J_zeta",
+               "J_cell", "E_xi", "E_eta", "E_zeta", "Eface_xi", "Eface_eta", "Eface_zeta", "RHS_H", "RHS_B_xi",
+               "RHS_B_eta", "RHS_B_zeta"]
+GROUPS = ["Ucell", "Bface", "Eface", "Eedge", "B_cell", "Jedge", "J_cell", "Uplus"]
+
+
+def run(args, cwd):
+    subprocess.run([REF_BIN] + args, cwd=cwd, check=True, stdout=subprocess.PIPE)
+
+
+def flatten(rf: rst.RestartFile, names, block=0):
+    out = {}
+    for n in names:
+        fa = rf.fields[n].blocks[block]
+        out[n] = fa.data
+        out[n + "__lo"] = np.array(fa.lo, dtype=np.int32)
+    return out
+
+
+def periodic(n=(8, 6, 5), steps=2, seed=20261203):
+    tag = "periodic_%dx%dx%d" % n
+    with tempfile.TemporaryDirectory() as d:
+        spec = case.periodic_box_case(n)
+        case.write_case(d, spec)
+        st = case.initial_state(spec, seed=seed)
+        rst.write(os.path.join(d, "init.rst"), st)
+        run(["geom", "geom.bin"], d)
+        g = rst.read(os.path.join(d, "geom.bin"))
+        np.savez_compressed(os.path.join(OUT, tag + "_geom.npz"), **flatten(g, list(g.fields)))
+        probes = {}
+        for grp in GROUPS:
+            run(["probe", "init.rst", grp, "p.bin"], d)
+            p = rst.read(os.path.join(d, "p.bin"))
+            for fname, rec in p.fields.items():
+                v = rec.blocks[0].data.reshape(-1)
+                own = np.arange(v.size, dtype=np.float64) + 1.0
+                changed = np.nonzero(v != own)[0]
+                probes[grp + "/" + fname + "/dst"] = changed.astype(np.int64)
+                probes[grp + "/" + fname + "/src"] = (v[changed] - 1.0).astype(np.int64)
+        np.savez_compressed(os.path.join(OUT, tag + "_probe.npz"), **probes)
+        run(["run", "init.rst", str(steps), "step"], d)
+        arr = {}
+        init = flatten(st, ["U_H", "B_xi", "B_eta", "B_zeta"])
+        for k, v in init.items():
+            arr["init/" + k] = v
+        for s in range(steps + 1):
+            r = rst.read(os.path.join(d, "step_%04d.bin" % s))
+            for k, v in flatten(r, STEP_FIELDS).items():
+                arr["s%d/%s" % (s, k)] = v
+            arr["s%d/dt" % s] = r.fields["dt"].blocks[0].data.reshape(())
+            arr["s%d/time" % s] = np.array(r.time)
+        arr["n"] = np.array(n)
+        arr["seed"] = np.array(seed)
+        np.savez_compressed(os.path.join(OUT, tag + "_steps.npz"), **arr)
+    print("wrote", tag)
+
+
+if __name__ == "__main__":
+    if not os.path.exists(REF_BIN):
+        sys.exit("build the oracle first: make -C oracle -j8")
+    periodic((8, 6, 5), steps=2)
