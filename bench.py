@@ -1,0 +1,324 @@
+"""Benchmark of the per-timestep MHD hot path (one StepOnce = one step).
+
+Default workload: the plain FP64 64^3 periodic curvilinear block of the
+reference's CPU-runnable configuration (ideal MHD, Rusanov + CT, CFL 0.4,
+seeded 1e-3 noise), stepped on the GPU through the C ABI.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Multi-GPU (torchrun): the path does not shard (north star: no multi-GPU
+path), so N ranks run N independent replicas; value = all cells updated by
+all ranks / max-over-ranks time.
+
+Rank 0 prints one JSON line.  Inputs are seeded synthetic states in the
+reference's restart format; the device working set (~0.36 GB at 64^3) is
+larger than the 126 MB L2, so no L2 flush is inserted between steps.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "ref_lunar")
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+# Algorithmic bytes per cell of each kernel (FP64, every array the kernel
+# must read or write counted once per cell, 8 bytes per element).
+ALGO_BYTES_PER_CELL = {
+    # U 5, PV 5, JD 9, Jac 1, B_cell 3, J_cell 3 read; RHS_H 5 written
+    "k_fluid_rhs": 31 * 8,
+    # B 3, Badd 3, JD 9, Jac 1, U_plus 3 read; Eface 9 written
+    "k_eface": 28 * 8,
+    # Eface 6, B 3, JD 9, Jac 1, U_plus 3 read; E 3 written
+    "k_eedge": 25 * 8,
+    # E 3 read, RHS_B 3 written, B 3 read + written
+    "k_curl_e2f": 12 * 8,
+    # U 5 read + written, RHS_H 5 read
+    "k_update_u": 15 * 8,
+    # B 3, Badd 3, W_B 18 read; B_cell 3, Bind_cell 3 written
+    "k_bcell": 30 * 8,
+    # B 3, beta 3, alpha 3 read; J 3 written
+    "k_jedge": 12 * 8,
+    # J 3, W_J 36 read; J_cell 3 written
+    "k_jcell": 42 * 8,
+    # U 5, Jac 1, B_cell 3, JD 9 read; PV 5, U_plus 3 written
+    "k_pv_uplus_dt": 26 * 8,
+}
+
+# DRAM traffic per launch from one ncu capture of the 64^3 case
+# (profiles/k_fluid_rhs_periodic64.md); None where not captured.
+NCU_TRAFFIC_BYTES = {}
+
+
+def sample_clocks(stop: threading.Event, out: list, gpu_id: str):
+    """nvidia-smi clock / throttle samples of this rank's GPU every 100 ms."""
+    cmd = ["nvidia-smi", "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+           "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+           "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-i", gpu_id]
+    while not stop.is_set():
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=5)
+            if r.returncode == 0 and r.stdout.strip():
+                out.append(r.stdout.strip().splitlines()[0])
+        except Exception:
+            pass
+        stop.wait(0.1)
+
+
+def summarize_clocks(lines):
+    if not lines:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+    sm, smax, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for ln in lines:
+        p = [x.strip() for x in ln.split(",")]
+        try:
+            sm.append(float(p[0]))
+            smax.append(float(p[1]))
+        except ValueError:
+            continue
+        for nm, v in zip(names, p[3:7]):
+            if v.lower() == "active":
+                reasons.add(nm)
+    return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(PEAKS) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def build_case(n):
+    from beta1_b200 import case
+    spec = case.periodic_box_case((n, n, n))
+    st = case.initial_state(spec)
+    return spec, st
+
+
+def cpu_reference(n, steps, nproc):
+    """Times the reference's own StepOnce loop (oracle/_ref/ref_lunar, built
+    from the reference sources) on `nproc` concurrent single-threaded
+    processes, each on the same bounded sample; returns aggregate
+    cell-updates/s and the per-process figures."""
+    from beta1_b200 import case, rst
+    if not os.path.exists(REF_BIN):
+        return None
+    spec, st = build_case(n)
+    d = tempfile.mkdtemp(prefix="b1ref_")
+    try:
+        case.write_case(d, spec)
+        rst.write(os.path.join(d, "init.rst"), st)
+        procs = []
+        for p in range(nproc):
+            wd = os.path.join(d, "r%d" % p)
+            os.makedirs(wd)
+            os.symlink(os.path.join(d, "CASE"), os.path.join(wd, "CASE"))
+            procs.append(subprocess.Popen([REF_BIN, "time", os.path.join(d, "init.rst"), str(steps)], cwd=wd,
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
+        vals = []
+        for pr in procs:
+            out, _ = pr.communicate()
+            vals.append(json.loads(out.strip().splitlines()[-1]))
+        agg = sum(v["cell_updates_per_s"] for v in vals)
+        return agg, vals
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    nproc = os.cpu_count() or 1
+    res = cpu_reference(args.n, args.ref_steps, nproc)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_lunar not built (no reference tree)"}))
+        return 0
+    agg, vals = res
+    sample = "%d^3 periodic block, %d StepOnce per process, %d concurrent single-threaded processes" % (
+        args.n, args.ref_steps, nproc)
+    line = {
+        "impl": "reference", "metric": "cell-updates/s", "value": agg, "unit": "cell-updates/s",
+        "n_gpus": args.gpus, "steps": args.ref_steps, "warmup": 0,
+        "ms_per_step": 1000.0 * vals[0]["seconds"] / vals[0]["steps"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "c1_periodic_%dcubed_fp64" % args.n, "cells": args.n ** 3},
+        "cpu_baseline": {"value": agg, "unit": "cell-updates/s", "cores": nproc, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": agg, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=64, help="cells per direction of the periodic block")
+    ap.add_argument("--ref-steps", type=int, default=40, help="StepOnce per reference CPU sample")
+    ap.add_argument("--e2e-iters", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from beta1_b200 import solver
+
+    spec, st = build_case(args.n)
+    s = solver.Solver(spec)
+    s.load_state(st)
+    ctx = s.ctx
+    cells = args.n ** 3
+    stream = torch.cuda.ExternalStream(ctx.stream())
+
+    # warm-up (also builds and instantiates the step graph)
+    ctx.step(args.warmup)
+
+    # timed region
+    clocks, stop = [], threading.Event()
+    try:
+        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        gpu_id = str(local)
+    th = threading.Thread(target=sample_clocks, args=(stop, clocks, gpu_id), daemon=True)
+    th.start()
+    time.sleep(0.25)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = ctx.launches()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    launches = ctx.launches() - l0
+    stop.set()
+    th.join()
+    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * cells * args.steps / (ms_max / 1000.0)
+
+    # per-kernel durations: eager steps with an event pair around every launch
+    prof = {}
+    for _ in range(5):
+        for name, t in ctx.profile_step():
+            prof.setdefault(name, []).append(t)
+    per_step = {k: sum(v) / 5.0 for k, v in prof.items()}
+    total = sum(per_step.values())
+    dominant = max((k for k in per_step if k in ALGO_BYTES_PER_CELL), key=lambda k: per_step[k])
+    launches_of = {k: len(v) / 5.0 for k, v in prof.items()}
+    avg_launch_ms = per_step[dominant] / launches_of[dominant]
+    bytes_per_launch = ALGO_BYTES_PER_CELL[dominant] * cells / launches_of[dominant]
+    achieved = bytes_per_launch / (avg_launch_ms / 1000.0) / 1e9
+    peak, peak_kind = measured_peak()
+
+    # end to end through host buffers (pinned), H2D + D2H inside the region
+    from beta1_b200.mhd import PinnedArray
+    nstate = ctx.state_count()
+    hin, hout = PinnedArray(nstate), PinnedArray(nstate)
+    # the state after the timed steps, as the caller would hold it
+    off = 0
+    for name in ("U_H", "B_xi", "B_eta", "B_zeta"):
+        a = ctx.download(name, 0).ravel()
+        hin.a[off:off + a.size] = a
+        off += a.size
+    ctx.step_host(1, hin.a, hout.a)
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.e2e_iters):
+        ctx.step_host(1, hin.a, hout.a)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1) / args.e2e_iters
+    e2e_t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = world * cells / (float(e2e_t.item()) / 1000.0)
+    hin.free()
+    hout.free()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        res = cpu_reference(args.n, args.ref_steps, 1)
+        if res is not None:
+            agg, vals = res
+            cpu = {"value": agg, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+                   "sample": "%d^3 periodic block, %d StepOnce of the reference solver built from its own "
+                             "sources, one single-threaded process" % (args.n, args.ref_steps)}
+
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded 1e-3 noise on rho, v and div-free B; reference restart format)",
+            "config": {"workload": "c1_periodic_%dcubed_fp64" % args.n, "cells_per_gpu": cells, "blocks": 1,
+                       "integrator": "forward Euler StepOnce (reference parity mode)", "precision": "fp64",
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "no flush: per-step working set %.2f GB > 126 MB L2" % (
+                           (args.n + 9) ** 3 * 138 * 8 / 1e9)},
+            "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": nstate * 8,
+                    "d2h_bytes_per_step": nstate * 8},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": NCU_TRAFFIC_BYTES.get((dominant, args.n)),
+                         "algo_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_launch_ms,
+                         "kernel_share": per_step[dominant] / total},
+            "kernels_ms_per_step": {k: round(v, 5) for k, v in sorted(per_step.items(), key=lambda kv: -kv[1])},
+            "cpu_baseline": cpu,
+            "clocks": summarize_clocks(clocks),
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    s.ctx.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -52,6 +52,13 @@ struct SyncMap
 
 constexpr int kThreads = 256;
 
+const char *const kKernelNames[] = {"k_fluid_rhs",   "k_eface",        "k_eedge",         "k_curl_e2f",
+                                    "k_update_u",    "k_bcell",        "k_jedge",         "k_jcell",
+                                    "k_pv_uplus_dt", "k_begin_step",   "k_arm_dt",        "k_end_step",
+                                    "k_gather",      "k_gather_stage", "k_scatter_stage", "k_aos_to_soa",
+                                    "k_soa_to_aos"};
+constexpr int kNumKernelNames = int(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
+
 } // namespace
 
 struct mhd_ctx
@@ -82,6 +89,10 @@ struct mhd_ctx
     int64_t max_cells = 0;
     bool capturing = false;
     std::string msg;
+    // eager profiling: one event pair per launch
+    bool profiling = false;
+    std::vector<const char *> prof_names;
+    std::vector<cudaEvent_t> prof_ev;
 };
 
 namespace
@@ -157,9 +168,37 @@ int ensure_staging(mhd_ctx *ctx, size_t n)
     return MHD_OK;
 }
 
+#define RUN(x)                 \
+    do                         \
+    {                          \
+        int rc_ = (x);         \
+        if (rc_ != MHD_OK)     \
+            return rc_;        \
+    } while (0)
+
 // ---- launch helpers (all on ctx->stream) ----
+// Eager profiling: prof_begin() records an event before a launch, launched()
+// one after it, so each kernel's duration is measured on the launching stream.
+void prof_begin(mhd_ctx *ctx, const char *name)
+{
+    if (!ctx->profiling)
+        return;
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, ctx->stream);
+    ctx->prof_ev.push_back(e);
+    ctx->prof_names.push_back(name);
+}
+
 int launched(mhd_ctx *ctx, int nk = 1)
 {
+    if (ctx->profiling)
+    {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, ctx->stream);
+        ctx->prof_ev.push_back(e);
+    }
     ctx->launches += nk;
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
@@ -175,43 +214,44 @@ int run_sync(mhd_ctx *ctx, const char *group)
     SyncMap &s = it->second;
     if (s.tmp)
     {
+        prof_begin(ctx, "k_gather_stage");
         k_gather_stage<<<grid_for(s.n), kThreads, 0, ctx->stream>>>(s.tmp, ctx->pool, s.src, s.n);
+        RUN(launched(ctx));
+        prof_begin(ctx, "k_scatter_stage");
         k_scatter_stage<<<grid_for(s.n), kThreads, 0, ctx->stream>>>(ctx->pool, s.tmp, s.dst, s.n);
-        return launched(ctx, 2);
+        return launched(ctx);
     }
+    prof_begin(ctx, "k_gather");
     k_gather<<<grid_for(s.n), kThreads, 0, ctx->stream>>>(ctx->pool, s.dst, s.src, s.n);
     return launched(ctx);
 }
-
-#define RUN(x)                 \
-    do                         \
-    {                          \
-        int rc_ = (x);         \
-        if (rc_ != MHD_OK)     \
-            return rc_;        \
-    } while (0)
 
 int launch_update_derived(mhd_ctx *ctx)
 {
     const int nb = ctx->nblocks;
     cudaStream_t s = ctx->stream;
     const int64_t nc = max_box(ctx, LOC_CELL, 0);
+    prof_begin(ctx, "k_bcell");
     k_bcell<<<dim3(grid_for(nc), nb), kThreads, 0, s>>>(ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "B_cell"));
     const int64_t ne = max_box(ctx, LOC_EZETA, 0) > max_box(ctx, LOC_EXI, 0) ? max_box(ctx, LOC_EZETA, 0)
                                                                               : max_box(ctx, LOC_EXI, 0);
     const int64_t ne2 = max_box(ctx, LOC_EETA, 0) > ne ? max_box(ctx, LOC_EETA, 0) : ne;
+    prof_begin(ctx, "k_jedge");
     k_jedge<<<dim3(grid_for(ne2), nb, 3), kThreads, 0, s>>>(ctx->dbv, F_Bxi, F_Jxi, 1.0);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Jedge"));
+    prof_begin(ctx, "k_jcell");
     k_jcell<<<dim3(grid_for(nc), nb), kThreads, 0, s>>>(ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "J_cell"));
     // arm the dt reduction, then PV / U_plus / CFL bound of the next step
+    prof_begin(ctx, "k_arm_dt");
     k_arm_dt<<<1, 1, 0, s>>>(ctx->dt_key);
     RUN(launched(ctx));
     const int64_t ng = max_box(ctx, LOC_CELL, ctx->G);
+    prof_begin(ctx, "k_pv_uplus_dt");
     k_pv_uplus_dt<<<dim3(grid_for(ng), nb), kThreads, 0, s>>>(ctx->dbv, ctx->c, ctx->dt_key);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Uplus"));
@@ -221,6 +261,7 @@ int launch_update_derived(mhd_ctx *ctx)
 int launch_fluid_rhs(mhd_ctx *ctx)
 {
     const int64_t nc = max_box(ctx, LOC_CELL, 0);
+    prof_begin(ctx, "k_fluid_rhs");
     k_fluid_rhs<<<dim3(grid_for(nc), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv, ctx->c, nc);
     return launched(ctx);
 }
@@ -232,15 +273,18 @@ int launch_induction(mhd_ctx *ctx, bool update_b)
     int64_t nf = 0;
     for (int l = LOC_FXI; l <= LOC_FZETA; ++l)
         nf = max_box(ctx, l, 0) > nf ? max_box(ctx, l, 0) : nf;
+    prof_begin(ctx, "k_eface");
     k_eface<<<dim3(grid_for(nf), nb, 3), kThreads, 0, s>>>(ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Eface"));
     int64_t ne = 0;
     for (int l = LOC_EXI; l <= LOC_EZETA; ++l)
         ne = max_box(ctx, l, ctx->G) > ne ? max_box(ctx, l, ctx->G) : ne;
+    prof_begin(ctx, "k_eedge");
     k_eedge<<<dim3(grid_for(ne), nb, 3), kThreads, 0, s>>>(ctx->dbv, ctx->G);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Eedge"));
+    prof_begin(ctx, "k_curl_e2f");
     k_curl_e2f<<<dim3(grid_for(nf), nb, 3), kThreads, 0, s>>>(ctx->dbv, F_Exi, F_RBxi, update_b ? F_Bxi : -1,
                                                                -1.0, ctx->dt, 1.0);
     return launched(ctx);
@@ -249,6 +293,7 @@ int launch_induction(mhd_ctx *ctx, bool update_b)
 int launch_update_u(mhd_ctx *ctx)
 {
     const int64_t nc = max_box(ctx, LOC_CELL, 0);
+    prof_begin(ctx, "k_update_u");
     k_update_u<<<dim3(grid_for(nc), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv, ctx->dt);
     return launched(ctx);
 }
@@ -257,11 +302,13 @@ int launch_update_u(mhd_ctx *ctx)
 int launch_step(mhd_ctx *ctx)
 {
     cudaStream_t s = ctx->stream;
+    prof_begin(ctx, "k_begin_step");
     k_begin_step<<<1, 1, 0, s>>>(ctx->dt_key, ctx->dt, ctx->err, ctx->prm.dt_abort);
     RUN(launched(ctx));
     RUN(launch_fluid_rhs(ctx));
     RUN(launch_induction(ctx, /*update_b=*/true));
     RUN(launch_update_u(ctx));
+    prof_begin(ctx, "k_end_step");
     k_end_step<<<1, 1, 0, s>>>(ctx->dt, ctx->time, ctx->step);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Ucell"));
@@ -484,6 +531,7 @@ static int transfer(mhd_ctx *ctx, const char *name, int32_t block, const double 
     if (hin)
     {
         CK(ctx, cudaMemcpyAsync(ctx->staging, hin, size_t(n) * 8, cudaMemcpyHostToDevice, ctx->stream));
+        prof_begin(ctx, "k_aos_to_soa");
         k_aos_to_soa<<<grid_for(n), kThreads, 0, ctx->stream>>>(ctx->dbv, block, f, nc, lo[0], lo[1], lo[2],
                                                                 hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2],
                                                                 ctx->staging);
@@ -491,6 +539,7 @@ static int transfer(mhd_ctx *ctx, const char *name, int32_t block, const double 
     }
     else
     {
+        prof_begin(ctx, "k_soa_to_aos");
         k_soa_to_aos<<<grid_for(n), kThreads, 0, ctx->stream>>>(ctx->dbv, block, f, nc, lo[0], lo[1], lo[2],
                                                                 hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2],
                                                                 ctx->staging);
@@ -656,6 +705,7 @@ int mhd_step_host(mhd_ctx *ctx, int32_t nsteps, const double *state_in, double *
             int lo[3], hi[3];
             field_box(ctx, f, b, lo, hi);
             const int64_t n = field_count(ctx, f, b);
+            prof_begin(ctx, "k_aos_to_soa");
             k_aos_to_soa<<<grid_for(n), kThreads, 0, ctx->stream>>>(ctx->dbv, b, f, kFields[f].ncomp, lo[0], lo[1],
                                                                     lo[2], hi[0] - lo[0], hi[1] - lo[1],
                                                                     hi[2] - lo[2], ctx->staging + off);
@@ -678,6 +728,7 @@ int mhd_step_host(mhd_ctx *ctx, int32_t nsteps, const double *state_in, double *
             int lo[3], hi[3];
             field_box(ctx, f, b, lo, hi);
             const int64_t n = field_count(ctx, f, b);
+            prof_begin(ctx, "k_soa_to_aos");
             k_soa_to_aos<<<grid_for(n), kThreads, 0, ctx->stream>>>(ctx->dbv, b, f, kFields[f].ncomp, lo[0], lo[1],
                                                                     lo[2], hi[0] - lo[0], hi[1] - lo[1],
                                                                     hi[2] - lo[2], ctx->staging + off);
@@ -710,6 +761,7 @@ int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
     switch (stage_id)
     {
     case MHD_STAGE_TIMESTEP:
+        prof_begin(ctx, "k_begin_step");
         k_begin_step<<<1, 1, 0, ctx->stream>>>(ctx->dt_key, ctx->dt, ctx->err, ctx->prm.dt_abort);
         RUN(launched(ctx));
         break;
@@ -725,6 +777,7 @@ int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
             int64_t nf = 0;
             for (int l = LOC_FXI; l <= LOC_FZETA; ++l)
                 nf = max_box(ctx, l, 0) > nf ? max_box(ctx, l, 0) : nf;
+            prof_begin(ctx, "k_curl_e2f");
             k_curl_e2f<<<dim3(grid_for(nf), ctx->nblocks, 3), kThreads, 0, ctx->stream>>>(ctx->dbv, F_Exi, -1, F_Bxi,
                                                                                          -1.0, ctx->dt, 1.0);
             RUN(launched(ctx));
@@ -766,6 +819,44 @@ int mhd_set_time(mhd_ctx *ctx, double dt, double time, int64_t step)
 }
 
 int64_t mhd_kernel_launches(const mhd_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+int mhd_profile_step(mhd_ctx *ctx, int32_t cap, int32_t *kernel_ids, float *ms, int32_t *count)
+{
+    if (!ctx || !count || cap < 0)
+        return MHD_EINVAL;
+    ctx->profiling = true;
+    ctx->prof_ev.clear();
+    ctx->prof_names.clear();
+    const int rc = launch_step(ctx);
+    ctx->profiling = false;
+    if (rc != MHD_OK)
+        return rc;
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    const int n = int(ctx->prof_names.size());
+    *count = n;
+    for (int q = 0; q < n && q < cap; ++q)
+    {
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, ctx->prof_ev[size_t(2 * q)], ctx->prof_ev[size_t(2 * q + 1)]);
+        if (ms)
+            ms[q] = t;
+        if (kernel_ids)
+        {
+            int id = 0;
+            for (; id < kNumKernelNames; ++id)
+                if (std::strcmp(kKernelNames[id], ctx->prof_names[size_t(q)]) == 0)
+                    break;
+            kernel_ids[q] = id;
+        }
+    }
+    for (auto e : ctx->prof_ev)
+        cudaEventDestroy(e);
+    ctx->prof_ev.clear();
+    ctx->prof_names.clear();
+    return check_err(ctx);
+}
+
+const char *mhd_kernel_name(int32_t id) { return (id >= 0 && id < kNumKernelNames) ? kKernelNames[id] : ""; }
 
 void *mhd_stream(const mhd_ctx *ctx) { return ctx ? static_cast<void *>(ctx->stream) : nullptr; }
 

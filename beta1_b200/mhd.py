@@ -60,6 +60,9 @@ _SIGS = {
     "mhd_get_time": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "mhd_set_time": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_int64]),
     "mhd_kernel_launches": (C.c_int64, [C.c_void_p]),
+    "mhd_profile_step": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_float),
+                                   C.POINTER(C.c_int32)]),
+    "mhd_kernel_name": (C.c_char_p, [C.c_int32]),
     "mhd_stream": (C.c_void_p, [C.c_void_p]),
 }
 
@@ -184,6 +187,15 @@ class Context:
 
     def launches(self) -> int:
         return int(self.lib.mhd_kernel_launches(self.h))
+
+    def profile_step(self):
+        """One eager StepOnce with per-launch CUDA events: list of (kernel, ms)."""
+        cap = 4096
+        ids = (C.c_int32 * cap)()
+        ms = (C.c_float * cap)()
+        n = C.c_int32()
+        self._check(self.lib.mhd_profile_step(self.h, cap, ids, ms, C.byref(n)), "profile_step")
+        return [(self.lib.mhd_kernel_name(ids[q]).decode(), float(ms[q])) for q in range(min(n.value, cap))]
 
     def stream(self) -> int:
         return int(self.lib.mhd_stream(self.h) or 0)

@@ -153,6 +153,14 @@ int mhd_set_time(mhd_ctx *ctx, double dt, double time, int64_t step);
 /* Launch statistics: number of kernels this library launched since creation. */
 int64_t mhd_kernel_launches(const mhd_ctx *ctx);
 
+/* One StepOnce launched kernel by kernel (no graph) with a CUDA event pair
+   around every launch: fills kernel_ids[q] / ms[q] for the first `cap`
+   launches and *count with the number of launches. */
+int mhd_profile_step(mhd_ctx *ctx, int32_t cap, int32_t *kernel_ids, float *ms, int32_t *count);
+
+/* Name of a kernel id reported by mhd_profile_step. */
+const char *mhd_kernel_name(int32_t id);
+
 /* CUDA stream of the context (cudaStream_t), for callers that time with events. */
 void *mhd_stream(const mhd_ctx *ctx);
 
