@@ -322,6 +322,21 @@ def _embed(interior: np.ndarray, loc: int, ncell, nghost: int, ncomp: int) -> rs
 
 def initial_state(spec: CaseSpec, rho0=1.0, p0=0.1, v0=(0.1, 0.0, 0.0), B0=(1.0, 0.0, 0.0),
                   sigma=1e-3, seed=20261203, periodic=True, gamma=GAMMA) -> rst.RestartFile:
+    """See _initial_state; B0 = None leaves the induced field to the noise
+    alone (the applied field then lives in Badd)."""
+    return _initial_state(spec, rho0, p0, v0, B0, sigma, seed, periodic, gamma)
+
+
+def inflow_state(spec: CaseSpec, sigma=1e-3, seed=20261203) -> rst.RestartFile:
+    """Farfield state everywhere plus seeded noise; the induced B is the curl
+    of a random edge potential only (the IMF enters through Badd)."""
+    from . import physics
+    q, _ = physics.farfield_state(spec.params)
+    p0 = (GAMMA - 1.0) * (q[4] - 0.5 * (q[1] ** 2 + q[2] ** 2 + q[3] ** 2) / q[0])
+    return _initial_state(spec, q[0], p0, (q[1] / q[0], q[2] / q[0], q[3] / q[0]), None, sigma, seed, False, GAMMA)
+
+
+def _initial_state(spec, rho0, p0, v0, B0, sigma, seed, periodic, gamma) -> rst.RestartFile:
     """Uniform state plus seeded Gaussian noise (numpy PCG64): rho and the
     three velocity components per cell, then a random edge potential whose
     face circulation is added to B, so div B stays at round-off.  U_H holds
@@ -340,7 +355,7 @@ def initial_state(spec: CaseSpec, rho0=1.0, p0=0.1, v0=(0.1, 0.0, 0.0), B0=(1.0,
         U = np.stack([rho, rho * vel[0], rho * vel[1], rho * vel[2], E], axis=-1)
         fields["U_H"].blocks.append(_embed(U, rst.CELL, (ni, nj, nk), ng, 5))
         Sxi, Set, Sze = _face_area_vectors(blk.x, blk.y, blk.z)
-        b = np.asarray(B0, dtype=float)
+        b = np.asarray(B0 if B0 is not None else (0.0, 0.0, 0.0), dtype=float)
         bxi, bet, bze = Sxi @ b, Set @ b, Sze @ b
         h2 = float(np.mean(np.linalg.norm(Sxi, axis=-1)))
         if periodic:
@@ -357,3 +372,216 @@ def initial_state(spec: CaseSpec, rho0=1.0, p0=0.1, v0=(0.1, 0.0, 0.0), B0=(1.0,
         fields["B_eta"].blocks.append(_embed(bet + det, rst.FACE_ET, (ni, nj, nk), ng, 1))
         fields["B_zeta"].blocks.append(_embed(bze + dze, rst.FACE_ZE, (ni, nj, nk), ng, 1))
     return rst.RestartFile(0, 0.0, len(spec.blocks), fields)
+
+
+# --------------------------------------------------------------------------
+# Six-block cubed-sphere shell
+# --------------------------------------------------------------------------
+
+# cube faces: centre direction, first and second tangential axes; (r, e1, e2)
+# is right-handed for every face
+_CUBE_FACES = [
+    ((1, 0, 0), (0, 1, 0), (0, 0, 1)),
+    ((-1, 0, 0), (0, -1, 0), (0, 0, 1)),
+    ((0, 1, 0), (-1, 0, 0), (0, 0, 1)),
+    ((0, -1, 0), (1, 0, 0), (0, 0, 1)),
+    ((0, 0, 1), (0, 1, 0), (-1, 0, 0)),
+    ((0, 0, -1), (0, 1, 0), (1, 0, 0)),
+]
+
+
+def cubed_sphere_blocks(nr: int, na: int, r0: float = 1.0, r1: float = 8.0) -> List[BlockGrid]:
+    """Six blocks of nr log-spaced radial cells over [r0, r1] (index i, outward)
+    times na x na equiangular gnomonic cells (indices j, k).  Inner radius is a
+    Solid_Surface, outer radius a Farfield."""
+    r = r0 * (r1 / r0) ** (np.arange(nr + 1) / nr)
+    a = -np.pi / 4 + (np.pi / 2) * np.arange(na + 1) / na
+    TA, TB = np.meshgrid(np.tan(a), np.tan(a), indexing="ij")
+    blocks = []
+    for c, e1, e2 in _CUBE_FACES:
+        c, e1, e2 = (np.asarray(v, dtype=float) for v in (c, e1, e2))
+        d = c[None, None, :] + TA[..., None] * e1[None, None, :] + TB[..., None] * e2[None, None, :]
+        d = d / np.linalg.norm(d, axis=-1, keepdims=True)
+        P = r[:, None, None, None] * d[None, :, :, :]
+        blk = BlockGrid("Fluid", P[..., 0].copy(), P[..., 1].copy(), P[..., 2].copy())
+        blk.physical = [((0, 0, 0, na, 0, na), "Solid_Surface"), ((nr, nr, 0, na, 0, na), "Farfield")]
+        blocks.append(blk)
+    return blocks
+
+
+def _face_nodes(b: BlockGrid, axis: int, side: int) -> np.ndarray:
+    P = np.stack([b.x, b.y, b.z], axis=-1)
+    idx = [slice(None)] * 3
+    idx[axis] = 0 if side == 0 else P.shape[axis] - 1
+    return P[tuple(idx)]
+
+
+def match_interfaces(blocks: List[BlockGrid], tol: float = 1e-9) -> List[List[InnerFace]]:
+    """Finds conforming block faces by node coordinates and writes each pair in
+    the inner-file convention: on the first side the first tangential axis
+    runs 1..N (positive), the second -1..-N (negative); on the target side the
+    axis matching the first carries positive, the one matching the second
+    negative indices, each descending where the target runs the opposite way
+    (pairing rules of include/1_grid/Grid_Boundary.h:236-330 and
+    src/2_topology/2_MPCNS_Topology.cpp:76-160).  The neighbour's entry is
+    the exact mirror (its range = our target range and vice versa), which is
+    how the reader pairs the two sides (src/1_grid/1_MPCNS_Grid.cpp:468-520)."""
+    inner: List[List[InnerFace]] = [[] for _ in blocks]
+    done = {}
+    faces = [(ia, ax, sd) for ia in range(len(blocks)) for ax in range(3) for sd in (0, 1)]
+    for (ia, axA, sA) in faces:
+        A = blocks[ia]
+        if (ia, axA, sA) in done:
+            continue
+        FA = _face_nodes(A, axA, sA)
+        found = None
+        for (ib, axB, sB) in faces:
+            if (ib, axB, sB) == (ia, axA, sA):
+                continue
+            m = _match(FA, _face_nodes(blocks[ib], axB, sB), tol)
+            if m is not None:
+                found = (ib, axB, sB, m)
+                break
+        if not found:
+            continue
+        ib, axB, sB, (t1B, rev1, t2B, rev2) = found
+        B = blocks[ib]
+        nA = [s_ - 1 for s_ in A.x.shape]
+        nB = [s_ - 1 for s_ in B.x.shape]
+        tA = [d for d in range(3) if d != axA]
+        tBax = [d for d in range(3) if d != axB]
+        rngA = [0] * 6
+        rngB = [0] * 6
+        for d in range(3):
+            if d == axA:
+                v = 1 if sA == 0 else nA[d] + 1
+                rngA[2 * d], rngA[2 * d + 1] = v, v
+            elif d == tA[0]:
+                rngA[2 * d], rngA[2 * d + 1] = 1, nA[d] + 1
+            else:
+                rngA[2 * d], rngA[2 * d + 1] = -1, -(nA[d] + 1)
+        for d in range(3):
+            if d == axB:
+                v = 1 if sB == 0 else nB[d] + 1
+                rngB[2 * d], rngB[2 * d + 1] = v, v
+            elif d == tBax[t1B]:
+                lo_, hi_ = 1, nB[d] + 1
+                rngB[2 * d], rngB[2 * d + 1] = (hi_, lo_) if rev1 else (lo_, hi_)
+            else:
+                lo_, hi_ = -1, -(nB[d] + 1)
+                rngB[2 * d], rngB[2 * d + 1] = (hi_, lo_) if rev2 else (lo_, hi_)
+        inner[ia].append(InnerFace(tuple(rngA), ia + 1, tuple(rngB), ib + 1))
+        inner[ib].append(InnerFace(tuple(rngB), ib + 1, tuple(rngA), ia + 1))
+        done[(ia, axA, sA)] = True
+        done[(ib, axB, sB)] = True
+    return inner
+
+
+def _match(FA: np.ndarray, FB: np.ndarray, tol: float):
+    """If face node arrays coincide up to an axis swap/reversal, returns
+    (which B tangential axis matches A's first, reversed?, the one matching
+    A's second, reversed?)."""
+    for swap in (False, True):
+        G = np.transpose(FB, (1, 0, 2)) if swap else FB
+        if G.shape[:2] != FA.shape[:2]:
+            continue
+        for r1 in (False, True):
+            for r2 in (False, True):
+                H = G[::-1] if r1 else G
+                H = H[:, ::-1] if r2 else H
+                if np.max(np.abs(H - FA)) < tol:
+                    # A axis 0 <-> B axis (1 if swap else 0)
+                    t1B = 1 if swap else 0
+                    t2B = 0 if swap else 1
+                    rev1 = r1
+                    rev2 = r2
+                    return t1B, rev1, t2B, rev2
+    return None
+
+
+def cubed_sphere_case(nr=96, na=48, **param_over) -> CaseSpec:
+    blocks = cubed_sphere_blocks(nr, na)
+    return CaseSpec(blocks, match_interfaces(blocks), default_params(**param_over))
+
+
+def inflow_params(mach_u=8.0, B=(0.0, 0.5 / math.sqrt(2.0), 0.5 / math.sqrt(2.0)), p0=0.05, **over):
+    """Parameters whose Farfield/initial state (BuildLunarBackgroundState,
+    Z4_Lunar/include/0_BackgroundState.h:20-66) is rho = 1, v = (-mach_u, 0, 0),
+    p = p0 and B = `B` in nondimensional units."""
+    p = default_params(**over)
+    r = p["REF"]
+    k_B = R_UNI / NA
+    rho_ref = r["Molecular_mass"] / NA * r["n"]
+    T = p0 * rho_ref * r["U"] * r["U"] / (r["n"] * k_B)
+    p["INITIAL"] = dict(U=mach_u * r["U"], T=T, n=r["n"], Molecular_mass=r["Molecular_mass"], c_y=0.0, c_z=0.0,
+                        Bx=B[0] * r["B_ref"], By=B[1] * r["B_ref"], Bz=B[2] * r["B_ref"])
+    return p
+
+
+def cubed_sphere_inflow_case(nr=96, na=48, **over) -> CaseSpec:
+    blocks = cubed_sphere_blocks(nr, na)
+    return CaseSpec(blocks, match_interfaces(blocks), inflow_params(**over))
+
+
+# --------------------------------------------------------------------------
+# Tiled slab: radial direction bounded by a Solid_Surface (x = r0) and a
+# Farfield (x = r1), transverse directions periodic and split into tiles
+# --------------------------------------------------------------------------
+
+def slab_blocks(nr: int, nt: Tuple[int, int], tiles: Tuple[int, int], r0: float = 1.0, r1: float = 8.0,
+                amp: float = 0.03) -> List[BlockGrid]:
+    """Blocks of nr log-spaced cells over x in [r0, r1] (index i) times
+    nt[0] x nt[1] cells (indices j, k) each, tiles[0] x tiles[1] tiles over
+    the unit square in (y, z) with the map y = Y + amp sin(2 pi Z),
+    z = Z + amp sin(2 pi Y), periodic with period 1 in Y and Z.  All blocks
+    share one orientation (interfaces map indices by translation)."""
+    TJ, TK = tiles
+    NJ, NK = nt[0] * TJ, nt[1] * TK
+    X = r0 * (r1 / r0) ** (np.arange(nr + 1) / nr)
+    blocks = []
+    for tj in range(TJ):
+        for tk in range(TK):
+            Y = (tj * nt[0] + np.arange(nt[0] + 1)) / NJ
+            Z = (tk * nt[1] + np.arange(nt[1] + 1)) / NK
+            XX, YY, ZZ = np.meshgrid(X, Y, Z, indexing="ij")
+            x = XX.copy()
+            y = YY + amp * np.sin(2.0 * np.pi * ZZ)
+            z = ZZ + amp * np.sin(2.0 * np.pi * YY)
+            blk = BlockGrid("Fluid", x, y, z)
+            blk.physical = [((0, 0, 0, nt[0], 0, nt[1]), "Solid_Surface"),
+                            ((nr, nr, 0, nt[0], 0, nt[1]), "Farfield")]
+            blocks.append(blk)
+    return blocks
+
+
+def slab_interfaces(nr: int, nt: Tuple[int, int], tiles: Tuple[int, int]) -> List[List[InnerFace]]:
+    """Transverse interfaces of the tile array (with wrap-around).  Every
+    interface is flagged periodic (negative block numbers), so that ghost
+    nodes are built by reflection (the reference skips the node copy for
+    periodic interfaces, src/1_grid/1_MPCNS_Grid.cpp:1262-1281)."""
+    TJ, TK = tiles
+    I, J, K = nr + 1, nt[0] + 1, nt[1] + 1
+
+    def bid(tj, tk):
+        return (tj % TJ) * TK + (tk % TK)
+
+    inner = [[] for _ in range(TJ * TK)]
+    jmin = (1, I, 1, 1, -1, -K)
+    jmax = (1, I, J, J, -1, -K)
+    kmin = (1, I, -1, -J, 1, 1)
+    kmax = (1, I, -1, -J, K, K)
+    for tj in range(TJ):
+        for tk in range(TK):
+            b = bid(tj, tk)
+            inner[b].append(InnerFace(jmin, -(b + 1), jmax, -(bid(tj - 1, tk) + 1)))
+            inner[b].append(InnerFace(jmax, -(b + 1), jmin, -(bid(tj + 1, tk) + 1)))
+            inner[b].append(InnerFace(kmin, -(b + 1), kmax, -(bid(tj, tk - 1) + 1)))
+            inner[b].append(InnerFace(kmax, -(b + 1), kmin, -(bid(tj, tk + 1) + 1)))
+    return inner
+
+
+def slab_case(nr=96, nt=(48, 48), tiles=(3, 2), **over) -> CaseSpec:
+    blocks = slab_blocks(nr, nt, tiles)
+    spec = CaseSpec(blocks, slab_interfaces(nr, nt, tiles), inflow_params(**over))
+    spec.tiles = tiles
+    return spec

@@ -44,6 +44,12 @@ int field_by_name(const char *name)
 
 struct SyncMap
 {
+    // phase A: constants and wall handlers
+    uint64_t *cdst = nullptr;
+    double *cval = nullptr;
+    int64_t nconst = 0;
+    std::vector<std::pair<int, int>> walls; // (block, direction) of Solid_Surface fluid handlers
+    // phase B: composed copies
     uint64_t *dst = nullptr;
     uint64_t *src = nullptr;
     double *tmp = nullptr; // non-null when a source is also a destination
@@ -56,7 +62,7 @@ const char *const kKernelNames[] = {"k_fluid_rhs",   "k_eface",        "k_eedge"
                                     "k_update_u",    "k_bcell",        "k_jedge",         "k_jcell",
                                     "k_pv_uplus_dt", "k_begin_step",   "k_arm_dt",        "k_end_step",
                                     "k_gather",      "k_gather_stage", "k_scatter_stage", "k_aos_to_soa",
-                                    "k_soa_to_aos"};
+                                    "k_soa_to_aos",  "k_set_consts",   "k_wall_u"};
 constexpr int kNumKernelNames = int(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
 
 } // namespace
@@ -209,9 +215,26 @@ int launched(mhd_ctx *ctx, int nk = 1)
 int run_sync(mhd_ctx *ctx, const char *group)
 {
     auto it = ctx->syncs.find(group);
-    if (it == ctx->syncs.end() || it->second.n == 0)
+    if (it == ctx->syncs.end())
         return MHD_OK;
     SyncMap &s = it->second;
+    if (s.nconst > 0)
+    {
+        prof_begin(ctx, "k_set_consts");
+        k_set_consts<<<grid_for(s.nconst), kThreads, 0, ctx->stream>>>(ctx->pool, s.cdst, s.cval, s.nconst);
+        RUN(launched(ctx));
+    }
+    for (const auto &w : s.walls)
+    {
+        const BlockView &v = ctx->hbv[size_t(w.first)];
+        const int ax = std::abs(w.second) - 1;
+        const int64_t ncol = (ax == 0) ? int64_t(v.nj) * v.nk : (ax == 1) ? int64_t(v.ni) * v.nk : int64_t(v.ni) * v.nj;
+        prof_begin(ctx, "k_wall_u");
+        k_wall_u<<<grid_for(ncol), kThreads, 0, ctx->stream>>>(ctx->dbv, w.first, w.second, ctx->c.gamma);
+        RUN(launched(ctx));
+    }
+    if (s.n == 0)
+        return MHD_OK;
     if (s.tmp)
     {
         prof_begin(ctx, "k_gather_stage");
@@ -469,6 +492,8 @@ int mhd_ctx_destroy(mhd_ctx *ctx)
         cudaFree(kv.second.dst);
         cudaFree(kv.second.src);
         cudaFree(kv.second.tmp);
+        cudaFree(kv.second.cdst);
+        cudaFree(kv.second.cval);
     }
     if (ctx->dt_key)
         cudaFree(ctx->dt_key);
@@ -627,7 +652,9 @@ int mhd_set_sync_map(mhd_ctx *ctx, const char *group, const int64_t *dst, const 
     cudaFree(m.dst);
     cudaFree(m.src);
     cudaFree(m.tmp);
-    m = SyncMap{};
+    m.dst = m.src = nullptr;
+    m.tmp = nullptr;
+    m.n = 0;
     drop_graph(ctx);
     if (n == 0)
         return MHD_OK;
@@ -638,6 +665,44 @@ int mhd_set_sync_map(mhd_ctx *ctx, const char *group, const int64_t *dst, const 
     if (staged)
         CK(ctx, cudaMalloc(&m.tmp, size_t(n) * 8));
     m.n = n;
+    return MHD_OK;
+}
+
+int mhd_set_sync_consts(mhd_ctx *ctx, const char *group, const int64_t *dst, const double *val, int64_t n)
+{
+    if (!ctx || !group || n < 0 || (n > 0 && (!dst || !val)))
+        return fail(ctx, MHD_EINVAL, "bad sync constant arguments");
+    std::vector<uint64_t> d(static_cast<size_t>(n));
+    for (int64_t t = 0; t < n; ++t)
+    {
+        const int64_t od = pool_offset(ctx, dst[t]);
+        if (od < 0)
+            return fail(ctx, MHD_EINVAL, "sync constant %lld has an invalid point id", (long long)t);
+        d[size_t(t)] = uint64_t(od);
+    }
+    SyncMap &m = ctx->syncs[group];
+    cudaFree(m.cdst);
+    cudaFree(m.cval);
+    m.cdst = nullptr;
+    m.cval = nullptr;
+    m.nconst = 0;
+    drop_graph(ctx);
+    if (n == 0)
+        return MHD_OK;
+    CK(ctx, cudaMalloc(&m.cdst, size_t(n) * 8));
+    CK(ctx, cudaMalloc(&m.cval, size_t(n) * 8));
+    CK(ctx, cudaMemcpy(m.cdst, d.data(), size_t(n) * 8, cudaMemcpyHostToDevice));
+    CK(ctx, cudaMemcpy(m.cval, val, size_t(n) * 8, cudaMemcpyHostToDevice));
+    m.nconst = n;
+    return MHD_OK;
+}
+
+int mhd_set_sync_wall(mhd_ctx *ctx, const char *group, int32_t block, int32_t direction)
+{
+    if (!ctx || !group || block < 0 || block >= ctx->nblocks || direction == 0 || direction < -3 || direction > 3)
+        return fail(ctx, MHD_EINVAL, "bad wall handler arguments");
+    ctx->syncs[group].walls.emplace_back(block, direction);
+    drop_graph(ctx);
     return MHD_OK;
 }
 
@@ -819,6 +884,21 @@ int mhd_set_time(mhd_ctx *ctx, double dt, double time, int64_t step)
 }
 
 int64_t mhd_kernel_launches(const mhd_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+int mhd_field_spec(int32_t index, const char **name, int32_t *loc, int32_t *ncomp, int32_t *nghost)
+{
+    if (index < 0 || index >= NFIELD)
+        return MHD_EINVAL;
+    if (name)
+        *name = kFields[index].name;
+    if (loc)
+        *loc = kFields[index].loc;
+    if (ncomp)
+        *ncomp = kFields[index].ncomp;
+    if (nghost)
+        *nghost = kFields[index].nghost;
+    return MHD_OK;
+}
 
 int mhd_profile_step(mhd_ctx *ctx, int32_t cap, int32_t *kernel_ids, float *ms, int32_t *count)
 {

@@ -33,6 +33,8 @@ __global__ void k_begin_step(const unsigned long long *dt_key, double *dt, int *
 __global__ void k_arm_dt(unsigned long long *dt_key);
 __global__ void k_end_step(const double *dt, double *time, long long *step);
 __global__ void k_gather(double *pool, const uint64_t *dst, const uint64_t *src, int64_t n);
+__global__ void k_set_consts(double *pool, const uint64_t *dst, const double *val, int64_t n);
+__global__ void k_wall_u(const BlockView *bvs, int blk, int dir, double gamma);
 __global__ void k_gather_stage(double *tmp, const double *pool, const uint64_t *src, int64_t n);
 __global__ void k_scatter_stage(double *pool, const double *tmp, const uint64_t *dst, int64_t n);
 __global__ void k_aos_to_soa(const BlockView *bvs, int blk, int fid, int ncomp, int lo0, int lo1, int lo2, int n0,

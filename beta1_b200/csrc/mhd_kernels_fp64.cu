@@ -676,6 +676,82 @@ __global__ void k_gather(double *__restrict__ pool, const uint64_t *__restrict__
         pool[dst[t]] = pool[src[t]];
 }
 
+// phase A of a Sync: points set to fixed values by physical handlers
+// (Farfield states, zero-curl edge EMF, zeroed wall layers)
+__global__ void k_set_consts(double *__restrict__ pool, const uint64_t *__restrict__ dst,
+                             const double *__restrict__ val, int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        pool[dst[t]] = val[t];
+}
+
+// phase A of Sync("Ucell") on a Solid_Surface face: LunarBoundary::BC_Solid_Surface_
+// (Z4_Lunar/src/boundary/Boundary_Condition_Fluid.cpp:19-185).  The first inner
+// cell layer takes the density of the next cell inwards (floored at 2.5e-3),
+// zero velocity and its pressure; every ghost layer then repeats that
+// layer's state.  One thread per boundary cell column; dir = +-1, +-2, +-3.
+__global__ void k_wall_u(const BlockView *__restrict__ bvs, int blk, int dir, double gamma)
+{
+    const BlockView &b = bvs[blk];
+    const int ax = (dir < 0 ? -dir : dir) - 1;
+    const int sgn = dir > 0 ? 1 : -1;
+    const int n[3] = {b.ni, b.nj, b.nk};
+    const int t1 = (ax == 0) ? 1 : 0;
+    const int t2 = (ax == 2) ? 1 : 2;
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= int64_t(n[t1]) * n[t2])
+        return;
+    int c[3];
+    c[t1] = int(t / n[t2]);
+    c[t2] = int(t % n[t2]);
+    c[ax] = (sgn < 0) ? 0 : n[ax] - 1;
+    const double rho_floor = 2.5e-3, p_floor = 1e-12;
+    double *U = b.f[F_U];
+    const int64_t v = b.vol;
+    auto pressure = [&](double rho, double mx, double my, double mz, double E) {
+        rho = smax(rho, rho_floor);
+        const double ke = 0.5 * (mx * mx + my * my + mz * mz) / rho;
+        double eint = E - ke;
+        if (eint < 0.0)
+            eint = 0.0;
+        double p = (gamma - 1.0) * eint;
+        return smax(p, p_floor);
+    };
+    // first layer from the cell one further inside
+    int r[3] = {c[0], c[1], c[2]};
+    r[ax] -= sgn;
+    const int64_t pr = pidx(b, r[0], r[1], r[2]);
+    const int64_t p0 = pidx(b, c[0], c[1], c[2]);
+    {
+        const double rho_r = smax(U[pr], rho_floor);
+        const double p_r = pressure(rho_r, U[v + pr], U[2 * v + pr], U[3 * v + pr], U[4 * v + pr]);
+        const double vz = 0.0;
+        const double ke_g = 0.5 * rho_r * (vz * vz + vz * vz + vz * vz);
+        U[p0] = rho_r;
+        U[v + p0] = rho_r * vz;
+        U[2 * v + p0] = rho_r * vz;
+        U[3 * v + p0] = rho_r * vz;
+        U[4 * v + p0] = p_r / (gamma - 1.0) + ke_g;
+    }
+    // ghost layers repeat the (updated) first layer
+    const double rho_r = smax(U[p0], rho_floor);
+    const double p_r = pressure(rho_r, U[v + p0], U[2 * v + p0], U[3 * v + p0], U[4 * v + p0]);
+    const double vz = 0.0;
+    const double ke_g = 0.5 * rho_r * (vz * vz + vz * vz + vz * vz);
+    for (int ng = 1; ng <= b.G; ++ng)
+    {
+        int gidx[3] = {c[0], c[1], c[2]};
+        gidx[ax] += ng * sgn;
+        const int64_t pg = pidx(b, gidx[0], gidx[1], gidx[2]);
+        U[pg] = rho_r;
+        U[v + pg] = rho_r * vz;
+        U[2 * v + pg] = rho_r * vz;
+        U[3 * v + pg] = rho_r * vz;
+        U[4 * v + pg] = p_r / (gamma - 1.0) + ke_g;
+    }
+}
+
 // two-phase variant when a source is also a destination
 __global__ void k_gather_stage(double *__restrict__ tmp, const double *__restrict__ pool,
                                const uint64_t *__restrict__ src, int64_t n)

@@ -50,6 +50,8 @@ _SIGS = {
     "mhd_point_id": (C.c_int64, [C.c_void_p, C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "mhd_set_sync_map": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64]),
     "mhd_sync": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "mhd_set_sync_consts": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64]),
+    "mhd_set_sync_wall": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_int32]),
     "mhd_update_derived": (C.c_int, [C.c_void_p]),
     "mhd_step": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "mhd_step_host": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_double)]),
@@ -64,6 +66,8 @@ _SIGS = {
                                    C.POINTER(C.c_int32)]),
     "mhd_kernel_name": (C.c_char_p, [C.c_int32]),
     "mhd_stream": (C.c_void_p, [C.c_void_p]),
+    "mhd_field_spec": (C.c_int, [C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                 C.POINTER(C.c_int32)]),
 }
 
 _lib: Optional[C.CDLL] = None
@@ -91,6 +95,42 @@ def exported_symbols() -> List[str]:
 
 class MHDError(RuntimeError):
     pass
+
+
+def field_table():
+    """[(name, loc, ncomp, nghost)] in the library's field-index order."""
+    lib = load()
+    out = []
+    i = 0
+    while True:
+        nm, loc, nc, ng = C.c_char_p(), C.c_int32(), C.c_int32(), C.c_int32()
+        if lib.mhd_field_spec(i, C.byref(nm), C.byref(loc), C.byref(nc), C.byref(ng)) != MHD_OK:
+            break
+        out.append((nm.value.decode(), loc.value, nc.value, ng.value))
+        i += 1
+    return out
+
+
+class HostLayout:
+    """Host-side twin of a context's field addressing (field boxes and point
+    ids), usable without a GPU to compile sync tables."""
+
+    PLUS = {0: (0, 0, 0), 1: (1, 0, 0), 2: (0, 1, 0), 3: (0, 0, 1), 4: (0, 1, 1), 5: (1, 0, 1), 6: (1, 1, 0)}
+
+    def __init__(self, ncells):
+        self.ncells = [tuple(map(int, n)) for n in ncells]
+        self.table = field_table()
+        self.index = {t[0]: i for i, t in enumerate(self.table)}
+
+    def field_info(self, name, block=0):
+        _, loc, nc, ng = self.table[self.index[name]]
+        n = self.ncells[block]
+        p = self.PLUS[loc]
+        return dict(loc=loc, ncomp=nc, nghost=ng, lo=(-ng, -ng, -ng),
+                    hi=(n[0] + p[0] + ng, n[1] + p[1] + ng, n[2] + p[2] + ng))
+
+    def point_base(self, name, block):
+        return (self.index[name] << 56) | (int(block) << 40)
 
 
 class Context:
@@ -156,6 +196,16 @@ class Context:
         assert d.shape == s.shape
         self._check(self.lib.mhd_set_sync_map(self.h, group.encode(), d.ctypes.data, s.ctypes.data, d.size),
                     f"set_sync_map {group}")
+
+    def set_sync_consts(self, group: str, dst: np.ndarray, val: np.ndarray):
+        d = np.ascontiguousarray(dst, dtype=np.int64)
+        v = np.ascontiguousarray(val, dtype=np.float64)
+        assert d.shape == v.shape
+        self._check(self.lib.mhd_set_sync_consts(self.h, group.encode(), d.ctypes.data, v.ctypes.data, d.size),
+                    f"set_sync_consts {group}")
+
+    def set_sync_wall(self, group: str, block: int, direction: int):
+        self._check(self.lib.mhd_set_sync_wall(self.h, group.encode(), block, direction), f"set_sync_wall {group}")
 
     def sync(self, group: str):
         self._check(self.lib.mhd_sync(self.h, group.encode()), f"sync {group}")

@@ -23,24 +23,55 @@ def make_params(p, precision=mhd.PREC_FP64) -> mhd.Params:
                       precision=int(precision))
 
 
+def badd_faces(JD: np.ndarray, B0) -> np.ndarray:
+    """Applied field flux of the IMF on every face (DipoleField::Build_Badd_FaceFlux
+    without dipoles, Z4_Lunar/include/operators/Dipole.h:89-375): B0 . JD."""
+    return ((B0[0] * JD[..., 0] + B0[1] * JD[..., 1]) + B0[2] * JD[..., 2])[..., None]
+
+
 class Solver:
     def __init__(self, spec: case_mod.CaseSpec, topology: str = "periodic", precision=mhd.PREC_FP64):
         self.spec = spec
         ngg = int(spec.params["ngg"])
         self.ctx = mhd.Context([b.ncell for b in spec.blocks], make_params(spec.params, precision))
         self.geom = []
+        self.nodes = []
+        _, B_imf = physics.farfield_state(spec.params)
         for ib, b in enumerate(spec.blocks):
             X = geometry.ghost_mesh(b.x, b.y, b.z, ngg)
             g = geometry.build(X, b.ncell, ngg)
             for name in GEOM_FIELDS:
                 lo, hi, a = g[name]
                 self.ctx.upload(name, ib, a)
+            if any(v != 0.0 for v in B_imf):
+                for fname, jd in (("Badd_xi", "JDxi"), ("Badd_eta", "JDet"), ("Badd_zeta", "JDze")):
+                    self.ctx.upload(fname, ib, badd_faces(g[jd][2], B_imf))
             self.geom.append(g)
+            self.nodes.append(X)
         if topology == "periodic":
             assert len(spec.blocks) == 1
             self.sync_sizes = syncmap.install_periodic(self.ctx, spec.blocks[0].ncell)
+        elif topology == "tiled":
+            self.install_tiled()
         else:
             raise ValueError(f"unknown topology {topology}")
+        self.ctx.sync("Badd")
+
+    def install_tiled(self):
+        spec = self.spec
+        q, B = physics.farfield_state(spec.params)
+        u = [q[1] / q[0], q[2] / q[0], q[3] / q[0]]
+        E_inf = [B[1] * u[2] - B[2] * u[1], B[2] * u[0] - B[0] * u[2], B[0] * u[1] - B[1] * u[0]]
+        resistive = bool(spec.params.get("is_Lunar_resistance", 0))
+        maps = syncmap.compile_tiled(self.ctx, syncmap.TiledLayout(spec.blocks[0].ncell, spec.tiles), resistive,
+                                     dict(qinf=q, B_imf=B, E_inf=E_inf), self.nodes)
+        self.sync_sizes = {}
+        for group, m in maps.items():
+            self.ctx.set_sync_map(group, m["dst"], m["src"])
+            self.ctx.set_sync_consts(group, m["cdst"], m["cval"])
+            for (b, d) in m["walls"]:
+                self.ctx.set_sync_wall(group, b, d)
+            self.sync_sizes[group] = (int(m["dst"].size), int(m["cdst"].size), len(m["walls"]))
 
     def load_state(self, state: rst.RestartFile):
         """Restart load + the syncs that make ghosts consistent, then

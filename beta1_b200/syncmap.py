@@ -37,6 +37,7 @@ GROUPS: Dict[str, List[str]] = {
     "Eres": ["Eres_xi", "Eres_eta", "Eres_zeta"],
     "Eres1form": ["Eres_xi", "Eres_eta", "Eres_zeta"],
     "dB": ["dB_xi", "dB_eta", "dB_zeta"],
+    "Badd": ["Badd_xi", "Badd_eta", "Badd_zeta"],
 }
 
 # +1 planes per axis of each location code (restart numbering)
@@ -84,3 +85,209 @@ def install_periodic(ctx, ncell) -> Dict[str, int]:
         ctx.set_sync_map(group, dst, src)
         sizes[group] = int(dst.size)
     return sizes
+
+
+# ---------------------------------------------------------------------------
+# Tiled layouts with physical walls
+# ---------------------------------------------------------------------------
+#
+# Blocks of one orientation tile the transverse (j, k) directions
+# periodically; the radial direction i ends in a Solid_Surface (i = 0) and a
+# Farfield (i = n_i).  A Sync(group) then is
+#   phase A: the physical handlers that compute or set values
+#            (Z4_Lunar/src/boundary/Boundary_Condition_Fluid.cpp,
+#             Boundary_Condition.cpp, Boundary_Condition_EM.cpp),
+#   phase B: every copy -- default physical copies of the ghost slab from the
+#            first inner layer (src/6_boundary/Boundary.cpp:303-331) and the
+#            face/edge/vertex halos -- composed into one gather.
+# The composition is obtained by replaying the copies on an index map.
+
+# what each handler of the shipped Lunar set-up does to a field on the
+# Solid_Surface / Farfield faces (Z4_Lunar/src/boundary/Boundary_Build.cpp:5-271):
+#   copy        ghost slab <- first inner layer
+#   nop         nothing
+#   wall_u      Solid_Surface fluid handler (phase A kernel)
+#   ghost_const ghost slab <- constant (phase A)
+#   slab_zero_copy   inner slab (and, for J_cell, the next layer) <- 0, then copy
+#   slab_const_copy  inner slab <- E_inf . dr (zero-curl far field), then copy
+#   eface_ghost_zero normal component field: inner slab <- 0; ghost slab <- 0
+
+
+def wall_rules(field: str, resistive: bool):
+    """(Solid_Surface rule, Farfield rule) of a field."""
+    if field == "U_H":
+        return "wall_u", "ghost_const"
+    if field == "U_plus":
+        return "nop", "nop"
+    if field in ("B_xi", "B_eta", "B_zeta"):
+        return "copy", "nop"
+    if field == "B_cell":
+        return "copy", "ghost_const"
+    if field == "Bind_cell":
+        return "copy", "ghost_const"
+    if field == "J_cell":
+        return ("copy" if resistive else "slab_zero2_copy"), "copy"
+    if field.startswith("Eface_"):
+        return ("eface_ghost_zero" if resistive else "slab_zero_copy"), "nop"
+    if field in ("E_xi", "E_eta", "E_zeta"):
+        return ("copy" if resistive else "nop"), "slab_const_copy"
+    if field in ("Eres_xi", "Eres_eta", "Eres_zeta"):
+        # the zero-curl handler recognises only E_xi/E_eta/E_zeta and falls
+        # back to the default copy for any other field (Boundary_Condition.cpp:573-597)
+        return "copy", "copy"
+    return "copy", "copy"
+
+
+class TiledLayout:
+    """Block b sits at tile (b // TK, b % TK); all blocks have the same cells."""
+
+    def __init__(self, ncell, tiles):
+        self.n = tuple(ncell)
+        self.TJ, self.TK = tiles
+
+    def tile(self, b):
+        return b // self.TK, b % self.TK
+
+    def block(self, tj, tk):
+        return (tj % self.TJ) * self.TK + (tk % self.TK)
+
+
+def _field_points(info):
+    lo, hi = info["lo"], info["hi"]
+    I, J, K = np.meshgrid(np.arange(lo[0], hi[0]), np.arange(lo[1], hi[1]), np.arange(lo[2], hi[2]), indexing="ij")
+    return I.ravel(), J.ravel(), K.ravel()
+
+
+def compile_tiled(ctx, layout: TiledLayout, resistive: bool, farfield_consts, node_coords):
+    """Builds phase A tables and the composed gather of every group.
+    farfield_consts: dict with 'qinf' (5), 'B_imf' (3), 'E_inf' (3).
+    node_coords: per block, Padded node array (ghost nodes included).
+    Returns {group: dict(dst, src, cdst, cval, walls)}."""
+    n = layout.n
+    nb = layout.TJ * layout.TK
+    out = {}
+    for group, fields in GROUPS.items():
+        dsts, srcs, cd, cv, walls = [], [], [], [], []
+        for f in fields:
+            info0 = ctx.field_info(f, 0)
+            loc, nc = info0["loc"], info0["ncomp"]
+            lo, hi = info0["lo"], info0["hi"]
+            pl = PLUS[loc]
+            inner_hi = (n[0] + pl[0], n[1] + pl[1], n[2] + pl[2])
+            shape = (hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2])
+            npt = shape[0] * shape[1] * shape[2]
+            I, J, K = _field_points(info0)
+            # src_of as (block, point-offset) pairs over all blocks of this field
+            sb = np.repeat(np.arange(nb), npt)
+            sp = np.tile(np.arange(npt), nb)
+            phaseA = np.zeros(nb * npt, dtype=bool)
+
+            def off(i, j, k):
+                return ((i - lo[0]) * shape[1] + (j - lo[1])) * shape[2] + (k - lo[2])
+
+            solid, far = wall_rules(f, resistive)
+            tin = (J >= 0) & (J < inner_hi[1]) & (K >= 0) & (K < inner_hi[2])
+            g_lo = tin & (I < 0)
+            g_hi = tin & (I >= inner_hi[0])
+            slab_lo = tin & (I == 0)
+            slab_hi = tin & (I == inner_hi[0] - 1)
+            for b in range(nb):
+                base = b * npt
+                # Solid_Surface (i = 0)
+                if solid == "copy":
+                    idx = np.nonzero(g_lo)[0]
+                    sp[base + idx] = off(np.zeros_like(I[idx]), J[idx], K[idx])
+                elif solid == "wall_u":
+                    sel = g_lo | slab_lo
+                    phaseA[base + np.nonzero(sel)[0]] = True
+                    walls.append((b, -1))
+                elif solid in ("slab_zero_copy", "slab_zero2_copy"):
+                    zsel = slab_lo | (tin & (I == 1)) if solid == "slab_zero2_copy" else slab_lo
+                    for m in range(nc):
+                        for q in np.nonzero(zsel)[0]:
+                            pass
+                    zidx = np.nonzero(zsel)[0]
+                    phaseA[base + zidx] = True
+                    for m in range(nc):
+                        cd.append((f, b, I[zidx], J[zidx], K[zidx], m))
+                        cv.append(np.zeros(zidx.size))
+                    idx = np.nonzero(g_lo)[0]
+                    sp[base + idx] = off(np.zeros_like(I[idx]), J[idx], K[idx])
+                elif solid == "eface_ghost_zero":
+                    normal = f == "Eface_xi"
+                    zsel = g_lo | (slab_lo if normal else np.zeros_like(g_lo))
+                    zidx = np.nonzero(zsel)[0]
+                    phaseA[base + zidx] = True
+                    for m in range(nc):
+                        cd.append((f, b, I[zidx], J[zidx], K[zidx], m))
+                        cv.append(np.zeros(zidx.size))
+                # Farfield (i = n_i)
+                if far == "copy":
+                    idx = np.nonzero(g_hi)[0]
+                    sp[base + idx] = off(np.full_like(I[idx], inner_hi[0] - 1), J[idx], K[idx])
+                elif far == "ghost_const":
+                    idx = np.nonzero(g_hi)[0]
+                    phaseA[base + idx] = True
+                    vals = {"U_H": farfield_consts["qinf"], "B_cell": farfield_consts["B_imf"],
+                            "Bind_cell": [0.0, 0.0, 0.0]}[f]
+                    for m in range(nc):
+                        cd.append((f, b, I[idx], J[idx], K[idx], m))
+                        cv.append(np.full(idx.size, float(vals[m])))
+                elif far == "slab_const_copy":
+                    sidx = np.nonzero(slab_hi)[0]
+                    phaseA[base + sidx] = True
+                    X = node_coords[b]
+                    d = {"E_xi": (1, 0, 0), "Eres_xi": (1, 0, 0), "E_eta": (0, 1, 0), "Eres_eta": (0, 1, 0),
+                         "E_zeta": (0, 0, 1), "Eres_zeta": (0, 0, 1)}[f]
+                    Ei, Ej, Ek = I[sidx], J[sidx], K[sidx]
+                    o = X.off
+                    p0 = X.a[Ei + o, Ej + o, Ek + o]
+                    p1 = X.a[Ei + d[0] + o, Ej + d[1] + o, Ek + d[2] + o]
+                    E = farfield_consts["E_inf"]
+                    val = (E[0] * (p1[:, 0] - p0[:, 0]) + E[1] * (p1[:, 1] - p0[:, 1])) + E[2] * (p1[:, 2] - p0[:, 2])
+                    cd.append((f, b, Ei, Ej, Ek, 0))
+                    cv.append(val)
+                    idx = np.nonzero(g_hi)[0]
+                    sp[base + idx] = off(np.full_like(I[idx], inner_hi[0] - 1), J[idx], K[idx])
+            # transverse halos: tangential ghost -> owner tile's point (i unchanged)
+            tg = ~tin
+            for b in range(nb):
+                tj, tk = layout.tile(b)
+                idx = np.nonzero(tg)[0]
+                Jg, Kg = J[idx], K[idx]
+                wj = (Jg < 0) | (Jg >= inner_hi[1])
+                wk = (Kg < 0) | (Kg >= inner_hi[2])
+                gj = tj * n[1] + Jg
+                gk = tk * n[2] + Kg
+                otj = np.where(wj, np.floor_divide(gj, n[1]), tj)
+                otk = np.where(wk, np.floor_divide(gk, n[2]), tk)
+                jj = np.where(wj, gj - otj * n[1], Jg)
+                kk = np.where(wk, gk - otk * n[2], Kg)
+                ob = (np.mod(otj, layout.TJ) * layout.TK + np.mod(otk, layout.TK))
+                opt = off(I[idx], jj, kk)
+                srcflat = ob * npt + opt
+                sb[b * npt + idx] = sb[srcflat]
+                sp[b * npt + idx] = sp[srcflat]
+                phaseA[b * npt + idx] = False
+            allp = np.arange(nb * npt)
+            own_b = allp // npt
+            own_p = allp % npt
+            moved = ~phaseA & ~((sb == own_b) & (sp == own_p))
+            mi = np.nonzero(moved)[0]
+            bases = np.array([ctx.point_base(f, b) for b in range(nb)], dtype=np.int64)
+            for m in range(nc):
+                dsts.append(bases[own_b[mi]] + own_p[mi] * nc + m)
+                srcs.append(bases[sb[mi]] + sp[mi] * nc + m)
+        cdst = []
+        cval = []
+        for (f, b, Ii, Jj, Kk, m), v in zip(cd, cv):
+            info = ctx.field_info(f, b)
+            base = ctx.point_base(f, b)
+            cdst.append(base + aos_index(info["lo"], info["hi"], info["ncomp"], Ii, Jj, Kk, m))
+            cval.append(v)
+        out[group] = dict(dst=np.concatenate(dsts) if dsts else np.zeros(0, np.int64),
+                          src=np.concatenate(srcs) if srcs else np.zeros(0, np.int64),
+                          cdst=np.concatenate(cdst).astype(np.int64) if cdst else np.zeros(0, np.int64),
+                          cval=np.concatenate(cval) if cval else np.zeros(0),
+                          walls=sorted(set(walls)))
+    return out

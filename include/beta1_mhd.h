@@ -95,6 +95,12 @@ int mhd_field_info(const mhd_ctx *ctx, const char *name, int32_t block, int32_t 
 int mhd_upload_field(mhd_ctx *ctx, const char *name, int32_t block, const double *data, int64_t count);
 int mhd_download_field(mhd_ctx *ctx, const char *name, int32_t block, double *data, int64_t count);
 
+/* Field table of the library (no context, no GPU needed): name, location,
+   components and ghost layers of field `index`; MHD_EINVAL past the end.
+   A point id (below) is (index << 56) | (block << 40) | AoS offset of the
+   point within the field's logical box on that block. */
+int mhd_field_spec(int32_t index, const char **name, int32_t *loc, int32_t *ncomp, int32_t *nghost);
+
 /* Point id of (field, block, i, j, k, m) for the gather tables below. */
 int64_t mhd_point_id(const mhd_ctx *ctx, const char *name, int32_t block, int32_t i, int32_t j, int32_t k,
                      int32_t m);
@@ -106,8 +112,19 @@ int64_t mhd_point_id(const mhd_ctx *ctx, const char *name, int32_t block, int32_
    sequence of copies is given as its composition: after the sync, point
    dst[n] holds the value point src[n] had before it.  Groups: "Ucell",
    "Bface", "Eface", "Eedge", "B_cell", "Jedge", "J_cell", "Uplus",
-   "Eres", "Eres1form", "dB". */
+   "Eres", "Eres1form", "dB", "Badd". */
 int mhd_set_sync_map(mhd_ctx *ctx, const char *group, const int64_t *dst, const int64_t *src, int64_t n);
+
+/* Phase A of a group's sync, run before its composed copies: points that
+   the physical handlers set to fixed values (the Farfield state of
+   BC_UH_Farfield_H_ and BC_Farfield_Bface, the zero-curl edge EMF of
+   BC_Farfield_Eedge_set_zerocurl, the zeroed wall layers of
+   BC_Solid_Surface_Jcell / BC_Solid_Surface_Eface_*, Z4_Lunar/src/boundary/
+   Boundary_Condition*.cpp), and the Solid_Surface fluid handler
+   BC_Solid_Surface_ (Boundary_Condition_Fluid.cpp:19-185) on a block face
+   (direction +-1, +-2, +-3 as in PhysicalPatch::direction). */
+int mhd_set_sync_consts(mhd_ctx *ctx, const char *group, const int64_t *dst, const double *val, int64_t n);
+int mhd_set_sync_wall(mhd_ctx *ctx, const char *group, int32_t block, int32_t direction);
 
 /* LunarBoundary::Sync(group) on the device. */
 int mhd_sync(mhd_ctx *ctx, const char *group);

@@ -42,6 +42,10 @@
 #include <utility>
 #include <vector>
 
+#include <csignal>
+#include <execinfo.h>
+#include <unistd.h>
+
 #include <mpi.h>
 #include <petscksp.h>
 #include <petscsnes.h>
@@ -208,6 +212,7 @@ struct Harness
     Halo *hal = nullptr;
     HALO_OWNER::EdgeOwnerSyncPattern edge_owner_pattern;
     std::unique_ptr<LunarSolver> solver;
+    bool topo_only = false;
 
     // Z4_Lunar/main.cpp:43-212, unchanged in substance.
     void setup()
@@ -218,6 +223,8 @@ struct Harness
         grd = new Grid;
         grd->Grid_Preprocess(par);
         topology = TOPO::build_topology(*grd, myid, par->GetInt("dimension"));
+        if (topo_only)
+            return;
         TOPO::build_topology_equiv(topology, *grd, myid, par->GetInt("dimension"), topo_equiv);
         const int ngg = par->GetInt("ngg");
         fld = new Field(grd, par, ngg);
@@ -410,6 +417,26 @@ int cmd_probe(Harness &h, const std::string &state, const std::string &group, co
     return 0;
 }
 
+// Topology summary: physical, inner, edge and vertex patches (text).
+int cmd_topo(Harness &h, const std::string &out)
+{
+    std::ofstream o(out);
+    const auto &t = h.topology;
+    for (const auto &p : t.physical_patches)
+        o << "physical " << p.this_block << " " << p.bc_name << " dir " << p.direction << " box " << p.this_box_node.lo.i
+          << " " << p.this_box_node.lo.j << " " << p.this_box_node.lo.k << " " << p.this_box_node.hi.i << " "
+          << p.this_box_node.hi.j << " " << p.this_box_node.hi.k << "\n";
+    for (const auto &p : t.inner_patches)
+        o << "inner " << p.this_block << "->" << p.nb_block << " [" << p.this_block_name << "|" << p.nb_block_name
+          << "] coupling " << p.is_coupling << " perm " << p.trans.perm[0] << p.trans.perm[1] << p.trans.perm[2]
+          << " sign " << p.trans.sign[0] << " " << p.trans.sign[1] << " " << p.trans.sign[2] << " off "
+          << p.trans.offset.i << " " << p.trans.offset.j << " " << p.trans.offset.k << "\n";
+    o << "inner_edge " << t.inner_edge_patches.size() << " physical_edge " << t.physical_edge_patches.size()
+      << " inner_vertex " << t.inner_vertex_patches.size() << " physical_vertex " << t.physical_vertex_patches.size()
+      << "\n";
+    return 0;
+}
+
 int cmd_time(Harness &h, const std::string &state, int nsteps)
 {
     h.load_state(state);
@@ -434,8 +461,19 @@ int cmd_time(Harness &h, const std::string &state, int nsteps)
 
 } // namespace
 
+// On abort (e.g. a failed bounds assertion in a checked build) print the
+// call stack, to locate the failing reference routine.
+void on_abort(int)
+{
+    void *frames[64];
+    const int n = backtrace(frames, 64);
+    backtrace_symbols_fd(frames, n, 2);
+    _exit(134);
+}
+
 int main(int argc, char **argv)
 {
+    std::signal(SIGABRT, on_abort);
     if (argc < 3)
     {
         std::fprintf(stderr, "usage: ref_lunar geom|run|probe|time ...\n");
@@ -450,9 +488,13 @@ int main(int argc, char **argv)
         std::ofstream sink("ref_harness.log");
         std::cout.rdbuf(sink.rdbuf());
         Harness h;
+        if (std::string(argv[1]) == "topo")
+            h.topo_only = true;
         h.setup();
         const std::string cmd = argv[1];
-        if (cmd == "geom")
+        if (cmd == "topo")
+            rc = cmd_topo(h, argv[2]);
+        else if (cmd == "geom")
             rc = cmd_geom(h, argv[2]);
         else if (cmd == "run" && argc >= 5)
             rc = cmd_run(h, argv[2], std::atoi(argv[3]), argv[4]);

@@ -86,7 +86,35 @@ def periodic(n=(8, 6, 5), steps=2, seed=20261203):
     print("wrote", tag)
 
 
+def slab(nr=6, nt=(5, 6), tiles=(2, 2), steps=2, resistive=0, implicit=0, seed=20261204):
+    tag = "slab_%dx%dx%d_t%dx%d_r%d%d" % ((nr,) + tuple(nt) + tuple(tiles) + (resistive, implicit))
+    with tempfile.TemporaryDirectory() as d:
+        spec = case.slab_case(nr, nt, tiles, is_Lunar_resistance=resistive, use_implicit_lunar_resistance=implicit)
+        case.write_case(d, spec)
+        st = case.inflow_state(spec, seed=seed)
+        rst.write(os.path.join(d, "init.rst"), st)
+        run(["run", "init.rst", str(steps), "step"], d)
+        arr = {}
+        for b in range(len(spec.blocks)):
+            for k, v in flatten(st, ["U_H", "B_xi", "B_eta", "B_zeta"], b).items():
+                arr["init/b%d/%s" % (b, k)] = v
+        for s_ in range(steps + 1):
+            r = rst.read(os.path.join(d, "step_%04d.bin" % s_))
+            for b in range(len(spec.blocks)):
+                for k, v in flatten(r, STEP_FIELDS + ["Eres_xi", "Eres_eta", "Eres_zeta"], b).items():
+                    arr["s%d/b%d/%s" % (s_, b, k)] = v
+            arr["s%d/dt" % s_] = r.fields["dt"].blocks[0].data.reshape(())
+        arr["nr"] = np.array(nr)
+        arr["nt"] = np.array(nt)
+        arr["tiles"] = np.array(tiles)
+        arr["resistive"] = np.array([resistive, implicit])
+        arr["seed"] = np.array(seed)
+        np.savez_compressed(os.path.join(OUT, tag + "_steps.npz"), **arr)
+    print("wrote", tag)
+
+
 if __name__ == "__main__":
     if not os.path.exists(REF_BIN):
         sys.exit("build the oracle first: make -C oracle -j8")
     periodic((8, 6, 5), steps=2)
+    slab(steps=2)

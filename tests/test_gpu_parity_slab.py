@@ -1,0 +1,76 @@
+"""GPU parity on a multi-block layout with physical walls: four blocks
+tiling the transverse directions periodically, a Solid_Surface at x = 1 and
+a Farfield at x = 8, against the reference solver's own outputs
+(tests/golden/make_golden.py, slab()).  Exercises the compiled syncs with
+their physical-handler phase (wall kernel, far-field constants) and the
+inter-block halos.  FP64 tolerance 1e-12 relative L2 per field per step."""
+import numpy as np
+import pytest
+
+from conftest import load_golden, rel_l2
+
+from beta1_b200 import case, rst, solver
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+FIELDS = ["U_H", "B_xi", "B_eta", "B_zeta", "PV_H", "U_plus", "B_cell", "Bind_cell", "J_xi", "J_eta", "J_zeta",
+          "J_cell", "E_xi", "E_eta", "E_zeta", "Eface_xi", "Eface_eta", "Eface_zeta", "RHS_H", "RHS_B_xi",
+          "RHS_B_eta", "RHS_B_zeta"]
+LOCS = {"U_H": rst.CELL, "B_xi": rst.FACE_XI, "B_eta": rst.FACE_ET, "B_zeta": rst.FACE_ZE}
+
+
+def slab_setup(g):
+    nr = int(g["nr"])
+    nt = tuple(int(v) for v in g["nt"])
+    tiles = tuple(int(v) for v in g["tiles"])
+    res = [int(v) for v in g["resistive"]]
+    spec = case.slab_case(nr, nt, tiles, is_Lunar_resistance=res[0], use_implicit_lunar_resistance=res[1])
+    st = rst.RestartFile(0, 0.0, len(spec.blocks), {})
+    for name, loc in LOCS.items():
+        rec = rst.FieldRecord(name, loc, 5 if name == "U_H" else 1, 4)
+        for b in range(len(spec.blocks)):
+            a = g["init/b%d/%s" % (b, name)]
+            lo = tuple(int(v) for v in g["init/b%d/%s__lo" % (b, name)])
+            rec.blocks.append(rst.FieldArray(lo, tuple(l + s for l, s in zip(lo, a.shape[:3])), a))
+        st.fields[name] = rec
+    return spec, st
+
+
+@pytest.fixture(scope="module")
+def slab_run():
+    g = load_golden("slab_6x5x6_t2x2_r00_steps.npz")
+    spec, st = slab_setup(g)
+    s = solver.Solver(spec, topology="tiled")
+    s.load_state(st)
+    nb = len(spec.blocks)
+    out = {0: {(f, b): s.field(f, b) for f in FIELDS for b in range(nb)}}
+    dts = {}
+    nsteps = max(int(k.split("/")[0][1:]) for k in g.files if k[0] == "s" and k[1].isdigit())
+    for n in range(1, nsteps + 1):
+        dts[n], _ = s.step(1)
+        out[n] = {(f, b): s.field(f, b) for f in FIELDS for b in range(nb)}
+    s.ctx.close()
+    return g, out, dts, nsteps, nb
+
+
+def test_slab_fields_match_reference(slab_run):
+    g, out, dts, nsteps, nb = slab_run
+    worst = 0.0
+    for n in range(nsteps + 1):
+        for f in FIELDS:
+            if n == 0 and f.startswith(("E", "RHS")):
+                continue
+            for b in range(nb):
+                ref = g["s%d/b%d/%s" % (n, b, f)]
+                got = out[n][(f, b)]
+                e = rel_l2(got, ref)
+                worst = max(worst, e)
+                assert e <= TOL, f"step {n} block {b} field {f}: rel L2 {e:.3e}"
+    print("slab: max rel L2 %.3e" % worst)
+
+
+def test_slab_dt_matches_reference(slab_run):
+    g, out, dts, nsteps, nb = slab_run
+    for n in range(1, nsteps + 1):
+        assert dts[n] == float(g["s%d/dt" % n])
