@@ -532,17 +532,19 @@ def slab_blocks(nr: int, nt: Tuple[int, int], tiles: Tuple[int, int], r0: float 
                 amp: float = 0.03) -> List[BlockGrid]:
     """Blocks of nr log-spaced cells over x in [r0, r1] (index i) times
     nt[0] x nt[1] cells (indices j, k) each, tiles[0] x tiles[1] tiles over
-    the unit square in (y, z) with the map y = Y + amp sin(2 pi Z),
+    the square [-1/2, 1/2)^2 in (Y, Z) with the map y = Y + amp sin(2 pi Z),
     z = Z + amp sin(2 pi Y), periodic with period 1 in Y and Z.  All blocks
-    share one orientation (interfaces map indices by translation)."""
+    share one orientation (interfaces map indices by translation).  The
+    reference's resistive shell 0.84 < |x| < 1.04 then covers the patch of
+    the wall around y = z = 0."""
     TJ, TK = tiles
     NJ, NK = nt[0] * TJ, nt[1] * TK
     X = r0 * (r1 / r0) ** (np.arange(nr + 1) / nr)
     blocks = []
     for tj in range(TJ):
         for tk in range(TK):
-            Y = (tj * nt[0] + np.arange(nt[0] + 1)) / NJ
-            Z = (tk * nt[1] + np.arange(nt[1] + 1)) / NK
+            Y = (tj * nt[0] + np.arange(nt[0] + 1)) / NJ - 0.5
+            Z = (tk * nt[1] + np.arange(nt[1] + 1)) / NK - 0.5
             XX, YY, ZZ = np.meshgrid(X, Y, Z, indexing="ij")
             x = XX.copy()
             y = YY + amp * np.sin(2.0 * np.pi * ZZ)

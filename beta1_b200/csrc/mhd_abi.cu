@@ -62,7 +62,11 @@ const char *const kKernelNames[] = {"k_fluid_rhs",   "k_eface",        "k_eedge"
                                     "k_update_u",    "k_bcell",        "k_jedge",         "k_jcell",
                                     "k_pv_uplus_dt", "k_begin_step",   "k_arm_dt",        "k_end_step",
                                     "k_gather",      "k_gather_stage", "k_scatter_stage", "k_aos_to_soa",
-                                    "k_soa_to_aos",  "k_set_consts",   "k_wall_u"};
+                                    "k_soa_to_aos",  "k_set_consts",   "k_wall_u",
+                                    "k_alias_copy",  "k_scatter_vec",  "k_resist_out",    "k_resist_rhs",
+                                    "k_dots_partial", "k_dots_final",  "k_sub_proj",      "k_add_small",
+                                    "k_div_dev",     "k_gmres_column", "k_gmres_start",   "k_gmres_solve_y",
+                                    "k_add_basis",   "k_residual"};
 constexpr int kNumKernelNames = int(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
 
 } // namespace
@@ -79,9 +83,9 @@ struct mhd_ctx
     size_t pool_n = 0;
     std::vector<std::vector<size_t>> base; // [field][block] offset in pool
     cudaStream_t stream = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t gexec = nullptr;
-    int64_t graph_kernels = 0;
+    cudaGraph_t graph = nullptr, graph_a = nullptr, graph_c = nullptr;
+    cudaGraphExec_t gexec = nullptr, gexec_a = nullptr, gexec_c = nullptr;
+    int64_t graph_kernels = 0, graph_kernels_a = 0, graph_kernels_c = 0;
     // device scalars
     unsigned long long *dt_key = nullptr;
     double *dt = nullptr;
@@ -95,6 +99,31 @@ struct mhd_ctx
     int64_t max_cells = 0;
     bool capturing = false;
     std::string msg;
+    // implicit resistive solve (LunarSolver::SolveImplicitResistiveDiffusion_)
+    struct Resistive
+    {
+        bool on = false;
+        int64_t n = 0;                 // unknowns (owner edges with eta > 0)
+        uint64_t *e = nullptr;         // pool offsets of the unknowns in Eres_*
+        uint64_t *dj = nullptr;        // ... in dJ_*
+        uint64_t *j = nullptr;         // ... in J_*
+        double *eta = nullptr;
+        int64_t nalias = 0;            // edge aliases <- owners (sync_edge_1form)
+        uint64_t *alias_e = nullptr, *owner_e = nullptr, *alias_dj = nullptr, *owner_dj = nullptr;
+        double *sign = nullptr;
+        double rtol = 1e-8, atol = 1e-12;
+        int maxit = 200, restart = 30;
+        // workspace
+        double *V = nullptr, *w = nullptr, *x = nullptr, *b = nullptr, *r = nullptr;
+        double *partial = nullptr, *dots = nullptr;
+        GmresState *st = nullptr;
+        int ngroups = 1;
+        // statistics of the last solve
+        int its = 0;
+        double rnorm = 0.0, bnorm = 0.0;
+        int reason = 0;
+    } res;
+
     // eager profiling: one event pair per launch
     bool profiling = false;
     std::vector<const char *> prof_names;
@@ -309,7 +338,7 @@ int launch_induction(mhd_ctx *ctx, bool update_b)
     RUN(run_sync(ctx, "Eedge"));
     prof_begin(ctx, "k_curl_e2f");
     k_curl_e2f<<<dim3(grid_for(nf), nb, 3), kThreads, 0, s>>>(ctx->dbv, F_Exi, F_RBxi, update_b ? F_Bxi : -1,
-                                                               -1.0, ctx->dt, 1.0);
+                                                               -1.0, ctx->dt, 1.0, 0);
     return launched(ctx);
 }
 
@@ -321,23 +350,263 @@ int launch_update_u(mhd_ctx *ctx)
     return launched(ctx);
 }
 
-// one LunarSolver::StepOnce
-int launch_step(mhd_ctx *ctx)
+
+// ---------------------------------------------------------------------------
+// implicit resistive step (Z4_Lunar/src/implicit/Lunar_ImplicitResistive.cpp:264-518)
+// ---------------------------------------------------------------------------
+
+// clear_triplet: zero every point of three fields on every block
+int clear_fields(mhd_ctx *ctx, int f0)
 {
-    cudaStream_t s = ctx->stream;
+    for (int f = f0; f < f0 + 3; ++f)
+        for (int b = 0; b < ctx->nblocks; ++b)
+            CK(ctx, cudaMemsetAsync(ctx->pool + ctx->base[size_t(f)][size_t(b)], 0,
+                                    size_t(ctx->hbv[size_t(b)].vol) * 8 * size_t(kFields[f].ncomp), ctx->stream));
+    return MHD_OK;
+}
+
+int launch_curl(mhd_ctx *ctx, int fE0, int fR0, int fB0, double mult, int mult_is_neg_dt)
+{
+    int64_t nf = 0;
+    for (int l = LOC_FXI; l <= LOC_FZETA; ++l)
+        nf = max_box(ctx, l, 0) > nf ? max_box(ctx, l, 0) : nf;
+    prof_begin(ctx, "k_curl_e2f");
+    k_curl_e2f<<<dim3(grid_for(nf), ctx->nblocks, 3), kThreads, 0, ctx->stream>>>(ctx->dbv, fE0, fR0, fB0, mult, ctx->dt,
+                                                                                 1.0, mult_is_neg_dt);
+    return launched(ctx);
+}
+
+int launch_jedge(mhd_ctx *ctx, int fB0, int fJ0)
+{
+    int64_t ne = 0;
+    for (int l = LOC_EXI; l <= LOC_EZETA; ++l)
+        ne = max_box(ctx, l, 0) > ne ? max_box(ctx, l, 0) : ne;
+    prof_begin(ctx, "k_jedge");
+    k_jedge<<<dim3(grid_for(ne), ctx->nblocks, 3), kThreads, 0, ctx->stream>>>(ctx->dbv, fB0, fJ0, 1.0);
+    return launched(ctx);
+}
+
+int alias_copy(mhd_ctx *ctx, uint64_t *alias, uint64_t *owner)
+{
+    auto &R = ctx->res;
+    if (R.nalias == 0)
+        return MHD_OK;
+    prof_begin(ctx, "k_alias_copy");
+    k_alias_copy<<<grid_for(R.nalias), kThreads, 0, ctx->stream>>>(ctx->pool, alias, owner, R.sign, R.nalias);
+    return launched(ctx);
+}
+
+// UnpackVecToImplicitEres_: Eres <- 0, Eres[unknowns] <- x, aliases, Sync("Eres1form")
+int unpack_eres(mhd_ctx *ctx, const double *x)
+{
+    auto &R = ctx->res;
+    RUN(clear_fields(ctx, F_Eresxi));
+    prof_begin(ctx, "k_scatter_vec");
+    k_scatter_vec<<<grid_for(R.n), kThreads, 0, ctx->stream>>>(ctx->pool, R.e, x, R.n);
+    RUN(launched(ctx));
+    RUN(alias_copy(ctx, R.alias_e, R.owner_e));
+    return run_sync(ctx, "Eres1form");
+}
+
+// y = A x  (MatMultImplicitResistive_)
+int resist_matvec(mhd_ctx *ctx, const double *x, double *y)
+{
+    auto &R = ctx->res;
+    RUN(unpack_eres(ctx, x));
+    RUN(clear_fields(ctx, F_dBxi));
+    RUN(launch_curl(ctx, F_Eresxi, F_dBxi, -1, 0.0, /*mult_is_neg_dt=*/1));
+    RUN(run_sync(ctx, "dB"));
+    RUN(clear_fields(ctx, F_dJxi));
+    RUN(launch_jedge(ctx, F_dBxi, F_dJxi));
+    RUN(alias_copy(ctx, R.alias_dj, R.owner_dj));
+    RUN(run_sync(ctx, "dJ"));
+    prof_begin(ctx, "k_resist_out");
+    k_resist_out<<<grid_for(R.n), kThreads, 0, ctx->stream>>>(ctx->pool, R.e, R.dj, R.eta, y, R.n);
+    return launched(ctx);
+}
+
+int dots(mhd_ctx *ctx, const double *V, int nvec, const double *w, double *out, bool with_norm, bool accumulate)
+{
+    auto &R = ctx->res;
+    const int ny = nvec + (with_norm ? 1 : 0);
+    prof_begin(ctx, "k_dots_partial");
+    k_dots_partial<<<dim3(R.ngroups, ny), 256, 0, ctx->stream>>>(V, R.n, nvec, w, R.n, R.partial, with_norm);
+    RUN(launched(ctx));
+    prof_begin(ctx, "k_dots_final");
+    k_dots_final<<<1, 64, 0, ctx->stream>>>(R.partial, R.ngroups, ny, out, accumulate ? 1 : 0);
+    return launched(ctx);
+}
+
+int read_scalar(mhd_ctx *ctx, const double *dev, double *host)
+{
+    CK(ctx, cudaMemcpyAsync(host, dev, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return MHD_OK;
+}
+
+// Restarted GMRES from x = 0 with the convergence test
+// ||r|| <= max(rtol ||b||, atol) of the PETSc default (KSPConvergedDefault).
+int resist_gmres(mhd_ctx *ctx)
+{
+    auto &R = ctx->res;
+    const int m = R.restart;
+    const int64_t n = R.n;
+    CK(ctx, cudaMemsetAsync(R.x, 0, size_t(n) * 8, ctx->stream));
+    // ||b||
+    RUN(dots(ctx, R.b, 1, R.b, R.dots, false, false));
+    double b2 = 0.0;
+    RUN(read_scalar(ctx, R.dots, &b2));
+    R.bnorm = std::sqrt(b2);
+    const double ttol = std::max(R.rtol * R.bnorm, R.atol);
+    R.its = 0;
+    R.reason = 0;
+    bool first = true;
+    while (true)
+    {
+        // r = b - A x   (x = 0 on the first cycle: r = b)
+        if (first)
+            CK(ctx, cudaMemcpyAsync(R.r, R.b, size_t(n) * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        else
+        {
+            RUN(resist_matvec(ctx, R.x, R.w));
+            prof_begin(ctx, "k_residual");
+            k_residual<<<grid_for(n), kThreads, 0, ctx->stream>>>(R.b, R.w, R.r, n);
+            RUN(launched(ctx));
+        }
+        first = false;
+        RUN(dots(ctx, R.r, 1, R.r, R.dots, false, false));
+        prof_begin(ctx, "k_gmres_start");
+        k_gmres_start<<<1, 1, 0, ctx->stream>>>(R.st, R.dots);
+        RUN(launched(ctx));
+        double beta = 0.0;
+        RUN(read_scalar(ctx, &R.st->beta, &beta));
+        R.rnorm = beta;
+        if (beta <= ttol)
+        {
+            R.reason = (beta <= R.atol) ? 3 : 2;
+            return MHD_OK;
+        }
+        if (R.its >= R.maxit)
+        {
+            R.reason = -3;
+            return MHD_OK;
+        }
+        prof_begin(ctx, "k_div_dev");
+        k_div_dev<<<grid_for(n), kThreads, 0, ctx->stream>>>(R.V, R.r, &R.st->beta, n);
+        RUN(launched(ctx));
+        int j = 0;
+        bool done = false;
+        for (; j < m && R.its < R.maxit; ++j)
+        {
+            double *vj = R.V + int64_t(j) * n;
+            RUN(resist_matvec(ctx, vj, R.w));
+            double *hcol = R.st->hcol;
+            // classical Gram-Schmidt, twice: h = V^T w, w -= V h; h2 = V^T w, w -= V h2, h += h2
+            RUN(dots(ctx, R.V, j + 1, R.w, hcol, false, false));
+            prof_begin(ctx, "k_sub_proj");
+            k_sub_proj<<<grid_for(n), kThreads, 0, ctx->stream>>>(R.V, n, j + 1, hcol, R.w, n);
+            RUN(launched(ctx));
+            RUN(dots(ctx, R.V, j + 1, R.w, R.dots, false, false));
+            prof_begin(ctx, "k_sub_proj");
+            k_sub_proj<<<grid_for(n), kThreads, 0, ctx->stream>>>(R.V, n, j + 1, R.dots, R.w, n);
+            RUN(launched(ctx));
+            prof_begin(ctx, "k_add_small");
+            k_add_small<<<1, 32, 0, ctx->stream>>>(hcol, R.dots, j + 1);
+            RUN(launched(ctx));
+            RUN(dots(ctx, nullptr, 0, R.w, R.dots + 32, true, false)); // ||w||^2
+            prof_begin(ctx, "k_gmres_column");
+            k_gmres_column<<<1, 1, 0, ctx->stream>>>(R.st, j, R.dots + 32);
+            RUN(launched(ctx));
+            double *vn = R.V + int64_t(j + 1) * n;
+            prof_begin(ctx, "k_div_dev");
+            k_div_dev<<<grid_for(n), kThreads, 0, ctx->stream>>>(vn, R.w, &R.st->hcol[j + 1], n);
+            RUN(launched(ctx));
+            ++R.its;
+            double resid = 0.0;
+            RUN(read_scalar(ctx, &R.st->resid, &resid));
+            R.rnorm = resid;
+            int brk = 0;
+            CK(ctx, cudaMemcpy(&brk, &R.st->breakdown, sizeof(int), cudaMemcpyDeviceToHost));
+            if (resid <= ttol || brk)
+            {
+                done = true;
+                ++j;
+                break;
+            }
+        }
+        prof_begin(ctx, "k_gmres_solve_y");
+        k_gmres_solve_y<<<1, 1, 0, ctx->stream>>>(R.st, j);
+        RUN(launched(ctx));
+        prof_begin(ctx, "k_add_basis");
+        k_add_basis<<<grid_for(n), kThreads, 0, ctx->stream>>>(R.V, n, R.st, j, R.x, n);
+        RUN(launched(ctx));
+        if (done)
+        {
+            R.reason = (R.rnorm <= R.atol) ? 3 : 2;
+            return MHD_OK;
+        }
+        if (R.its >= R.maxit)
+        {
+            R.reason = -3;
+            return MHD_OK;
+        }
+    }
+}
+
+// the resistive part of StepOnce: Sync("Bface") (twice, as the driver and the
+// solver each call it), J from B*, b = eta J, solve, unpack, apply the update
+int launch_resistive(mhd_ctx *ctx)
+{
+    auto &R = ctx->res;
+    RUN(run_sync(ctx, "Bface"));
+    RUN(run_sync(ctx, "Bface"));
+    RUN(launch_jedge(ctx, F_Bxi, F_Jxi));
+    RUN(run_sync(ctx, "Jedge"));
+    if (R.n > 0)
+    {
+        prof_begin(ctx, "k_resist_rhs");
+        k_resist_rhs<<<grid_for(R.n), kThreads, 0, ctx->stream>>>(ctx->pool, R.j, R.eta, R.b, R.n);
+        RUN(launched(ctx));
+        RUN(resist_gmres(ctx));
+        RUN(unpack_eres(ctx, R.x));
+    }
+    else
+        RUN(unpack_eres(ctx, R.x));
+    // ApplyImplicitResistiveUpdate_
+    RUN(run_sync(ctx, "Eres1form"));
+    RUN(clear_fields(ctx, F_RBresxi));
+    RUN(launch_curl(ctx, F_Eresxi, F_RBresxi, F_Bxi, -1.0, 0));
+    return run_sync(ctx, "Bface");
+}
+
+// one LunarSolver::StepOnce, explicit part: dt, fluid RHS, CT induction, update
+int launch_step_a(mhd_ctx *ctx)
+{
     prof_begin(ctx, "k_begin_step");
-    k_begin_step<<<1, 1, 0, s>>>(ctx->dt_key, ctx->dt, ctx->err, ctx->prm.dt_abort);
+    k_begin_step<<<1, 1, 0, ctx->stream>>>(ctx->dt_key, ctx->dt, ctx->err, ctx->prm.dt_abort);
     RUN(launched(ctx));
     RUN(launch_fluid_rhs(ctx));
     RUN(launch_induction(ctx, /*update_b=*/true));
-    RUN(launch_update_u(ctx));
+    return launch_update_u(ctx);
+}
+
+// ... and its closing part: run data, Sync("Ucell"), Sync("Bface"), derived fields
+int launch_step_c(mhd_ctx *ctx)
+{
     prof_begin(ctx, "k_end_step");
-    k_end_step<<<1, 1, 0, s>>>(ctx->dt, ctx->time, ctx->step);
+    k_end_step<<<1, 1, 0, ctx->stream>>>(ctx->dt, ctx->time, ctx->step);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Ucell"));
     RUN(run_sync(ctx, "Bface"));
-    RUN(launch_update_derived(ctx));
-    return MHD_OK;
+    return launch_update_derived(ctx);
+}
+
+int launch_step(mhd_ctx *ctx)
+{
+    RUN(launch_step_a(ctx));
+    if (ctx->res.on)
+        RUN(launch_resistive(ctx));
+    return launch_step_c(ctx);
 }
 
 int check_err(mhd_ctx *ctx)
@@ -358,21 +627,25 @@ int check_err(mhd_ctx *ctx)
 
 void drop_graph(mhd_ctx *ctx)
 {
-    if (ctx->gexec)
-        cudaGraphExecDestroy(ctx->gexec);
-    if (ctx->graph)
-        cudaGraphDestroy(ctx->graph);
-    ctx->gexec = nullptr;
-    ctx->graph = nullptr;
+    for (auto *ge : {&ctx->gexec, &ctx->gexec_a, &ctx->gexec_c})
+        if (*ge)
+        {
+            cudaGraphExecDestroy(*ge);
+            *ge = nullptr;
+        }
+    for (auto *g : {&ctx->graph, &ctx->graph_a, &ctx->graph_c})
+        if (*g)
+        {
+            cudaGraphDestroy(*g);
+            *g = nullptr;
+        }
 }
 
-int build_graph(mhd_ctx *ctx)
+int capture(mhd_ctx *ctx, int (*body)(mhd_ctx *), cudaGraph_t *graph, cudaGraphExec_t *exec, int64_t *nodes)
 {
-    if (ctx->gexec)
-        return MHD_OK;
     const int64_t before = ctx->launches;
     CK(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    const int rc = launch_step(ctx);
+    const int rc = body(ctx);
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
     ctx->launches = before;
@@ -384,11 +657,51 @@ int build_graph(mhd_ctx *ctx)
     }
     if (e != cudaSuccess)
         return fail(ctx, MHD_ECUDA, "graph capture failed: %s", cudaGetErrorString(e));
-    ctx->graph = g;
-    CK(ctx, cudaGraphInstantiate(&ctx->gexec, g, 0));
+    *graph = g;
+    CK(ctx, cudaGraphInstantiate(exec, g, 0));
     size_t nn = 0;
     CK(ctx, cudaGraphGetNodes(g, nullptr, &nn));
-    ctx->graph_kernels = int64_t(nn);
+    *nodes = int64_t(nn);
+    return MHD_OK;
+}
+
+// The step is one CUDA graph; with the implicit resistive solve (whose
+// Krylov loop is steered by the host) it is the explicit part and the
+// closing part as two graphs around the eagerly launched solve.
+int build_graph(mhd_ctx *ctx)
+{
+    if (ctx->res.on)
+    {
+        if (!ctx->gexec_a)
+            RUN(capture(ctx, launch_step_a, &ctx->graph_a, &ctx->gexec_a, &ctx->graph_kernels_a));
+        if (!ctx->gexec_c)
+            RUN(capture(ctx, launch_step_c, &ctx->graph_c, &ctx->gexec_c, &ctx->graph_kernels_c));
+        return MHD_OK;
+    }
+    if (ctx->gexec)
+        return MHD_OK;
+    return capture(ctx, launch_step, &ctx->graph, &ctx->gexec, &ctx->graph_kernels);
+}
+
+int run_steps(mhd_ctx *ctx, int nsteps)
+{
+    RUN(build_graph(ctx));
+    for (int s = 0; s < nsteps; ++s)
+    {
+        if (ctx->res.on)
+        {
+            CK(ctx, cudaGraphLaunch(ctx->gexec_a, ctx->stream));
+            ctx->launches += ctx->graph_kernels_a;
+            RUN(launch_resistive(ctx));
+            CK(ctx, cudaGraphLaunch(ctx->gexec_c, ctx->stream));
+            ctx->launches += ctx->graph_kernels_c;
+        }
+        else
+        {
+            CK(ctx, cudaGraphLaunch(ctx->gexec, ctx->stream));
+            ctx->launches += ctx->graph_kernels;
+        }
+    }
     return MHD_OK;
 }
 
@@ -706,6 +1019,110 @@ int mhd_set_sync_wall(mhd_ctx *ctx, const char *group, int32_t block, int32_t di
     return MHD_OK;
 }
 
+int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const double *eta, int64_t nalias,
+                      const int64_t *alias, const int64_t *owner, const double *sign, double rtol, double atol,
+                      int32_t maxit, int32_t restart)
+{
+    if (!ctx || n < 0 || nalias < 0 || (n > 0 && (!unknowns || !eta)) || (nalias > 0 && (!alias || !owner || !sign)))
+        return fail(ctx, MHD_EINVAL, "bad resistive arguments");
+    if (restart <= 0 || restart > kMaxRestart)
+        return fail(ctx, MHD_EINVAL, "GMRES restart must be in [1, %d]", kMaxRestart);
+    auto &R = ctx->res;
+    for (auto **p : {&R.e, &R.dj, &R.j, &R.alias_e, &R.owner_e, &R.alias_dj, &R.owner_dj})
+    {
+        cudaFree(*p);
+        *p = nullptr;
+    }
+    for (auto **p : {&R.eta, &R.sign, &R.V, &R.w, &R.x, &R.b, &R.r, &R.partial, &R.dots})
+    {
+        cudaFree(*p);
+        *p = nullptr;
+    }
+    cudaFree(R.st);
+    R.st = nullptr;
+    // Eres point ids -> offsets in Eres, dJ and J (same locations, same boxes)
+    auto remap = [&](const int64_t *ids, int64_t cnt, int to0, std::vector<uint64_t> &out) -> int {
+        out.resize(size_t(cnt));
+        for (int64_t t = 0; t < cnt; ++t)
+        {
+            const int f = int(ids[t] >> 56);
+            if (f < F_Eresxi || f > F_Eresxi + 2)
+                return fail(ctx, MHD_EINVAL, "resistive unknown %lld is not an Eres point", (long long)t);
+            const int64_t id = (int64_t(to0 + (f - F_Eresxi)) << 56) | (ids[t] & ((int64_t(1) << 56) - 1));
+            const int64_t o = pool_offset(ctx, id);
+            if (o < 0)
+                return fail(ctx, MHD_EINVAL, "resistive point %lld is outside its field", (long long)t);
+            out[size_t(t)] = uint64_t(o);
+        }
+        return MHD_OK;
+    };
+    auto upload_u64 = [&](const std::vector<uint64_t> &v, uint64_t **d) -> int {
+        if (v.empty())
+            return MHD_OK;
+        CK(ctx, cudaMalloc(d, v.size() * 8));
+        CK(ctx, cudaMemcpy(*d, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
+        return MHD_OK;
+    };
+    std::vector<uint64_t> he, hdj, hj, ae, oe, adj, odj;
+    RUN(remap(unknowns, n, F_Eresxi, he));
+    RUN(remap(unknowns, n, F_dJxi, hdj));
+    RUN(remap(unknowns, n, F_Jxi, hj));
+    RUN(remap(alias, nalias, F_Eresxi, ae));
+    RUN(remap(owner, nalias, F_Eresxi, oe));
+    RUN(remap(alias, nalias, F_dJxi, adj));
+    RUN(remap(owner, nalias, F_dJxi, odj));
+    RUN(upload_u64(he, &R.e));
+    RUN(upload_u64(hdj, &R.dj));
+    RUN(upload_u64(hj, &R.j));
+    RUN(upload_u64(ae, &R.alias_e));
+    RUN(upload_u64(oe, &R.owner_e));
+    RUN(upload_u64(adj, &R.alias_dj));
+    RUN(upload_u64(odj, &R.owner_dj));
+    R.n = n;
+    R.nalias = nalias;
+    const size_t nn = size_t(n > 0 ? n : 1);
+    CK(ctx, cudaMalloc(&R.eta, nn * 8));
+    if (n > 0)
+        CK(ctx, cudaMemcpy(R.eta, eta, size_t(n) * 8, cudaMemcpyHostToDevice));
+    if (nalias > 0)
+    {
+        CK(ctx, cudaMalloc(&R.sign, size_t(nalias) * 8));
+        CK(ctx, cudaMemcpy(R.sign, sign, size_t(nalias) * 8, cudaMemcpyHostToDevice));
+    }
+    R.restart = restart;
+    R.rtol = rtol;
+    R.atol = atol;
+    R.maxit = maxit;
+    R.ngroups = int(std::min<int64_t>(std::max<int64_t>((n + 255) / 256, 1), 592));
+    CK(ctx, cudaMalloc(&R.V, nn * size_t(restart + 1) * 8));
+    CK(ctx, cudaMalloc(&R.w, nn * 8));
+    CK(ctx, cudaMalloc(&R.x, nn * 8));
+    CK(ctx, cudaMalloc(&R.b, nn * 8));
+    CK(ctx, cudaMalloc(&R.r, nn * 8));
+    CK(ctx, cudaMalloc(&R.partial, size_t(R.ngroups) * size_t(restart + 2) * 8));
+    CK(ctx, cudaMalloc(&R.dots, 64 * 8));
+    CK(ctx, cudaMalloc(&R.st, sizeof(GmresState)));
+    CK(ctx, cudaMemset(R.x, 0, nn * 8));
+    R.on = true;
+    drop_graph(ctx);
+    return MHD_OK;
+}
+
+int mhd_resistive_stats(const mhd_ctx *ctx, int32_t *its, double *rnorm, double *bnorm, int32_t *reason)
+{
+    if (!ctx)
+        return MHD_EINVAL;
+    if (its)
+        *its = ctx->res.its;
+    if (rnorm)
+        *rnorm = ctx->res.rnorm;
+    if (bnorm)
+        *bnorm = ctx->res.bnorm;
+    if (reason)
+        *reason = ctx->res.reason;
+    return MHD_OK;
+}
+
 int mhd_sync(mhd_ctx *ctx, const char *group)
 {
     if (!ctx || !group)
@@ -728,12 +1145,7 @@ int mhd_step(mhd_ctx *ctx, int32_t nsteps, double *dt_out, double *time_out)
 {
     if (!ctx || nsteps < 0)
         return MHD_EINVAL;
-    RUN(build_graph(ctx));
-    for (int s = 0; s < nsteps; ++s)
-    {
-        CK(ctx, cudaGraphLaunch(ctx->gexec, ctx->stream));
-        ctx->launches += ctx->graph_kernels;
-    }
+    RUN(run_steps(ctx, nsteps));
     RUN(check_err(ctx));
     if (dt_out)
         CK(ctx, cudaMemcpy(dt_out, ctx->dt, 8, cudaMemcpyDeviceToHost));
@@ -780,12 +1192,7 @@ int mhd_step_host(mhd_ctx *ctx, int32_t nsteps, const double *state_in, double *
     RUN(run_sync(ctx, "Ucell"));
     RUN(run_sync(ctx, "Bface"));
     RUN(launch_update_derived(ctx));
-    RUN(build_graph(ctx));
-    for (int s = 0; s < nsteps; ++s)
-    {
-        CK(ctx, cudaGraphLaunch(ctx->gexec, ctx->stream));
-        ctx->launches += ctx->graph_kernels;
-    }
+    RUN(run_steps(ctx, nsteps));
     off = 0;
     for (int b = 0; b < ctx->nblocks; ++b)
         for (int f : {int(F_U), int(F_Bxi), int(F_Beta), int(F_Bzeta)})
@@ -844,7 +1251,7 @@ int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
                 nf = max_box(ctx, l, 0) > nf ? max_box(ctx, l, 0) : nf;
             prof_begin(ctx, "k_curl_e2f");
             k_curl_e2f<<<dim3(grid_for(nf), ctx->nblocks, 3), kThreads, 0, ctx->stream>>>(ctx->dbv, F_Exi, -1, F_Bxi,
-                                                                                         -1.0, ctx->dt, 1.0);
+                                                                                         -1.0, ctx->dt, 1.0, 0);
             RUN(launched(ctx));
         }
         break;

@@ -23,7 +23,7 @@ __global__ void k_fluid_rhs(const BlockView *bvs, Consts c, int64_t maxpts);
 __global__ void k_eface(const BlockView *bvs);
 __global__ void k_eedge(const BlockView *bvs, int G);
 __global__ void k_curl_e2f(const BlockView *bvs, int fE0, int fR0, int fB0, double mult, const double *dtp,
-                           double dtdiv);
+                           double dtdiv, int mult_is_neg_dt);
 __global__ void k_update_u(const BlockView *bvs, const double *dtp);
 __global__ void k_bcell(const BlockView *bvs);
 __global__ void k_jedge(const BlockView *bvs, int fB0, int fJ0, double mult);
@@ -41,5 +41,36 @@ __global__ void k_aos_to_soa(const BlockView *bvs, int blk, int fid, int ncomp, 
                              int n1, int n2, const double *aos);
 __global__ void k_soa_to_aos(const BlockView *bvs, int blk, int fid, int ncomp, int lo0, int lo1, int lo2, int n0,
                              int n1, int n2, double *aos);
+
+// Krylov (mhd_krylov.cu).  GMRES scalar state kept on the device; restart
+// length at most kMaxRestart.
+constexpr int kMaxRestart = 30;
+struct GmresState
+{
+    double H[31 * 31]; // H[i * 31 + j]: row i, column j (upper Hessenberg, rotated in place)
+    double cs[31], sn[31], g[32];
+    double hcol[32]; // h of the current column, then ||w|| at hcol[j + 1]
+    double resid;    // |g[j + 1]|
+    double beta;     // initial residual norm of the cycle
+    double y[31];
+    int breakdown;
+};
+__global__ void k_dots_partial(const double *V, int64_t ldv, int nvec, const double *w, int64_t n, double *partial,
+                               int with_norm);
+__global__ void k_dots_final(const double *partial, int ngroups, int nout, double *out, int accumulate);
+__global__ void k_sub_proj(const double *V, int64_t ldv, int nvec, const double *h, double *w, int64_t n);
+__global__ void k_div_dev(double *y, const double *x, const double *a, int64_t n);
+__global__ void k_add_small(double *a, const double *b, int n);
+__global__ void k_gmres_column(GmresState *st, int j, const double *wnorm2);
+__global__ void k_gmres_start(GmresState *st, const double *beta2);
+__global__ void k_gmres_solve_y(GmresState *st, int m);
+__global__ void k_add_basis(const double *V, int64_t ldv, const GmresState *st, int m, double *x, int64_t n);
+__global__ void k_residual(const double *b, const double *y, double *r, int64_t n);
+__global__ void k_scatter_vec(double *pool, const uint64_t *dst, const double *x, int64_t n);
+__global__ void k_resist_out(const double *pool, const uint64_t *e, const uint64_t *dj, const double *eta, double *y,
+                             int64_t n);
+__global__ void k_resist_rhs(const double *pool, const uint64_t *j, const double *eta, double *b, int64_t n);
+__global__ void k_alias_copy(double *pool, const uint64_t *alias, const uint64_t *owner, const double *sign,
+                             int64_t n);
 
 } // namespace mhd

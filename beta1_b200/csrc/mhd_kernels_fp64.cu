@@ -345,8 +345,10 @@ __global__ void k_eedge(const BlockView *__restrict__ bvs, int G)
 // blockIdx.z = face axis.
 // ---------------------------------------------------------------------------
 __global__ void k_curl_e2f(const BlockView *__restrict__ bvs, int fE0, int fR0, int fB0, double mult,
-                           const double *__restrict__ dtp, double dtdiv)
+                           const double *__restrict__ dtp, double dtdiv, int mult_is_neg_dt)
 {
+    if (mult_is_neg_dt)
+        mult = -dtp[0];
     const BlockView &b = bvs[blockIdx.y];
     const int fa = blockIdx.z;
     int lo[3], n[3];

@@ -1,0 +1,203 @@
+// Matrix-free restarted GMRES on the device, replacing the PETSc KSPSolve of
+// the implicit resistive step (Z4_Lunar/src/implicit/Lunar_ImplicitResistive.cpp:430-491).
+//
+// Vectors are dense over the solve's unknowns (owner edges with eta > 0).
+// Orthogonalisation is classical Gram-Schmidt applied twice (CGS2): every
+// pass needs only one batched dot-product kernel, instead of one reduction
+// per basis vector with modified Gram-Schmidt.  All reductions are
+// two-stage (per-CTA partial sums, then a fixed-order final sum), so a solve
+// is bit-reproducible from run to run.  The Hessenberg matrix, the Givens
+// rotations and the residual estimate live in device memory and are updated
+// by a one-thread kernel; the host reads back one scalar per iteration to
+// decide whether to stop.
+#include "mhd_kernels.cuh"
+
+namespace mhd
+{
+
+constexpr int kRedThreads = 256;
+
+// partial[c * ngroups + blockIdx.x] = sum over this CTA's slice of V_c . w
+// for c in [0, nvec); the last "vector" slot nvec computes w . w when
+// with_norm is set.
+__global__ void k_dots_partial(const double *__restrict__ V, int64_t ldv, int nvec, const double *__restrict__ w,
+                               int64_t n, double *__restrict__ partial, int with_norm)
+{
+    const int c = blockIdx.y;
+    const double *v = (c < nvec) ? V + int64_t(c) * ldv : w;
+    double s = 0.0;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x)
+        s += v[t] * w[t];
+    __shared__ double red[kRedThreads];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = blockDim.x / 2; off > 0; off >>= 1)
+    {
+        if (threadIdx.x < off)
+            red[threadIdx.x] += red[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        partial[int64_t(c) * gridDim.x + blockIdx.x] = red[0];
+    (void)with_norm;
+}
+
+// out[c] = sum_b partial[c * ngroups + b] (fixed order), optionally added to acc
+__global__ void k_dots_final(const double *__restrict__ partial, int ngroups, int nout, double *__restrict__ out,
+                             int accumulate)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nout)
+        return;
+    double s = 0.0;
+    for (int b = 0; b < ngroups; ++b)
+        s += partial[int64_t(c) * ngroups + b];
+    out[c] = accumulate ? out[c] + s : s;
+}
+
+// w -= sum_c h[c] V_c
+__global__ void k_sub_proj(const double *__restrict__ V, int64_t ldv, int nvec, const double *__restrict__ h,
+                           double *__restrict__ w, int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n)
+        return;
+    double s = w[t];
+    for (int c = 0; c < nvec; ++c)
+        s -= h[c] * V[int64_t(c) * ldv + t];
+    w[t] = s;
+}
+
+// a[c] += b[c] for c < n (small vectors)
+__global__ void k_add_small(double *__restrict__ a, const double *__restrict__ b, int n)
+{
+    const int c = threadIdx.x;
+    if (c < n)
+        a[c] += b[c];
+}
+
+// y = x / a   (a from device memory)
+__global__ void k_div_dev(double *__restrict__ y, const double *__restrict__ x, const double *__restrict__ a,
+                          int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        y[t] = x[t] / a[0];
+}
+
+
+// new column j: hcol[j + 1] = ||w||, H[0..j+1, j] = hcol; apply the
+// previous rotations, form a new one, update g and the residual estimate
+__global__ void k_gmres_column(GmresState *st, int j, const double *__restrict__ wnorm2)
+{
+    st->hcol[j + 1] = sqrt(wnorm2[0]);
+    double *H = st->H;
+    for (int i = 0; i <= j + 1; ++i)
+        H[i * 31 + j] = st->hcol[i];
+    for (int i = 0; i < j; ++i)
+    {
+        const double a = H[i * 31 + j], b = H[(i + 1) * 31 + j];
+        H[i * 31 + j] = st->cs[i] * a + st->sn[i] * b;
+        H[(i + 1) * 31 + j] = -st->sn[i] * a + st->cs[i] * b;
+    }
+    const double a = H[j * 31 + j], b = H[(j + 1) * 31 + j];
+    const double den = sqrt(a * a + b * b);
+    st->cs[j] = den > 0.0 ? a / den : 1.0;
+    st->sn[j] = den > 0.0 ? b / den : 0.0;
+    H[j * 31 + j] = den;
+    H[(j + 1) * 31 + j] = 0.0;
+    st->g[j + 1] = -st->sn[j] * st->g[j];
+    st->g[j] = st->cs[j] * st->g[j];
+    st->resid = fabs(st->g[j + 1]);
+    st->breakdown = (st->hcol[j + 1] == 0.0) ? 1 : 0;
+}
+
+// start of a cycle: beta = ||r||, g = beta e1
+__global__ void k_gmres_start(GmresState *st, const double *__restrict__ beta2)
+{
+    const double beta = sqrt(beta2[0]);
+    st->beta = beta;
+    for (int i = 0; i < 32; ++i)
+        st->g[i] = 0.0;
+    st->g[0] = beta;
+    st->resid = beta;
+    st->breakdown = 0;
+}
+
+// back substitution H y = g over the first m columns
+__global__ void k_gmres_solve_y(GmresState *st, int m)
+{
+    for (int i = m - 1; i >= 0; --i)
+    {
+        double s = st->g[i];
+        for (int q = i + 1; q < m; ++q)
+            s -= st->H[i * 31 + q] * st->y[q];
+        st->y[i] = s / st->H[i * 31 + i];
+    }
+}
+
+// x += V y over m columns
+__global__ void k_add_basis(const double *__restrict__ V, int64_t ldv, const GmresState *st, int m,
+                            double *__restrict__ x, int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n)
+        return;
+    double s = x[t];
+    for (int c = 0; c < m; ++c)
+        s += st->y[c] * V[int64_t(c) * ldv + t];
+    x[t] = s;
+}
+
+// r = b - y
+__global__ void k_residual(const double *__restrict__ b, const double *__restrict__ y, double *__restrict__ r,
+                           int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        r[t] = b[t] - y[t];
+}
+
+// ---------------------------------------------------------------------------
+// Resistive operator pieces (LunarSolver::MatMultImplicitResistive_ and its
+// helpers, Z4_Lunar/src/implicit/Lunar_ImplicitResistive.cpp:264-427)
+// ---------------------------------------------------------------------------
+
+// pool[dst[t]] = x[t]   (UnpackVecToImplicitEres_ after clear_triplet)
+__global__ void k_scatter_vec(double *__restrict__ pool, const uint64_t *__restrict__ dst,
+                              const double *__restrict__ x, int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        pool[dst[t]] = x[t];
+}
+
+// y[t] = pool[e[t]] - eta[t] * pool[dj[t]]   (end of MatMultImplicitResistive_)
+__global__ void k_resist_out(const double *__restrict__ pool, const uint64_t *__restrict__ e,
+                             const uint64_t *__restrict__ dj, const double *__restrict__ eta, double *__restrict__ y,
+                             int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        y[t] = pool[e[t]] - eta[t] * pool[dj[t]];
+}
+
+// b[t] = 0.0 + eta[t] * pool[j[t]]   (PackImplicitJedgeToVec_ with multiply_eta)
+__global__ void k_resist_rhs(const double *__restrict__ pool, const uint64_t *__restrict__ j,
+                             const double *__restrict__ eta, double *__restrict__ b, int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        b[t] = 0.0 + eta[t] * pool[j[t]];
+}
+
+// alias <- sign * owner (HALO_OWNER::sync_edge_1form)
+__global__ void k_alias_copy(double *__restrict__ pool, const uint64_t *__restrict__ alias,
+                             const uint64_t *__restrict__ owner, const double *__restrict__ sign, int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        pool[alias[t]] = sign[t] * pool[owner[t]];
+}
+
+} // namespace mhd

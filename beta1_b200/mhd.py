@@ -52,6 +52,10 @@ _SIGS = {
     "mhd_sync": (C.c_int, [C.c_void_p, C.c_char_p]),
     "mhd_set_sync_consts": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64]),
     "mhd_set_sync_wall": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_int32]),
+    "mhd_set_resistive": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int32, C.c_int32]),
+    "mhd_resistive_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                                      C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "mhd_update_derived": (C.c_int, [C.c_void_p]),
     "mhd_step": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "mhd_step_host": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_double)]),
@@ -206,6 +210,22 @@ class Context:
 
     def set_sync_wall(self, group: str, block: int, direction: int):
         self._check(self.lib.mhd_set_sync_wall(self.h, group.encode(), block, direction), f"set_sync_wall {group}")
+
+    def set_resistive(self, unknowns, eta, alias, owner, sign, rtol, atol, maxit, restart=30):
+        u = np.ascontiguousarray(unknowns, dtype=np.int64)
+        e = np.ascontiguousarray(eta, dtype=np.float64)
+        a = np.ascontiguousarray(alias, dtype=np.int64)
+        o = np.ascontiguousarray(owner, dtype=np.int64)
+        sg = np.ascontiguousarray(sign, dtype=np.float64)
+        self._check(self.lib.mhd_set_resistive(self.h, u.size, u.ctypes.data, e.ctypes.data, a.size, a.ctypes.data,
+                                               o.ctypes.data, sg.ctypes.data, rtol, atol, maxit, restart),
+                    "set_resistive")
+
+    def resistive_stats(self):
+        its, rn, bn, rs = C.c_int32(), C.c_double(), C.c_double(), C.c_int32()
+        self._check(self.lib.mhd_resistive_stats(self.h, C.byref(its), C.byref(rn), C.byref(bn), C.byref(rs)),
+                    "resistive_stats")
+        return dict(its=its.value, rnorm=rn.value, bnorm=bn.value, reason=rs.value)
 
     def sync(self, group: str):
         self._check(self.lib.mhd_sync(self.h, group.encode()), f"sync {group}")

@@ -8,7 +8,7 @@ from typing import Optional
 import numpy as np
 
 from . import case as case_mod
-from . import geometry, mhd, physics, rst, syncmap
+from . import edges, geometry, mhd, physics, rst, syncmap
 
 GEOM_FIELDS = ["Jac", "JDxi", "JDet", "JDze", "beta_xi", "beta_eta", "beta_zeta", "alpha_xi", "alpha_eta",
                "alpha_zeta", "dr_xi", "dr_eta", "dr_zeta", "Bcell_from_Bface_w", "Jcell_from_Jedge_w"]
@@ -56,6 +56,35 @@ class Solver:
         else:
             raise ValueError(f"unknown topology {topology}")
         self.ctx.sync("Badd")
+        p = spec.params
+        if p.get("is_Lunar_resistance", 0):
+            if not p.get("use_implicit_lunar_resistance", 0):
+                raise NotImplementedError("explicit resistive sub-cycles are not supported by this build")
+            self.install_resistive(topology)
+
+    def install_resistive(self, topology):
+        """Unknowns, resistivity and edge aliases of the implicit resistive
+        solve (LunarSolver::SetupImplicitResistiveDiffusion_)."""
+        spec = self.spec
+        n = spec.blocks[0].ncell
+        tiles = spec.tiles if topology == "tiled" else (1, 1)
+        alias, owner, owners = edges.tiled_owners(n, tiles)
+        c = physics.constants(spec.params)
+        dofs, eta = edges.resistive_dofs(owners, self.nodes, c["inver_Rem"])
+        names = {1: "Eres_xi", 2: "Eres_eta", 3: "Eres_zeta"}
+
+        def ids(rows):
+            out = np.empty(len(rows), dtype=np.int64)
+            for q, (b, d, i, j, k) in enumerate(rows.tolist()):
+                info = self.ctx.field_info(names[d], b)
+                out[q] = self.ctx.point_base(names[d], b) + syncmap.aos_index(info["lo"], info["hi"], 1, i, j, k, 0)
+            return out
+
+        p = spec.params
+        self.ctx.set_resistive(ids(dofs), eta, ids(alias), ids(owner), np.ones(len(alias)),
+                               float(p["implicit_resistive_ksp_rtol"]), float(p["implicit_resistive_ksp_atol"]),
+                               int(p["implicit_resistive_ksp_max_it"]), 30)
+        self.resistive_dofs = (dofs, eta)
 
     def install_tiled(self):
         spec = self.spec

@@ -126,6 +126,23 @@ int mhd_set_sync_map(mhd_ctx *ctx, const char *group, const int64_t *dst, const 
 int mhd_set_sync_consts(mhd_ctx *ctx, const char *group, const int64_t *dst, const double *val, int64_t n);
 int mhd_set_sync_wall(mhd_ctx *ctx, const char *group, int32_t block, int32_t direction);
 
+/* Implicit resistive step (LunarSolver::SolveImplicitResistiveDiffusion_,
+   Z4_Lunar/src/implicit/Lunar_ImplicitResistive.cpp:430-518, with the
+   PETSc KSPSolve/MatShell of :95-124 replaced by a device GMRES): unknowns
+   are Eres_xi/Eres_eta/Eres_zeta point ids of the owner edges with eta > 0
+   in solve order (BuildImplicitResistiveEdgeDofMap_, :147-164), `eta` their
+   resistivity; alias/owner/sign is the edge 1-form sync table
+   (HALO_OWNER::sync_edge_1form).  Convergence: ||r|| <= max(rtol ||b||, atol)
+   from x = 0, at most maxit iterations, restart <= 30.  Enables the solve in
+   every following StepOnce. */
+int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const double *eta, int64_t nalias,
+                      const int64_t *alias, const int64_t *owner, const double *sign, double rtol, double atol,
+                      int32_t maxit, int32_t restart);
+
+/* Iterations, final residual norm, ||b|| and convergence reason (2 rtol,
+   3 atol, -3 iteration limit, as KSPConvergedReason) of the last solve. */
+int mhd_resistive_stats(const mhd_ctx *ctx, int32_t *its, double *rnorm, double *bnorm, int32_t *reason);
+
 /* LunarBoundary::Sync(group) on the device. */
 int mhd_sync(mhd_ctx *ctx, const char *group);
 

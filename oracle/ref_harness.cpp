@@ -437,6 +437,24 @@ int cmd_topo(Harness &h, const std::string &out)
     return 0;
 }
 
+// Edge equivalence: alias -> owner copies (with sign) and, when the solver
+// built its implicit resistive system, its DOF list in solve order with eta.
+int cmd_owners(Harness &h, const std::string &out)
+{
+    std::ofstream o(out);
+    o << std::setprecision(17);
+    for (const auto &it : h.edge_owner_pattern.local_alias)
+        o << "alias " << it.rep.gblock << " " << it.rep.dir << " " << it.rep.i << " " << it.rep.j << " " << it.rep.k
+          << " owner " << it.owner.gblock << " " << it.owner.dir << " " << it.owner.i << " " << it.owner.j << " "
+          << it.owner.k << " sign " << int(it.sign) << "\n";
+    LunarSolver &s = *h.solver;
+    for (const auto &d : s.implicit_resistive_dofs_)
+        o << "dof " << d.edge.gblock << " " << d.edge.dir << " " << d.edge.i << " " << d.edge.j << " " << d.edge.k
+          << " eta " << d.eta << "\n";
+    o << "n_owner " << h.topo_equiv.n_local_edge_owner << "\n";
+    return 0;
+}
+
 int cmd_time(Harness &h, const std::string &state, int nsteps)
 {
     h.load_state(state);
@@ -494,6 +512,8 @@ int main(int argc, char **argv)
         const std::string cmd = argv[1];
         if (cmd == "topo")
             rc = cmd_topo(h, argv[2]);
+        else if (cmd == "owners")
+            rc = cmd_owners(h, argv[2]);
         else if (cmd == "geom")
             rc = cmd_geom(h, argv[2]);
         else if (cmd == "run" && argc >= 5)

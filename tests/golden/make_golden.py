@@ -86,10 +86,11 @@ def periodic(n=(8, 6, 5), steps=2, seed=20261203):
     print("wrote", tag)
 
 
-def slab(nr=6, nt=(5, 6), tiles=(2, 2), steps=2, resistive=0, implicit=0, seed=20261204):
+def slab(nr=6, nt=(5, 6), tiles=(2, 2), steps=2, resistive=0, implicit=0, seed=20261204, **over):
     tag = "slab_%dx%dx%d_t%dx%d_r%d%d" % ((nr,) + tuple(nt) + tuple(tiles) + (resistive, implicit))
     with tempfile.TemporaryDirectory() as d:
-        spec = case.slab_case(nr, nt, tiles, is_Lunar_resistance=resistive, use_implicit_lunar_resistance=implicit)
+        spec = case.slab_case(nr, nt, tiles, is_Lunar_resistance=resistive, use_implicit_lunar_resistance=implicit,
+                              **over)
         case.write_case(d, spec)
         st = case.inflow_state(spec, seed=seed)
         rst.write(os.path.join(d, "init.rst"), st)
@@ -108,6 +109,8 @@ def slab(nr=6, nt=(5, 6), tiles=(2, 2), steps=2, resistive=0, implicit=0, seed=2
         arr["nt"] = np.array(nt)
         arr["tiles"] = np.array(tiles)
         arr["resistive"] = np.array([resistive, implicit])
+        for k, v in over.items():
+            arr["param/" + k] = np.array(v)
         arr["seed"] = np.array(seed)
         np.savez_compressed(os.path.join(OUT, tag + "_steps.npz"), **arr)
     print("wrote", tag)
@@ -118,3 +121,7 @@ if __name__ == "__main__":
         sys.exit("build the oracle first: make -C oracle -j8")
     periodic((8, 6, 5), steps=2)
     slab(steps=2)
+    # implicit resistive shell with peak resistivity 1 (inver_Rem = 1), solved to rtol 1e-13
+    slab(steps=2, resistive=1, implicit=1, eta_max_lunar=1.0 * case.MU0 * case.ref_scales()["U"]
+         * case.ref_scales()["L_ref"], implicit_resistive_ksp_rtol=1e-13, implicit_resistive_ksp_atol=1e-30,
+         implicit_resistive_ksp_max_it=300)

@@ -3,7 +3,15 @@ tiling the transverse directions periodically, a Solid_Surface at x = 1 and
 a Farfield at x = 8, against the reference solver's own outputs
 (tests/golden/make_golden.py, slab()).  Exercises the compiled syncs with
 their physical-handler phase (wall kernel, far-field constants) and the
-inter-block halos.  FP64 tolerance 1e-12 relative L2 per field per step."""
+inter-block halos; the second case adds the implicit resistive step (device
+GMRES in place of the reference's Krylov solve).
+
+Tolerances (relative L2 per field per step): 1e-12 for the ideal case (the
+FP64 kernels follow the reference's operation order); 1e-10 with the
+implicit resistive solve, where both sides stop GMRES at ||r|| <= 1e-13 ||b||
+but orthogonalise in different orders (CGS2 here, modified Gram-Schmidt in
+the reference's solver), so the converged unknowns agree to about the
+solver tolerance times the operator's condition number."""
 import numpy as np
 import pytest
 
@@ -14,7 +22,7 @@ from beta1_b200 import case, rst, solver
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-12
-FIELDS = ["U_H", "B_xi", "B_eta", "B_zeta", "PV_H", "U_plus", "B_cell", "Bind_cell", "J_xi", "J_eta", "J_zeta",
+FIELDS = ["Eres_xi", "Eres_eta", "Eres_zeta", "U_H", "B_xi", "B_eta", "B_zeta", "PV_H", "U_plus", "B_cell", "Bind_cell", "J_xi", "J_eta", "J_zeta",
           "J_cell", "E_xi", "E_eta", "E_zeta", "Eface_xi", "Eface_eta", "Eface_zeta", "RHS_H", "RHS_B_xi",
           "RHS_B_eta", "RHS_B_zeta"]
 LOCS = {"U_H": rst.CELL, "B_xi": rst.FACE_XI, "B_eta": rst.FACE_ET, "B_zeta": rst.FACE_ZE}
@@ -25,7 +33,8 @@ def slab_setup(g):
     nt = tuple(int(v) for v in g["nt"])
     tiles = tuple(int(v) for v in g["tiles"])
     res = [int(v) for v in g["resistive"]]
-    spec = case.slab_case(nr, nt, tiles, is_Lunar_resistance=res[0], use_implicit_lunar_resistance=res[1])
+    over = {k.split("/", 1)[1]: g[k].item() for k in g.files if k.startswith("param/")}
+    spec = case.slab_case(nr, nt, tiles, is_Lunar_resistance=res[0], use_implicit_lunar_resistance=res[1], **over)
     st = rst.RestartFile(0, 0.0, len(spec.blocks), {})
     for name, loc in LOCS.items():
         rec = rst.FieldRecord(name, loc, 5 if name == "U_H" else 1, 4)
@@ -37,9 +46,14 @@ def slab_setup(g):
     return spec, st
 
 
-@pytest.fixture(scope="module")
-def slab_run():
-    g = load_golden("slab_6x5x6_t2x2_r00_steps.npz")
+CASES = {"ideal": ("slab_6x5x6_t2x2_r00_steps.npz", 1e-12),
+         "implicit_resistive": ("slab_6x5x6_t2x2_r11_steps.npz", 1e-10)}
+
+
+@pytest.fixture(scope="module", params=list(CASES))
+def slab_run(request):
+    fname, tol = CASES[request.param]
+    g = load_golden(fname)
     spec, st = slab_setup(g)
     s = solver.Solver(spec, topology="tiled")
     s.load_state(st)
@@ -50,16 +64,19 @@ def slab_run():
     for n in range(1, nsteps + 1):
         dts[n], _ = s.step(1)
         out[n] = {(f, b): s.field(f, b) for f in FIELDS for b in range(nb)}
+    stats = s.ctx.resistive_stats() if "Eres" in "".join(g.files) and int(g["resistive"][0]) else None
     s.ctx.close()
-    return g, out, dts, nsteps, nb
+    return g, out, dts, nsteps, nb, tol, stats
 
 
 def test_slab_fields_match_reference(slab_run):
-    g, out, dts, nsteps, nb = slab_run
+    g, out, dts, nsteps, nb, TOL, stats = slab_run
     worst = 0.0
     for n in range(nsteps + 1):
         for f in FIELDS:
             if n == 0 and f.startswith(("E", "RHS")):
+                continue
+            if f.startswith("Eres") and not int(g["resistive"][0]):
                 continue
             for b in range(nb):
                 ref = g["s%d/b%d/%s" % (n, b, f)]
@@ -67,10 +84,12 @@ def test_slab_fields_match_reference(slab_run):
                 e = rel_l2(got, ref)
                 worst = max(worst, e)
                 assert e <= TOL, f"step {n} block {b} field {f}: rel L2 {e:.3e}"
-    print("slab: max rel L2 %.3e" % worst)
+    print("slab: max rel L2 %.3e (tolerance %.0e) solver %s" % (worst, TOL, stats))
 
 
 def test_slab_dt_matches_reference(slab_run):
-    g, out, dts, nsteps, nb = slab_run
+    g, out, dts, nsteps, nb, TOL, stats = slab_run
     for n in range(1, nsteps + 1):
-        assert dts[n] == float(g["s%d/dt" % n])
+        # dt of step n depends on the state after step n-1: exact without the
+        # Krylov solve, to the solve tolerance with it
+        assert abs(dts[n] - float(g["s%d/dt" % n])) <= TOL * abs(float(g["s%d/dt" % n]))
