@@ -1,0 +1,645 @@
+"""CPU restatement of the reference's per-step MHD algorithm (numpy).
+
+TEST INFRASTRUCTURE ONLY: this module is the checker the GPU path is
+compared against in tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline; nothing in beta1_b200/ imports it.
+
+It restates LunarSolver::StepOnce (Z4_Lunar/src/LunarSolver_Driver.cpp:21-92)
+stage by stage with whole-array numpy operations in the reference's floating
+point operation order, so on the reference's own inputs it reproduces the
+reference's outputs (pinned against the fixtures in tests/golden, which the
+reference solver itself produced).  Boundary synchronisations apply the same
+composed tables the device receives (their own equality with the reference's
+Sync is pinned separately against the reference's probe fixtures).
+
+Data layout: per block, a field is a float64 array (ncomp, NI, NJ, NK) over
+the padded logical box [-G, n + 1 + G) in each direction.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+# name: (location code of the restart file, components, ghost layers), as the
+# reference registers them (Z4_Lunar/main.cpp:61-123, src/3_field/4_MPCNS_Geometry.cpp:4-69)
+FIELDS = {
+    "U_H": (0, 5, 4), "B_xi": (1, 1, 4), "B_eta": (2, 1, 4), "B_zeta": (3, 1, 4), "PV_H": (0, 5, 4),
+    "U_plus": (0, 3, 4), "B_cell": (0, 3, 4), "Bind_cell": (0, 3, 4), "J_xi": (4, 1, 4), "J_eta": (5, 1, 4),
+    "J_zeta": (6, 1, 4), "J_cell": (0, 3, 4), "Eface_xi": (1, 3, 4), "Eface_eta": (2, 3, 4),
+    "Eface_zeta": (3, 3, 4), "E_xi": (4, 1, 4), "E_eta": (5, 1, 4), "E_zeta": (6, 1, 4), "RHS_H": (0, 5, 0),
+    "RHS_B_xi": (1, 1, 0), "RHS_B_eta": (2, 1, 0), "RHS_B_zeta": (3, 1, 0), "Badd_xi": (1, 1, 4),
+    "Badd_eta": (2, 1, 4), "Badd_zeta": (3, 1, 4), "Jac": (0, 1, 3), "JDxi": (1, 3, 4), "JDet": (2, 3, 4),
+    "JDze": (3, 3, 4), "beta_xi": (1, 1, 3), "beta_eta": (2, 1, 3), "beta_zeta": (3, 1, 3), "alpha_xi": (4, 1, 3),
+    "alpha_eta": (5, 1, 3), "alpha_zeta": (6, 1, 3), "Bcell_from_Bface_w": (0, 18, 3),
+    "Jcell_from_Jedge_w": (0, 36, 3), "Eres_xi": (4, 1, 4), "Eres_eta": (5, 1, 4), "Eres_zeta": (6, 1, 4),
+    "dB_xi": (1, 1, 4), "dB_eta": (2, 1, 4), "dB_zeta": (3, 1, 4), "dJ_xi": (4, 1, 4), "dJ_eta": (5, 1, 4),
+    "dJ_zeta": (6, 1, 4), "RHS_Bres_xi": (1, 1, 0), "RHS_Bres_eta": (2, 1, 0), "RHS_Bres_zeta": (3, 1, 0),
+}
+PLUS = {0: (0, 0, 0), 1: (1, 0, 0), 2: (0, 1, 0), 3: (0, 0, 1), 4: (0, 1, 1), 5: (1, 0, 1), 6: (1, 1, 0)}
+
+
+class Block:
+    def __init__(self, n, G=4):
+        self.n = tuple(n)
+        self.G = G
+        self.f = {}
+        for name, (loc, nc, _) in FIELDS.items():
+            self.f[name] = np.zeros((nc, n[0] + 1 + 2 * G, n[1] + 1 + 2 * G, n[2] + 1 + 2 * G))
+
+    def s(self, lo, hi):
+        """slices of the logical box [lo, hi)"""
+        G = self.G
+        return tuple(slice(l + G, h + G) for l, h in zip(lo, hi))
+
+    def sh(self, lo, hi, d):
+        """box shifted by d"""
+        return self.s(tuple(l + x for l, x in zip(lo, d)), tuple(h + x for h, x in zip(hi, d)))
+
+    def box(self, name, m, lo, hi, d=(0, 0, 0)):
+        return self.f[name][m][self.sh(lo, hi, d)]
+
+    def inner(self, loc):
+        p = PLUS[loc]
+        return (0, 0, 0), (self.n[0] + p[0], self.n[1] + p[1], self.n[2] + p[2])
+
+    def set_ref(self, name, lo, data):
+        """store a reference-layout array (ni, nj, nk, ncomp) whose logical origin is lo"""
+        sl = tuple(slice(l + self.G, l + self.G + s) for l, s in zip(lo, data.shape[:3]))
+        for m in range(data.shape[3]):
+            self.f[name][m][sl] = data[..., m]
+
+    def get_ref(self, name):
+        """the field's logical box [lo, hi) in reference layout (ni, nj, nk, ncomp)"""
+        loc, nc, ng = FIELDS[name]
+        p = PLUS[loc]
+        lo = (-ng, -ng, -ng)
+        hi = (self.n[0] + p[0] + ng, self.n[1] + p[1] + ng, self.n[2] + p[2] + ng)
+        return np.stack([self.box(name, m, lo, hi) for m in range(nc)], axis=-1)
+
+
+def smax(a, b):
+    """std::max(a, b) elementwise (first argument unless the second is larger)."""
+    return np.where(a < b, b, a)
+
+
+class Oracle:
+    def __init__(self, ncells, consts, G=4):
+        self.blocks = [Block(n, G) for n in ncells]
+        self.c = consts
+        self.dt = 0.0
+        self.time = 0.0
+        self.syncs = {}  # group -> dict(gather=(dst, src) as (field, block, m, i, j, k) arrays, consts, walls)
+
+    # ------------------------------------------------------------------ syncs
+    def aos_points(self, name, b, offsets):
+        """(m, I, J, K) of AoS offsets within field `name`'s logical box on block b
+        (FieldBlock storage order, include/3_field/Field_Array.h:177)."""
+        blk = self.blocks[b]
+        loc, nc, ng = FIELDS[name]
+        p = PLUS[loc]
+        ext = [blk.n[a] + p[a] + 2 * ng for a in range(3)]
+        o = np.asarray(offsets, dtype=np.int64)
+        m = o % nc
+        t = o // nc
+        K = t % ext[2] - ng
+        t = t // ext[2]
+        J = t % ext[1] - ng
+        I = t // ext[1] - ng
+        return m, I, J, K
+
+    def add_copies(self, group, dst_name, dst_block, dst_off, src_name, src_block, src_off):
+        """Composed copies of a Sync group: point dst[n] takes the value src[n] had before the sync."""
+        g = self.syncs.setdefault(group, dict(copies=[], consts=[], walls=[]))
+        g["copies"].append(((dst_name, dst_block) + self.aos_points(dst_name, dst_block, dst_off),
+                            (src_name, src_block) + self.aos_points(src_name, src_block, src_off)))
+
+    def add_consts(self, group, name, block, off, val):
+        g = self.syncs.setdefault(group, dict(copies=[], consts=[], walls=[]))
+        g["consts"].append(((name, block) + self.aos_points(name, block, off), np.asarray(val, dtype=np.float64)))
+
+    def add_wall(self, group, block, direction):
+        g = self.syncs.setdefault(group, dict(copies=[], consts=[], walls=[]))
+        g["walls"].append((block, direction))
+
+    def add_point_tables(self, group, names, dst, src, cdst=(), cval=(), walls=()):
+        """A group's tables in point-id form ((field index << 56) | (block << 40) | AoS offset,
+        `names` maps field indices to names)."""
+        dst, src = np.asarray(dst, dtype=np.int64), np.asarray(src, dtype=np.int64)
+        mask = (1 << 40) - 1
+        key = np.stack([dst >> 56, (dst >> 40) & 0xFFFF, src >> 56, (src >> 40) & 0xFFFF], axis=1)
+        if len(key):
+            uk, inv = np.unique(key, axis=0, return_inverse=True)
+            for q, (fd, bd, fs, bs) in enumerate(uk.tolist()):
+                sel = inv.ravel() == q
+                self.add_copies(group, names[fd], bd, dst[sel] & mask, names[fs], bs, src[sel] & mask)
+        cdst = np.asarray(cdst, dtype=np.int64)
+        cval = np.asarray(cval, dtype=np.float64)
+        if len(cdst):
+            ck = np.stack([cdst >> 56, (cdst >> 40) & 0xFFFF], axis=1)
+            uk, inv = np.unique(ck, axis=0, return_inverse=True)
+            for q, (f, b) in enumerate(uk.tolist()):
+                sel = inv.ravel() == q
+                self.add_consts(group, names[f], b, cdst[sel] & mask, cval[sel])
+        for (b, d) in walls:
+            self.add_wall(group, b, d)
+        self.syncs.setdefault(group, dict(copies=[], consts=[], walls=[]))
+
+    def _view(self, pt):
+        name, b, m, I, J, K = pt
+        blk = self.blocks[b]
+        return blk.f[name], (m, I + blk.G, J + blk.G, K + blk.G)
+
+    def sync(self, group):
+        """LunarBoundary::Sync(group) (Z4_Lunar/src/boundary/Boundary.cpp:30-40): fixed values and wall
+        handlers first, then every copy reads the values from before the sync."""
+        s = self.syncs.get(group)
+        if s is None:
+            return
+        for pt, val in s["consts"]:
+            arr, idx = self._view(pt)
+            arr[idx] = val
+        for (b, d) in s["walls"]:
+            self.wall_u(b, d)
+        vals = []
+        for _, src in s["copies"]:
+            arr, idx = self._view(src)
+            vals.append(arr[idx].copy())
+        for (dst, _), v in zip(s["copies"], vals):
+            arr, idx = self._view(dst)
+            arr[idx] = v
+
+    def wall_u(self, b, d):
+        """LunarBoundary::BC_Solid_Surface_ on the i-minimum face
+        (Z4_Lunar/src/boundary/Boundary_Condition_Fluid.cpp:19-185)."""
+        assert d == -1
+        blk = self.blocks[b]
+        g = self.c["gamma"]
+        U = blk.f["U_H"]
+        G = blk.G
+        n = blk.n
+        J, K = slice(G, G + n[1]), slice(G, G + n[2])
+
+        def pressure(rho, mx, my, mz, E):
+            rho = smax(rho, 2.5e-3)
+            ke = 0.5 * (mx * mx + my * my + mz * mz) / rho
+            eint = E - ke
+            eint = np.where(eint < 0.0, 0.0, eint)
+            return smax((g - 1.0) * eint, 1e-12)
+
+        r = [U[m][G + 1, J, K] for m in range(5)]
+        rho_r = smax(r[0], 2.5e-3)
+        p_r = pressure(rho_r, r[1], r[2], r[3], r[4])
+        zero = 0.0
+        ke_g = 0.5 * rho_r * (zero * zero + zero * zero + zero * zero)
+        U[0][G, J, K] = rho_r
+        U[1][G, J, K] = rho_r * zero
+        U[2][G, J, K] = rho_r * zero
+        U[3][G, J, K] = rho_r * zero
+        U[4][G, J, K] = p_r / (g - 1.0) + ke_g
+        rho_r = smax(U[0][G, J, K], 2.5e-3)
+        p_r = pressure(rho_r, U[1][G, J, K], U[2][G, J, K], U[3][G, J, K], U[4][G, J, K])
+        ke_g = 0.5 * rho_r * (zero * zero + zero * zero + zero * zero)
+        for ng in range(1, G + 1):
+            U[0][G - ng, J, K] = rho_r
+            U[1][G - ng, J, K] = rho_r * zero
+            U[2][G - ng, J, K] = rho_r * zero
+            U[3][G - ng, J, K] = rho_r * zero
+            U[4][G - ng, J, K] = p_r / (g - 1.0) + ke_g
+
+    # ------------------------------------------------------- derived fields
+    def calc_bcell(self, blk):
+        """calc_Bcell (Z4_Lunar/src/physics/LunarSolver_Tools.cpp:163-240)"""
+        lo, hi = blk.inner(0)
+        bx = lambda d=(0, 0, 0): blk.box("B_xi", 0, lo, hi, d)
+        be = lambda d=(0, 0, 0): blk.box("B_eta", 0, lo, hi, d)
+        bz = lambda d=(0, 0, 0): blk.box("B_zeta", 0, lo, hi, d)
+        ax = lambda d=(0, 0, 0): blk.box("Badd_xi", 0, lo, hi, d)
+        ae = lambda d=(0, 0, 0): blk.box("Badd_eta", 0, lo, hi, d)
+        az = lambda d=(0, 0, 0): blk.box("Badd_zeta", 0, lo, hi, d)
+        tot = [-bx() - ax(), bx((1, 0, 0)) + ax((1, 0, 0)), -be() - ae(), be((0, 1, 0)) + ae((0, 1, 0)),
+               -bz() - az(), bz((0, 0, 1)) + az((0, 0, 1))]
+        ind = [-bx(), bx((1, 0, 0)), -be(), be((0, 1, 0)), -bz(), bz((0, 0, 1))]
+        W = lambda q: blk.box("Bcell_from_Bface_w", q, lo, hi)
+        acc_t = [0.0, 0.0, 0.0]
+        acc_i = [0.0, 0.0, 0.0]
+        for q in range(6):
+            for c in range(3):
+                w = W(6 * c + q)
+                acc_t[c] = acc_t[c] + w * tot[q]
+                acc_i[c] = acc_i[c] + w * ind[q]
+        for c in range(3):
+            blk.f["B_cell"][c][blk.s(lo, hi)] = acc_t[c]
+            blk.f["Bind_cell"][c][blk.s(lo, hi)] = acc_i[c]
+
+    def curl_adj(self, blk, fB, fJ, mult=1.0):
+        """CTOperators::CurlAdjFaceToEdge times alpha
+        (Z4_Lunar/src/operators/CTOperators.cpp:58-110, LunarSolver_Tools.cpp:777-835)"""
+        Fx, Fe, Fz = fB
+        for ea, nm in enumerate(fJ):
+            lo, hi = blk.inner(4 + ea)
+            bx = lambda d: blk.box("beta_xi", 0, lo, hi, d) * blk.box(Fx, 0, lo, hi, d)
+            be = lambda d: blk.box("beta_eta", 0, lo, hi, d) * blk.box(Fe, 0, lo, hi, d)
+            bz = lambda d: blk.box("beta_zeta", 0, lo, hi, d) * blk.box(Fz, 0, lo, hi, d)
+            z = (0, 0, 0)
+            if ea == 0:
+                val = (be((0, 0, -1)) - be(z)) + (bz(z) - bz((0, -1, 0)))
+            elif ea == 1:
+                val = (bx(z) - bx((0, 0, -1))) + (bz((-1, 0, 0)) - bz(z))
+            else:
+                val = (bx((0, -1, 0)) - bx(z)) + (be(z) - be((-1, 0, 0)))
+            alpha = blk.box(("alpha_xi", "alpha_eta", "alpha_zeta")[ea], 0, lo, hi)
+            blk.f[nm][0][blk.s(lo, hi)] = (mult * val) * alpha
+
+    def calc_jcell(self, blk):
+        """calc_Jcell (LunarSolver_Tools.cpp:837-892)"""
+        lo, hi = blk.inner(0)
+        jx = lambda d: blk.box("J_xi", 0, lo, hi, d)
+        je = lambda d: blk.box("J_eta", 0, lo, hi, d)
+        jz = lambda d: blk.box("J_zeta", 0, lo, hi, d)
+        s = [jx((0, 0, 0)), jx((0, 1, 0)), jx((0, 0, 1)), jx((0, 1, 1)), je((0, 0, 0)), je((1, 0, 0)),
+             je((0, 0, 1)), je((1, 0, 1)), jz((0, 0, 0)), jz((1, 0, 0)), jz((0, 1, 0)), jz((1, 1, 0))]
+        acc = [0.0, 0.0, 0.0]
+        for q in range(12):
+            for c in range(3):
+                acc[c] = acc[c] + blk.box("Jcell_from_Jedge_w", 12 * c + q, lo, hi) * s[q]
+        for c in range(3):
+            blk.f["J_cell"][c][blk.s(lo, hi)] = acc[c]
+
+    def calc_pv_uplus(self, blk):
+        """calc_PV + calc_Uplus over the whole array (LunarSolver_Tools.cpp:58-141)"""
+        g = self.c["gamma"]
+        U = blk.f["U_H"]
+        rho = smax(U[0], 1e-12)
+        u = U[1] / rho
+        v = U[2] / rho
+        w = U[3] / rho
+        ke = 0.5 * rho * (u * u + v * v + w * w)
+        eint = U[4] - ke
+        eint = np.where(eint < 0.0, 0.0, eint)
+        p = smax((g - 1.0) * eint, 1e-12)
+        T = p / (rho * self.c["state_coeff"])
+        PV = blk.f["PV_H"]
+        PV[0], PV[1], PV[2], PV[3], PV[4] = u, v, w, p, T
+        has = U[0] > 1e-20
+        Up = blk.f["U_plus"]
+        Up[0] = np.where(has, u, 0.0)
+        Up[1] = np.where(has, v, 0.0)
+        Up[2] = np.where(has, w, 0.0)
+
+    def update_derived(self):
+        """UpdateDerivedFields_ (LunarSolver_Tools.cpp:143-161)"""
+        for blk in self.blocks:
+            self.calc_bcell(blk)
+        self.sync("B_cell")
+        for blk in self.blocks:
+            self.curl_adj(blk, ("B_xi", "B_eta", "B_zeta"), ("J_xi", "J_eta", "J_zeta"))
+        self.sync("Jedge")
+        for blk in self.blocks:
+            self.calc_jcell(blk)
+        self.sync("J_cell")
+        for blk in self.blocks:
+            self.calc_pv_uplus(blk)
+        self.sync("Uplus")
+
+    # ---------------------------------------------------------------- time step
+    def compute_timestep(self):
+        """Compute_Timestep (Z4_Lunar/src/physics/LunarSolver_Timestep.cpp:8-140)"""
+        g = self.c["gamma"]
+        best = 1e100
+        for blk in self.blocks:
+            lo, hi = blk.inner(0)
+            V = np.abs(blk.box("Jac", 0, lo, hi))
+            U = [blk.box("U_H", m, lo, hi) for m in range(5)]
+            rho = smax(U[0], 1e-2)
+            ux, uy, uz = U[1] / rho, U[2] / rho, U[3] / rho
+            ke = 0.5 * rho * (ux * ux + uy * uy + uz * uz)
+            p = (g - 1.0) * (U[4] - ke)
+            cs2 = g * p / rho
+            Bx, By, Bz = (blk.box("B_cell", c, lo, hi) for c in range(3))
+            B2 = Bx * Bx + By * By + Bz * Bz
+            denom = np.zeros(V.shape)
+            for nm, d in (("JDxi", (1, 0, 0)), ("JDet", (0, 1, 0)), ("JDze", (0, 0, 1))):
+                for shift, outward in (((0, 0, 0), False), (d, True)):
+                    ax, ay, az = (blk.box(nm, c, lo, hi, shift) for c in range(3))
+                    A = np.sqrt(ax * ax + ay * ay + az * az)
+                    with np.errstate(invalid="ignore", divide="ignore"):
+                        nx, ny, nz = ax / A, ay / A, az / A
+                    if not outward:
+                        nx, ny, nz = -nx, -ny, -nz
+                    un = ux * nx + uy * ny + uz * nz
+                    Bn = Bx * nx + By * ny + Bz * nz
+                    vA2 = self.c["inver_MA2"] * B2 / rho
+                    vAn2 = self.c["inver_MA2"] * (Bn * Bn) / rho
+                    term = cs2 + vA2
+                    disc = term * term - 4.0 * cs2 * vAn2
+                    disc = np.where(disc < 0.0, 0.0, disc)
+                    cf = np.sqrt(0.5 * (term + np.sqrt(disc)))
+                    denom = denom + np.where(A <= 0.0, 0.0, (np.abs(un) + cf) * A)
+            ok = (V > 0.0) & (denom > 0.0)
+            with np.errstate(invalid="ignore", divide="ignore"):
+                dtc = np.where(ok, self.c["cfl"] * V / denom, 1e100)
+            best = min(best, float(np.min(dtc)))
+        self.dt = best
+        return best
+
+    # --------------------------------------------------------------- fluid RHS
+    def _face_flux(self, blk, d, lo, hi, shift):
+        """Reconstruction_Rusanov on the faces [lo, hi) + shift of direction d
+        (Z4_Lunar/src/physics/LunarSolver_FluidRHS.cpp:34-111)"""
+        g = self.c["gamma"]
+        nm = ("JDxi", "JDet", "JDze")[d]
+        e = tuple(-1 if q == d else 0 for q in range(3))
+        sL = tuple(a + b for a, b in zip(shift, e))
+        k1, k2, k3 = (blk.box(nm, c, lo, hi, shift) for c in range(3))
+        rhoL = blk.box("U_H", 0, lo, hi, sL)
+        rhoR = blk.box("U_H", 0, lo, hi, shift)
+        uL, vL, wL, pL = (blk.box("PV_H", c, lo, hi, sL) for c in range(4))
+        uR, vR, wR, pR = (blk.box("PV_H", c, lo, hi, shift) for c in range(4))
+        UL = [rhoL, rhoL * uL, rhoL * vL, rhoL * wL, pL / (g - 1.0) + 0.5 * rhoL * (uL * uL + vL * vL + wL * wL)]
+        UR = [rhoR, rhoR * uR, rhoR * vR, rhoR * wR, pR / (g - 1.0) + 0.5 * rhoR * (uR * uR + vR * vR + wR * wR)]
+        kk = (k1 * k1 + k2 * k2 + k3 * k3)
+
+        def rad(rho, u, v, w, p):
+            uvw = k1 * u + k2 * v + k3 * w
+            c = np.sqrt(smax(0.0, g * p / smax(rho, 1e-30)))
+            return np.abs(uvw) + c * np.sqrt(kk)
+
+        def flux(rho, u, v, w, p):
+            uvw = k1 * u + k2 * v + k3 * w
+            rhoe = p / (g - 1.0) + 0.5 * rho * (u * u + v * v + w * w)
+            return [rho * uvw, rho * uvw * u + k1 * p, rho * uvw * v + k2 * p, rho * uvw * w + k3 * p,
+                    uvw * (rhoe + p)]
+
+        r = smax(rad(rhoL, uL, vL, wL, pL), rad(rhoR, uR, vR, wR, pR))
+        FL = flux(rhoL, uL, vL, wL, pL)
+        FR = flux(rhoR, uR, vR, wR, pR)
+        return [0.5 * (FL[m] + FR[m]) - 0.5 * r * (UR[m] - UL[m]) for m in range(5)]
+
+    def fluid_rhs(self):
+        """ZeroRHS_ + Scheme_U_ + AddSourceToRHS_Fluid
+        (LunarSolver_Advance.cpp:4-59, LunarSolver_FluidRHS.cpp:3-201, :528-568)"""
+        c = self.c
+        for blk in self.blocks:
+            lo, hi = blk.inner(0)
+            invJ = 1.0 / blk.box("Jac", 0, lo, hi)
+            dF = []
+            for d in range(3):
+                e = tuple(1 if q == d else 0 for q in range(3))
+                Fm = self._face_flux(blk, d, lo, hi, (0, 0, 0))
+                Fp = self._face_flux(blk, d, lo, hi, e)
+                dF.append([Fp[m] - Fm[m] for m in range(5)])
+            R = []
+            for m in range(5):
+                r = 0.0 - dF[0][m] * invJ
+                r = r - dF[1][m] * invJ
+                r = r - dF[2][m] * invJ
+                R.append(r)
+            rho = blk.box("U_H", 0, lo, hi)
+            n_true = smax(rho, 0.0) / c["M_H"] * c["M_ref"]
+            ne = np.sqrt(n_true * n_true + c["ne_hall_floor"] * c["ne_hall_floor"])
+            fc = c["momentum_hall_coeff"] * (n_true / ne)
+            Jx, Jy, Jz = (blk.box("J_cell", q, lo, hi) for q in range(3))
+            Bx, By, Bz = (blk.box("B_cell", q, lo, hi) for q in range(3))
+            jxb = [Jy * Bz - Jz * By, Jz * Bx - Jx * Bz, Jx * By - Jy * Bx]
+            PV = [blk.box("PV_H", q, lo, hi) for q in range(3)]
+            R[1] = R[1] + fc * jxb[0]
+            R[2] = R[2] + fc * jxb[1]
+            R[3] = R[3] + fc * jxb[2]
+            R[4] = R[4] + fc * (jxb[0] * PV[0] + jxb[1] * PV[1] + jxb[2] * PV[2])
+            for m in range(5):
+                blk.f["RHS_H"][m][blk.s(lo, hi)] = R[m]
+
+    # ------------------------------------------------------------- induction
+    def _ucon(self, blk, axis, lo, hi, d):
+        """cell_u_contra (LunarSolver_MagExplicit_Ideal.cpp:95-115) on cells [lo,hi)+d"""
+        nm = ("JDxi", "JDet", "JDze")[axis]
+        e = tuple(x + (1 if q == axis else 0) for q, x in enumerate(d))
+        kx = 0.5 * (blk.box(nm, 0, lo, hi, d) + blk.box(nm, 0, lo, hi, e))
+        ky = 0.5 * (blk.box(nm, 1, lo, hi, d) + blk.box(nm, 1, lo, hi, e))
+        kz = 0.5 * (blk.box(nm, 2, lo, hi, d) + blk.box(nm, 2, lo, hi, e))
+        inv = 1.0 / (np.abs(blk.box("Jac", 0, lo, hi, d)) + 1.0e-30)
+        return (kx * blk.box("U_plus", 0, lo, hi, d) + ky * blk.box("U_plus", 1, lo, hi, d)
+                + kz * blk.box("U_plus", 2, lo, hi, d)) * inv
+
+    def eface(self, blk):
+        """AssembleOneDirectionEMF_ for the three directions (LunarSolver_MagExplicit_Ideal.cpp:348-496)"""
+        Bn = ("B_xi", "B_eta", "B_zeta")
+        An = ("Badd_xi", "Badd_eta", "Badd_zeta")
+        for fa in range(3):
+            lo, hi = blk.inner(1 + fa)
+            L = tuple(-1 if q == fa else 0 for q in range(3))
+            z = (0, 0, 0)
+            tot = lambda ax, d: blk.box(Bn[ax], 0, lo, hi, d) + blk.box(An[ax], 0, lo, hi, d)
+            ind = lambda ax, d: blk.box(Bn[ax], 0, lo, hi, d)
+            bff = tot(fa, z)
+
+            def G(ba):
+                e = tuple(1 if q == ba else 0 for q in range(3))
+                Le = tuple(a + b for a, b in zip(L, e))
+                btL = 0.5 * (tot(ba, L) + tot(ba, Le))
+                btR = 0.5 * (tot(ba, z) + tot(ba, e))
+                biL = 0.5 * (ind(ba, L) + ind(ba, Le))
+                biR = 0.5 * (ind(ba, z) + ind(ba, e))
+                ufL = self._ucon(blk, fa, lo, hi, L)
+                ufR = self._ucon(blk, fa, lo, hi, z)
+                ubL = self._ucon(blk, ba, lo, hi, L)
+                ubR = self._ucon(blk, ba, lo, hi, z)
+                GL = ufL * btL - ubL * bff
+                GR = ufR * btR - ubR * bff
+                radius = smax(np.abs(ufL), np.abs(ufR))
+                return 0.5 * (GL + GR) - 0.5 * radius * (biR - biL)
+
+            zero = np.zeros(bff.shape)
+            if fa == 0:
+                e = [zero, G(2), -G(1)]
+            elif fa == 1:
+                e = [-G(2), zero, G(0)]
+            else:
+                e = [G(1), -G(0), zero]
+            nm = ("Eface_xi", "Eface_eta", "Eface_zeta")[fa]
+            for c in range(3):
+                blk.f[nm][c][blk.s(lo, hi)] = e[c]
+
+    def eedge(self, blk):
+        """AssembleEdgeEMF_FromFaceE_Ideal_ after zeroing E_edge
+        (LunarSolver_MagExplicit_Ideal.cpp:53-287, LunarSolver_MagneticRHS.cpp:9-28)"""
+        for nm in ("E_xi", "E_eta", "E_zeta"):
+            blk.f[nm][:] = 0.0
+        C = 0.5
+        z = (0, 0, 0)
+
+        def a4(axis, lo, hi, cells):
+            a = 0.0
+            for d in cells:
+                a = smax(a, np.abs(self._ucon(blk, axis, lo, hi, d)))
+            return a
+
+        B = lambda nm, lo, hi, d: blk.box(nm, 0, lo, hi, d)
+        lo, hi = blk.inner(4)
+        Ec = 0.25 * (blk.box("Eface_eta", 0, lo, hi, z) + blk.box("Eface_eta", 0, lo, hi, (0, 0, -1))
+                     + blk.box("Eface_zeta", 0, lo, hi, z) + blk.box("Eface_zeta", 0, lo, hi, (0, -1, 0)))
+        cells = [z, (0, -1, 0), (0, 0, -1), (0, -1, -1)]
+        ae, az = a4(1, lo, hi, cells), a4(2, lo, hi, cells)
+        dz = B("B_zeta", lo, hi, z) - B("B_zeta", lo, hi, (0, -1, 0))
+        de = B("B_eta", lo, hi, z) - B("B_eta", lo, hi, (0, 0, -1))
+        blk.f["E_xi"][0][blk.s(lo, hi)] = Ec + C * (0.5 * ae * dz - 0.5 * az * de)
+        lo, hi = blk.inner(5)
+        Ec = 0.25 * (blk.box("Eface_xi", 1, lo, hi, z) + blk.box("Eface_xi", 1, lo, hi, (0, 0, -1))
+                     + blk.box("Eface_zeta", 1, lo, hi, z) + blk.box("Eface_zeta", 1, lo, hi, (-1, 0, 0)))
+        cells = [z, (-1, 0, 0), (0, 0, -1), (-1, 0, -1)]
+        az, ax = a4(2, lo, hi, cells), a4(0, lo, hi, cells)
+        dx = B("B_xi", lo, hi, z) - B("B_xi", lo, hi, (0, 0, -1))
+        dz = B("B_zeta", lo, hi, z) - B("B_zeta", lo, hi, (-1, 0, 0))
+        blk.f["E_eta"][0][blk.s(lo, hi)] = Ec + C * (0.5 * az * dx - 0.5 * ax * dz)
+        lo, hi = blk.inner(6)
+        Ec = 0.25 * (blk.box("Eface_xi", 2, lo, hi, z) + blk.box("Eface_xi", 2, lo, hi, (0, -1, 0))
+                     + blk.box("Eface_eta", 2, lo, hi, z) + blk.box("Eface_eta", 2, lo, hi, (-1, 0, 0)))
+        cells = [z, (-1, 0, 0), (0, -1, 0), (-1, -1, 0)]
+        ax, ae = a4(0, lo, hi, cells), a4(1, lo, hi, cells)
+        de = B("B_eta", lo, hi, z) - B("B_eta", lo, hi, (-1, 0, 0))
+        dx = B("B_xi", lo, hi, z) - B("B_xi", lo, hi, (0, -1, 0))
+        blk.f["E_zeta"][0][blk.s(lo, hi)] = Ec + C * (0.5 * ax * de - 0.5 * ae * dx)
+
+    def curl_e2f(self, blk, fE, fF, mult):
+        """CTOperators::CurlEdgeToFace (Z4_Lunar/src/operators/CTOperators.cpp:6-56)"""
+        Ex, Ee, Ez = fE
+        z = (0, 0, 0)
+        for fa, nm in enumerate(fF):
+            lo, hi = blk.inner(1 + fa)
+            e = lambda f_, d: blk.box(f_, 0, lo, hi, d)
+            if fa == 0:
+                c = (e(Ee, z) - e(Ee, (0, 0, 1))) + (e(Ez, (0, 1, 0)) - e(Ez, z))
+            elif fa == 1:
+                c = (e(Ex, (0, 0, 1)) - e(Ex, z)) + (e(Ez, z) - e(Ez, (1, 0, 0)))
+            else:
+                c = (e(Ex, z) - e(Ex, (0, 1, 0))) + (e(Ee, (1, 0, 0)) - e(Ee, z))
+            blk.f[nm][0][blk.s(lo, hi)] = mult * c
+
+    def step(self):
+        """One LunarSolver::StepOnce (Z4_Lunar/src/LunarSolver_Driver.cpp:21-92): CFL time step,
+        fluid RHS, CT induction, forward-Euler update, the implicit resistive
+        solve when it is set up, then the closing syncs and derived fields."""
+        self.compute_timestep()
+        dt = self.dt
+        self.fluid_rhs()
+        for blk in self.blocks:
+            self.eface(blk)
+        self.sync("Eface")
+        for blk in self.blocks:
+            self.eedge(blk)
+        self.sync("Eedge")
+        for blk in self.blocks:
+            self.curl_e2f(blk, ("E_xi", "E_eta", "E_zeta"), ("RHS_B_xi", "RHS_B_eta", "RHS_B_zeta"), -1.0)
+        for blk in self.blocks:
+            lo, hi = blk.inner(0)
+            for m in range(5):
+                blk.f["U_H"][m][blk.s(lo, hi)] += dt * blk.box("RHS_H", m, lo, hi)
+            for fa, (bn, rn) in enumerate((("B_xi", "RHS_B_xi"), ("B_eta", "RHS_B_eta"), ("B_zeta", "RHS_B_zeta"))):
+                lo, hi = blk.inner(1 + fa)
+                blk.f[bn][0][blk.s(lo, hi)] += dt * blk.box(rn, 0, lo, hi)
+        if self.resist is not None:
+            self.resistive_step()
+        self.time += dt
+        self.sync("Ucell")
+        self.sync("Bface")
+        self.update_derived()
+        return dt
+
+    # ------------------------------------------------------ implicit resistivity
+    def set_resistive(self, unknowns, eta, alias, owner, sign):
+        """Unknown edges (block, dir, i, j, k) with dir 1/2/3 = xi/eta/zeta in solve order and their
+        resistivity (BuildImplicitResistiveEdgeDofMap_, Z4_Lunar/src/implicit/Lunar_ImplicitResistive.cpp:147-164),
+        and the edge alias -> owner table with orientation signs (HALO_OWNER::sync_edge_1form)."""
+        self.resist = dict(u=np.asarray(unknowns), eta=np.asarray(eta, dtype=np.float64), alias=np.asarray(alias),
+                           owner=np.asarray(owner), sign=np.asarray(sign, dtype=np.float64))
+
+    resist = None
+    EDGE3 = {1: "_xi", 2: "_eta", 3: "_zeta"}
+
+    def _edge_get(self, prefix, rows):
+        out = np.empty(len(rows))
+        for d in (1, 2, 3):
+            sel = rows[:, 1] == d
+            for b in np.unique(rows[sel, 0]):
+                s2 = sel & (rows[:, 0] == b)
+                blk = self.blocks[int(b)]
+                G = blk.G
+                out[s2] = blk.f[prefix + self.EDGE3[d]][0][rows[s2, 2] + G, rows[s2, 3] + G, rows[s2, 4] + G]
+        return out
+
+    def _edge_set(self, prefix, rows, vals):
+        for d in (1, 2, 3):
+            sel = rows[:, 1] == d
+            for b in np.unique(rows[sel, 0]):
+                s2 = sel & (rows[:, 0] == b)
+                blk = self.blocks[int(b)]
+                G = blk.G
+                blk.f[prefix + self.EDGE3[d]][0][rows[s2, 2] + G, rows[s2, 3] + G, rows[s2, 4] + G] = vals[s2]
+
+    def _alias(self, prefix):
+        R = self.resist
+        if len(R["alias"]):
+            self._edge_set(prefix, R["alias"], R["sign"] * self._edge_get(prefix, R["owner"]))
+
+    def _clear(self, prefix):
+        for blk in self.blocks:
+            for sfx in ("_xi", "_eta", "_zeta"):
+                blk.f[prefix + sfx][:] = 0.0
+
+    def _unpack(self, x):
+        """UnpackVecToImplicitEres_ (Lunar_ImplicitResistive.cpp:332-360)"""
+        self._clear("Eres")
+        self._edge_set("Eres", self.resist["u"], x)
+        self._alias("Eres")
+        self.sync("Eres1form")
+
+    def resistive_matvec(self, x):
+        """MatMultImplicitResistive_ (Lunar_ImplicitResistive.cpp:380-427):
+        y = x - eta * alpha curlAdj(beta (-dt) curl(x))."""
+        self._unpack(x)
+        self._clear("dB")
+        for blk in self.blocks:
+            self.curl_e2f(blk, ("Eres_xi", "Eres_eta", "Eres_zeta"), ("dB_xi", "dB_eta", "dB_zeta"), -self.dt)
+        self.sync("dB")
+        self._clear("dJ")
+        for blk in self.blocks:
+            self.curl_adj(blk, ("dB_xi", "dB_eta", "dB_zeta"), ("dJ_xi", "dJ_eta", "dJ_zeta"))
+        self._alias("dJ")
+        R = self.resist
+        return self._edge_get("Eres", R["u"]) - R["eta"] * self._edge_get("dJ", R["u"])
+
+    def resistive_step(self):
+        """SolveImplicitResistiveDiffusion_ + ApplyImplicitResistiveUpdate_
+        (Lunar_ImplicitResistive.cpp:430-518).  The linear system is solved
+        directly (dense LU over the operator's columns) instead of by GMRES:
+        the result is the exact solution the Krylov solve approaches to its
+        tolerance, so it checks a GMRES solution to that tolerance."""
+        R = self.resist
+        self.sync("Bface")
+        self.sync("Bface")
+        for blk in self.blocks:
+            self.curl_adj(blk, ("B_xi", "B_eta", "B_zeta"), ("J_xi", "J_eta", "J_zeta"))
+        self.sync("Jedge")
+        n = len(R["u"])
+        if n:
+            b = 0.0 + R["eta"] * self._edge_get("J", R["u"])
+            A = np.empty((n, n))
+            e = np.zeros(n)
+            for q in range(n):
+                e[q] = 1.0
+                A[:, q] = self.resistive_matvec(e)
+                e[q] = 0.0
+            x = np.linalg.solve(A, b)
+            self.resist_last = dict(b=b, x=x, A=A)
+        else:
+            x = np.zeros(0)
+        self._unpack(x)
+        self.sync("Eres1form")
+        self._clear("RHS_Bres")
+        for blk in self.blocks:
+            self.curl_e2f(blk, ("Eres_xi", "Eres_eta", "Eres_zeta"), ("RHS_Bres_xi", "RHS_Bres_eta", "RHS_Bres_zeta"),
+                          -1.0)
+            for fa, (bn, rn) in enumerate((("B_xi", "RHS_Bres_xi"), ("B_eta", "RHS_Bres_eta"),
+                                           ("B_zeta", "RHS_Bres_zeta"))):
+                lo, hi = blk.inner(1 + fa)
+                blk.f[bn][0][blk.s(lo, hi)] += self.dt * blk.box(rn, 0, lo, hi)
+        self.sync("Bface")

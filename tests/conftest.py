@@ -32,3 +32,24 @@ def golden_periodic():
         "geom": load_golden("periodic_8x6x5_geom.npz"),
         "probe": load_golden("periodic_8x6x5_probe.npz"),
     }
+
+
+def slab_setup(g):
+    """(case spec, restart state) of a committed slab fixture."""
+    from beta1_b200 import case, rst
+    LOCS = {"U_H": rst.CELL, "B_xi": rst.FACE_XI, "B_eta": rst.FACE_ET, "B_zeta": rst.FACE_ZE}
+    nr = int(g["nr"])
+    nt = tuple(int(v) for v in g["nt"])
+    tiles = tuple(int(v) for v in g["tiles"])
+    res = [int(v) for v in g["resistive"]]
+    over = {k.split("/", 1)[1]: g[k].item() for k in g.files if k.startswith("param/")}
+    spec = case.slab_case(nr, nt, tiles, is_Lunar_resistance=res[0], use_implicit_lunar_resistance=res[1], **over)
+    st = rst.RestartFile(0, 0.0, len(spec.blocks), {})
+    for name, loc in LOCS.items():
+        rec = rst.FieldRecord(name, loc, 5 if name == "U_H" else 1, 4)
+        for b in range(len(spec.blocks)):
+            a = g["init/b%d/%s" % (b, name)]
+            lo = tuple(int(v) for v in g["init/b%d/%s__lo" % (b, name)])
+            rec.blocks.append(rst.FieldArray(lo, tuple(l + s for l, s in zip(lo, a.shape[:3])), a))
+        st.fields[name] = rec
+    return spec, st

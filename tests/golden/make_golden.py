@@ -116,6 +116,59 @@ def slab(nr=6, nt=(5, 6), tiles=(2, 2), steps=2, resistive=0, implicit=0, seed=2
     print("wrote", tag)
 
 
+def slab_probe(nr=6, nt=(5, 6), tiles=(2, 2), resistive=0, seed=20261204):
+    """Every Sync group of a tiled slab probed on the reference: for each
+    (group, field, block) the offsets whose value the Sync changed and the
+    value it left there (an encoded source point, a boundary constant, or a
+    wall-handler value)."""
+    from beta1_b200 import syncmap
+    tag = "slab_%dx%dx%d_t%dx%d_r%d%d" % ((nr,) + tuple(nt) + tuple(tiles) + (resistive, resistive))
+    with tempfile.TemporaryDirectory() as d:
+        spec = case.slab_case(nr, nt, tiles, is_Lunar_resistance=resistive, use_implicit_lunar_resistance=resistive)
+        case.write_case(d, spec)
+        rst.write(os.path.join(d, "init.rst"), case.inflow_state(spec, seed=seed))
+        arr = {}
+        for grp in syncmap.GROUPS:
+            run(["probe", "init.rst", grp, "p.bin"], d)
+            p = rst.read(os.path.join(d, "p.bin"))
+            for fname, rec in p.fields.items():
+                for b, fa in enumerate(rec.blocks):
+                    v = fa.data.reshape(-1)
+                    own = np.arange(v.size, dtype=np.float64) + b * 2.0 ** 32 + 1.0
+                    changed = np.nonzero(v != own)[0]
+                    arr["%s/%s/%d/dst" % (grp, fname, b)] = changed.astype(np.int32)
+                    arr["%s/%s/%d/val" % (grp, fname, b)] = v[changed]
+        np.savez_compressed(os.path.join(OUT, tag + "_probe.npz"), **arr)
+    print("wrote", tag + "_probe")
+
+
+def slab_owners(nr=6, nt=(5, 6), tiles=(2, 2), seed=20261204, **over):
+    """Edge alias/owner table and the implicit resistive unknowns (with eta)
+    of a tiled slab, as the reference builds them."""
+    tag = "slab_%dx%dx%d_t%dx%d_r11" % ((nr,) + tuple(nt) + tuple(tiles))
+    with tempfile.TemporaryDirectory() as d:
+        spec = case.slab_case(nr, nt, tiles, is_Lunar_resistance=1, use_implicit_lunar_resistance=1, **over)
+        case.write_case(d, spec)
+        rst.write(os.path.join(d, "init.rst"), case.inflow_state(spec, seed=seed))
+        run(["owners", "owners.txt"], d)
+        alias, dof, eta, n_owner = [], [], [], None
+        for line in open(os.path.join(d, "owners.txt")):
+            t = line.split()
+            if t[0] == "alias":
+                alias.append([int(x) for x in t[1:6]] + [int(x) for x in t[7:12]] + [int(t[13])])
+            elif t[0] == "dof":
+                dof.append([int(x) for x in t[1:6]])
+                eta.append(float(t[7]))
+            elif t[0] == "n_owner":
+                n_owner = int(t[1])
+        arr = dict(alias=np.array(alias, dtype=np.int32), dof=np.array(dof, dtype=np.int32),
+                   eta=np.array(eta), n_owner=np.array(n_owner))
+        for k, v in over.items():
+            arr["param/" + k] = np.array(v)
+        np.savez_compressed(os.path.join(OUT, tag + "_owners.npz"), **arr)
+    print("wrote", tag + "_owners")
+
+
 if __name__ == "__main__":
     if not os.path.exists(REF_BIN):
         sys.exit("build the oracle first: make -C oracle -j8")
@@ -125,3 +178,6 @@ if __name__ == "__main__":
     slab(steps=2, resistive=1, implicit=1, eta_max_lunar=1.0 * case.MU0 * case.ref_scales()["U"]
          * case.ref_scales()["L_ref"], implicit_resistive_ksp_rtol=1e-13, implicit_resistive_ksp_atol=1e-30,
          implicit_resistive_ksp_max_it=300)
+    slab_probe(resistive=0)
+    slab_probe(resistive=1)
+    slab_owners(eta_max_lunar=1.0 * case.MU0 * case.ref_scales()["U"] * case.ref_scales()["L_ref"])

@@ -15,9 +15,9 @@ solver tolerance times the operator's condition number."""
 import numpy as np
 import pytest
 
-from conftest import load_golden, rel_l2
+from conftest import load_golden, rel_l2, slab_setup
 
-from beta1_b200 import case, rst, solver
+from beta1_b200 import solver
 
 pytestmark = pytest.mark.gpu
 
@@ -25,27 +25,6 @@ TOL = 1e-12
 FIELDS = ["Eres_xi", "Eres_eta", "Eres_zeta", "U_H", "B_xi", "B_eta", "B_zeta", "PV_H", "U_plus", "B_cell", "Bind_cell", "J_xi", "J_eta", "J_zeta",
           "J_cell", "E_xi", "E_eta", "E_zeta", "Eface_xi", "Eface_eta", "Eface_zeta", "RHS_H", "RHS_B_xi",
           "RHS_B_eta", "RHS_B_zeta"]
-LOCS = {"U_H": rst.CELL, "B_xi": rst.FACE_XI, "B_eta": rst.FACE_ET, "B_zeta": rst.FACE_ZE}
-
-
-def slab_setup(g):
-    nr = int(g["nr"])
-    nt = tuple(int(v) for v in g["nt"])
-    tiles = tuple(int(v) for v in g["tiles"])
-    res = [int(v) for v in g["resistive"]]
-    over = {k.split("/", 1)[1]: g[k].item() for k in g.files if k.startswith("param/")}
-    spec = case.slab_case(nr, nt, tiles, is_Lunar_resistance=res[0], use_implicit_lunar_resistance=res[1], **over)
-    st = rst.RestartFile(0, 0.0, len(spec.blocks), {})
-    for name, loc in LOCS.items():
-        rec = rst.FieldRecord(name, loc, 5 if name == "U_H" else 1, 4)
-        for b in range(len(spec.blocks)):
-            a = g["init/b%d/%s" % (b, name)]
-            lo = tuple(int(v) for v in g["init/b%d/%s__lo" % (b, name)])
-            rec.blocks.append(rst.FieldArray(lo, tuple(l + s for l, s in zip(lo, a.shape[:3])), a))
-        st.fields[name] = rec
-    return spec, st
-
-
 CASES = {"ideal": ("slab_6x5x6_t2x2_r00_steps.npz", 1e-12),
          "implicit_resistive": ("slab_6x5x6_t2x2_r11_steps.npz", 1e-10)}
 
