@@ -1,18 +1,25 @@
 """Benchmark of the per-timestep MHD hot path (one StepOnce = one step).
 
-Default workload: the plain FP64 64^3 periodic curvilinear block of the
-reference's CPU-runnable configuration (ideal MHD, Rusanov + CT, CFL 0.4,
-seeded 1e-3 noise), stepped on the GPU through the C ABI.
+Workloads (--workload):
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+* c2 (default): 6 blocks of 96 x 48 x 48 cells (1,327,104 cells), radial
+  cells log-spaced over r in [1, 8], a Solid_Surface inner wall and a
+  Farfield outer boundary, inflow rho = 1, v = (-8, 0, 0),
+  B = (0, 0.5, 0.5)/sqrt(2), p = 0.05 with seeded 1e-3 noise, and the
+  implicit resistive step (peak resistivity 1e-3, GMRES to rtol 1e-10)
+  every step; the six blocks tile a curved slab (3 x 2 transverse tiles,
+  periodic across the tiles) because the reference's halo exchange cannot
+  run a cubed-sphere layout.  FP64.
+* c1: the plain FP64 64^3 periodic curvilinear block (ideal MHD).
 
-Multi-GPU (torchrun): the path does not shard (north star: no multi-GPU
-path), so N ranks run N independent replicas; value = all cells updated by
-all ranks / max-over-ranks time.
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload c2|c1]
+
+Multi-GPU (torchrun): the path does not shard, so N ranks run N independent
+replicas; value = all cells updated by all ranks / max-over-ranks time.
 
 Rank 0 prints one JSON line.  Inputs are seeded synthetic states in the
-reference's restart format; the device working set (~0.36 GB at 64^3) is
-larger than the 126 MB L2, so no L2 flush is inserted between steps.
+reference's restart format; the device working set (several GB) is larger
+than the 126 MB L2, so no L2 flush is inserted between steps.
 """
 from __future__ import annotations
 
@@ -105,22 +112,46 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def build_case(n):
+WORKLOADS = {
+    "c2": dict(name="c2_slab6x96x48x48_implicit_resistive_fp64", ref_steps=4, ref_rss_gb=12.0),
+    "c1": dict(name="c1_periodic_64cubed_fp64", ref_steps=40, ref_rss_gb=1.0),
+}
+
+
+def build_case(workload, n=64):
+    """(spec, restart state, topology, interior cells) of a workload."""
     from beta1_b200 import case
-    spec = case.periodic_box_case((n, n, n))
-    st = case.initial_state(spec)
-    return spec, st
+    if workload == "c1":
+        spec = case.periodic_box_case((n, n, n))
+        return spec, case.initial_state(spec), "periodic", n ** 3
+    sc = case.ref_scales()
+    spec = case.slab_case(96, (48, 48), (3, 2), is_Lunar_resistance=1, use_implicit_lunar_resistance=1,
+                          eta_max_lunar=1e-3 * case.MU0 * sc["U"] * sc["L_ref"], implicit_resistive_ksp_rtol=1e-10)
+    cells = sum(b.ncell[0] * b.ncell[1] * b.ncell[2] for b in spec.blocks)
+    return spec, case.inflow_state(spec), "tiled", cells
 
 
-def cpu_reference(n, steps, nproc):
+def mem_available_gb():
+    try:
+        for ln in open("/proc/meminfo"):
+            if ln.startswith("MemAvailable:"):
+                return int(ln.split()[1]) / 1e6
+    except OSError:
+        pass
+    return 16.0
+
+
+def cpu_reference(workload, n, steps, nproc):
     """Times the reference's own StepOnce loop (oracle/_ref/ref_lunar, built
     from the reference sources) on `nproc` concurrent single-threaded
-    processes, each on the same bounded sample; returns aggregate
-    cell-updates/s and the per-process figures."""
+    processes (bounded by host memory), each on the same bounded sample;
+    returns aggregate cell-updates/s, the per-process figures and the
+    process count."""
     from beta1_b200 import case, rst
     if not os.path.exists(REF_BIN):
         return None
-    spec, st = build_case(n)
+    nproc = max(1, min(nproc, int(0.6 * mem_available_gb() / WORKLOADS[workload]["ref_rss_gb"])))
+    spec, st, _, _ = build_case(workload, n)
     d = tempfile.mkdtemp(prefix="b1ref_")
     try:
         case.write_case(d, spec)
@@ -129,15 +160,20 @@ def cpu_reference(n, steps, nproc):
         for p in range(nproc):
             wd = os.path.join(d, "r%d" % p)
             os.makedirs(wd)
-            os.symlink(os.path.join(d, "CASE"), os.path.join(wd, "CASE"))
+            for entry in os.listdir(d):
+                if entry not in ("init.rst",) and not entry.startswith("r"):
+                    os.symlink(os.path.join(d, entry), os.path.join(wd, entry))
             procs.append(subprocess.Popen([REF_BIN, "time", os.path.join(d, "init.rst"), str(steps)], cwd=wd,
                                           stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
         vals = []
         for pr in procs:
             out, _ = pr.communicate()
-            vals.append(json.loads(out.strip().splitlines()[-1]))
+            lines = [ln for ln in out.strip().splitlines() if ln.startswith("{")]
+            if pr.returncode != 0 or not lines:
+                return None
+            vals.append(json.loads(lines[-1]))
         agg = sum(v["cell_updates_per_s"] for v in vals)
-        return agg, vals
+        return agg, vals, nproc
     finally:
         shutil.rmtree(d, ignore_errors=True)
 
@@ -146,20 +182,22 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    nproc = os.cpu_count() or 1
-    res = cpu_reference(args.n, args.ref_steps, nproc)
+    wl = WORKLOADS[args.workload]
+    steps = min(args.steps, args.ref_steps or wl["ref_steps"])
+    res = cpu_reference(args.workload, args.n, steps, os.cpu_count() or 1)
     if res is None:
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_lunar not built (no reference tree)"}))
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_lunar not built or failed"}))
         return 0
-    agg, vals = res
-    sample = "%d^3 periodic block, %d StepOnce per process, %d concurrent single-threaded processes" % (
-        args.n, args.ref_steps, nproc)
+    agg, vals, nproc = res
+    cells = vals[0]["cells"]
+    sample = "%s: %d StepOnce per process, %d concurrent single-threaded processes (bounded by host cores and " \
+             "memory)" % (wl["name"], steps, nproc)
     line = {
         "impl": "reference", "metric": "cell-updates/s", "value": agg, "unit": "cell-updates/s",
-        "n_gpus": args.gpus, "steps": args.ref_steps, "warmup": 0,
-        "ms_per_step": 1000.0 * vals[0]["seconds"] / vals[0]["steps"], "higher_is_better": True,
+        "n_gpus": args.gpus, "steps": steps, "warmup": 0,
+        "ms_per_step": 1000.0 * max(v["seconds"] / v["steps"] for v in vals), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "c1_periodic_%dcubed_fp64" % args.n, "cells": args.n ** 3},
+        "config": {"workload": wl["name"], "cells": cells},
         "cpu_baseline": {"value": agg, "unit": "cell-updates/s", "cores": nproc, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": agg, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -171,16 +209,19 @@ def run_reference_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=4000)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None, help="timed steps (default 200 for c2, 4000 for c1)")
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--n", type=int, default=64, help="cells per direction of the periodic block")
-    ap.add_argument("--ref-steps", type=int, default=40, help="StepOnce per reference CPU sample")
+    ap.add_argument("--workload", default="c2", choices=list(WORKLOADS))
+    ap.add_argument("--n", type=int, default=64, help="cells per direction of the c1 periodic block")
+    ap.add_argument("--ref-steps", type=int, default=None, help="StepOnce per reference CPU sample")
     ap.add_argument("--e2e-iters", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.steps is None:
+        args.steps = 200 if args.workload == "c2" else 4000
 
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -198,12 +239,18 @@ def main():
 
     from beta1_b200 import solver
 
-    spec, st = build_case(args.n)
-    s = solver.Solver(spec)
+    wl = WORKLOADS[args.workload]
+    spec, st, topology, cells = build_case(args.workload, args.n)
+    s = solver.Solver(spec, topology=topology)
     s.load_state(st)
     ctx = s.ctx
-    cells = args.n ** 3
     stream = torch.cuda.ExternalStream(ctx.stream())
+    ctx_bytes = sum(ctx.field_info(f, b)["ncomp"] * int(np.prod([h - l for l, h in zip(
+        ctx.field_info(f, b)["lo"], ctx.field_info(f, b)["hi"])])) * 8 for f in ("U_H", "PV_H", "JDxi", "JDet",
+                                                                                 "JDze", "Jcell_from_Jedge_w",
+                                                                                 "Bcell_from_Bface_w")
+        for b in range(len(spec.blocks)))
+    res_stats = None
 
     # warm-up (also builds and instantiates the step graph)
     ctx.step(args.warmup)
@@ -231,6 +278,10 @@ def main():
         dist.barrier()
     ms = e0.elapsed_time(e1)
     launches = ctx.launches() - l0
+    if spec.params.get("is_Lunar_resistance", 0):
+        rs = ctx.resistive_stats()
+        res_stats = {"krylov_its_last_step": rs["its"], "rnorm": rs["rnorm"], "bnorm": rs["bnorm"],
+                     "reason": rs["reason"], "unknowns": int(len(s.resistive_dofs[0])), "rtol": float(spec.params["implicit_resistive_ksp_rtol"])}
     stop.set()
     th.join()
     ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
@@ -259,10 +310,11 @@ def main():
     hin, hout = PinnedArray(nstate), PinnedArray(nstate)
     # the state after the timed steps, as the caller would hold it
     off = 0
-    for name in ("U_H", "B_xi", "B_eta", "B_zeta"):
-        a = ctx.download(name, 0).ravel()
-        hin.a[off:off + a.size] = a
-        off += a.size
+    for b in range(len(spec.blocks)):
+        for name in ("U_H", "B_xi", "B_eta", "B_zeta"):
+            a = ctx.download(name, b).ravel()
+            hin.a[off:off + a.size] = a
+            off += a.size
     ctx.step_host(1, hin.a, hout.a)
     torch.cuda.synchronize()
     f0 = torch.cuda.Event(enable_timing=True)
@@ -282,12 +334,13 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        res = cpu_reference(args.n, args.ref_steps, 1)
+        ref_steps = args.ref_steps or wl["ref_steps"]
+        res = cpu_reference(args.workload, args.n, ref_steps, 1)
         if res is not None:
-            agg, vals = res
+            agg, vals, _ = res
             cpu = {"value": agg, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
-                   "sample": "%d^3 periodic block, %d StepOnce of the reference solver built from its own "
-                             "sources, one single-threaded process" % (args.n, args.ref_steps)}
+                   "sample": "%s, %d StepOnce of the reference solver built from its own sources, one "
+                             "single-threaded process" % (wl["name"], ref_steps)}
 
     if rank == 0:
         line = {
@@ -295,11 +348,10 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded 1e-3 noise on rho, v and div-free B; reference restart format)",
-            "config": {"workload": "c1_periodic_%dcubed_fp64" % args.n, "cells_per_gpu": cells, "blocks": 1,
+            "config": {"workload": wl["name"], "cells_per_gpu": cells, "blocks": len(spec.blocks),
                        "integrator": "forward Euler StepOnce (reference parity mode)", "precision": "fp64",
                        "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "no flush: per-step working set %.2f GB > 126 MB L2" % (
-                           (args.n + 9) ** 3 * 138 * 8 / 1e9)},
+                       "l2": "no flush: per-step working set %.2f GB > 126 MB L2" % (ctx_bytes / 1e9)},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": nstate * 8,
                     "d2h_bytes_per_step": nstate * 8},
             "gpu_launches": int(launches),
@@ -309,6 +361,7 @@ def main():
                          "algo_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_launch_ms,
                          "kernel_share": per_step[dominant] / total},
             "kernels_ms_per_step": {k: round(v, 5) for k, v in sorted(per_step.items(), key=lambda kv: -kv[1])},
+            "resistive_solve": res_stats,
             "cpu_baseline": cpu,
             "clocks": summarize_clocks(clocks),
         }

@@ -63,24 +63,26 @@ def eta_at_edges(edges, nodes, inver_Rem):
     """Resistivity of edges (block, dir, i, j, k): inver_Rem times the tanh
     shell profile of the edge-midpoint radius, zero outside 0.84 < r < 1.04
     and on collapsed edges (LunarSolver::ImplicitResistiveEtaAtEdge_,
-    Z4_Lunar/src/implicit/Lunar_ImplicitResistive.cpp:166-199)."""
+    Z4_Lunar/src/implicit/Lunar_ImplicitResistive.cpp:166-199).  The radius
+    and length follow the reference's operation order; the profile uses the
+    C library's tanh, as the reference does."""
+    edges = np.asarray(edges)
     eta = np.zeros(len(edges))
-    for q, (b, d, i, j, k) in enumerate(edges):
+    for b in np.unique(edges[:, 0]) if len(edges) else []:
         X = nodes[int(b)]
         o = X.off
-        di, dj, dk = (d == 1), (d == 2), (d == 3)
+        sel = np.nonzero(edges[:, 0] == b)[0]
+        d, i, j, k = (edges[sel, c] for c in range(1, 5))
         p0 = X.a[i + o, j + o, k + o]
-        p1 = X.a[i + di + o, j + dj + o, k + dk + o]
-        dl = math.sqrt((p1[0] - p0[0]) ** 2 + (p1[1] - p0[1]) ** 2 + (p1[2] - p0[2]) ** 2)
-        if abs(dl) <= 1.0e-12:
-            continue
-        xm = 0.5 * (p0[0] + p1[0])
-        ym = 0.5 * (p0[1] + p1[1])
-        zm = 0.5 * (p0[2] + p1[2])
-        r = math.sqrt(xm * xm + ym * ym + zm * zm)
-        if r <= 0.84 or r >= 1.04:
-            continue
-        eta[q] = inver_Rem * (0.5 * (math.tanh((r - 0.84) / 0.02) - math.tanh((r - 1.04) / 0.02)))
+        p1 = X.a[i + (d == 1) + o, j + (d == 2) + o, k + (d == 3) + o]
+        dx, dy, dz = (p1[:, c] - p0[:, c] for c in range(3))
+        dl = np.sqrt(dx * dx + dy * dy + dz * dz)
+        xm, ym, zm = (0.5 * (p0[:, c] + p1[:, c]) for c in range(3))
+        r = np.sqrt(xm * xm + ym * ym + zm * zm)
+        live = ~(np.abs(dl) <= 1.0e-12) & ~(r <= 0.84) & ~(r >= 1.04)
+        for q in np.nonzero(live)[0]:
+            rq = float(r[q])
+            eta[sel[q]] = inver_Rem * (0.5 * (math.tanh((rq - 0.84) / 0.02) - math.tanh((rq - 1.04) / 0.02)))
     return eta
 
 
