@@ -46,10 +46,12 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 ALGO_BYTES_PER_CELL = {
     # U 5, PV 5, JD 9, Jac 1, B_cell 3, J_cell 3 read; RHS_H 5 written
     "k_fluid_rhs": 31 * 8,
-    # B 3, Badd 3, JD 9, Jac 1, U_plus 3 read; Eface 9 written
-    "k_eface": 28 * 8,
-    # Eface 6, B 3, JD 9, Jac 1, U_plus 3 read; E 3 written
-    "k_eedge": 25 * 8,
+    # JD 9, Jac 1, U_plus 3 read; U_contra 3 written
+    "k_ucontra": 16 * 8,
+    # B 3, Badd 3, U_contra 3 read; Eface 9 written
+    "k_eface": 18 * 8,
+    # Eface 6, B 3, U_contra 3 read; E 3 written
+    "k_eedge": 15 * 8,
     # E 3 read, RHS_B 3 written, B 3 read + written
     "k_curl_e2f": 12 * 8,
     # U 5 read + written, RHS_H 5 read

@@ -6,11 +6,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
+#include <cstdint>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <map>
 #include <string>
+#include <unordered_set>
 #include <vector>
 
 using namespace mhd;
@@ -58,15 +61,14 @@ struct SyncMap
 
 constexpr int kThreads = 256;
 
-const char *const kKernelNames[] = {"k_fluid_rhs",   "k_eface",        "k_eedge",         "k_curl_e2f",
-                                    "k_update_u",    "k_bcell",        "k_jedge",         "k_jcell",
-                                    "k_pv_uplus_dt", "k_begin_step",   "k_arm_dt",        "k_end_step",
-                                    "k_gather",      "k_gather_stage", "k_scatter_stage", "k_aos_to_soa",
-                                    "k_soa_to_aos",  "k_set_consts",   "k_wall_u",
-                                    "k_alias_copy",  "k_scatter_vec",  "k_resist_out",    "k_resist_rhs",
-                                    "k_dots_partial", "k_dots_final",  "k_sub_proj",      "k_add_small",
-                                    "k_div_dev",     "k_gmres_column", "k_gmres_start",   "k_gmres_solve_y",
-                                    "k_add_basis",   "k_residual"};
+const char *const kKernelNames[] = {
+    "k_fluid_rhs",    "k_eface",       "k_eedge",        "k_curl_e2f",     "k_update_u",      "k_bcell",
+    "k_jedge",        "k_jcell",       "k_pv_uplus_dt",  "k_begin_step",   "k_arm_dt",        "k_end_step",
+    "k_gather",       "k_gather_stage", "k_scatter_stage", "k_aos_to_soa", "k_soa_to_aos",    "k_set_consts",
+    "k_wall_u",       "k_alias_copy",  "k_scatter_vec",  "k_resist_out",   "k_resist_rhs",    "k_dots_partial",
+    "k_dots_final",   "k_sub_proj",    "k_add_small",    "k_div_guard",    "k_div_next",      "k_gmres_init",
+    "k_cycle_start",  "k_gmres_column", "k_inner_check", "k_gmres_solve_y", "k_add_basis",    "k_outer_check",
+    "k_zero",         "k_residual",    "k_ucontra"};
 constexpr int kNumKernelNames = int(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
 
 } // namespace
@@ -108,9 +110,14 @@ struct mhd_ctx
         uint64_t *dj = nullptr;        // ... in dJ_*
         uint64_t *j = nullptr;         // ... in J_*
         double *eta = nullptr;
-        int64_t nalias = 0;            // edge aliases <- owners (sync_edge_1form)
-        uint64_t *alias_e = nullptr, *owner_e = nullptr, *alias_dj = nullptr, *owner_dj = nullptr;
+        int64_t nalias = 0;            // aliases of unknown owners (sync_edge_1form)
+        uint64_t *alias_e = nullptr, *owner_e = nullptr;
         double *sign = nullptr;
+        // the operator's active region: copies with a destination inside it,
+        // and per (block, axis) sub-ranges of the inner faces / edges
+        SyncMap eres1form, db;
+        int *rng_face = nullptr, *rng_edge = nullptr;
+        int64_t nface_max = 0, nedge_max = 0;
         double rtol = 1e-8, atol = 1e-12;
         int maxit = 200, restart = 30;
         // workspace
@@ -118,17 +125,23 @@ struct mhd_ctx
         double *partial = nullptr, *dots = nullptr;
         GmresState *st = nullptr;
         int ngroups = 1;
-        // statistics of the last solve
-        int its = 0;
-        double rnorm = 0.0, bnorm = 0.0;
-        int reason = 0;
+        // launch accounting of the graph-resident loops
+        int64_t k_cycle = 0, k_inner = 0;        // kernels per restart cycle / per Arnoldi step
+        long long its_eager = 0, cycles_eager = 0;
+        bool graph_loops = true;                 // conditional graph nodes usable
+        std::vector<uint64_t> seed;              // unknown and alias offsets (Eres), for the region
     } res;
+    cudaStream_t spare[2] = {nullptr, nullptr}; // capture streams of conditional bodies
+    int spare_depth = 0;
 
     // eager profiling: one event pair per launch
     bool profiling = false;
     std::vector<const char *> prof_names;
     std::vector<cudaEvent_t> prof_ev;
 };
+
+static void free_resistive(mhd_ctx *ctx);
+static int resistive_region(mhd_ctx *ctx, const std::vector<uint64_t> &seed);
 
 namespace
 {
@@ -241,6 +254,25 @@ int launched(mhd_ctx *ctx, int nk = 1)
     return MHD_OK;
 }
 
+// phase B of a sync: the composed copies
+int gather_map(mhd_ctx *ctx, const SyncMap &s)
+{
+    if (s.n == 0)
+        return MHD_OK;
+    if (s.tmp)
+    {
+        prof_begin(ctx, "k_gather_stage");
+        k_gather_stage<<<grid_for(s.n), kThreads, 0, ctx->stream>>>(s.tmp, ctx->pool, s.src, s.n);
+        RUN(launched(ctx));
+        prof_begin(ctx, "k_scatter_stage");
+        k_scatter_stage<<<grid_for(s.n), kThreads, 0, ctx->stream>>>(ctx->pool, s.tmp, s.dst, s.n);
+        return launched(ctx);
+    }
+    prof_begin(ctx, "k_gather");
+    k_gather<<<grid_for(s.n), kThreads, 0, ctx->stream>>>(ctx->pool, s.dst, s.src, s.n);
+    return launched(ctx);
+}
+
 int run_sync(mhd_ctx *ctx, const char *group)
 {
     auto it = ctx->syncs.find(group);
@@ -262,20 +294,7 @@ int run_sync(mhd_ctx *ctx, const char *group)
         k_wall_u<<<grid_for(ncol), kThreads, 0, ctx->stream>>>(ctx->dbv, w.first, w.second, ctx->c.gamma);
         RUN(launched(ctx));
     }
-    if (s.n == 0)
-        return MHD_OK;
-    if (s.tmp)
-    {
-        prof_begin(ctx, "k_gather_stage");
-        k_gather_stage<<<grid_for(s.n), kThreads, 0, ctx->stream>>>(s.tmp, ctx->pool, s.src, s.n);
-        RUN(launched(ctx));
-        prof_begin(ctx, "k_scatter_stage");
-        k_scatter_stage<<<grid_for(s.n), kThreads, 0, ctx->stream>>>(ctx->pool, s.tmp, s.dst, s.n);
-        return launched(ctx);
-    }
-    prof_begin(ctx, "k_gather");
-    k_gather<<<grid_for(s.n), kThreads, 0, ctx->stream>>>(ctx->pool, s.dst, s.src, s.n);
-    return launched(ctx);
+    return gather_map(ctx, s);
 }
 
 int launch_update_derived(mhd_ctx *ctx)
@@ -291,7 +310,7 @@ int launch_update_derived(mhd_ctx *ctx)
                                                                               : max_box(ctx, LOC_EXI, 0);
     const int64_t ne2 = max_box(ctx, LOC_EETA, 0) > ne ? max_box(ctx, LOC_EETA, 0) : ne;
     prof_begin(ctx, "k_jedge");
-    k_jedge<<<dim3(grid_for(ne2), nb, 3), kThreads, 0, s>>>(ctx->dbv, F_Bxi, F_Jxi, 1.0);
+    k_jedge<<<dim3(grid_for(ne2), nb, 3), kThreads, 0, s>>>(ctx->dbv, F_Bxi, F_Jxi, 1.0, nullptr);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Jedge"));
     prof_begin(ctx, "k_jcell");
@@ -325,6 +344,9 @@ int launch_induction(mhd_ctx *ctx, bool update_b)
     int64_t nf = 0;
     for (int l = LOC_FXI; l <= LOC_FZETA; ++l)
         nf = max_box(ctx, l, 0) > nf ? max_box(ctx, l, 0) : nf;
+    prof_begin(ctx, "k_ucontra");
+    k_ucontra<<<dim3(grid_for(max_box(ctx, LOC_CELL, 1)), nb), kThreads, 0, s>>>(ctx->dbv);
+    RUN(launched(ctx));
     prof_begin(ctx, "k_eface");
     k_eface<<<dim3(grid_for(nf), nb, 3), kThreads, 0, s>>>(ctx->dbv);
     RUN(launched(ctx));
@@ -338,7 +360,7 @@ int launch_induction(mhd_ctx *ctx, bool update_b)
     RUN(run_sync(ctx, "Eedge"));
     prof_begin(ctx, "k_curl_e2f");
     k_curl_e2f<<<dim3(grid_for(nf), nb, 3), kThreads, 0, s>>>(ctx->dbv, F_Exi, F_RBxi, update_b ? F_Bxi : -1,
-                                                               -1.0, ctx->dt, 1.0, 0);
+                                                               -1.0, ctx->dt, 1.0, 0, nullptr);
     return launched(ctx);
 }
 
@@ -353,230 +375,288 @@ int launch_update_u(mhd_ctx *ctx)
 
 // ---------------------------------------------------------------------------
 // implicit resistive step (Z4_Lunar/src/implicit/Lunar_ImplicitResistive.cpp:264-518)
+//
+// The operator only touches the unknowns' neighbourhood: Eres is non-zero at
+// the unknowns, their aliases and the sync images of those, and dB next to
+// them.  mhd_set_resistive computes per block a box holding all of these
+// (closed under the Eres1form and dB copies, widened by the curl stencils);
+// the curls, J edges and copies of the solve run on that box only.  Outside
+// it the fields stay zero, as the reference's full-array clears and loops
+// leave them, so restricting the work changes no value the solve reads.
 // ---------------------------------------------------------------------------
 
-// clear_triplet: zero every point of three fields on every block
-int clear_fields(mhd_ctx *ctx, int f0)
-{
-    for (int f = f0; f < f0 + 3; ++f)
-        for (int b = 0; b < ctx->nblocks; ++b)
-            CK(ctx, cudaMemsetAsync(ctx->pool + ctx->base[size_t(f)][size_t(b)], 0,
-                                    size_t(ctx->hbv[size_t(b)].vol) * 8 * size_t(kFields[f].ncomp), ctx->stream));
-    return MHD_OK;
-}
-
-int launch_curl(mhd_ctx *ctx, int fE0, int fR0, int fB0, double mult, int mult_is_neg_dt)
-{
-    int64_t nf = 0;
-    for (int l = LOC_FXI; l <= LOC_FZETA; ++l)
-        nf = max_box(ctx, l, 0) > nf ? max_box(ctx, l, 0) : nf;
-    prof_begin(ctx, "k_curl_e2f");
-    k_curl_e2f<<<dim3(grid_for(nf), ctx->nblocks, 3), kThreads, 0, ctx->stream>>>(ctx->dbv, fE0, fR0, fB0, mult, ctx->dt,
-                                                                                 1.0, mult_is_neg_dt);
-    return launched(ctx);
-}
-
-int launch_jedge(mhd_ctx *ctx, int fB0, int fJ0)
-{
-    int64_t ne = 0;
-    for (int l = LOC_EXI; l <= LOC_EZETA; ++l)
-        ne = max_box(ctx, l, 0) > ne ? max_box(ctx, l, 0) : ne;
-    prof_begin(ctx, "k_jedge");
-    k_jedge<<<dim3(grid_for(ne), ctx->nblocks, 3), kThreads, 0, ctx->stream>>>(ctx->dbv, fB0, fJ0, 1.0);
-    return launched(ctx);
-}
-
-int alias_copy(mhd_ctx *ctx, uint64_t *alias, uint64_t *owner)
+int launch_curl_rng(mhd_ctx *ctx, int fE0, int fR0, int fB0, double mult, int mult_is_neg_dt)
 {
     auto &R = ctx->res;
-    if (R.nalias == 0)
+    if (R.nface_max == 0)
         return MHD_OK;
-    prof_begin(ctx, "k_alias_copy");
-    k_alias_copy<<<grid_for(R.nalias), kThreads, 0, ctx->stream>>>(ctx->pool, alias, owner, R.sign, R.nalias);
+    prof_begin(ctx, "k_curl_e2f");
+    k_curl_e2f<<<dim3(grid_for(R.nface_max), ctx->nblocks, 3), kThreads, 0, ctx->stream>>>(
+        ctx->dbv, fE0, fR0, fB0, mult, ctx->dt, 1.0, mult_is_neg_dt, R.rng_face);
     return launched(ctx);
 }
 
-// UnpackVecToImplicitEres_: Eres <- 0, Eres[unknowns] <- x, aliases, Sync("Eres1form")
-int unpack_eres(mhd_ctx *ctx, const double *x)
+int launch_jedge_rng(mhd_ctx *ctx, int fB0, int fJ0)
 {
     auto &R = ctx->res;
-    RUN(clear_fields(ctx, F_Eresxi));
-    prof_begin(ctx, "k_scatter_vec");
-    k_scatter_vec<<<grid_for(R.n), kThreads, 0, ctx->stream>>>(ctx->pool, R.e, x, R.n);
-    RUN(launched(ctx));
-    RUN(alias_copy(ctx, R.alias_e, R.owner_e));
-    return run_sync(ctx, "Eres1form");
+    if (R.nedge_max == 0)
+        return MHD_OK;
+    prof_begin(ctx, "k_jedge");
+    k_jedge<<<dim3(grid_for(R.nedge_max), ctx->nblocks, 3), kThreads, 0, ctx->stream>>>(ctx->dbv, fB0, fJ0, 1.0,
+                                                                                      R.rng_edge);
+    return launched(ctx);
 }
 
-// y = A x  (MatMultImplicitResistive_)
-int resist_matvec(mhd_ctx *ctx, const double *x, double *y)
+// UnpackVecToImplicitEres_: Eres[unknowns] <- x (column *jdev of x0 when
+// jdev is given), aliases <- sign * owner, Sync("Eres1form")
+int unpack_eres(mhd_ctx *ctx, const double *x0, const int *jdev)
 {
     auto &R = ctx->res;
-    RUN(unpack_eres(ctx, x));
-    RUN(clear_fields(ctx, F_dBxi));
-    RUN(launch_curl(ctx, F_Eresxi, F_dBxi, -1, 0.0, /*mult_is_neg_dt=*/1));
-    RUN(run_sync(ctx, "dB"));
-    RUN(clear_fields(ctx, F_dJxi));
-    RUN(launch_jedge(ctx, F_dBxi, F_dJxi));
-    RUN(alias_copy(ctx, R.alias_dj, R.owner_dj));
-    RUN(run_sync(ctx, "dJ"));
+    if (R.n > 0)
+    {
+        prof_begin(ctx, "k_scatter_vec");
+        k_scatter_vec<<<grid_for(R.n), kThreads, 0, ctx->stream>>>(ctx->pool, R.e, x0, R.n, jdev, R.n);
+        RUN(launched(ctx));
+    }
+    if (R.nalias > 0)
+    {
+        prof_begin(ctx, "k_alias_copy");
+        k_alias_copy<<<grid_for(R.nalias), kThreads, 0, ctx->stream>>>(ctx->pool, R.alias_e, R.owner_e, R.sign,
+                                                                        R.nalias);
+        RUN(launched(ctx));
+    }
+    return gather_map(ctx, R.eres1form);
+}
+
+// y = A x  (MatMultImplicitResistive_): dB = -dt curl Eres, Sync("dB"),
+// dJ = alpha curlAdj(beta dB), y = Eres - eta dJ at the unknowns.  The
+// owner->alias copy of dJ is not needed: y reads dJ at owners only.
+int resist_matvec(mhd_ctx *ctx, const double *x0, const int *jdev, double *y)
+{
+    auto &R = ctx->res;
+    RUN(unpack_eres(ctx, x0, jdev));
+    RUN(launch_curl_rng(ctx, F_Eresxi, F_dBxi, -1, 0.0, /*mult_is_neg_dt=*/1));
+    RUN(gather_map(ctx, R.db));
+    RUN(launch_jedge_rng(ctx, F_dBxi, F_dJxi));
     prof_begin(ctx, "k_resist_out");
     k_resist_out<<<grid_for(R.n), kThreads, 0, ctx->stream>>>(ctx->pool, R.e, R.dj, R.eta, y, R.n);
     return launched(ctx);
 }
 
-int dots(mhd_ctx *ctx, const double *V, int nvec, const double *w, double *out, bool with_norm, bool accumulate)
+// out[c] = V_c . w for c < nvec (or c <= *jdev), out[0] = w . w when V is null
+int dots(mhd_ctx *ctx, const double *V, int nvec, const int *jdev, const double *w, double *out)
 {
     auto &R = ctx->res;
-    const int ny = nvec + (with_norm ? 1 : 0);
+    const int ny = jdev ? R.restart + 1 : nvec;
     prof_begin(ctx, "k_dots_partial");
-    k_dots_partial<<<dim3(R.ngroups, ny), 256, 0, ctx->stream>>>(V, R.n, nvec, w, R.n, R.partial, with_norm);
+    k_dots_partial<<<dim3(R.ngroups, ny), 256, 0, ctx->stream>>>(V, R.n, nvec, w, R.n, R.partial, jdev);
     RUN(launched(ctx));
     prof_begin(ctx, "k_dots_final");
-    k_dots_final<<<1, 64, 0, ctx->stream>>>(R.partial, R.ngroups, ny, out, accumulate ? 1 : 0);
+    k_dots_final<<<1, 64, 0, ctx->stream>>>(R.partial, R.ngroups, nvec, out, jdev);
     return launched(ctx);
 }
 
-int read_scalar(mhd_ctx *ctx, const double *dev, double *host)
+#define LAUNCH1(name, ...)                                        \
+    do                                                            \
+    {                                                             \
+        prof_begin(ctx, #name);                                   \
+        name<<<1, 1, 0, ctx->stream>>>(__VA_ARGS__);              \
+        RUN(launched(ctx));                                       \
+    } while (0)
+#define LAUNCHN(name, n, ...)                                     \
+    do                                                            \
+    {                                                             \
+        prof_begin(ctx, #name);                                   \
+        name<<<grid_for(n), kThreads, 0, ctx->stream>>>(__VA_ARGS__); \
+        RUN(launched(ctx));                                       \
+    } while (0)
+
+// GMRES(m) with x0 = 0 and the convergence test ||r|| <= max(rtol ||b||, atol)
+// of PETSc's default (KSPConvergedDefault), in three pieces that run either
+// eagerly (the host reads the loop flags) or inside the step graph (the
+// kernels set conditional handles).
+int gmres_prologue(mhd_ctx *ctx)
 {
-    CK(ctx, cudaMemcpyAsync(host, dev, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    auto &R = ctx->res;
+    RUN(dots(ctx, nullptr, 1, nullptr, R.b, R.dots + 40));
+    LAUNCH1(k_gmres_init, R.st, R.dots + 40, R.rtol, R.atol, R.maxit, R.restart);
+    LAUNCHN(k_zero, R.n, R.x, R.n);
+    return MHD_OK;
+}
+
+int gmres_cycle_start(mhd_ctx *ctx, cudaGraphConditionalHandle h, int use)
+{
+    auto &R = ctx->res;
+    RUN(resist_matvec(ctx, R.x, nullptr, R.w));
+    LAUNCHN(k_residual, R.n, R.b, R.w, R.r, R.n);
+    RUN(dots(ctx, nullptr, 1, nullptr, R.r, R.dots));
+    LAUNCH1(k_cycle_start, R.st, R.dots, h, use);
+    LAUNCHN(k_div_guard, R.n, R.V, R.r, &R.st->beta, R.n, &R.st->inner);
+    return MHD_OK;
+}
+
+// one Arnoldi step on column j, classical Gram-Schmidt applied twice
+int gmres_step(mhd_ctx *ctx, cudaGraphConditionalHandle h, int use)
+{
+    auto &R = ctx->res;
+    const int *j = &R.st->j;
+    double *hcol = R.st->hcol;
+    RUN(resist_matvec(ctx, R.V, j, R.w));
+    RUN(dots(ctx, R.V, 0, j, R.w, hcol));
+    LAUNCHN(k_sub_proj, R.n, R.V, R.n, 0, hcol, R.w, R.n, j);
+    RUN(dots(ctx, R.V, 0, j, R.w, R.dots));
+    LAUNCHN(k_sub_proj, R.n, R.V, R.n, 0, R.dots, R.w, R.n, j);
+    prof_begin(ctx, "k_add_small");
+    k_add_small<<<1, 32, 0, ctx->stream>>>(hcol, R.dots, j);
+    RUN(launched(ctx));
+    RUN(dots(ctx, nullptr, 1, nullptr, R.w, R.dots + 32));
+    LAUNCH1(k_gmres_column, R.st, R.dots + 32);
+    LAUNCHN(k_div_next, R.n, R.V, R.n, R.w, R.st, R.n);
+    LAUNCH1(k_inner_check, R.st, h, use);
+    return MHD_OK;
+}
+
+int gmres_cycle_end(mhd_ctx *ctx, cudaGraphConditionalHandle h, int use)
+{
+    auto &R = ctx->res;
+    LAUNCH1(k_gmres_solve_y, R.st);
+    LAUNCHN(k_add_basis, R.n, R.V, R.n, R.st, R.x, R.n);
+    LAUNCH1(k_outer_check, R.st, h, use);
+    return MHD_OK;
+}
+
+int read_flag(mhd_ctx *ctx, const int *dev, int *host)
+{
+    CK(ctx, cudaMemcpyAsync(host, dev, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CK(ctx, cudaStreamSynchronize(ctx->stream));
     return MHD_OK;
 }
 
-// Restarted GMRES from x = 0 with the convergence test
-// ||r|| <= max(rtol ||b||, atol) of the PETSc default (KSPConvergedDefault).
-int resist_gmres(mhd_ctx *ctx)
+int gmres_eager(mhd_ctx *ctx)
 {
     auto &R = ctx->res;
-    const int m = R.restart;
-    const int64_t n = R.n;
-    CK(ctx, cudaMemsetAsync(R.x, 0, size_t(n) * 8, ctx->stream));
-    // ||b||
-    RUN(dots(ctx, R.b, 1, R.b, R.dots, false, false));
-    double b2 = 0.0;
-    RUN(read_scalar(ctx, R.dots, &b2));
-    R.bnorm = std::sqrt(b2);
-    const double ttol = std::max(R.rtol * R.bnorm, R.atol);
-    R.its = 0;
-    R.reason = 0;
-    bool first = true;
-    while (true)
+    RUN(gmres_prologue(ctx));
+    int outer = 1;
+    while (outer)
     {
-        // r = b - A x   (x = 0 on the first cycle: r = b)
-        if (first)
-            CK(ctx, cudaMemcpyAsync(R.r, R.b, size_t(n) * 8, cudaMemcpyDeviceToDevice, ctx->stream));
-        else
+        RUN(gmres_cycle_start(ctx, 0, 0));
+        int inner = 0;
+        RUN(read_flag(ctx, &R.st->inner, &inner));
+        while (inner)
         {
-            RUN(resist_matvec(ctx, R.x, R.w));
-            prof_begin(ctx, "k_residual");
-            k_residual<<<grid_for(n), kThreads, 0, ctx->stream>>>(R.b, R.w, R.r, n);
-            RUN(launched(ctx));
+            RUN(gmres_step(ctx, 0, 0));
+            ++R.its_eager;
+            RUN(read_flag(ctx, &R.st->inner, &inner));
         }
-        first = false;
-        RUN(dots(ctx, R.r, 1, R.r, R.dots, false, false));
-        prof_begin(ctx, "k_gmres_start");
-        k_gmres_start<<<1, 1, 0, ctx->stream>>>(R.st, R.dots);
-        RUN(launched(ctx));
-        double beta = 0.0;
-        RUN(read_scalar(ctx, &R.st->beta, &beta));
-        R.rnorm = beta;
-        if (beta <= ttol)
-        {
-            R.reason = (beta <= R.atol) ? 3 : 2;
-            return MHD_OK;
-        }
-        if (R.its >= R.maxit)
-        {
-            R.reason = -3;
-            return MHD_OK;
-        }
-        prof_begin(ctx, "k_div_dev");
-        k_div_dev<<<grid_for(n), kThreads, 0, ctx->stream>>>(R.V, R.r, &R.st->beta, n);
-        RUN(launched(ctx));
-        int j = 0;
-        bool done = false;
-        for (; j < m && R.its < R.maxit; ++j)
-        {
-            double *vj = R.V + int64_t(j) * n;
-            RUN(resist_matvec(ctx, vj, R.w));
-            double *hcol = R.st->hcol;
-            // classical Gram-Schmidt, twice: h = V^T w, w -= V h; h2 = V^T w, w -= V h2, h += h2
-            RUN(dots(ctx, R.V, j + 1, R.w, hcol, false, false));
-            prof_begin(ctx, "k_sub_proj");
-            k_sub_proj<<<grid_for(n), kThreads, 0, ctx->stream>>>(R.V, n, j + 1, hcol, R.w, n);
-            RUN(launched(ctx));
-            RUN(dots(ctx, R.V, j + 1, R.w, R.dots, false, false));
-            prof_begin(ctx, "k_sub_proj");
-            k_sub_proj<<<grid_for(n), kThreads, 0, ctx->stream>>>(R.V, n, j + 1, R.dots, R.w, n);
-            RUN(launched(ctx));
-            prof_begin(ctx, "k_add_small");
-            k_add_small<<<1, 32, 0, ctx->stream>>>(hcol, R.dots, j + 1);
-            RUN(launched(ctx));
-            RUN(dots(ctx, nullptr, 0, R.w, R.dots + 32, true, false)); // ||w||^2
-            prof_begin(ctx, "k_gmres_column");
-            k_gmres_column<<<1, 1, 0, ctx->stream>>>(R.st, j, R.dots + 32);
-            RUN(launched(ctx));
-            double *vn = R.V + int64_t(j + 1) * n;
-            prof_begin(ctx, "k_div_dev");
-            k_div_dev<<<grid_for(n), kThreads, 0, ctx->stream>>>(vn, R.w, &R.st->hcol[j + 1], n);
-            RUN(launched(ctx));
-            ++R.its;
-            double resid = 0.0;
-            RUN(read_scalar(ctx, &R.st->resid, &resid));
-            R.rnorm = resid;
-            int brk = 0;
-            CK(ctx, cudaMemcpy(&brk, &R.st->breakdown, sizeof(int), cudaMemcpyDeviceToHost));
-            if (resid <= ttol || brk)
-            {
-                done = true;
-                ++j;
-                break;
-            }
-        }
-        prof_begin(ctx, "k_gmres_solve_y");
-        k_gmres_solve_y<<<1, 1, 0, ctx->stream>>>(R.st, j);
-        RUN(launched(ctx));
-        prof_begin(ctx, "k_add_basis");
-        k_add_basis<<<grid_for(n), kThreads, 0, ctx->stream>>>(R.V, n, R.st, j, R.x, n);
-        RUN(launched(ctx));
-        if (done)
-        {
-            R.reason = (R.rnorm <= R.atol) ? 3 : 2;
-            return MHD_OK;
-        }
-        if (R.its >= R.maxit)
-        {
-            R.reason = -3;
-            return MHD_OK;
-        }
+        RUN(gmres_cycle_end(ctx, 0, 0));
+        ++R.cycles_eager;
+        RUN(read_flag(ctx, &R.st->outer, &outer));
     }
+    return MHD_OK;
 }
 
-// the resistive part of StepOnce: Sync("Bface") (twice, as the driver and the
-// solver each call it), J from B*, b = eta J, solve, unpack, apply the update
+int capture_graph_of(mhd_ctx *ctx, cudaGraph_t *g)
+{
+    cudaStreamCaptureStatus st;
+    CK(ctx, cudaStreamGetCaptureInfo(ctx->stream, &st, nullptr, g, nullptr, nullptr));
+    if (st != cudaStreamCaptureStatusActive)
+        return fail(ctx, MHD_ESTATE, "stream is not capturing");
+    return MHD_OK;
+}
+
+// Appends a conditional while node (handle h) at the capture position of
+// ctx->stream and captures body(ctx, h) into it on a spare stream; *kernels
+// receives the kernels one pass of the body launches.
+int capture_while(mhd_ctx *ctx, cudaGraphConditionalHandle h, int (*body)(mhd_ctx *, cudaGraphConditionalHandle),
+                  int64_t *kernels)
+{
+    if (ctx->spare_depth >= 2)
+        return fail(ctx, MHD_ESTATE, "conditional nodes nested too deep");
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    CK(ctx, cudaStreamGetCaptureInfo(ctx->stream, &st, nullptr, &g, &deps, &ndeps));
+    cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(ctx, cudaGraphAddNode(&node, g, deps, ndeps, &p));
+    CK(ctx, cudaStreamUpdateCaptureDependencies(ctx->stream, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaGraph_t bodyg = p.conditional.phGraph_out[0];
+    cudaStream_t s2 = ctx->spare[ctx->spare_depth];
+    if (!s2)
+        return fail(ctx, MHD_ESTATE, "no capture stream");
+    CK(ctx, cudaStreamBeginCaptureToGraph(s2, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    cudaStream_t saved = ctx->stream;
+    ctx->stream = s2;
+    ctx->spare_depth += 1;
+    const int64_t before = ctx->launches;
+    const int rc = body(ctx, h);
+    *kernels = ctx->launches - before;
+    ctx->spare_depth -= 1;
+    ctx->stream = saved;
+    cudaGraph_t out = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s2, &out);
+    if (rc != MHD_OK)
+        return rc;
+    if (e != cudaSuccess)
+        return fail(ctx, MHD_ECUDA, "conditional body capture failed: %s", cudaGetErrorString(e));
+    return MHD_OK;
+}
+
+int gmres_step_graph(mhd_ctx *ctx, cudaGraphConditionalHandle h) { return gmres_step(ctx, h, 1); }
+
+int gmres_outer_body(mhd_ctx *ctx, cudaGraphConditionalHandle hout)
+{
+    auto &R = ctx->res;
+    cudaGraph_t g = nullptr;
+    RUN(capture_graph_of(ctx, &g));
+    cudaGraphConditionalHandle hin;
+    CK(ctx, cudaGraphConditionalHandleCreate(&hin, g, 0, 0));
+    RUN(gmres_cycle_start(ctx, hin, 1));
+    RUN(capture_while(ctx, hin, gmres_step_graph, &R.k_inner));
+    return gmres_cycle_end(ctx, hout, 1);
+}
+
+// the solve as graph nodes: prologue, then while(outer) { cycle start,
+// while(inner) { Arnoldi step }, cycle end }
+int gmres_graph(mhd_ctx *ctx)
+{
+    auto &R = ctx->res;
+    RUN(gmres_prologue(ctx));
+    cudaGraph_t g = nullptr;
+    RUN(capture_graph_of(ctx, &g));
+    cudaGraphConditionalHandle hout;
+    CK(ctx, cudaGraphConditionalHandleCreate(&hout, g, 1, cudaGraphCondAssignDefault));
+    int64_t kcyc = 0;
+    RUN(capture_while(ctx, hout, gmres_outer_body, &kcyc));
+    R.k_cycle = kcyc - R.k_inner;
+    return MHD_OK;
+}
+
+// the resistive part of StepOnce (SolveImplicitResistiveDiffusion_ +
+// ApplyImplicitResistiveUpdate_).  The reference syncs Bface twice before
+// the solve and once after the update; one sync before is equivalent (a
+// composed sync is idempotent) and the closing Sync("Bface") of the step
+// repeats the one after.  J is needed at the unknowns only here (the
+// derived-field pass recomputes it everywhere).
 int launch_resistive(mhd_ctx *ctx)
 {
     auto &R = ctx->res;
     RUN(run_sync(ctx, "Bface"));
-    RUN(run_sync(ctx, "Bface"));
-    RUN(launch_jedge(ctx, F_Bxi, F_Jxi));
-    RUN(run_sync(ctx, "Jedge"));
+    RUN(launch_jedge_rng(ctx, F_Bxi, F_Jxi));
     if (R.n > 0)
     {
-        prof_begin(ctx, "k_resist_rhs");
-        k_resist_rhs<<<grid_for(R.n), kThreads, 0, ctx->stream>>>(ctx->pool, R.j, R.eta, R.b, R.n);
-        RUN(launched(ctx));
-        RUN(resist_gmres(ctx));
-        RUN(unpack_eres(ctx, R.x));
+        LAUNCHN(k_resist_rhs, R.n, ctx->pool, R.j, R.eta, R.b, R.n);
+        if (ctx->capturing && R.graph_loops)
+            RUN(gmres_graph(ctx));
+        else
+            RUN(gmres_eager(ctx));
     }
-    else
-        RUN(unpack_eres(ctx, R.x));
-    // ApplyImplicitResistiveUpdate_
-    RUN(run_sync(ctx, "Eres1form"));
-    RUN(clear_fields(ctx, F_RBresxi));
-    RUN(launch_curl(ctx, F_Eresxi, F_RBresxi, F_Bxi, -1.0, 0));
-    return run_sync(ctx, "Bface");
+    RUN(unpack_eres(ctx, R.x, nullptr));
+    return launch_curl_rng(ctx, F_Eresxi, F_RBresxi, F_Bxi, -1.0, 0);
 }
 
 // one LunarSolver::StepOnce, explicit part: dt, fluid RHS, CT induction, update
@@ -645,9 +725,12 @@ int capture(mhd_ctx *ctx, int (*body)(mhd_ctx *), cudaGraph_t *graph, cudaGraphE
 {
     const int64_t before = ctx->launches;
     CK(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    ctx->capturing = true;
     const int rc = body(ctx);
+    ctx->capturing = false;
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    const int64_t captured = ctx->launches - before;
     ctx->launches = before;
     if (rc != MHD_OK)
     {
@@ -659,27 +742,37 @@ int capture(mhd_ctx *ctx, int (*body)(mhd_ctx *), cudaGraph_t *graph, cudaGraphE
         return fail(ctx, MHD_ECUDA, "graph capture failed: %s", cudaGetErrorString(e));
     *graph = g;
     CK(ctx, cudaGraphInstantiate(exec, g, 0));
-    size_t nn = 0;
-    CK(ctx, cudaGraphGetNodes(g, nullptr, &nn));
-    *nodes = int64_t(nn);
+    *nodes = captured;
     return MHD_OK;
 }
 
-// The step is one CUDA graph; with the implicit resistive solve (whose
-// Krylov loop is steered by the host) it is the explicit part and the
-// closing part as two graphs around the eagerly launched solve.
+// The step is one CUDA graph.  With the implicit resistive solve the Krylov
+// loop is part of it (conditional while nodes steered by the device); where
+// conditional nodes cannot be built, the step falls back to the explicit and
+// closing parts as two graphs around an eagerly launched solve.
 int build_graph(mhd_ctx *ctx)
 {
+    if (ctx->gexec || ctx->gexec_a)
+        return MHD_OK;
+    if (ctx->res.on && ctx->res.graph_loops)
+    {
+        const int rc = capture(ctx, launch_step, &ctx->graph, &ctx->gexec, &ctx->graph_kernels);
+        if (rc == MHD_OK)
+        {
+            // the loop bodies were captured once; their launches are counted per pass
+            ctx->graph_kernels -= ctx->res.k_cycle + ctx->res.k_inner;
+            return MHD_OK;
+        }
+        // conditional nodes unavailable: clear the error state of the stream and fall back
+        cudaGetLastError();
+        drop_graph(ctx);
+        ctx->res.graph_loops = false;
+    }
     if (ctx->res.on)
     {
-        if (!ctx->gexec_a)
-            RUN(capture(ctx, launch_step_a, &ctx->graph_a, &ctx->gexec_a, &ctx->graph_kernels_a));
-        if (!ctx->gexec_c)
-            RUN(capture(ctx, launch_step_c, &ctx->graph_c, &ctx->gexec_c, &ctx->graph_kernels_c));
-        return MHD_OK;
+        RUN(capture(ctx, launch_step_a, &ctx->graph_a, &ctx->gexec_a, &ctx->graph_kernels_a));
+        return capture(ctx, launch_step_c, &ctx->graph_c, &ctx->gexec_c, &ctx->graph_kernels_c);
     }
-    if (ctx->gexec)
-        return MHD_OK;
     return capture(ctx, launch_step, &ctx->graph, &ctx->gexec, &ctx->graph_kernels);
 }
 
@@ -688,18 +781,18 @@ int run_steps(mhd_ctx *ctx, int nsteps)
     RUN(build_graph(ctx));
     for (int s = 0; s < nsteps; ++s)
     {
-        if (ctx->res.on)
+        if (ctx->gexec)
+        {
+            CK(ctx, cudaGraphLaunch(ctx->gexec, ctx->stream));
+            ctx->launches += ctx->graph_kernels;
+        }
+        else
         {
             CK(ctx, cudaGraphLaunch(ctx->gexec_a, ctx->stream));
             ctx->launches += ctx->graph_kernels_a;
             RUN(launch_resistive(ctx));
             CK(ctx, cudaGraphLaunch(ctx->gexec_c, ctx->stream));
             ctx->launches += ctx->graph_kernels_c;
-        }
-        else
-        {
-            CK(ctx, cudaGraphLaunch(ctx->gexec, ctx->stream));
-            ctx->launches += ctx->graph_kernels;
         }
     }
     return MHD_OK;
@@ -754,7 +847,6 @@ int mhd_ctx_create(const mhd_block_desc *blocks, int32_t nblocks, const mhd_para
         }
     }
     ctx->pool_n = off;
-    int rc = MHD_OK;
     auto bail = [&](int code) {
         mhd_ctx_destroy(ctx);
         return code;
@@ -790,7 +882,6 @@ int mhd_ctx_create(const mhd_block_desc *blocks, int32_t nblocks, const mhd_para
         return bail(MHD_ECUDA);
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
         return bail(MHD_ECUDA);
-    (void)rc;
     *out = ctx;
     return MHD_OK;
 }
@@ -808,6 +899,10 @@ int mhd_ctx_destroy(mhd_ctx *ctx)
         cudaFree(kv.second.cdst);
         cudaFree(kv.second.cval);
     }
+    free_resistive(ctx);
+    for (auto &sp : ctx->spare)
+        if (sp)
+            cudaStreamDestroy(sp);
     if (ctx->dt_key)
         cudaFree(ctx->dt_key);
     cudaFree(ctx->staging);
@@ -942,6 +1037,230 @@ static int64_t pool_offset(const mhd_ctx *ctx, int64_t id)
     return int64_t(ctx->base[size_t(f)][size_t(b)]) + int64_t(m) * v.vol + pidx(v, i, j, k);
 }
 
+} // extern "C"
+
+template <typename T> static int upload_vec(mhd_ctx *ctx, const std::vector<T> &v, T **d)
+{
+    *d = nullptr;
+    if (v.empty())
+        return MHD_OK;
+    CK(ctx, cudaMalloc(d, v.size() * sizeof(T)));
+    CK(ctx, cudaMemcpy(*d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return MHD_OK;
+}
+
+static void free_map(SyncMap &m)
+{
+    cudaFree(m.dst);
+    cudaFree(m.src);
+    cudaFree(m.tmp);
+    cudaFree(m.cdst);
+    cudaFree(m.cval);
+    m = SyncMap();
+}
+
+static void free_resistive(mhd_ctx *ctx)
+{
+    auto &R = ctx->res;
+    for (void *p : {(void *)R.e, (void *)R.dj, (void *)R.j, (void *)R.eta, (void *)R.alias_e, (void *)R.owner_e,
+                    (void *)R.sign, (void *)R.rng_face, (void *)R.rng_edge, (void *)R.V, (void *)R.w, (void *)R.x,
+                    (void *)R.b, (void *)R.r, (void *)R.partial, (void *)R.dots, (void *)R.st})
+        cudaFree(p);
+    free_map(R.eres1form);
+    free_map(R.db);
+    const bool loops = R.graph_loops;
+    R = mhd_ctx::Resistive();
+    R.graph_loops = loops;
+}
+
+// pool offset -> (block, i, j, k) of the point (component dropped)
+struct PoolDecoder
+{
+    std::vector<std::pair<uint64_t, int>> starts; // (base offset, field * nblocks + block), sorted
+    const mhd_ctx *ctx;
+    explicit PoolDecoder(const mhd_ctx *c) : ctx(c)
+    {
+        for (int f = 0; f < NFIELD; ++f)
+            for (int b = 0; b < c->nblocks; ++b)
+                starts.push_back({uint64_t(c->base[size_t(f)][size_t(b)]), f * c->nblocks + b});
+        std::sort(starts.begin(), starts.end());
+    }
+    bool operator()(uint64_t off, int &b, int &i, int &j, int &k) const
+    {
+        auto it = std::upper_bound(starts.begin(), starts.end(), std::make_pair(off, INT32_MAX));
+        if (it == starts.begin())
+            return false;
+        --it;
+        const int f = it->second / ctx->nblocks;
+        b = it->second % ctx->nblocks;
+        const BlockView &v = ctx->hbv[size_t(b)];
+        const uint64_t rel = off - it->first;
+        if (rel >= uint64_t(v.vol) * uint64_t(kFields[f].ncomp))
+            return false;
+        const int64_t p = int64_t(rel % uint64_t(v.vol));
+        k = int(p % v.NK) - v.G;
+        j = int((p / v.NK) % v.NJ) - v.G;
+        i = int(p / (int64_t(v.NK) * v.NJ)) - v.G;
+        return true;
+    }
+};
+
+struct IBox
+{
+    int lo[3] = {INT32_MAX, INT32_MAX, INT32_MAX};
+    int hi[3] = {INT32_MIN, INT32_MIN, INT32_MIN}; // exclusive
+    bool empty() const { return lo[0] >= hi[0]; }
+    void add(int i, int j, int k)
+    {
+        const int p[3] = {i, j, k};
+        for (int a = 0; a < 3; ++a)
+        {
+            lo[a] = std::min(lo[a], p[a]);
+            hi[a] = std::max(hi[a], p[a] + 1);
+        }
+    }
+    bool has(int i, int j, int k, int widen = 0) const
+    {
+        return !empty() && i >= lo[0] - widen && i < hi[0] + widen && j >= lo[1] - widen && j < hi[1] + widen &&
+               k >= lo[2] - widen && k < hi[2] + widen;
+    }
+};
+
+static int read_map(mhd_ctx *ctx, const char *group, std::vector<uint64_t> &d, std::vector<uint64_t> &s, bool &staged)
+{
+    d.clear();
+    s.clear();
+    staged = false;
+    auto it = ctx->syncs.find(group);
+    if (it == ctx->syncs.end() || it->second.n == 0)
+        return MHD_OK;
+    const SyncMap &m = it->second;
+    d.resize(size_t(m.n));
+    s.resize(size_t(m.n));
+    CK(ctx, cudaMemcpy(d.data(), m.dst, size_t(m.n) * 8, cudaMemcpyDeviceToHost));
+    CK(ctx, cudaMemcpy(s.data(), m.src, size_t(m.n) * 8, cudaMemcpyDeviceToHost));
+    staged = m.tmp != nullptr;
+    return MHD_OK;
+}
+
+// The region of the resistive operator.  Eres can be non-zero only at the
+// unknown and alias edges and at their images under the Eres1form copies
+// (closed point by point).  dB can be non-zero only on faces next to those
+// edges (their bounding box widened by one point) and at the images of those
+// faces under the dB copies.  The region of block b is the bounding box of
+// all these points widened by one more point for the curl-adjoint stencil.
+// Builds the per (block, axis) face and edge sub-ranges and the copy lists
+// restricted to destinations inside the region.
+static int resistive_region(mhd_ctx *ctx, const std::vector<uint64_t> &seed)
+{
+    auto &R = ctx->res;
+    const int nb = ctx->nblocks;
+    const PoolDecoder dec(ctx);
+    std::vector<uint64_t> md[2], ms[2];
+    bool staged[2];
+    RUN(read_map(ctx, "Eres1form", md[0], ms[0], staged[0]));
+    RUN(read_map(ctx, "dB", md[1], ms[1], staged[1]));
+    int b, i, j, k;
+    // Eres: exact closure of the seed under the Eres1form copies
+    std::unordered_set<uint64_t> enz(seed.begin(), seed.end());
+    for (int iter = 0; iter < 64; ++iter)
+    {
+        bool changed = false;
+        for (size_t t = 0; t < md[0].size(); ++t)
+            if (enz.count(ms[0][t]) && enz.insert(md[0][t]).second)
+                changed = true;
+        if (!changed)
+            break;
+    }
+    std::vector<IBox> ebox(static_cast<size_t>(nb)), box(static_cast<size_t>(nb));
+    for (uint64_t off : enz)
+    {
+        if (!dec(off, b, i, j, k))
+            return fail(ctx, MHD_EINVAL, "resistive point outside the pool");
+        ebox[size_t(b)].add(i, j, k);
+        box[size_t(b)].add(i, j, k);
+    }
+    // dB: faces within one point of the Eres box, closed under the dB copies
+    std::unordered_set<uint64_t> fnz;
+    for (int iter = 0; iter < 64; ++iter)
+    {
+        bool changed = false;
+        for (size_t t = 0; t < md[1].size(); ++t)
+        {
+            const uint64_t src = ms[1][t];
+            const bool live = fnz.count(src) || (dec(src, b, i, j, k) && ebox[size_t(b)].has(i, j, k, 1));
+            if (live && fnz.insert(md[1][t]).second)
+                changed = true;
+        }
+        if (!changed)
+            break;
+    }
+    for (uint64_t off : fnz)
+        if (dec(off, b, i, j, k))
+            box[size_t(b)].add(i, j, k);
+    for (int q = 0; q < nb; ++q)
+    {
+        IBox &x = box[size_t(q)];
+        if (x.empty())
+            continue;
+        const BlockView &v = ctx->hbv[size_t(q)];
+        const int n[3] = {v.ni, v.nj, v.nk};
+        for (int a = 0; a < 3; ++a)
+        {
+            x.lo[a] = std::max(x.lo[a] - 2, -v.G);
+            x.hi[a] = std::min(x.hi[a] + 2, n[a] + 1 + v.G);
+        }
+    }
+    // sub-ranges of the inner faces / edges inside the region
+    std::vector<int> rf(size_t(nb) * 18, 0), re(size_t(nb) * 18, 0);
+    R.nface_max = R.nedge_max = 0;
+    for (int q = 0; q < nb; ++q)
+    {
+        const BlockView &v = ctx->hbv[size_t(q)];
+        const int n[3] = {v.ni, v.nj, v.nk};
+        for (int a = 0; a < 3; ++a)
+            for (int kind = 0; kind < 2; ++kind)
+            {
+                int plus[3];
+                loc_plus((kind == 0 ? LOC_FXI : LOC_EXI) + a, plus[0], plus[1], plus[2]);
+                int *r = (kind == 0 ? rf.data() : re.data()) + (q * 3 + a) * 6;
+                int64_t cnt = 1;
+                for (int d = 0; d < 3; ++d)
+                {
+                    const int lo = box[size_t(q)].empty() ? 0 : std::max(0, box[size_t(q)].lo[d]);
+                    const int hi = box[size_t(q)].empty() ? 0 : std::min(n[d] + plus[d], box[size_t(q)].hi[d]);
+                    r[d] = lo;
+                    r[3 + d] = std::max(0, hi - lo);
+                    cnt *= r[3 + d];
+                }
+                int64_t &mx = (kind == 0) ? R.nface_max : R.nedge_max;
+                mx = std::max(mx, cnt);
+            }
+    }
+    RUN(upload_vec(ctx, rf, &R.rng_face));
+    RUN(upload_vec(ctx, re, &R.rng_edge));
+    // copies with a destination inside the region
+    SyncMap *out[2] = {&R.eres1form, &R.db};
+    for (int q = 0; q < 2; ++q)
+    {
+        std::vector<uint64_t> d, s2;
+        for (size_t t = 0; t < md[q].size(); ++t)
+            if (dec(md[q][t], b, i, j, k) && box[size_t(b)].has(i, j, k))
+            {
+                d.push_back(md[q][t]);
+                s2.push_back(ms[q][t]);
+            }
+        RUN(upload_vec(ctx, d, &out[q]->dst));
+        RUN(upload_vec(ctx, s2, &out[q]->src));
+        out[q]->n = int64_t(d.size());
+        if (staged[q] && !d.empty())
+            CK(ctx, cudaMalloc(&out[q]->tmp, d.size() * 8));
+    }
+    return MHD_OK;
+}
+
+extern "C" {
+
 int mhd_set_sync_map(mhd_ctx *ctx, const char *group, const int64_t *dst, const int64_t *src, int64_t n)
 {
     if (!ctx || !group || n < 0 || (n > 0 && (!dst || !src)))
@@ -978,6 +1297,16 @@ int mhd_set_sync_map(mhd_ctx *ctx, const char *group, const int64_t *dst, const 
     if (staged)
         CK(ctx, cudaMalloc(&m.tmp, size_t(n) * 8));
     m.n = n;
+    // the resistive operator's region depends on these two groups
+    if (ctx->res.on && (std::strcmp(group, "Eres1form") == 0 || std::strcmp(group, "dB") == 0))
+    {
+        free_map(ctx->res.eres1form);
+        free_map(ctx->res.db);
+        cudaFree(ctx->res.rng_face);
+        cudaFree(ctx->res.rng_edge);
+        ctx->res.rng_face = ctx->res.rng_edge = nullptr;
+        RUN(resistive_region(ctx, ctx->res.seed));
+    }
     return MHD_OK;
 }
 
@@ -1027,27 +1356,19 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
         return fail(ctx, MHD_EINVAL, "bad resistive arguments");
     if (restart <= 0 || restart > kMaxRestart)
         return fail(ctx, MHD_EINVAL, "GMRES restart must be in [1, %d]", kMaxRestart);
+    if (maxit < 0)
+        return fail(ctx, MHD_EINVAL, "negative iteration limit");
     auto &R = ctx->res;
-    for (auto **p : {&R.e, &R.dj, &R.j, &R.alias_e, &R.owner_e, &R.alias_dj, &R.owner_dj})
-    {
-        cudaFree(*p);
-        *p = nullptr;
-    }
-    for (auto **p : {&R.eta, &R.sign, &R.V, &R.w, &R.x, &R.b, &R.r, &R.partial, &R.dots})
-    {
-        cudaFree(*p);
-        *p = nullptr;
-    }
-    cudaFree(R.st);
-    R.st = nullptr;
-    // Eres point ids -> offsets in Eres, dJ and J (same locations, same boxes)
+    free_resistive(ctx);
+    drop_graph(ctx);
+    // Eres point ids -> pool offsets in Eres, dJ and J (same locations, same boxes)
     auto remap = [&](const int64_t *ids, int64_t cnt, int to0, std::vector<uint64_t> &out) -> int {
         out.resize(size_t(cnt));
         for (int64_t t = 0; t < cnt; ++t)
         {
             const int f = int(ids[t] >> 56);
             if (f < F_Eresxi || f > F_Eresxi + 2)
-                return fail(ctx, MHD_EINVAL, "resistive unknown %lld is not an Eres point", (long long)t);
+                return fail(ctx, MHD_EINVAL, "resistive point %lld is not an Eres point", (long long)t);
             const int64_t id = (int64_t(to0 + (f - F_Eresxi)) << 56) | (ids[t] & ((int64_t(1) << 56) - 1));
             const int64_t o = pool_offset(ctx, id);
             if (o < 0)
@@ -1056,44 +1377,50 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
         }
         return MHD_OK;
     };
-    auto upload_u64 = [&](const std::vector<uint64_t> &v, uint64_t **d) -> int {
-        if (v.empty())
-            return MHD_OK;
-        CK(ctx, cudaMalloc(d, v.size() * 8));
-        CK(ctx, cudaMemcpy(*d, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
-        return MHD_OK;
-    };
-    std::vector<uint64_t> he, hdj, hj, ae, oe, adj, odj;
+    std::vector<uint64_t> he, hdj, hj, ae, oe;
     RUN(remap(unknowns, n, F_Eresxi, he));
     RUN(remap(unknowns, n, F_dJxi, hdj));
     RUN(remap(unknowns, n, F_Jxi, hj));
     RUN(remap(alias, nalias, F_Eresxi, ae));
     RUN(remap(owner, nalias, F_Eresxi, oe));
-    RUN(remap(alias, nalias, F_dJxi, adj));
-    RUN(remap(owner, nalias, F_dJxi, odj));
-    RUN(upload_u64(he, &R.e));
-    RUN(upload_u64(hdj, &R.dj));
-    RUN(upload_u64(hj, &R.j));
-    RUN(upload_u64(ae, &R.alias_e));
-    RUN(upload_u64(oe, &R.owner_e));
-    RUN(upload_u64(adj, &R.alias_dj));
-    RUN(upload_u64(odj, &R.owner_dj));
+    // only aliases of unknown owners can be non-zero
+    std::vector<uint64_t> sorted_e(he);
+    std::sort(sorted_e.begin(), sorted_e.end());
+    std::vector<uint64_t> fa, fo;
+    std::vector<double> fs;
+    for (int64_t t = 0; t < nalias; ++t)
+        if (std::binary_search(sorted_e.begin(), sorted_e.end(), oe[size_t(t)]))
+        {
+            fa.push_back(ae[size_t(t)]);
+            fo.push_back(oe[size_t(t)]);
+            fs.push_back(sign[t]);
+        }
+    RUN(upload_vec(ctx, he, &R.e));
+    RUN(upload_vec(ctx, hdj, &R.dj));
+    RUN(upload_vec(ctx, hj, &R.j));
+    RUN(upload_vec(ctx, fa, &R.alias_e));
+    RUN(upload_vec(ctx, fo, &R.owner_e));
+    RUN(upload_vec(ctx, fs, &R.sign));
+    std::vector<double> heta(eta, eta + n);
+    RUN(upload_vec(ctx, heta, &R.eta));
     R.n = n;
-    R.nalias = nalias;
-    const size_t nn = size_t(n > 0 ? n : 1);
-    CK(ctx, cudaMalloc(&R.eta, nn * 8));
-    if (n > 0)
-        CK(ctx, cudaMemcpy(R.eta, eta, size_t(n) * 8, cudaMemcpyHostToDevice));
-    if (nalias > 0)
-    {
-        CK(ctx, cudaMalloc(&R.sign, size_t(nalias) * 8));
-        CK(ctx, cudaMemcpy(R.sign, sign, size_t(nalias) * 8, cudaMemcpyHostToDevice));
-    }
+    R.nalias = int64_t(fa.size());
+    // the operator's active region
+    R.seed = he;
+    R.seed.insert(R.seed.end(), fa.begin(), fa.end());
+    RUN(resistive_region(ctx, R.seed));
+    // every point of the solve's fields starts at zero
+    for (int f0 : {int(F_Eresxi), int(F_dBxi), int(F_dJxi), int(F_RBresxi)})
+        for (int f = f0; f < f0 + 3; ++f)
+            for (int b = 0; b < ctx->nblocks; ++b)
+                CK(ctx, cudaMemset(ctx->pool + ctx->base[size_t(f)][size_t(b)], 0,
+                                   size_t(ctx->hbv[size_t(b)].vol) * 8 * size_t(kFields[f].ncomp)));
     R.restart = restart;
     R.rtol = rtol;
     R.atol = atol;
     R.maxit = maxit;
     R.ngroups = int(std::min<int64_t>(std::max<int64_t>((n + 255) / 256, 1), 592));
+    const size_t nn = size_t(n > 0 ? n : 1);
     CK(ctx, cudaMalloc(&R.V, nn * size_t(restart + 1) * 8));
     CK(ctx, cudaMalloc(&R.w, nn * 8));
     CK(ctx, cudaMalloc(&R.x, nn * 8));
@@ -1103,8 +1430,13 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
     CK(ctx, cudaMalloc(&R.dots, 64 * 8));
     CK(ctx, cudaMalloc(&R.st, sizeof(GmresState)));
     CK(ctx, cudaMemset(R.x, 0, nn * 8));
+    CK(ctx, cudaMemset(R.st, 0, sizeof(GmresState)));
+    R.its_eager = R.cycles_eager = 0;
+    R.k_cycle = R.k_inner = 0;
+    for (auto &sp : ctx->spare)
+        if (!sp)
+            CK(ctx, cudaStreamCreateWithFlags(&sp, cudaStreamNonBlocking));
     R.on = true;
-    drop_graph(ctx);
     return MHD_OK;
 }
 
@@ -1112,14 +1444,22 @@ int mhd_resistive_stats(const mhd_ctx *ctx, int32_t *its, double *rnorm, double 
 {
     if (!ctx)
         return MHD_EINVAL;
+    GmresState h;
+    std::memset(&h, 0, sizeof(h));
+    if (ctx->res.st)
+    {
+        if (cudaMemcpyAsync(&h, ctx->res.st, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+            cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+            return MHD_ECUDA;
+    }
     if (its)
-        *its = ctx->res.its;
+        *its = h.its;
     if (rnorm)
-        *rnorm = ctx->res.rnorm;
+        *rnorm = h.resid;
     if (bnorm)
-        *bnorm = ctx->res.bnorm;
+        *bnorm = h.bnorm;
     if (reason)
-        *reason = ctx->res.reason;
+        *reason = h.reason;
     return MHD_OK;
 }
 
@@ -1251,7 +1591,7 @@ int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
                 nf = max_box(ctx, l, 0) > nf ? max_box(ctx, l, 0) : nf;
             prof_begin(ctx, "k_curl_e2f");
             k_curl_e2f<<<dim3(grid_for(nf), ctx->nblocks, 3), kThreads, 0, ctx->stream>>>(ctx->dbv, F_Exi, -1, F_Bxi,
-                                                                                         -1.0, ctx->dt, 1.0, 0);
+                                                                                         -1.0, ctx->dt, 1.0, 0, nullptr);
             RUN(launched(ctx));
         }
         break;
@@ -1290,7 +1630,22 @@ int mhd_set_time(mhd_ctx *ctx, double dt, double time, int64_t step)
     return MHD_OK;
 }
 
-int64_t mhd_kernel_launches(const mhd_ctx *ctx) { return ctx ? ctx->launches : -1; }
+int64_t mhd_kernel_launches(const mhd_ctx *ctx)
+{
+    if (!ctx)
+        return -1;
+    int64_t n = ctx->launches;
+    const auto &R = ctx->res;
+    if (R.st && (R.k_cycle > 0 || R.k_inner > 0))
+    {
+        // passes of the graph-resident Krylov loops, counted on the device
+        GmresState h;
+        if (cudaMemcpyAsync(&h, R.st, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream) == cudaSuccess &&
+            cudaStreamSynchronize(ctx->stream) == cudaSuccess)
+            n += R.k_cycle * (h.total_cycles - R.cycles_eager) + R.k_inner * (h.total_its - R.its_eager);
+    }
+    return n;
+}
 
 int mhd_field_spec(int32_t index, const char **name, int32_t *loc, int32_t *ncomp, int32_t *nghost)
 {

@@ -20,13 +20,15 @@ struct Consts
 };
 
 __global__ void k_fluid_rhs(const BlockView *bvs, Consts c, int64_t maxpts);
+__global__ void k_ucontra(const BlockView *bvs);
 __global__ void k_eface(const BlockView *bvs);
 __global__ void k_eedge(const BlockView *bvs, int G);
+// rng (may be null): per (block, axis) sub-range lo[3], n[3] of the inner faces / edges to process
 __global__ void k_curl_e2f(const BlockView *bvs, int fE0, int fR0, int fB0, double mult, const double *dtp,
-                           double dtdiv, int mult_is_neg_dt);
+                           double dtdiv, int mult_is_neg_dt, const int *rng);
 __global__ void k_update_u(const BlockView *bvs, const double *dtp);
 __global__ void k_bcell(const BlockView *bvs);
-__global__ void k_jedge(const BlockView *bvs, int fB0, int fJ0, double mult);
+__global__ void k_jedge(const BlockView *bvs, int fB0, int fJ0, double mult, const int *rng);
 __global__ void k_jcell(const BlockView *bvs);
 __global__ void k_pv_uplus_dt(const BlockView *bvs, Consts c, unsigned long long *dt_key);
 __global__ void k_begin_step(const unsigned long long *dt_key, double *dt, int *err, double dt_abort);
@@ -42,8 +44,10 @@ __global__ void k_aos_to_soa(const BlockView *bvs, int blk, int fid, int ncomp, 
 __global__ void k_soa_to_aos(const BlockView *bvs, int blk, int fid, int ncomp, int lo0, int lo1, int lo2, int n0,
                              int n1, int n2, double *aos);
 
-// Krylov (mhd_krylov.cu).  GMRES scalar state kept on the device; restart
-// length at most kMaxRestart.
+// Krylov (mhd_krylov.cu).  GMRES state kept on the device, including the
+// loop control, so that a whole solve runs inside one CUDA graph (conditional
+// while nodes) or, eagerly, with the host reading the two loop flags.
+// Restart length at most kMaxRestart.
 constexpr int kMaxRestart = 30;
 struct GmresState
 {
@@ -54,19 +58,39 @@ struct GmresState
     double beta;     // initial residual norm of the cycle
     double y[31];
     int breakdown;
+    // control
+    int j;                  // columns built in the current cycle
+    int its;                // iterations of the current solve
+    int m, maxit;           // restart length, iteration limit
+    double ttol, atol;      // max(rtol ||b||, atol), atol
+    double bnorm;
+    int reason;             // 0 running, 2 rtol, 3 atol, -3 iteration limit
+    int inner, outer;       // loop conditions (mirrors of the graph conditionals)
+    long long total_its;    // cumulative over all solves
+    long long total_cycles; // cumulative over all solves
 };
+// dot products: partial[c * gridDim.x + cta] for c < nvec (nvec = *jdev + 1 when jdev is given);
+// V == nullptr computes w . w
 __global__ void k_dots_partial(const double *V, int64_t ldv, int nvec, const double *w, int64_t n, double *partial,
-                               int with_norm);
-__global__ void k_dots_final(const double *partial, int ngroups, int nout, double *out, int accumulate);
-__global__ void k_sub_proj(const double *V, int64_t ldv, int nvec, const double *h, double *w, int64_t n);
-__global__ void k_div_dev(double *y, const double *x, const double *a, int64_t n);
-__global__ void k_add_small(double *a, const double *b, int n);
-__global__ void k_gmres_column(GmresState *st, int j, const double *wnorm2);
-__global__ void k_gmres_start(GmresState *st, const double *beta2);
-__global__ void k_gmres_solve_y(GmresState *st, int m);
-__global__ void k_add_basis(const double *V, int64_t ldv, const GmresState *st, int m, double *x, int64_t n);
+                               const int *jdev);
+__global__ void k_dots_final(const double *partial, int ngroups, int nout, double *out, const int *jdev);
+__global__ void k_sub_proj(const double *V, int64_t ldv, int nvec, const double *h, double *w, int64_t n,
+                           const int *jdev);
+__global__ void k_add_small(double *a, const double *b, const int *jdev);
+__global__ void k_div_guard(double *y, const double *x, const double *a, int64_t n, const int *guard);
+__global__ void k_div_next(double *V, int64_t ldv, const double *w, const GmresState *st, int64_t n);
+__global__ void k_gmres_init(GmresState *st, const double *b2, double rtol, double atol, int maxit, int m);
+__global__ void k_cycle_start(GmresState *st, const double *beta2, cudaGraphConditionalHandle h, int use_handle);
+__global__ void k_gmres_column(GmresState *st, const double *wnorm2);
+__global__ void k_inner_check(GmresState *st, cudaGraphConditionalHandle h, int use_handle);
+__global__ void k_gmres_solve_y(GmresState *st);
+__global__ void k_add_basis(const double *V, int64_t ldv, const GmresState *st, double *x, int64_t n);
+__global__ void k_outer_check(GmresState *st, cudaGraphConditionalHandle h, int use_handle);
+__global__ void k_zero(double *x, int64_t n);
 __global__ void k_residual(const double *b, const double *y, double *r, int64_t n);
-__global__ void k_scatter_vec(double *pool, const uint64_t *dst, const double *x, int64_t n);
+// pool[dst[t]] = x[t] with x = x0 + (*jdev) * ldx when jdev is given
+__global__ void k_scatter_vec(double *pool, const uint64_t *dst, const double *x0, int64_t ldx, const int *jdev,
+                              int64_t n);
 __global__ void k_resist_out(const double *pool, const uint64_t *e, const uint64_t *dj, const double *eta, double *y,
                              int64_t n);
 __global__ void k_resist_rhs(const double *pool, const uint64_t *j, const double *eta, double *b, int64_t n);

@@ -48,6 +48,24 @@ __device__ __forceinline__ void loc_box(const BlockView &b, int loc, int g, int 
     n[2] = b.nk + pk + 2 * g;
 }
 
+// Inner range of a location, or the sub-range rng[6 * q .. 6 * q + 5]
+// (lo[3], n[3]) when a restricted range table is given.
+__device__ __forceinline__ void sub_range(const BlockView &b, int loc, const int *rng, int q, int lo[3], int n[3])
+{
+    if (rng)
+    {
+        const int *r = rng + 6 * q;
+        lo[0] = r[0];
+        lo[1] = r[1];
+        lo[2] = r[2];
+        n[0] = r[3];
+        n[1] = r[4];
+        n[2] = r[5];
+    }
+    else
+        loc_box(b, loc, 0, lo, n);
+}
+
 // ---------------------------------------------------------------------------
 // Scheme_U_ + AddSourceToRHS_Fluid
 // (Z4_Lunar/src/physics/LunarSolver_FluidRHS.cpp:3-201, :528-568)
@@ -188,7 +206,8 @@ __device__ __forceinline__ double face_tot(const BlockView &b, int axis, int i, 
     const int64_t p = pidx(b, i, j, k);
     return b.f[F][p] + b.f[A][p];
 }
-// contravariant velocity of a cell along `axis` (cell_u_contra)
+// contravariant velocity of a cell along `axis` (cell_u_contra,
+// LunarSolver_MagExplicit_Ideal.cpp:95-115)
 __device__ __forceinline__ double u_contra(const BlockView &b, int axis, int i, int j, int k)
 {
     const int JD = (axis == 0) ? F_JDxi : (axis == 1) ? F_JDeta : F_JDzeta;
@@ -204,6 +223,29 @@ __device__ __forceinline__ double u_contra(const BlockView &b, int axis, int i, 
     return (kx * Up[p] + ky * Up[v + p] + kz * Up[2 * v + p]) * inv_jac;
 }
 
+// the three contravariant velocities of every cell within one layer of the
+// inner range, stored once per step instead of being recomputed by every
+// face and edge stencil that needs them (up to eight times per point)
+__global__ void k_ucontra(const BlockView *__restrict__ bvs)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    int lo[3], n[3];
+    loc_box(b, LOC_CELL, 1, lo, n);
+    int i, j, k;
+    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+        return;
+    const int64_t p = pidx(b, i, j, k);
+    double *UC = b.f[F_UC];
+    UC[p] = u_contra(b, 0, i, j, k);
+    UC[b.vol + p] = u_contra(b, 1, i, j, k);
+    UC[2 * b.vol + p] = u_contra(b, 2, i, j, k);
+}
+
+__device__ __forceinline__ double uc(const BlockView &b, int axis, int i, int j, int k)
+{
+    return b.f[F_UC][axis * b.vol + pidx(b, i, j, k)];
+}
+
 __device__ __forceinline__ double emf_flux(const BlockView &b, int ba, int fa, int iL, int jL, int kL, int iR, int jR,
                                            int kR, double bff)
 {
@@ -212,10 +254,10 @@ __device__ __forceinline__ double emf_flux(const BlockView &b, int ba, int fa, i
     const double btR = 0.5 * (face_tot(b, ba, iR, jR, kR) + face_tot(b, ba, iR + sa, jR + sb, kR + sc));
     const double biL = 0.5 * (face_ind(b, ba, iL, jL, kL) + face_ind(b, ba, iL + sa, jL + sb, kL + sc));
     const double biR = 0.5 * (face_ind(b, ba, iR, jR, kR) + face_ind(b, ba, iR + sa, jR + sb, kR + sc));
-    const double ufL = u_contra(b, fa, iL, jL, kL);
-    const double ufR = u_contra(b, fa, iR, jR, kR);
-    const double ubL = u_contra(b, ba, iL, jL, kL);
-    const double ubR = u_contra(b, ba, iR, jR, kR);
+    const double ufL = uc(b, fa, iL, jL, kL);
+    const double ufR = uc(b, fa, iR, jR, kR);
+    const double ubL = uc(b, ba, iL, jL, kL);
+    const double ubR = uc(b, ba, iR, jR, kR);
     const double GL = ufL * btL - ubL * bff;
     const double GR = ufR * btR - ubR * bff;
     const double radius = smax(fabs(ufL), fabs(ufR));
@@ -272,10 +314,10 @@ __device__ __forceinline__ double max_abs_u4(const BlockView &b, int axis, int i
                                              int k1, int i2, int j2, int k2, int i3, int j3, int k3)
 {
     double a = 0.0;
-    a = smax(a, fabs(u_contra(b, axis, i0, j0, k0)));
-    a = smax(a, fabs(u_contra(b, axis, i1, j1, k1)));
-    a = smax(a, fabs(u_contra(b, axis, i2, j2, k2)));
-    a = smax(a, fabs(u_contra(b, axis, i3, j3, k3)));
+    a = smax(a, fabs(uc(b, axis, i0, j0, k0)));
+    a = smax(a, fabs(uc(b, axis, i1, j1, k1)));
+    a = smax(a, fabs(uc(b, axis, i2, j2, k2)));
+    a = smax(a, fabs(uc(b, axis, i3, j3, k3)));
     return a;
 }
 
@@ -345,14 +387,14 @@ __global__ void k_eedge(const BlockView *__restrict__ bvs, int G)
 // blockIdx.z = face axis.
 // ---------------------------------------------------------------------------
 __global__ void k_curl_e2f(const BlockView *__restrict__ bvs, int fE0, int fR0, int fB0, double mult,
-                           const double *__restrict__ dtp, double dtdiv, int mult_is_neg_dt)
+                           const double *__restrict__ dtp, double dtdiv, int mult_is_neg_dt, const int *__restrict__ rng)
 {
     if (mult_is_neg_dt)
         mult = -dtp[0];
     const BlockView &b = bvs[blockIdx.y];
     const int fa = blockIdx.z;
     int lo[3], n[3];
-    loc_box(b, LOC_FXI + fa, 0, lo, n);
+    sub_range(b, LOC_FXI + fa, rng, blockIdx.y * 3 + fa, lo, n);
     int i, j, k;
     if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
         return;
@@ -439,12 +481,12 @@ __global__ void k_bcell(const BlockView *__restrict__ bvs)
 // the face Hodge scale beta, times the edge scale alpha
 // (LunarSolver_Tools.cpp:777-835).  blockIdx.z = edge axis.
 // ---------------------------------------------------------------------------
-__global__ void k_jedge(const BlockView *__restrict__ bvs, int fB0, int fJ0, double mult)
+__global__ void k_jedge(const BlockView *__restrict__ bvs, int fB0, int fJ0, double mult, const int *__restrict__ rng)
 {
     const BlockView &b = bvs[blockIdx.y];
     const int ea = blockIdx.z;
     int lo[3], n[3];
-    loc_box(b, LOC_EXI + ea, 0, lo, n);
+    sub_range(b, LOC_EXI + ea, rng, blockIdx.y * 3 + ea, lo, n);
     int i, j, k;
     if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
         return;
@@ -550,10 +592,8 @@ __global__ void k_pv_uplus_dt(const BlockView *__restrict__ bvs, Consts c, unsig
     loc_box(b, LOC_CELL, b.G, lo, n);
     int i, j, k;
     double dtc = 1e100;
-    bool any = false;
     if (box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
     {
-        any = true;
         const int64_t p = pidx(b, i, j, k);
         const int64_t v = b.vol;
         const double *U = b.f[F_U];
@@ -616,7 +656,6 @@ __global__ void k_pv_uplus_dt(const BlockView *__restrict__ bvs, Consts c, unsig
             }
         }
     }
-    (void)any;
     if (!dt_key)
         return;
     // block-wide minimum of the order-preserving keys

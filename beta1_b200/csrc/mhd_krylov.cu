@@ -6,10 +6,16 @@
 // pass needs only one batched dot-product kernel, instead of one reduction
 // per basis vector with modified Gram-Schmidt.  All reductions are
 // two-stage (per-CTA partial sums, then a fixed-order final sum), so a solve
-// is bit-reproducible from run to run.  The Hessenberg matrix, the Givens
-// rotations and the residual estimate live in device memory and are updated
-// by a one-thread kernel; the host reads back one scalar per iteration to
-// decide whether to stop.
+// is bit-reproducible from run to run.
+//
+// The whole control state lives in device memory (GmresState): the
+// Hessenberg matrix, the Givens rotations, the residual estimate, the column
+// and iteration counters and the two loop conditions.  One-thread kernels
+// update it and, when the solve runs inside a CUDA graph, set the graph's
+// conditional handles (an inner while loop over Arnoldi steps, an outer one
+// over restart cycles), so a solve needs no host round trip.  Run eagerly,
+// the host reads the two loop flags instead.  Kernels that work on "column
+// j" read j from the state.
 #include "mhd_kernels.cuh"
 
 namespace mhd
@@ -17,14 +23,14 @@ namespace mhd
 
 constexpr int kRedThreads = 256;
 
-// partial[c * ngroups + blockIdx.x] = sum over this CTA's slice of V_c . w
-// for c in [0, nvec); the last "vector" slot nvec computes w . w when
-// with_norm is set.
 __global__ void k_dots_partial(const double *__restrict__ V, int64_t ldv, int nvec, const double *__restrict__ w,
-                               int64_t n, double *__restrict__ partial, int with_norm)
+                               int64_t n, double *__restrict__ partial, const int *__restrict__ jdev)
 {
     const int c = blockIdx.y;
-    const double *v = (c < nvec) ? V + int64_t(c) * ldv : w;
+    const int nv = jdev ? jdev[0] + 1 : nvec;
+    if (c >= nv)
+        return;
+    const double *v = V ? V + int64_t(c) * ldv : w;
     double s = 0.0;
     for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x)
         s += v[t] * w[t];
@@ -39,57 +45,116 @@ __global__ void k_dots_partial(const double *__restrict__ V, int64_t ldv, int nv
     }
     if (threadIdx.x == 0)
         partial[int64_t(c) * gridDim.x + blockIdx.x] = red[0];
-    (void)with_norm;
 }
 
-// out[c] = sum_b partial[c * ngroups + b] (fixed order), optionally added to acc
+// out[c] = sum_b partial[c * ngroups + b] in a fixed order
 __global__ void k_dots_final(const double *__restrict__ partial, int ngroups, int nout, double *__restrict__ out,
-                             int accumulate)
+                             const int *__restrict__ jdev)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nout)
+    const int no = jdev ? jdev[0] + 1 : nout;
+    if (c >= no)
         return;
     double s = 0.0;
     for (int b = 0; b < ngroups; ++b)
         s += partial[int64_t(c) * ngroups + b];
-    out[c] = accumulate ? out[c] + s : s;
+    out[c] = s;
 }
 
 // w -= sum_c h[c] V_c
 __global__ void k_sub_proj(const double *__restrict__ V, int64_t ldv, int nvec, const double *__restrict__ h,
-                           double *__restrict__ w, int64_t n)
+                           double *__restrict__ w, int64_t n, const int *__restrict__ jdev)
 {
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= n)
         return;
+    const int nv = jdev ? jdev[0] + 1 : nvec;
     double s = w[t];
-    for (int c = 0; c < nvec; ++c)
+    for (int c = 0; c < nv; ++c)
         s -= h[c] * V[int64_t(c) * ldv + t];
     w[t] = s;
 }
 
-// a[c] += b[c] for c < n (small vectors)
-__global__ void k_add_small(double *__restrict__ a, const double *__restrict__ b, int n)
+// a[c] += b[c] for c <= j
+__global__ void k_add_small(double *__restrict__ a, const double *__restrict__ b, const int *__restrict__ jdev)
 {
     const int c = threadIdx.x;
-    if (c < n)
+    if (c <= jdev[0])
         a[c] += b[c];
 }
 
-// y = x / a   (a from device memory)
-__global__ void k_div_dev(double *__restrict__ y, const double *__restrict__ x, const double *__restrict__ a,
-                          int64_t n)
+// y = x / a[0] unless guard[0] == 0
+__global__ void k_div_guard(double *__restrict__ y, const double *__restrict__ x, const double *__restrict__ a,
+                            int64_t n, const int *__restrict__ guard)
 {
+    if (guard && guard[0] == 0)
+        return;
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t < n)
         y[t] = x[t] / a[0];
 }
 
+// V_{j+1} = w / ||w|| (skipped on breakdown)
+__global__ void k_div_next(double *__restrict__ V, int64_t ldv, const double *__restrict__ w,
+                           const GmresState *__restrict__ st, int64_t n)
+{
+    if (st->breakdown)
+        return;
+    const int j = st->j;
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        V[int64_t(j + 1) * ldv + t] = w[t] / st->hcol[j + 1];
+}
+
+// start of a solve: ||b||, the stopping threshold, counters
+__global__ void k_gmres_init(GmresState *st, const double *__restrict__ b2, double rtol, double atol, int maxit, int m)
+{
+    const double bnorm = sqrt(b2[0]);
+    st->bnorm = bnorm;
+    st->ttol = fmax(rtol * bnorm, atol);
+    st->atol = atol;
+    st->maxit = maxit;
+    st->m = m;
+    st->its = 0;
+    st->reason = 0;
+    st->j = 0;
+    st->inner = 0;
+    st->outer = 1;
+}
+
+// start of a cycle: beta = ||r||, g = beta e1; decides whether the cycle runs
+__global__ void k_cycle_start(GmresState *st, const double *__restrict__ beta2, cudaGraphConditionalHandle h,
+                              int use_handle)
+{
+    const double beta = sqrt(beta2[0]);
+    st->beta = beta;
+    for (int i = 0; i < 32; ++i)
+        st->g[i] = 0.0;
+    st->g[0] = beta;
+    st->resid = beta;
+    st->breakdown = 0;
+    st->j = 0;
+    int go = 1;
+    if (beta <= st->ttol)
+    {
+        st->reason = (beta <= st->atol) ? 3 : 2;
+        go = 0;
+    }
+    else if (st->its >= st->maxit)
+    {
+        st->reason = -3;
+        go = 0;
+    }
+    st->inner = go;
+    if (use_handle)
+        cudaGraphSetConditional(h, unsigned(go));
+}
 
 // new column j: hcol[j + 1] = ||w||, H[0..j+1, j] = hcol; apply the
 // previous rotations, form a new one, update g and the residual estimate
-__global__ void k_gmres_column(GmresState *st, int j, const double *__restrict__ wnorm2)
+__global__ void k_gmres_column(GmresState *st, const double *__restrict__ wnorm2)
 {
+    const int j = st->j;
     st->hcol[j + 1] = sqrt(wnorm2[0]);
     double *H = st->H;
     for (int i = 0; i <= j + 1; ++i)
@@ -112,21 +177,22 @@ __global__ void k_gmres_column(GmresState *st, int j, const double *__restrict__
     st->breakdown = (st->hcol[j + 1] == 0.0) ? 1 : 0;
 }
 
-// start of a cycle: beta = ||r||, g = beta e1
-__global__ void k_gmres_start(GmresState *st, const double *__restrict__ beta2)
+// end of an Arnoldi step: counters and the inner loop condition
+__global__ void k_inner_check(GmresState *st, cudaGraphConditionalHandle h, int use_handle)
 {
-    const double beta = sqrt(beta2[0]);
-    st->beta = beta;
-    for (int i = 0; i < 32; ++i)
-        st->g[i] = 0.0;
-    st->g[0] = beta;
-    st->resid = beta;
-    st->breakdown = 0;
+    st->its += 1;
+    st->total_its += 1;
+    st->j += 1;
+    const int go = !(st->resid <= st->ttol || st->breakdown || st->j >= st->m || st->its >= st->maxit);
+    st->inner = go;
+    if (use_handle)
+        cudaGraphSetConditional(h, unsigned(go));
 }
 
-// back substitution H y = g over the first m columns
-__global__ void k_gmres_solve_y(GmresState *st, int m)
+// back substitution H y = g over the cycle's j columns
+__global__ void k_gmres_solve_y(GmresState *st)
 {
+    const int m = st->j;
     for (int i = m - 1; i >= 0; --i)
     {
         double s = st->g[i];
@@ -136,17 +202,43 @@ __global__ void k_gmres_solve_y(GmresState *st, int m)
     }
 }
 
-// x += V y over m columns
-__global__ void k_add_basis(const double *__restrict__ V, int64_t ldv, const GmresState *st, int m,
+// x += V y over the cycle's j columns
+__global__ void k_add_basis(const double *__restrict__ V, int64_t ldv, const GmresState *__restrict__ st,
                             double *__restrict__ x, int64_t n)
 {
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= n)
         return;
+    const int m = st->j;
     double s = x[t];
     for (int c = 0; c < m; ++c)
         s += st->y[c] * V[int64_t(c) * ldv + t];
     x[t] = s;
+}
+
+// end of a cycle: converged (PETSc's default test), out of iterations, or restart
+__global__ void k_outer_check(GmresState *st, cudaGraphConditionalHandle h, int use_handle)
+{
+    st->total_cycles += 1;
+    int go = 0;
+    if (st->reason != 0)
+        go = 0;
+    else if (st->resid <= st->ttol || st->breakdown)
+        st->reason = (st->resid <= st->atol) ? 3 : 2;
+    else if (st->its >= st->maxit)
+        st->reason = -3;
+    else
+        go = 1;
+    st->outer = go;
+    if (use_handle)
+        cudaGraphSetConditional(h, unsigned(go));
+}
+
+__global__ void k_zero(double *__restrict__ x, int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        x[t] = 0.0;
 }
 
 // r = b - y
@@ -163,13 +255,15 @@ __global__ void k_residual(const double *__restrict__ b, const double *__restric
 // helpers, Z4_Lunar/src/implicit/Lunar_ImplicitResistive.cpp:264-427)
 // ---------------------------------------------------------------------------
 
-// pool[dst[t]] = x[t]   (UnpackVecToImplicitEres_ after clear_triplet)
+// pool[dst[t]] = x[t]   (UnpackVecToImplicitEres_)
 __global__ void k_scatter_vec(double *__restrict__ pool, const uint64_t *__restrict__ dst,
-                              const double *__restrict__ x, int64_t n)
+                              const double *__restrict__ x0, int64_t ldx, const int *__restrict__ jdev, int64_t n)
 {
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t < n)
-        pool[dst[t]] = x[t];
+    if (t >= n)
+        return;
+    const double *x = jdev ? x0 + int64_t(jdev[0]) * ldx : x0;
+    pool[dst[t]] = x[t];
 }
 
 // y[t] = pool[e[t]] - eta[t] * pool[dj[t]]   (end of MatMultImplicitResistive_)

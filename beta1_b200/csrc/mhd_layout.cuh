@@ -72,7 +72,8 @@ namespace mhd
     X(dJzeta, "dJ_zeta", 6, 1, 4)                          \
     X(etaxi, "eta_edge_xi", 4, 1, 0)                         \
     X(etaeta, "eta_edge_eta", 5, 1, 0)                     \
-    X(etazeta, "eta_edge_zeta", 6, 1, 0)
+    X(etazeta, "eta_edge_zeta", 6, 1, 0)                   \
+    X(UC, "U_contra_cell", 0, 3, 1)
 
 enum FieldId : int
 {
