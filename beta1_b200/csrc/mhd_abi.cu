@@ -45,18 +45,32 @@ int field_by_name(const char *name)
     return -1;
 }
 
-struct SyncMap
+// Device lists of one sync: fixed values (phase A) and composed copies (phase B).
+struct CopyList
 {
-    // phase A: constants and wall handlers
     uint64_t *cdst = nullptr;
     double *cval = nullptr;
     int64_t nconst = 0;
-    std::vector<std::pair<int, int>> walls; // (block, direction) of Solid_Surface fluid handlers
-    // phase B: composed copies
     uint64_t *dst = nullptr;
     uint64_t *src = nullptr;
     double *tmp = nullptr; // non-null when a source is also a destination
     int64_t n = 0;
+};
+
+// One sync group.  The full tables are what the reference's Sync writes.
+// The hot lists keep only the points a later kernel of the step reads (the
+// ghost layers within each field's stencil depth, and inner points); the
+// rest is written by the full lists when a field is read out (materialised),
+// which gives the same values because a composed copy's source does not
+// change between the sync and the read-out.
+struct SyncMap
+{
+    std::vector<uint64_t> hd, hs, hcd; // full tables (pool offsets) on the host
+    std::vector<double> hcv;
+    std::vector<std::pair<int, int>> walls; // (block, direction) of Solid_Surface fluid handlers
+    bool staged = false;
+    bool built = false; // device lists match the host tables
+    CopyList full, hot;
 };
 
 constexpr int kThreads = 256;
@@ -95,6 +109,11 @@ struct mhd_ctx
     long long *step = nullptr;
     int *err = nullptr;
     std::map<std::string, SyncMap> syncs;
+    // materialisation state: groups whose last sync ran its hot list only,
+    // and PV / U_plus computed on the first ghost layer only
+    std::map<std::string, bool> dirty;
+    bool pv_dirty = false;
+    std::vector<std::string> field_group = std::vector<std::string>(NFIELD); // group that syncs a field
     double *staging = nullptr;
     size_t staging_n = 0;
     int64_t launches = 0;
@@ -115,7 +134,7 @@ struct mhd_ctx
         double *sign = nullptr;
         // the operator's active region: copies with a destination inside it,
         // and per (block, axis) sub-ranges of the inner faces / edges
-        SyncMap eres1form, db;
+        CopyList eres1form, db;
         int *rng_face = nullptr, *rng_edge = nullptr;
         int64_t nface_max = 0, nedge_max = 0;
         double rtol = 1e-8, atol = 1e-12;
@@ -142,6 +161,13 @@ struct mhd_ctx
 
 static void free_resistive(mhd_ctx *ctx);
 static int resistive_region(mhd_ctx *ctx, const std::vector<uint64_t> &seed);
+static void free_list(CopyList &m);
+static int build_all_syncs(mhd_ctx *ctx);
+static int materialise_field(mhd_ctx *ctx, int f);
+static int materialise_group(mhd_ctx *ctx, const std::string &group);
+static int materialise_all(mhd_ctx *ctx);
+static void mark_dirty(mhd_ctx *ctx);
+int build_sync(mhd_ctx *ctx, const std::string &group, SyncMap &m);
 
 namespace
 {
@@ -255,7 +281,7 @@ int launched(mhd_ctx *ctx, int nk = 1)
 }
 
 // phase B of a sync: the composed copies
-int gather_map(mhd_ctx *ctx, const SyncMap &s)
+int gather_map(mhd_ctx *ctx, const CopyList &s)
 {
     if (s.n == 0)
         return MHD_OK;
@@ -273,19 +299,40 @@ int gather_map(mhd_ctx *ctx, const SyncMap &s)
     return launched(ctx);
 }
 
-int run_sync(mhd_ctx *ctx, const char *group)
+// fixed values then copies of a list (no wall handlers)
+int apply_list(mhd_ctx *ctx, const CopyList &l)
+{
+    if (l.nconst > 0)
+    {
+        prof_begin(ctx, "k_set_consts");
+        k_set_consts<<<grid_for(l.nconst), kThreads, 0, ctx->stream>>>(ctx->pool, l.cdst, l.cval, l.nconst);
+        RUN(launched(ctx));
+    }
+    return gather_map(ctx, l);
+}
+
+// LunarBoundary::Sync(group): phase A (fixed values, wall handlers), then
+// the composed copies; the hot lists unless `full`
+int run_sync(mhd_ctx *ctx, const char *group, bool full = false)
 {
     auto it = ctx->syncs.find(group);
     if (it == ctx->syncs.end())
         return MHD_OK;
-    SyncMap &s = it->second;
-    if (s.nconst > 0)
+    SyncMap &m = it->second;
+    if (!m.built)
+    {
+        if (ctx->capturing)
+            return fail(ctx, MHD_ESTATE, "sync group %s changed during capture", group);
+        RUN(build_sync(ctx, it->first, m));
+    }
+    const CopyList &l = full ? m.full : m.hot;
+    if (l.nconst > 0)
     {
         prof_begin(ctx, "k_set_consts");
-        k_set_consts<<<grid_for(s.nconst), kThreads, 0, ctx->stream>>>(ctx->pool, s.cdst, s.cval, s.nconst);
+        k_set_consts<<<grid_for(l.nconst), kThreads, 0, ctx->stream>>>(ctx->pool, l.cdst, l.cval, l.nconst);
         RUN(launched(ctx));
     }
-    for (const auto &w : s.walls)
+    for (const auto &w : m.walls)
     {
         const BlockView &v = ctx->hbv[size_t(w.first)];
         const int ax = std::abs(w.second) - 1;
@@ -294,7 +341,9 @@ int run_sync(mhd_ctx *ctx, const char *group)
         k_wall_u<<<grid_for(ncol), kThreads, 0, ctx->stream>>>(ctx->dbv, w.first, w.second, ctx->c.gamma);
         RUN(launched(ctx));
     }
-    return gather_map(ctx, s);
+    RUN(gather_map(ctx, l));
+    ctx->dirty[it->first] = !full && (m.hot.n != m.full.n || m.hot.nconst != m.full.nconst);
+    return MHD_OK;
 }
 
 int launch_update_derived(mhd_ctx *ctx)
@@ -321,9 +370,12 @@ int launch_update_derived(mhd_ctx *ctx)
     prof_begin(ctx, "k_arm_dt");
     k_arm_dt<<<1, 1, 0, s>>>(ctx->dt_key);
     RUN(launched(ctx));
-    const int64_t ng = max_box(ctx, LOC_CELL, ctx->G);
+    // first ghost layer only: deeper PV / U_plus ghosts are read by no kernel
+    // of the step and are filled when read out (materialise_pv)
+    const int64_t ng = max_box(ctx, LOC_CELL, 1);
     prof_begin(ctx, "k_pv_uplus_dt");
-    k_pv_uplus_dt<<<dim3(grid_for(ng), nb), kThreads, 0, s>>>(ctx->dbv, ctx->c, ctx->dt_key);
+    k_pv_uplus_dt<<<dim3(grid_for(ng), nb), kThreads, 0, s>>>(ctx->dbv, ctx->c, ctx->dt_key, 1);
+    ctx->pv_dirty = true;
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Uplus"));
     return MHD_OK;
@@ -351,11 +403,13 @@ int launch_induction(mhd_ctx *ctx, bool update_b)
     k_eface<<<dim3(grid_for(nf), nb, 3), kThreads, 0, s>>>(ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Eface"));
+    // inner edges; ghost edges keep their zero of AssembleRHS_Induction_CT_
+    // except where the Eedge sync writes them
     int64_t ne = 0;
     for (int l = LOC_EXI; l <= LOC_EZETA; ++l)
-        ne = max_box(ctx, l, ctx->G) > ne ? max_box(ctx, l, ctx->G) : ne;
+        ne = max_box(ctx, l, 0) > ne ? max_box(ctx, l, 0) : ne;
     prof_begin(ctx, "k_eedge");
-    k_eedge<<<dim3(grid_for(ne), nb, 3), kThreads, 0, s>>>(ctx->dbv, ctx->G);
+    k_eedge<<<dim3(grid_for(ne), nb, 3), kThreads, 0, s>>>(ctx->dbv, 0);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Eedge"));
     prof_begin(ctx, "k_curl_e2f");
@@ -425,7 +479,7 @@ int unpack_eres(mhd_ctx *ctx, const double *x0, const int *jdev)
                                                                         R.nalias);
         RUN(launched(ctx));
     }
-    return gather_map(ctx, R.eres1form);
+    return apply_list(ctx, R.eres1form);
 }
 
 // y = A x  (MatMultImplicitResistive_): dB = -dt curl Eres, Sync("dB"),
@@ -436,7 +490,7 @@ int resist_matvec(mhd_ctx *ctx, const double *x0, const int *jdev, double *y)
     auto &R = ctx->res;
     RUN(unpack_eres(ctx, x0, jdev));
     RUN(launch_curl_rng(ctx, F_Eresxi, F_dBxi, -1, 0.0, /*mult_is_neg_dt=*/1));
-    RUN(gather_map(ctx, R.db));
+    RUN(apply_list(ctx, R.db));
     RUN(launch_jedge_rng(ctx, F_dBxi, F_dJxi));
     prof_begin(ctx, "k_resist_out");
     k_resist_out<<<grid_for(R.n), kThreads, 0, ctx->stream>>>(ctx->pool, R.e, R.dj, R.eta, y, R.n);
@@ -754,6 +808,7 @@ int build_graph(mhd_ctx *ctx)
 {
     if (ctx->gexec || ctx->gexec_a)
         return MHD_OK;
+    RUN(build_all_syncs(ctx));
     if (ctx->res.on && ctx->res.graph_loops)
     {
         const int rc = capture(ctx, launch_step, &ctx->graph, &ctx->gexec, &ctx->graph_kernels);
@@ -795,6 +850,8 @@ int run_steps(mhd_ctx *ctx, int nsteps)
             ctx->launches += ctx->graph_kernels_c;
         }
     }
+    if (nsteps > 0)
+        mark_dirty(ctx);
     return MHD_OK;
 }
 
@@ -893,11 +950,8 @@ int mhd_ctx_destroy(mhd_ctx *ctx)
     drop_graph(ctx);
     for (auto &kv : ctx->syncs)
     {
-        cudaFree(kv.second.dst);
-        cudaFree(kv.second.src);
-        cudaFree(kv.second.tmp);
-        cudaFree(kv.second.cdst);
-        cudaFree(kv.second.cval);
+        free_list(kv.second.full);
+        free_list(kv.second.hot);
     }
     free_resistive(ctx);
     for (auto &sp : ctx->spare)
@@ -985,15 +1039,20 @@ static int transfer(mhd_ctx *ctx, const char *name, int32_t block, const double 
 
 int mhd_upload_field(mhd_ctx *ctx, const char *name, int32_t block, const double *data, int64_t count)
 {
-    if (!data)
+    if (!ctx || !data)
         return fail(ctx, MHD_EINVAL, "null data");
+    // every field the device holds is brought to the reference's state first
+    RUN(materialise_all(ctx));
     return transfer(ctx, name, block, data, nullptr, count);
 }
 
 int mhd_download_field(mhd_ctx *ctx, const char *name, int32_t block, double *data, int64_t count)
 {
-    if (!data)
+    if (!ctx || !data)
         return fail(ctx, MHD_EINVAL, "null data");
+    const int f = field_by_name(name);
+    if (f >= 0)
+        RUN(materialise_field(ctx, f));
     return transfer(ctx, name, block, nullptr, data, count);
 }
 
@@ -1049,14 +1108,14 @@ template <typename T> static int upload_vec(mhd_ctx *ctx, const std::vector<T> &
     return MHD_OK;
 }
 
-static void free_map(SyncMap &m)
+static void free_list(CopyList &m)
 {
     cudaFree(m.dst);
     cudaFree(m.src);
     cudaFree(m.tmp);
     cudaFree(m.cdst);
     cudaFree(m.cval);
-    m = SyncMap();
+    m = CopyList();
 }
 
 static void free_resistive(mhd_ctx *ctx)
@@ -1066,8 +1125,8 @@ static void free_resistive(mhd_ctx *ctx)
                     (void *)R.sign, (void *)R.rng_face, (void *)R.rng_edge, (void *)R.V, (void *)R.w, (void *)R.x,
                     (void *)R.b, (void *)R.r, (void *)R.partial, (void *)R.dots, (void *)R.st})
         cudaFree(p);
-    free_map(R.eres1form);
-    free_map(R.db);
+    free_list(R.eres1form);
+    free_list(R.db);
     const bool loops = R.graph_loops;
     R = mhd_ctx::Resistive();
     R.graph_loops = loops;
@@ -1087,11 +1146,16 @@ struct PoolDecoder
     }
     bool operator()(uint64_t off, int &b, int &i, int &j, int &k) const
     {
+        int f;
+        return decode(off, f, b, i, j, k);
+    }
+    bool decode(uint64_t off, int &f, int &b, int &i, int &j, int &k) const
+    {
         auto it = std::upper_bound(starts.begin(), starts.end(), std::make_pair(off, INT32_MAX));
         if (it == starts.begin())
             return false;
         --it;
-        const int f = it->second / ctx->nblocks;
+        f = it->second / ctx->nblocks;
         b = it->second % ctx->nblocks;
         const BlockView &v = ctx->hbv[size_t(b)];
         const uint64_t rel = off - it->first;
@@ -1126,21 +1190,170 @@ struct IBox
     }
 };
 
-static int read_map(mhd_ctx *ctx, const char *group, std::vector<uint64_t> &d, std::vector<uint64_t> &s, bool &staged)
+static void host_map(mhd_ctx *ctx, const char *group, std::vector<uint64_t> &d, std::vector<uint64_t> &s,
+                     bool &staged)
 {
-    d.clear();
-    s.clear();
-    staged = false;
     auto it = ctx->syncs.find(group);
-    if (it == ctx->syncs.end() || it->second.n == 0)
-        return MHD_OK;
-    const SyncMap &m = it->second;
-    d.resize(size_t(m.n));
-    s.resize(size_t(m.n));
-    CK(ctx, cudaMemcpy(d.data(), m.dst, size_t(m.n) * 8, cudaMemcpyDeviceToHost));
-    CK(ctx, cudaMemcpy(s.data(), m.src, size_t(m.n) * 8, cudaMemcpyDeviceToHost));
-    staged = m.tmp != nullptr;
+    if (it == ctx->syncs.end())
+    {
+        d.clear();
+        s.clear();
+        staged = false;
+        return;
+    }
+    d = it->second.hd;
+    s = it->second.hs;
+    staged = it->second.staged;
+}
+
+static int upload_list(mhd_ctx *ctx, CopyList &l, const std::vector<uint64_t> &cd, const std::vector<double> &cv,
+                       const std::vector<uint64_t> &d, const std::vector<uint64_t> &s2, bool staged)
+{
+    free_list(l);
+    RUN(upload_vec(ctx, cd, &l.cdst));
+    RUN(upload_vec(ctx, cv, &l.cval));
+    l.nconst = int64_t(cd.size());
+    RUN(upload_vec(ctx, d, &l.dst));
+    RUN(upload_vec(ctx, s2, &l.src));
+    l.n = int64_t(d.size());
+    if (staged && l.n > 0)
+        CK(ctx, cudaMalloc(&l.tmp, size_t(l.n) * 8));
     return MHD_OK;
+}
+
+// Ghost depth of each field that a kernel of the step reads: the face,
+// edge and contravariant-velocity stencils reach one layer into U_H, the
+// face B, Eface and U_plus; the edge EMF and J edges, B_cell, Bind_cell and
+// J_cell are read on inner points only.  Other fields keep every layer.
+static int hot_depth(int f)
+{
+    switch (f)
+    {
+    case F_U:
+    case F_Bxi:
+    case F_Beta:
+    case F_Bzeta:
+    case F_Efxi:
+    case F_Efeta:
+    case F_Efzeta:
+    case F_Uplus:
+        return 1;
+    case F_Exi:
+    case F_Eeta:
+    case F_Ezeta:
+    case F_Bcell:
+    case F_Bind:
+    case F_Jxi:
+    case F_Jeta:
+    case F_Jzeta:
+    case F_Jcell:
+        return 0;
+    default:
+        return 1 << 20;
+    }
+}
+
+static bool hot_point(const mhd_ctx *ctx, const PoolDecoder &dec, uint64_t off)
+{
+    int f, b, i, j, k;
+    if (!dec.decode(off, f, b, i, j, k))
+        return true;
+    const int d = hot_depth(f);
+    const BlockView &v = ctx->hbv[size_t(b)];
+    int pl[3];
+    loc_plus(kFields[f].loc, pl[0], pl[1], pl[2]);
+    return i >= -d && j >= -d && k >= -d && i < v.ni + pl[0] + d && j < v.nj + pl[1] + d && k < v.nk + pl[2] + d;
+}
+
+// device lists of a group from its host tables: the full lists, and the hot
+// ones (copies to hot points; fixed values at hot points or at sources of
+// hot copies)
+int build_sync(mhd_ctx *ctx, const std::string &group, SyncMap &m)
+{
+    RUN(upload_list(ctx, m.full, m.hcd, m.hcv, m.hd, m.hs, m.staged));
+    const PoolDecoder dec(ctx);
+    std::vector<uint64_t> d, s2, cd;
+    std::vector<double> cv;
+    for (size_t t = 0; t < m.hd.size(); ++t)
+        if (hot_point(ctx, dec, m.hd[t]))
+        {
+            d.push_back(m.hd[t]);
+            s2.push_back(m.hs[t]);
+        }
+    std::unordered_set<uint64_t> srcs(s2.begin(), s2.end());
+    for (size_t t = 0; t < m.hcd.size(); ++t)
+        if (hot_point(ctx, dec, m.hcd[t]) || srcs.count(m.hcd[t]))
+        {
+            cd.push_back(m.hcd[t]);
+            cv.push_back(m.hcv[t]);
+        }
+    RUN(upload_list(ctx, m.hot, cd, cv, d, s2, m.staged));
+    int f, b, i, j, k;
+    for (const auto *tab : {&m.hd, &m.hcd})
+        for (uint64_t off : *tab)
+            if (dec.decode(off, f, b, i, j, k))
+                ctx->field_group[size_t(f)] = group;
+    m.built = true;
+    return MHD_OK;
+}
+
+static int build_all_syncs(mhd_ctx *ctx)
+{
+    for (auto &kv : ctx->syncs)
+        if (!kv.second.built)
+            RUN(build_sync(ctx, kv.first, kv.second));
+    return MHD_OK;
+}
+
+// read-out of fields whose last sync ran its hot list only
+static int materialise_group(mhd_ctx *ctx, const std::string &group)
+{
+    auto it = ctx->dirty.find(group);
+    if (it == ctx->dirty.end() || !it->second)
+        return MHD_OK;
+    return run_sync(ctx, group.c_str(), true);
+}
+
+static int materialise_pv(mhd_ctx *ctx)
+{
+    const bool up = ctx->dirty.count("Uplus") && ctx->dirty["Uplus"];
+    if (!ctx->pv_dirty && !up)
+        return MHD_OK;
+    RUN(materialise_group(ctx, "Ucell"));
+    prof_begin(ctx, "k_pv_uplus_dt");
+    k_pv_uplus_dt<<<dim3(grid_for(max_box(ctx, LOC_CELL, ctx->G)), ctx->nblocks), kThreads, 0, ctx->stream>>>(
+        ctx->dbv, ctx->c, nullptr, ctx->G);
+    RUN(launched(ctx));
+    RUN(run_sync(ctx, "Uplus", true));
+    ctx->pv_dirty = false;
+    return MHD_OK;
+}
+
+static int materialise_field(mhd_ctx *ctx, int f)
+{
+    if (f == F_PV || f == F_Uplus)
+        return materialise_pv(ctx);
+    if (!ctx->field_group[size_t(f)].empty())
+        return materialise_group(ctx, ctx->field_group[size_t(f)]);
+    return MHD_OK;
+}
+
+static int materialise_all(mhd_ctx *ctx)
+{
+    RUN(materialise_pv(ctx));
+    for (auto &kv : ctx->dirty)
+        if (kv.second)
+            RUN(run_sync(ctx, kv.first.c_str(), true));
+    return MHD_OK;
+}
+
+// after graph replays: every group ran its hot list
+static void mark_dirty(mhd_ctx *ctx)
+{
+    for (auto &kv : ctx->syncs)
+        if (kv.second.built)
+            ctx->dirty[kv.first] = kv.second.hot.n != kv.second.full.n || kv.second.hot.nconst != kv.second.full.nconst;
+    ctx->pv_dirty = true;
 }
 
 // The region of the resistive operator.  Eres can be non-zero only at the
@@ -1158,8 +1371,8 @@ static int resistive_region(mhd_ctx *ctx, const std::vector<uint64_t> &seed)
     const PoolDecoder dec(ctx);
     std::vector<uint64_t> md[2], ms[2];
     bool staged[2];
-    RUN(read_map(ctx, "Eres1form", md[0], ms[0], staged[0]));
-    RUN(read_map(ctx, "dB", md[1], ms[1], staged[1]));
+    host_map(ctx, "Eres1form", md[0], ms[0], staged[0]);
+    host_map(ctx, "dB", md[1], ms[1], staged[1]);
     int b, i, j, k;
     // Eres: exact closure of the seed under the Eres1form copies
     std::unordered_set<uint64_t> enz(seed.begin(), seed.end());
@@ -1240,21 +1453,27 @@ static int resistive_region(mhd_ctx *ctx, const std::vector<uint64_t> &seed)
     RUN(upload_vec(ctx, rf, &R.rng_face));
     RUN(upload_vec(ctx, re, &R.rng_edge));
     // copies with a destination inside the region
-    SyncMap *out[2] = {&R.eres1form, &R.db};
+    CopyList *out[2] = {&R.eres1form, &R.db};
+    const char *names[2] = {"Eres1form", "dB"};
     for (int q = 0; q < 2; ++q)
     {
-        std::vector<uint64_t> d, s2;
+        std::vector<uint64_t> d, s2, cd;
+        std::vector<double> cv;
         for (size_t t = 0; t < md[q].size(); ++t)
             if (dec(md[q][t], b, i, j, k) && box[size_t(b)].has(i, j, k))
             {
                 d.push_back(md[q][t]);
                 s2.push_back(ms[q][t]);
             }
-        RUN(upload_vec(ctx, d, &out[q]->dst));
-        RUN(upload_vec(ctx, s2, &out[q]->src));
-        out[q]->n = int64_t(d.size());
-        if (staged[q] && !d.empty())
-            CK(ctx, cudaMalloc(&out[q]->tmp, d.size() * 8));
+        auto it = ctx->syncs.find(names[q]);
+        if (it != ctx->syncs.end())
+            for (size_t t = 0; t < it->second.hcd.size(); ++t)
+                if (dec(it->second.hcd[t], b, i, j, k) && box[size_t(b)].has(i, j, k))
+                {
+                    cd.push_back(it->second.hcd[t]);
+                    cv.push_back(it->second.hcv[t]);
+                }
+        RUN(upload_list(ctx, *out[q], cd, cv, d, s2, staged[q]));
     }
     return MHD_OK;
 }
@@ -1266,7 +1485,6 @@ int mhd_set_sync_map(mhd_ctx *ctx, const char *group, const int64_t *dst, const 
     if (!ctx || !group || n < 0 || (n > 0 && (!dst || !src)))
         return fail(ctx, MHD_EINVAL, "bad sync map arguments");
     std::vector<uint64_t> d(static_cast<size_t>(n)), s(static_cast<size_t>(n));
-    std::vector<char> is_dst(ctx->pool_n, 0);
     for (int64_t t = 0; t < n; ++t)
     {
         const int64_t od = pool_offset(ctx, dst[t]);
@@ -1275,33 +1493,22 @@ int mhd_set_sync_map(mhd_ctx *ctx, const char *group, const int64_t *dst, const 
             return fail(ctx, MHD_EINVAL, "sync map entry %lld has an invalid point id", (long long)t);
         d[size_t(t)] = uint64_t(od);
         s[size_t(t)] = uint64_t(os);
-        is_dst[size_t(od)] = 1;
     }
+    // staged (gather, then scatter) when a source is also a destination
+    std::vector<uint64_t> sorted_d(d);
+    std::sort(sorted_d.begin(), sorted_d.end());
     bool staged = false;
     for (int64_t t = 0; t < n && !staged; ++t)
-        staged = is_dst[size_t(s[size_t(t)])] != 0;
+        staged = std::binary_search(sorted_d.begin(), sorted_d.end(), s[size_t(t)]);
     SyncMap &m = ctx->syncs[group];
-    cudaFree(m.dst);
-    cudaFree(m.src);
-    cudaFree(m.tmp);
-    m.dst = m.src = nullptr;
-    m.tmp = nullptr;
-    m.n = 0;
+    m.hd.swap(d);
+    m.hs.swap(s);
+    m.staged = staged;
+    m.built = false;
     drop_graph(ctx);
-    if (n == 0)
-        return MHD_OK;
-    CK(ctx, cudaMalloc(&m.dst, size_t(n) * 8));
-    CK(ctx, cudaMalloc(&m.src, size_t(n) * 8));
-    CK(ctx, cudaMemcpy(m.dst, d.data(), size_t(n) * 8, cudaMemcpyHostToDevice));
-    CK(ctx, cudaMemcpy(m.src, s.data(), size_t(n) * 8, cudaMemcpyHostToDevice));
-    if (staged)
-        CK(ctx, cudaMalloc(&m.tmp, size_t(n) * 8));
-    m.n = n;
     // the resistive operator's region depends on these two groups
     if (ctx->res.on && (std::strcmp(group, "Eres1form") == 0 || std::strcmp(group, "dB") == 0))
     {
-        free_map(ctx->res.eres1form);
-        free_map(ctx->res.db);
         cudaFree(ctx->res.rng_face);
         cudaFree(ctx->res.rng_edge);
         ctx->res.rng_face = ctx->res.rng_edge = nullptr;
@@ -1323,19 +1530,17 @@ int mhd_set_sync_consts(mhd_ctx *ctx, const char *group, const int64_t *dst, con
         d[size_t(t)] = uint64_t(od);
     }
     SyncMap &m = ctx->syncs[group];
-    cudaFree(m.cdst);
-    cudaFree(m.cval);
-    m.cdst = nullptr;
-    m.cval = nullptr;
-    m.nconst = 0;
+    m.hcd.swap(d);
+    m.hcv.assign(val, val + n);
+    m.built = false;
     drop_graph(ctx);
-    if (n == 0)
-        return MHD_OK;
-    CK(ctx, cudaMalloc(&m.cdst, size_t(n) * 8));
-    CK(ctx, cudaMalloc(&m.cval, size_t(n) * 8));
-    CK(ctx, cudaMemcpy(m.cdst, d.data(), size_t(n) * 8, cudaMemcpyHostToDevice));
-    CK(ctx, cudaMemcpy(m.cval, val, size_t(n) * 8, cudaMemcpyHostToDevice));
-    m.nconst = n;
+    if (ctx->res.on && (std::strcmp(group, "Eres1form") == 0 || std::strcmp(group, "dB") == 0))
+    {
+        cudaFree(ctx->res.rng_face);
+        cudaFree(ctx->res.rng_edge);
+        ctx->res.rng_face = ctx->res.rng_edge = nullptr;
+        RUN(resistive_region(ctx, ctx->res.seed));
+    }
     return MHD_OK;
 }
 
@@ -1467,7 +1672,7 @@ int mhd_sync(mhd_ctx *ctx, const char *group)
 {
     if (!ctx || !group)
         return MHD_EINVAL;
-    RUN(run_sync(ctx, group));
+    RUN(run_sync(ctx, group, true));
     CK(ctx, cudaStreamSynchronize(ctx->stream));
     return MHD_OK;
 }
@@ -1533,6 +1738,8 @@ int mhd_step_host(mhd_ctx *ctx, int32_t nsteps, const double *state_in, double *
     RUN(run_sync(ctx, "Bface"));
     RUN(launch_update_derived(ctx));
     RUN(run_steps(ctx, nsteps));
+    for (int f : {int(F_U), int(F_Bxi)})
+        RUN(materialise_field(ctx, f));
     off = 0;
     for (int b = 0; b < ctx->nblocks; ++b)
         for (int f : {int(F_U), int(F_Bxi), int(F_Beta), int(F_Bzeta)})

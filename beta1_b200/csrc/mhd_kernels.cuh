@@ -30,7 +30,7 @@ __global__ void k_update_u(const BlockView *bvs, const double *dtp);
 __global__ void k_bcell(const BlockView *bvs);
 __global__ void k_jedge(const BlockView *bvs, int fB0, int fJ0, double mult, const int *rng);
 __global__ void k_jcell(const BlockView *bvs);
-__global__ void k_pv_uplus_dt(const BlockView *bvs, Consts c, unsigned long long *dt_key);
+__global__ void k_pv_uplus_dt(const BlockView *bvs, Consts c, unsigned long long *dt_key, int depth);
 __global__ void k_begin_step(const unsigned long long *dt_key, double *dt, int *err, double dt_abort);
 __global__ void k_arm_dt(unsigned long long *dt_key);
 __global__ void k_end_step(const double *dt, double *time, long long *step);

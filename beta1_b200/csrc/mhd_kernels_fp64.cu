@@ -547,10 +547,11 @@ __global__ void k_jcell(const BlockView *__restrict__ bvs)
 }
 
 // ---------------------------------------------------------------------------
-// calc_PV + calc_Uplus over the whole array (LunarSolver_Tools.cpp:58-141)
-// and, on inner cells, the CFL time-step bound of the next
-// Compute_Timestep (LunarSolver_Timestep.cpp:8-140) reduced with warp
-// shuffles and one atomicMin per thread block.
+// calc_PV + calc_Uplus (LunarSolver_Tools.cpp:58-141) on the inner cells
+// and `depth` ghost layers (the reference covers the whole array) and, on
+// inner cells, the CFL time-step bound of the next Compute_Timestep
+// (LunarSolver_Timestep.cpp:8-140) reduced with warp shuffles and one
+// atomicMin per thread block.
 // ---------------------------------------------------------------------------
 
 __device__ __forceinline__ double cfl_face_term(double ax, double ay, double az, bool outward_plus, double ux,
@@ -585,11 +586,11 @@ __device__ __forceinline__ unsigned long long dbl_key(double x)
     return (unsigned long long)__double_as_longlong(x);
 }
 
-__global__ void k_pv_uplus_dt(const BlockView *__restrict__ bvs, Consts c, unsigned long long *dt_key)
+__global__ void k_pv_uplus_dt(const BlockView *__restrict__ bvs, Consts c, unsigned long long *dt_key, int depth)
 {
     const BlockView &b = bvs[blockIdx.y];
     int lo[3], n[3];
-    loc_box(b, LOC_CELL, b.G, lo, n);
+    loc_box(b, LOC_CELL, depth, lo, n);
     int i, j, k;
     double dtc = 1e100;
     if (box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
