@@ -44,7 +44,7 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # Algorithmic bytes per cell of each kernel (FP64, every array the kernel
 # must read or write counted once per cell, 8 bytes per element).
 ALGO_BYTES_PER_CELL = {
-    # U 5, PV 5, JD 9, Jac 1, B_cell 3, J_cell 3 read; RHS_H 5 written
+    # rho 1, PV 4, RhoE 1, Csound 1, JD 9, face area 3, Jac 1, B_cell 3, J_cell 3 read; RHS_H 5 written
     "k_fluid_rhs": 31 * 8,
     # JD 9, Jac 1, U_plus 3 read; U_contra 3 written
     "k_ucontra": 16 * 8,
@@ -62,8 +62,8 @@ ALGO_BYTES_PER_CELL = {
     "k_jedge": 12 * 8,
     # J 3, W_J 36 read; J_cell 3 written
     "k_jcell": 42 * 8,
-    # U 5, Jac 1, B_cell 3, JD 9 read; PV 5, U_plus 3 written
-    "k_pv_uplus_dt": 26 * 8,
+    # U 5, Jac 1, B_cell 3, face area + unit normal 12 read; PV 5, U_plus 3, Csound 1, RhoE 1 written
+    "k_pv_uplus_dt": 31 * 8,
 }
 
 # DRAM traffic per launch from one ncu capture of the 64^3 case

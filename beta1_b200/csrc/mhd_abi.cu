@@ -82,7 +82,7 @@ const char *const kKernelNames[] = {
     "k_wall_u",       "k_alias_copy",  "k_scatter_vec",  "k_resist_out",   "k_resist_rhs",    "k_dots_partial",
     "k_dots_final",   "k_sub_proj",    "k_add_small",    "k_div_guard",    "k_div_next",      "k_gmres_init",
     "k_cycle_start",  "k_gmres_column", "k_inner_check", "k_gmres_solve_y", "k_add_basis",    "k_outer_check",
-    "k_zero",         "k_residual",    "k_ucontra"};
+    "k_zero",         "k_residual",    "k_ucontra",      "k_face_normals"};
 constexpr int kNumKernelNames = int(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
 
 } // namespace
@@ -113,6 +113,7 @@ struct mhd_ctx
     // and PV / U_plus computed on the first ghost layer only
     std::map<std::string, bool> dirty;
     bool pv_dirty = false;
+    bool geom_dirty = true; // face areas / normals to recompute from JD
     std::vector<std::string> field_group = std::vector<std::string>(NFIELD); // group that syncs a field
     double *staging = nullptr;
     size_t staging_n = 0;
@@ -135,8 +136,8 @@ struct mhd_ctx
         // the operator's active region: copies with a destination inside it,
         // and per (block, axis) sub-ranges of the inner faces / edges
         CopyList eres1form, db;
-        int *rng_face = nullptr, *rng_edge = nullptr;
-        int64_t nface_max = 0, nedge_max = 0;
+        int *rng = nullptr;      // per block: region box lo[3], hi[3] within [0, n + 1)^3
+        int64_t nreg_max = 0;    // points of the largest region box
         double rtol = 1e-8, atol = 1e-12;
         int maxit = 200, restart = 30;
         // workspace
@@ -226,6 +227,15 @@ int64_t max_box(const mhd_ctx *ctx, int loc, int g)
         const int64_t n = int64_t(v.ni + pi + 2 * g) * (v.nj + pj + 2 * g) * (v.nk + pk + 2 * g);
         m = n > m ? n : m;
     }
+    return m;
+}
+
+// staggered points [0, n + 1)^3 of the largest block
+int64_t max_stagger(const mhd_ctx *ctx)
+{
+    int64_t m = 0;
+    for (const auto &v : ctx->hbv)
+        m = std::max(m, int64_t(v.ni + 1) * (v.nj + 1) * (v.nk + 1));
     return m;
 }
 
@@ -346,6 +356,23 @@ int run_sync(mhd_ctx *ctx, const char *group, bool full = false)
     return MHD_OK;
 }
 
+// face areas and unit normals from the uploaded JD (eager, outside graphs)
+int ensure_geom(mhd_ctx *ctx)
+{
+    if (!ctx->geom_dirty)
+        return MHD_OK;
+    if (ctx->capturing)
+        return fail(ctx, MHD_ESTATE, "geometry changed during capture");
+    int64_t nf = 0;
+    for (int l = LOC_FXI; l <= LOC_FZETA; ++l)
+        nf = std::max(nf, max_box(ctx, l, ctx->G));
+    prof_begin(ctx, "k_face_normals");
+    k_face_normals<<<dim3(grid_for(nf), ctx->nblocks, 3), kThreads, 0, ctx->stream>>>(ctx->dbv);
+    RUN(launched(ctx));
+    ctx->geom_dirty = false;
+    return MHD_OK;
+}
+
 int launch_update_derived(mhd_ctx *ctx)
 {
     const int nb = ctx->nblocks;
@@ -355,11 +382,8 @@ int launch_update_derived(mhd_ctx *ctx)
     k_bcell<<<dim3(grid_for(nc), nb), kThreads, 0, s>>>(ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "B_cell"));
-    const int64_t ne = max_box(ctx, LOC_EZETA, 0) > max_box(ctx, LOC_EXI, 0) ? max_box(ctx, LOC_EZETA, 0)
-                                                                              : max_box(ctx, LOC_EXI, 0);
-    const int64_t ne2 = max_box(ctx, LOC_EETA, 0) > ne ? max_box(ctx, LOC_EETA, 0) : ne;
     prof_begin(ctx, "k_jedge");
-    k_jedge<<<dim3(grid_for(ne2), nb, 3), kThreads, 0, s>>>(ctx->dbv, F_Bxi, F_Jxi, 1.0, nullptr);
+    k_jedge<<<dim3(grid_for(max_stagger(ctx)), nb), kThreads, 0, s>>>(ctx->dbv, F_Bxi, F_Jxi, 1.0, nullptr);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Jedge"));
     prof_begin(ctx, "k_jcell");
@@ -393,27 +417,21 @@ int launch_induction(mhd_ctx *ctx, bool update_b)
 {
     const int nb = ctx->nblocks;
     cudaStream_t s = ctx->stream;
-    int64_t nf = 0;
-    for (int l = LOC_FXI; l <= LOC_FZETA; ++l)
-        nf = max_box(ctx, l, 0) > nf ? max_box(ctx, l, 0) : nf;
     prof_begin(ctx, "k_ucontra");
     k_ucontra<<<dim3(grid_for(max_box(ctx, LOC_CELL, 1)), nb), kThreads, 0, s>>>(ctx->dbv);
     RUN(launched(ctx));
     prof_begin(ctx, "k_eface");
-    k_eface<<<dim3(grid_for(nf), nb, 3), kThreads, 0, s>>>(ctx->dbv);
+    k_eface<<<dim3(grid_for(max_stagger(ctx)), nb), kThreads, 0, s>>>(ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Eface"));
     // inner edges; ghost edges keep their zero of AssembleRHS_Induction_CT_
     // except where the Eedge sync writes them
-    int64_t ne = 0;
-    for (int l = LOC_EXI; l <= LOC_EZETA; ++l)
-        ne = max_box(ctx, l, 0) > ne ? max_box(ctx, l, 0) : ne;
     prof_begin(ctx, "k_eedge");
-    k_eedge<<<dim3(grid_for(ne), nb, 3), kThreads, 0, s>>>(ctx->dbv, 0);
+    k_eedge<<<dim3(grid_for(max_stagger(ctx)), nb), kThreads, 0, s>>>(ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Eedge"));
     prof_begin(ctx, "k_curl_e2f");
-    k_curl_e2f<<<dim3(grid_for(nf), nb, 3), kThreads, 0, s>>>(ctx->dbv, F_Exi, F_RBxi, update_b ? F_Bxi : -1,
+    k_curl_e2f<<<dim3(grid_for(max_stagger(ctx)), nb), kThreads, 0, s>>>(ctx->dbv, F_Exi, F_RBxi, update_b ? F_Bxi : -1,
                                                                -1.0, ctx->dt, 1.0, 0, nullptr);
     return launched(ctx);
 }
@@ -442,22 +460,21 @@ int launch_update_u(mhd_ctx *ctx)
 int launch_curl_rng(mhd_ctx *ctx, int fE0, int fR0, int fB0, double mult, int mult_is_neg_dt)
 {
     auto &R = ctx->res;
-    if (R.nface_max == 0)
+    if (R.nreg_max == 0)
         return MHD_OK;
     prof_begin(ctx, "k_curl_e2f");
-    k_curl_e2f<<<dim3(grid_for(R.nface_max), ctx->nblocks, 3), kThreads, 0, ctx->stream>>>(
-        ctx->dbv, fE0, fR0, fB0, mult, ctx->dt, 1.0, mult_is_neg_dt, R.rng_face);
+    k_curl_e2f<<<dim3(grid_for(R.nreg_max), ctx->nblocks), kThreads, 0, ctx->stream>>>(
+        ctx->dbv, fE0, fR0, fB0, mult, ctx->dt, 1.0, mult_is_neg_dt, R.rng);
     return launched(ctx);
 }
 
 int launch_jedge_rng(mhd_ctx *ctx, int fB0, int fJ0)
 {
     auto &R = ctx->res;
-    if (R.nedge_max == 0)
+    if (R.nreg_max == 0)
         return MHD_OK;
     prof_begin(ctx, "k_jedge");
-    k_jedge<<<dim3(grid_for(R.nedge_max), ctx->nblocks, 3), kThreads, 0, ctx->stream>>>(ctx->dbv, fB0, fJ0, 1.0,
-                                                                                      R.rng_edge);
+    k_jedge<<<dim3(grid_for(R.nreg_max), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv, fB0, fJ0, 1.0, R.rng);
     return launched(ctx);
 }
 
@@ -806,6 +823,7 @@ int capture(mhd_ctx *ctx, int (*body)(mhd_ctx *), cudaGraph_t *graph, cudaGraphE
 // closing parts as two graphs around an eagerly launched solve.
 int build_graph(mhd_ctx *ctx)
 {
+    RUN(ensure_geom(ctx));
     if (ctx->gexec || ctx->gexec_a)
         return MHD_OK;
     RUN(build_all_syncs(ctx));
@@ -1017,6 +1035,8 @@ static int transfer(mhd_ctx *ctx, const char *name, int32_t block, const double 
     const int nc = kFields[f].ncomp;
     if (hin)
     {
+        if (f == F_JDxi || f == F_JDeta || f == F_JDzeta)
+            ctx->geom_dirty = true;
         CK(ctx, cudaMemcpyAsync(ctx->staging, hin, size_t(n) * 8, cudaMemcpyHostToDevice, ctx->stream));
         prof_begin(ctx, "k_aos_to_soa");
         k_aos_to_soa<<<grid_for(n), kThreads, 0, ctx->stream>>>(ctx->dbv, block, f, nc, lo[0], lo[1], lo[2],
@@ -1122,7 +1142,7 @@ static void free_resistive(mhd_ctx *ctx)
 {
     auto &R = ctx->res;
     for (void *p : {(void *)R.e, (void *)R.dj, (void *)R.j, (void *)R.eta, (void *)R.alias_e, (void *)R.owner_e,
-                    (void *)R.sign, (void *)R.rng_face, (void *)R.rng_edge, (void *)R.V, (void *)R.w, (void *)R.x,
+                    (void *)R.sign, (void *)R.rng, (void *)R.V, (void *)R.w, (void *)R.x,
                     (void *)R.b, (void *)R.r, (void *)R.partial, (void *)R.dots, (void *)R.st})
         cudaFree(p);
     free_list(R.eres1form);
@@ -1320,6 +1340,7 @@ static int materialise_pv(mhd_ctx *ctx)
     if (!ctx->pv_dirty && !up)
         return MHD_OK;
     RUN(materialise_group(ctx, "Ucell"));
+    RUN(ensure_geom(ctx));
     prof_begin(ctx, "k_pv_uplus_dt");
     k_pv_uplus_dt<<<dim3(grid_for(max_box(ctx, LOC_CELL, ctx->G)), ctx->nblocks), kThreads, 0, ctx->stream>>>(
         ctx->dbv, ctx->c, nullptr, ctx->G);
@@ -1424,34 +1445,25 @@ static int resistive_region(mhd_ctx *ctx, const std::vector<uint64_t> &seed)
             x.hi[a] = std::min(x.hi[a] + 2, n[a] + 1 + v.G);
         }
     }
-    // sub-ranges of the inner faces / edges inside the region
-    std::vector<int> rf(size_t(nb) * 18, 0), re(size_t(nb) * 18, 0);
-    R.nface_max = R.nedge_max = 0;
+    // per block: the region box within the staggered points [0, n + 1)^3
+    std::vector<int> rg(size_t(nb) * 6, 0);
+    R.nreg_max = 0;
     for (int q = 0; q < nb; ++q)
     {
         const BlockView &v = ctx->hbv[size_t(q)];
         const int n[3] = {v.ni, v.nj, v.nk};
-        for (int a = 0; a < 3; ++a)
-            for (int kind = 0; kind < 2; ++kind)
-            {
-                int plus[3];
-                loc_plus((kind == 0 ? LOC_FXI : LOC_EXI) + a, plus[0], plus[1], plus[2]);
-                int *r = (kind == 0 ? rf.data() : re.data()) + (q * 3 + a) * 6;
-                int64_t cnt = 1;
-                for (int d = 0; d < 3; ++d)
-                {
-                    const int lo = box[size_t(q)].empty() ? 0 : std::max(0, box[size_t(q)].lo[d]);
-                    const int hi = box[size_t(q)].empty() ? 0 : std::min(n[d] + plus[d], box[size_t(q)].hi[d]);
-                    r[d] = lo;
-                    r[3 + d] = std::max(0, hi - lo);
-                    cnt *= r[3 + d];
-                }
-                int64_t &mx = (kind == 0) ? R.nface_max : R.nedge_max;
-                mx = std::max(mx, cnt);
-            }
+        int64_t cnt = 1;
+        for (int d = 0; d < 3; ++d)
+        {
+            const int lo = box[size_t(q)].empty() ? 0 : std::max(0, box[size_t(q)].lo[d]);
+            const int hi = box[size_t(q)].empty() ? 0 : std::min(n[d] + 1, box[size_t(q)].hi[d]);
+            rg[size_t(q) * 6 + d] = lo;
+            rg[size_t(q) * 6 + 3 + d] = std::max(lo, hi);
+            cnt *= std::max(0, hi - lo);
+        }
+        R.nreg_max = std::max(R.nreg_max, cnt);
     }
-    RUN(upload_vec(ctx, rf, &R.rng_face));
-    RUN(upload_vec(ctx, re, &R.rng_edge));
+    RUN(upload_vec(ctx, rg, &R.rng));
     // copies with a destination inside the region
     CopyList *out[2] = {&R.eres1form, &R.db};
     const char *names[2] = {"Eres1form", "dB"};
@@ -1509,9 +1521,8 @@ int mhd_set_sync_map(mhd_ctx *ctx, const char *group, const int64_t *dst, const 
     // the resistive operator's region depends on these two groups
     if (ctx->res.on && (std::strcmp(group, "Eres1form") == 0 || std::strcmp(group, "dB") == 0))
     {
-        cudaFree(ctx->res.rng_face);
-        cudaFree(ctx->res.rng_edge);
-        ctx->res.rng_face = ctx->res.rng_edge = nullptr;
+        cudaFree(ctx->res.rng);
+        ctx->res.rng = nullptr;
         RUN(resistive_region(ctx, ctx->res.seed));
     }
     return MHD_OK;
@@ -1536,9 +1547,8 @@ int mhd_set_sync_consts(mhd_ctx *ctx, const char *group, const int64_t *dst, con
     drop_graph(ctx);
     if (ctx->res.on && (std::strcmp(group, "Eres1form") == 0 || std::strcmp(group, "dB") == 0))
     {
-        cudaFree(ctx->res.rng_face);
-        cudaFree(ctx->res.rng_edge);
-        ctx->res.rng_face = ctx->res.rng_edge = nullptr;
+        cudaFree(ctx->res.rng);
+        ctx->res.rng = nullptr;
         RUN(resistive_region(ctx, ctx->res.seed));
     }
     return MHD_OK;
@@ -1681,6 +1691,7 @@ int mhd_update_derived(mhd_ctx *ctx)
 {
     if (!ctx)
         return MHD_EINVAL;
+    RUN(ensure_geom(ctx));
     RUN(launch_update_derived(ctx));
     CK(ctx, cudaStreamSynchronize(ctx->stream));
     return MHD_OK;
@@ -1734,6 +1745,7 @@ int mhd_step_host(mhd_ctx *ctx, int32_t nsteps, const double *state_in, double *
             RUN(launched(ctx));
             off += n;
         }
+    RUN(ensure_geom(ctx));
     RUN(run_sync(ctx, "Ucell"));
     RUN(run_sync(ctx, "Bface"));
     RUN(launch_update_derived(ctx));
@@ -1777,6 +1789,7 @@ int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
 {
     if (!ctx)
         return MHD_EINVAL;
+    RUN(ensure_geom(ctx));
     switch (stage_id)
     {
     case MHD_STAGE_TIMESTEP:
@@ -1793,11 +1806,8 @@ int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
     case MHD_STAGE_UPDATE:
         RUN(launch_update_u(ctx));
         {
-            int64_t nf = 0;
-            for (int l = LOC_FXI; l <= LOC_FZETA; ++l)
-                nf = max_box(ctx, l, 0) > nf ? max_box(ctx, l, 0) : nf;
             prof_begin(ctx, "k_curl_e2f");
-            k_curl_e2f<<<dim3(grid_for(nf), ctx->nblocks, 3), kThreads, 0, ctx->stream>>>(ctx->dbv, F_Exi, -1, F_Bxi,
+            k_curl_e2f<<<dim3(grid_for(max_stagger(ctx)), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv, F_Exi, -1, F_Bxi,
                                                                                          -1.0, ctx->dt, 1.0, 0, nullptr);
             RUN(launched(ctx));
         }
@@ -1873,6 +1883,8 @@ int mhd_profile_step(mhd_ctx *ctx, int32_t cap, int32_t *kernel_ids, float *ms, 
 {
     if (!ctx || !count || cap < 0)
         return MHD_EINVAL;
+    RUN(ensure_geom(ctx));
+    RUN(build_all_syncs(ctx));
     ctx->profiling = true;
     ctx->prof_ev.clear();
     ctx->prof_names.clear();

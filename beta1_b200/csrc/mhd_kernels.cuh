@@ -21,9 +21,12 @@ struct Consts
 
 __global__ void k_fluid_rhs(const BlockView *bvs, Consts c, int64_t maxpts);
 __global__ void k_ucontra(const BlockView *bvs);
+__global__ void k_face_normals(const BlockView *bvs);
 __global__ void k_eface(const BlockView *bvs);
-__global__ void k_eedge(const BlockView *bvs, int G);
-// rng (may be null): per (block, axis) sub-range lo[3], n[3] of the inner faces / edges to process
+__global__ void k_eedge(const BlockView *bvs);
+// Face / edge kernels run one thread per staggered point (i, j, k) in
+// [0, n + 1)^3 and handle all three axes there.  rng (may be null): per
+// block a region box lo[3], hi[3]; only points inside it are processed.
 __global__ void k_curl_e2f(const BlockView *bvs, int fE0, int fR0, int fB0, double mult, const double *dtp,
                            double dtdiv, int mult_is_neg_dt, const int *rng);
 __global__ void k_update_u(const BlockView *bvs, const double *dtp);

@@ -48,30 +48,16 @@ __device__ __forceinline__ void loc_box(const BlockView &b, int loc, int g, int 
     n[2] = b.nk + pk + 2 * g;
 }
 
-// Inner range of a location, or the sub-range rng[6 * q .. 6 * q + 5]
-// (lo[3], n[3]) when a restricted range table is given.
-__device__ __forceinline__ void sub_range(const BlockView &b, int loc, const int *rng, int q, int lo[3], int n[3])
-{
-    if (rng)
-    {
-        const int *r = rng + 6 * q;
-        lo[0] = r[0];
-        lo[1] = r[1];
-        lo[2] = r[2];
-        n[0] = r[3];
-        n[1] = r[4];
-        n[2] = r[5];
-    }
-    else
-        loc_box(b, loc, 0, lo, n);
-}
-
 // ---------------------------------------------------------------------------
 // Scheme_U_ + AddSourceToRHS_Fluid
 // (Z4_Lunar/src/physics/LunarSolver_FluidRHS.cpp:3-201, :528-568)
 // ---------------------------------------------------------------------------
 
-// One Rusanov face flux (Reconstruction_Rusanov, piecewise-constant states)
+// One Rusanov face flux (Reconstruction_Rusanov, piecewise-constant states).
+// The sound speed sqrt(max(0, gamma p / max(rho, 1e-30))) and the total
+// energy p / (gamma - 1) + rho |u|^2 / 2 of each cell, and the face area
+// |k|, are the reference's expressions evaluated once (k_pv_uplus_dt,
+// k_face_normals) instead of once per face side; the values are identical.
 __device__ __forceinline__ void rusanov_face(const BlockView &b, const Consts &c, int dir, int i, int j, int k,
                                              double out[5])
 {
@@ -80,6 +66,7 @@ __device__ __forceinline__ void rusanov_face(const BlockView &b, const Consts &c
     const double k1 = b.f[JD][p];
     const double k2 = b.f[JD][b.vol + p];
     const double k3 = b.f[JD][2 * b.vol + p];
+    const double area = b.f[F_NAxi + dir][p];
     const int iL = i - (dir == 0), jL = j - (dir == 1), kL = k - (dir == 2);
     const int64_t pL = pidx(b, iL, jL, kL);
     const double *U = b.f[F_U];
@@ -88,31 +75,27 @@ __device__ __forceinline__ void rusanov_face(const BlockView &b, const Consts &c
 
     const double rhoL = U[pL], uL = PV[pL], vL = PV[v + pL], wL = PV[2 * v + pL], pLp = PV[3 * v + pL];
     const double rhoR = U[p], uR = PV[p], vR = PV[v + p], wR = PV[2 * v + p], pR = PV[3 * v + p];
-    const double g = c.gamma;
+    const double rhoeL = b.f[F_RhoE][pL], rhoeR = b.f[F_RhoE][p];
+    const double cL = b.f[F_Cs][pL], cR = b.f[F_Cs][p];
 
     double UL[5], UR[5];
     UL[0] = rhoL;
     UL[1] = rhoL * uL;
     UL[2] = rhoL * vL;
     UL[3] = rhoL * wL;
-    UL[4] = pLp / (g - 1.0) + 0.5 * rhoL * (uL * uL + vL * vL + wL * wL);
+    UL[4] = rhoeL;
     UR[0] = rhoR;
     UR[1] = rhoR * uR;
     UR[2] = rhoR * vR;
     UR[3] = rhoR * wR;
-    UR[4] = pR / (g - 1.0) + 0.5 * rhoR * (uR * uR + vR * vR + wR * wR);
+    UR[4] = rhoeR;
 
-    const double kk = (k1 * k1 + k2 * k2 + k3 * k3);
     const double uvwL = k1 * uL + k2 * vL + k3 * wL;
     const double uvwR = k1 * uR + k2 * vR + k3 * wR;
-    const double cL = sqrt(smax(0.0, g * pLp / smax(rhoL, 1e-30)));
-    const double cR = sqrt(smax(0.0, g * pR / smax(rhoR, 1e-30)));
-    const double radL = fabs(uvwL) + cL * sqrt(kk);
-    const double radR = fabs(uvwR) + cR * sqrt(kk);
+    const double radL = fabs(uvwL) + cL * area;
+    const double radR = fabs(uvwR) + cR * area;
     const double rad = smax(radL, radR);
 
-    const double rhoeL = pLp / (g - 1.0) + 0.5 * rhoL * (uL * uL + vL * vL + wL * wL);
-    const double rhoeR = pR / (g - 1.0) + 0.5 * rhoR * (uR * uR + vR * vR + wR * wR);
     double FL[5], FR[5];
     FL[0] = rhoL * uvwL;
     FL[1] = rhoL * uvwL * uL + k1 * pLp;
@@ -127,6 +110,28 @@ __device__ __forceinline__ void rusanov_face(const BlockView &b, const Consts &c
 #pragma unroll
     for (int m = 0; m < 5; ++m)
         out[m] = 0.5 * (FL[m] + FR[m]) - 0.5 * rad * (UR[m] - UL[m]);
+}
+
+// |JD| and JD / |JD| of every face (geometry; once per set-up)
+__global__ void k_face_normals(const BlockView *__restrict__ bvs)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    const int fa = blockIdx.z;
+    int lo[3], n[3];
+    loc_box(b, LOC_FXI + fa, b.G, lo, n);
+    int i, j, k;
+    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+        return;
+    const int64_t p = pidx(b, i, j, k);
+    const int64_t v = b.vol;
+    const double *M = b.f[F_JDxi + fa];
+    const double ax = M[p], ay = M[v + p], az = M[2 * v + p];
+    const double A = sqrt(ax * ax + ay * ay + az * az);
+    double *N = b.f[F_NAxi + fa];
+    N[p] = A;
+    N[v + p] = ax / A;
+    N[2 * v + p] = ay / A;
+    N[3 * v + p] = az / A;
 }
 
 __global__ void k_fluid_rhs(const BlockView *__restrict__ bvs, Consts c, int64_t /*maxpts*/)
@@ -264,16 +269,9 @@ __device__ __forceinline__ double emf_flux(const BlockView &b, int ba, int fa, i
     return 0.5 * (GL + GR) - 0.5 * radius * (biR - biL);
 }
 
-// blockIdx.z = flux axis
-__global__ void k_eface(const BlockView *__restrict__ bvs)
+// the two non-zero Eface components of face (i, j, k) of axis fa
+__device__ __forceinline__ void eface_one(const BlockView &b, int fa, int i, int j, int k)
 {
-    const BlockView &b = bvs[blockIdx.y];
-    const int fa = blockIdx.z;
-    int lo[3], n[3];
-    loc_box(b, LOC_FXI + fa, 0, lo, n);
-    int i, j, k;
-    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
-        return;
     const int iL = i - (fa == 0), jL = j - (fa == 1), kL = k - (fa == 2);
     const double bff = face_tot(b, fa, i, j, k);
     double e0 = 0.0, e1 = 0.0, e2 = 0.0;
@@ -305,6 +303,47 @@ __global__ void k_eface(const BlockView *__restrict__ bvs)
     b.f[F][2 * b.vol + p] = e2;
 }
 
+// Staggered points (i, j, k) of a block in [0, n + 1) per axis, one thread
+// each, or in the box rng[6 * block] (lo[3], hi[3], within [0, n + 1)^3)
+// when a region table is given; the kernels below handle all three face or
+// edge axes of a point in one thread so that the fields they share are read
+// once.
+__device__ __forceinline__ bool stagger_point(const BlockView &b, const int *rng, int blk, int &i, int &j, int &k)
+{
+    int lo[3] = {0, 0, 0};
+    int n[3] = {b.ni + 1, b.nj + 1, b.nk + 1};
+    if (rng)
+    {
+        const int *r = rng + 6 * blk;
+        for (int a = 0; a < 3; ++a)
+        {
+            lo[a] = r[a];
+            n[a] = r[3 + a] - r[a];
+        }
+    }
+    return box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k);
+}
+
+// is (i, j, k) an inner point of the face (kind 0) or edge (kind 1) axis a
+__device__ __forceinline__ bool inner_of(const BlockView &b, int kind, int a, int i, int j, int k)
+{
+    int pl[3];
+    loc_plus((kind == 0 ? LOC_FXI : LOC_EXI) + a, pl[0], pl[1], pl[2]);
+    return i < b.ni + pl[0] && j < b.nj + pl[1] && k < b.nk + pl[2];
+}
+
+__global__ void k_eface(const BlockView *__restrict__ bvs)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    int i, j, k;
+    if (!stagger_point(b, nullptr, 0, i, j, k))
+        return;
+#pragma unroll
+    for (int fa = 0; fa < 3; ++fa)
+        if (inner_of(b, 0, fa, i, j, k))
+            eface_one(b, fa, i, j, k);
+}
+
 // ---------------------------------------------------------------------------
 // AssembleEdgeEMF_FromFaceE_Ideal_ (LunarSolver_MagExplicit_Ideal.cpp:53-287)
 // with the zeroing of E_edge over the whole array (LunarSolver_MagneticRHS.cpp:9-28)
@@ -321,70 +360,70 @@ __device__ __forceinline__ double max_abs_u4(const BlockView &b, int axis, int i
     return a;
 }
 
-// blockIdx.z = edge axis; covers the full array (ghost edges are zeroed)
-__global__ void k_eedge(const BlockView *__restrict__ bvs, int G)
+// edge EMF of edge (i, j, k) of axis ea (inner edges)
+__device__ __forceinline__ double eedge_one(const BlockView &b, int ea, int i, int j, int k)
 {
-    const BlockView &b = bvs[blockIdx.y];
-    const int ea = blockIdx.z;
-    int lo[3], n[3];
-    loc_box(b, LOC_EXI + ea, G, lo, n);
-    int i, j, k;
-    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
-        return;
-    int pi, pj, pk;
-    loc_plus(LOC_EXI + ea, pi, pj, pk);
-    const bool inner = (i >= 0 && j >= 0 && k >= 0 && i < b.ni + pi && j < b.nj + pj && k < b.nk + pk);
     const double Cuct = 0.5;
     double E = 0.0;
-    if (inner)
+    if (ea == 0)
     {
-        if (ea == 0)
-        {
-            const double *Fe = b.f[F_Efeta];
-            const double *Fz = b.f[F_Efzeta];
-            const double Ec = 0.25 * (Fe[pidx(b, i, j, k)] + Fe[pidx(b, i, j, k - 1)] + Fz[pidx(b, i, j, k)] +
-                                      Fz[pidx(b, i, j - 1, k)]);
-            const double a_eta = max_abs_u4(b, 1, i, j, k, i, j - 1, k, i, j, k - 1, i, j - 1, k - 1);
-            const double a_zeta = max_abs_u4(b, 2, i, j, k, i, j - 1, k, i, j, k - 1, i, j - 1, k - 1);
-            const double dBzeta_eta = face_ind(b, 2, i, j, k) - face_ind(b, 2, i, j - 1, k);
-            const double dBeta_zeta = face_ind(b, 1, i, j, k) - face_ind(b, 1, i, j, k - 1);
-            E = Ec + Cuct * (0.5 * a_eta * dBzeta_eta - 0.5 * a_zeta * dBeta_zeta);
-        }
-        else if (ea == 1)
-        {
-            const double *Fx = b.f[F_Efxi];
-            const double *Fz = b.f[F_Efzeta];
-            const int64_t v = b.vol;
-            const double Ec = 0.25 * (Fx[v + pidx(b, i, j, k)] + Fx[v + pidx(b, i, j, k - 1)] +
-                                      Fz[v + pidx(b, i, j, k)] + Fz[v + pidx(b, i - 1, j, k)]);
-            const double a_zeta = max_abs_u4(b, 2, i, j, k, i - 1, j, k, i, j, k - 1, i - 1, j, k - 1);
-            const double a_xi = max_abs_u4(b, 0, i, j, k, i - 1, j, k, i, j, k - 1, i - 1, j, k - 1);
-            const double dBxi_zeta = face_ind(b, 0, i, j, k) - face_ind(b, 0, i, j, k - 1);
-            const double dBzeta_xi = face_ind(b, 2, i, j, k) - face_ind(b, 2, i - 1, j, k);
-            E = Ec + Cuct * (0.5 * a_zeta * dBxi_zeta - 0.5 * a_xi * dBzeta_xi);
-        }
-        else
-        {
-            const double *Fx = b.f[F_Efxi];
-            const double *Fe = b.f[F_Efeta];
-            const int64_t v2 = 2 * b.vol;
-            const double Ec = 0.25 * (Fx[v2 + pidx(b, i, j, k)] + Fx[v2 + pidx(b, i, j - 1, k)] +
-                                      Fe[v2 + pidx(b, i, j, k)] + Fe[v2 + pidx(b, i - 1, j, k)]);
-            const double a_xi = max_abs_u4(b, 0, i, j, k, i - 1, j, k, i, j - 1, k, i - 1, j - 1, k);
-            const double a_eta = max_abs_u4(b, 1, i, j, k, i - 1, j, k, i, j - 1, k, i - 1, j - 1, k);
-            const double dBeta_xi = face_ind(b, 1, i, j, k) - face_ind(b, 1, i - 1, j, k);
-            const double dBxi_eta = face_ind(b, 0, i, j, k) - face_ind(b, 0, i, j - 1, k);
-            E = Ec + Cuct * (0.5 * a_xi * dBeta_xi - 0.5 * a_eta * dBxi_eta);
-        }
+        const double *Fe = b.f[F_Efeta];
+        const double *Fz = b.f[F_Efzeta];
+        const double Ec = 0.25 * (Fe[pidx(b, i, j, k)] + Fe[pidx(b, i, j, k - 1)] + Fz[pidx(b, i, j, k)] +
+                                  Fz[pidx(b, i, j - 1, k)]);
+        const double a_eta = max_abs_u4(b, 1, i, j, k, i, j - 1, k, i, j, k - 1, i, j - 1, k - 1);
+        const double a_zeta = max_abs_u4(b, 2, i, j, k, i, j - 1, k, i, j, k - 1, i, j - 1, k - 1);
+        const double dBzeta_eta = face_ind(b, 2, i, j, k) - face_ind(b, 2, i, j - 1, k);
+        const double dBeta_zeta = face_ind(b, 1, i, j, k) - face_ind(b, 1, i, j, k - 1);
+        E = Ec + Cuct * (0.5 * a_eta * dBzeta_eta - 0.5 * a_zeta * dBeta_zeta);
     }
-    b.f[F_Exi + ea][pidx(b, i, j, k)] = E;
+    else if (ea == 1)
+    {
+        const double *Fx = b.f[F_Efxi];
+        const double *Fz = b.f[F_Efzeta];
+        const int64_t v = b.vol;
+        const double Ec = 0.25 * (Fx[v + pidx(b, i, j, k)] + Fx[v + pidx(b, i, j, k - 1)] +
+                                  Fz[v + pidx(b, i, j, k)] + Fz[v + pidx(b, i - 1, j, k)]);
+        const double a_zeta = max_abs_u4(b, 2, i, j, k, i - 1, j, k, i, j, k - 1, i - 1, j, k - 1);
+        const double a_xi = max_abs_u4(b, 0, i, j, k, i - 1, j, k, i, j, k - 1, i - 1, j, k - 1);
+        const double dBxi_zeta = face_ind(b, 0, i, j, k) - face_ind(b, 0, i, j, k - 1);
+        const double dBzeta_xi = face_ind(b, 2, i, j, k) - face_ind(b, 2, i - 1, j, k);
+        E = Ec + Cuct * (0.5 * a_zeta * dBxi_zeta - 0.5 * a_xi * dBzeta_xi);
+    }
+    else
+    {
+        const double *Fx = b.f[F_Efxi];
+        const double *Fe = b.f[F_Efeta];
+        const int64_t v2 = 2 * b.vol;
+        const double Ec = 0.25 * (Fx[v2 + pidx(b, i, j, k)] + Fx[v2 + pidx(b, i, j - 1, k)] +
+                                  Fe[v2 + pidx(b, i, j, k)] + Fe[v2 + pidx(b, i - 1, j, k)]);
+        const double a_xi = max_abs_u4(b, 0, i, j, k, i - 1, j, k, i, j - 1, k, i - 1, j - 1, k);
+        const double a_eta = max_abs_u4(b, 1, i, j, k, i - 1, j, k, i, j - 1, k, i - 1, j - 1, k);
+        const double dBeta_xi = face_ind(b, 1, i, j, k) - face_ind(b, 1, i - 1, j, k);
+        const double dBxi_eta = face_ind(b, 0, i, j, k) - face_ind(b, 0, i, j - 1, k);
+        E = Ec + Cuct * (0.5 * a_xi * dBeta_xi - 0.5 * a_eta * dBxi_eta);
+    }
+    return E;
+}
+
+// inner edges of all three axes; ghost edges keep the zero of
+// AssembleRHS_Induction_CT_ except where the Eedge sync writes them
+__global__ void k_eedge(const BlockView *__restrict__ bvs)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    int i, j, k;
+    if (!stagger_point(b, nullptr, 0, i, j, k))
+        return;
+#pragma unroll
+    for (int ea = 0; ea < 3; ++ea)
+        if (inner_of(b, 1, ea, i, j, k))
+            b.f[F_Exi + ea][pidx(b, i, j, k)] = eedge_one(b, ea, i, j, k);
 }
 
 // ---------------------------------------------------------------------------
 // CTOperators::CurlEdgeToFace (Z4_Lunar/src/operators/CTOperators.cpp:6-56)
 // with multiplier `mult`, written to RHS_B, optionally followed by the face
 // part of ApplyUpdate_Euler_ (LunarSolver_Advance.cpp:95-121): B += dt*RHS_B.
-// blockIdx.z = face axis.
 // ---------------------------------------------------------------------------
 __global__ void k_curl_e2f(const BlockView *__restrict__ bvs, int fE0, int fR0, int fB0, double mult,
                            const double *__restrict__ dtp, double dtdiv, int mult_is_neg_dt, const int *__restrict__ rng)
@@ -392,28 +431,31 @@ __global__ void k_curl_e2f(const BlockView *__restrict__ bvs, int fE0, int fR0, 
     if (mult_is_neg_dt)
         mult = -dtp[0];
     const BlockView &b = bvs[blockIdx.y];
-    const int fa = blockIdx.z;
-    int lo[3], n[3];
-    sub_range(b, LOC_FXI + fa, rng, blockIdx.y * 3 + fa, lo, n);
     int i, j, k;
-    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+    if (!stagger_point(b, rng, blockIdx.y, i, j, k))
         return;
     const double *Ex = b.f[fE0], *Ee = b.f[fE0 + 1], *Ez = b.f[fE0 + 2];
-    double curl;
-    if (fa == 0)
-        curl = (Ee[pidx(b, i, j, k)] - Ee[pidx(b, i, j, k + 1)]) + (Ez[pidx(b, i, j + 1, k)] - Ez[pidx(b, i, j, k)]);
-    else if (fa == 1)
-        curl = (Ex[pidx(b, i, j, k + 1)] - Ex[pidx(b, i, j, k)]) + (Ez[pidx(b, i, j, k)] - Ez[pidx(b, i + 1, j, k)]);
-    else
-        curl = (Ex[pidx(b, i, j, k)] - Ex[pidx(b, i, j + 1, k)]) + (Ee[pidx(b, i + 1, j, k)] - Ee[pidx(b, i, j, k)]);
     const int64_t p = pidx(b, i, j, k);
-    const double rhs = mult * curl;
-    if (fR0 >= 0)
-        b.f[fR0 + fa][p] = rhs;
-    if (fB0 >= 0)
+#pragma unroll
+    for (int fa = 0; fa < 3; ++fa)
     {
-        const double dt = dtp[0] / dtdiv;
-        b.f[fB0 + fa][p] += dt * rhs;
+        if (!inner_of(b, 0, fa, i, j, k))
+            continue;
+        double curl;
+        if (fa == 0)
+            curl = (Ee[p] - Ee[pidx(b, i, j, k + 1)]) + (Ez[pidx(b, i, j + 1, k)] - Ez[p]);
+        else if (fa == 1)
+            curl = (Ex[pidx(b, i, j, k + 1)] - Ex[p]) + (Ez[p] - Ez[pidx(b, i + 1, j, k)]);
+        else
+            curl = (Ex[p] - Ex[pidx(b, i, j + 1, k)]) + (Ee[pidx(b, i + 1, j, k)] - Ee[p]);
+        const double rhs = mult * curl;
+        if (fR0 >= 0)
+            b.f[fR0 + fa][p] = rhs;
+        if (fB0 >= 0)
+        {
+            const double dt = dtp[0] / dtdiv;
+            b.f[fB0 + fa][p] += dt * rhs;
+        }
     }
 }
 
@@ -479,38 +521,41 @@ __global__ void k_bcell(const BlockView *__restrict__ bvs)
 // ---------------------------------------------------------------------------
 // Calc_J_Edge: CTOperators::CurlAdjFaceToEdge (CTOperators.cpp:58-110) with
 // the face Hodge scale beta, times the edge scale alpha
-// (LunarSolver_Tools.cpp:777-835).  blockIdx.z = edge axis.
+// (LunarSolver_Tools.cpp:777-835).
 // ---------------------------------------------------------------------------
 __global__ void k_jedge(const BlockView *__restrict__ bvs, int fB0, int fJ0, double mult, const int *__restrict__ rng)
 {
     const BlockView &b = bvs[blockIdx.y];
-    const int ea = blockIdx.z;
-    int lo[3], n[3];
-    sub_range(b, LOC_EXI + ea, rng, blockIdx.y * 3 + ea, lo, n);
     int i, j, k;
-    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+    if (!stagger_point(b, rng, blockIdx.y, i, j, k))
         return;
     const double *Fx = b.f[fB0], *Fe = b.f[fB0 + 1], *Fz = b.f[fB0 + 2];
     const double *bx = b.f[F_betaxi], *be = b.f[F_betaeta], *bz = b.f[F_betazeta];
-    double val;
-    if (ea == 0)
+    const int64_t c0 = pidx(b, i, j, k);
+#pragma unroll
+    for (int ea = 0; ea < 3; ++ea)
     {
-        const int64_t a = pidx(b, i, j, k - 1), c0 = pidx(b, i, j, k), d = pidx(b, i, j - 1, k);
-        val = (be[a] * Fe[a] - be[c0] * Fe[c0]) + (bz[c0] * Fz[c0] - bz[d] * Fz[d]);
+        if (!inner_of(b, 1, ea, i, j, k))
+            continue;
+        double val;
+        if (ea == 0)
+        {
+            const int64_t a = pidx(b, i, j, k - 1), d = pidx(b, i, j - 1, k);
+            val = (be[a] * Fe[a] - be[c0] * Fe[c0]) + (bz[c0] * Fz[c0] - bz[d] * Fz[d]);
+        }
+        else if (ea == 1)
+        {
+            const int64_t a = pidx(b, i, j, k - 1), d = pidx(b, i - 1, j, k);
+            val = (bx[c0] * Fx[c0] - bx[a] * Fx[a]) + (bz[d] * Fz[d] - bz[c0] * Fz[c0]);
+        }
+        else
+        {
+            const int64_t a = pidx(b, i, j - 1, k), d = pidx(b, i - 1, j, k);
+            val = (bx[a] * Fx[a] - bx[c0] * Fx[c0]) + (be[c0] * Fe[c0] - be[d] * Fe[d]);
+        }
+        const double J = mult * val;
+        b.f[fJ0 + ea][c0] = J * b.f[F_alphaxi + ea][c0];
     }
-    else if (ea == 1)
-    {
-        const int64_t c0 = pidx(b, i, j, k), a = pidx(b, i, j, k - 1), d = pidx(b, i - 1, j, k);
-        val = (bx[c0] * Fx[c0] - bx[a] * Fx[a]) + (bz[d] * Fz[d] - bz[c0] * Fz[c0]);
-    }
-    else
-    {
-        const int64_t a = pidx(b, i, j - 1, k), c0 = pidx(b, i, j, k), d = pidx(b, i - 1, j, k);
-        val = (bx[a] * Fx[a] - bx[c0] * Fx[c0]) + (be[c0] * Fe[c0] - be[d] * Fe[d]);
-    }
-    const int64_t p = pidx(b, i, j, k);
-    const double J = mult * val;
-    b.f[fJ0 + ea][p] = J * b.f[F_alphaxi + ea][p];
 }
 
 // ---------------------------------------------------------------------------
@@ -554,14 +599,16 @@ __global__ void k_jcell(const BlockView *__restrict__ bvs)
 // atomicMin per thread block.
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ double cfl_face_term(double ax, double ay, double az, bool outward_plus, double ux,
+// one face of the CFL bound: (|u . n| + c_f) A with n the outward unit
+// normal (A and JD / A precomputed per face, k_face_normals)
+__device__ __forceinline__ double cfl_face_term(const double *N, int64_t v, int64_t p, bool outward_plus, double ux,
                                                 double uy, double uz, double Bx, double By, double Bz, double B2,
                                                 double rho, double cs2, double inver_MA2)
 {
-    const double A = sqrt(ax * ax + ay * ay + az * az);
+    const double A = N[p];
     if (A <= 0.0)
         return 0.0;
-    double nx = ax / A, ny = ay / A, nz = az / A;
+    double nx = N[v + p], ny = N[2 * v + p], nz = N[3 * v + p];
     if (!outward_plus)
     {
         nx = -nx;
@@ -599,9 +646,10 @@ __global__ void k_pv_uplus_dt(const BlockView *__restrict__ bvs, Consts c, unsig
         const int64_t v = b.vol;
         const double *U = b.f[F_U];
         const double U0 = U[p], U1 = U[v + p], U2 = U[2 * v + p], U3 = U[3 * v + p], U4 = U[4 * v + p];
+        const double rho_pv = smax(U0, 1e-12);
+        const double u = U1 / rho_pv, vv = U2 / rho_pv, w = U3 / rho_pv;
         {
-            const double rho = smax(U0, 1e-12);
-            const double u = U1 / rho, vv = U2 / rho, w = U3 / rho;
+            const double rho = rho_pv;
             const double ke = 0.5 * rho * (u * u + vv * vv + w * w);
             double eint = U4 - ke;
             if (eint < 0.0)
@@ -620,6 +668,10 @@ __global__ void k_pv_uplus_dt(const BlockView *__restrict__ bvs, Consts c, unsig
             Up[p] = has_plasma ? u : 0.0;
             Up[v + p] = has_plasma ? vv : 0.0;
             Up[2 * v + p] = has_plasma ? w : 0.0;
+            // sound speed and total energy of the Rusanov face states
+            // (Reconstruction_Rusanov, LunarSolver_FluidRHS.cpp:34-111)
+            b.f[F_Cs][p] = sqrt(smax(0.0, c.gamma * pr / smax(U0, 1e-30)));
+            b.f[F_RhoE][p] = pr / (c.gamma - 1.0) + 0.5 * U0 * (u * u + vv * vv + w * w);
         }
         const bool inner = (i >= 0 && j >= 0 && k >= 0 && i < b.ni && j < b.nj && k < b.nk);
         if (inner && dt_key)
@@ -628,7 +680,9 @@ __global__ void k_pv_uplus_dt(const BlockView *__restrict__ bvs, Consts c, unsig
             if (V > 0.0)
             {
                 const double rho = smax(U0, 1e-2);
-                const double ux = U1 / rho, uy = U2 / rho, uz = U3 / rho;
+                // same quotients as the primitive velocities when both floors leave rho alone
+                const bool same = (rho == rho_pv);
+                const double ux = same ? u : U1 / rho, uy = same ? vv : U2 / rho, uz = same ? w : U3 / rho;
                 const double ke = 0.5 * rho * (ux * ux + uy * uy + uz * uz);
                 const double eint = U4 - ke;
                 const double pr = (c.gamma - 1.0) * eint;
@@ -636,21 +690,15 @@ __global__ void k_pv_uplus_dt(const BlockView *__restrict__ bvs, Consts c, unsig
                 const double *Bc = b.f[F_Bcell];
                 const double Bx = Bc[p], By = Bc[v + p], Bz = Bc[2 * v + p];
                 const double B2 = Bx * Bx + By * By + Bz * Bz;
-                const double *X = b.f[F_JDxi], *Y = b.f[F_JDeta], *Z = b.f[F_JDzeta];
+                const double *X = b.f[F_NAxi], *Y = b.f[F_NAeta], *Z = b.f[F_NAzeta];
                 const int64_t pi1 = pidx(b, i + 1, j, k), pj1 = pidx(b, i, j + 1, k), pk1 = pidx(b, i, j, k + 1);
                 double denom = 0.0;
-                denom += cfl_face_term(X[p], X[v + p], X[2 * v + p], false, ux, uy, uz, Bx, By, Bz, B2, rho, cs2,
-                                       c.inver_MA2);
-                denom += cfl_face_term(X[pi1], X[v + pi1], X[2 * v + pi1], true, ux, uy, uz, Bx, By, Bz, B2, rho,
-                                       cs2, c.inver_MA2);
-                denom += cfl_face_term(Y[p], Y[v + p], Y[2 * v + p], false, ux, uy, uz, Bx, By, Bz, B2, rho, cs2,
-                                       c.inver_MA2);
-                denom += cfl_face_term(Y[pj1], Y[v + pj1], Y[2 * v + pj1], true, ux, uy, uz, Bx, By, Bz, B2, rho,
-                                       cs2, c.inver_MA2);
-                denom += cfl_face_term(Z[p], Z[v + p], Z[2 * v + p], false, ux, uy, uz, Bx, By, Bz, B2, rho, cs2,
-                                       c.inver_MA2);
-                denom += cfl_face_term(Z[pk1], Z[v + pk1], Z[2 * v + pk1], true, ux, uy, uz, Bx, By, Bz, B2, rho,
-                                       cs2, c.inver_MA2);
+                denom += cfl_face_term(X, v, p, false, ux, uy, uz, Bx, By, Bz, B2, rho, cs2, c.inver_MA2);
+                denom += cfl_face_term(X, v, pi1, true, ux, uy, uz, Bx, By, Bz, B2, rho, cs2, c.inver_MA2);
+                denom += cfl_face_term(Y, v, p, false, ux, uy, uz, Bx, By, Bz, B2, rho, cs2, c.inver_MA2);
+                denom += cfl_face_term(Y, v, pj1, true, ux, uy, uz, Bx, By, Bz, B2, rho, cs2, c.inver_MA2);
+                denom += cfl_face_term(Z, v, p, false, ux, uy, uz, Bx, By, Bz, B2, rho, cs2, c.inver_MA2);
+                denom += cfl_face_term(Z, v, pk1, true, ux, uy, uz, Bx, By, Bz, B2, rho, cs2, c.inver_MA2);
                 // cells with denom <= 0 (or NaN) do not bound dt, as in the reference
                 if (denom > 0.0)
                     dtc = c.cfl * V / denom;

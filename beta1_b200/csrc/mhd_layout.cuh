@@ -73,7 +73,12 @@ namespace mhd
     X(etaxi, "eta_edge_xi", 4, 1, 0)                         \
     X(etaeta, "eta_edge_eta", 5, 1, 0)                     \
     X(etazeta, "eta_edge_zeta", 6, 1, 0)                   \
-    X(UC, "U_contra_cell", 0, 3, 1)
+    X(UC, "U_contra_cell", 0, 3, 1)                        \
+    X(NAxi, "Anorm_xi", 1, 4, 4)                           \
+    X(NAeta, "Anorm_eta", 2, 4, 4)                         \
+    X(NAzeta, "Anorm_zeta", 3, 4, 4)                       \
+    X(Cs, "Csound_cell", 0, 1, 1)                          \
+    X(RhoE, "RhoE_cell", 0, 1, 1)
 
 enum FieldId : int
 {
