@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <unordered_set>
 #include <vector>
@@ -1064,6 +1065,78 @@ int mhd_upload_field(mhd_ctx *ctx, const char *name, int32_t block, const double
     // every field the device holds is brought to the reference's state first
     RUN(materialise_all(ctx));
     return transfer(ctx, name, block, data, nullptr, count);
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free read-out (no counterpart in the reference).  The staging
+// array is a fixed device array in this file; host code may not use its name
+// as a device address, so its address is looked up once per device.
+// ---------------------------------------------------------------------------
+} // extern "C"
+
+static __device__ __align__(256) double g_noalloc_staging[MHD_NOALLOC_MAX_DOUBLES];
+
+namespace
+{
+constexpr int kNoallocDevices = 64;
+std::mutex g_noalloc_mutex;
+double *g_noalloc_ptr[kNoallocDevices] = {};
+
+// device address of the staging array on the current device
+int noalloc_staging(mhd_ctx *ctx, double **out)
+{
+    int dev = -1;
+    CK(ctx, cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoallocDevices)
+        return fail(ctx, MHD_EINVAL, "device %d is beyond the %d devices of the read-out table", dev,
+                    kNoallocDevices);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev])
+    {
+        void *p = nullptr;
+        CK(ctx, cudaGetSymbolAddress(&p, g_noalloc_staging));
+        g_noalloc_ptr[dev] = static_cast<double *>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return MHD_OK;
+}
+} // namespace
+
+extern "C" {
+
+int mhd_download_field_noalloc(mhd_ctx *ctx, const char *name, int32_t block, double *data, int64_t count)
+{
+    if (!ctx || !data)
+        return fail(ctx, MHD_EINVAL, "null data");
+    const int f = field_by_name(name);
+    if (f < 0 || block < 0 || block >= ctx->nblocks)
+        return fail(ctx, MHD_EINVAL, "unknown field '%s' or block %d", name ? name : "(null)", block);
+    const int64_t n = field_count(ctx, f, block);
+    if (count != n)
+        return fail(ctx, MHD_EINVAL, "field %s block %d holds %lld values, got %lld", name, block, (long long)n,
+                    (long long)count);
+    if (n > int64_t(MHD_NOALLOC_MAX_DOUBLES))
+        return fail(ctx, MHD_EINVAL,
+                    "field %s block %d holds %lld values; the allocation-free read-out holds at most %d",
+                    name, block, (long long)n, MHD_NOALLOC_MAX_DOUBLES);
+    // bringing the field to the reference's state must only replay tables
+    // that are already on the device
+    for (const auto &kv : ctx->syncs)
+        if (!kv.second.built)
+            return fail(ctx, MHD_ESTATE, "sync group %s is not on the device yet; step or update the derived "
+                        "fields once before an allocation-free read-out", kv.first.c_str());
+    double *stage = nullptr;
+    RUN(noalloc_staging(ctx, &stage));
+    RUN(materialise_field(ctx, f));
+    int lo[3], hi[3];
+    field_box(ctx, f, block, lo, hi);
+    prof_begin(ctx, "k_soa_to_aos");
+    k_soa_to_aos<<<grid_for(n), kThreads, 0, ctx->stream>>>(ctx->dbv, block, f, kFields[f].ncomp, lo[0], lo[1],
+                                                            lo[2], hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], stage);
+    RUN(launched(ctx));
+    CK(ctx, cudaMemcpyAsync(data, stage, size_t(n) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return MHD_OK;
 }
 
 int mhd_download_field(mhd_ctx *ctx, const char *name, int32_t block, double *data, int64_t count)

@@ -21,6 +21,8 @@ LIB_PATH = os.path.join(HERE, "libbeta1_mhd.so")
 MHD_OK = 0
 ERRORS = {1: "EINVAL", 2: "ECUDA", 3: "ENOMEM", 4: "EDT", 5: "ESTATE", 6: "EKRYLOV"}
 
+NOALLOC_MAX_DOUBLES = 1 << 21
+
 PREC_FP64 = 0
 PREC_MIXED = 1
 
@@ -47,6 +49,7 @@ _SIGS = {
                                  C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "mhd_upload_field": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_void_p, C.c_int64]),
     "mhd_download_field": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_void_p, C.c_int64]),
+    "mhd_download_field_noalloc": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_void_p, C.c_int64]),
     "mhd_point_id": (C.c_int64, [C.c_void_p, C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "mhd_set_sync_map": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64]),
     "mhd_sync": (C.c_int, [C.c_void_p, C.c_char_p]),
@@ -185,6 +188,16 @@ class Context:
         out = np.empty(shape, dtype=np.float64)
         self._check(self.lib.mhd_download_field(self.h, name.encode(), block, out.ctypes.data, out.size),
                     f"download {name}")
+        return out
+
+    def download_noalloc(self, name: str, block: int = 0) -> np.ndarray:
+        """As download(), through the library's fixed staging array: no device
+        memory is allocated (fields up to NOALLOC_MAX_DOUBLES values)."""
+        inf = self.field_info(name, block)
+        shape = tuple(h - l for l, h in zip(inf["lo"], inf["hi"])) + (inf["ncomp"],)
+        out = np.empty(shape, dtype=np.float64)
+        self._check(self.lib.mhd_download_field_noalloc(self.h, name.encode(), block, out.ctypes.data, out.size),
+                    f"download_noalloc {name}")
         return out
 
     def point_base(self, name: str, block: int) -> int:

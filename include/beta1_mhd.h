@@ -95,6 +95,34 @@ int mhd_field_info(const mhd_ctx *ctx, const char *name, int32_t block, int32_t 
 int mhd_upload_field(mhd_ctx *ctx, const char *name, int32_t block, const double *data, int64_t count);
 int mhd_download_field(mhd_ctx *ctx, const char *name, int32_t block, double *data, int64_t count);
 
+/* Allocation-free read-out.  No counterpart in the reference: its drivers
+   read FieldBlock storage directly.  Same result as mhd_download_field, but
+   the device-side AoS staging goes through a fixed array of
+   MHD_NOALLOC_MAX_DOUBLES doubles (16 MiB) compiled into the library, instead
+   of a staging buffer the context allocates on first use.  Every GPU that
+   loads the library holds that array until the process exits.
+
+   Callers that cannot allocate:
+   - a driver that writes an emergency restart dump after a device allocation
+     has failed, where a further cudaMalloc would fail too;
+   - a driver that hands the GPU's memory to its own pool up front, sizing the
+     solver's blocks to fill it, so that no memory is left at output steps.
+
+   Limits and rules:
+   - A field of one block larger than MHD_NOALLOC_MAX_DOUBLES values is
+     rejected with MHD_EINVAL.
+   - The fields must have been synchronised on the device at least once (a
+     step or mhd_update_derived) before the call, so that the read-out needs
+     no new device tables.  Otherwise the call returns MHD_ESTATE.
+   - The first call on a device looks up the array's device address once for
+     that device, with the context's device current; make that first call
+     before any stream capture begins.
+   - All calls share the one array.  Each call overwrites the part it uses
+     and waits for its copy to finish before it returns.  Calls that overlap
+     on the same GPU (other host threads, other contexts) race. */
+#define MHD_NOALLOC_MAX_DOUBLES (1 << 21)
+int mhd_download_field_noalloc(mhd_ctx *ctx, const char *name, int32_t block, double *data, int64_t count);
+
 /* Field table of the library (no context, no GPU needed): name, location,
    components and ghost layers of field `index`; MHD_EINVAL past the end.
    A point id (below) is (index << 56) | (block << 40) | AoS offset of the
