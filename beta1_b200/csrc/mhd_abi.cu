@@ -83,7 +83,7 @@ const char *const kKernelNames[] = {
     "k_wall_u",       "k_alias_copy",  "k_scatter_vec",  "k_resist_out",   "k_resist_rhs",    "k_dots_partial",
     "k_dots_final",   "k_sub_proj",    "k_add_small",    "k_div_guard",    "k_div_next",      "k_gmres_init",
     "k_cycle_start",  "k_gmres_column", "k_inner_check", "k_gmres_solve_y", "k_add_basis",    "k_outer_check",
-    "k_zero",         "k_residual",    "k_ucontra",      "k_face_normals"};
+    "k_zero",         "k_residual",    "k_ucontra",      "k_face_normals", "k_divb",          "k_eres_explicit"};
 constexpr int kNumKernelNames = int(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
 
 } // namespace
@@ -152,6 +152,9 @@ struct mhd_ctx
         bool graph_loops = true;                 // conditional graph nodes usable
         std::vector<uint64_t> seed;              // unknown and alias offsets (Eres), for the region
     } res;
+    // explicit resistive sub-cycles (ResistiveDiffusionSubcycles_): 0 = off
+    int res_nsub = 0;
+    double res_inver_Rem = 0.0;
     cudaStream_t spare[2] = {nullptr, nullptr}; // capture streams of conditional bodies
     int spare_depth = 0;
 
@@ -753,11 +756,50 @@ int launch_step_c(mhd_ctx *ctx)
     return launch_update_derived(ctx);
 }
 
+// ResistiveDiffusionSubcycles_ (Z4_Lunar/src/physics/LunarSolver_MagneticRHS.cpp:53-115):
+// per sub-cycle Sync("Bface"), B_cell / J edge / J_cell with their syncs,
+// the resistive edge EMF, Sync("Eres"), then B += (dt / nsub) (-curl Eres)
+// and Sync("Bface")
+int launch_resistive_explicit(mhd_ctx *ctx)
+{
+    const int nb = ctx->nblocks;
+    cudaStream_t s = ctx->stream;
+    const unsigned gs = grid_for(max_stagger(ctx));
+    for (int q = 0; q < ctx->res_nsub; ++q)
+    {
+        RUN(run_sync(ctx, "Bface"));
+        prof_begin(ctx, "k_bcell");
+        k_bcell<<<dim3(grid_for(max_box(ctx, LOC_CELL, 0)), nb), kThreads, 0, s>>>(ctx->dbv);
+        RUN(launched(ctx));
+        RUN(run_sync(ctx, "B_cell"));
+        prof_begin(ctx, "k_jedge");
+        k_jedge<<<dim3(gs, nb), kThreads, 0, s>>>(ctx->dbv, F_Bxi, F_Jxi, 1.0, nullptr);
+        RUN(launched(ctx));
+        RUN(run_sync(ctx, "Jedge"));
+        prof_begin(ctx, "k_jcell");
+        k_jcell<<<dim3(grid_for(max_box(ctx, LOC_CELL, 0)), nb), kThreads, 0, s>>>(ctx->dbv);
+        RUN(launched(ctx));
+        RUN(run_sync(ctx, "J_cell"));
+        prof_begin(ctx, "k_eres_explicit");
+        k_eres_explicit<<<dim3(gs, nb), kThreads, 0, s>>>(ctx->dbv, ctx->res_inver_Rem);
+        RUN(launched(ctx));
+        RUN(run_sync(ctx, "Eres"));
+        prof_begin(ctx, "k_curl_e2f");
+        k_curl_e2f<<<dim3(gs, nb), kThreads, 0, s>>>(ctx->dbv, F_Eresxi, F_RBresxi, F_Bxi, -1.0, ctx->dt,
+                                                     double(ctx->res_nsub), 0, nullptr);
+        RUN(launched(ctx));
+        RUN(run_sync(ctx, "Bface"));
+    }
+    return MHD_OK;
+}
+
 int launch_step(mhd_ctx *ctx)
 {
     RUN(launch_step_a(ctx));
     if (ctx->res.on)
         RUN(launch_resistive(ctx));
+    else if (ctx->res_nsub > 0)
+        RUN(launch_resistive_explicit(ctx));
     return launch_step_c(ctx);
 }
 
@@ -1318,8 +1360,12 @@ static int upload_list(mhd_ctx *ctx, CopyList &l, const std::vector<uint64_t> &c
 // edge and contravariant-velocity stencils reach one layer into U_H, the
 // face B, Eface and U_plus; the edge EMF and J edges, B_cell, Bind_cell and
 // J_cell are read on inner points only.  Other fields keep every layer.
-static int hot_depth(int f)
+static int hot_depth(const mhd_ctx *ctx, int f)
 {
+    // the explicit resistive EMF averages J_cell over the four cells around
+    // an edge, one ghost layer deep
+    if (f == F_Jcell && ctx->res_nsub > 0)
+        return 1;
     switch (f)
     {
     case F_U:
@@ -1340,6 +1386,9 @@ static int hot_depth(int f)
     case F_Jeta:
     case F_Jzeta:
     case F_Jcell:
+    case F_Eresxi:
+    case F_Ereseta:
+    case F_Ereszeta:
         return 0;
     default:
         return 1 << 20;
@@ -1351,7 +1400,7 @@ static bool hot_point(const mhd_ctx *ctx, const PoolDecoder &dec, uint64_t off)
     int f, b, i, j, k;
     if (!dec.decode(off, f, b, i, j, k))
         return true;
-    const int d = hot_depth(f);
+    const int d = hot_depth(ctx, f);
     const BlockView &v = ctx->hbv[size_t(b)];
     int pl[3];
     loc_plus(kFields[f].loc, pl[0], pl[1], pl[2]);
@@ -1728,6 +1777,21 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
     return MHD_OK;
 }
 
+int mhd_set_resistive_explicit(mhd_ctx *ctx, double inver_Rem, int32_t nsub)
+{
+    if (!ctx || nsub < 0)
+        return fail(ctx, MHD_EINVAL, "bad explicit resistive arguments");
+    if (nsub > 0 && ctx->res.on)
+        return fail(ctx, MHD_ESTATE, "the implicit resistive solve is set up; the two are exclusive");
+    ctx->res_nsub = nsub;
+    ctx->res_inver_Rem = inver_Rem;
+    // the hot sync lists depend on it (J_cell ghost depth)
+    for (auto &kv : ctx->syncs)
+        kv.second.built = false;
+    drop_graph(ctx);
+    return MHD_OK;
+}
+
 int mhd_resistive_stats(const mhd_ctx *ctx, int32_t *its, double *rnorm, double *bnorm, int32_t *reason)
 {
     if (!ctx)
@@ -1884,6 +1948,11 @@ int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
                                                                                          -1.0, ctx->dt, 1.0, 0, nullptr);
             RUN(launched(ctx));
         }
+        break;
+    case MHD_STAGE_DIVB:
+        prof_begin(ctx, "k_divb");
+        k_divb<<<dim3(grid_for(max_box(ctx, LOC_CELL, 0)), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv);
+        RUN(launched(ctx));
         break;
     default:
         return fail(ctx, MHD_EINVAL, "unknown stage %d", stage_id);

@@ -30,6 +30,8 @@ __global__ void k_eedge(const BlockView *bvs);
 __global__ void k_curl_e2f(const BlockView *bvs, int fE0, int fR0, int fB0, double mult, const double *dtp,
                            double dtdiv, int mult_is_neg_dt, const int *rng);
 __global__ void k_update_u(const BlockView *bvs, const double *dtp);
+__global__ void k_divb(const BlockView *bvs);
+__global__ void k_eres_explicit(const BlockView *bvs, double inver_Rem);
 __global__ void k_bcell(const BlockView *bvs);
 __global__ void k_jedge(const BlockView *bvs, int fB0, int fJ0, double mult, const int *rng);
 __global__ void k_jcell(const BlockView *bvs);

@@ -459,6 +459,88 @@ __global__ void k_curl_e2f(const BlockView *__restrict__ bvs, int fE0, int fR0, 
     }
 }
 
+// calc_divB on inner cells (Z4_Lunar/src/physics/LunarSolver_Tools.cpp:685-775;
+// layouts with Pole patches, whose first shell the reference zeroes, are not
+// handled here)
+__global__ void k_divb(const BlockView *__restrict__ bvs)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    int lo[3], n[3];
+    loc_box(b, LOC_CELL, 0, lo, n);
+    int i, j, k;
+    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+        return;
+    const int64_t p = pidx(b, i, j, k);
+    const double *Bx = b.f[F_Bxi], *Be = b.f[F_Beta], *Bz = b.f[F_Bzeta];
+    const double num = Bx[pidx(b, i + 1, j, k)] - Bx[p] + Be[pidx(b, i, j + 1, k)] - Be[p] + Bz[pidx(b, i, j, k + 1)] -
+                       Bz[p];
+    b.f[F_divB][p] = num / b.f[F_Jac][p];
+}
+
+// Explicit resistive edge EMF, AddResistiveEdgeEMF_To_ on a zeroed Eres
+// (Z4_Lunar/src/physics/LunarSolver_MagExplicit_Resis.cpp:67-209): on inner
+// edges with a non-zero shell profile yita0 (eta_edge_*, from the edge
+// midpoint radius), Eres = (inver_Rem yita0) (J_avg . dr) with J_avg the mean
+// cell current of the four cells around the edge; zero elsewhere.
+__global__ void k_eres_explicit(const BlockView *__restrict__ bvs, double inver_Rem)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    int i, j, k;
+    if (!stagger_point(b, nullptr, 0, i, j, k))
+        return;
+    const double *Jc = b.f[F_Jcell];
+    const int64_t v = b.vol;
+    const int64_t p = pidx(b, i, j, k);
+#pragma unroll
+    for (int ea = 0; ea < 3; ++ea)
+    {
+        if (!inner_of(b, 1, ea, i, j, k))
+            continue;
+        const double yita0 = b.f[F_etaxi + ea][p];
+        double E = 0.0;
+        if (yita0 != 0.0)
+        {
+            int64_t c[4];
+            if (ea == 0)
+            {
+                c[0] = p;
+                c[1] = pidx(b, i, j - 1, k);
+                c[2] = pidx(b, i, j, k - 1);
+                c[3] = pidx(b, i, j - 1, k - 1);
+            }
+            else if (ea == 1)
+            {
+                c[0] = p;
+                c[1] = pidx(b, i - 1, j, k);
+                c[2] = pidx(b, i, j, k - 1);
+                c[3] = pidx(b, i - 1, j, k - 1);
+            }
+            else
+            {
+                c[0] = p;
+                c[1] = pidx(b, i - 1, j, k);
+                c[2] = pidx(b, i, j - 1, k);
+                c[3] = pidx(b, i - 1, j - 1, k);
+            }
+            double Jx = 0.0, Jy = 0.0, Jz = 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+            {
+                Jx += Jc[c[q]];
+                Jy += Jc[v + c[q]];
+                Jz += Jc[2 * v + c[q]];
+            }
+            Jx *= 0.25;
+            Jy *= 0.25;
+            Jz *= 0.25;
+            const double *dr = b.f[F_drxi + ea];
+            const double Jedge = Jx * dr[p] + Jy * dr[v + p] + Jz * dr[2 * v + p];
+            E = 0.0 + (inver_Rem * yita0) * Jedge;
+        }
+        b.f[F_Eresxi + ea][p] = E;
+    }
+}
+
 // cell part of ApplyUpdate_Euler_ (LunarSolver_Advance.cpp:82-93): U += dt*RHS_H
 __global__ void k_update_u(const BlockView *__restrict__ bvs, const double *__restrict__ dtp)
 {

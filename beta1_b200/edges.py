@@ -92,3 +92,28 @@ def resistive_dofs(owners, nodes, inver_Rem):
     eta = eta_at_edges(o, nodes, inver_Rem)
     keep = eta > 0.0
     return o[keep], eta[keep]
+
+
+def shell_profile(nodes, ncell):
+    """yita0(r) of every inner edge of a block (per axis an array over the
+    edge's inner box): 0.5 [tanh((r - 0.84)/0.02) - tanh((r - 1.04)/0.02)] of
+    the edge-midpoint radius, zero outside 0.84 < r < 1.04
+    (LunarSolver::AddResistiveEdgeEMF_To_,
+    Z4_Lunar/src/physics/LunarSolver_MagExplicit_Resis.cpp:72-88, 160-167).
+    `nodes` is the block's node array with its ghost layers (geometry.Padded)."""
+    o = nodes.off
+    out = []
+    for d in (1, 2, 3):
+        p = _EXT[d]
+        n = (ncell[0] + p[0], ncell[1] + p[1], ncell[2] + p[2])
+        di, dj, dk = (d == 1), (d == 2), (d == 3)
+        p0 = nodes.a[o:o + n[0], o:o + n[1], o:o + n[2]]
+        p1 = nodes.a[o + di:o + di + n[0], o + dj:o + dj + n[1], o + dk:o + dk + n[2]]
+        xm, ym, zm = (0.5 * (p0[..., c] + p1[..., c]) for c in range(3))
+        r = np.sqrt(xm * xm + ym * ym + zm * zm)
+        y = np.zeros(r.shape)
+        for idx in zip(*np.nonzero(~(r <= 0.84) & ~(r >= 1.04))):
+            rr = float(r[idx])
+            y[idx] = 0.5 * (math.tanh((rr - 0.84) / 0.02) - math.tanh((rr - 1.04) / 0.02))
+        out.append(y)
+    return out

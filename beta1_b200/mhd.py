@@ -26,7 +26,7 @@ NOALLOC_MAX_DOUBLES = 1 << 21
 PREC_FP64 = 0
 PREC_MIXED = 1
 
-STAGE_TIMESTEP, STAGE_FLUID_RHS, STAGE_INDUCTION, STAGE_UPDATE = 1, 2, 3, 4
+STAGE_TIMESTEP, STAGE_FLUID_RHS, STAGE_INDUCTION, STAGE_UPDATE, STAGE_DIVB = 1, 2, 3, 4, 5
 
 
 class BlockDesc(C.Structure):
@@ -57,6 +57,7 @@ _SIGS = {
     "mhd_set_sync_wall": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_int32]),
     "mhd_set_resistive": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int32, C.c_int32]),
+    "mhd_set_resistive_explicit": (C.c_int, [C.c_void_p, C.c_double, C.c_int32]),
     "mhd_resistive_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double),
                                       C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "mhd_update_derived": (C.c_int, [C.c_void_p]),
@@ -233,6 +234,9 @@ class Context:
         self._check(self.lib.mhd_set_resistive(self.h, u.size, u.ctypes.data, e.ctypes.data, a.size, a.ctypes.data,
                                                o.ctypes.data, sg.ctypes.data, rtol, atol, maxit, restart),
                     "set_resistive")
+
+    def set_resistive_explicit(self, inver_Rem: float, nsub: int):
+        self._check(self.lib.mhd_set_resistive_explicit(self.h, float(inver_Rem), int(nsub)), "set_resistive_explicit")
 
     def resistive_stats(self):
         its, rn, bn, rs = C.c_int32(), C.c_double(), C.c_double(), C.c_int32()

@@ -57,10 +57,13 @@ class Solver:
             raise ValueError(f"unknown topology {topology}")
         self.ctx.sync("Badd")
         p = spec.params
+        if float(p.get("arti_eta_max", 0.0)) > 0.0:
+            raise NotImplementedError("the artificial-resistivity edge EMF is not supported by this build")
         if p.get("is_Lunar_resistance", 0):
-            if not p.get("use_implicit_lunar_resistance", 0):
-                raise NotImplementedError("explicit resistive sub-cycles are not supported by this build")
-            self.install_resistive(topology)
+            if p.get("use_implicit_lunar_resistance", 0):
+                self.install_resistive(topology)
+            else:
+                self.install_explicit_resistive()
 
     def install_resistive(self, topology):
         """Unknowns, resistivity and edge aliases of the implicit resistive
@@ -85,6 +88,17 @@ class Solver:
                                float(p["implicit_resistive_ksp_rtol"]), float(p["implicit_resistive_ksp_atol"]),
                                int(p["implicit_resistive_ksp_max_it"]), 30)
         self.resistive_dofs = (dofs, eta)
+
+    def install_explicit_resistive(self):
+        """Shell profile of every inner edge and the sub-cycle count of
+        LunarSolver::ResistiveDiffusionSubcycles_."""
+        spec = self.spec
+        for ib, b in enumerate(spec.blocks):
+            for name, y in zip(("eta_edge_xi", "eta_edge_eta", "eta_edge_zeta"),
+                               edges.shell_profile(self.nodes[ib], b.ncell)):
+                self.ctx.upload(name, ib, y[..., None])
+        c = physics.constants(spec.params)
+        self.ctx.set_resistive_explicit(c["inver_Rem"], max(1, int(spec.params["n_resistive_subcycles"])))
 
     def install_tiled(self):
         spec = self.spec

@@ -167,6 +167,16 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
                       const int64_t *alias, const int64_t *owner, const double *sign, double rtol, double atol,
                       int32_t maxit, int32_t restart);
 
+/* Explicit resistive sub-cycles (LunarSolver::ResistiveDiffusionSubcycles_,
+   Z4_Lunar/src/physics/LunarSolver_MagneticRHS.cpp:53-115, with the edge EMF of
+   AddResistiveEdgeEMF_To_, Z4_Lunar/src/physics/LunarSolver_MagExplicit_Resis.cpp:67-209):
+   `nsub` sub-cycles of dt / nsub in every following StepOnce (0 switches them
+   off).  The shell profile yita0(r) of every inner edge is read from the
+   fields eta_edge_xi / eta_edge_eta / eta_edge_zeta, which the caller
+   uploads; the EMF is (inver_Rem yita0) (J . dr).  Exclusive with
+   mhd_set_resistive. */
+int mhd_set_resistive_explicit(mhd_ctx *ctx, double inver_Rem, int32_t nsub);
+
 /* Iterations, final residual norm, ||b|| and convergence reason (2 rtol,
    3 atol, -3 iteration limit, as KSPConvergedReason) of the last solve. */
 int mhd_resistive_stats(const mhd_ctx *ctx, int32_t *its, double *rnorm, double *bnorm, int32_t *reason);
@@ -206,6 +216,7 @@ int mhd_host_free(void *ptr);
 #define MHD_STAGE_FLUID_RHS 2  /* ZeroRHS_ + Scheme_U_ + AddSourceToRHS_Fluid -> RHS_H */
 #define MHD_STAGE_INDUCTION 3  /* AssembleRHS_Induction_CT_ -> Eface, E, RHS_B */
 #define MHD_STAGE_UPDATE 4     /* ApplyUpdate_Euler_ with the current dt */
+#define MHD_STAGE_DIVB 5       /* calc_divB -> divB (inner cells; no Pole patches) */
 int mhd_stage(mhd_ctx *ctx, int32_t stage_id);
 
 /* Current dt / time / step counters (device -> host). */

@@ -33,6 +33,7 @@ FIELDS = {
     "Jcell_from_Jedge_w": (0, 36, 3), "Eres_xi": (4, 1, 4), "Eres_eta": (5, 1, 4), "Eres_zeta": (6, 1, 4),
     "dB_xi": (1, 1, 4), "dB_eta": (2, 1, 4), "dB_zeta": (3, 1, 4), "dJ_xi": (4, 1, 4), "dJ_eta": (5, 1, 4),
     "dJ_zeta": (6, 1, 4), "RHS_Bres_xi": (1, 1, 0), "RHS_Bres_eta": (2, 1, 0), "RHS_Bres_zeta": (3, 1, 0),
+    "divB": (0, 1, 1), "dr_xi": (4, 3, 3), "dr_eta": (5, 3, 3), "dr_zeta": (6, 3, 3),
 }
 PLUS = {0: (0, 0, 0), 1: (1, 0, 0), 2: (0, 1, 0), 3: (0, 0, 1), 4: (0, 1, 1), 5: (1, 0, 1), 6: (1, 1, 0)}
 
@@ -285,8 +286,8 @@ class Oracle:
         Up[1] = np.where(has, v, 0.0)
         Up[2] = np.where(has, w, 0.0)
 
-    def update_derived(self):
-        """UpdateDerivedFields_ (LunarSolver_Tools.cpp:143-161)"""
+    def update_magnetic_derived(self):
+        """UpdateMagneticDerivedFields_ (LunarSolver_Tools.cpp:149-155)"""
         for blk in self.blocks:
             self.calc_bcell(blk)
         self.sync("B_cell")
@@ -296,6 +297,10 @@ class Oracle:
         for blk in self.blocks:
             self.calc_jcell(blk)
         self.sync("J_cell")
+
+    def update_derived(self):
+        """UpdateDerivedFields_ (LunarSolver_Tools.cpp:157-161)"""
+        self.update_magnetic_derived()
         for blk in self.blocks:
             self.calc_pv_uplus(blk)
         self.sync("Uplus")
@@ -538,6 +543,8 @@ class Oracle:
                 blk.f[bn][0][blk.s(lo, hi)] += dt * blk.box(rn, 0, lo, hi)
         if self.resist is not None:
             self.resistive_step()
+        elif self.explicit is not None:
+            self.resistive_subcycles()
         self.time += dt
         self.sync("Ucell")
         self.sync("Bface")
@@ -643,3 +650,80 @@ class Oracle:
                 lo, hi = blk.inner(1 + fa)
                 blk.f[bn][0][blk.s(lo, hi)] += self.dt * blk.box(rn, 0, lo, hi)
         self.sync("Bface")
+
+    # ------------------------------------------------------- divB diagnostic
+    def calc_divb(self):
+        """calc_divB without Pole patches (Z4_Lunar/src/physics/LunarSolver_Tools.cpp:685-775)"""
+        for blk in self.blocks:
+            lo, hi = blk.inner(0)
+            z = (0, 0, 0)
+            bx = lambda d: blk.box("B_xi", 0, lo, hi, d)
+            be = lambda d: blk.box("B_eta", 0, lo, hi, d)
+            bz = lambda d: blk.box("B_zeta", 0, lo, hi, d)
+            num = bx((1, 0, 0)) - bx(z) + be((0, 1, 0)) - be(z) + bz((0, 0, 1)) - bz(z)
+            blk.f["divB"][0][blk.s(lo, hi)] = num / blk.box("Jac", 0, lo, hi)
+
+    # ------------------------------------------------ explicit resistivity
+    explicit = None
+
+    def set_explicit_resistive(self, nodes, inver_Rem, nsub):
+        """ResistiveDiffusionSubcycles_ set-up: edge-midpoint radii of the inner
+        edges from the node coordinates (per block a (ni+1, nj+1, nk+1, 3)
+        array of the inner nodes) and the tanh shell profile yita0
+        (Z4_Lunar/src/physics/LunarSolver_MagExplicit_Resis.cpp:72-88, 160-167)."""
+        import math
+        prof = []
+        for blk, X in zip(self.blocks, nodes):
+            per = []
+            for ea, (di, dj, dk) in enumerate(((1, 0, 0), (0, 1, 0), (0, 0, 1))):
+                lo, hi = blk.inner(4 + ea)
+                p0 = X[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]]
+                p1 = X[lo[0] + di:hi[0] + di, lo[1] + dj:hi[1] + dj, lo[2] + dk:hi[2] + dk]
+                xm, ym, zm = (0.5 * (p0[..., c] + p1[..., c]) for c in range(3))
+                r = np.sqrt(xm * xm + ym * ym + zm * zm)
+                y = np.zeros(r.shape)
+                for idx in zip(*np.nonzero((r > 0.84) & (r < 1.04))):
+                    rr = float(r[idx])
+                    y[idx] = 0.5 * (math.tanh((rr - 0.84) / 0.02) - math.tanh((rr - 1.04) / 0.02))
+                per.append(y)
+            prof.append(per)
+        self.explicit = dict(yita0=prof, inver_Rem=float(inver_Rem), nsub=max(1, int(nsub)))
+
+    def eres_explicit(self, blk, yita0):
+        """AddResistiveEdgeEMF_To_ on zeroed Eres (LunarSolver_MagExplicit_Resis.cpp:67-209)"""
+        cells = {0: [(0, 0, 0), (0, -1, 0), (0, 0, -1), (0, -1, -1)],
+                 1: [(0, 0, 0), (-1, 0, 0), (0, 0, -1), (-1, 0, -1)],
+                 2: [(0, 0, 0), (-1, 0, 0), (0, -1, 0), (-1, -1, 0)]}
+        for ea, (en, dn) in enumerate((("Eres_xi", "dr_xi"), ("Eres_eta", "dr_eta"), ("Eres_zeta", "dr_zeta"))):
+            lo, hi = blk.inner(4 + ea)
+            J = [0.0, 0.0, 0.0]
+            for d in cells[ea]:
+                for c in range(3):
+                    J[c] = J[c] + blk.box("J_cell", c, lo, hi, d)
+            J = [x * 0.25 for x in J]
+            Jedge = J[0] * blk.box(dn, 0, lo, hi) + J[1] * blk.box(dn, 1, lo, hi) + J[2] * blk.box(dn, 2, lo, hi)
+            y = yita0[ea]
+            with np.errstate(invalid="ignore"):
+                val = 0.0 + (self.explicit["inver_Rem"] * y) * Jedge
+            blk.f[en][0][blk.s(lo, hi)] = np.where(y == 0.0, 0.0, val)
+
+    def resistive_subcycles(self):
+        """ResistiveDiffusionSubcycles_ (Z4_Lunar/src/physics/LunarSolver_MagneticRHS.cpp:53-115)"""
+        nsub = self.explicit["nsub"]
+        dt_res = self.dt / float(nsub)
+        for _ in range(nsub):
+            self.sync("Bface")
+            self.update_magnetic_derived()
+            self._clear("Eres")
+            self._clear("RHS_Bres")
+            for blk, y in zip(self.blocks, self.explicit["yita0"]):
+                self.eres_explicit(blk, y)
+            self.sync("Eres")
+            for blk in self.blocks:
+                self.curl_e2f(blk, ("Eres_xi", "Eres_eta", "Eres_zeta"),
+                              ("RHS_Bres_xi", "RHS_Bres_eta", "RHS_Bres_zeta"), -1.0)
+                for fa, (bn, rn) in enumerate((("B_xi", "RHS_Bres_xi"), ("B_eta", "RHS_Bres_eta"),
+                                               ("B_zeta", "RHS_Bres_zeta"))):
+                    lo, hi = blk.inner(1 + fa)
+                    blk.f[bn][0][blk.s(lo, hi)] += dt_res * blk.box(rn, 0, lo, hi)
+            self.sync("Bface")

@@ -31,7 +31,7 @@ OUT = os.path.dirname(os.path.abspath(__file__))
 
 STEP_FIELDS = ["U_H", "B_xi", "B_eta", "B_zeta", "PV_H", "U_plus", "B_cell", "Bind_cell", "J_xi", "J_eta", "J_zeta",
                "J_cell", "E_xi", "E_eta", "E_zeta", "Eface_xi", "Eface_eta", "Eface_zeta", "RHS_H", "RHS_B_xi",
-               "RHS_B_eta", "RHS_B_zeta"]
+               "RHS_B_eta", "RHS_B_zeta", "divB"]
 GROUPS = ["Ucell", "Bface", "Eface", "Eedge", "B_cell", "Jedge", "J_cell", "Uplus"]
 
 
@@ -178,6 +178,9 @@ if __name__ == "__main__":
     slab(steps=2, resistive=1, implicit=1, eta_max_lunar=1.0 * case.MU0 * case.ref_scales()["U"]
          * case.ref_scales()["L_ref"], implicit_resistive_ksp_rtol=1e-13, implicit_resistive_ksp_atol=1e-30,
          implicit_resistive_ksp_max_it=300)
+    # explicit resistive sub-cycles (two per step) with the same resistivity
+    slab(steps=2, resistive=1, implicit=0, eta_max_lunar=1.0 * case.MU0 * case.ref_scales()["U"]
+         * case.ref_scales()["L_ref"], n_resistive_subcycles=2)
     slab_probe(resistive=0)
     slab_probe(resistive=1)
     slab_owners(eta_max_lunar=1.0 * case.MU0 * case.ref_scales()["U"] * case.ref_scales()["L_ref"])

@@ -17,16 +17,17 @@ import pytest
 
 from conftest import load_golden, rel_l2, slab_setup
 
-from beta1_b200 import solver
+from beta1_b200 import mhd, solver
 
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-12
 FIELDS = ["Eres_xi", "Eres_eta", "Eres_zeta", "U_H", "B_xi", "B_eta", "B_zeta", "PV_H", "U_plus", "B_cell", "Bind_cell", "J_xi", "J_eta", "J_zeta",
           "J_cell", "E_xi", "E_eta", "E_zeta", "Eface_xi", "Eface_eta", "Eface_zeta", "RHS_H", "RHS_B_xi",
-          "RHS_B_eta", "RHS_B_zeta"]
+          "RHS_B_eta", "RHS_B_zeta", "divB"]
 CASES = {"ideal": ("slab_6x5x6_t2x2_r00_steps.npz", 1e-12),
-         "implicit_resistive": ("slab_6x5x6_t2x2_r11_steps.npz", 1e-10)}
+         "implicit_resistive": ("slab_6x5x6_t2x2_r11_steps.npz", 1e-10),
+         "explicit_resistive": ("slab_6x5x6_t2x2_r10_steps.npz", 1e-12)}
 
 
 @pytest.fixture(scope="module", params=list(CASES))
@@ -36,12 +37,14 @@ def slab_run(request):
     spec, st = slab_setup(g)
     s = solver.Solver(spec, topology="tiled")
     s.load_state(st)
+    s.ctx.stage(mhd.STAGE_DIVB)
     nb = len(spec.blocks)
     out = {0: {(f, b): s.field(f, b) for f in FIELDS for b in range(nb)}}
     dts = {}
     nsteps = max(int(k.split("/")[0][1:]) for k in g.files if k[0] == "s" and k[1].isdigit())
     for n in range(1, nsteps + 1):
         dts[n], _ = s.step(1)
+        s.ctx.stage(mhd.STAGE_DIVB)
         out[n] = {(f, b): s.field(f, b) for f in FIELDS for b in range(nb)}
     stats = s.ctx.resistive_stats() if "Eres" in "".join(g.files) and int(g["resistive"][0]) else None
     s.ctx.close()
@@ -60,6 +63,10 @@ def test_slab_fields_match_reference(slab_run):
             for b in range(nb):
                 ref = g["s%d/b%d/%s" % (n, b, f)]
                 got = out[n][(f, b)]
+                if f == "divB":
+                    # round-off quantity (~1e-16): compared absolutely
+                    assert np.abs(got - ref).max() <= TOL, (n, b, f)
+                    continue
                 e = rel_l2(got, ref)
                 worst = max(worst, e)
                 assert e <= TOL, f"step {n} block {b} field {f}: rel L2 {e:.3e}"
