@@ -44,7 +44,9 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # Algorithmic bytes per cell of each kernel (FP64, every array the kernel
 # must read or write counted once per cell, 8 bytes per element).
 ALGO_BYTES_PER_CELL = {
-    # rho 1, PV 4, RhoE 1, Csound 1, JD 9, face area 3, Jac 1, B_cell 3, J_cell 3 read; RHS_H 5 written
+    # fluid RHS: rho 1, PV 4, RhoE 1, Csound 1, JD 9, face area 3, Jac 1, B_cell 3, J_cell 3 read, RHS_H 5
+    # written; with the contravariant velocities: U_plus 3 read, U_contra 3 written
+    "k_fluid_ucontra": 37 * 8,
     "k_fluid_rhs": 31 * 8,
     # JD 9, Jac 1, U_plus 3 read; U_contra 3 written
     "k_ucontra": 16 * 8,
@@ -56,14 +58,11 @@ ALGO_BYTES_PER_CELL = {
     "k_curl_e2f": 12 * 8,
     # U 5 read + written, RHS_H 5 read
     "k_update_u": 15 * 8,
-    # B 3, Badd 3, W_B 18 read; B_cell 3, Bind_cell 3 written
-    "k_bcell": 30 * 8,
-    # B 3, beta 3, alpha 3 read; J 3 written
-    "k_jedge": 12 * 8,
-    # J 3, W_J 36 read; J_cell 3 written
-    "k_jcell": 42 * 8,
-    # U 5, Jac 1, B_cell 3, face area + unit normal 12 read; PV 5, U_plus 3, Csound 1, RhoE 1 written
-    "k_pv_uplus_dt": 31 * 8,
+    # B_cell + J edges: B 3, Badd 3, W_B 18, beta 3, alpha 3 read; B_cell 3, Bind_cell 3, J 3 written
+    "k_bcell_jedge": 39 * 8,
+    # PV / U_plus / CFL with J_cell: U 5, Jac 1, B_cell 3, face area + normal 12, J 3, W_J 36 read;
+    # PV 5, U_plus 3, Csound 1, RhoE 1, J_cell 3 written
+    "k_pv_uplus_dt": 73 * 8,
 }
 
 # DRAM traffic per launch from one ncu capture of the 64^3 case

@@ -72,6 +72,8 @@ struct SyncMap
     bool staged = false;
     bool built = false; // device lists match the host tables
     CopyList full, hot;
+    int *dwalls = nullptr;  // walls on the device (block, direction pairs)
+    int64_t wall_cols = 0;  // boundary cell columns of the largest wall
 };
 
 constexpr int kThreads = 256;
@@ -80,10 +82,11 @@ const char *const kKernelNames[] = {
     "k_fluid_rhs",    "k_eface",       "k_eedge",        "k_curl_e2f",     "k_update_u",      "k_bcell",
     "k_jedge",        "k_jcell",       "k_pv_uplus_dt",  "k_begin_step",   "k_arm_dt",        "k_end_step",
     "k_gather",       "k_gather_stage", "k_scatter_stage", "k_aos_to_soa", "k_soa_to_aos",    "k_set_consts",
-    "k_wall_u",       "k_alias_copy",  "k_scatter_vec",  "k_resist_out",   "k_resist_rhs",    "k_dots_partial",
-    "k_dots_final",   "k_sub_proj",    "k_add_small",    "k_div_guard",    "k_div_next",      "k_gmres_init",
+    "k_wall_u",       "k_alias_copy",  "k_scatter_vec",  "k_resist_out",   "k_resist_rhs",    "k_dots",
+    "k_sub_proj",    "k_add_small",    "k_div_guard",    "k_div_next",      "k_gmres_init",
     "k_cycle_start",  "k_gmres_column", "k_inner_check", "k_gmres_solve_y", "k_add_basis",    "k_outer_check",
-    "k_zero",         "k_residual",    "k_ucontra",      "k_face_normals", "k_divb",          "k_eres_explicit"};
+    "k_zero",         "k_residual",    "k_ucontra",      "k_face_normals", "k_divb",          "k_eres_explicit",
+    "k_bcell_jedge",  "k_fluid_ucontra", "k_wall_u_all"};
 constexpr int kNumKernelNames = int(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
 
 } // namespace
@@ -346,13 +349,11 @@ int run_sync(mhd_ctx *ctx, const char *group, bool full = false)
         k_set_consts<<<grid_for(l.nconst), kThreads, 0, ctx->stream>>>(ctx->pool, l.cdst, l.cval, l.nconst);
         RUN(launched(ctx));
     }
-    for (const auto &w : m.walls)
+    if (!m.walls.empty())
     {
-        const BlockView &v = ctx->hbv[size_t(w.first)];
-        const int ax = std::abs(w.second) - 1;
-        const int64_t ncol = (ax == 0) ? int64_t(v.nj) * v.nk : (ax == 1) ? int64_t(v.ni) * v.nk : int64_t(v.ni) * v.nj;
-        prof_begin(ctx, "k_wall_u");
-        k_wall_u<<<grid_for(ncol), kThreads, 0, ctx->stream>>>(ctx->dbv, w.first, w.second, ctx->c.gamma);
+        prof_begin(ctx, "k_wall_u_all");
+        k_wall_u_all<<<dim3(grid_for(m.wall_cols), unsigned(m.walls.size())), kThreads, 0, ctx->stream>>>(
+            ctx->dbv, m.dwalls, ctx->c.gamma);
         RUN(launched(ctx));
     }
     RUN(gather_map(ctx, l));
@@ -377,24 +378,21 @@ int ensure_geom(mhd_ctx *ctx)
     return MHD_OK;
 }
 
+// UpdateDerivedFields_ as two passes: B_cell with the J edges (both read the
+// face B), then J_cell with PV / U_plus / the CFL bound (J_cell's weight
+// stream beside PV's FP64 work).  Each sync runs after the pass that writes
+// its fields and before any pass that reads them; the reference's order
+// among these independent fields does not change any value.
 int launch_update_derived(mhd_ctx *ctx)
 {
     const int nb = ctx->nblocks;
     cudaStream_t s = ctx->stream;
-    const int64_t nc = max_box(ctx, LOC_CELL, 0);
-    prof_begin(ctx, "k_bcell");
-    k_bcell<<<dim3(grid_for(nc), nb), kThreads, 0, s>>>(ctx->dbv);
+    prof_begin(ctx, "k_bcell_jedge");
+    k_bcell_jedge<<<dim3(grid_for(max_stagger(ctx)), nb), kThreads, 0, s>>>(ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "B_cell"));
-    prof_begin(ctx, "k_jedge");
-    k_jedge<<<dim3(grid_for(max_stagger(ctx)), nb), kThreads, 0, s>>>(ctx->dbv, F_Bxi, F_Jxi, 1.0, nullptr);
-    RUN(launched(ctx));
     RUN(run_sync(ctx, "Jedge"));
-    prof_begin(ctx, "k_jcell");
-    k_jcell<<<dim3(grid_for(nc), nb), kThreads, 0, s>>>(ctx->dbv);
-    RUN(launched(ctx));
-    RUN(run_sync(ctx, "J_cell"));
-    // arm the dt reduction, then PV / U_plus / CFL bound of the next step
+    // arm the dt reduction, then J_cell, PV / U_plus and the CFL bound of the next step
     prof_begin(ctx, "k_arm_dt");
     k_arm_dt<<<1, 1, 0, s>>>(ctx->dt_key);
     RUN(launched(ctx));
@@ -402,9 +400,10 @@ int launch_update_derived(mhd_ctx *ctx)
     // of the step and are filled when read out (materialise_pv)
     const int64_t ng = max_box(ctx, LOC_CELL, 1);
     prof_begin(ctx, "k_pv_uplus_dt");
-    k_pv_uplus_dt<<<dim3(grid_for(ng), nb), kThreads, 0, s>>>(ctx->dbv, ctx->c, ctx->dt_key, 1);
+    k_pv_uplus_dt<<<dim3(grid_for(ng), nb), kThreads, 0, s>>>(ctx->dbv, ctx->c, ctx->dt_key, 1, 1);
     ctx->pv_dirty = true;
     RUN(launched(ctx));
+    RUN(run_sync(ctx, "J_cell"));
     RUN(run_sync(ctx, "Uplus"));
     return MHD_OK;
 }
@@ -417,13 +416,26 @@ int launch_fluid_rhs(mhd_ctx *ctx)
     return launched(ctx);
 }
 
-int launch_induction(mhd_ctx *ctx, bool update_b)
+// fluid RHS together with the contravariant velocities of the EMF stencils
+int launch_fluid_ucontra(mhd_ctx *ctx)
+{
+    prof_begin(ctx, "k_fluid_ucontra");
+    k_fluid_ucontra<<<dim3(grid_for(max_box(ctx, LOC_CELL, 1)), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv,
+                                                                                                          ctx->c);
+    return launched(ctx);
+}
+
+// AssembleRHS_Induction_CT_; with_ucontra unless the fluid pass computed them
+int launch_induction(mhd_ctx *ctx, bool update_b, bool with_ucontra = true)
 {
     const int nb = ctx->nblocks;
     cudaStream_t s = ctx->stream;
-    prof_begin(ctx, "k_ucontra");
-    k_ucontra<<<dim3(grid_for(max_box(ctx, LOC_CELL, 1)), nb), kThreads, 0, s>>>(ctx->dbv);
-    RUN(launched(ctx));
+    if (with_ucontra)
+    {
+        prof_begin(ctx, "k_ucontra");
+        k_ucontra<<<dim3(grid_for(max_box(ctx, LOC_CELL, 1)), nb), kThreads, 0, s>>>(ctx->dbv);
+        RUN(launched(ctx));
+    }
     prof_begin(ctx, "k_eface");
     k_eface<<<dim3(grid_for(max_stagger(ctx)), nb), kThreads, 0, s>>>(ctx->dbv);
     RUN(launched(ctx));
@@ -523,11 +535,8 @@ int dots(mhd_ctx *ctx, const double *V, int nvec, const int *jdev, const double 
 {
     auto &R = ctx->res;
     const int ny = jdev ? R.restart + 1 : nvec;
-    prof_begin(ctx, "k_dots_partial");
-    k_dots_partial<<<dim3(R.ngroups, ny), 256, 0, ctx->stream>>>(V, R.n, nvec, w, R.n, R.partial, jdev);
-    RUN(launched(ctx));
-    prof_begin(ctx, "k_dots_final");
-    k_dots_final<<<1, 64, 0, ctx->stream>>>(R.partial, R.ngroups, nvec, out, jdev);
+    prof_begin(ctx, "k_dots");
+    k_dots<<<dim3(R.ngroups, ny), 256, 0, ctx->stream>>>(V, R.n, nvec, w, R.n, R.partial, jdev, out, R.st->dot_done);
     return launched(ctx);
 }
 
@@ -740,8 +749,8 @@ int launch_step_a(mhd_ctx *ctx)
     prof_begin(ctx, "k_begin_step");
     k_begin_step<<<1, 1, 0, ctx->stream>>>(ctx->dt_key, ctx->dt, ctx->err, ctx->prm.dt_abort);
     RUN(launched(ctx));
-    RUN(launch_fluid_rhs(ctx));
-    RUN(launch_induction(ctx, /*update_b=*/true));
+    RUN(launch_fluid_ucontra(ctx));
+    RUN(launch_induction(ctx, /*update_b=*/true, /*with_ucontra=*/false));
     return launch_update_u(ctx);
 }
 
@@ -1013,6 +1022,7 @@ int mhd_ctx_destroy(mhd_ctx *ctx)
     {
         free_list(kv.second.full);
         free_list(kv.second.hot);
+        cudaFree(kv.second.dwalls);
     }
     free_resistive(ctx);
     for (auto &sp : ctx->spare)
@@ -1413,6 +1423,20 @@ static bool hot_point(const mhd_ctx *ctx, const PoolDecoder &dec, uint64_t off)
 int build_sync(mhd_ctx *ctx, const std::string &group, SyncMap &m)
 {
     RUN(upload_list(ctx, m.full, m.hcd, m.hcv, m.hd, m.hs, m.staged));
+    cudaFree(m.dwalls);
+    m.dwalls = nullptr;
+    m.wall_cols = 0;
+    std::vector<int> wv;
+    for (const auto &w : m.walls)
+    {
+        const BlockView &v = ctx->hbv[size_t(w.first)];
+        const int ax = std::abs(w.second) - 1;
+        const int64_t ncol = (ax == 0) ? int64_t(v.nj) * v.nk : (ax == 1) ? int64_t(v.ni) * v.nk : int64_t(v.ni) * v.nj;
+        m.wall_cols = std::max(m.wall_cols, ncol);
+        wv.push_back(w.first);
+        wv.push_back(w.second);
+    }
+    RUN(upload_vec(ctx, wv, &m.dwalls));
     const PoolDecoder dec(ctx);
     std::vector<uint64_t> d, s2, cd;
     std::vector<double> cv;
@@ -1465,7 +1489,7 @@ static int materialise_pv(mhd_ctx *ctx)
     RUN(ensure_geom(ctx));
     prof_begin(ctx, "k_pv_uplus_dt");
     k_pv_uplus_dt<<<dim3(grid_for(max_box(ctx, LOC_CELL, ctx->G)), ctx->nblocks), kThreads, 0, ctx->stream>>>(
-        ctx->dbv, ctx->c, nullptr, ctx->G);
+        ctx->dbv, ctx->c, nullptr, ctx->G, 0);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Uplus", true));
     ctx->pv_dirty = false;

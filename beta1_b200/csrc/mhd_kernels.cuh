@@ -35,13 +35,16 @@ __global__ void k_eres_explicit(const BlockView *bvs, double inver_Rem);
 __global__ void k_bcell(const BlockView *bvs);
 __global__ void k_jedge(const BlockView *bvs, int fB0, int fJ0, double mult, const int *rng);
 __global__ void k_jcell(const BlockView *bvs);
-__global__ void k_pv_uplus_dt(const BlockView *bvs, Consts c, unsigned long long *dt_key, int depth);
+__global__ void k_pv_uplus_dt(const BlockView *bvs, Consts c, unsigned long long *dt_key, int depth, int with_jcell);
+__global__ void k_bcell_jedge(const BlockView *bvs);
 __global__ void k_begin_step(const unsigned long long *dt_key, double *dt, int *err, double dt_abort);
 __global__ void k_arm_dt(unsigned long long *dt_key);
 __global__ void k_end_step(const double *dt, double *time, long long *step);
 __global__ void k_gather(double *pool, const uint64_t *dst, const uint64_t *src, int64_t n);
 __global__ void k_set_consts(double *pool, const uint64_t *dst, const double *val, int64_t n);
 __global__ void k_wall_u(const BlockView *bvs, int blk, int dir, double gamma);
+__global__ void k_wall_u_all(const BlockView *bvs, const int *walls, double gamma);
+__global__ void k_fluid_ucontra(const BlockView *bvs, Consts c);
 __global__ void k_gather_stage(double *tmp, const double *pool, const uint64_t *src, int64_t n);
 __global__ void k_scatter_stage(double *pool, const double *tmp, const uint64_t *dst, int64_t n);
 __global__ void k_aos_to_soa(const BlockView *bvs, int blk, int fid, int ncomp, int lo0, int lo1, int lo2, int n0,
@@ -73,12 +76,13 @@ struct GmresState
     int inner, outer;       // loop conditions (mirrors of the graph conditionals)
     long long total_its;    // cumulative over all solves
     long long total_cycles; // cumulative over all solves
+    unsigned int dot_done[32]; // CTAs finished per dot product (the last one sums the partials)
 };
-// dot products: partial[c * gridDim.x + cta] for c < nvec (nvec = *jdev + 1 when jdev is given);
-// V == nullptr computes w . w
-__global__ void k_dots_partial(const double *V, int64_t ldv, int nvec, const double *w, int64_t n, double *partial,
-                               const int *jdev);
-__global__ void k_dots_final(const double *partial, int ngroups, int nout, double *out, const int *jdev);
+// dot products out[c] = V_c . w for c < nvec (nvec = *jdev + 1 when jdev is
+// given); V == nullptr computes w . w.  Each CTA stores its partial sum; the
+// last CTA of each product adds the partials in a fixed order.
+__global__ void k_dots(const double *V, int64_t ldv, int nvec, const double *w, int64_t n, double *partial,
+                       const int *jdev, double *out, unsigned int *done);
 __global__ void k_sub_proj(const double *V, int64_t ldv, int nvec, const double *h, double *w, int64_t n,
                            const int *jdev);
 __global__ void k_add_small(double *a, const double *b, const int *jdev);

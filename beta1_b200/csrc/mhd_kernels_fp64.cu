@@ -134,14 +134,8 @@ __global__ void k_face_normals(const BlockView *__restrict__ bvs)
     N[3 * v + p] = az / A;
 }
 
-__global__ void k_fluid_rhs(const BlockView *__restrict__ bvs, Consts c, int64_t /*maxpts*/)
+__device__ __forceinline__ void fluid_one(const BlockView &b, const Consts &c, int i, int j, int k)
 {
-    const BlockView &b = bvs[blockIdx.y];
-    int lo[3], n[3];
-    loc_box(b, LOC_CELL, 0, lo, n);
-    int i, j, k;
-    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
-        return;
     const int64_t p = pidx(b, i, j, k);
     const int64_t v = b.vol;
     double Fm[5], Fp[5];
@@ -195,6 +189,17 @@ __global__ void k_fluid_rhs(const BlockView *__restrict__ bvs, Consts c, int64_t
         R[m * v + p] = r[m];
 }
 
+__global__ void k_fluid_rhs(const BlockView *__restrict__ bvs, Consts c, int64_t /*maxpts*/)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    int lo[3], n[3];
+    loc_box(b, LOC_CELL, 0, lo, n);
+    int i, j, k;
+    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+        return;
+    fluid_one(b, c, i, j, k);
+}
+
 // ---------------------------------------------------------------------------
 // AssembleOneDirectionEMF_ (Z4_Lunar/src/physics/LunarSolver_MagExplicit_Ideal.cpp:348-496)
 // ---------------------------------------------------------------------------
@@ -239,6 +244,26 @@ __global__ void k_ucontra(const BlockView *__restrict__ bvs)
     int i, j, k;
     if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
         return;
+    const int64_t p = pidx(b, i, j, k);
+    double *UC = b.f[F_UC];
+    UC[p] = u_contra(b, 0, i, j, k);
+    UC[b.vol + p] = u_contra(b, 1, i, j, k);
+    UC[2 * b.vol + p] = u_contra(b, 2, i, j, k);
+}
+
+// the fluid RHS of the inner cells and the contravariant velocities of the
+// cells within one ghost layer in one pass (both read JD and Jac around the
+// same cells; U_contra is read only by the EMF kernels that follow)
+__global__ void k_fluid_ucontra(const BlockView *__restrict__ bvs, Consts c)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    int lo[3], n[3];
+    loc_box(b, LOC_CELL, 1, lo, n);
+    int i, j, k;
+    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+        return;
+    if (i >= 0 && j >= 0 && k >= 0 && i < b.ni && j < b.nj && k < b.nk)
+        fluid_one(b, c, i, j, k);
     const int64_t p = pidx(b, i, j, k);
     double *UC = b.f[F_UC];
     UC[p] = u_contra(b, 0, i, j, k);
@@ -560,14 +585,8 @@ __global__ void k_update_u(const BlockView *__restrict__ bvs, const double *__re
 // ---------------------------------------------------------------------------
 // calc_Bcell (Z4_Lunar/src/physics/LunarSolver_Tools.cpp:163-241)
 // ---------------------------------------------------------------------------
-__global__ void k_bcell(const BlockView *__restrict__ bvs)
+__device__ __forceinline__ void bcell_one(const BlockView &b, int i, int j, int k)
 {
-    const BlockView &b = bvs[blockIdx.y];
-    int lo[3], n[3];
-    loc_box(b, LOC_CELL, 0, lo, n);
-    int i, j, k;
-    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
-        return;
     const double *Bx = b.f[F_Bxi], *Be = b.f[F_Beta], *Bz = b.f[F_Bzeta];
     const double *Ax = b.f[F_Baddxi], *Ae = b.f[F_Baddeta], *Az = b.f[F_Baddzeta];
     const int64_t p = pidx(b, i, j, k);
@@ -600,50 +619,7 @@ __global__ void k_bcell(const BlockView *__restrict__ bvs)
     Bi[2 * v + p] = bzi;
 }
 
-// ---------------------------------------------------------------------------
-// Calc_J_Edge: CTOperators::CurlAdjFaceToEdge (CTOperators.cpp:58-110) with
-// the face Hodge scale beta, times the edge scale alpha
-// (LunarSolver_Tools.cpp:777-835).
-// ---------------------------------------------------------------------------
-__global__ void k_jedge(const BlockView *__restrict__ bvs, int fB0, int fJ0, double mult, const int *__restrict__ rng)
-{
-    const BlockView &b = bvs[blockIdx.y];
-    int i, j, k;
-    if (!stagger_point(b, rng, blockIdx.y, i, j, k))
-        return;
-    const double *Fx = b.f[fB0], *Fe = b.f[fB0 + 1], *Fz = b.f[fB0 + 2];
-    const double *bx = b.f[F_betaxi], *be = b.f[F_betaeta], *bz = b.f[F_betazeta];
-    const int64_t c0 = pidx(b, i, j, k);
-#pragma unroll
-    for (int ea = 0; ea < 3; ++ea)
-    {
-        if (!inner_of(b, 1, ea, i, j, k))
-            continue;
-        double val;
-        if (ea == 0)
-        {
-            const int64_t a = pidx(b, i, j, k - 1), d = pidx(b, i, j - 1, k);
-            val = (be[a] * Fe[a] - be[c0] * Fe[c0]) + (bz[c0] * Fz[c0] - bz[d] * Fz[d]);
-        }
-        else if (ea == 1)
-        {
-            const int64_t a = pidx(b, i, j, k - 1), d = pidx(b, i - 1, j, k);
-            val = (bx[c0] * Fx[c0] - bx[a] * Fx[a]) + (bz[d] * Fz[d] - bz[c0] * Fz[c0]);
-        }
-        else
-        {
-            const int64_t a = pidx(b, i, j - 1, k), d = pidx(b, i - 1, j, k);
-            val = (bx[a] * Fx[a] - bx[c0] * Fx[c0]) + (be[c0] * Fe[c0] - be[d] * Fe[d]);
-        }
-        const double J = mult * val;
-        b.f[fJ0 + ea][c0] = J * b.f[F_alphaxi + ea][c0];
-    }
-}
-
-// ---------------------------------------------------------------------------
-// calc_Jcell (LunarSolver_Tools.cpp:837-892)
-// ---------------------------------------------------------------------------
-__global__ void k_jcell(const BlockView *__restrict__ bvs)
+__global__ void k_bcell(const BlockView *__restrict__ bvs)
 {
     const BlockView &b = bvs[blockIdx.y];
     int lo[3], n[3];
@@ -651,6 +627,74 @@ __global__ void k_jcell(const BlockView *__restrict__ bvs)
     int i, j, k;
     if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
         return;
+    bcell_one(b, i, j, k);
+}
+
+// ---------------------------------------------------------------------------
+// Calc_J_Edge: CTOperators::CurlAdjFaceToEdge (CTOperators.cpp:58-110) with
+// the face Hodge scale beta, times the edge scale alpha
+// (LunarSolver_Tools.cpp:777-835).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void jedge_one(const BlockView &b, int ea, int i, int j, int k, int fB0, int fJ0,
+                                          double mult)
+{
+    const double *Fx = b.f[fB0], *Fe = b.f[fB0 + 1], *Fz = b.f[fB0 + 2];
+    const double *bx = b.f[F_betaxi], *be = b.f[F_betaeta], *bz = b.f[F_betazeta];
+    const int64_t c0 = pidx(b, i, j, k);
+    double val;
+    if (ea == 0)
+    {
+        const int64_t a = pidx(b, i, j, k - 1), d = pidx(b, i, j - 1, k);
+        val = (be[a] * Fe[a] - be[c0] * Fe[c0]) + (bz[c0] * Fz[c0] - bz[d] * Fz[d]);
+    }
+    else if (ea == 1)
+    {
+        const int64_t a = pidx(b, i, j, k - 1), d = pidx(b, i - 1, j, k);
+        val = (bx[c0] * Fx[c0] - bx[a] * Fx[a]) + (bz[d] * Fz[d] - bz[c0] * Fz[c0]);
+    }
+    else
+    {
+        const int64_t a = pidx(b, i, j - 1, k), d = pidx(b, i - 1, j, k);
+        val = (bx[a] * Fx[a] - bx[c0] * Fx[c0]) + (be[c0] * Fe[c0] - be[d] * Fe[d]);
+    }
+    const double J = mult * val;
+    b.f[fJ0 + ea][c0] = J * b.f[F_alphaxi + ea][c0];
+}
+
+__global__ void k_jedge(const BlockView *__restrict__ bvs, int fB0, int fJ0, double mult, const int *__restrict__ rng)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    int i, j, k;
+    if (!stagger_point(b, rng, blockIdx.y, i, j, k))
+        return;
+#pragma unroll
+    for (int ea = 0; ea < 3; ++ea)
+        if (inner_of(b, 1, ea, i, j, k))
+            jedge_one(b, ea, i, j, k, fB0, fJ0, mult);
+}
+
+// calc_Bcell and Calc_J_Edge in one pass over the staggered points: both
+// read the face B around the same points (the B_cell sync between them in
+// the reference touches neither input)
+__global__ void k_bcell_jedge(const BlockView *__restrict__ bvs)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    int i, j, k;
+    if (!stagger_point(b, nullptr, 0, i, j, k))
+        return;
+    if (i < b.ni && j < b.nj && k < b.nk)
+        bcell_one(b, i, j, k);
+#pragma unroll
+    for (int ea = 0; ea < 3; ++ea)
+        if (inner_of(b, 1, ea, i, j, k))
+            jedge_one(b, ea, i, j, k, F_Bxi, F_Jxi, 1.0);
+}
+
+// ---------------------------------------------------------------------------
+// calc_Jcell (LunarSolver_Tools.cpp:837-892)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void jcell_one(const BlockView &b, int i, int j, int k)
+{
     const double *Jx = b.f[F_Jxi], *Je = b.f[F_Jeta], *Jz = b.f[F_Jzeta];
     const double s[12] = {Jx[pidx(b, i, j, k)],         Jx[pidx(b, i, j + 1, k)],     Jx[pidx(b, i, j, k + 1)],
                           Jx[pidx(b, i, j + 1, k + 1)], Je[pidx(b, i, j, k)],         Je[pidx(b, i + 1, j, k)],
@@ -671,6 +715,17 @@ __global__ void k_jcell(const BlockView *__restrict__ bvs)
     Jc[p] = jx;
     Jc[v + p] = jy;
     Jc[2 * v + p] = jz;
+}
+
+__global__ void k_jcell(const BlockView *__restrict__ bvs)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    int lo[3], n[3];
+    loc_box(b, LOC_CELL, 0, lo, n);
+    int i, j, k;
+    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+        return;
+    jcell_one(b, i, j, k);
 }
 
 // ---------------------------------------------------------------------------
@@ -715,7 +770,8 @@ __device__ __forceinline__ unsigned long long dbl_key(double x)
     return (unsigned long long)__double_as_longlong(x);
 }
 
-__global__ void k_pv_uplus_dt(const BlockView *__restrict__ bvs, Consts c, unsigned long long *dt_key, int depth)
+__global__ void k_pv_uplus_dt(const BlockView *__restrict__ bvs, Consts c, unsigned long long *dt_key, int depth,
+                              int with_jcell)
 {
     const BlockView &b = bvs[blockIdx.y];
     int lo[3], n[3];
@@ -724,6 +780,10 @@ __global__ void k_pv_uplus_dt(const BlockView *__restrict__ bvs, Consts c, unsig
     double dtc = 1e100;
     if (box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
     {
+        // calc_Jcell on inner cells in the same pass: its weight stream
+        // overlaps this kernel's FP64 work (J_cell is not read here)
+        if (with_jcell && i >= 0 && j >= 0 && k >= 0 && i < b.ni && j < b.nj && k < b.nk)
+            jcell_one(b, i, j, k);
         const int64_t p = pidx(b, i, j, k);
         const int64_t v = b.vol;
         const double *U = b.f[F_U];
@@ -863,15 +923,28 @@ __global__ void k_set_consts(double *__restrict__ pool, const uint64_t *__restri
 // cell layer takes the density of the next cell inwards (floored at 2.5e-3),
 // zero velocity and its pressure; every ghost layer then repeats that
 // layer's state.  One thread per boundary cell column; dir = +-1, +-2, +-3.
+__device__ __forceinline__ void wall_u_one(const BlockView &b, int dir, double gamma, int64_t t);
+
 __global__ void k_wall_u(const BlockView *__restrict__ bvs, int blk, int dir, double gamma)
 {
-    const BlockView &b = bvs[blk];
+    wall_u_one(bvs[blk], dir, gamma, int64_t(blockIdx.x) * blockDim.x + threadIdx.x);
+}
+
+// all Solid_Surface handlers of a sync in one launch: walls[2 q] = block,
+// walls[2 q + 1] = direction of handler q = blockIdx.y
+__global__ void k_wall_u_all(const BlockView *__restrict__ bvs, const int *__restrict__ walls, double gamma)
+{
+    const int q = blockIdx.y;
+    wall_u_one(bvs[walls[2 * q]], walls[2 * q + 1], gamma, int64_t(blockIdx.x) * blockDim.x + threadIdx.x);
+}
+
+__device__ __forceinline__ void wall_u_one(const BlockView &b, int dir, double gamma, int64_t t)
+{
     const int ax = (dir < 0 ? -dir : dir) - 1;
     const int sgn = dir > 0 ? 1 : -1;
     const int n[3] = {b.ni, b.nj, b.nk};
     const int t1 = (ax == 0) ? 1 : 0;
     const int t2 = (ax == 2) ? 1 : 2;
-    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= int64_t(n[t1]) * n[t2])
         return;
     int c[3];

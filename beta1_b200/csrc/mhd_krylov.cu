@@ -23,8 +23,9 @@ namespace mhd
 
 constexpr int kRedThreads = 256;
 
-__global__ void k_dots_partial(const double *__restrict__ V, int64_t ldv, int nvec, const double *__restrict__ w,
-                               int64_t n, double *__restrict__ partial, const int *__restrict__ jdev)
+__global__ void k_dots(const double *__restrict__ V, int64_t ldv, int nvec, const double *__restrict__ w, int64_t n,
+                       double *__restrict__ partial, const int *__restrict__ jdev, double *__restrict__ out,
+                       unsigned int *__restrict__ done)
 {
     const int c = blockIdx.y;
     const int nv = jdev ? jdev[0] + 1 : nvec;
@@ -35,6 +36,7 @@ __global__ void k_dots_partial(const double *__restrict__ V, int64_t ldv, int nv
     for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x)
         s += v[t] * w[t];
     __shared__ double red[kRedThreads];
+    __shared__ bool last;
     red[threadIdx.x] = s;
     __syncthreads();
     for (int off = blockDim.x / 2; off > 0; off >>= 1)
@@ -44,21 +46,31 @@ __global__ void k_dots_partial(const double *__restrict__ V, int64_t ldv, int nv
         __syncthreads();
     }
     if (threadIdx.x == 0)
+    {
         partial[int64_t(c) * gridDim.x + blockIdx.x] = red[0];
-}
-
-// out[c] = sum_b partial[c * ngroups + b] in a fixed order
-__global__ void k_dots_final(const double *__restrict__ partial, int ngroups, int nout, double *__restrict__ out,
-                             const int *__restrict__ jdev)
-{
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    const int no = jdev ? jdev[0] + 1 : nout;
-    if (c >= no)
+        __threadfence();
+        last = (atomicAdd(&done[c], 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last)
         return;
-    double s = 0.0;
-    for (int b = 0; b < ngroups; ++b)
-        s += partial[int64_t(c) * ngroups + b];
-    out[c] = s;
+    // the last CTA: partials of product c in a fixed order
+    double q = 0.0;
+    for (int b = threadIdx.x; b < int(gridDim.x); b += blockDim.x)
+        q += __ldcg(&partial[int64_t(c) * gridDim.x + b]);
+    red[threadIdx.x] = q;
+    __syncthreads();
+    for (int off = blockDim.x / 2; off > 0; off >>= 1)
+    {
+        if (threadIdx.x < off)
+            red[threadIdx.x] += red[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+    {
+        out[c] = red[0];
+        done[c] = 0u;
+    }
 }
 
 // w -= sum_c h[c] V_c
