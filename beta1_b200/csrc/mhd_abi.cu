@@ -86,7 +86,7 @@ const char *const kKernelNames[] = {
     "k_sub_proj",    "k_add_small",    "k_div_guard",    "k_div_next",      "k_gmres_init",
     "k_cycle_start",  "k_gmres_column", "k_inner_check", "k_gmres_solve_y", "k_add_basis",    "k_outer_check",
     "k_zero",         "k_residual",    "k_ucontra",      "k_face_normals", "k_divb",          "k_eres_explicit",
-    "k_bcell_jedge",  "k_fluid_ucontra", "k_wall_u_all"};
+    "k_bcell_jedge",  "k_fluid_ucontra", "k_wall_u_all",   "k_hall_cell",    "k_hall_edge"};
 constexpr int kNumKernelNames = int(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
 
 } // namespace
@@ -155,6 +155,10 @@ struct mhd_ctx
         bool graph_loops = true;                 // conditional graph nodes usable
         std::vector<uint64_t> seed;              // unknown and alias offsets (Eres), for the region
     } res;
+    // Hall edge EMF: coefficient and zero boxes (block, axis, lo[3], hi[3])
+    double hall_coef = 0.0;
+    int *hall_zb = nullptr;
+    int hall_nzb = 0;
     // explicit resistive sub-cycles (ResistiveDiffusionSubcycles_): 0 = off
     int res_nsub = 0;
     double res_inver_Rem = 0.0;
@@ -1025,6 +1029,7 @@ int mhd_ctx_destroy(mhd_ctx *ctx)
         cudaFree(kv.second.dwalls);
     }
     free_resistive(ctx);
+    cudaFree(ctx->hall_zb);
     for (auto &sp : ctx->spare)
         if (sp)
             cudaStreamDestroy(sp);
@@ -1801,6 +1806,29 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
     return MHD_OK;
 }
 
+int mhd_set_hall(mhd_ctx *ctx, double hall_coef, const int32_t *zero_boxes, int32_t nbox)
+{
+    if (!ctx || nbox < 0 || (nbox > 0 && !zero_boxes))
+        return fail(ctx, MHD_EINVAL, "bad Hall arguments");
+    for (int q = 0; q < nbox; ++q)
+    {
+        const int32_t *z = zero_boxes + 8 * q;
+        if (z[0] < 0 || z[0] >= ctx->nblocks || z[1] < 0 || z[1] > 2)
+            return fail(ctx, MHD_EINVAL, "Hall zero box %d: bad block or axis", q);
+    }
+    cudaFree(ctx->hall_zb);
+    ctx->hall_zb = nullptr;
+    ctx->hall_nzb = 0;
+    if (nbox > 0)
+    {
+        CK(ctx, cudaMalloc(&ctx->hall_zb, size_t(nbox) * 8 * sizeof(int)));
+        CK(ctx, cudaMemcpy(ctx->hall_zb, zero_boxes, size_t(nbox) * 8 * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    ctx->hall_nzb = nbox;
+    ctx->hall_coef = hall_coef;
+    return MHD_OK;
+}
+
 int mhd_set_resistive_explicit(mhd_ctx *ctx, double inver_Rem, int32_t nsub)
 {
     if (!ctx || nsub < 0)
@@ -1972,6 +2000,19 @@ int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
                                                                                          -1.0, ctx->dt, 1.0, 0, nullptr);
             RUN(launched(ctx));
         }
+        break;
+    case MHD_STAGE_HALL_EMF:
+        // the edge stencils read B_cell / J_cell one ghost layer deep
+        RUN(materialise_group(ctx, "B_cell"));
+        RUN(materialise_group(ctx, "J_cell"));
+        prof_begin(ctx, "k_hall_cell");
+        k_hall_cell<<<dim3(grid_for(max_box(ctx, LOC_CELL, ctx->G)), ctx->nblocks), kThreads, 0, ctx->stream>>>(
+            ctx->dbv, ctx->c, ctx->hall_coef);
+        RUN(launched(ctx));
+        prof_begin(ctx, "k_hall_edge");
+        k_hall_edge<<<dim3(grid_for(max_stagger(ctx)), ctx->nblocks), kThreads, 0, ctx->stream>>>(
+            ctx->dbv, ctx->hall_zb, ctx->hall_nzb);
+        RUN(launched(ctx));
         break;
     case MHD_STAGE_DIVB:
         prof_begin(ctx, "k_divb");

@@ -31,6 +31,8 @@ __global__ void k_curl_e2f(const BlockView *bvs, int fE0, int fR0, int fB0, doub
                            double dtdiv, int mult_is_neg_dt, const int *rng);
 __global__ void k_update_u(const BlockView *bvs, const double *dtp);
 __global__ void k_divb(const BlockView *bvs);
+__global__ void k_hall_cell(const BlockView *bvs, Consts c, double hall_coef);
+__global__ void k_hall_edge(const BlockView *bvs, const int *zb, int nzb);
 __global__ void k_eres_explicit(const BlockView *bvs, double inver_Rem);
 __global__ void k_bcell(const BlockView *bvs);
 __global__ void k_jedge(const BlockView *bvs, int fB0, int fJ0, double mult, const int *rng);

@@ -566,6 +566,117 @@ __global__ void k_eres_explicit(const BlockView *__restrict__ bvs, double inver_
     }
 }
 
+// ---------------------------------------------------------------------------
+// Hall edge EMF, BuildHallFaceEMF_Rusanov_diff_
+// (Z4_Lunar/src/physics/LunarSolver_MagExplicit_Hall.cpp:8-457)
+// ---------------------------------------------------------------------------
+
+// Ehc = alpha (J x B) and beta = |alpha| |B| on every cell of the array, with
+// alpha = hall_coef / ne_eff (Hall_Num_Limiter)
+__global__ void k_hall_cell(const BlockView *__restrict__ bvs, Consts c, double hall_coef)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    int lo[3], n[3];
+    loc_box(b, LOC_CELL, b.G, lo, n);
+    int i, j, k;
+    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+        return;
+    const int64_t p = pidx(b, i, j, k);
+    const int64_t v = b.vol;
+    const double n_true = smax(b.f[F_U][p], 0.0) / c.M_H * c.M_ref;
+    const double ne = sqrt(n_true * n_true + c.ne_floor * c.ne_floor);
+    const double alpha = hall_coef / ne;
+    const double *J = b.f[F_Jcell], *B = b.f[F_Bcell];
+    const double Jx = J[p], Jy = J[v + p], Jz = J[2 * v + p];
+    const double Bx = B[p], By = B[v + p], Bz = B[2 * v + p];
+    double *E = b.f[F_Ehc];
+    E[p] = alpha * (Jy * Bz - Jz * By);
+    E[v + p] = alpha * (Jz * Bx - Jx * Bz);
+    E[2 * v + p] = alpha * (Jx * By - Jy * Bx);
+    b.f[F_HallBeta][p] = fabs(alpha) * sqrt(Bx * Bx + By * By + Bz * Bz);
+}
+
+// one inner edge of axis ea: 4-cell mean of Ehc along dr, minus the
+// whistler diffusion of the two face-B jumps across the edge
+__device__ __forceinline__ double hall_edge_one(const BlockView &b, int ea, int i, int j, int k)
+{
+    const double eps = 1e-14, Cwh = 0.1;
+    const int64_t v = b.vol;
+    const int64_t p = pidx(b, i, j, k);
+    int64_t c[4];
+    int Fm, Fp, Am, Ap;
+    int64_t qm, qp, am, ap;
+    if (ea == 0)
+    {
+        c[0] = pidx(b, i, j - 1, k - 1);
+        c[1] = pidx(b, i, j - 1, k);
+        c[2] = pidx(b, i, j, k - 1);
+        c[3] = p;
+        Fm = F_Bzeta, qm = pidx(b, i, j - 1, k), Fp = F_Beta, qp = pidx(b, i, j, k - 1);
+        Am = F_Areazeta, am = pidx(b, i, j - 1, k), Ap = F_Areaeta, ap = pidx(b, i, j, k - 1);
+    }
+    else if (ea == 1)
+    {
+        c[0] = pidx(b, i - 1, j, k - 1);
+        c[1] = pidx(b, i - 1, j, k);
+        c[2] = pidx(b, i, j, k - 1);
+        c[3] = p;
+        Fm = F_Bxi, qm = pidx(b, i, j, k - 1), Fp = F_Bzeta, qp = pidx(b, i - 1, j, k);
+        Am = F_Areaxi, am = pidx(b, i, j, k - 1), Ap = F_Areazeta, ap = pidx(b, i - 1, j, k);
+    }
+    else
+    {
+        c[0] = pidx(b, i - 1, j - 1, k);
+        c[1] = pidx(b, i - 1, j, k);
+        c[2] = pidx(b, i, j - 1, k);
+        c[3] = p;
+        Fm = F_Beta, qm = pidx(b, i - 1, j, k), Fp = F_Bxi, qp = pidx(b, i, j - 1, k);
+        Am = F_Areaeta, am = pidx(b, i - 1, j, k), Ap = F_Areaxi, ap = pidx(b, i, j - 1, k);
+    }
+    const double *E = b.f[F_Ehc], *be = b.f[F_HallBeta];
+    const double Ecx = 0.25 * (E[c[0]] + E[c[1]] + E[c[2]] + E[c[3]]);
+    const double Ecy = 0.25 * (E[v + c[0]] + E[v + c[1]] + E[v + c[2]] + E[v + c[3]]);
+    const double Ecz = 0.25 * (E[2 * v + c[0]] + E[2 * v + c[1]] + E[2 * v + c[2]] + E[2 * v + c[3]]);
+    const double *dr = b.f[F_drxi + ea];
+    const double Ecen = Ecx * dr[p] + Ecy * dr[v + p] + Ecz * dr[2 * v + p];
+    const double beta_e = smax(smax(be[c[0]], be[c[1]]), smax(be[c[2]], be[c[3]]));
+    const double L = smax(b.f[F_dlxi + ea][p], eps);
+    const double Abar_m = 0.5 * (b.f[Am][p] + b.f[Am][am]);
+    const double inv_m = L / smax(Abar_m, eps);
+    const double mu_m = Cwh * beta_e * inv_m * inv_m;
+    const double Abar_p = 0.5 * (b.f[Ap][p] + b.f[Ap][ap]);
+    const double inv_p = L / smax(Abar_p, eps);
+    const double mu_p = Cwh * beta_e * inv_p * inv_p;
+    const double dB_m = b.f[Fm][p] - b.f[Fm][qm];
+    const double dB_p = b.f[Fp][p] - b.f[Fp][qp];
+    return Ecen - 0.5 * mu_m * dB_m + 0.5 * mu_p * dB_p;
+}
+
+// inner Hall edge EMF of all three axes; zero inside the boxes zb[8 q ..]:
+// block, edge axis, lo[3], hi[3] (Solid_Surface layers and Pole edges)
+__global__ void k_hall_edge(const BlockView *__restrict__ bvs, const int *__restrict__ zb, int nzb)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    int i, j, k;
+    if (!stagger_point(b, nullptr, 0, i, j, k))
+        return;
+    const int64_t p = pidx(b, i, j, k);
+#pragma unroll
+    for (int ea = 0; ea < 3; ++ea)
+    {
+        if (!inner_of(b, 1, ea, i, j, k))
+            continue;
+        bool zero = false;
+        for (int q = 0; q < nzb && !zero; ++q)
+        {
+            const int *z = zb + 8 * q;
+            zero = (z[0] == int(blockIdx.y) && z[1] == ea && i >= z[2] && j >= z[3] && k >= z[4] && i < z[5] &&
+                    j < z[6] && k < z[7]);
+        }
+        b.f[F_Ehxi + ea][p] = zero ? 0.0 : hall_edge_one(b, ea, i, j, k);
+    }
+}
+
 // cell part of ApplyUpdate_Euler_ (LunarSolver_Advance.cpp:82-93): U += dt*RHS_H
 __global__ void k_update_u(const BlockView *__restrict__ bvs, const double *__restrict__ dtp)
 {

@@ -78,7 +78,18 @@ namespace mhd
     X(NAeta, "Anorm_eta", 2, 4, 4)                         \
     X(NAzeta, "Anorm_zeta", 3, 4, 4)                       \
     X(Cs, "Csound_cell", 0, 1, 1)                          \
-    X(RhoE, "RhoE_cell", 0, 1, 1)
+    X(RhoE, "RhoE_cell", 0, 1, 1)                          \
+    X(Areaxi, "Area_xi", 1, 1, 3)                          \
+    X(Areaeta, "Area_eta", 2, 1, 3)                        \
+    X(Areazeta, "Area_zeta", 3, 1, 3)                      \
+    X(dlxi, "dl_xi", 4, 1, 3)                              \
+    X(dleta, "dl_eta", 5, 1, 3)                            \
+    X(dlzeta, "dl_zeta", 6, 1, 3)                          \
+    X(Ehxi, "Ehall_xi", 4, 1, 4)                           \
+    X(Eheta, "Ehall_eta", 5, 1, 4)                         \
+    X(Ehzeta, "Ehall_zeta", 6, 1, 4)                       \
+    X(Ehc, "Ehall_cell", 0, 3, 4)                          \
+    X(HallBeta, "hall_beta_cell", 0, 1, 4)
 
 enum FieldId : int
 {

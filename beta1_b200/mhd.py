@@ -26,7 +26,7 @@ NOALLOC_MAX_DOUBLES = 1 << 21
 PREC_FP64 = 0
 PREC_MIXED = 1
 
-STAGE_TIMESTEP, STAGE_FLUID_RHS, STAGE_INDUCTION, STAGE_UPDATE, STAGE_DIVB = 1, 2, 3, 4, 5
+STAGE_TIMESTEP, STAGE_FLUID_RHS, STAGE_INDUCTION, STAGE_UPDATE, STAGE_DIVB, STAGE_HALL_EMF = 1, 2, 3, 4, 5, 6
 
 
 class BlockDesc(C.Structure):
@@ -57,6 +57,7 @@ _SIGS = {
     "mhd_set_sync_wall": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_int32]),
     "mhd_set_resistive": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int32, C.c_int32]),
+    "mhd_set_hall": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_int32]),
     "mhd_set_resistive_explicit": (C.c_int, [C.c_void_p, C.c_double, C.c_int32]),
     "mhd_resistive_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double),
                                       C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
@@ -234,6 +235,10 @@ class Context:
         self._check(self.lib.mhd_set_resistive(self.h, u.size, u.ctypes.data, e.ctypes.data, a.size, a.ctypes.data,
                                                o.ctypes.data, sg.ctypes.data, rtol, atol, maxit, restart),
                     "set_resistive")
+
+    def set_hall(self, hall_coef: float, zero_boxes):
+        z = np.ascontiguousarray(np.asarray(zero_boxes, dtype=np.int32).reshape(-1, 8))
+        self._check(self.lib.mhd_set_hall(self.h, float(hall_coef), z.ctypes.data, len(z)), "set_hall")
 
     def set_resistive_explicit(self, inver_Rem: float, nsub: int):
         self._check(self.lib.mhd_set_resistive_explicit(self.h, float(inver_Rem), int(nsub)), "set_resistive_explicit")

@@ -11,7 +11,42 @@ from . import case as case_mod
 from . import edges, geometry, mhd, physics, rst, syncmap
 
 GEOM_FIELDS = ["Jac", "JDxi", "JDet", "JDze", "beta_xi", "beta_eta", "beta_zeta", "alpha_xi", "alpha_eta",
-               "alpha_zeta", "dr_xi", "dr_eta", "dr_zeta", "Bcell_from_Bface_w", "Jcell_from_Jedge_w"]
+               "alpha_zeta", "dr_xi", "dr_eta", "dr_zeta", "Bcell_from_Bface_w", "Jcell_from_Jedge_w", "Area_xi",
+               "Area_eta", "Area_zeta", "dl_xi", "dl_eta", "dl_zeta"]
+
+_EDGE_PLUS = {0: (0, 1, 1), 1: (1, 0, 1), 2: (1, 1, 0)}
+
+
+def hall_zero_boxes(ncell, patches):
+    """Edge boxes the Hall EMF zeroes (LunarSolver::BuildHallFaceEMF_Rusanov_diff_,
+    Z4_Lunar/src/physics/LunarSolver_MagExplicit_Hall.cpp:300-450): the node box
+    of every Solid_Surface patch widened 20 node layers inwards, and every Pole
+    patch's node box (eta edges for a xi-normal pole, xi edges for an
+    eta-normal pole, zeta edges always), as half-open edge boxes clipped to
+    the inner edges.  patches: (bc name, direction, node lo, node hi).
+    Returns rows (edge axis, lo[3], hi[3])."""
+    out = []
+    for name, direction, nlo, nhi in patches:
+        ax = abs(direction) - 1
+        for ea in range(3):
+            if name == "Pole":
+                if not ((abs(direction) == 1 and ea == 1) or (abs(direction) == 2 and ea == 0) or ea == 2):
+                    continue
+            elif name != "Solid_Surface":
+                continue
+            lo, hi = list(nlo), list(nhi)
+            if name == "Solid_Surface":
+                if direction < 0:
+                    hi[ax] += 20
+                else:
+                    lo[ax] -= 20
+            hi[ea] -= 1
+            plus = _EDGE_PLUS[ea]
+            lo = [max(lo[a], 0) for a in range(3)]
+            hi = [min(hi[a], ncell[a] + plus[a]) for a in range(3)]
+            if all(lo[a] < hi[a] for a in range(3)):
+                out.append([ea] + lo + hi)
+    return out
 STATE_FIELDS = ["U_H", "B_xi", "B_eta", "B_zeta"]
 
 
@@ -56,6 +91,7 @@ class Solver:
         else:
             raise ValueError(f"unknown topology {topology}")
         self.ctx.sync("Badd")
+        self.install_hall(topology)
         p = spec.params
         if float(p.get("arti_eta_max", 0.0)) > 0.0:
             raise NotImplementedError("the artificial-resistivity edge EMF is not supported by this build")
@@ -88,6 +124,17 @@ class Solver:
                                float(p["implicit_resistive_ksp_rtol"]), float(p["implicit_resistive_ksp_atol"]),
                                int(p["implicit_resistive_ksp_max_it"]), 30)
         self.resistive_dofs = (dofs, eta)
+
+    def install_hall(self, topology):
+        """Hall coefficient and the Hall EMF's zeroed edge boxes: the tiled
+        slab has a Solid_Surface patch on the i-minimum face of every block,
+        the periodic box has no physical patch."""
+        rows = []
+        for ib, b in enumerate(self.spec.blocks):
+            n = b.ncell
+            patches = [("Solid_Surface", -1, (0, 0, 0), (1, n[1] + 1, n[2] + 1))] if topology == "tiled" else []
+            rows += [[ib] + r for r in hall_zero_boxes(n, patches)]
+        self.ctx.set_hall(physics.constants(self.spec.params)["hall_coef"], rows)
 
     def install_explicit_resistive(self):
         """Shell profile of every inner edge and the sub-cycle count of

@@ -167,6 +167,16 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
                       const int64_t *alias, const int64_t *owner, const double *sign, double rtol, double atol,
                       int32_t maxit, int32_t restart);
 
+/* Hall edge EMF set-up (LunarSolver::BuildHallFaceEMF_Rusanov_diff_,
+   Z4_Lunar/src/physics/LunarSolver_MagExplicit_Hall.cpp:8-457): the Hall
+   coefficient (hall_coef of calc_physical_constant) and the edge boxes the
+   reference zeroes, 8 int32 each: block, edge axis (0/1/2 = xi/eta/zeta),
+   lo[3], hi[3] (half-open, inner edge indices) -- the Solid_Surface node box
+   widened 20 layers inwards and the Pole node boxes, turned into edge boxes.
+   The geometry fields Area_* and dl_* must be uploaded.  MHD_STAGE_HALL_EMF
+   then computes Ehall_xi / Ehall_eta / Ehall_zeta of the current state. */
+int mhd_set_hall(mhd_ctx *ctx, double hall_coef, const int32_t *zero_boxes, int32_t nbox);
+
 /* Explicit resistive sub-cycles (LunarSolver::ResistiveDiffusionSubcycles_,
    Z4_Lunar/src/physics/LunarSolver_MagneticRHS.cpp:53-115, with the edge EMF of
    AddResistiveEdgeEMF_To_, Z4_Lunar/src/physics/LunarSolver_MagExplicit_Resis.cpp:67-209):
@@ -217,6 +227,7 @@ int mhd_host_free(void *ptr);
 #define MHD_STAGE_INDUCTION 3  /* AssembleRHS_Induction_CT_ -> Eface, E, RHS_B */
 #define MHD_STAGE_UPDATE 4     /* ApplyUpdate_Euler_ with the current dt */
 #define MHD_STAGE_DIVB 5       /* calc_divB -> divB (inner cells; no Pole patches) */
+#define MHD_STAGE_HALL_EMF 6   /* BuildHallFaceEMF_Rusanov_diff_ -> Ehall_xi/eta/zeta (see mhd_set_hall) */
 int mhd_stage(mhd_ctx *ctx, int32_t stage_id);
 
 /* Current dt / time / step counters (device -> host). */

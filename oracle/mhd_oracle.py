@@ -34,6 +34,8 @@ FIELDS = {
     "dB_xi": (1, 1, 4), "dB_eta": (2, 1, 4), "dB_zeta": (3, 1, 4), "dJ_xi": (4, 1, 4), "dJ_eta": (5, 1, 4),
     "dJ_zeta": (6, 1, 4), "RHS_Bres_xi": (1, 1, 0), "RHS_Bres_eta": (2, 1, 0), "RHS_Bres_zeta": (3, 1, 0),
     "divB": (0, 1, 1), "dr_xi": (4, 3, 3), "dr_eta": (5, 3, 3), "dr_zeta": (6, 3, 3),
+    "Area_xi": (1, 1, 3), "Area_eta": (2, 1, 3), "Area_zeta": (3, 1, 3), "dl_xi": (4, 1, 3), "dl_eta": (5, 1, 3),
+    "dl_zeta": (6, 1, 3), "Ehall_xi": (4, 1, 4), "Ehall_eta": (5, 1, 4), "Ehall_zeta": (6, 1, 4),
 }
 PLUS = {0: (0, 0, 0), 1: (1, 0, 0), 2: (0, 1, 0), 3: (0, 0, 1), 4: (0, 1, 1), 5: (1, 0, 1), 6: (1, 1, 0)}
 
@@ -727,3 +729,96 @@ class Oracle:
                     lo, hi = blk.inner(1 + fa)
                     blk.f[bn][0][blk.s(lo, hi)] += dt_res * blk.box(rn, 0, lo, hi)
             self.sync("Bface")
+
+    # ------------------------------------------------------------ Hall EMF
+    @staticmethod
+    def hall_zero_boxes(n, patches):
+        """Edge boxes (axis, lo, hi) that BuildHallFaceEMF_Rusanov_diff_ zeroes
+        (Z4_Lunar/src/physics/LunarSolver_MagExplicit_Hall.cpp:300-450): the
+        node box of every Solid_Surface patch widened 20 layers inwards, and
+        of every Pole patch, turned into edge boxes and clipped to the inner
+        edges.  patches: (bc name, direction, node lo, node hi)."""
+        out = []
+        for name, direction, nlo, nhi in patches:
+            ax = abs(direction) - 1
+            for ea in range(3):
+                if name == "Pole":
+                    if not ((abs(direction) == 1 and ea == 1) or (abs(direction) == 2 and ea == 0) or ea == 2):
+                        continue
+                elif name != "Solid_Surface":
+                    continue
+                lo, hi = list(nlo), list(nhi)
+                if name == "Solid_Surface":
+                    if direction < 0:
+                        hi[ax] += 20
+                    else:
+                        lo[ax] -= 20
+                hi[ea] -= 1
+                plus = PLUS[4 + ea]
+                lo = [max(lo[a], 0) for a in range(3)]
+                hi = [min(hi[a], n[a] + plus[a]) for a in range(3)]
+                if all(lo[a] < hi[a] for a in range(3)):
+                    out.append((ea, tuple(lo), tuple(hi)))
+        return out
+
+    def hall_emf(self, blk, hall_coef, zero_boxes=()):
+        """BuildHallFaceEMF_Rusanov_diff_ (Z4_Lunar/src/physics/LunarSolver_MagExplicit_Hall.cpp:8-457):
+        Ehc = alpha (J x B) and beta = |alpha| |B| on every cell of the array
+        (alpha = hall_coef / ne_eff of Hall_Num_Limiter), then per inner edge the
+        4-cell mean of Ehc along dr minus the whistler diffusion of the face-B
+        jumps, zeroed in zero_boxes."""
+        c = self.c
+        G = blk.G
+        ng = FIELDS["B_cell"][2]
+        n = blk.n
+        lo, hi = (-ng, -ng, -ng), (n[0] + ng, n[1] + ng, n[2] + ng)
+        rho = blk.box("U_H", 0, lo, hi)
+        n_true = smax(rho, 0.0) / c["M_H"] * c["M_ref"]
+        ne = np.sqrt(n_true * n_true + c["ne_hall_floor"] * c["ne_hall_floor"])
+        alpha = hall_coef / ne
+        Jx, Jy, Jz = (blk.box("J_cell", q, lo, hi) for q in range(3))
+        Bx, By, Bz = (blk.box("B_cell", q, lo, hi) for q in range(3))
+        shape = blk.f["B_cell"][0].shape
+        Ehc = np.zeros((3,) + shape)
+        beta = np.zeros(shape)
+        sl = blk.s(lo, hi)
+        Ehc[0][sl] = alpha * (Jy * Bz - Jz * By)
+        Ehc[1][sl] = alpha * (Jz * Bx - Jx * Bz)
+        Ehc[2][sl] = alpha * (Jx * By - Jy * Bx)
+        beta[sl] = np.abs(alpha) * np.sqrt(Bx * Bx + By * By + Bz * Bz)
+        eps, Cwh = 1e-14, 0.1
+        # per edge axis: the 4 cells, the two transverse axes (t1, t2) and
+        # the face areas that give h_t1 and h_t2
+        spec = {0: ([(0, -1, -1), (0, -1, 0), (0, 0, -1), (0, 0, 0)], "B_zeta", (0, -1, 0), "B_eta", (0, 0, -1),
+                    "Area_zeta", (0, -1, 0), "Area_eta", (0, 0, -1), "dl_xi", "dr_xi"),
+                1: ([(-1, 0, -1), (-1, 0, 0), (0, 0, -1), (0, 0, 0)], "B_xi", (0, 0, -1), "B_zeta", (-1, 0, 0),
+                    "Area_xi", (0, 0, -1), "Area_zeta", (-1, 0, 0), "dl_eta", "dr_eta"),
+                2: ([(-1, -1, 0), (-1, 0, 0), (0, -1, 0), (0, 0, 0)], "B_eta", (-1, 0, 0), "B_xi", (0, -1, 0),
+                    "Area_eta", (-1, 0, 0), "Area_xi", (0, -1, 0), "dl_zeta", "dr_zeta")}
+        for ea in range(3):
+            cells, Bm, dm, Bp, dp, Am, dAm, Ap, dAp, dln, drn = spec[ea]
+            elo, ehi = blk.inner(4 + ea)
+            cbox = lambda arr, d: arr[blk.sh(elo, ehi, d)]
+            Ec = []
+            for q in range(3):
+                a, b_, c2, d2 = (cbox(Ehc[q], d) for d in cells)
+                Ec.append(0.25 * (a + b_ + c2 + d2))
+            Ecen = Ec[0] * blk.box(drn, 0, elo, ehi) + Ec[1] * blk.box(drn, 1, elo, ehi) + Ec[2] * blk.box(drn, 2, elo, ehi)
+            b0, b1, b2, b3 = (cbox(beta, d) for d in cells)
+            beta_e = smax(smax(b0, b1), smax(b2, b3))
+            L = smax(blk.box(dln, 0, elo, ehi), eps)
+            z = (0, 0, 0)
+            Abar_m = 0.5 * (blk.box(Am, 0, elo, ehi) + blk.box(Am, 0, elo, ehi, dAm))
+            inv_m = L / smax(Abar_m, eps)
+            mu_m = Cwh * beta_e * inv_m * inv_m
+            Abar_p = 0.5 * (blk.box(Ap, 0, elo, ehi) + blk.box(Ap, 0, elo, ehi, dAp))
+            inv_p = L / smax(Abar_p, eps)
+            mu_p = Cwh * beta_e * inv_p * inv_p
+            dB_m = blk.box(Bm, 0, elo, ehi) - blk.box(Bm, 0, elo, ehi, dm)
+            dB_p = blk.box(Bp, 0, elo, ehi) - blk.box(Bp, 0, elo, ehi, dp)
+            E = Ecen - 0.5 * mu_m * dB_m + 0.5 * mu_p * dB_p
+            name = ("Ehall_xi", "Ehall_eta", "Ehall_zeta")[ea]
+            blk.f[name][0][blk.s(elo, ehi)] = E
+            for (za, zlo, zhi) in zero_boxes:
+                if za == ea:
+                    blk.f[name][0][blk.s(zlo, zhi)] = 0.0

@@ -11,6 +11,7 @@
 //   ref_lunar geom  <out.bin>                      geometry + node coordinates
 //   ref_lunar run   <state.rst> <nsteps> <prefix>  state after each StepOnce
 //   ref_lunar probe <state.rst> <group> <out.bin>  index-encoded Sync(group)
+//   ref_lunar hall <state.rst> <out.bin>           Hall edge EMF of the state
 //   ref_lunar time  <state.rst> <nsteps>           wall time of the step loop
 //
 // The member functions are private in the reference; this translation unit
@@ -458,6 +459,21 @@ int cmd_owners(Harness &h, const std::string &out)
     return 0;
 }
 
+// The Hall edge EMF of a state (LunarSolver::BuildHallFaceEMF_Rusanov_diff_,
+// after the derived fields), with the fields it reads.
+int cmd_hall(Harness &h, const std::string &state, const std::string &out)
+{
+    h.load_state(state);
+    LunarSolver &s = *h.solver;
+    s.UpdateDerivedFields_();
+    s.BuildHallFaceEMF_Rusanov_diff_();
+    std::vector<DumpItem> items;
+    for (const char *n : {"Ehall_xi", "Ehall_eta", "Ehall_zeta", "B_cell", "J_cell", "U_H", "B_xi", "B_eta", "B_zeta"})
+        items.push_back(field_item(h.fld, n));
+    write_dump(out, 0, 0.0, h.fld->num_blocks(), items);
+    return 0;
+}
+
 int cmd_time(Harness &h, const std::string &state, int nsteps)
 {
     h.load_state(state);
@@ -517,6 +533,8 @@ int main(int argc, char **argv)
             rc = cmd_topo(h, argv[2]);
         else if (cmd == "owners")
             rc = cmd_owners(h, argv[2]);
+        else if (cmd == "hall" && argc >= 4)
+            rc = cmd_hall(h, argv[2], argv[3]);
         else if (cmd == "geom")
             rc = cmd_geom(h, argv[2]);
         else if (cmd == "run" && argc >= 5)

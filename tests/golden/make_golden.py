@@ -116,6 +116,38 @@ def slab(nr=6, nt=(5, 6), tiles=(2, 2), steps=2, resistive=0, implicit=0, seed=2
     print("wrote", tag)
 
 
+def hall(spec_kind, seed=20261205):
+    """The reference's Hall edge EMF (BuildHallFaceEMF_Rusanov_diff_) of a
+    seeded state: a periodic box (no walls) and a slab whose Solid_Surface
+    zeroing reaches 20 node layers into the block."""
+    if spec_kind == "periodic":
+        spec = case.periodic_box_case((8, 6, 5))
+        st = case.initial_state(spec, seed=seed)
+        tag = "hall_periodic_8x6x5"
+    else:
+        spec = case.slab_case(24, (5, 6), (2, 2))
+        st = case.inflow_state(spec, seed=seed)
+        tag = "hall_slab_24x5x6_t2x2"
+    with tempfile.TemporaryDirectory() as d:
+        case.write_case(d, spec)
+        rst.write(os.path.join(d, "init.rst"), st)
+        run(["hall", "init.rst", "hall.bin"], d)
+        r = rst.read(os.path.join(d, "hall.bin"))
+        arr = {}
+        for b in range(len(spec.blocks)):
+            for name in ("U_H", "B_xi", "B_eta", "B_zeta"):
+                fa = st.fields[name].blocks[b]
+                arr["init/b%d/%s" % (b, name)] = fa.data
+                arr["init/b%d/%s__lo" % (b, name)] = np.array(fa.lo, dtype=np.int32)
+            for name in ("Ehall_xi", "Ehall_eta", "Ehall_zeta", "B_cell", "J_cell", "U_H", "B_xi", "B_eta", "B_zeta"):
+                fa = r.fields[name].blocks[b]
+                arr["b%d/%s" % (b, name)] = fa.data
+                arr["b%d/%s__lo" % (b, name)] = np.array(fa.lo, dtype=np.int32)
+        arr["kind"] = np.array(spec_kind)
+        np.savez_compressed(os.path.join(OUT, tag + ".npz"), **arr)
+    print("wrote", tag)
+
+
 def slab_probe(nr=6, nt=(5, 6), tiles=(2, 2), resistive=0, seed=20261204):
     """Every Sync group of a tiled slab probed on the reference: for each
     (group, field, block) the offsets whose value the Sync changed and the
@@ -183,4 +215,6 @@ if __name__ == "__main__":
          * case.ref_scales()["L_ref"], n_resistive_subcycles=2)
     slab_probe(resistive=0)
     slab_probe(resistive=1)
+    hall("periodic")
+    hall("slab")
     slab_owners(eta_max_lunar=1.0 * case.MU0 * case.ref_scales()["U"] * case.ref_scales()["L_ref"])

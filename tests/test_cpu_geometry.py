@@ -8,7 +8,8 @@ import numpy as np
 from beta1_b200 import case, geometry
 
 FIELDS = ["Jac", "JDxi", "JDet", "JDze", "beta_xi", "beta_eta", "beta_zeta", "alpha_xi", "alpha_eta",
-          "alpha_zeta", "dr_xi", "dr_eta", "dr_zeta", "Bcell_from_Bface_w", "Jcell_from_Jedge_w"]
+          "alpha_zeta", "dr_xi", "dr_eta", "dr_zeta", "Bcell_from_Bface_w", "Jcell_from_Jedge_w", "Area_xi", "Area_eta",
+          "Area_zeta", "dl_xi", "dl_eta", "dl_zeta"]
 
 
 def test_ghost_nodes_bitwise(golden_periodic):
