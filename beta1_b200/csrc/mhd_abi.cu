@@ -86,7 +86,8 @@ const char *const kKernelNames[] = {
     "k_sub_proj",    "k_add_small",    "k_div_guard",    "k_div_next",      "k_gmres_init",
     "k_cycle_start",  "k_gmres_column", "k_inner_check", "k_gmres_solve_y", "k_add_basis",    "k_outer_check",
     "k_zero",         "k_residual",    "k_ucontra",      "k_face_normals", "k_divb",          "k_eres_explicit",
-    "k_bcell_jedge",  "k_fluid_ucontra", "k_wall_u_all",   "k_hall_cell",    "k_hall_edge"};
+    "k_bcell_jedge",  "k_fluid_ucontra", "k_wall_u_all",   "k_hall_cell",    "k_hall_edge",
+    "k_pack_vec",     "k_hall_residual", "k_axpy_to",      "k_fd_quotient",  "k_negate"};
 constexpr int kNumKernelNames = int(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
 
 } // namespace
@@ -155,6 +156,29 @@ struct mhd_ctx
         bool graph_loops = true;                 // conditional graph nodes usable
         std::vector<uint64_t> seed;              // unknown and alias offsets (Eres), for the region
     } res;
+    // implicit Hall solve (ImplicitHallSolver::SolveOneStep): Newton on
+    // F(X) = X - Ehall(B* - theta dt curl X) over the inner Hall edges of
+    // every block, GMRES on finite-difference Jacobian-vector products
+    struct HallImplicit
+    {
+        bool on = false;
+        int64_t n = 0;
+        uint64_t *e = nullptr;                     // pool offsets of the unknowns (owner Hall edges)
+        int64_t nalias = 0;                        // alias <- sign * owner (edge 1-form sync)
+        uint64_t *alias = nullptr, *owner = nullptr;
+        double *sign = nullptr;
+        double rtol = 1e-8, atol = 1e-50;          // Newton stopping test (PETSc SNES defaults)
+        int maxit = 50;
+        double ksp_rtol = 1e-5;                    // linear solves (PETSc KSP default)
+        int ksp_maxit = 10000, restart = 30;
+        double *bstar = nullptr;                   // snapshot of the face B arrays
+        double *X = nullptr, *F = nullptr, *Xt = nullptr, *Ft = nullptr, *dx = nullptr, *b = nullptr, *r = nullptr;
+        double *V = nullptr, *w = nullptr, *partial = nullptr, *dots = nullptr;
+        GmresState *st = nullptr;
+        int ngroups = 1;
+        int its = 0, lin_its = 0, reason = 0;      // statistics of the last solve
+        double fnorm = 0.0, fnorm0 = 0.0;
+    } hall;
     // Hall edge EMF: coefficient and zero boxes (block, axis, lo[3], hi[3])
     double hall_coef = 0.0;
     int *hall_zb = nullptr;
@@ -613,6 +637,13 @@ int gmres_cycle_end(mhd_ctx *ctx, cudaGraphConditionalHandle h, int use)
     return MHD_OK;
 }
 
+int read_scalar(mhd_ctx *ctx, const double *dev, double *host)
+{
+    CK(ctx, cudaMemcpyAsync(host, dev, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return MHD_OK;
+}
+
 int read_flag(mhd_ctx *ctx, const int *dev, int *host)
 {
     CK(ctx, cudaMemcpyAsync(host, dev, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -806,6 +837,248 @@ int launch_resistive_explicit(mhd_ctx *ctx)
     return MHD_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Implicit Hall solve (ImplicitHallSolver::SolveOneStep,
+// Z4_Lunar/src/implicit/Hall_Implicit_Solver.cpp:268-391, residual of
+// Hall_Implicit_Formfunction.cpp:7-106).  Newton with a backtracking line
+// search; each Newton system J dx = -F solved by restarted GMRES whose
+// products J v are finite differences of F (the reference uses an
+// approximate whistler Jacobian; both converge to the root of F).  Driven
+// from the host: one scalar read per Krylov iteration.
+// ---------------------------------------------------------------------------
+
+// B <- B* (restore) or B* <- B (snapshot), the whole face B arrays
+int hall_snapshot(mhd_ctx *ctx, bool restore)
+{
+    auto &H = ctx->hall;
+    size_t off = 0;
+    for (int f = F_Bxi; f <= F_Bzeta; ++f)
+        for (int b = 0; b < ctx->nblocks; ++b)
+        {
+            const size_t n = size_t(ctx->hbv[size_t(b)].vol);
+            double *field = ctx->pool + ctx->base[size_t(f)][size_t(b)];
+            if (restore)
+                CK(ctx, cudaMemcpyAsync(field, H.bstar + off, n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+            else
+                CK(ctx, cudaMemcpyAsync(H.bstar + off, field, n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+            off += n;
+        }
+    return MHD_OK;
+}
+
+// UpdateMagneticDerivedFields_ with the B_cell / J_cell ghosts the Hall
+// stencils read, then the Hall edge EMF
+int hall_emf_from_current_b(mhd_ctx *ctx)
+{
+    const int nb = ctx->nblocks;
+    cudaStream_t s = ctx->stream;
+    prof_begin(ctx, "k_bcell");
+    k_bcell<<<dim3(grid_for(max_box(ctx, LOC_CELL, 0)), nb), kThreads, 0, s>>>(ctx->dbv);
+    RUN(launched(ctx));
+    RUN(run_sync(ctx, "B_cell", true));
+    prof_begin(ctx, "k_jedge");
+    k_jedge<<<dim3(grid_for(max_stagger(ctx)), nb), kThreads, 0, s>>>(ctx->dbv, F_Bxi, F_Jxi, 1.0, nullptr);
+    RUN(launched(ctx));
+    RUN(run_sync(ctx, "Jedge"));
+    prof_begin(ctx, "k_jcell");
+    k_jcell<<<dim3(grid_for(max_box(ctx, LOC_CELL, 0)), nb), kThreads, 0, s>>>(ctx->dbv);
+    RUN(launched(ctx));
+    RUN(run_sync(ctx, "J_cell", true));
+    prof_begin(ctx, "k_hall_cell");
+    k_hall_cell<<<dim3(grid_for(max_box(ctx, LOC_CELL, ctx->G)), nb), kThreads, 0, s>>>(ctx->dbv, ctx->c,
+                                                                                        ctx->hall_coef);
+    RUN(launched(ctx));
+    prof_begin(ctx, "k_hall_edge");
+    k_hall_edge<<<dim3(grid_for(max_stagger(ctx)), nb), kThreads, 0, s>>>(ctx->dbv, ctx->hall_zb, ctx->hall_nzb);
+    return launched(ctx);
+}
+
+// Ehall <- X, Sync("Ehall"), B = B* + dt (-curl Ehall) on inner faces (theta = 1), Sync("Bface")
+int hall_trial_b(mhd_ctx *ctx, const double *X)
+{
+    auto &H = ctx->hall;
+    RUN(hall_snapshot(ctx, true));
+    // UnpackVecToEhallField_: owners, then their aliases
+    LAUNCHN(k_scatter_vec, H.n, ctx->pool, H.e, X, H.n, nullptr, H.n);
+    if (H.nalias > 0)
+        LAUNCHN(k_alias_copy, H.nalias, ctx->pool, H.alias, H.owner, H.sign, H.nalias);
+    RUN(run_sync(ctx, "Ehall", true));
+    prof_begin(ctx, "k_curl_e2f");
+    k_curl_e2f<<<dim3(grid_for(max_stagger(ctx)), ctx->nblocks), kThreads, 0, ctx->stream>>>(
+        ctx->dbv, F_Ehxi, F_RBxi, F_Bxi, -1.0, ctx->dt, 1.0, 0, nullptr);
+    RUN(launched(ctx));
+    return run_sync(ctx, "Bface");
+}
+
+// F = X - Ehall(trial B of X)   (FormFunction_)
+int hall_residual(mhd_ctx *ctx, const double *X, double *F)
+{
+    auto &H = ctx->hall;
+    RUN(hall_trial_b(ctx, X));
+    RUN(hall_emf_from_current_b(ctx));
+    LAUNCHN(k_hall_residual, H.n, ctx->pool, H.e, X, F, H.n);
+    return MHD_OK;
+}
+
+int hall_dots(mhd_ctx *ctx, const double *V, int nvec, const int *jdev, const double *w, double *out)
+{
+    auto &H = ctx->hall;
+    const int ny = jdev ? H.restart + 1 : nvec;
+    prof_begin(ctx, "k_dots");
+    k_dots<<<dim3(H.ngroups, ny), 256, 0, ctx->stream>>>(V, H.n, nvec, w, H.n, H.partial, jdev, out, H.st->dot_done);
+    return launched(ctx);
+}
+
+int hall_norm(mhd_ctx *ctx, const double *x, double *out)
+{
+    auto &H = ctx->hall;
+    RUN(hall_dots(ctx, nullptr, 1, nullptr, x, H.dots + 48));
+    double v = 0.0;
+    RUN(read_scalar(ctx, H.dots + 48, &v));
+    *out = std::sqrt(v);
+    return MHD_OK;
+}
+
+// w = J v by a forward difference around X (F = F(X) given)
+int hall_jv(mhd_ctx *ctx, const double *v, double vnorm, double xnorm, double *w)
+{
+    auto &H = ctx->hall;
+    if (vnorm <= 0.0)
+    {
+        LAUNCHN(k_zero, H.n, w, H.n);
+        return MHD_OK;
+    }
+    const double h = std::sqrt(2.220446049250313e-16) * (1.0 + xnorm) / vnorm;
+    LAUNCHN(k_axpy_to, H.n, H.Xt, H.X, h, v, H.n);
+    RUN(hall_residual(ctx, H.Xt, H.Ft));
+    LAUNCHN(k_fd_quotient, H.n, w, H.Ft, H.F, h, H.n);
+    return MHD_OK;
+}
+
+// restarted GMRES for J dx = -F (x0 = 0), the kernels of the resistive solve
+int hall_gmres(mhd_ctx *ctx, double xnorm)
+{
+    auto &H = ctx->hall;
+    LAUNCHN(k_negate, H.n, H.b, H.F, H.n);
+    RUN(hall_dots(ctx, nullptr, 1, nullptr, H.b, H.dots + 40));
+    LAUNCH1(k_gmres_init, H.st, H.dots + 40, H.ksp_rtol, 0.0, H.ksp_maxit, H.restart);
+    LAUNCHN(k_zero, H.n, H.dx, H.n);
+    bool first = true;
+    int outer = 1;
+    while (outer)
+    {
+        if (first)
+            CK(ctx, cudaMemcpyAsync(H.r, H.b, size_t(H.n) * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        else
+        {
+            double dn = 0.0;
+            RUN(hall_norm(ctx, H.dx, &dn));
+            RUN(hall_jv(ctx, H.dx, dn, xnorm, H.w));
+            LAUNCHN(k_residual, H.n, H.b, H.w, H.r, H.n);
+        }
+        first = false;
+        RUN(hall_dots(ctx, nullptr, 1, nullptr, H.r, H.dots));
+        LAUNCH1(k_cycle_start, H.st, H.dots, 0, 0);
+        LAUNCHN(k_div_guard, H.n, H.V, H.r, &H.st->beta, H.n, &H.st->inner);
+        int inner = 0;
+        RUN(read_flag(ctx, &H.st->inner, &inner));
+        int j = 0;
+        while (inner)
+        {
+            // basis vectors have unit norm
+            RUN(hall_jv(ctx, H.V + int64_t(j) * H.n, 1.0, xnorm, H.w));
+            const int *jd = &H.st->j;
+            double *hcol = H.st->hcol;
+            RUN(hall_dots(ctx, H.V, 0, jd, H.w, hcol));
+            LAUNCHN(k_sub_proj, H.n, H.V, H.n, 0, hcol, H.w, H.n, jd);
+            RUN(hall_dots(ctx, H.V, 0, jd, H.w, H.dots));
+            LAUNCHN(k_sub_proj, H.n, H.V, H.n, 0, H.dots, H.w, H.n, jd);
+            prof_begin(ctx, "k_add_small");
+            k_add_small<<<1, 32, 0, ctx->stream>>>(hcol, H.dots, jd);
+            RUN(launched(ctx));
+            RUN(hall_dots(ctx, nullptr, 1, nullptr, H.w, H.dots + 32));
+            LAUNCH1(k_gmres_column, H.st, H.dots + 32);
+            LAUNCHN(k_div_next, H.n, H.V, H.n, H.w, H.st, H.n);
+            LAUNCH1(k_inner_check, H.st, 0, 0);
+            ++j;
+            ++H.lin_its;
+            RUN(read_flag(ctx, &H.st->inner, &inner));
+        }
+        LAUNCH1(k_gmres_solve_y, H.st);
+        LAUNCHN(k_add_basis, H.n, H.V, H.n, H.st, H.dx, H.n);
+        LAUNCH1(k_outer_check, H.st, 0, 0);
+        RUN(read_flag(ctx, &H.st->outer, &outer));
+    }
+    return MHD_OK;
+}
+
+// One implicit Hall solve at the current dt: Newton on F from the current
+// Ehall (the reference's initial guess), then B = B* + dt (-curl Ehall) and
+// Sync("Bface")
+int launch_hall_implicit(mhd_ctx *ctx)
+{
+    auto &H = ctx->hall;
+    if (!H.on || H.n == 0)
+        return MHD_OK;
+    RUN(build_all_syncs(ctx));
+    RUN(hall_snapshot(ctx, false));
+    LAUNCHN(k_pack_vec, H.n, ctx->pool, H.e, H.X, H.n);
+    RUN(hall_residual(ctx, H.X, H.F));
+    double f = 0.0;
+    RUN(hall_norm(ctx, H.F, &f));
+    H.fnorm0 = f;
+    H.its = 0;
+    H.lin_its = 0;
+    H.reason = -5; // iteration limit
+    for (int it = 0; it <= H.maxit; ++it)
+    {
+        if (f <= H.atol)
+        {
+            H.reason = 2; // SNES_CONVERGED_FNORM_ABS
+            break;
+        }
+        if (f <= H.rtol * H.fnorm0)
+        {
+            H.reason = 3; // SNES_CONVERGED_FNORM_RELATIVE
+            break;
+        }
+        if (it == H.maxit)
+            break;
+        double xnorm = 0.0;
+        RUN(hall_norm(ctx, H.X, &xnorm));
+        RUN(hall_gmres(ctx, xnorm));
+        // backtracking: halve the step until ||F|| decreases sufficiently
+        double lambda = 1.0, ft = 0.0;
+        for (int ls = 0; ls < 12; ++ls)
+        {
+            LAUNCHN(k_axpy_to, H.n, H.Xt, H.X, lambda, H.dx, H.n);
+            RUN(hall_residual(ctx, H.Xt, H.Ft));
+            RUN(hall_norm(ctx, H.Ft, &ft));
+            if (ft <= (1.0 - 1e-4 * lambda) * f)
+                break;
+            lambda *= 0.5;
+        }
+        std::swap(H.X, H.Xt);
+        std::swap(H.F, H.Ft);
+        f = ft;
+        H.its = it + 1;
+    }
+    H.fnorm = f;
+    // final update with the converged Hall EMF
+    RUN(hall_trial_b(ctx, H.X));
+    return MHD_OK;
+}
+
+// the part of a step before the eagerly driven solves: the explicit step,
+// with the explicit resistive sub-cycles when they are on
+int launch_step_a_mid(mhd_ctx *ctx)
+{
+    RUN(launch_step_a(ctx));
+    if (!ctx->res.on && ctx->res_nsub > 0)
+        RUN(launch_resistive_explicit(ctx));
+    return MHD_OK;
+}
+
 int launch_step(mhd_ctx *ctx)
 {
     RUN(launch_step_a(ctx));
@@ -813,6 +1086,7 @@ int launch_step(mhd_ctx *ctx)
         RUN(launch_resistive(ctx));
     else if (ctx->res_nsub > 0)
         RUN(launch_resistive_explicit(ctx));
+    RUN(launch_hall_implicit(ctx));
     return launch_step_c(ctx);
 }
 
@@ -883,7 +1157,7 @@ int build_graph(mhd_ctx *ctx)
     if (ctx->gexec || ctx->gexec_a)
         return MHD_OK;
     RUN(build_all_syncs(ctx));
-    if (ctx->res.on && ctx->res.graph_loops)
+    if (ctx->res.on && ctx->res.graph_loops && !ctx->hall.on)
     {
         const int rc = capture(ctx, launch_step, &ctx->graph, &ctx->gexec, &ctx->graph_kernels);
         if (rc == MHD_OK)
@@ -897,9 +1171,9 @@ int build_graph(mhd_ctx *ctx)
         drop_graph(ctx);
         ctx->res.graph_loops = false;
     }
-    if (ctx->res.on)
+    if (ctx->res.on || ctx->hall.on)
     {
-        RUN(capture(ctx, launch_step_a, &ctx->graph_a, &ctx->gexec_a, &ctx->graph_kernels_a));
+        RUN(capture(ctx, launch_step_a_mid, &ctx->graph_a, &ctx->gexec_a, &ctx->graph_kernels_a));
         return capture(ctx, launch_step_c, &ctx->graph_c, &ctx->gexec_c, &ctx->graph_kernels_c);
     }
     return capture(ctx, launch_step, &ctx->graph, &ctx->gexec, &ctx->graph_kernels);
@@ -919,7 +1193,9 @@ int run_steps(mhd_ctx *ctx, int nsteps)
         {
             CK(ctx, cudaGraphLaunch(ctx->gexec_a, ctx->stream));
             ctx->launches += ctx->graph_kernels_a;
-            RUN(launch_resistive(ctx));
+            if (ctx->res.on)
+                RUN(launch_resistive(ctx));
+            RUN(launch_hall_implicit(ctx));
             CK(ctx, cudaGraphLaunch(ctx->gexec_c, ctx->stream));
             ctx->launches += ctx->graph_kernels_c;
         }
@@ -1030,6 +1306,7 @@ int mhd_ctx_destroy(mhd_ctx *ctx)
     }
     free_resistive(ctx);
     cudaFree(ctx->hall_zb);
+    mhd_set_hall_implicit(ctx, 0, nullptr, 0, nullptr, nullptr, nullptr, 0.0, 0.0, 0, 0.0, 1);
     for (auto &sp : ctx->spare)
         if (sp)
             cudaStreamDestroy(sp);
@@ -1829,6 +2106,86 @@ int mhd_set_hall(mhd_ctx *ctx, double hall_coef, const int32_t *zero_boxes, int3
     return MHD_OK;
 }
 
+int mhd_set_hall_implicit(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, int64_t nalias, const int64_t *alias,
+                          const int64_t *owner, const double *sign, double rtol, double atol, int32_t maxit,
+                          double ksp_rtol, int32_t ksp_maxit)
+{
+    if (!ctx || n < 0 || nalias < 0 || maxit < 0 || ksp_maxit < 1 || (n > 0 && !unknowns) ||
+        (nalias > 0 && (!alias || !owner || !sign)))
+        return fail(ctx, MHD_EINVAL, "bad implicit Hall arguments");
+    auto &H = ctx->hall;
+    for (void *p : {(void *)H.e, (void *)H.alias, (void *)H.owner, (void *)H.sign, (void *)H.bstar, (void *)H.X,
+                    (void *)H.F, (void *)H.Xt, (void *)H.Ft, (void *)H.dx, (void *)H.b, (void *)H.r, (void *)H.V,
+                    (void *)H.w, (void *)H.partial, (void *)H.dots, (void *)H.st})
+        cudaFree(p);
+    H = mhd_ctx::HallImplicit();
+    drop_graph(ctx);
+    if (n == 0)
+        return MHD_OK;
+    auto remap = [&](const int64_t *ids, int64_t cnt, std::vector<uint64_t> &out) -> int {
+        out.resize(size_t(cnt));
+        for (int64_t t = 0; t < cnt; ++t)
+        {
+            const int f = int(ids[t] >> 56);
+            const int64_t o = pool_offset(ctx, ids[t]);
+            if (f < F_Ehxi || f > F_Ehxi + 2 || o < 0)
+                return fail(ctx, MHD_EINVAL, "implicit Hall point %lld is not an Ehall point", (long long)t);
+            out[size_t(t)] = uint64_t(o);
+        }
+        return MHD_OK;
+    };
+    std::vector<uint64_t> he, ha, ho;
+    RUN(remap(unknowns, n, he));
+    RUN(remap(alias, nalias, ha));
+    RUN(remap(owner, nalias, ho));
+    RUN(upload_vec(ctx, he, &H.e));
+    RUN(upload_vec(ctx, ha, &H.alias));
+    RUN(upload_vec(ctx, ho, &H.owner));
+    std::vector<double> hs(sign, sign + nalias);
+    RUN(upload_vec(ctx, hs, &H.sign));
+    H.n = n;
+    H.nalias = nalias;
+    H.rtol = rtol;
+    H.atol = atol;
+    H.maxit = maxit;
+    H.ksp_rtol = ksp_rtol;
+    H.ksp_maxit = ksp_maxit;
+    H.ngroups = int(std::min<int64_t>(std::max<int64_t>((H.n + 255) / 256, 1), 592));
+    size_t nbs = 0;
+    for (int b = 0; b < ctx->nblocks; ++b)
+        nbs += 3 * size_t(ctx->hbv[size_t(b)].vol);
+    CK(ctx, cudaMalloc(&H.bstar, nbs * 8));
+    const size_t nn = size_t(H.n);
+    for (double **p : {&H.X, &H.F, &H.Xt, &H.Ft, &H.dx, &H.b, &H.r, &H.w})
+        CK(ctx, cudaMalloc(p, nn * 8));
+    CK(ctx, cudaMalloc(&H.V, nn * size_t(H.restart + 1) * 8));
+    CK(ctx, cudaMalloc(&H.partial, size_t(H.ngroups) * size_t(H.restart + 2) * 8));
+    CK(ctx, cudaMalloc(&H.dots, 64 * 8));
+    CK(ctx, cudaMalloc(&H.st, sizeof(GmresState)));
+    CK(ctx, cudaMemset(H.st, 0, sizeof(GmresState)));
+    H.on = true;
+    return MHD_OK;
+}
+
+int mhd_hall_stats(const mhd_ctx *ctx, int32_t *newton_its, int32_t *linear_its, double *fnorm, double *fnorm0,
+                   int32_t *reason)
+{
+    if (!ctx)
+        return MHD_EINVAL;
+    const auto &H = ctx->hall;
+    if (newton_its)
+        *newton_its = H.its;
+    if (linear_its)
+        *linear_its = H.lin_its;
+    if (fnorm)
+        *fnorm = H.fnorm;
+    if (fnorm0)
+        *fnorm0 = H.fnorm0;
+    if (reason)
+        *reason = H.reason;
+    return MHD_OK;
+}
+
 int mhd_set_resistive_explicit(mhd_ctx *ctx, double inver_Rem, int32_t nsub)
 {
     if (!ctx || nsub < 0)
@@ -2013,6 +2370,16 @@ int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
         k_hall_edge<<<dim3(grid_for(max_stagger(ctx)), ctx->nblocks), kThreads, 0, ctx->stream>>>(
             ctx->dbv, ctx->hall_zb, ctx->hall_nzb);
         RUN(launched(ctx));
+        break;
+    case MHD_STAGE_HALL_SOLVE:
+        // one implicit Hall solve at the current dt, then calc_Bcell (as StepOnce)
+        if (!ctx->hall.on)
+            return fail(ctx, MHD_ESTATE, "the implicit Hall solve is not set up");
+        RUN(launch_hall_implicit(ctx));
+        prof_begin(ctx, "k_bcell");
+        k_bcell<<<dim3(grid_for(max_box(ctx, LOC_CELL, 0)), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv);
+        RUN(launched(ctx));
+        RUN(run_sync(ctx, "B_cell"));
         break;
     case MHD_STAGE_DIVB:
         prof_begin(ctx, "k_divb");

@@ -107,5 +107,10 @@ __global__ void k_resist_out(const double *pool, const uint64_t *e, const uint64
 __global__ void k_resist_rhs(const double *pool, const uint64_t *j, const double *eta, double *b, int64_t n);
 __global__ void k_alias_copy(double *pool, const uint64_t *alias, const uint64_t *owner, const double *sign,
                              int64_t n);
+__global__ void k_pack_vec(const double *pool, const uint64_t *src, double *x, int64_t n);
+__global__ void k_hall_residual(const double *pool, const uint64_t *e, const double *x, double *F, int64_t n);
+__global__ void k_axpy_to(double *out, const double *x, double a, const double *y, int64_t n);
+__global__ void k_fd_quotient(double *out, const double *a, const double *b, double h, int64_t n);
+__global__ void k_negate(double *out, const double *x, int64_t n);
 
 } // namespace mhd

@@ -306,4 +306,54 @@ __global__ void k_alias_copy(double *__restrict__ pool, const uint64_t *__restri
         pool[alias[t]] = sign[t] * pool[owner[t]];
 }
 
+// ---------------------------------------------------------------------------
+// Vector pieces of the implicit Hall Newton-Krylov solve
+// (ImplicitHallSolver::SolveOneStep / FormFunction_,
+// Z4_Lunar/src/implicit/Hall_Implicit_Solver.cpp:268-391, Hall_Implicit_Formfunction.cpp:7-106)
+// ---------------------------------------------------------------------------
+
+// x[t] = pool[src[t]]   (pack an edge field into a vector)
+__global__ void k_pack_vec(const double *__restrict__ pool, const uint64_t *__restrict__ src, double *__restrict__ x,
+                           int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        x[t] = pool[src[t]];
+}
+
+// F[t] = x[t] - pool[e[t]]   (WriteResidual_: unknown minus predicted Hall EMF)
+__global__ void k_hall_residual(const double *__restrict__ pool, const uint64_t *__restrict__ e,
+                                const double *__restrict__ x, double *__restrict__ F, int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        F[t] = x[t] - pool[e[t]];
+}
+
+// out = x + a y
+__global__ void k_axpy_to(double *__restrict__ out, const double *__restrict__ x, double a, const double *__restrict__ y,
+                          int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        out[t] = x[t] + a * y[t];
+}
+
+// out = (a - b) / h   (finite-difference Jacobian-vector product)
+__global__ void k_fd_quotient(double *__restrict__ out, const double *__restrict__ a, const double *__restrict__ b,
+                              double h, int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        out[t] = (a[t] - b[t]) / h;
+}
+
+// out = -x
+__global__ void k_negate(double *__restrict__ out, const double *__restrict__ x, int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        out[t] = -x[t];
+}
+
 } // namespace mhd

@@ -32,9 +32,10 @@ def local_edges(ncell):
     return np.concatenate(out)
 
 
-def tiled_owners(ncell, tiles):
+def tiled_owners(ncell, tiles, periodic_i=False):
     """(alias, owner) pairs of a tiled layout with identity orientation, as
-    arrays of (block, dir, i, j, k); all signs are +1."""
+    arrays of (block, dir, i, j, k); all signs are +1.  periodic_i also
+    identifies the node planes i = 0 and i = n_i (a self-periodic block)."""
     TJ, TK = tiles
     nb = TJ * TK
     NJ, NK = ncell[1] * TJ, ncell[2] * TK
@@ -42,9 +43,10 @@ def tiled_owners(ncell, tiles):
     for b in range(nb):
         tj, tk = b // TK, b % TK
         e = local_edges(ncell)
+        gi = np.mod(e[:, 1], ncell[0]) if periodic_i else e[:, 1]
         gj = np.mod(tj * ncell[1] + e[:, 2], NJ)
         gk = np.mod(tk * ncell[2] + e[:, 3], NK)
-        rows.append(np.stack([np.full(len(e), b), e[:, 0], e[:, 1], e[:, 2], e[:, 3], e[:, 1], gj, gk], axis=1))
+        rows.append(np.stack([np.full(len(e), b), e[:, 0], e[:, 1], e[:, 2], e[:, 3], gi, gj, gk], axis=1))
     R = np.concatenate(rows)  # block, dir, i, j, k, key_i, key_j, key_k
     # owner = min (block, i, j, k, dir) within each key (dir, gi, gj, gk)
     order = np.lexsort((R[:, 1], R[:, 4], R[:, 3], R[:, 2], R[:, 0], R[:, 7], R[:, 6], R[:, 5], R[:, 1]))

@@ -27,6 +27,7 @@ PREC_FP64 = 0
 PREC_MIXED = 1
 
 STAGE_TIMESTEP, STAGE_FLUID_RHS, STAGE_INDUCTION, STAGE_UPDATE, STAGE_DIVB, STAGE_HALL_EMF = 1, 2, 3, 4, 5, 6
+STAGE_HALL_SOLVE = 7
 
 
 class BlockDesc(C.Structure):
@@ -57,6 +58,10 @@ _SIGS = {
     "mhd_set_sync_wall": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_int32]),
     "mhd_set_resistive": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int32, C.c_int32]),
+    "mhd_set_hall_implicit": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_double, C.c_double, C.c_int32, C.c_double, C.c_int32]),
+    "mhd_hall_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                                 C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "mhd_set_hall": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_int32]),
     "mhd_set_resistive_explicit": (C.c_int, [C.c_void_p, C.c_double, C.c_int32]),
     "mhd_resistive_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double),
@@ -239,6 +244,22 @@ class Context:
     def set_hall(self, hall_coef: float, zero_boxes):
         z = np.ascontiguousarray(np.asarray(zero_boxes, dtype=np.int32).reshape(-1, 8))
         self._check(self.lib.mhd_set_hall(self.h, float(hall_coef), z.ctypes.data, len(z)), "set_hall")
+
+    def set_hall_implicit(self, unknowns, alias, owner, sign, rtol=1e-8, atol=1e-50, maxit=50, ksp_rtol=1e-5,
+                          ksp_maxit=10000):
+        u = np.ascontiguousarray(unknowns, dtype=np.int64)
+        a = np.ascontiguousarray(alias, dtype=np.int64)
+        o = np.ascontiguousarray(owner, dtype=np.int64)
+        sg = np.ascontiguousarray(sign, dtype=np.float64)
+        self._check(self.lib.mhd_set_hall_implicit(self.h, u.size, u.ctypes.data, a.size, a.ctypes.data,
+                                                   o.ctypes.data, sg.ctypes.data, float(rtol), float(atol), int(maxit),
+                                                   float(ksp_rtol), int(ksp_maxit)), "set_hall_implicit")
+
+    def hall_stats(self):
+        its, lin, fn, f0, rs = C.c_int32(), C.c_int32(), C.c_double(), C.c_double(), C.c_int32()
+        self._check(self.lib.mhd_hall_stats(self.h, C.byref(its), C.byref(lin), C.byref(fn), C.byref(f0),
+                                            C.byref(rs)), "hall_stats")
+        return dict(its=its.value, linear_its=lin.value, fnorm=fn.value, fnorm0=f0.value, reason=rs.value)
 
     def set_resistive_explicit(self, inver_Rem: float, nsub: int):
         self._check(self.lib.mhd_set_resistive_explicit(self.h, float(inver_Rem), int(nsub)), "set_resistive_explicit")

@@ -136,6 +136,24 @@ class Solver:
             rows += [[ib] + r for r in hall_zero_boxes(n, patches)]
         self.ctx.set_hall(physics.constants(self.spec.params)["hall_coef"], rows)
 
+    def install_hall_implicit(self, topology, rtol=1e-8, atol=1e-50, maxit=50, ksp_rtol=1e-5, ksp_maxit=10000):
+        """Owner edges and aliases of the implicit Hall unknowns
+        (ImplicitHallSolver: owner_edges_sorted_ and the edge 1-form table)."""
+        n = self.spec.blocks[0].ncell
+        tiles = self.spec.tiles if topology == "tiled" else (1, 1)
+        alias, owner, owners = edges.tiled_owners(n, tiles, periodic_i=(topology == "periodic"))
+        names = {1: "Ehall_xi", 2: "Ehall_eta", 3: "Ehall_zeta"}
+
+        def ids(rows):
+            out = np.empty(len(rows), dtype=np.int64)
+            for q, (b, d, i, j, k) in enumerate(rows.tolist()):
+                info = self.ctx.field_info(names[d], b)
+                out[q] = self.ctx.point_base(names[d], b) + syncmap.aos_index(info["lo"], info["hi"], 1, i, j, k, 0)
+            return out
+
+        self.ctx.set_hall_implicit(ids(owners), ids(alias), ids(owner), np.ones(len(alias)), rtol, atol, maxit,
+                                   ksp_rtol, ksp_maxit)
+
     def install_explicit_resistive(self):
         """Shell profile of every inner edge and the sub-cycle count of
         LunarSolver::ResistiveDiffusionSubcycles_."""

@@ -38,6 +38,7 @@ GROUPS: Dict[str, List[str]] = {
     "Eres1form": ["Eres_xi", "Eres_eta", "Eres_zeta"],
     "dB": ["dB_xi", "dB_eta", "dB_zeta"],
     "Badd": ["Badd_xi", "Badd_eta", "Badd_zeta"],
+    "Ehall": ["Ehall_xi", "Ehall_eta", "Ehall_zeta"],
 }
 
 # +1 planes per axis of each location code (restart numbering)

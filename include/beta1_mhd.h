@@ -177,6 +177,29 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
    then computes Ehall_xi / Ehall_eta / Ehall_zeta of the current state. */
 int mhd_set_hall(mhd_ctx *ctx, double hall_coef, const int32_t *zero_boxes, int32_t nbox);
 
+/* Implicit Hall solve in every following StepOnce, after the resistive
+   part (ImplicitHallSolver::SolveOneStep with theta = 1,
+   Z4_Lunar/src/implicit/Hall_Implicit_Solver.cpp:268-391, the step the
+   reference runs when HALL_IMPLICIT is 1).  The unknowns are the owner edges
+   of Ehall (`unknowns`: Ehall_xi / Ehall_eta / Ehall_zeta point ids, the
+   reference's owner_edges_sorted_), alias/owner/sign the edge 1-form table of
+   HALO_OWNER (unpack_owner_edge_1form_local).  Newton on
+   F(E) = E - E_hall(B* - dt curl E) from the current Ehall, with a
+   backtracking line search; each Newton system is solved by restarted
+   GMRES(30) with finite-difference Jacobian-vector products.  Stops at
+   ||F|| <= max(rtol ||F0||, atol) or after maxit Newton steps (PETSc SNES
+   defaults: 1e-8, 1e-50, 50); ksp_rtol / ksp_maxit bound the linear
+   solves.  Needs mhd_set_hall and the "Ehall" sync group.  n = 0 switches
+   it off. */
+int mhd_set_hall_implicit(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, int64_t nalias, const int64_t *alias,
+                          const int64_t *owner, const double *sign, double rtol, double atol, int32_t maxit,
+                          double ksp_rtol, int32_t ksp_maxit);
+
+/* Newton steps, GMRES iterations, final and initial ||F|| and reason
+   (2 atol, 3 rtol, -5 Newton iteration limit) of the last implicit Hall solve. */
+int mhd_hall_stats(const mhd_ctx *ctx, int32_t *newton_its, int32_t *linear_its, double *fnorm, double *fnorm0,
+                   int32_t *reason);
+
 /* Explicit resistive sub-cycles (LunarSolver::ResistiveDiffusionSubcycles_,
    Z4_Lunar/src/physics/LunarSolver_MagneticRHS.cpp:53-115, with the edge EMF of
    AddResistiveEdgeEMF_To_, Z4_Lunar/src/physics/LunarSolver_MagExplicit_Resis.cpp:67-209):
@@ -228,6 +251,7 @@ int mhd_host_free(void *ptr);
 #define MHD_STAGE_UPDATE 4     /* ApplyUpdate_Euler_ with the current dt */
 #define MHD_STAGE_DIVB 5       /* calc_divB -> divB (inner cells; no Pole patches) */
 #define MHD_STAGE_HALL_EMF 6   /* BuildHallFaceEMF_Rusanov_diff_ -> Ehall_xi/eta/zeta (see mhd_set_hall) */
+#define MHD_STAGE_HALL_SOLVE 7 /* ImplicitHallSolver::SolveOneStep at the current dt, then calc_Bcell */
 int mhd_stage(mhd_ctx *ctx, int32_t stage_id);
 
 /* Current dt / time / step counters (device -> host). */

@@ -12,6 +12,7 @@
 //   ref_lunar run   <state.rst> <nsteps> <prefix>  state after each StepOnce
 //   ref_lunar probe <state.rst> <group> <out.bin>  index-encoded Sync(group)
 //   ref_lunar hall <state.rst> <out.bin>           Hall edge EMF of the state
+//   ref_lunar hallstep <state.rst> <out.bin>       one implicit Hall solve (tight tolerances)
 //   ref_lunar time  <state.rst> <nsteps>           wall time of the step loop
 //
 // The member functions are private in the reference; this translation unit
@@ -474,6 +475,39 @@ int cmd_hall(Harness &h, const std::string &state, const std::string &out)
     return 0;
 }
 
+// One implicit Hall solve (ImplicitHallSolver::SolveOneStep with the CFL dt
+// of the state, then calc_Bcell as StepOnce does), the nonlinear solve
+// tightened to ||F|| <= 1e-12 ||F0|| so that its root is pinned closely.
+int cmd_hallstep(Harness &h, const std::string &state, const std::string &out)
+{
+    h.load_state(state);
+    LunarSolver &s = *h.solver;
+    s.UpdateDerivedFields_();
+    s.Compute_Timestep();
+    SNESSetTolerances(s.hall_implicit_.snes_, 1e-30, 1e-12, 1e-30, 200, PETSC_DEFAULT);
+    s.hall_implicit_.SolveOneStep(s.dt, true);
+    s.calc_Bcell();
+    std::vector<DumpItem> items;
+    for (const char *n : {"B_xi", "B_eta", "B_zeta", "Ehall_xi", "Ehall_eta", "Ehall_zeta", "B_cell", "RHS_B_xi",
+                          "RHS_B_eta", "RHS_B_zeta"})
+        items.push_back(field_item(h.fld, n));
+    DumpItem dti;
+    dti.name = "dt";
+    dti.loc = -1;
+    dti.ncomp = 1;
+    dti.nghost = 0;
+    dti.extent = [](int, Int3 &lo, Int3 &hi, bool &active)
+    {
+        lo = Int3{0, 0, 0};
+        hi = Int3{1, 1, 1};
+        active = true;
+    };
+    dti.value = [&s](int, int, int, int, int) { return s.dt; };
+    items.push_back(dti);
+    write_dump(out, 0, 0.0, h.fld->num_blocks(), items);
+    return 0;
+}
+
 int cmd_time(Harness &h, const std::string &state, int nsteps)
 {
     h.load_state(state);
@@ -535,6 +569,8 @@ int main(int argc, char **argv)
             rc = cmd_owners(h, argv[2]);
         else if (cmd == "hall" && argc >= 4)
             rc = cmd_hall(h, argv[2], argv[3]);
+        else if (cmd == "hallstep" && argc >= 4)
+            rc = cmd_hallstep(h, argv[2], argv[3]);
         else if (cmd == "geom")
             rc = cmd_geom(h, argv[2]);
         else if (cmd == "run" && argc >= 5)

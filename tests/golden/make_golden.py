@@ -148,6 +148,39 @@ def hall(spec_kind, seed=20261205):
     print("wrote", tag)
 
 
+def hallstep(spec_kind, seed=20261205):
+    """One implicit Hall solve of the reference (ImplicitHallSolver::SolveOneStep
+    at the state's CFL dt, nonlinear tolerance 1e-12) from a seeded state:
+    the face B after the solve, the converged Hall EMF and B_cell."""
+    if spec_kind == "periodic":
+        spec = case.periodic_box_case((8, 6, 5))
+        st = case.initial_state(spec, seed=seed)
+        tag = "hallstep_periodic_8x6x5"
+    else:
+        spec = case.slab_case(24, (5, 6), (2, 2))
+        st = case.inflow_state(spec, seed=seed)
+        tag = "hallstep_slab_24x5x6_t2x2"
+    with tempfile.TemporaryDirectory() as d:
+        case.write_case(d, spec)
+        rst.write(os.path.join(d, "init.rst"), st)
+        run(["hallstep", "init.rst", "out.bin"], d)
+        r = rst.read(os.path.join(d, "out.bin"))
+        arr = {}
+        for b in range(len(spec.blocks)):
+            for name in ("U_H", "B_xi", "B_eta", "B_zeta"):
+                fa = st.fields[name].blocks[b]
+                arr["init/b%d/%s" % (b, name)] = fa.data
+                arr["init/b%d/%s__lo" % (b, name)] = np.array(fa.lo, dtype=np.int32)
+            for name in ("B_xi", "B_eta", "B_zeta", "Ehall_xi", "Ehall_eta", "Ehall_zeta", "B_cell", "RHS_B_xi",
+                         "RHS_B_eta", "RHS_B_zeta"):
+                fa = r.fields[name].blocks[b]
+                arr["b%d/%s" % (b, name)] = fa.data
+                arr["b%d/%s__lo" % (b, name)] = np.array(fa.lo, dtype=np.int32)
+        arr["dt"] = r.fields["dt"].blocks[0].data.reshape(())
+        np.savez_compressed(os.path.join(OUT, tag + ".npz"), **arr)
+    print("wrote", tag)
+
+
 def slab_probe(nr=6, nt=(5, 6), tiles=(2, 2), resistive=0, seed=20261204):
     """Every Sync group of a tiled slab probed on the reference: for each
     (group, field, block) the offsets whose value the Sync changed and the
@@ -217,4 +250,6 @@ if __name__ == "__main__":
     slab_probe(resistive=1)
     hall("periodic")
     hall("slab")
+    hallstep("periodic")
+    hallstep("slab")
     slab_owners(eta_max_lunar=1.0 * case.MU0 * case.ref_scales()["U"] * case.ref_scales()["L_ref"])
