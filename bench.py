@@ -63,7 +63,12 @@ ALGO_BYTES_PER_CELL = {
     # PV / U_plus / CFL with J_cell: U 5, Jac 1, B_cell 3, face area + normal 12, J 3, W_J 36 read;
     # PV 5, U_plus 3, Csound 1, RhoE 1, J_cell 3 written
     "k_pv_uplus_dt": 73 * 8,
+    # mixed form: FP32 face states rho, u, v, w, p, RhoE, c 7 and face area 3 read; FP64 JD 9, Jac 1,
+    # U_plus 3, rho 1, u/v/w 3, B_cell 3, J_cell 3 read, RHS_H 5 and U_contra 3 written
+    "k_fluid_mixed": 10 * 4 + 31 * 8,
 }
+# the mixed form's PV pass also writes the 7 FP32 face states
+ALGO_BYTES_MIXED_EXTRA = {"k_pv_uplus_dt": 7 * 4}
 
 # DRAM traffic per launch from one ncu capture of the 64^3 case
 # (profiles/k_fluid_rhs_periodic64.md); None where not captured.
@@ -218,6 +223,8 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=None, help="StepOnce per reference CPU sample")
     ap.add_argument("--e2e-iters", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="fp64, or FP32 face fluxes with FP64 CT / state / residuals")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -238,11 +245,12 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    from beta1_b200 import solver
+    from beta1_b200 import mhd, solver
 
     wl = WORKLOADS[args.workload]
     spec, st, topology, cells = build_case(args.workload, args.n)
-    s = solver.Solver(spec, topology=topology)
+    mixed = args.precision == "mixed"
+    s = solver.Solver(spec, topology=topology, precision=mhd.PREC_MIXED if mixed else mhd.PREC_FP64)
     s.load_state(st)
     ctx = s.ctx
     stream = torch.cuda.ExternalStream(ctx.stream())
@@ -301,7 +309,8 @@ def main():
     dominant = max((k for k in per_step if k in ALGO_BYTES_PER_CELL), key=lambda k: per_step[k])
     launches_of = {k: len(v) / 5.0 for k, v in prof.items()}
     avg_launch_ms = per_step[dominant] / launches_of[dominant]
-    bytes_per_launch = ALGO_BYTES_PER_CELL[dominant] * cells / launches_of[dominant]
+    algo = ALGO_BYTES_PER_CELL[dominant] + (ALGO_BYTES_MIXED_EXTRA.get(dominant, 0) if mixed else 0)
+    bytes_per_launch = algo * cells / launches_of[dominant]
     achieved = bytes_per_launch / (avg_launch_ms / 1000.0) / 1e9
     peak, peak_kind = measured_peak()
 
@@ -347,10 +356,11 @@ def main():
         line = {
             "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 fluxes + f64 CT/state" if mixed else "f64",
             "data": "synthetic (seeded 1e-3 noise on rho, v and div-free B; reference restart format)",
-            "config": {"workload": wl["name"], "cells_per_gpu": cells, "blocks": len(spec.blocks),
-                       "integrator": "forward Euler StepOnce (reference parity mode)", "precision": "fp64",
+            "config": {"workload": wl["name"].replace("_fp64", "_mixed") if mixed else wl["name"], "cells_per_gpu": cells, "blocks": len(spec.blocks),
+                       "integrator": "forward Euler StepOnce (reference parity mode)", "precision": args.precision,
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "no flush: per-step working set %.2f GB > 126 MB L2" % (ctx_bytes / 1e9)},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": nstate * 8,

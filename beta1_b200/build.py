@@ -20,6 +20,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 # (source, extra flags)
 UNITS = [
     ("mhd_kernels_fp64.cu", ["-fmad=false"]),
+    ("mhd_kernels_mixed.cu", []),
     ("mhd_krylov.cu", []),
     ("mhd_abi.cu", []),
 ]

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <cstdint>
 #include <cstdarg>
 #include <cstdio>
@@ -87,7 +88,8 @@ const char *const kKernelNames[] = {
     "k_cycle_start",  "k_gmres_column", "k_inner_check", "k_gmres_solve_y", "k_add_basis",    "k_outer_check",
     "k_zero",         "k_residual",    "k_ucontra",      "k_face_normals", "k_divb",          "k_eres_explicit",
     "k_bcell_jedge",  "k_fluid_ucontra", "k_wall_u_all",   "k_hall_cell",    "k_hall_edge",
-    "k_pack_vec",     "k_hall_residual", "k_axpy_to",      "k_fd_quotient",  "k_negate"};
+    "k_pack_vec",     "k_hall_residual", "k_axpy_to",      "k_fd_quotient",  "k_negate",
+    "k_geom32",       "k_fluid_mixed"};
 constexpr int kNumKernelNames = int(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
 
 } // namespace
@@ -102,6 +104,7 @@ struct mhd_ctx
     BlockView *dbv = nullptr;
     double *pool = nullptr;
     size_t pool_n = 0;
+    float *pool32 = nullptr; // FP32 planes of the mixed-precision form
     std::vector<std::vector<size_t>> base; // [field][block] offset in pool
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr, graph_a = nullptr, graph_c = nullptr;
@@ -402,6 +405,15 @@ int ensure_geom(mhd_ctx *ctx)
     prof_begin(ctx, "k_face_normals");
     k_face_normals<<<dim3(grid_for(nf), ctx->nblocks, 3), kThreads, 0, ctx->stream>>>(ctx->dbv);
     RUN(launched(ctx));
+    if (ctx->pool32)
+    {
+        int64_t vmax = 0;
+        for (const auto &v : ctx->hbv)
+            vmax = std::max(vmax, v.vol);
+        prof_begin(ctx, "k_geom32");
+        k_geom32<<<dim3(grid_for(vmax), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv);
+        RUN(launched(ctx));
+    }
     ctx->geom_dirty = false;
     return MHD_OK;
 }
@@ -436,8 +448,12 @@ int launch_update_derived(mhd_ctx *ctx)
     return MHD_OK;
 }
 
+int launch_fluid_ucontra(mhd_ctx *ctx);
+
 int launch_fluid_rhs(mhd_ctx *ctx)
 {
+    if (ctx->pool32) // the mixed form's flux pass (its FP32 U_contra are a by-product)
+        return launch_fluid_ucontra(ctx);
     const int64_t nc = max_box(ctx, LOC_CELL, 0);
     prof_begin(ctx, "k_fluid_rhs");
     k_fluid_rhs<<<dim3(grid_for(nc), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv, ctx->c, nc);
@@ -447,6 +463,13 @@ int launch_fluid_rhs(mhd_ctx *ctx)
 // fluid RHS together with the contravariant velocities of the EMF stencils
 int launch_fluid_ucontra(mhd_ctx *ctx)
 {
+    if (ctx->pool32)
+    {
+        prof_begin(ctx, "k_fluid_mixed");
+        k_fluid_mixed<<<dim3(grid_for(max_box(ctx, LOC_CELL, 1)), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv,
+                                                                                                            ctx->c);
+        return launched(ctx);
+    }
     prof_begin(ctx, "k_fluid_ucontra");
     k_fluid_ucontra<<<dim3(grid_for(max_box(ctx, LOC_CELL, 1)), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv,
                                                                                                           ctx->c);
@@ -1267,6 +1290,26 @@ int mhd_ctx_create(const mhd_block_desc *blocks, int32_t nblocks, const mhd_para
     for (int b = 0; b < nblocks; ++b)
         for (int f = 0; f < NFIELD; ++f)
             ctx->hbv[size_t(b)].f[f] = ctx->pool + ctx->base[size_t(f)][size_t(b)];
+    if (params->precision == MHD_PREC_MIXED)
+    {
+        size_t n32 = 0;
+        for (int b = 0; b < nblocks; ++b)
+            n32 += size_t(G32_N + Q32_N) * size_t(ctx->hbv[size_t(b)].vol);
+        if (cudaMalloc(&ctx->pool32, n32 * sizeof(float)) != cudaSuccess)
+            return bail(MHD_ENOMEM);
+        if (cudaMemset(ctx->pool32, 0, n32 * sizeof(float)) != cudaSuccess)
+            return bail(MHD_ECUDA);
+        size_t o = 0;
+        for (int b = 0; b < nblocks; ++b)
+        {
+            BlockView &v = ctx->hbv[size_t(b)];
+            v.g32 = ctx->pool32 + o;
+            v.q32 = v.g32 + size_t(G32_N) * size_t(v.vol);
+            o += size_t(G32_N + Q32_N) * size_t(v.vol);
+        }
+    }
+    else if (params->precision != MHD_PREC_FP64)
+        return bail(MHD_EINVAL);
     if (cudaMalloc(&ctx->dbv, sizeof(BlockView) * size_t(nblocks)) != cudaSuccess)
         return bail(MHD_ENOMEM);
     if (cudaMemcpy(ctx->dbv, ctx->hbv.data(), sizeof(BlockView) * size_t(nblocks), cudaMemcpyHostToDevice) !=
@@ -1315,6 +1358,7 @@ int mhd_ctx_destroy(mhd_ctx *ctx)
     cudaFree(ctx->staging);
     cudaFree(ctx->dbv);
     cudaFree(ctx->pool);
+    cudaFree(ctx->pool32);
     if (ctx->stream)
         cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -2197,6 +2241,21 @@ int mhd_set_resistive_explicit(mhd_ctx *ctx, double inver_Rem, int32_t nsub)
     // the hot sync lists depend on it (J_cell ghost depth)
     for (auto &kv : ctx->syncs)
         kv.second.built = false;
+    drop_graph(ctx);
+    return MHD_OK;
+}
+
+int mhd_set_flux_reference(mhd_ctx *ctx, const double prim[5])
+{
+    if (!ctx || !prim)
+        return fail(ctx, MHD_EINVAL, "null flux reference");
+    for (int m = 0; m < 5; ++m)
+        if (!std::isfinite(prim[m]))
+            return fail(ctx, MHD_EINVAL, "non-finite flux reference");
+    const double rho = prim[0], u = prim[1], v = prim[2], w = prim[3], p = prim[4];
+    const double q[6] = {rho, u, v, w, p, p / (ctx->c.gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w)};
+    std::memcpy(ctx->c.qref, q, sizeof(q));
+    // the constants are kernel arguments inside the captured step
     drop_graph(ctx);
     return MHD_OK;
 }

@@ -17,6 +17,9 @@ struct Consts
     double state_coeff;
     double M_H, M_ref;
     double ne_floor;
+    // mixed form: reference state rho, u, v, w, p, E about which the FP32
+    // face states are stored as deviations (zero unless set)
+    double qref[6];
 };
 
 __global__ void k_fluid_rhs(const BlockView *bvs, Consts c, int64_t maxpts);
@@ -31,6 +34,9 @@ __global__ void k_curl_e2f(const BlockView *bvs, int fE0, int fR0, int fB0, doub
                            double dtdiv, int mult_is_neg_dt, const int *rng);
 __global__ void k_update_u(const BlockView *bvs, const double *dtp);
 __global__ void k_divb(const BlockView *bvs);
+// mixed precision (mhd_kernels_mixed.cu)
+__global__ void k_geom32(const BlockView *bvs);
+__global__ void k_fluid_mixed(const BlockView *bvs, Consts c);
 __global__ void k_hall_cell(const BlockView *bvs, Consts c, double hall_coef);
 __global__ void k_hall_edge(const BlockView *bvs, const int *zb, int nzb);
 __global__ void k_eres_explicit(const BlockView *bvs, double inver_Rem);

@@ -271,6 +271,7 @@ __global__ void k_fluid_ucontra(const BlockView *__restrict__ bvs, Consts c)
     UC[2 * b.vol + p] = u_contra(b, 2, i, j, k);
 }
 
+// contravariant velocity of a cell, as stored by the fluid pass
 __device__ __forceinline__ double uc(const BlockView &b, int axis, int i, int j, int k)
 {
     return b.f[F_UC][axis * b.vol + pidx(b, i, j, k)];
@@ -923,8 +924,23 @@ __global__ void k_pv_uplus_dt(const BlockView *__restrict__ bvs, Consts c, unsig
             Up[2 * v + p] = has_plasma ? w : 0.0;
             // sound speed and total energy of the Rusanov face states
             // (Reconstruction_Rusanov, LunarSolver_FluidRHS.cpp:34-111)
-            b.f[F_Cs][p] = sqrt(smax(0.0, c.gamma * pr / smax(U0, 1e-30)));
-            b.f[F_RhoE][p] = pr / (c.gamma - 1.0) + 0.5 * U0 * (u * u + vv * vv + w * w);
+            const double cs = sqrt(smax(0.0, c.gamma * pr / smax(U0, 1e-30)));
+            const double rhoe = pr / (c.gamma - 1.0) + 0.5 * U0 * (u * u + vv * vv + w * w);
+            b.f[F_Cs][p] = cs;
+            b.f[F_RhoE][p] = rhoe;
+            if (b.q32)
+            {
+                // FP32 face states of the mixed-precision flux: deviations
+                // from the reference state (formed in FP64), sound speed
+                float *q = b.q32;
+                q[Q32_RHO * v + p] = float(U0 - c.qref[0]);
+                q[(Q32_U + 0) * v + p] = float(u - c.qref[1]);
+                q[(Q32_U + 1) * v + p] = float(vv - c.qref[2]);
+                q[(Q32_U + 2) * v + p] = float(w - c.qref[3]);
+                q[Q32_P * v + p] = float(pr - c.qref[4]);
+                q[Q32_RHOE * v + p] = float(rhoe - c.qref[5]);
+                q[Q32_C * v + p] = float(cs);
+            }
         }
         const bool inner = (i >= 0 && j >= 0 && k >= 0 && i < b.ni && j < b.nj && k < b.nk);
         if (inner && dt_key)

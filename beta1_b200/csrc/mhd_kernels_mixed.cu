@@ -1,0 +1,173 @@
+// Mixed-precision kernels (MHD_PREC_MIXED).  The Rusanov face fluxes of the
+// fluid right-hand side are evaluated in FP32 and accumulated in FP32, in
+// deviation form: the face states are stored as FP32 deviations from a
+// constant reference state q0 (the far-field inflow), and each face computes
+//     dF = Rusanov(qL, qR; k) - Phi0(k),   Phi0(k) = F_phys(q0) . k
+// from the deviations with the algebra rearranged so that no large term is
+// formed and then cancelled (rho U - rho0 U0 = drho U + rho0 dU, etc.).  The
+// part Phi0 is linear in the face vector k, so its divergence is
+// Phi0(sum of the cell's signed face vectors), evaluated in FP64 from the
+// FP64 metric.  FP32 rounding therefore scales with the departure from q0,
+// not with the flux itself.  The J x B source, the stored RHS_H, the
+// conserved update, the contravariant velocities of the CT EMF, the EMF
+// itself, its curl and the face-B update stay FP64 (the contravariant
+// velocities here, the rest in other translation units), so div B stays at
+// FP64 round-off.  Compiled with contracted multiply-adds.
+#include "mhd_kernels.cuh"
+
+namespace mhd
+{
+
+__device__ __forceinline__ float fmaxs(float a, float b) { return (a < b) ? b : a; }
+
+// FP32 copy of the face areas |JD| on every point of the padded box
+__global__ void k_geom32(const BlockView *__restrict__ bvs)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    const int64_t v = b.vol;
+    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= v)
+        return;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        b.g32[(G32_AREA + a) * v + p] = float(b.f[F_NAxi + a][p]);
+}
+
+// reference-state constants of the deviation flux, FP32
+struct Ref32
+{
+    float rho, u[3], H; // rho0, u0, E0 + p0
+};
+
+// one Rusanov face flux minus the reference-state flux Phi0(k), in FP32:
+// face vector (k1, k2, k3), face area, left cell pL, right cell p.  Per side,
+// with U = k . u = U0 + dU:
+//   mass    rho U - rho0 U0               = drho U + rho0 dU          (= dm)
+//   mom x   rho U u + k1 p - (same at q0) = dm u + rho0 U0 du + k1 dp
+//   energy  U (E + p) - U0 (E0 + p0)      = dU (E + p) + U0 (dE + dp)
+// and the dissipation uses conserved differences of the deviations
+// (rho u - rho0 u0 = drho u + rho0 du).
+__device__ __forceinline__ void rusanov_dev32(const BlockView &b, const Ref32 &r0, float k1, float k2, float k3,
+                                              float area, int64_t p, int64_t pL, float out[5])
+{
+    const int64_t v = b.vol;
+    const float *q = b.q32;
+    const float U0 = k1 * r0.u[0] + k2 * r0.u[1] + k3 * r0.u[2];
+    float dF[2][5], dC[2][5], rad = 0.0f;
+#pragma unroll
+    for (int s = 0; s < 2; ++s)
+    {
+        const int64_t c = s ? p : pL;
+        const float dr = q[Q32_RHO * v + c];
+        const float du = q[Q32_U * v + c], dv = q[(Q32_U + 1) * v + c], dw = q[(Q32_U + 2) * v + c];
+        const float dp = q[Q32_P * v + c], dE = q[Q32_RHOE * v + c], cs = q[Q32_C * v + c];
+        const float u = r0.u[0] + du, vv = r0.u[1] + dv, w = r0.u[2] + dw;
+        const float dU = k1 * du + k2 * dv + k3 * dw;
+        const float U = U0 + dU;
+        const float dm = dr * U + r0.rho * dU;
+        const float mU0 = r0.rho * U0;
+        dF[s][0] = dm;
+        dF[s][1] = dm * u + mU0 * du + k1 * dp;
+        dF[s][2] = dm * vv + mU0 * dv + k2 * dp;
+        dF[s][3] = dm * w + mU0 * dw + k3 * dp;
+        dF[s][4] = dU * (r0.H + dE + dp) + U0 * (dE + dp);
+        dC[s][0] = dr;
+        dC[s][1] = dr * u + r0.rho * du;
+        dC[s][2] = dr * vv + r0.rho * dv;
+        dC[s][3] = dr * w + r0.rho * dw;
+        dC[s][4] = dE;
+        rad = fmaxs(rad, fabsf(U) + cs * area);
+    }
+#pragma unroll
+    for (int m = 0; m < 5; ++m)
+        out[m] = 0.5f * (dF[0][m] + dF[1][m]) - 0.5f * rad * (dC[1][m] - dC[0][m]);
+}
+
+// Fluid RHS of the inner cells (FP32 flux divergence, FP64 J x B source) and
+// the FP64 contravariant velocities of the cells within one ghost layer; the
+// FP64 face metric read for the velocities is the one the fluxes round.
+__global__ void k_fluid_mixed(const BlockView *__restrict__ bvs, Consts c)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    const int lo = -1;
+    const int n0 = b.ni + 2, n1 = b.nj + 2, n2 = b.nk + 2;
+    int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= int64_t(n0) * n1 * n2)
+        return;
+    const int k = lo + int(t % n2);
+    t /= n2;
+    const int j = lo + int(t % n1);
+    const int i = lo + int(t / n1);
+    const int64_t v = b.vol;
+    const int64_t p = pidx(b, i, j, k);
+    const int64_t pp[3] = {pidx(b, i + 1, j, k), pidx(b, i, j + 1, k), pidx(b, i, j, k + 1)};
+    const double jac = b.f[F_Jac][p];
+    double km[3][3], kp[3][3]; // face metric at the low (p) and high (pp) face of each axis
+    {
+        // contravariant velocities (cell_u_contra): (k-bar . U_plus) / (|Jac| + 1e-30)
+        const double *Up = b.f[F_Uplus];
+        const double ux = Up[p], uy = Up[v + p], uz = Up[2 * v + p];
+        const double inv_jac = 1.0 / (fabs(jac) + 1.0e-30);
+        double *UC = b.f[F_UC];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+        {
+            const double *M = b.f[F_JDxi + a];
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+            {
+                km[a][d] = M[d * v + p];
+                kp[a][d] = M[d * v + pp[a]];
+            }
+            const double kx = 0.5 * (km[a][0] + kp[a][0]);
+            const double ky = 0.5 * (km[a][1] + kp[a][1]);
+            const double kz = 0.5 * (km[a][2] + kp[a][2]);
+            UC[a * v + p] = (kx * ux + ky * uy + kz * uz) * inv_jac;
+        }
+    }
+    if (i < 0 || j < 0 || k < 0 || i >= b.ni || j >= b.nj || k >= b.nk)
+        return;
+    const float *g = b.g32;
+    const int64_t pm[3] = {pidx(b, i - 1, j, k), pidx(b, i, j - 1, k), pidx(b, i, j, k - 1)};
+    const Ref32 r0 = {float(c.qref[0]), {float(c.qref[1]), float(c.qref[2]), float(c.qref[3])},
+                      float(c.qref[5] + c.qref[4])};
+    float r[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    double S[3] = {0.0, 0.0, 0.0}; // sum of the signed face vectors of the cell
+#pragma unroll
+    for (int dir = 0; dir < 3; ++dir)
+    {
+        float Fm[5], Fp[5];
+        rusanov_dev32(b, r0, float(km[dir][0]), float(km[dir][1]), float(km[dir][2]), g[(G32_AREA + dir) * v + p], p,
+                      pm[dir], Fm);
+        rusanov_dev32(b, r0, float(kp[dir][0]), float(kp[dir][1]), float(kp[dir][2]),
+                      g[(G32_AREA + dir) * v + pp[dir]], pp[dir], p, Fp);
+#pragma unroll
+        for (int m = 0; m < 5; ++m)
+            r[m] += Fp[m] - Fm[m];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            S[d] += kp[dir][d] - km[dir][d];
+    }
+    // divergence of the reference-state flux, FP64: Phi0(S)
+    const double US = S[0] * c.qref[1] + S[1] * c.qref[2] + S[2] * c.qref[3];
+    const double mS = c.qref[0] * US;
+    const double phi[5] = {mS, mS * c.qref[1] + S[0] * c.qref[4], mS * c.qref[2] + S[1] * c.qref[4],
+                           mS * c.qref[3] + S[2] * c.qref[4], US * (c.qref[5] + c.qref[4])};
+    // J x B force with the Hall_Num_Limiter weight, FP64
+    const double rho = b.f[F_U][p];
+    const double n_true = ((rho < 0.0) ? 0.0 : rho) / c.M_H * c.M_ref;
+    const double fc = c.mom_hall * (n_true / sqrt(n_true * n_true + c.ne_floor * c.ne_floor));
+    const double *J = b.f[F_Jcell], *B = b.f[F_Bcell], *PV = b.f[F_PV];
+    const double jx = J[p], jy = J[v + p], jz = J[2 * v + p];
+    const double bx = B[p], by = B[v + p], bz = B[2 * v + p];
+    const double fx = jy * bz - jz * by, fy = jz * bx - jx * bz, fz = jx * by - jy * bx;
+    const double invJ = 1.0 / jac;
+    double *R = b.f[F_RHS];
+    R[p] = -(double(r[0]) + phi[0]) * invJ;
+    R[v + p] = -(double(r[1]) + phi[1]) * invJ + fc * fx;
+    R[2 * v + p] = -(double(r[2]) + phi[2]) * invJ + fc * fy;
+    R[3 * v + p] = -(double(r[3]) + phi[3]) * invJ + fc * fz;
+    R[4 * v + p] = -(double(r[4]) + phi[4]) * invJ + fc * (fx * PV[p] + fy * PV[v + p] + fz * PV[2 * v + p]);
+}
+
+} // namespace mhd

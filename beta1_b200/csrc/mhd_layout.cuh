@@ -125,6 +125,22 @@ struct BlockView
     int G;            // padding ghost layers
     int NJ, NK;       // padded extents (j, k)
     int64_t vol;      // doubles per component plane
+    // mixed precision only (null otherwise): FP32 planes on the same padded box
+    float *g32;       // face area xi, eta, zeta
+    float *q32;       // face-state quantities rho, u, v, w, p, rhoE, c
+};
+
+// plane indices of BlockView::g32 / q32
+enum : int
+{
+    G32_AREA = 0,
+    G32_N = 3,
+    Q32_RHO = 0,
+    Q32_U = 1,
+    Q32_P = 4,
+    Q32_RHOE = 5,
+    Q32_C = 6,
+    Q32_N = 7
 };
 
 __host__ __device__ inline int64_t pidx(const BlockView &b, int i, int j, int k)

@@ -64,6 +64,7 @@ _SIGS = {
                                  C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "mhd_set_hall": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_int32]),
     "mhd_set_resistive_explicit": (C.c_int, [C.c_void_p, C.c_double, C.c_int32]),
+    "mhd_set_flux_reference": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "mhd_resistive_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double),
                                       C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "mhd_update_derived": (C.c_int, [C.c_void_p]),
@@ -263,6 +264,11 @@ class Context:
 
     def set_resistive_explicit(self, inver_Rem: float, nsub: int):
         self._check(self.lib.mhd_set_resistive_explicit(self.h, float(inver_Rem), int(nsub)), "set_resistive_explicit")
+
+    def set_flux_reference(self, prim):
+        """reference state (rho, u, v, w, p) of the mixed-precision deviation flux"""
+        a = (C.c_double * 5)(*[float(x) for x in prim])
+        self._check(self.lib.mhd_set_flux_reference(self.h, a), "set_flux_reference")
 
     def resistive_stats(self):
         its, rn, bn, rs = C.c_int32(), C.c_double(), C.c_double(), C.c_int32()

@@ -64,17 +64,39 @@ def badd_faces(JD: np.ndarray, B0) -> np.ndarray:
     return ((B0[0] * JD[..., 0] + B0[1] * JD[..., 1]) + B0[2] * JD[..., 2])[..., None]
 
 
+# host-side set-up of a case (geometry, node arrays, compiled sync tables),
+# kept for solvers of the same case (e.g. the FP64 and the mixed-precision
+# form side by side)
+_HOST_CACHE: dict = {}
+
+
 class Solver:
     def __init__(self, spec: case_mod.CaseSpec, topology: str = "periodic", precision=mhd.PREC_FP64):
         self.spec = spec
         ngg = int(spec.params["ngg"])
         self.ctx = mhd.Context([b.ncell for b in spec.blocks], make_params(spec.params, precision))
+        cache = _HOST_CACHE.get(id(spec))
+        if cache is None or cache["spec"] is not spec:
+            cache = {"spec": spec, "geom": [], "nodes": []}
+            for b in spec.blocks:
+                X = geometry.ghost_mesh(b.x, b.y, b.z, ngg)
+                cache["nodes"].append(X)
+                cache["geom"].append(geometry.build(X, b.ncell, ngg))
+            _HOST_CACHE.clear()
+            _HOST_CACHE[id(spec)] = cache
+        self._cache = cache
+        if precision == mhd.PREC_MIXED:
+            q0, _ = physics.farfield_state(spec.params)
+            u0 = [q0[1] / q0[0], q0[2] / q0[0], q0[3] / q0[0]]
+            p0 = (physics.constants(spec.params)["gamma"] - 1.0) * (
+                q0[4] - 0.5 * q0[0] * (u0[0] ** 2 + u0[1] ** 2 + u0[2] ** 2))
+            self.ctx.set_flux_reference([q0[0]] + u0 + [p0])
         self.geom = []
         self.nodes = []
         _, B_imf = physics.farfield_state(spec.params)
         for ib, b in enumerate(spec.blocks):
-            X = geometry.ghost_mesh(b.x, b.y, b.z, ngg)
-            g = geometry.build(X, b.ncell, ngg)
+            X = cache["nodes"][ib]
+            g = cache["geom"][ib]
             for name in GEOM_FIELDS:
                 lo, hi, a = g[name]
                 self.ctx.upload(name, ib, a)
@@ -171,8 +193,11 @@ class Solver:
         u = [q[1] / q[0], q[2] / q[0], q[3] / q[0]]
         E_inf = [B[1] * u[2] - B[2] * u[1], B[2] * u[0] - B[0] * u[2], B[0] * u[1] - B[1] * u[0]]
         resistive = bool(spec.params.get("is_Lunar_resistance", 0))
-        maps = syncmap.compile_tiled(self.ctx, syncmap.TiledLayout(spec.blocks[0].ncell, spec.tiles), resistive,
-                                     dict(qinf=q, B_imf=B, E_inf=E_inf), self.nodes)
+        key = ("maps", resistive)
+        if key not in self._cache:
+            self._cache[key] = syncmap.compile_tiled(self.ctx, syncmap.TiledLayout(spec.blocks[0].ncell, spec.tiles),
+                                                     resistive, dict(qinf=q, B_imf=B, E_inf=E_inf), self.nodes)
+        maps = self._cache[key]
         self.sync_sizes = {}
         for group, m in maps.items():
             self.ctx.set_sync_map(group, m["dst"], m["src"])

@@ -210,6 +210,17 @@ int mhd_hall_stats(const mhd_ctx *ctx, int32_t *newton_its, int32_t *linear_its,
    mhd_set_resistive. */
 int mhd_set_resistive_explicit(mhd_ctx *ctx, double inver_Rem, int32_t nsub);
 
+/* Reference state of the mixed-precision flux (no counterpart in the
+   reference, which has no mixed-precision form): primitive rho, u, v, w, p
+   of a constant state, normally the far-field inflow.  The FP32 face states
+   are stored as deviations from it and the Rusanov flux is evaluated in FP32
+   in deviation form, with the reference-state part added in FP64, so the
+   FP32 rounding scales with the departure from this state.  Any state gives
+   the same result up to that rounding (zero, the default, is the plain FP32
+   flux).  Takes effect at the next UpdateDerivedFields_ (mhd_update_derived,
+   or the end of a step); has no effect in MHD_PREC_FP64. */
+int mhd_set_flux_reference(mhd_ctx *ctx, const double prim[5]);
+
 /* Iterations, final residual norm, ||b|| and convergence reason (2 rtol,
    3 atol, -3 iteration limit, as KSPConvergedReason) of the last solve. */
 int mhd_resistive_stats(const mhd_ctx *ctx, int32_t *its, double *rnorm, double *bnorm, int32_t *reason);

@@ -116,6 +116,47 @@ def slab(nr=6, nt=(5, 6), tiles=(2, 2), steps=2, resistive=0, implicit=0, seed=2
     print("wrote", tag)
 
 
+LONG_FIELDS = ["U_H", "B_xi", "B_eta", "B_zeta", "PV_H", "B_cell", "J_cell", "divB"]
+
+
+def slab_long(nr=16, nt=(8, 8), tiles=(2, 2), steps=100, resistive=0, implicit=0, seed=20261206, **over):
+    """The reference's state after `steps` StepOnce of a slab (only the
+    initial and the final state are kept): the FP64 target of the
+    long-horizon parity and of the mixed-precision error report."""
+    tag = "slab_%dx%dx%d_t%dx%d_r%d%d_long%d" % ((nr,) + tuple(nt) + tuple(tiles) + (resistive, implicit, steps))
+    with tempfile.TemporaryDirectory() as d:
+        spec = case.slab_case(nr, nt, tiles, is_Lunar_resistance=resistive, use_implicit_lunar_resistance=implicit,
+                              **over)
+        case.write_case(d, spec)
+        st = case.inflow_state(spec, seed=seed)
+        rst.write(os.path.join(d, "init.rst"), st)
+        run(["run", "init.rst", str(steps), "step"], d)
+        # the initial state is regenerated from (case, seed) by the reader;
+        # the final fields are kept on the inner points only
+        arr = {}
+        r = rst.read(os.path.join(d, "step_%04d.bin" % steps))
+        for b, blk in enumerate(spec.blocks):
+            for name in LONG_FIELDS:
+                fa = r.fields[name].blocks[b]
+                hi = [n + (1 if name == "B_" + ax else 0) for n, ax in zip(blk.ncell, ("xi", "eta", "zeta"))]
+                sl = tuple(slice(-lo, -lo + h) for lo, h in zip(fa.lo, hi))
+                arr["final/b%d/%s" % (b, name)] = np.ascontiguousarray(fa.data[sl])
+        t = 0.0
+        for s_ in range(1, steps + 1):
+            t += float(rst.read(os.path.join(d, "step_%04d.bin" % s_)).fields["dt"].blocks[0].data.reshape(()))
+        arr["time"] = np.array(t)
+        arr["steps"] = np.array(steps)
+        arr["nr"] = np.array(nr)
+        arr["nt"] = np.array(nt)
+        arr["tiles"] = np.array(tiles)
+        arr["resistive"] = np.array([resistive, implicit])
+        for k, v in over.items():
+            arr["param/" + k] = np.array(v)
+        arr["seed"] = np.array(seed)
+        np.savez_compressed(os.path.join(OUT, tag + ".npz"), **arr)
+    print("wrote", tag)
+
+
 def hall(spec_kind, seed=20261205):
     """The reference's Hall edge EMF (BuildHallFaceEMF_Rusanov_diff_) of a
     seeded state: a periodic box (no walls) and a slab whose Solid_Surface
@@ -252,4 +293,8 @@ if __name__ == "__main__":
     hall("slab")
     hallstep("periodic")
     hallstep("slab")
+    slab_long()
+    slab_long(resistive=1, implicit=1, eta_max_lunar=0.1 * case.MU0 * case.ref_scales()["U"]
+              * case.ref_scales()["L_ref"], implicit_resistive_ksp_rtol=1e-12, implicit_resistive_ksp_atol=1e-30,
+              implicit_resistive_ksp_max_it=300)
     slab_owners(eta_max_lunar=1.0 * case.MU0 * case.ref_scales()["U"] * case.ref_scales()["L_ref"])
