@@ -110,12 +110,19 @@ struct mhd_ctx
     cudaGraph_t graph = nullptr, graph_a = nullptr, graph_c = nullptr;
     cudaGraphExec_t gexec = nullptr, gexec_a = nullptr, gexec_c = nullptr;
     int64_t graph_kernels = 0, graph_kernels_a = 0, graph_kernels_c = 0;
-    // device scalars
+    // independent runs (a batch): per run its dt reduction key, dt, time and
+    // step count, and the reference state of the mixed-precision flux
+    int nruns = 1;
     unsigned long long *dt_key = nullptr;
     double *dt = nullptr;
     double *time = nullptr;
     long long *step = nullptr;
     int *err = nullptr;
+    double *qref = nullptr; // [nruns][6]
+    // flattened launches (batches): block of every CTA per launch kind
+    bool flat = false;
+    int *cta_tab = nullptr;
+    int64_t cta_total[NKIND] = {0, 0, 0};
     std::map<std::string, SyncMap> syncs;
     // materialisation state: groups whose last sync ran its hot list only,
     // and PV / U_plus computed on the first ghost layer only
@@ -277,6 +284,28 @@ int64_t max_stagger(const mhd_ctx *ctx)
     return m;
 }
 
+// points of a block in a launch kind's box
+int64_t kind_points(const BlockView &v, int kind)
+{
+    if (kind == KIND_CELL0)
+        return int64_t(v.ni) * v.nj * v.nk;
+    if (kind == KIND_CELL1)
+        return int64_t(v.ni + 2) * (v.nj + 2) * (v.nk + 2);
+    return int64_t(v.ni + 1) * (v.nj + 1) * (v.nk + 1);
+}
+
+// grid of a hot-path launch: one row of exactly the CTAs every block needs
+// (batches of uneven blocks), else one row per block sized for the largest
+dim3 grid_kind(const mhd_ctx *ctx, int kind)
+{
+    if (ctx->flat)
+        return dim3(unsigned(ctx->cta_total[kind]), 1);
+    int64_t m = 0;
+    for (const auto &v : ctx->hbv)
+        m = std::max(m, kind_points(v, kind));
+    return dim3(unsigned(grid_for(m)), unsigned(ctx->nblocks));
+}
+
 int ensure_staging(mhd_ctx *ctx, size_t n)
 {
     if (ctx->staging_n >= n)
@@ -425,22 +454,20 @@ int ensure_geom(mhd_ctx *ctx)
 // among these independent fields does not change any value.
 int launch_update_derived(mhd_ctx *ctx)
 {
-    const int nb = ctx->nblocks;
     cudaStream_t s = ctx->stream;
     prof_begin(ctx, "k_bcell_jedge");
-    k_bcell_jedge<<<dim3(grid_for(max_stagger(ctx)), nb), kThreads, 0, s>>>(ctx->dbv);
+    k_bcell_jedge<<<grid_kind(ctx, KIND_STAG), kThreads, 0, s>>>(ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "B_cell"));
     RUN(run_sync(ctx, "Jedge"));
     // arm the dt reduction, then J_cell, PV / U_plus and the CFL bound of the next step
     prof_begin(ctx, "k_arm_dt");
-    k_arm_dt<<<1, 1, 0, s>>>(ctx->dt_key);
+    k_arm_dt<<<1, 128, 0, s>>>(ctx->dt_key, ctx->nruns);
     RUN(launched(ctx));
     // first ghost layer only: deeper PV / U_plus ghosts are read by no kernel
     // of the step and are filled when read out (materialise_pv)
-    const int64_t ng = max_box(ctx, LOC_CELL, 1);
     prof_begin(ctx, "k_pv_uplus_dt");
-    k_pv_uplus_dt<<<dim3(grid_for(ng), nb), kThreads, 0, s>>>(ctx->dbv, ctx->c, ctx->dt_key, 1, 1);
+    k_pv_uplus_dt<<<grid_kind(ctx, KIND_CELL1), kThreads, 0, s>>>(ctx->dbv, ctx->c, ctx->dt_key, 1, 1);
     ctx->pv_dirty = true;
     RUN(launched(ctx));
     RUN(run_sync(ctx, "J_cell"));
@@ -466,13 +493,11 @@ int launch_fluid_ucontra(mhd_ctx *ctx)
     if (ctx->pool32)
     {
         prof_begin(ctx, "k_fluid_mixed");
-        k_fluid_mixed<<<dim3(grid_for(max_box(ctx, LOC_CELL, 1)), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv,
-                                                                                                            ctx->c);
+        k_fluid_mixed<<<grid_kind(ctx, KIND_CELL1), kThreads, 0, ctx->stream>>>(ctx->dbv, ctx->c);
         return launched(ctx);
     }
     prof_begin(ctx, "k_fluid_ucontra");
-    k_fluid_ucontra<<<dim3(grid_for(max_box(ctx, LOC_CELL, 1)), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv,
-                                                                                                          ctx->c);
+    k_fluid_ucontra<<<grid_kind(ctx, KIND_CELL1), kThreads, 0, ctx->stream>>>(ctx->dbv, ctx->c);
     return launched(ctx);
 }
 
@@ -488,26 +513,25 @@ int launch_induction(mhd_ctx *ctx, bool update_b, bool with_ucontra = true)
         RUN(launched(ctx));
     }
     prof_begin(ctx, "k_eface");
-    k_eface<<<dim3(grid_for(max_stagger(ctx)), nb), kThreads, 0, s>>>(ctx->dbv);
+    k_eface<<<grid_kind(ctx, KIND_STAG), kThreads, 0, s>>>(ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Eface"));
     // inner edges; ghost edges keep their zero of AssembleRHS_Induction_CT_
     // except where the Eedge sync writes them
     prof_begin(ctx, "k_eedge");
-    k_eedge<<<dim3(grid_for(max_stagger(ctx)), nb), kThreads, 0, s>>>(ctx->dbv);
+    k_eedge<<<grid_kind(ctx, KIND_STAG), kThreads, 0, s>>>(ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Eedge"));
     prof_begin(ctx, "k_curl_e2f");
-    k_curl_e2f<<<dim3(grid_for(max_stagger(ctx)), nb), kThreads, 0, s>>>(ctx->dbv, F_Exi, F_RBxi, update_b ? F_Bxi : -1,
-                                                               -1.0, ctx->dt, 1.0, 0, nullptr);
+    k_curl_e2f<<<grid_kind(ctx, KIND_STAG), kThreads, 0, s>>>(ctx->dbv, F_Exi, F_RBxi, update_b ? F_Bxi : -1, -1.0,
+                                                             ctx->dt, 1.0, 0, nullptr);
     return launched(ctx);
 }
 
 int launch_update_u(mhd_ctx *ctx)
 {
-    const int64_t nc = max_box(ctx, LOC_CELL, 0);
     prof_begin(ctx, "k_update_u");
-    k_update_u<<<dim3(grid_for(nc), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv, ctx->dt);
+    k_update_u<<<grid_kind(ctx, KIND_CELL0), kThreads, 0, ctx->stream>>>(ctx->dbv, ctx->dt);
     return launched(ctx);
 }
 
@@ -805,7 +829,7 @@ int launch_resistive(mhd_ctx *ctx)
 int launch_step_a(mhd_ctx *ctx)
 {
     prof_begin(ctx, "k_begin_step");
-    k_begin_step<<<1, 1, 0, ctx->stream>>>(ctx->dt_key, ctx->dt, ctx->err, ctx->prm.dt_abort);
+    k_begin_step<<<1, 128, 0, ctx->stream>>>(ctx->dt_key, ctx->dt, ctx->err, ctx->prm.dt_abort, ctx->nruns);
     RUN(launched(ctx));
     RUN(launch_fluid_ucontra(ctx));
     RUN(launch_induction(ctx, /*update_b=*/true, /*with_ucontra=*/false));
@@ -816,7 +840,7 @@ int launch_step_a(mhd_ctx *ctx)
 int launch_step_c(mhd_ctx *ctx)
 {
     prof_begin(ctx, "k_end_step");
-    k_end_step<<<1, 1, 0, ctx->stream>>>(ctx->dt, ctx->time, ctx->step);
+    k_end_step<<<1, 128, 0, ctx->stream>>>(ctx->dt, ctx->time, ctx->step, ctx->nruns);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Ucell"));
     RUN(run_sync(ctx, "Bface"));
@@ -1232,13 +1256,34 @@ int run_steps(mhd_ctx *ctx, int nsteps)
 
 extern "C" {
 
-int mhd_ctx_create(const mhd_block_desc *blocks, int32_t nblocks, const mhd_params *params, mhd_ctx **out)
+namespace
 {
-    if (!blocks || nblocks <= 0 || !params || !out)
+int create_ctx(const mhd_block_desc *blocks, int32_t nblocks, const int32_t *run_of_block, int32_t nruns,
+               const mhd_params *params, mhd_ctx **out)
+{
+    if (!blocks || nblocks <= 0 || !params || !out || nruns <= 0 || nruns > nblocks)
         return MHD_EINVAL;
     *out = nullptr;
+    std::vector<int> run(size_t(nblocks), 0);
+    if (run_of_block)
+    {
+        std::vector<int> seen(size_t(nruns), 0);
+        for (int b = 0; b < nblocks; ++b)
+        {
+            if (run_of_block[b] < 0 || run_of_block[b] >= nruns)
+                return MHD_EINVAL;
+            run[size_t(b)] = run_of_block[b];
+            seen[size_t(run_of_block[b])] = 1;
+        }
+        for (int r = 0; r < nruns; ++r)
+            if (!seen[size_t(r)])
+                return MHD_EINVAL; // every run owns at least one block
+    }
+    else if (nruns != 1)
+        return MHD_EINVAL;
     mhd_ctx *ctx = new mhd_ctx;
     ctx->nblocks = nblocks;
+    ctx->nruns = nruns;
     ctx->prm = *params;
     ctx->G = params->ngg > 0 ? params->ngg : 4;
     ctx->c = Consts{params->gamma,     params->cfl, params->inver_MA2,   params->momentum_hall_coeff,
@@ -1260,6 +1305,7 @@ int mhd_ctx_create(const mhd_block_desc *blocks, int32_t nblocks, const mhd_para
             return MHD_EINVAL;
         }
         BlockView &v = ctx->hbv[size_t(b)];
+        v.run = run[size_t(b)];
         v.ni = blocks[b].ni;
         v.nj = blocks[b].nj;
         v.nk = blocks[b].nk;
@@ -1310,30 +1356,83 @@ int mhd_ctx_create(const mhd_block_desc *blocks, int32_t nblocks, const mhd_para
     }
     else if (params->precision != MHD_PREC_FP64)
         return bail(MHD_EINVAL);
+    // per-run scalars: dt keys, dt, time, step (8 bytes each per run), the
+    // error word, then the flux reference states
+    const size_t nr = size_t(nruns);
+    const size_t scal_bytes = 32 * nr + 64 + 48 * nr;
+    void *scal = nullptr;
+    if (cudaMalloc(&scal, scal_bytes) != cudaSuccess)
+        return bail(MHD_ENOMEM);
+    if (cudaMemset(scal, 0, scal_bytes) != cudaSuccess)
+        return bail(MHD_ECUDA);
+    char *sc = static_cast<char *>(scal);
+    ctx->dt_key = reinterpret_cast<unsigned long long *>(sc);
+    ctx->dt = reinterpret_cast<double *>(sc + 8 * nr);
+    ctx->time = reinterpret_cast<double *>(sc + 16 * nr);
+    ctx->step = reinterpret_cast<long long *>(sc + 24 * nr);
+    ctx->err = reinterpret_cast<int *>(sc + 32 * nr);
+    ctx->qref = reinterpret_cast<double *>(sc + 32 * nr + 64);
+    {
+        const double big = 1e100;
+        unsigned long long key;
+        std::memcpy(&key, &big, 8);
+        const std::vector<unsigned long long> keys(nr, key);
+        if (cudaMemcpy(ctx->dt_key, keys.data(), 8 * nr, cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(MHD_ECUDA);
+    }
+    for (int b = 0; b < nblocks; ++b)
+        ctx->hbv[size_t(b)].qref = ctx->qref + 6 * size_t(run[size_t(b)]);
+    // flattened launches when the batch holds several runs
+    if (nruns > 1)
+    {
+        std::vector<int> tab;
+        int64_t first[NKIND] = {0, 0, 0};
+        for (int kind = 0; kind < NKIND; ++kind)
+        {
+            first[kind] = int64_t(tab.size());
+            for (int b = 0; b < nblocks; ++b)
+            {
+                BlockView &v = ctx->hbv[size_t(b)];
+                const int64_t n = grid_for(kind_points(v, kind));
+                v.cta0[kind] = int(int64_t(tab.size()) - first[kind]);
+                tab.insert(tab.end(), size_t(n), b);
+            }
+            ctx->cta_total[kind] = int64_t(tab.size()) - first[kind];
+            if (ctx->cta_total[kind] > INT_MAX)
+                return bail(MHD_EINVAL);
+        }
+        if (cudaMalloc(&ctx->cta_tab, tab.size() * sizeof(int)) != cudaSuccess)
+            return bail(MHD_ENOMEM);
+        if (cudaMemcpy(ctx->cta_tab, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(MHD_ECUDA);
+        for (auto &v : ctx->hbv)
+            for (int kind = 0; kind < NKIND; ++kind)
+                v.cta_blk[kind] = ctx->cta_tab + first[kind];
+        ctx->flat = true;
+    }
     if (cudaMalloc(&ctx->dbv, sizeof(BlockView) * size_t(nblocks)) != cudaSuccess)
         return bail(MHD_ENOMEM);
     if (cudaMemcpy(ctx->dbv, ctx->hbv.data(), sizeof(BlockView) * size_t(nblocks), cudaMemcpyHostToDevice) !=
         cudaSuccess)
         return bail(MHD_ECUDA);
-    void *scal = nullptr;
-    if (cudaMalloc(&scal, 256) != cudaSuccess)
-        return bail(MHD_ENOMEM);
-    cudaMemset(scal, 0, 256);
-    char *sc = static_cast<char *>(scal);
-    ctx->dt_key = reinterpret_cast<unsigned long long *>(sc);
-    ctx->dt = reinterpret_cast<double *>(sc + 8);
-    ctx->time = reinterpret_cast<double *>(sc + 16);
-    ctx->step = reinterpret_cast<long long *>(sc + 24);
-    ctx->err = reinterpret_cast<int *>(sc + 32);
-    const double big = 1e100;
-    unsigned long long key;
-    std::memcpy(&key, &big, 8);
-    if (cudaMemcpy(ctx->dt_key, &key, 8, cudaMemcpyHostToDevice) != cudaSuccess)
-        return bail(MHD_ECUDA);
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
         return bail(MHD_ECUDA);
     *out = ctx;
     return MHD_OK;
+}
+} // namespace
+
+int mhd_ctx_create(const mhd_block_desc *blocks, int32_t nblocks, const mhd_params *params, mhd_ctx **out)
+{
+    return create_ctx(blocks, nblocks, nullptr, 1, params, out);
+}
+
+int mhd_batch_create(const mhd_block_desc *blocks, int32_t nblocks, const int32_t *run_of_block, int32_t nruns,
+                     const mhd_params *params, mhd_ctx **out)
+{
+    if (!run_of_block)
+        return MHD_EINVAL;
+    return create_ctx(blocks, nblocks, run_of_block, nruns, params, out);
 }
 
 int mhd_ctx_destroy(mhd_ctx *ctx)
@@ -1355,6 +1454,7 @@ int mhd_ctx_destroy(mhd_ctx *ctx)
             cudaStreamDestroy(sp);
     if (ctx->dt_key)
         cudaFree(ctx->dt_key);
+    cudaFree(ctx->cta_tab);
     cudaFree(ctx->staging);
     cudaFree(ctx->dbv);
     cudaFree(ctx->pool);
@@ -2041,6 +2141,8 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
 {
     if (!ctx || n < 0 || nalias < 0 || (n > 0 && (!unknowns || !eta)) || (nalias > 0 && (!alias || !owner || !sign)))
         return fail(ctx, MHD_EINVAL, "bad resistive arguments");
+    if (ctx->nruns > 1 && n > 0)
+        return fail(ctx, MHD_ESTATE, "the implicit resistive solve is not available in a batch of runs (one shared dt per solve)");
     if (restart <= 0 || restart > kMaxRestart)
         return fail(ctx, MHD_EINVAL, "GMRES restart must be in [1, %d]", kMaxRestart);
     if (maxit < 0)
@@ -2157,6 +2259,8 @@ int mhd_set_hall_implicit(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, int6
     if (!ctx || n < 0 || nalias < 0 || maxit < 0 || ksp_maxit < 1 || (n > 0 && !unknowns) ||
         (nalias > 0 && (!alias || !owner || !sign)))
         return fail(ctx, MHD_EINVAL, "bad implicit Hall arguments");
+    if (ctx->nruns > 1 && n > 0)
+        return fail(ctx, MHD_ESTATE, "the implicit Hall solve is not available in a batch of runs (one shared dt per solve)");
     auto &H = ctx->hall;
     for (void *p : {(void *)H.e, (void *)H.alias, (void *)H.owner, (void *)H.sign, (void *)H.bstar, (void *)H.X,
                     (void *)H.F, (void *)H.Xt, (void *)H.Ft, (void *)H.dx, (void *)H.b, (void *)H.r, (void *)H.V,
@@ -2234,6 +2338,8 @@ int mhd_set_resistive_explicit(mhd_ctx *ctx, double inver_Rem, int32_t nsub)
 {
     if (!ctx || nsub < 0)
         return fail(ctx, MHD_EINVAL, "bad explicit resistive arguments");
+    if (ctx->nruns > 1 && nsub > 0)
+        return fail(ctx, MHD_ESTATE, "the explicit resistive sub-cycling is not available in a batch of runs (one shared dt per solve)");
     if (nsub > 0 && ctx->res.on)
         return fail(ctx, MHD_ESTATE, "the implicit resistive solve is set up; the two are exclusive");
     ctx->res_nsub = nsub;
@@ -2245,19 +2351,26 @@ int mhd_set_resistive_explicit(mhd_ctx *ctx, double inver_Rem, int32_t nsub)
     return MHD_OK;
 }
 
-int mhd_set_flux_reference(mhd_ctx *ctx, const double prim[5])
+int mhd_set_flux_reference_run(mhd_ctx *ctx, int32_t run, const double prim[5])
 {
     if (!ctx || !prim)
         return fail(ctx, MHD_EINVAL, "null flux reference");
+    if (run < -1 || run >= ctx->nruns)
+        return fail(ctx, MHD_EINVAL, "run %d out of range", run);
     for (int m = 0; m < 5; ++m)
         if (!std::isfinite(prim[m]))
             return fail(ctx, MHD_EINVAL, "non-finite flux reference");
     const double rho = prim[0], u = prim[1], v = prim[2], w = prim[3], p = prim[4];
     const double q[6] = {rho, u, v, w, p, p / (ctx->c.gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w)};
-    std::memcpy(ctx->c.qref, q, sizeof(q));
-    // the constants are kernel arguments inside the captured step
-    drop_graph(ctx);
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int r = (run < 0 ? 0 : run); r < (run < 0 ? ctx->nruns : run + 1); ++r)
+        CK(ctx, cudaMemcpy(ctx->qref + 6 * size_t(r), q, sizeof(q), cudaMemcpyHostToDevice));
     return MHD_OK;
+}
+
+int mhd_set_flux_reference(mhd_ctx *ctx, const double prim[5])
+{
+    return mhd_set_flux_reference_run(ctx, -1, prim);
 }
 
 int mhd_resistive_stats(const mhd_ctx *ctx, int32_t *its, double *rnorm, double *bnorm, int32_t *reason)
@@ -2399,7 +2512,7 @@ int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
     {
     case MHD_STAGE_TIMESTEP:
         prof_begin(ctx, "k_begin_step");
-        k_begin_step<<<1, 1, 0, ctx->stream>>>(ctx->dt_key, ctx->dt, ctx->err, ctx->prm.dt_abort);
+        k_begin_step<<<1, 128, 0, ctx->stream>>>(ctx->dt_key, ctx->dt, ctx->err, ctx->prm.dt_abort, ctx->nruns);
         RUN(launched(ctx));
         break;
     case MHD_STAGE_FLUID_RHS:
@@ -2412,8 +2525,8 @@ int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
         RUN(launch_update_u(ctx));
         {
             prof_begin(ctx, "k_curl_e2f");
-            k_curl_e2f<<<dim3(grid_for(max_stagger(ctx)), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv, F_Exi, -1, F_Bxi,
-                                                                                         -1.0, ctx->dt, 1.0, 0, nullptr);
+            k_curl_e2f<<<grid_kind(ctx, KIND_STAG), kThreads, 0, ctx->stream>>>(ctx->dbv, F_Exi, -1, F_Bxi, -1.0,
+                                                                                ctx->dt, 1.0, 0, nullptr);
             RUN(launched(ctx));
         }
         break;
@@ -2452,31 +2565,41 @@ int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
     return check_err(ctx);
 }
 
-int mhd_get_time(mhd_ctx *ctx, double *dt, double *time, int64_t *step)
+int mhd_run_time(mhd_ctx *ctx, int32_t run, double *dt, double *time, int64_t *step)
 {
-    if (!ctx)
+    if (!ctx || run < 0 || run >= ctx->nruns)
         return MHD_EINVAL;
-    double d[2];
+    double d = 0.0, t = 0.0;
     long long s = 0;
-    CK(ctx, cudaMemcpy(d, ctx->dt, 16, cudaMemcpyDeviceToHost));
-    CK(ctx, cudaMemcpy(&s, ctx->step, 8, cudaMemcpyDeviceToHost));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    CK(ctx, cudaMemcpy(&d, ctx->dt + run, 8, cudaMemcpyDeviceToHost));
+    CK(ctx, cudaMemcpy(&t, ctx->time + run, 8, cudaMemcpyDeviceToHost));
+    CK(ctx, cudaMemcpy(&s, ctx->step + run, 8, cudaMemcpyDeviceToHost));
     if (dt)
-        *dt = d[0];
+        *dt = d;
     if (time)
-        *time = d[1];
+        *time = t;
     if (step)
         *step = s;
     return MHD_OK;
+}
+
+int mhd_get_time(mhd_ctx *ctx, double *dt, double *time, int64_t *step)
+{
+    return mhd_run_time(ctx, 0, dt, time, step);
 }
 
 int mhd_set_time(mhd_ctx *ctx, double dt, double time, int64_t step)
 {
     if (!ctx)
         return MHD_EINVAL;
-    const double d[2] = {dt, time};
-    const long long s = step;
-    CK(ctx, cudaMemcpy(ctx->dt, d, 16, cudaMemcpyHostToDevice));
-    CK(ctx, cudaMemcpy(ctx->step, &s, 8, cudaMemcpyHostToDevice));
+    const size_t nr = size_t(ctx->nruns);
+    const std::vector<double> d(nr, dt), t(nr, time);
+    const std::vector<long long> s(nr, step);
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    CK(ctx, cudaMemcpy(ctx->dt, d.data(), 8 * nr, cudaMemcpyHostToDevice));
+    CK(ctx, cudaMemcpy(ctx->time, t.data(), 8 * nr, cudaMemcpyHostToDevice));
+    CK(ctx, cudaMemcpy(ctx->step, s.data(), 8 * nr, cudaMemcpyHostToDevice));
     return MHD_OK;
 }
 

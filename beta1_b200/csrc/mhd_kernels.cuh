@@ -17,9 +17,6 @@ struct Consts
     double state_coeff;
     double M_H, M_ref;
     double ne_floor;
-    // mixed form: reference state rho, u, v, w, p, E about which the FP32
-    // face states are stored as deviations (zero unless set)
-    double qref[6];
 };
 
 __global__ void k_fluid_rhs(const BlockView *bvs, Consts c, int64_t maxpts);
@@ -45,9 +42,9 @@ __global__ void k_jedge(const BlockView *bvs, int fB0, int fJ0, double mult, con
 __global__ void k_jcell(const BlockView *bvs);
 __global__ void k_pv_uplus_dt(const BlockView *bvs, Consts c, unsigned long long *dt_key, int depth, int with_jcell);
 __global__ void k_bcell_jedge(const BlockView *bvs);
-__global__ void k_begin_step(const unsigned long long *dt_key, double *dt, int *err, double dt_abort);
-__global__ void k_arm_dt(unsigned long long *dt_key);
-__global__ void k_end_step(const double *dt, double *time, long long *step);
+__global__ void k_begin_step(const unsigned long long *dt_key, double *dt, int *err, double dt_abort, int nruns);
+__global__ void k_arm_dt(unsigned long long *dt_key, int nruns);
+__global__ void k_end_step(const double *dt, double *time, long long *step, int nruns);
 __global__ void k_gather(double *pool, const uint64_t *dst, const uint64_t *src, int64_t n);
 __global__ void k_set_consts(double *pool, const uint64_t *dst, const double *val, int64_t n);
 __global__ void k_wall_u(const BlockView *bvs, int blk, int dir, double gamma);

@@ -256,11 +256,12 @@ __global__ void k_ucontra(const BlockView *__restrict__ bvs)
 // same cells; U_contra is read only by the EMF kernels that follow)
 __global__ void k_fluid_ucontra(const BlockView *__restrict__ bvs, Consts c)
 {
-    const BlockView &b = bvs[blockIdx.y];
+    int64_t t;
+    const BlockView &b = bvs[cta_block(bvs, KIND_CELL1, t)];
     int lo[3], n[3];
     loc_box(b, LOC_CELL, 1, lo, n);
     int i, j, k;
-    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+    if (!box_point(lo, n, t, i, j, k))
         return;
     if (i >= 0 && j >= 0 && k >= 0 && i < b.ni && j < b.nj && k < b.nk)
         fluid_one(b, c, i, j, k);
@@ -334,7 +335,8 @@ __device__ __forceinline__ void eface_one(const BlockView &b, int fa, int i, int
 // when a region table is given; the kernels below handle all three face or
 // edge axes of a point in one thread so that the fields they share are read
 // once.
-__device__ __forceinline__ bool stagger_point(const BlockView &b, const int *rng, int blk, int &i, int &j, int &k)
+__device__ __forceinline__ bool stagger_point(const BlockView &b, const int *rng, int blk, int64_t t, int &i, int &j,
+                                              int &k)
 {
     int lo[3] = {0, 0, 0};
     int n[3] = {b.ni + 1, b.nj + 1, b.nk + 1};
@@ -347,7 +349,7 @@ __device__ __forceinline__ bool stagger_point(const BlockView &b, const int *rng
             n[a] = r[3 + a] - r[a];
         }
     }
-    return box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k);
+    return box_point(lo, n, t, i, j, k);
 }
 
 // is (i, j, k) an inner point of the face (kind 0) or edge (kind 1) axis a
@@ -360,9 +362,10 @@ __device__ __forceinline__ bool inner_of(const BlockView &b, int kind, int a, in
 
 __global__ void k_eface(const BlockView *__restrict__ bvs)
 {
-    const BlockView &b = bvs[blockIdx.y];
+    int64_t t;
+    const BlockView &b = bvs[cta_block(bvs, KIND_STAG, t)];
     int i, j, k;
-    if (!stagger_point(b, nullptr, 0, i, j, k))
+    if (!stagger_point(b, nullptr, 0, t, i, j, k))
         return;
 #pragma unroll
     for (int fa = 0; fa < 3; ++fa)
@@ -436,9 +439,10 @@ __device__ __forceinline__ double eedge_one(const BlockView &b, int ea, int i, i
 // AssembleRHS_Induction_CT_ except where the Eedge sync writes them
 __global__ void k_eedge(const BlockView *__restrict__ bvs)
 {
-    const BlockView &b = bvs[blockIdx.y];
+    int64_t t;
+    const BlockView &b = bvs[cta_block(bvs, KIND_STAG, t)];
     int i, j, k;
-    if (!stagger_point(b, nullptr, 0, i, j, k))
+    if (!stagger_point(b, nullptr, 0, t, i, j, k))
         return;
 #pragma unroll
     for (int ea = 0; ea < 3; ++ea)
@@ -454,11 +458,13 @@ __global__ void k_eedge(const BlockView *__restrict__ bvs)
 __global__ void k_curl_e2f(const BlockView *__restrict__ bvs, int fE0, int fR0, int fB0, double mult,
                            const double *__restrict__ dtp, double dtdiv, int mult_is_neg_dt, const int *__restrict__ rng)
 {
+    int64_t t;
+    const int bi = cta_block(bvs, KIND_STAG, t);
+    const BlockView &b = bvs[bi];
     if (mult_is_neg_dt)
-        mult = -dtp[0];
-    const BlockView &b = bvs[blockIdx.y];
+        mult = -dtp[b.run];
     int i, j, k;
-    if (!stagger_point(b, rng, blockIdx.y, i, j, k))
+    if (!stagger_point(b, rng, bi, t, i, j, k))
         return;
     const double *Ex = b.f[fE0], *Ee = b.f[fE0 + 1], *Ez = b.f[fE0 + 2];
     const int64_t p = pidx(b, i, j, k);
@@ -479,7 +485,7 @@ __global__ void k_curl_e2f(const BlockView *__restrict__ bvs, int fE0, int fR0, 
             b.f[fR0 + fa][p] = rhs;
         if (fB0 >= 0)
         {
-            const double dt = dtp[0] / dtdiv;
+            const double dt = dtp[b.run] / dtdiv;
             b.f[fB0 + fa][p] += dt * rhs;
         }
     }
@@ -510,9 +516,10 @@ __global__ void k_divb(const BlockView *__restrict__ bvs)
 // cell current of the four cells around the edge; zero elsewhere.
 __global__ void k_eres_explicit(const BlockView *__restrict__ bvs, double inver_Rem)
 {
-    const BlockView &b = bvs[blockIdx.y];
+    int64_t t;
+    const BlockView &b = bvs[cta_block(bvs, KIND_STAG, t)];
     int i, j, k;
-    if (!stagger_point(b, nullptr, 0, i, j, k))
+    if (!stagger_point(b, nullptr, 0, t, i, j, k))
         return;
     const double *Jc = b.f[F_Jcell];
     const int64_t v = b.vol;
@@ -657,9 +664,11 @@ __device__ __forceinline__ double hall_edge_one(const BlockView &b, int ea, int 
 // block, edge axis, lo[3], hi[3] (Solid_Surface layers and Pole edges)
 __global__ void k_hall_edge(const BlockView *__restrict__ bvs, const int *__restrict__ zb, int nzb)
 {
-    const BlockView &b = bvs[blockIdx.y];
+    int64_t t;
+    const int bi = cta_block(bvs, KIND_STAG, t);
+    const BlockView &b = bvs[bi];
     int i, j, k;
-    if (!stagger_point(b, nullptr, 0, i, j, k))
+    if (!stagger_point(b, nullptr, 0, t, i, j, k))
         return;
     const int64_t p = pidx(b, i, j, k);
 #pragma unroll
@@ -671,7 +680,7 @@ __global__ void k_hall_edge(const BlockView *__restrict__ bvs, const int *__rest
         for (int q = 0; q < nzb && !zero; ++q)
         {
             const int *z = zb + 8 * q;
-            zero = (z[0] == int(blockIdx.y) && z[1] == ea && i >= z[2] && j >= z[3] && k >= z[4] && i < z[5] &&
+            zero = (z[0] == bi && z[1] == ea && i >= z[2] && j >= z[3] && k >= z[4] && i < z[5] &&
                     j < z[6] && k < z[7]);
         }
         b.f[F_Ehxi + ea][p] = zero ? 0.0 : hall_edge_one(b, ea, i, j, k);
@@ -681,13 +690,14 @@ __global__ void k_hall_edge(const BlockView *__restrict__ bvs, const int *__rest
 // cell part of ApplyUpdate_Euler_ (LunarSolver_Advance.cpp:82-93): U += dt*RHS_H
 __global__ void k_update_u(const BlockView *__restrict__ bvs, const double *__restrict__ dtp)
 {
-    const BlockView &b = bvs[blockIdx.y];
+    int64_t t;
+    const BlockView &b = bvs[cta_block(bvs, KIND_CELL0, t)];
     int lo[3], n[3];
     loc_box(b, LOC_CELL, 0, lo, n);
     int i, j, k;
-    if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+    if (!box_point(lo, n, t, i, j, k))
         return;
-    const double dt = dtp[0];
+    const double dt = dtp[b.run];
     const int64_t p = pidx(b, i, j, k);
 #pragma unroll
     for (int m = 0; m < 5; ++m)
@@ -775,9 +785,11 @@ __device__ __forceinline__ void jedge_one(const BlockView &b, int ea, int i, int
 
 __global__ void k_jedge(const BlockView *__restrict__ bvs, int fB0, int fJ0, double mult, const int *__restrict__ rng)
 {
-    const BlockView &b = bvs[blockIdx.y];
+    int64_t t;
+    const int bi = cta_block(bvs, KIND_STAG, t);
+    const BlockView &b = bvs[bi];
     int i, j, k;
-    if (!stagger_point(b, rng, blockIdx.y, i, j, k))
+    if (!stagger_point(b, rng, bi, t, i, j, k))
         return;
 #pragma unroll
     for (int ea = 0; ea < 3; ++ea)
@@ -790,9 +802,10 @@ __global__ void k_jedge(const BlockView *__restrict__ bvs, int fB0, int fJ0, dou
 // the reference touches neither input)
 __global__ void k_bcell_jedge(const BlockView *__restrict__ bvs)
 {
-    const BlockView &b = bvs[blockIdx.y];
+    int64_t t;
+    const BlockView &b = bvs[cta_block(bvs, KIND_STAG, t)];
     int i, j, k;
-    if (!stagger_point(b, nullptr, 0, i, j, k))
+    if (!stagger_point(b, nullptr, 0, t, i, j, k))
         return;
     if (i < b.ni && j < b.nj && k < b.nk)
         bcell_one(b, i, j, k);
@@ -885,12 +898,13 @@ __device__ __forceinline__ unsigned long long dbl_key(double x)
 __global__ void k_pv_uplus_dt(const BlockView *__restrict__ bvs, Consts c, unsigned long long *dt_key, int depth,
                               int with_jcell)
 {
-    const BlockView &b = bvs[blockIdx.y];
+    int64_t t;
+    const BlockView &b = bvs[cta_block(bvs, KIND_CELL1, t)];
     int lo[3], n[3];
     loc_box(b, LOC_CELL, depth, lo, n);
     int i, j, k;
     double dtc = 1e100;
-    if (box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
+    if (box_point(lo, n, t, i, j, k))
     {
         // calc_Jcell on inner cells in the same pass: its weight stream
         // overlaps this kernel's FP64 work (J_cell is not read here)
@@ -933,12 +947,13 @@ __global__ void k_pv_uplus_dt(const BlockView *__restrict__ bvs, Consts c, unsig
                 // FP32 face states of the mixed-precision flux: deviations
                 // from the reference state (formed in FP64), sound speed
                 float *q = b.q32;
-                q[Q32_RHO * v + p] = float(U0 - c.qref[0]);
-                q[(Q32_U + 0) * v + p] = float(u - c.qref[1]);
-                q[(Q32_U + 1) * v + p] = float(vv - c.qref[2]);
-                q[(Q32_U + 2) * v + p] = float(w - c.qref[3]);
-                q[Q32_P * v + p] = float(pr - c.qref[4]);
-                q[Q32_RHOE * v + p] = float(rhoe - c.qref[5]);
+                const double *q0 = b.qref;
+                q[Q32_RHO * v + p] = float(U0 - q0[0]);
+                q[(Q32_U + 0) * v + p] = float(u - q0[1]);
+                q[(Q32_U + 1) * v + p] = float(vv - q0[2]);
+                q[(Q32_U + 2) * v + p] = float(w - q0[3]);
+                q[Q32_P * v + p] = float(pr - q0[4]);
+                q[Q32_RHOE * v + p] = float(rhoe - q0[5]);
                 q[Q32_C * v + p] = float(cs);
             }
         }
@@ -1000,28 +1015,38 @@ __global__ void k_pv_uplus_dt(const BlockView *__restrict__ bvs, Consts c, unsig
             key = (o < key) ? o : key;
         }
         if (lane == 0)
-            atomicMin(dt_key, key);
+            atomicMin(dt_key + b.run, key);
     }
 }
 
 // Start of StepOnce: dt = global minimum of the CFL bounds, abort check
 // (dt < dt_abort or NaN sets the error word, LunarSolver_Timestep.cpp:128-139).
-__global__ void k_begin_step(const unsigned long long *dt_key, double *dt, int *err, double dt_abort)
+__global__ void k_begin_step(const unsigned long long *dt_key, double *dt, int *err, double dt_abort, int nruns)
 {
-    const double d = __longlong_as_double((long long)dt_key[0]);
-    dt[0] = d;
-    if (!isfinite(d) || d < dt_abort)
-        err[0] = MHD_EDT;
+    for (int r = threadIdx.x; r < nruns; r += blockDim.x)
+    {
+        const double d = __longlong_as_double((long long)dt_key[r]);
+        dt[r] = d;
+        if (!isfinite(d) || d < dt_abort)
+            err[0] = MHD_EDT;
+    }
 }
 
-// Arms the dt reduction with the reference's initial bound (dt_local = 1e100).
-__global__ void k_arm_dt(unsigned long long *dt_key) { dt_key[0] = dbl_key(1e100); }
+// Arms the dt reductions with the reference's initial bound (dt_local = 1e100).
+__global__ void k_arm_dt(unsigned long long *dt_key, int nruns)
+{
+    for (int r = threadIdx.x; r < nruns; r += blockDim.x)
+        dt_key[r] = dbl_key(1e100);
+}
 
 // End of StepOnce: run-data counters (Z4_Lunar/src/LunarSolver_Driver.cpp:75-79)
-__global__ void k_end_step(const double *dt, double *time, long long *step)
+__global__ void k_end_step(const double *dt, double *time, long long *step, int nruns)
 {
-    time[0] += dt[0];
-    step[0] += 1;
+    for (int r = threadIdx.x; r < nruns; r += blockDim.x)
+    {
+        time[r] += dt[r];
+        step[r] += 1;
+    }
 }
 
 // ---------------------------------------------------------------------------

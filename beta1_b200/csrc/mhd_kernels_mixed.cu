@@ -88,10 +88,10 @@ __device__ __forceinline__ void rusanov_dev32(const BlockView &b, const Ref32 &r
 // FP64 face metric read for the velocities is the one the fluxes round.
 __global__ void k_fluid_mixed(const BlockView *__restrict__ bvs, Consts c)
 {
-    const BlockView &b = bvs[blockIdx.y];
+    int64_t t;
+    const BlockView &b = bvs[cta_block(bvs, KIND_CELL1, t)];
     const int lo = -1;
     const int n0 = b.ni + 2, n1 = b.nj + 2, n2 = b.nk + 2;
-    int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= int64_t(n0) * n1 * n2)
         return;
     const int k = lo + int(t % n2);
@@ -129,8 +129,8 @@ __global__ void k_fluid_mixed(const BlockView *__restrict__ bvs, Consts c)
         return;
     const float *g = b.g32;
     const int64_t pm[3] = {pidx(b, i - 1, j, k), pidx(b, i, j - 1, k), pidx(b, i, j, k - 1)};
-    const Ref32 r0 = {float(c.qref[0]), {float(c.qref[1]), float(c.qref[2]), float(c.qref[3])},
-                      float(c.qref[5] + c.qref[4])};
+    const double *q0 = b.qref;
+    const Ref32 r0 = {float(q0[0]), {float(q0[1]), float(q0[2]), float(q0[3])}, float(q0[5] + q0[4])};
     float r[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
     double S[3] = {0.0, 0.0, 0.0}; // sum of the signed face vectors of the cell
 #pragma unroll
@@ -149,10 +149,10 @@ __global__ void k_fluid_mixed(const BlockView *__restrict__ bvs, Consts c)
             S[d] += kp[dir][d] - km[dir][d];
     }
     // divergence of the reference-state flux, FP64: Phi0(S)
-    const double US = S[0] * c.qref[1] + S[1] * c.qref[2] + S[2] * c.qref[3];
-    const double mS = c.qref[0] * US;
-    const double phi[5] = {mS, mS * c.qref[1] + S[0] * c.qref[4], mS * c.qref[2] + S[1] * c.qref[4],
-                           mS * c.qref[3] + S[2] * c.qref[4], US * (c.qref[5] + c.qref[4])};
+    const double US = S[0] * q0[1] + S[1] * q0[2] + S[2] * q0[3];
+    const double mS = q0[0] * US;
+    const double phi[5] = {mS, mS * q0[1] + S[0] * q0[4], mS * q0[2] + S[1] * q0[4], mS * q0[3] + S[2] * q0[4],
+                           US * (q0[5] + q0[4])};
     // J x B force with the Hall_Num_Limiter weight, FP64
     const double rho = b.f[F_U][p];
     const double n_true = ((rho < 0.0) ? 0.0 : rho) / c.M_H * c.M_ref;

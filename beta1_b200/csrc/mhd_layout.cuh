@@ -128,7 +128,43 @@ struct BlockView
     // mixed precision only (null otherwise): FP32 planes on the same padded box
     float *g32;       // face area xi, eta, zeta
     float *q32;       // face-state quantities rho, u, v, w, p, rhoE, c
+    // run (independent time line) the block belongs to, and that run's
+    // reference state of the mixed-precision flux (rho, u, v, w, p, E)
+    int run;
+    const double *qref;
+    // flattened launches over blocks of uneven sizes: per launch kind the
+    // block of every CTA (same table in every view; null = 2-D launches with
+    // one grid row per block) and this block's first CTA
+    const int *cta_blk[3];
+    int cta0[3];
 };
+
+// launch kinds of the flattened grids: cells with depth 0, cells with depth
+// 1, and the staggered box [0, n + 1)^3 of the face / edge kernels
+enum : int
+{
+    KIND_CELL0 = 0,
+    KIND_CELL1 = 1,
+    KIND_STAG = 2,
+    NKIND = 3
+};
+
+#ifdef __CUDACC__
+// Block and thread-in-block of the calling thread: flattened launches (one
+// grid row) look the block up per CTA, 2-D launches take blockIdx.y.
+__device__ __forceinline__ int cta_block(const BlockView *bvs, int kind, int64_t &t)
+{
+    const int *tab = bvs[0].cta_blk[kind];
+    if (tab && gridDim.y == 1)
+    {
+        const int bi = tab[blockIdx.x];
+        t = int64_t(blockIdx.x - bvs[bi].cta0[kind]) * blockDim.x + threadIdx.x;
+        return bi;
+    }
+    t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    return int(blockIdx.y);
+}
+#endif
 
 // plane indices of BlockView::g32 / q32
 enum : int

@@ -126,7 +126,22 @@ def _idx(lo, hi):
 
 
 def _take(P: Padded, I, J, K):
+    """P at the logical points (I, J, K).  The callers pass index grids of a
+    box (from _idx) shifted by constants, which become a strided slice; any
+    other index arrays take the general gather."""
     o = P.off
+    n = I.shape
+    if len(n) == 3 and J.shape == n and K.shape == n and min(n) > 0:
+        i0, j0, k0 = int(I[0, 0, 0]), int(J[0, 0, 0]), int(K[0, 0, 0])
+        if (I[-1, 0, 0] - i0 == n[0] - 1 and J[0, -1, 0] - j0 == n[1] - 1 and K[0, 0, -1] - k0 == n[2] - 1
+                and I[0, -1, -1] == i0 and J[-1, 0, -1] == j0 and K[-1, -1, 0] == k0
+                and np.array_equal(I[:, 0, 0], np.arange(i0, i0 + n[0]))
+                and np.array_equal(J[0, :, 0], np.arange(j0, j0 + n[1]))
+                and np.array_equal(K[0, 0, :], np.arange(k0, k0 + n[2]))
+                and i0 + o >= 0 and j0 + o >= 0 and k0 + o >= 0):
+            # a grid iff each index varies along its own axis only
+            if ((I == I[:, :1, :1]).all() and (J == J[:1, :, :1]).all() and (K == K[:1, :1, :]).all()):
+                return P.a[i0 + o:i0 + o + n[0], j0 + o:j0 + o + n[1], k0 + o:k0 + o + n[2]]
     return P.a[I + o, J + o, K + o]
 
 

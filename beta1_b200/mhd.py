@@ -44,6 +44,11 @@ class Params(C.Structure):
 # every symbol the header declares, with its signature
 _SIGS = {
     "mhd_ctx_create": (C.c_int, [C.POINTER(BlockDesc), C.c_int32, C.POINTER(Params), C.POINTER(C.c_void_p)]),
+    "mhd_batch_create": (C.c_int, [C.POINTER(BlockDesc), C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.POINTER(Params),
+                                   C.POINTER(C.c_void_p)]),
+    "mhd_run_time": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                               C.POINTER(C.c_int64)]),
+    "mhd_set_flux_reference_run": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
     "mhd_ctx_destroy": (C.c_int, [C.c_void_p]),
     "mhd_last_error": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),
     "mhd_field_info": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
@@ -151,11 +156,19 @@ class HostLayout:
 class Context:
     """One device context (all blocks of one grid on the current GPU)."""
 
-    def __init__(self, ncells: Sequence[Sequence[int]], params: Params):
+    def __init__(self, ncells: Sequence[Sequence[int]], params: Params, runs: Optional[Sequence[int]] = None):
+        """runs: the run of every block for a batch of independent runs
+        (mhd_batch_create); None for one run."""
         self.lib = load()
         arr = (BlockDesc * len(ncells))(*[BlockDesc(*map(int, n)) for n in ncells])
         h = C.c_void_p()
-        rc = self.lib.mhd_ctx_create(arr, len(ncells), C.byref(params), C.byref(h))
+        if runs is None:
+            self.nruns = 1
+            rc = self.lib.mhd_ctx_create(arr, len(ncells), C.byref(params), C.byref(h))
+        else:
+            self.nruns = int(max(runs)) + 1
+            ra = (C.c_int32 * len(runs))(*[int(r) for r in runs])
+            rc = self.lib.mhd_batch_create(arr, len(ncells), ra, self.nruns, C.byref(params), C.byref(h))
         if rc != MHD_OK:
             raise MHDError(f"mhd_ctx_create failed: {ERRORS.get(rc, rc)}")
         self.h = h
@@ -265,10 +278,20 @@ class Context:
     def set_resistive_explicit(self, inver_Rem: float, nsub: int):
         self._check(self.lib.mhd_set_resistive_explicit(self.h, float(inver_Rem), int(nsub)), "set_resistive_explicit")
 
-    def set_flux_reference(self, prim):
-        """reference state (rho, u, v, w, p) of the mixed-precision deviation flux"""
+    def set_flux_reference(self, prim, run: int = -1):
+        """reference state (rho, u, v, w, p) of the mixed-precision deviation
+        flux, of one run of a batch or (run -1) of every run"""
         a = (C.c_double * 5)(*[float(x) for x in prim])
-        self._check(self.lib.mhd_set_flux_reference(self.h, a), "set_flux_reference")
+        if run < 0:
+            self._check(self.lib.mhd_set_flux_reference(self.h, a), "set_flux_reference")
+        else:
+            self._check(self.lib.mhd_set_flux_reference_run(self.h, int(run), a), "set_flux_reference_run")
+
+    def run_time(self, run: int):
+        """(dt of the last step, time, step count) of one run"""
+        dt, t, n = C.c_double(), C.c_double(), C.c_int64()
+        self._check(self.lib.mhd_run_time(self.h, int(run), C.byref(dt), C.byref(t), C.byref(n)), "run_time")
+        return dt.value, t.value, n.value
 
     def resistive_stats(self):
         its, rn, bn, rs = C.c_int32(), C.c_double(), C.c_double(), C.c_int32()

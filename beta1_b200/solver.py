@@ -222,3 +222,121 @@ class Solver:
 
     def field(self, name, block=0) -> np.ndarray:
         return self.ctx.download(name, block)
+
+
+def host_setup(spec: case_mod.CaseSpec):
+    """Host-side geometry of a case: per block the ghost node mesh and the
+    geometry fields (a pure function of the grid, safe to run in worker
+    processes)."""
+    ngg = int(spec.params["ngg"])
+    nodes, geom = [], []
+    for b in spec.blocks:
+        X = geometry.ghost_mesh(b.x, b.y, b.z, ngg)
+        nodes.append(X)
+        geom.append(geometry.build(X, b.ncell, ngg))
+    return nodes, geom
+
+
+def _farfield_prim(params):
+    q0, _ = physics.farfield_state(params)
+    u0 = [q0[1] / q0[0], q0[2] / q0[0], q0[3] / q0[0]]
+    p0 = (physics.constants(params)["gamma"] - 1.0) * (q0[4] - 0.5 * q0[0] * (u0[0] ** 2 + u0[1] ** 2 + u0[2] ** 2))
+    return [q0[0]] + u0 + [p0]
+
+
+class Batch:
+    """Independent runs in one context (mhd_batch_create): a parameter sweep
+    whose runs differ in grid size, inflow and IMF, each with its own time
+    step, all advanced by one step graph.  runs: (case spec, topology) per
+    run, topology "periodic" (one block) or "tiled"; the runs must agree on
+    the constants of the step (gamma, CFL, the J x B and state scales) and
+    may not use the resistive or Hall solves.  host: optional host_setup()
+    result per run (e.g. computed by a process pool)."""
+
+    CONSTS = ("gamma", "cfl", "inver_MA2", "momentum_hall_coeff", "state_coeff", "M_H", "M_ref", "ne_hall_floor")
+
+    def __init__(self, runs, precision=mhd.PREC_FP64, host=None):
+        self.runs = [(spec, topo) for spec, topo in runs]
+        c0 = physics.constants(self.runs[0][0].params)
+        for spec, topo in self.runs:
+            c = physics.constants(spec.params)
+            bad = [k for k in self.CONSTS if c[k] != c0[k]]
+            if bad:
+                raise ValueError(f"runs of a batch must share the step constants; differing: {bad}")
+            if spec.params.get("is_Lunar_resistance", 0):
+                raise ValueError("resistive runs cannot be batched")
+            if topo == "periodic" and len(spec.blocks) != 1:
+                raise ValueError("a periodic run has one block")
+        ncells, run_of, self.offset = [], [], []
+        for r, (spec, _) in enumerate(self.runs):
+            self.offset.append(len(ncells))
+            ncells += [b.ncell for b in spec.blocks]
+            run_of += [r] * len(spec.blocks)
+        self.ctx = mhd.Context(ncells, make_params(self.runs[0][0].params, precision), runs=run_of)
+        if host is None:
+            host = [host_setup(spec) for spec, _ in self.runs]
+        tables = {}
+        zero_rows = []
+        for r, ((spec, topo), (nodes, geom)) in enumerate(zip(self.runs, host)):
+            off = self.offset[r]
+            q, B = physics.farfield_state(spec.params)
+            for ib, g in enumerate(geom):
+                for name in GEOM_FIELDS:
+                    self.ctx.upload(name, off + ib, g[name][2])
+                if any(v != 0.0 for v in B):
+                    for fname, jd in (("Badd_xi", "JDxi"), ("Badd_eta", "JDet"), ("Badd_zeta", "JDze")):
+                        self.ctx.upload(fname, off + ib, badd_faces(g[jd][2], B))
+            lay = mhd.HostLayout([b.ncell for b in spec.blocks])
+            if topo == "periodic":
+                maps = syncmap.periodic_maps(lay, spec.blocks[0].ncell)
+            elif topo == "tiled":
+                u = [q[1] / q[0], q[2] / q[0], q[3] / q[0]]
+                E_inf = [B[1] * u[2] - B[2] * u[1], B[2] * u[0] - B[0] * u[2], B[0] * u[1] - B[1] * u[0]]
+                maps = syncmap.compile_tiled(lay, syncmap.TiledLayout(spec.blocks[0].ncell, spec.tiles), False,
+                                             dict(qinf=q, B_imf=B, E_inf=E_inf), nodes)
+            else:
+                raise ValueError(f"unknown topology {topo}")
+            for group, m in syncmap.shift_blocks(maps, off).items():
+                tables.setdefault(group, []).append(m)
+            for ib, b in enumerate(spec.blocks):
+                n = b.ncell
+                patches = [("Solid_Surface", -1, (0, 0, 0), (1, n[1] + 1, n[2] + 1))] if topo == "tiled" else []
+                zero_rows += [[off + ib] + row for row in hall_zero_boxes(n, patches)]
+            if precision == mhd.PREC_MIXED:
+                self.ctx.set_flux_reference(_farfield_prim(spec.params), run=r)
+        self.sync_sizes = {}
+        for group, ms in tables.items():
+            dst = np.concatenate([m["dst"] for m in ms])
+            src = np.concatenate([m["src"] for m in ms])
+            cdst = np.concatenate([m["cdst"] for m in ms])
+            cval = np.concatenate([m["cval"] for m in ms])
+            self.ctx.set_sync_map(group, dst, src)
+            if cdst.size:
+                self.ctx.set_sync_consts(group, cdst, cval)
+            walls = [w for m in ms for w in m["walls"]]
+            for (b, d) in walls:
+                self.ctx.set_sync_wall(group, b, d)
+            self.sync_sizes[group] = (int(dst.size), int(cdst.size), len(walls))
+        self.ctx.sync("Badd")
+        self.ctx.set_hall(c0["hall_coef"], zero_rows)
+
+    @property
+    def cells(self):
+        return [sum(b.ncell[0] * b.ncell[1] * b.ncell[2] for b in spec.blocks) for spec, _ in self.runs]
+
+    def load_states(self, states):
+        """Restart state of every run, then the syncs and UpdateDerivedFields_."""
+        for r, st in enumerate(states):
+            for name in STATE_FIELDS:
+                for ib, fa in enumerate(st.fields[name].blocks):
+                    self.ctx.upload(name, self.offset[r] + ib, fa.data)
+        self.ctx.sync("Ucell")
+        self.ctx.sync("Bface")
+        self.ctx.update_derived()
+
+    def step(self, n=1):
+        return self.ctx.step(n)
+
+    def field(self, run, name, block=0) -> np.ndarray:
+        return self.ctx.download(name, self.offset[run] + block)
+

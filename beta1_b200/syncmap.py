@@ -70,9 +70,10 @@ def periodic_field_map(info: dict, ncell: Tuple[int, int, int]):
     return np.concatenate(dst).astype(np.int64), np.concatenate(src).astype(np.int64)
 
 
-def install_periodic(ctx, ncell) -> Dict[str, int]:
-    """Sets the periodic gather table of every group on a one-block context."""
-    sizes = {}
+def periodic_maps(ctx, ncell) -> Dict[str, dict]:
+    """group -> gather table (dst, src point ids; no constants or walls) of
+    the periodic one-block layout; ctx: a context or a HostLayout."""
+    out = {}
     for group, fields in GROUPS.items():
         dsts, srcs = [], []
         for f in fields:
@@ -81,11 +82,26 @@ def install_periodic(ctx, ncell) -> Dict[str, int]:
             d, s = periodic_field_map(info, ncell)
             dsts.append(d + base)
             srcs.append(s + base)
-        dst = np.concatenate(dsts)
-        src = np.concatenate(srcs)
-        ctx.set_sync_map(group, dst, src)
-        sizes[group] = int(dst.size)
+        out[group] = dict(dst=np.concatenate(dsts), src=np.concatenate(srcs), cdst=np.zeros(0, dtype=np.int64),
+                          cval=np.zeros(0), walls=[])
+    return out
+
+
+def install_periodic(ctx, ncell) -> Dict[str, int]:
+    """Sets the periodic gather table of every group on a one-block context."""
+    sizes = {}
+    for group, m in periodic_maps(ctx, ncell).items():
+        ctx.set_sync_map(group, m["dst"], m["src"])
+        sizes[group] = int(m["dst"].size)
     return sizes
+
+
+def shift_blocks(maps: Dict[str, dict], off: int) -> Dict[str, dict]:
+    """The tables of a layout whose blocks become blocks off, off + 1, ... of
+    a larger context (point ids carry the block in bits 40-55)."""
+    sh = np.int64(off) << np.int64(40)
+    return {g: dict(dst=m["dst"] + sh, src=m["src"] + sh, cdst=m["cdst"] + sh, cval=m["cval"],
+                    walls=[(b + off, d) for (b, d) in m["walls"]]) for g, m in maps.items()}
 
 
 # ---------------------------------------------------------------------------

@@ -77,6 +77,25 @@ typedef struct
    on the current CUDA device, zero-filled. */
 int mhd_ctx_create(const mhd_block_desc *blocks, int32_t nblocks, const mhd_params *params, mhd_ctx **out);
 
+/* A batch of independent runs in one context (no counterpart in the
+   reference, which advances one grid per process): run_of_block[b] in
+   [0, nruns) names the run of block b, every run owns at least one block.
+   Each run has its own time step (the CFL minimum over its own blocks), time
+   and step count; the blocks of all runs advance together, every hot-path
+   stage as one launch whose grid holds exactly the CTAs of every block
+   (blocks of uneven sizes waste no CTAs), and the whole step is one CUDA
+   graph.  Blocks of different runs share no halo: the sync tables the caller
+   installs connect blocks of the same run only.  Every other entry point
+   works on a batch, with block indices over all runs; mhd_step and
+   mhd_get_time report run 0, mhd_run_time any run.  The implicit resistive
+   and Hall solves and the explicit resistive sub-cycles are rejected on a
+   batch (MHD_ESTATE). */
+int mhd_batch_create(const mhd_block_desc *blocks, int32_t nblocks, const int32_t *run_of_block, int32_t nruns,
+                     const mhd_params *params, mhd_ctx **out);
+
+/* dt of the last step, simulated time and step count of one run. */
+int mhd_run_time(mhd_ctx *ctx, int32_t run, double *dt, double *time, int64_t *step);
+
 /* ~LunarSolver / delete fld (Z4_Lunar/main.cpp:216-222). */
 int mhd_ctx_destroy(mhd_ctx *ctx);
 
@@ -217,9 +236,12 @@ int mhd_set_resistive_explicit(mhd_ctx *ctx, double inver_Rem, int32_t nsub);
    in deviation form, with the reference-state part added in FP64, so the
    FP32 rounding scales with the departure from this state.  Any state gives
    the same result up to that rounding (zero, the default, is the plain FP32
-   flux).  Takes effect at the next UpdateDerivedFields_ (mhd_update_derived,
-   or the end of a step); has no effect in MHD_PREC_FP64. */
+   flux).  Sets every run of a batch.  Takes effect at the next
+   UpdateDerivedFields_ (mhd_update_derived, or the end of a step); has no
+   effect in MHD_PREC_FP64. */
 int mhd_set_flux_reference(mhd_ctx *ctx, const double prim[5]);
+/* The same for one run of a batch (run -1: every run). */
+int mhd_set_flux_reference_run(mhd_ctx *ctx, int32_t run, const double prim[5]);
 
 /* Iterations, final residual norm, ||b|| and convergence reason (2 rtol,
    3 atol, -3 iteration limit, as KSPConvergedReason) of the last solve. */
@@ -265,7 +287,8 @@ int mhd_host_free(void *ptr);
 #define MHD_STAGE_HALL_SOLVE 7 /* ImplicitHallSolver::SolveOneStep at the current dt, then calc_Bcell */
 int mhd_stage(mhd_ctx *ctx, int32_t stage_id);
 
-/* Current dt / time / step counters (device -> host). */
+/* Current dt / time / step counters (device -> host; run 0 of a batch).
+   mhd_set_time sets every run. */
 int mhd_get_time(mhd_ctx *ctx, double *dt, double *time, int64_t *step);
 int mhd_set_time(mhd_ctx *ctx, double dt, double time, int64_t step);
 

@@ -53,3 +53,18 @@ def slab_setup(g):
             rec.blocks.append(rst.FieldArray(lo, tuple(l + s for l, s in zip(lo, a.shape[:3])), a))
         st.fields[name] = rec
     return spec, st
+
+
+def periodic_setup(g):
+    """(case spec, restart state) of the committed periodic fixture."""
+    from beta1_b200 import case, rst
+    n = tuple(int(v) for v in g["n"])
+    spec = case.periodic_box_case(n)
+    st = rst.RestartFile(0, 0.0, 1, {})
+    for name, loc in (("U_H", rst.CELL), ("B_xi", rst.FACE_XI), ("B_eta", rst.FACE_ET), ("B_zeta", rst.FACE_ZE)):
+        a = g["init/" + name]
+        lo = tuple(int(v) for v in g["init/" + name + "__lo"])
+        hi = tuple(l + s for l, s in zip(lo, a.shape[:3]))
+        st.fields[name] = rst.FieldRecord(name, loc, a.shape[3], 4, [rst.FieldArray(lo, hi, a)])
+    return spec, st
+

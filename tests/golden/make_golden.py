@@ -287,6 +287,8 @@ if __name__ == "__main__":
     # explicit resistive sub-cycles (two per step) with the same resistivity
     slab(steps=2, resistive=1, implicit=0, eta_max_lunar=1.0 * case.MU0 * case.ref_scales()["U"]
          * case.ref_scales()["L_ref"], n_resistive_subcycles=2)
+    # one block periodic onto itself across the transverse directions
+    slab(steps=2, tiles=(1, 1))
     slab_probe(resistive=0)
     slab_probe(resistive=1)
     hall("periodic")

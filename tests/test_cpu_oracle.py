@@ -104,7 +104,8 @@ def test_oracle_dt_exact(oracle_run):
 SLAB_FIELDS = COMPARE + ["Eres_xi", "Eres_eta", "Eres_zeta"]
 SLAB_CASES = {"ideal": ("slab_6x5x6_t2x2_r00_steps.npz", 1e-12),
               "implicit_resistive": ("slab_6x5x6_t2x2_r11_steps.npz", 1e-10),
-              "explicit_resistive": ("slab_6x5x6_t2x2_r10_steps.npz", 1e-12)}
+              "explicit_resistive": ("slab_6x5x6_t2x2_r10_steps.npz", 1e-12),
+              "single_tile": ("slab_6x5x6_t1x1_r00_steps.npz", 1e-12)}
 
 
 def build_slab_oracle(g):

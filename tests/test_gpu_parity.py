@@ -10,7 +10,7 @@ separately for the conserved state.
 import numpy as np
 import pytest
 
-from conftest import rel_l2
+from conftest import periodic_setup, rel_l2
 
 from beta1_b200 import case, mhd, rst, solver
 
@@ -22,22 +22,10 @@ COMPARE = ["U_H", "B_xi", "B_eta", "B_zeta", "PV_H", "U_plus", "B_cell", "Bind_c
            "RHS_B_eta", "RHS_B_zeta", "divB"]
 
 
-def _init_state(g):
-    n = tuple(int(v) for v in g["n"])
-    spec = case.periodic_box_case(n)
-    st = rst.RestartFile(0, 0.0, 1, {})
-    for name, loc in (("U_H", rst.CELL), ("B_xi", rst.FACE_XI), ("B_eta", rst.FACE_ET), ("B_zeta", rst.FACE_ZE)):
-        a = g["init/" + name]
-        lo = tuple(int(v) for v in g["init/" + name + "__lo"])
-        hi = tuple(l + s for l, s in zip(lo, a.shape[:3]))
-        st.fields[name] = rst.FieldRecord(name, loc, a.shape[3], 4, [rst.FieldArray(lo, hi, a)])
-    return spec, st
-
-
 @pytest.fixture(scope="module")
 def run_periodic(golden_periodic):
     g = golden_periodic["steps"]
-    spec, st = _init_state(g)
+    spec, st = periodic_setup(g)
     s = solver.Solver(spec)
     s.load_state(st)
     s.ctx.stage(mhd.STAGE_DIVB)

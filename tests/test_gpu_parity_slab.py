@@ -27,7 +27,8 @@ FIELDS = ["Eres_xi", "Eres_eta", "Eres_zeta", "U_H", "B_xi", "B_eta", "B_zeta", 
           "RHS_B_eta", "RHS_B_zeta", "divB"]
 CASES = {"ideal": ("slab_6x5x6_t2x2_r00_steps.npz", 1e-12),
          "implicit_resistive": ("slab_6x5x6_t2x2_r11_steps.npz", 1e-10),
-         "explicit_resistive": ("slab_6x5x6_t2x2_r10_steps.npz", 1e-12)}
+         "explicit_resistive": ("slab_6x5x6_t2x2_r10_steps.npz", 1e-12),
+         "single_tile": ("slab_6x5x6_t1x1_r00_steps.npz", 1e-12)}
 
 
 @pytest.fixture(scope="module", params=list(CASES))

@@ -15,7 +15,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from conftest import rel_l2
+from conftest import periodic_setup, rel_l2
 
 from beta1_b200 import case, mhd, solver
 
@@ -27,8 +27,7 @@ FIELDS = ["U_H", "B_xi", "PV_H", "U_plus", "Eface_eta", "E_zeta", "J_cell", "RHS
 
 @pytest.fixture(scope="module")
 def stepped(golden_periodic):
-    from test_gpu_parity import _init_state
-    spec, st = _init_state(golden_periodic["steps"])
+    spec, st = periodic_setup(golden_periodic["steps"])
     s = solver.Solver(spec)
     s.load_state(st)
     s.step(2)
