@@ -11,8 +11,15 @@ Workloads (--workload):
   periodic across the tiles) because the reference's halo exchange cannot
   run a cubed-sphere layout.  FP64.
 * c1: the plain FP64 64^3 periodic curvilinear block (ideal MHD).
+* c5: a parameter sweep of 48 independent runs in one batch context, each
+  one slab block of Nr x Nt x Nt cells (Nr in 32..128, Nt in 24..96),
+  inflow speed 4..12 and IMF clock angle 0..180 degrees drawn from
+  MT19937_64(5) (beta1_b200.case.sweep_cases; 14.7 M cells in all), ideal
+  MHD, each run with its own time step; mixed precision unless --precision
+  fp64.  Host geometry is built by a spawned process pool.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload c2|c1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload c2|c1|c5]
+                    [--precision fp64|mixed]
 
 Multi-GPU (torchrun): the path does not shard, so N ranks run N independent
 replicas; value = all cells updated by all ranks / max-over-ranks time.
@@ -121,7 +128,14 @@ def measured_peak():
 WORKLOADS = {
     "c2": dict(name="c2_slab6x96x48x48_implicit_resistive_fp64", ref_steps=4, ref_rss_gb=12.0),
     "c1": dict(name="c1_periodic_64cubed_fp64", ref_steps=40, ref_rss_gb=1.0),
+    "c5": dict(name="c5_sweep48_slab_runs_mixed", ref_steps=2, ref_rss_gb=4.0),
 }
+SWEEP_RUNS = 48
+
+
+def workload_name(name, mixed):
+    base = name.rsplit("_", 1)[0]
+    return base + ("_mixed" if mixed else "_fp64")
 
 
 def build_case(workload, n=64):
@@ -184,20 +198,77 @@ def cpu_reference(workload, n, steps, nproc):
         shutil.rmtree(d, ignore_errors=True)
 
 
+def cpu_reference_sweep(steps, nproc, nruns=SWEEP_RUNS):
+    """The reference's StepOnce loop on a sample of the sweep's runs: the
+    first `nproc` runs (bounded by host cores and memory), one
+    single-threaded process per run, concurrently; returns aggregate
+    cell-updates/s, the per-process figures and the process count."""
+    from beta1_b200 import case, rst
+    if not os.path.exists(REF_BIN):
+        return None
+    runs = case.sweep_cases(nruns)
+    nproc = max(1, min(nproc, len(runs), int(0.6 * mem_available_gb() / WORKLOADS["c5"]["ref_rss_gb"])))
+    d = tempfile.mkdtemp(prefix="b1sweep_")
+    try:
+        procs = []
+        for r in range(nproc):
+            spec = runs[r][0]
+            wd = os.path.join(d, "r%d" % r)
+            os.makedirs(wd)
+            case.write_case(wd, spec)
+            rst.write(os.path.join(wd, "init.rst"), case.inflow_state(spec, seed=SWEEP_SEED0 + r))
+            procs.append(subprocess.Popen([REF_BIN, "time", os.path.join(wd, "init.rst"), str(steps)], cwd=wd,
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
+        vals = []
+        for pr in procs:
+            out, _ = pr.communicate()
+            lines = [ln for ln in out.strip().splitlines() if ln.startswith("{")]
+            if pr.returncode != 0 or not lines:
+                return None
+            vals.append(json.loads(lines[-1]))
+        return sum(v["cell_updates_per_s"] for v in vals), vals, nproc
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+SWEEP_SEED0 = 5000
+
+
+def build_sweep(precision, nruns=SWEEP_RUNS):
+    """The c5 batch: host geometry of every run from a spawned process pool
+    (bounded by cores and memory), uploaded run by run as it arrives."""
+    import multiprocessing as mp
+    from beta1_b200 import case, solver
+    runs = case.sweep_cases(nruns)
+    nproc = max(1, min(len(runs), os.cpu_count() or 1, 16, int(mem_available_gb() / 8.0)))
+    with mp.get_context("spawn").Pool(nproc) as pool:
+        host = pool.imap(solver.host_setup_run, [(spec, "tiled") for spec, _ in runs])
+        bt = solver.Batch([(spec, "tiled") for spec, _ in runs], precision=precision, host=host)
+    bt.load_states([case.inflow_state(spec, seed=SWEEP_SEED0 + r) for r, (spec, _) in enumerate(runs)])
+    return bt, sum(bt.cells), runs
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     wl = WORKLOADS[args.workload]
     steps = min(args.steps, args.ref_steps or wl["ref_steps"])
-    res = cpu_reference(args.workload, args.n, steps, os.cpu_count() or 1)
+    if args.workload == "c5":
+        res = cpu_reference_sweep(steps, os.cpu_count() or 1)
+    else:
+        res = cpu_reference(args.workload, args.n, steps, os.cpu_count() or 1)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_lunar not built or failed"}))
         return 0
     agg, vals, nproc = res
-    cells = vals[0]["cells"]
-    sample = "%s: %d StepOnce per process, %d concurrent single-threaded processes (bounded by host cores and " \
-             "memory)" % (wl["name"], steps, nproc)
+    cells = vals[0]["cells"] if args.workload != "c5" else sum(v["cells"] for v in vals)
+    if args.workload == "c5":
+        sample = "%s: the first %d runs of the sweep, one single-threaded process each, %d StepOnce per " \
+                 "process, concurrently (bounded by host cores and memory)" % (wl["name"], nproc, steps)
+    else:
+        sample = "%s: %d StepOnce per process, %d concurrent single-threaded processes (bounded by host cores " \
+                 "and memory)" % (wl["name"], steps, nproc)
     line = {
         "impl": "reference", "metric": "cell-updates/s", "value": agg, "unit": "cell-updates/s",
         "n_gpus": args.gpus, "steps": steps, "warmup": 0,
@@ -223,13 +294,15 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=None, help="StepOnce per reference CPU sample")
     ap.add_argument("--e2e-iters", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
-                    help="fp64, or FP32 face fluxes with FP64 CT / state / residuals")
+    ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
+                    help="fp64, or FP32 face fluxes with FP64 CT / state / residuals (default: fp64, mixed for c5)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.steps is None:
-        args.steps = 200 if args.workload == "c2" else 4000
+        args.steps = {"c2": 200, "c1": 4000, "c5": 100}[args.workload]
+    if args.precision is None:
+        args.precision = "mixed" if args.workload == "c5" else "fp64"
 
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -248,17 +321,24 @@ def main():
     from beta1_b200 import mhd, solver
 
     wl = WORKLOADS[args.workload]
-    spec, st, topology, cells = build_case(args.workload, args.n)
     mixed = args.precision == "mixed"
-    s = solver.Solver(spec, topology=topology, precision=mhd.PREC_MIXED if mixed else mhd.PREC_FP64)
-    s.load_state(st)
+    prec = mhd.PREC_MIXED if mixed else mhd.PREC_FP64
+    if args.workload == "c5":
+        s, cells, sweep = build_sweep(prec)
+        spec = None
+        nblocks = len(sweep)
+    else:
+        spec, st, topology, cells = build_case(args.workload, args.n)
+        s = solver.Solver(spec, topology=topology, precision=prec)
+        s.load_state(st)
+        nblocks = len(spec.blocks)
     ctx = s.ctx
     stream = torch.cuda.ExternalStream(ctx.stream())
     ctx_bytes = sum(ctx.field_info(f, b)["ncomp"] * int(np.prod([h - l for l, h in zip(
         ctx.field_info(f, b)["lo"], ctx.field_info(f, b)["hi"])])) * 8 for f in ("U_H", "PV_H", "JDxi", "JDet",
                                                                                  "JDze", "Jcell_from_Jedge_w",
                                                                                  "Bcell_from_Bface_w")
-        for b in range(len(spec.blocks)))
+        for b in range(nblocks))
     res_stats = None
 
     # warm-up (also builds and instantiates the step graph)
@@ -287,7 +367,7 @@ def main():
         dist.barrier()
     ms = e0.elapsed_time(e1)
     launches = ctx.launches() - l0
-    if spec.params.get("is_Lunar_resistance", 0):
+    if spec is not None and spec.params.get("is_Lunar_resistance", 0):
         rs = ctx.resistive_stats()
         res_stats = {"krylov_its_last_step": rs["its"], "rnorm": rs["rnorm"], "bnorm": rs["bnorm"],
                      "reason": rs["reason"], "unknowns": int(len(s.resistive_dofs[0])), "rtol": float(spec.params["implicit_resistive_ksp_rtol"])}
@@ -320,7 +400,7 @@ def main():
     hin, hout = PinnedArray(nstate), PinnedArray(nstate)
     # the state after the timed steps, as the caller would hold it
     off = 0
-    for b in range(len(spec.blocks)):
+    for b in range(nblocks):
         for name in ("U_H", "B_xi", "B_eta", "B_zeta"):
             a = ctx.download(name, b).ravel()
             hin.a[off:off + a.size] = a
@@ -345,12 +425,20 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ref_steps = args.ref_steps or wl["ref_steps"]
-        res = cpu_reference(args.workload, args.n, ref_steps, 1)
-        if res is not None:
-            agg, vals, _ = res
-            cpu = {"value": agg, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
-                   "sample": "%s, %d StepOnce of the reference solver built from its own sources, one "
-                             "single-threaded process" % (wl["name"], ref_steps)}
+        if args.workload == "c5":
+            res = cpu_reference_sweep(ref_steps, 1)
+            if res is not None:
+                cpu = {"value": res[0], "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+                       "sample": "%s, run 0 of the sweep (%d cells), %d StepOnce of the reference solver built "
+                                 "from its own sources, one single-threaded process"
+                                 % (wl["name"], res[1][0]["cells"], ref_steps)}
+        else:
+            res = cpu_reference(args.workload, args.n, ref_steps, 1)
+            if res is not None:
+                agg, vals, _ = res
+                cpu = {"value": agg, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+                       "sample": "%s, %d StepOnce of the reference solver built from its own sources, one "
+                                 "single-threaded process" % (wl["name"], ref_steps)}
 
     if rank == 0:
         line = {
@@ -359,7 +447,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 fluxes + f64 CT/state" if mixed else "f64",
             "data": "synthetic (seeded 1e-3 noise on rho, v and div-free B; reference restart format)",
-            "config": {"workload": wl["name"].replace("_fp64", "_mixed") if mixed else wl["name"], "cells_per_gpu": cells, "blocks": len(spec.blocks),
+            "config": {"workload": workload_name(wl["name"], mixed), "cells_per_gpu": cells, "blocks": nblocks,
                        "integrator": "forward Euler StepOnce (reference parity mode)", "precision": args.precision,
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "no flush: per-step working set %.2f GB > 126 MB L2" % (ctx_bytes / 1e9)},

@@ -587,3 +587,73 @@ def slab_case(nr=96, nt=(48, 48), tiles=(3, 2), **over) -> CaseSpec:
     spec = CaseSpec(blocks, slab_interfaces(nr, nt, tiles), inflow_params(**over))
     spec.tiles = tiles
     return spec
+
+
+# --------------------------------------------------------------------------
+# Parameter sweep: independent single-block runs of uneven sizes
+# --------------------------------------------------------------------------
+
+class MT19937_64:
+    """The 64-bit Mersenne Twister (Matsumoto and Nishimura, 2000) with the
+    parameters of std::mt19937_64, for the sweep's draws."""
+
+    N, M = 312, 156
+    UPPER, LOWER = 0xFFFFFFFF80000000, 0x7FFFFFFF
+    MASK = (1 << 64) - 1
+
+    def __init__(self, seed: int):
+        self.mt = [0] * self.N
+        self.mt[0] = seed & self.MASK
+        for i in range(1, self.N):
+            self.mt[i] = (6364136223846793005 * (self.mt[i - 1] ^ (self.mt[i - 1] >> 62)) + i) & self.MASK
+        self.i = self.N
+
+    def _twist(self):
+        mt = self.mt
+        for i in range(self.N):
+            x = (mt[i] & self.UPPER) | (mt[(i + 1) % self.N] & self.LOWER)
+            xa = x >> 1
+            if x & 1:
+                xa ^= 0xB5026F5AA96619E9
+            mt[i] = mt[(i + self.M) % self.N] ^ xa
+        self.i = 0
+
+    def next(self) -> int:
+        if self.i >= self.N:
+            self._twist()
+        y = self.mt[self.i]
+        self.i += 1
+        y ^= (y >> 29) & 0x5555555555555555
+        y ^= (y << 17) & 0x71D67FFFEDA60000
+        y ^= (y << 37) & 0xFFF7EEE000000000
+        y ^= y >> 43
+        return y & self.MASK
+
+    def integer(self, lo: int, hi: int) -> int:
+        """lo + x mod (hi - lo + 1): uniform on {lo..hi} up to a bias below 1e-16"""
+        return lo + self.next() % (hi - lo + 1)
+
+    def real(self, lo: float, hi: float) -> float:
+        """lo + (hi - lo) u with u the top 53 bits of a draw over 2^53"""
+        return lo + (hi - lo) * ((self.next() >> 11) * 2.0 ** -53)
+
+
+def sweep_cases(nruns: int = 48, seed: int = 5, nr=(32, 128), nt=(24, 96), mach=(4.0, 12.0), angle=(0.0, 180.0)):
+    """Runs of a parameter sweep: per run (drawn in this order from
+    MT19937_64(seed)) radial cells Nr, transverse cells Nt (the block is
+    Nr x Nt x Nt), inflow speed `mach` (v = (-mach, 0, 0) in units of the
+    reference speed) and IMF clock angle theta in degrees, B = 0.5 (0,
+    cos theta, sin theta).  Each run is one slab block between a
+    Solid_Surface and a Farfield, periodic onto itself transversally.
+    Returns [(spec, dict of the drawn values)]."""
+    g = MT19937_64(seed)
+    out = []
+    for _ in range(nruns):
+        n_r = g.integer(*nr)
+        n_t = g.integer(*nt)
+        m = g.real(*mach)
+        th = g.real(*angle)
+        B = (0.0, 0.5 * math.cos(math.radians(th)), 0.5 * math.sin(math.radians(th)))
+        spec = slab_case(n_r, (n_t, n_t), (1, 1), mach_u=m, B=B)
+        out.append((spec, dict(nr=n_r, nt=n_t, mach=m, angle=th)))
+    return out

@@ -224,17 +224,37 @@ class Solver:
         return self.ctx.download(name, block)
 
 
-def host_setup(spec: case_mod.CaseSpec):
-    """Host-side geometry of a case: per block the ghost node mesh and the
-    geometry fields (a pure function of the grid, safe to run in worker
-    processes)."""
+def host_setup(spec: case_mod.CaseSpec, topology: Optional[str] = None):
+    """Host-side set-up of a case: per block the ghost node mesh and the
+    geometry fields, and (given the topology) the run's sync tables compiled
+    on its own blocks 0, 1, ...  A pure function of the case, safe to run in
+    worker processes.  Returns (nodes, geom, tables or None)."""
     ngg = int(spec.params["ngg"])
     nodes, geom = [], []
     for b in spec.blocks:
         X = geometry.ghost_mesh(b.x, b.y, b.z, ngg)
         nodes.append(X)
         geom.append(geometry.build(X, b.ncell, ngg))
-    return nodes, geom
+    return nodes, geom, (run_tables(spec, topology, nodes) if topology else None)
+
+
+def host_setup_run(run):
+    """host_setup of a (spec, topology) pair (process-pool entry)"""
+    return host_setup(*run)
+
+
+def run_tables(spec: case_mod.CaseSpec, topology: str, nodes):
+    """Sync tables of one non-resistive run on its own blocks 0, 1, ..."""
+    lay = mhd.HostLayout([b.ncell for b in spec.blocks])
+    if topology == "periodic":
+        return syncmap.periodic_maps(lay, spec.blocks[0].ncell)
+    if topology != "tiled":
+        raise ValueError(f"unknown topology {topology}")
+    q, B = physics.farfield_state(spec.params)
+    u = [q[1] / q[0], q[2] / q[0], q[3] / q[0]]
+    E_inf = [B[1] * u[2] - B[2] * u[1], B[2] * u[0] - B[0] * u[2], B[0] * u[1] - B[1] * u[0]]
+    return syncmap.compile_tiled(lay, syncmap.TiledLayout(spec.blocks[0].ncell, spec.tiles), False,
+                                 dict(qinf=q, B_imf=B, E_inf=E_inf), nodes)
 
 
 def _farfield_prim(params):
@@ -250,8 +270,9 @@ class Batch:
     step, all advanced by one step graph.  runs: (case spec, topology) per
     run, topology "periodic" (one block) or "tiled"; the runs must agree on
     the constants of the step (gamma, CFL, the J x B and state scales) and
-    may not use the resistive or Hall solves.  host: optional host_setup()
-    result per run (e.g. computed by a process pool)."""
+    may not use the resistive or Hall solves.  host: optional iterable of
+    the host_setup(spec, topology) results of the runs in order (e.g. from a
+    process pool); each is uploaded and released as it arrives."""
 
     CONSTS = ("gamma", "cfl", "inver_MA2", "momentum_hall_coeff", "state_coeff", "M_H", "M_ref", "ne_hall_floor")
 
@@ -274,10 +295,10 @@ class Batch:
             run_of += [r] * len(spec.blocks)
         self.ctx = mhd.Context(ncells, make_params(self.runs[0][0].params, precision), runs=run_of)
         if host is None:
-            host = [host_setup(spec) for spec, _ in self.runs]
-        tables = {}
+            host = (host_setup(spec, topo) for spec, topo in self.runs)
+        per_run = []
         zero_rows = []
-        for r, ((spec, topo), (nodes, geom)) in enumerate(zip(self.runs, host)):
+        for r, ((spec, topo), (nodes, geom, maps)) in enumerate(zip(self.runs, host)):
             off = self.offset[r]
             q, B = physics.farfield_state(spec.params)
             for ib, g in enumerate(geom):
@@ -286,18 +307,10 @@ class Batch:
                 if any(v != 0.0 for v in B):
                     for fname, jd in (("Badd_xi", "JDxi"), ("Badd_eta", "JDet"), ("Badd_zeta", "JDze")):
                         self.ctx.upload(fname, off + ib, badd_faces(g[jd][2], B))
-            lay = mhd.HostLayout([b.ncell for b in spec.blocks])
-            if topo == "periodic":
-                maps = syncmap.periodic_maps(lay, spec.blocks[0].ncell)
-            elif topo == "tiled":
-                u = [q[1] / q[0], q[2] / q[0], q[3] / q[0]]
-                E_inf = [B[1] * u[2] - B[2] * u[1], B[2] * u[0] - B[0] * u[2], B[0] * u[1] - B[1] * u[0]]
-                maps = syncmap.compile_tiled(lay, syncmap.TiledLayout(spec.blocks[0].ncell, spec.tiles), False,
-                                             dict(qinf=q, B_imf=B, E_inf=E_inf), nodes)
-            else:
-                raise ValueError(f"unknown topology {topo}")
-            for group, m in syncmap.shift_blocks(maps, off).items():
-                tables.setdefault(group, []).append(m)
+            if maps is None:
+                maps = run_tables(spec, topo, nodes)
+            per_run.append((maps, off))
+            del nodes, geom
             for ib, b in enumerate(spec.blocks):
                 n = b.ncell
                 patches = [("Solid_Surface", -1, (0, 0, 0), (1, n[1] + 1, n[2] + 1))] if topo == "tiled" else []
@@ -305,18 +318,13 @@ class Batch:
             if precision == mhd.PREC_MIXED:
                 self.ctx.set_flux_reference(_farfield_prim(spec.params), run=r)
         self.sync_sizes = {}
-        for group, ms in tables.items():
-            dst = np.concatenate([m["dst"] for m in ms])
-            src = np.concatenate([m["src"] for m in ms])
-            cdst = np.concatenate([m["cdst"] for m in ms])
-            cval = np.concatenate([m["cval"] for m in ms])
-            self.ctx.set_sync_map(group, dst, src)
-            if cdst.size:
-                self.ctx.set_sync_consts(group, cdst, cval)
-            walls = [w for m in ms for w in m["walls"]]
-            for (b, d) in walls:
+        for group, m in syncmap.merge_runs(per_run).items():
+            self.ctx.set_sync_map(group, m["dst"], m["src"])
+            if m["cdst"].size:
+                self.ctx.set_sync_consts(group, m["cdst"], m["cval"])
+            for (b, d) in m["walls"]:
                 self.ctx.set_sync_wall(group, b, d)
-            self.sync_sizes[group] = (int(dst.size), int(cdst.size), len(walls))
+            self.sync_sizes[group] = (int(m["dst"].size), int(m["cdst"].size), len(m["walls"]))
         self.ctx.sync("Badd")
         self.ctx.set_hall(c0["hall_coef"], zero_rows)
 

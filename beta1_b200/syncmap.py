@@ -96,6 +96,25 @@ def install_periodic(ctx, ncell) -> Dict[str, int]:
     return sizes
 
 
+def merge_runs(per_run) -> Dict[str, dict]:
+    """One table per group for a batch of runs: per_run holds (tables of a
+    run compiled on its own blocks 0, 1, ..., first block of the run in the
+    batch); the runs' tables are shifted to their blocks and concatenated
+    (runs share no halo)."""
+    out: Dict[str, dict] = {}
+    for maps, off in per_run:
+        for group, m in shift_blocks(maps, off).items():
+            o = out.setdefault(group, dict(dst=[], src=[], cdst=[], cval=[], walls=[]))
+            for k in ("dst", "src", "cdst", "cval"):
+                o[k].append(m[k])
+            o["walls"] += m["walls"]
+    for o in out.values():
+        for k in ("dst", "src", "cdst"):
+            o[k] = np.concatenate(o[k]).astype(np.int64)
+        o["cval"] = np.concatenate(o["cval"]).astype(np.float64)
+    return out
+
+
 def shift_blocks(maps: Dict[str, dict], off: int) -> Dict[str, dict]:
     """The tables of a layout whose blocks become blocks off, off + 1, ... of
     a larger context (point ids carry the block in bits 40-55)."""
