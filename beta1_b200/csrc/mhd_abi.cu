@@ -89,7 +89,7 @@ const char *const kKernelNames[] = {
     "k_zero",         "k_residual",    "k_ucontra",      "k_face_normals", "k_divb",          "k_eres_explicit",
     "k_bcell_jedge",  "k_fluid_ucontra", "k_wall_u_all",   "k_hall_cell",    "k_hall_edge",
     "k_pack_vec",     "k_hall_residual", "k_axpy_to",      "k_fd_quotient",  "k_negate",
-    "k_geom32",       "k_fluid_mixed"};
+    "k_geom32",       "k_fluid_mixed",  "k_gmres_resist"};
 constexpr int kNumKernelNames = int(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
 
 } // namespace
@@ -165,6 +165,11 @@ struct mhd_ctx
         long long its_eager = 0, cycles_eager = 0;
         bool graph_loops = true;                 // conditional graph nodes usable
         std::vector<uint64_t> seed;              // unknown and alias offsets (Eres), for the region
+        // the persistent solve (one cooperative kernel per solve)
+        int64_t *alias_of = nullptr;             // unknown index of each alias's owner
+        double *ppartial = nullptr;              // per-CTA partial dot products, double-buffered
+        unsigned *bar = nullptr;                 // grid barrier: arrival count, generation
+        int pgrid = 0;                           // CTAs of the persistent kernel (0: unavailable)
     } res;
     // implicit Hall solve (ImplicitHallSolver::SolveOneStep): Newton on
     // F(X) = X - Ehall(B* - theta dt curl X) over the inner Hall edges of
@@ -808,12 +813,69 @@ int gmres_graph(mhd_ctx *ctx)
 // composed sync is idempotent) and the closing Sync("Bface") of the step
 // repeats the one after.  J is needed at the unknowns only here (the
 // derived-field pass recomputes it everywhere).
+DevCopy dev_copy(const CopyList &l)
+{
+    return DevCopy{l.cdst, l.cval, l.nconst, l.dst, l.src, l.tmp, l.n};
+}
+
+// the whole solve as one cooperative kernel (k_gmres_resist)
+int launch_gmres_persistent(mhd_ctx *ctx)
+{
+    auto &R = ctx->res;
+    ResistSolve a{};
+    a.bvs = ctx->dbv;
+    a.pool = ctx->pool;
+    a.nblocks = ctx->nblocks;
+    a.e = R.e;
+    a.dj = R.dj;
+    a.j = R.j;
+    a.eta = R.eta;
+    a.n = R.n;
+    a.alias = R.alias_e;
+    a.alias_of = R.alias_of;
+    a.sign = R.sign;
+    a.nalias = R.nalias;
+    a.eres1form = dev_copy(R.eres1form);
+    a.db = dev_copy(R.db);
+    a.rng = R.rng;
+    a.nreg = R.nreg_max;
+    a.dtp = ctx->dt;
+    a.V = R.V;
+    a.w = R.w;
+    a.x = R.x;
+    a.b = R.b;
+    a.r = R.r;
+    a.partial = R.ppartial;
+    a.st = R.st;
+    a.m = R.restart;
+    a.maxit = R.maxit;
+    a.rtol = R.rtol;
+    a.atol = R.atol;
+    a.bar = R.bar;
+    a.err = ctx->err;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(R.pgrid));
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    prof_begin(ctx, "k_gmres_resist");
+    CK(ctx, cudaLaunchKernelEx(&cfg, k_gmres_resist, a));
+    return launched(ctx);
+}
+
 int launch_resistive(mhd_ctx *ctx)
 {
     auto &R = ctx->res;
     RUN(run_sync(ctx, "Bface"));
     RUN(launch_jedge_rng(ctx, F_Bxi, F_Jxi));
-    if (R.n > 0)
+    if (R.n > 0 && R.pgrid > 0)
+        RUN(launch_gmres_persistent(ctx));
+    else if (R.n > 0)
     {
         LAUNCHN(k_resist_rhs, R.n, ctx->pool, R.j, R.eta, R.b, R.n);
         if (ctx->capturing && R.graph_loops)
@@ -1149,6 +1211,14 @@ int check_err(mhd_ctx *ctx)
         const int z = 0;
         cudaMemcpy(ctx->err, &z, sizeof(int), cudaMemcpyHostToDevice);
         return fail(ctx, MHD_EDT, "dt too small or NaN: dt=%.3e", d);
+    }
+    if (e == MHD_EKRYLOV)
+    {
+        const int z = 0;
+        cudaMemcpy(ctx->err, &z, sizeof(int), cudaMemcpyHostToDevice);
+        if (ctx->res.bar)
+            cudaMemset(ctx->res.bar, 0, 4 * sizeof(unsigned));
+        return fail(ctx, MHD_EKRYLOV, "persistent Krylov solve: a grid barrier wait gave up");
     }
     return MHD_OK;
 }
@@ -1694,7 +1764,8 @@ static void free_resistive(mhd_ctx *ctx)
     auto &R = ctx->res;
     for (void *p : {(void *)R.e, (void *)R.dj, (void *)R.j, (void *)R.eta, (void *)R.alias_e, (void *)R.owner_e,
                     (void *)R.sign, (void *)R.rng, (void *)R.V, (void *)R.w, (void *)R.x,
-                    (void *)R.b, (void *)R.r, (void *)R.partial, (void *)R.dots, (void *)R.st})
+                    (void *)R.b, (void *)R.r, (void *)R.partial, (void *)R.dots, (void *)R.st,
+                    (void *)R.alias_of, (void *)R.ppartial, (void *)R.bar})
         cudaFree(p);
     free_list(R.eres1form);
     free_list(R.db);
@@ -2177,12 +2248,17 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
     std::sort(sorted_e.begin(), sorted_e.end());
     std::vector<uint64_t> fa, fo;
     std::vector<double> fs;
+    std::vector<int64_t> fidx; // unknown index of the owner
+    std::map<uint64_t, int64_t> index_of;
+    for (int64_t t = 0; t < n; ++t)
+        index_of[he[size_t(t)]] = t;
     for (int64_t t = 0; t < nalias; ++t)
         if (std::binary_search(sorted_e.begin(), sorted_e.end(), oe[size_t(t)]))
         {
             fa.push_back(ae[size_t(t)]);
             fo.push_back(oe[size_t(t)]);
             fs.push_back(sign[t]);
+            fidx.push_back(index_of[oe[size_t(t)]]);
         }
     RUN(upload_vec(ctx, he, &R.e));
     RUN(upload_vec(ctx, hdj, &R.dj));
@@ -2190,6 +2266,7 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
     RUN(upload_vec(ctx, fa, &R.alias_e));
     RUN(upload_vec(ctx, fo, &R.owner_e));
     RUN(upload_vec(ctx, fs, &R.sign));
+    RUN(upload_vec(ctx, fidx, &R.alias_of));
     std::vector<double> heta(eta, eta + n);
     RUN(upload_vec(ctx, heta, &R.eta));
     R.n = n;
@@ -2220,6 +2297,25 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
     CK(ctx, cudaMalloc(&R.st, sizeof(GmresState)));
     CK(ctx, cudaMemset(R.x, 0, nn * 8));
     CK(ctx, cudaMemset(R.st, 0, sizeof(GmresState)));
+    // the persistent solve: as many CTAs as the work needs, at most two per
+    // SM (more gave no further gain) and no more than can be resident
+    // together (cooperative launch)
+    {
+        int dev = 0, sms = 0, per_sm = 0, coop = 0;
+        CK(ctx, cudaGetDevice(&dev));
+        CK(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        CK(ctx, cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        CK(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gmres_resist, 256, 0));
+        const int64_t work = std::max<int64_t>(n, int64_t(ctx->nblocks) * R.nreg_max);
+        const int64_t want = std::max<int64_t>(1, (work + 255) / 256);
+        R.pgrid = (coop && per_sm > 0) ? int(std::min<int64_t>(want, int64_t(sms) * std::min(per_sm, 2))) : 0;
+        if (R.pgrid > 0)
+        {
+            CK(ctx, cudaMalloc(&R.ppartial, size_t(2 * 32) * size_t(R.pgrid) * 8));
+            CK(ctx, cudaMalloc(&R.bar, 4 * sizeof(unsigned)));
+            CK(ctx, cudaMemset(R.bar, 0, 4 * sizeof(unsigned)));
+        }
+    }
     R.its_eager = R.cycles_eager = 0;
     R.k_cycle = R.k_inner = 0;
     for (auto &sp : ctx->spare)

@@ -83,6 +83,44 @@ struct GmresState
     long long total_cycles; // cumulative over all solves
     unsigned int dot_done[32]; // CTAs finished per dot product (the last one sums the partials)
 };
+// The implicit resistive solve as one persistent (cooperative) kernel:
+// GMRES(m) with the operator, the orthogonalisation and the control flow
+// all on the device, CTAs meeting at grid barriers between phases.
+struct DevCopy // fixed values then copies of a point list (apply_list)
+{
+    const uint64_t *cdst;
+    const double *cval;
+    int64_t nconst;
+    const uint64_t *dst, *src;
+    double *tmp; // staging when a source is also a destination
+    int64_t n;
+};
+struct ResistSolve
+{
+    const BlockView *bvs;
+    double *pool;
+    int nblocks;
+    const uint64_t *e, *dj, *j; // unknowns' offsets in Eres, dJ and J
+    const double *eta;
+    int64_t n;
+    const uint64_t *alias; // aliases of unknown owners ...
+    const int64_t *alias_of; // ... and the owner's unknown index
+    const double *sign;
+    int64_t nalias;
+    DevCopy eres1form, db;
+    const int *rng; // per block region box
+    int64_t nreg;   // points of the largest region box
+    const double *dtp;
+    double *V, *w, *x, *b, *r;
+    double *partial; // 2 x 32 x gridDim.x
+    GmresState *st;
+    int m, maxit;
+    double rtol, atol;
+    unsigned *bar; // arrival count, generation
+    int *err;      // set to MHD_EKRYLOV when a barrier wait gives up
+};
+__global__ void k_gmres_resist(ResistSolve a);
+
 // dot products out[c] = V_c . w for c < nvec (nvec = *jdev + 1 when jdev is
 // given); V == nullptr computes w . w.  Each CTA stores its partial sum; the
 // last CTA of each product adds the partials in a fixed order.

@@ -455,17 +455,11 @@ __global__ void k_eedge(const BlockView *__restrict__ bvs)
 // with multiplier `mult`, written to RHS_B, optionally followed by the face
 // part of ApplyUpdate_Euler_ (LunarSolver_Advance.cpp:95-121): B += dt*RHS_B.
 // ---------------------------------------------------------------------------
-__global__ void k_curl_e2f(const BlockView *__restrict__ bvs, int fE0, int fR0, int fB0, double mult,
-                           const double *__restrict__ dtp, double dtdiv, int mult_is_neg_dt, const int *__restrict__ rng)
+// the three inner faces at staggered point (i, j, k): RHS = mult * curl E,
+// optionally B += dtB * RHS
+__device__ __forceinline__ void curl_point(const BlockView &b, int fE0, int fR0, int fB0, double mult, double dtB,
+                                           int i, int j, int k)
 {
-    int64_t t;
-    const int bi = cta_block(bvs, KIND_STAG, t);
-    const BlockView &b = bvs[bi];
-    if (mult_is_neg_dt)
-        mult = -dtp[b.run];
-    int i, j, k;
-    if (!stagger_point(b, rng, bi, t, i, j, k))
-        return;
     const double *Ex = b.f[fE0], *Ee = b.f[fE0 + 1], *Ez = b.f[fE0 + 2];
     const int64_t p = pidx(b, i, j, k);
 #pragma unroll
@@ -484,11 +478,22 @@ __global__ void k_curl_e2f(const BlockView *__restrict__ bvs, int fE0, int fR0, 
         if (fR0 >= 0)
             b.f[fR0 + fa][p] = rhs;
         if (fB0 >= 0)
-        {
-            const double dt = dtp[b.run] / dtdiv;
-            b.f[fB0 + fa][p] += dt * rhs;
-        }
+            b.f[fB0 + fa][p] += dtB * rhs;
     }
+}
+
+__global__ void k_curl_e2f(const BlockView *__restrict__ bvs, int fE0, int fR0, int fB0, double mult,
+                           const double *__restrict__ dtp, double dtdiv, int mult_is_neg_dt, const int *__restrict__ rng)
+{
+    int64_t t;
+    const int bi = cta_block(bvs, KIND_STAG, t);
+    const BlockView &b = bvs[bi];
+    if (mult_is_neg_dt)
+        mult = -dtp[b.run];
+    int i, j, k;
+    if (!stagger_point(b, rng, bi, t, i, j, k))
+        return;
+    curl_point(b, fE0, fR0, fB0, mult, fB0 >= 0 ? dtp[b.run] / dtdiv : 0.0, i, j, k);
 }
 
 // calc_divB on inner cells (Z4_Lunar/src/physics/LunarSolver_Tools.cpp:685-775;
@@ -1202,6 +1207,370 @@ __global__ void k_soa_to_aos(const BlockView *__restrict__ bvs, int blk, int fid
     const int j = lo1 + int(r % n1);
     const int i = lo0 + int(r / n1);
     aos[t] = b.f[fid][m * b.vol + pidx(b, i, j, k)];
+}
+
+// ---------------------------------------------------------------------------
+// The implicit resistive solve in one persistent kernel
+// (SolveImplicitResistiveDiffusion_, Z4_Lunar/src/implicit/Lunar_ImplicitResistive.cpp:430-491,
+// with the operator MatMultImplicitResistive_, :369-427)
+//
+// Launched cooperatively (every CTA resident), so CTAs can wait for one
+// another at grid barriers.  Every barrier wait is bounded: a CTA that gives
+// up sets the error word and leaves, and the others give up at their next
+// barrier.  Dot products: each CTA writes its partial sums, and after the
+// barrier every CTA adds all partials in the same fixed order, so all CTAs
+// hold bit-identical results and take the same control decisions without a
+// second barrier.  The GMRES scalars (Hessenberg matrix, rotations, counters)
+// live in each CTA's shared memory; CTA 0 writes them back at the end.
+// ---------------------------------------------------------------------------
+
+constexpr long long kBarrierSpins = 1ll << 22; // about a second of polling
+
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err)
+{
+    __shared__ int ok; // one decision for the whole CTA
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        volatile unsigned *gen = bar + 1;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) + 1u == gridDim.x)
+        {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        }
+        else
+        {
+            long long spins = 0;
+            while (*gen == g)
+            {
+                if (++spins > kBarrierSpins)
+                {
+                    atomicExch(err, MHD_EKRYLOV);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        ok = *(volatile int *)err != MHD_EKRYLOV;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+struct GmresScalars
+{
+    double H[31 * 31], cs[31], sn[31], g[32], hcol[32], y[31], d[32];
+    double beta, resid, bnorm, ttol;
+    int j, its, reason, breakdown, inner, outer, cycles;
+};
+
+// out[c] = V_c . w for c < nv, or out[0] = w . w (V null); every CTA ends
+// with the same values in out (shared memory)
+__device__ bool grid_dots(const ResistSolve &a, const double *V, int nv, const double *w, double *out, int &pbuf)
+{
+    __shared__ double wred[8][8];
+    const int G = gridDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double *part = a.partial + int64_t(pbuf) * 32 * G;
+    pbuf ^= 1;
+    for (int c0 = 0; c0 < nv; c0 += 8)
+    {
+        double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int64_t t = int64_t(blockIdx.x) * blockDim.x + tid; t < a.n; t += int64_t(G) * blockDim.x)
+        {
+            const double wt = w[t];
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (c0 + q < nv)
+                    acc[q] += (V ? V[int64_t(c0 + q) * a.n + t] : wt) * wt;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            for (int off = 16; off > 0; off >>= 1)
+                acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+        if (lane == 0)
+            for (int q = 0; q < 8; ++q)
+                wred[warp][q] = acc[q];
+        __syncthreads();
+        if (tid < 8 && c0 + tid < nv)
+        {
+            double sum = 0.0;
+            for (int wp = 0; wp < int(blockDim.x >> 5); ++wp)
+                sum += wred[wp][tid];
+            part[int64_t(c0 + tid) * G + blockIdx.x] = sum;
+        }
+        __syncthreads();
+    }
+    if (!grid_barrier(a.bar, a.err))
+        return false;
+    for (int c = warp; c < nv; c += int(blockDim.x >> 5))
+    {
+        double sum = 0.0;
+        for (int g = lane; g < G; g += 32)
+            sum += __ldcg(&part[int64_t(c) * G + g]);
+        for (int off = 16; off > 0; off >>= 1)
+            sum += __shfl_xor_sync(0xffffffffu, sum, off);
+        if (lane == 0)
+            out[c] = sum;
+    }
+    __syncthreads();
+    return true;
+}
+
+// fixed values then copies of a point list
+__device__ bool grid_apply(const ResistSolve &a, const DevCopy &l)
+{
+    const int64_t t0 = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, ts = int64_t(gridDim.x) * blockDim.x;
+    if (l.nconst > 0)
+    {
+        for (int64_t t = t0; t < l.nconst; t += ts)
+            a.pool[l.cdst[t]] = l.cval[t];
+        if (!grid_barrier(a.bar, a.err))
+            return false;
+    }
+    if (l.n == 0)
+        return true;
+    if (l.tmp)
+    {
+        for (int64_t t = t0; t < l.n; t += ts)
+            l.tmp[t] = a.pool[l.src[t]];
+        if (!grid_barrier(a.bar, a.err))
+            return false;
+        for (int64_t t = t0; t < l.n; t += ts)
+            a.pool[l.dst[t]] = __ldcg(&l.tmp[t]);
+    }
+    else
+        for (int64_t t = t0; t < l.n; t += ts)
+            a.pool[l.dst[t]] = a.pool[l.src[t]];
+    return grid_barrier(a.bar, a.err);
+}
+
+// y = A x (MatMultImplicitResistive_): Eres at the unknowns and their aliases
+// from x, Sync("Eres1form"), dB = -dt curl Eres on the region, Sync("dB"),
+// dJ = alpha curlAdj(beta dB) on the region, y = Eres - eta dJ
+__device__ bool grid_matvec(const ResistSolve &a, const double *x, double *y)
+{
+    const int64_t t0 = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, ts = int64_t(gridDim.x) * blockDim.x;
+    if (!grid_barrier(a.bar, a.err)) // x complete
+        return false;
+    for (int64_t t = t0; t < a.n; t += ts)
+        a.pool[a.e[t]] = x[t];
+    for (int64_t q = t0; q < a.nalias; q += ts)
+        a.pool[a.alias[q]] = a.sign[q] * x[a.alias_of[q]];
+    if (!grid_barrier(a.bar, a.err))
+        return false;
+    if (!grid_apply(a, a.eres1form))
+        return false;
+    const double mdt = -a.dtp[0];
+    const int64_t np = int64_t(a.nblocks) * a.nreg;
+    for (int64_t q = t0; q < np; q += ts)
+    {
+        const int blk = int(q / a.nreg);
+        const BlockView &b = a.bvs[blk];
+        int i, j, k;
+        if (stagger_point(b, a.rng, blk, q % a.nreg, i, j, k))
+            curl_point(b, F_Eresxi, F_dBxi, -1, mdt, 0.0, i, j, k);
+    }
+    if (!grid_barrier(a.bar, a.err))
+        return false;
+    if (!grid_apply(a, a.db))
+        return false;
+    for (int64_t q = t0; q < np; q += ts)
+    {
+        const int blk = int(q / a.nreg);
+        const BlockView &b = a.bvs[blk];
+        int i, j, k;
+        if (stagger_point(b, a.rng, blk, q % a.nreg, i, j, k))
+#pragma unroll
+            for (int ea = 0; ea < 3; ++ea)
+                if (inner_of(b, 1, ea, i, j, k))
+                    jedge_one(b, ea, i, j, k, F_dBxi, F_dJxi, 1.0);
+    }
+    if (!grid_barrier(a.bar, a.err))
+        return false;
+    for (int64_t t = t0; t < a.n; t += ts)
+        y[t] = a.pool[a.e[t]] - a.eta[t] * a.pool[a.dj[t]];
+    return true;
+}
+
+__global__ void __launch_bounds__(256) k_gmres_resist(ResistSolve a)
+{
+    __shared__ GmresScalars S;
+    __shared__ double dv[32];
+    const int tid = threadIdx.x;
+    const int64_t t0 = int64_t(blockIdx.x) * blockDim.x + tid, ts = int64_t(gridDim.x) * blockDim.x;
+    const int64_t n = a.n;
+    int pbuf = 0;
+    // right-hand side b = eta J at the unknowns (PackImplicitJedgeToVec_), x = 0
+    for (int64_t t = t0; t < n; t += ts)
+    {
+        a.b[t] = 0.0 + a.eta[t] * a.pool[a.j[t]];
+        a.x[t] = 0.0;
+    }
+    if (!grid_dots(a, nullptr, 1, a.b, dv, pbuf))
+        return;
+    if (tid == 0)
+    {
+        S.bnorm = sqrt(dv[0]);
+        S.ttol = fmax(a.rtol * S.bnorm, a.atol);
+        S.its = 0;
+        S.reason = 0;
+        S.cycles = 0;
+        S.resid = S.bnorm;
+    }
+    __syncthreads();
+    for (;;)
+    {
+        // cycle start: r = b - A x, beta = ||r||
+        if (!grid_matvec(a, a.x, a.w))
+            return;
+        for (int64_t t = t0; t < n; t += ts)
+            a.r[t] = a.b[t] - a.w[t];
+        if (!grid_dots(a, nullptr, 1, a.r, dv, pbuf))
+            return;
+        if (tid == 0)
+        {
+            S.beta = sqrt(dv[0]);
+            for (int q = 0; q < 32; ++q)
+                S.g[q] = 0.0;
+            S.g[0] = S.beta;
+            S.resid = S.beta;
+            S.breakdown = 0;
+            S.j = 0;
+            S.inner = 1;
+            if (S.beta <= S.ttol)
+            {
+                S.reason = (S.beta <= a.atol) ? 3 : 2;
+                S.inner = 0;
+            }
+            else if (S.its >= a.maxit)
+            {
+                S.reason = -3;
+                S.inner = 0;
+            }
+        }
+        __syncthreads();
+        if (S.inner)
+            for (int64_t t = t0; t < n; t += ts)
+                a.V[t] = a.r[t] / S.beta;
+        while (S.inner)
+        {
+            const int j = S.j;
+            double *Vj = a.V + int64_t(j) * n;
+            if (!grid_matvec(a, Vj, a.w))
+                return;
+            // classical Gram-Schmidt, twice
+            if (!grid_dots(a, a.V, j + 1, a.w, S.hcol, pbuf))
+                return;
+            for (int64_t t = t0; t < n; t += ts)
+            {
+                double s = a.w[t];
+                for (int c = 0; c <= j; ++c)
+                    s -= S.hcol[c] * a.V[int64_t(c) * n + t];
+                a.w[t] = s;
+            }
+            if (!grid_dots(a, a.V, j + 1, a.w, S.d, pbuf))
+                return;
+            for (int64_t t = t0; t < n; t += ts)
+            {
+                double s = a.w[t];
+                for (int c = 0; c <= j; ++c)
+                    s -= S.d[c] * a.V[int64_t(c) * n + t];
+                a.w[t] = s;
+            }
+            if (tid <= j)
+                S.hcol[tid] += S.d[tid];
+            __syncthreads();
+            if (!grid_dots(a, nullptr, 1, a.w, dv, pbuf))
+                return;
+            if (tid == 0)
+            {
+                // new column: rotations, residual estimate
+                S.hcol[j + 1] = sqrt(dv[0]);
+                for (int i = 0; i <= j + 1; ++i)
+                    S.H[i * 31 + j] = S.hcol[i];
+                for (int i = 0; i < j; ++i)
+                {
+                    const double x0 = S.H[i * 31 + j], x1 = S.H[(i + 1) * 31 + j];
+                    S.H[i * 31 + j] = S.cs[i] * x0 + S.sn[i] * x1;
+                    S.H[(i + 1) * 31 + j] = -S.sn[i] * x0 + S.cs[i] * x1;
+                }
+                const double x0 = S.H[j * 31 + j], x1 = S.H[(j + 1) * 31 + j];
+                const double den = sqrt(x0 * x0 + x1 * x1);
+                S.cs[j] = den > 0.0 ? x0 / den : 1.0;
+                S.sn[j] = den > 0.0 ? x1 / den : 0.0;
+                S.H[j * 31 + j] = den;
+                S.H[(j + 1) * 31 + j] = 0.0;
+                S.g[j + 1] = -S.sn[j] * S.g[j];
+                S.g[j] = S.cs[j] * S.g[j];
+                S.resid = fabs(S.g[j + 1]);
+                S.breakdown = (S.hcol[j + 1] == 0.0) ? 1 : 0;
+            }
+            __syncthreads();
+            if (!S.breakdown)
+                for (int64_t t = t0; t < n; t += ts)
+                    a.V[int64_t(j + 1) * n + t] = a.w[t] / S.hcol[j + 1];
+            __syncthreads();
+            if (tid == 0)
+            {
+                S.its += 1;
+                S.j += 1;
+                S.inner = !(S.resid <= S.ttol || S.breakdown || S.j >= a.m || S.its >= a.maxit);
+            }
+            __syncthreads();
+        }
+        // cycle end: H y = g, x += V y
+        if (tid == 0)
+        {
+            const int m = S.j;
+            for (int i = m - 1; i >= 0; --i)
+            {
+                double s = S.g[i];
+                for (int q = i + 1; q < m; ++q)
+                    s -= S.H[i * 31 + q] * S.y[q];
+                S.y[i] = s / S.H[i * 31 + i];
+            }
+            S.cycles += 1;
+        }
+        __syncthreads();
+        for (int64_t t = t0; t < n; t += ts)
+        {
+            double s = a.x[t];
+            for (int c = 0; c < S.j; ++c)
+                s += S.y[c] * a.V[int64_t(c) * n + t];
+            a.x[t] = s;
+        }
+        if (tid == 0)
+        {
+            S.outer = 0;
+            if (S.reason != 0)
+                S.outer = 0;
+            else if (S.resid <= S.ttol || S.breakdown)
+                S.reason = (S.resid <= a.atol) ? 3 : 2;
+            else if (S.its >= a.maxit)
+                S.reason = -3;
+            else
+                S.outer = 1;
+        }
+        __syncthreads();
+        if (!S.outer)
+            break;
+    }
+    if (blockIdx.x == 0 && tid == 0)
+    {
+        GmresState *st = a.st;
+        st->its = S.its;
+        st->resid = S.resid;
+        st->bnorm = S.bnorm;
+        st->ttol = S.ttol;
+        st->reason = S.reason;
+        st->j = S.j;
+        st->total_its += S.its;
+        st->total_cycles += S.cycles;
+    }
 }
 
 } // namespace mhd
