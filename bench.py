@@ -77,9 +77,12 @@ ALGO_BYTES_PER_CELL = {
 # the mixed form's PV pass also writes the 7 FP32 face states
 ALGO_BYTES_MIXED_EXTRA = {"k_pv_uplus_dt": 7 * 4}
 
-# DRAM traffic per launch from one ncu capture of the 64^3 case
-# (profiles/k_fluid_rhs_periodic64.md); None where not captured.
-NCU_TRAFFIC_BYTES = {}
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of
+# the dominant kernel, from one ncu capture of the C2 workload at half the
+# cells per direction (165,888 cells: 114.26 MB read + 10.32 MB written),
+# scaled by the cell count to a full C2 launch (1,327,104 cells; the kernel's
+# traffic grows with the cells it covers); profiles/k_pv_uplus_dt_c2small_fp64.md
+NCU_TRAFFIC_BYTES = {("k_pv_uplus_dt", "c2_slab6x96x48x48_implicit_resistive_fp64"): (114.25536e6 + 10.321408e6) * 8.0}
 
 
 def sample_clocks(stop: threading.Event, out: list, gpu_id: str):
@@ -138,14 +141,15 @@ def workload_name(name, mixed):
     return base + ("_mixed" if mixed else "_fp64")
 
 
-def build_case(workload, n=64):
-    """(spec, restart state, topology, interior cells) of a workload."""
+def build_case(workload, n=64, size=(96, 48)):
+    """(spec, restart state, topology, interior cells) of a workload; size:
+    (radial, transverse) cells per block of the c2 slab."""
     from beta1_b200 import case
     if workload == "c1":
         spec = case.periodic_box_case((n, n, n))
         return spec, case.initial_state(spec), "periodic", n ** 3
     sc = case.ref_scales()
-    spec = case.slab_case(96, (48, 48), (3, 2), is_Lunar_resistance=1, use_implicit_lunar_resistance=1,
+    spec = case.slab_case(size[0], (size[1], size[1]), (3, 2), is_Lunar_resistance=1, use_implicit_lunar_resistance=1,
                           eta_max_lunar=1e-3 * case.MU0 * sc["U"] * sc["L_ref"], implicit_resistive_ksp_rtol=1e-10)
     cells = sum(b.ncell[0] * b.ncell[1] * b.ncell[2] for b in spec.blocks)
     return spec, case.inflow_state(spec), "tiled", cells
@@ -291,6 +295,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="c2", choices=list(WORKLOADS))
     ap.add_argument("--n", type=int, default=64, help="cells per direction of the c1 periodic block")
+    ap.add_argument("--c2-size", default="96x48", help="radial x transverse cells per c2 block (profiling runs "
+                                                         "use a smaller case; the bench line is quoted on 96x48)")
     ap.add_argument("--ref-steps", type=int, default=None, help="StepOnce per reference CPU sample")
     ap.add_argument("--e2e-iters", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -328,7 +334,8 @@ def main():
         spec = None
         nblocks = len(sweep)
     else:
-        spec, st, topology, cells = build_case(args.workload, args.n)
+        c2size = tuple(int(v) for v in args.c2_size.split("x"))
+        spec, st, topology, cells = build_case(args.workload, args.n, c2size)
         s = solver.Solver(spec, topology=topology, precision=prec)
         s.load_state(st)
         nblocks = len(spec.blocks)
@@ -440,6 +447,8 @@ def main():
                        "sample": "%s, %d StepOnce of the reference solver built from its own sources, one "
                                  "single-threaded process" % (wl["name"], ref_steps)}
 
+    config_name = workload_name(wl["name"] if args.workload != "c2" or args.c2_size == "96x48" else
+                                "c2_slab6x%sx%s_implicit_resistive_fp64" % (args.c2_size, args.c2_size.split("x")[1]), mixed)
     if rank == 0:
         line = {
             "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
@@ -447,7 +456,8 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 fluxes + f64 CT/state" if mixed else "f64",
             "data": "synthetic (seeded 1e-3 noise on rho, v and div-free B; reference restart format)",
-            "config": {"workload": workload_name(wl["name"], mixed), "cells_per_gpu": cells, "blocks": nblocks,
+            "config": {"workload": config_name,
+                       "cells_per_gpu": cells, "blocks": nblocks,
                        "integrator": "forward Euler StepOnce (reference parity mode)", "precision": args.precision,
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "no flush: per-step working set %.2f GB > 126 MB L2" % (ctx_bytes / 1e9)},
@@ -456,7 +466,7 @@ def main():
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": NCU_TRAFFIC_BYTES.get((dominant, args.n)),
+                         "traffic": NCU_TRAFFIC_BYTES.get((dominant, config_name)),
                          "algo_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_launch_ms,
                          "kernel_share": per_step[dominant] / total},
             "kernels_ms_per_step": {k: round(v, 5) for k, v in sorted(per_step.items(), key=lambda kv: -kv[1])},
