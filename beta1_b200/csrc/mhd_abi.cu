@@ -167,6 +167,8 @@ struct mhd_ctx
         std::vector<uint64_t> seed;              // unknown and alias offsets (Eres), for the region
         // the persistent solve (one cooperative kernel per solve)
         int64_t *alias_of = nullptr;             // unknown index of each alias's owner
+        int *uloc = nullptr;                     // per unknown: block, edge axis, i, j, k
+        int merge1 = 0, merge2 = 0;              // fixed values written in the phase before
         double *ppartial = nullptr;              // per-CTA partial dot products, double-buffered
         unsigned *bar = nullptr;                 // grid barrier: arrival count, generation
         int pgrid = 0;                           // CTAs of the persistent kernel (0: unavailable)
@@ -837,6 +839,9 @@ int launch_gmres_persistent(mhd_ctx *ctx)
     a.nalias = R.nalias;
     a.eres1form = dev_copy(R.eres1form);
     a.db = dev_copy(R.db);
+    a.uloc = R.uloc;
+    a.merge1 = R.merge1;
+    a.merge2 = R.merge2;
     a.rng = R.rng;
     a.nreg = R.nreg_max;
     a.dtp = ctx->dt;
@@ -1765,7 +1770,7 @@ static void free_resistive(mhd_ctx *ctx)
     for (void *p : {(void *)R.e, (void *)R.dj, (void *)R.j, (void *)R.eta, (void *)R.alias_e, (void *)R.owner_e,
                     (void *)R.sign, (void *)R.rng, (void *)R.V, (void *)R.w, (void *)R.x,
                     (void *)R.b, (void *)R.r, (void *)R.partial, (void *)R.dots, (void *)R.st,
-                    (void *)R.alias_of, (void *)R.ppartial, (void *)R.bar})
+                    (void *)R.alias_of, (void *)R.ppartial, (void *)R.bar, (void *)R.uloc})
         cudaFree(p);
     free_list(R.eres1form);
     free_list(R.db);
@@ -2275,6 +2280,54 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
     R.seed = he;
     R.seed.insert(R.seed.end(), fa.begin(), fa.end());
     RUN(resistive_region(ctx, R.seed));
+    // the persistent solve's phase merges and unknown locations
+    {
+        PoolDecoder dec(ctx);
+        std::vector<int> uloc(size_t(5 * n));
+        for (int64_t t = 0; t < n; ++t)
+        {
+            int f, b, i, j, k;
+            if (!dec.decode(he[size_t(t)], f, b, i, j, k))
+                return fail(ctx, MHD_EINVAL, "resistive unknown %lld does not decode", (long long)t);
+            const int loc[5] = {b, f - F_Eresxi, i, j, k};
+            std::copy(loc, loc + 5, uloc.begin() + 5 * t);
+        }
+        RUN(upload_vec(ctx, uloc, &R.uloc));
+        auto fetch = [&](const CopyList &l, std::vector<uint64_t> &h) -> int {
+            h.resize(size_t(l.nconst));
+            if (l.nconst > 0)
+                CK(ctx, cudaMemcpy(h.data(), l.cdst, size_t(l.nconst) * 8, cudaMemcpyDeviceToHost));
+            return MHD_OK;
+        };
+        // Sync("Eres1form")'s fixed values may be written with the unknowns
+        // and aliases when they touch none of them
+        std::vector<uint64_t> c1, c2;
+        RUN(fetch(R.eres1form, c1));
+        RUN(fetch(R.db, c2));
+        std::vector<uint64_t> written(he);
+        written.insert(written.end(), fa.begin(), fa.end());
+        std::sort(written.begin(), written.end());
+        R.merge1 = 1;
+        for (uint64_t o : c1)
+            if (std::binary_search(written.begin(), written.end(), o))
+                R.merge1 = 0;
+        // Sync("dB")'s fixed values may be written with the curl, which
+        // writes inner faces only, when none of them is an inner face
+        R.merge2 = 1;
+        for (uint64_t o : c2)
+        {
+            int f, b, i, j, k;
+            if (!dec.decode(o, f, b, i, j, k))
+            {
+                R.merge2 = 0;
+                continue;
+            }
+            const BlockView &v = ctx->hbv[size_t(b)];
+            const int a = f - F_dBxi;
+            if (i >= 0 && j >= 0 && k >= 0 && i < v.ni + (a == 0) && j < v.nj + (a == 1) && k < v.nk + (a == 2))
+                R.merge2 = 0;
+        }
+    }
     // every point of the solve's fields starts at zero
     for (int f0 : {int(F_Eresxi), int(F_dBxi), int(F_dJxi), int(F_RBresxi)})
         for (int f = f0; f < f0 + 3; ++f)

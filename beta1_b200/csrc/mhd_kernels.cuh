@@ -108,6 +108,9 @@ struct ResistSolve
     const double *sign;
     int64_t nalias;
     DevCopy eres1form, db;
+    const int *uloc; // per unknown: block, edge axis, i, j, k
+    int merge1;      // Sync("Eres1form")'s fixed values may go with the unknowns' writes
+    int merge2;      // Sync("dB")'s fixed values may go with the curl
     const int *rng; // per block region box
     int64_t nreg;   // points of the largest region box
     const double *dtp;

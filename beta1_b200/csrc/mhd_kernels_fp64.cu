@@ -1323,11 +1323,11 @@ __device__ bool grid_dots(const ResistSolve &a, const double *V, int nv, const d
     return true;
 }
 
-// fixed values then copies of a point list
-__device__ bool grid_apply(const ResistSolve &a, const DevCopy &l)
+// fixed values (unless already written) then copies of a point list
+__device__ bool grid_apply(const ResistSolve &a, const DevCopy &l, bool consts_done)
 {
     const int64_t t0 = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, ts = int64_t(gridDim.x) * blockDim.x;
-    if (l.nconst > 0)
+    if (l.nconst > 0 && !consts_done)
     {
         for (int64_t t = t0; t < l.nconst; t += ts)
             a.pool[l.cdst[t]] = l.cval[t];
@@ -1351,21 +1351,28 @@ __device__ bool grid_apply(const ResistSolve &a, const DevCopy &l)
     return grid_barrier(a.bar, a.err);
 }
 
-// y = A x (MatMultImplicitResistive_): Eres at the unknowns and their aliases
-// from x, Sync("Eres1form"), dB = -dt curl Eres on the region, Sync("dB"),
-// dJ = alpha curlAdj(beta dB) on the region, y = Eres - eta dJ
-__device__ bool grid_matvec(const ResistSolve &a, const double *x, double *y)
+// y = A (src / div) (MatMultImplicitResistive_): Eres at the unknowns and
+// their aliases, Sync("Eres1form"), dB = -dt curl Eres on the region,
+// Sync("dB"), then per unknown dJ = alpha curlAdj(beta dB) at its edge and
+// y = Eres - eta dJ.  src must be complete at entry unless first_barrier:
+// the aliases read other threads' elements.  src / div is the stored basis
+// vector bit for bit (the same division), so the basis vector itself need
+// not be complete.
+__device__ bool grid_matvec(const ResistSolve &a, const double *src, double div, bool first_barrier, double *y)
 {
     const int64_t t0 = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, ts = int64_t(gridDim.x) * blockDim.x;
-    if (!grid_barrier(a.bar, a.err)) // x complete
+    if (first_barrier && !grid_barrier(a.bar, a.err))
         return false;
     for (int64_t t = t0; t < a.n; t += ts)
-        a.pool[a.e[t]] = x[t];
+        a.pool[a.e[t]] = src[t] / div;
     for (int64_t q = t0; q < a.nalias; q += ts)
-        a.pool[a.alias[q]] = a.sign[q] * x[a.alias_of[q]];
+        a.pool[a.alias[q]] = a.sign[q] * (src[a.alias_of[q]] / div);
+    if (a.merge1)
+        for (int64_t t = t0; t < a.eres1form.nconst; t += ts)
+            a.pool[a.eres1form.cdst[t]] = a.eres1form.cval[t];
     if (!grid_barrier(a.bar, a.err))
         return false;
-    if (!grid_apply(a, a.eres1form))
+    if (!grid_apply(a, a.eres1form, a.merge1 != 0))
         return false;
     const double mdt = -a.dtp[0];
     const int64_t np = int64_t(a.nblocks) * a.nreg;
@@ -1377,25 +1384,19 @@ __device__ bool grid_matvec(const ResistSolve &a, const double *x, double *y)
         if (stagger_point(b, a.rng, blk, q % a.nreg, i, j, k))
             curl_point(b, F_Eresxi, F_dBxi, -1, mdt, 0.0, i, j, k);
     }
+    if (a.merge2)
+        for (int64_t t = t0; t < a.db.nconst; t += ts)
+            a.pool[a.db.cdst[t]] = a.db.cval[t];
     if (!grid_barrier(a.bar, a.err))
         return false;
-    if (!grid_apply(a, a.db))
-        return false;
-    for (int64_t q = t0; q < np; q += ts)
-    {
-        const int blk = int(q / a.nreg);
-        const BlockView &b = a.bvs[blk];
-        int i, j, k;
-        if (stagger_point(b, a.rng, blk, q % a.nreg, i, j, k))
-#pragma unroll
-            for (int ea = 0; ea < 3; ++ea)
-                if (inner_of(b, 1, ea, i, j, k))
-                    jedge_one(b, ea, i, j, k, F_dBxi, F_dJxi, 1.0);
-    }
-    if (!grid_barrier(a.bar, a.err))
+    if (!grid_apply(a, a.db, a.merge2 != 0))
         return false;
     for (int64_t t = t0; t < a.n; t += ts)
+    {
+        const int *u = a.uloc + 5 * t;
+        jedge_one(a.bvs[u[0]], u[1], u[2], u[3], u[4], F_dBxi, F_dJxi, 1.0);
         y[t] = a.pool[a.e[t]] - a.eta[t] * a.pool[a.dj[t]];
+    }
     return true;
 }
 
@@ -1428,7 +1429,7 @@ __global__ void __launch_bounds__(256) k_gmres_resist(ResistSolve a)
     for (;;)
     {
         // cycle start: r = b - A x, beta = ||r||
-        if (!grid_matvec(a, a.x, a.w))
+        if (!grid_matvec(a, a.x, 1.0, true, a.w))
             return;
         for (int64_t t = t0; t < n; t += ts)
             a.r[t] = a.b[t] - a.w[t];
@@ -1462,8 +1463,9 @@ __global__ void __launch_bounds__(256) k_gmres_resist(ResistSolve a)
         while (S.inner)
         {
             const int j = S.j;
-            double *Vj = a.V + int64_t(j) * n;
-            if (!grid_matvec(a, Vj, a.w))
+            // V_j = r / beta (j = 0) or the previous step's w / ||w||, both
+            // complete at the last reduction's barrier
+            if (!grid_matvec(a, j == 0 ? a.r : a.w, j == 0 ? S.beta : S.hcol[j], false, a.w))
                 return;
             // classical Gram-Schmidt, twice
             if (!grid_dots(a, a.V, j + 1, a.w, S.hcol, pbuf))
