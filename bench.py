@@ -340,6 +340,8 @@ def main():
         s.load_state(st)
         nblocks = len(spec.blocks)
     ctx = s.ctx
+    # register / occupancy variant of each hot kernel, timed on this state
+    tuned = ctx.autotune(reps=10)
     stream = torch.cuda.ExternalStream(ctx.stream())
     ctx_bytes = sum(ctx.field_info(f, b)["ncomp"] * int(np.prod([h - l for l, h in zip(
         ctx.field_info(f, b)["lo"], ctx.field_info(f, b)["hi"])])) * 8 for f in ("U_H", "PV_H", "JDxi", "JDet",
@@ -457,7 +459,7 @@ def main():
             "dtype": "f32 fluxes + f64 CT/state" if mixed else "f64",
             "data": "synthetic (seeded 1e-3 noise on rho, v and div-free B; reference restart format)",
             "config": {"workload": config_name,
-                       "cells_per_gpu": cells, "blocks": nblocks,
+                       "cells_per_gpu": cells, "blocks": nblocks, "autotune_min_ctas_per_sm": tuned,
                        "integrator": "forward Euler StepOnce (reference parity mode)", "precision": args.precision,
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "no flush: per-step working set %.2f GB > 126 MB L2" % (ctx_bytes / 1e9)},

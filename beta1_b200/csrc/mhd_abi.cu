@@ -94,6 +94,23 @@ constexpr int kNumKernelNames = int(sizeof(kKernelNames) / sizeof(kKernelNames[0
 
 } // namespace
 
+// kernels compiled in register / occupancy variants (mhd_kernels.cuh)
+enum TuneId
+{
+    TUNE_k_pv_uplus_dt,
+    TUNE_k_fluid_ucontra,
+    TUNE_k_bcell_jedge,
+    TUNE_k_eface,
+    TUNE_k_curl_e2f,
+    TUNE_k_eedge,
+    TUNE_k_fluid_mixed,
+    NTUNE
+};
+const char *const kTuneNames[NTUNE] = {"k_pv_uplus_dt", "k_fluid_ucontra", "k_bcell_jedge", "k_eface",
+                                       "k_curl_e2f",    "k_eedge",         "k_fluid_mixed"};
+// minimum CTAs per SM of each variant (variant 0 first)
+const int kTuneMinCtas[NTUNE][3] = {{4, 1, 5}, {1, 3, 0}, {1, 6, 0}, {1, 6, 0}, {1, 6, 0}, {1, 8, 0}, {2, 1, 3}};
+
 struct mhd_ctx
 {
     int nblocks = 0;
@@ -205,6 +222,9 @@ struct mhd_ctx
     double res_inver_Rem = 0.0;
     cudaStream_t spare[2] = {nullptr, nullptr}; // capture streams of conditional bodies
     int spare_depth = 0;
+
+    // register / occupancy variant of each tunable kernel (mhd_autotune)
+    int tune[NTUNE] = {0, 0, 0, 0, 0, 0, 0};
 
     // eager profiling: one event pair per launch
     bool profiling = false;
@@ -463,7 +483,7 @@ int launch_update_derived(mhd_ctx *ctx)
 {
     cudaStream_t s = ctx->stream;
     prof_begin(ctx, "k_bcell_jedge");
-    k_bcell_jedge<<<grid_kind(ctx, KIND_STAG), kThreads, 0, s>>>(ctx->dbv);
+    launch_k_bcell_jedge(ctx->tune[TUNE_k_bcell_jedge], grid_kind(ctx, KIND_STAG), s, ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "B_cell"));
     RUN(run_sync(ctx, "Jedge"));
@@ -474,7 +494,7 @@ int launch_update_derived(mhd_ctx *ctx)
     // first ghost layer only: deeper PV / U_plus ghosts are read by no kernel
     // of the step and are filled when read out (materialise_pv)
     prof_begin(ctx, "k_pv_uplus_dt");
-    k_pv_uplus_dt<<<grid_kind(ctx, KIND_CELL1), kThreads, 0, s>>>(ctx->dbv, ctx->c, ctx->dt_key, 1, 1);
+    launch_k_pv_uplus_dt(ctx->tune[TUNE_k_pv_uplus_dt], grid_kind(ctx, KIND_CELL1), s, ctx->dbv, ctx->c, ctx->dt_key, 1, 1);
     ctx->pv_dirty = true;
     RUN(launched(ctx));
     RUN(run_sync(ctx, "J_cell"));
@@ -500,11 +520,11 @@ int launch_fluid_ucontra(mhd_ctx *ctx)
     if (ctx->pool32)
     {
         prof_begin(ctx, "k_fluid_mixed");
-        k_fluid_mixed<<<grid_kind(ctx, KIND_CELL1), kThreads, 0, ctx->stream>>>(ctx->dbv, ctx->c);
+        launch_k_fluid_mixed(ctx->tune[TUNE_k_fluid_mixed], grid_kind(ctx, KIND_CELL1), ctx->stream, ctx->dbv, ctx->c);
         return launched(ctx);
     }
     prof_begin(ctx, "k_fluid_ucontra");
-    k_fluid_ucontra<<<grid_kind(ctx, KIND_CELL1), kThreads, 0, ctx->stream>>>(ctx->dbv, ctx->c);
+    launch_k_fluid_ucontra(ctx->tune[TUNE_k_fluid_ucontra], grid_kind(ctx, KIND_CELL1), ctx->stream, ctx->dbv, ctx->c);
     return launched(ctx);
 }
 
@@ -520,17 +540,17 @@ int launch_induction(mhd_ctx *ctx, bool update_b, bool with_ucontra = true)
         RUN(launched(ctx));
     }
     prof_begin(ctx, "k_eface");
-    k_eface<<<grid_kind(ctx, KIND_STAG), kThreads, 0, s>>>(ctx->dbv);
+    launch_k_eface(ctx->tune[TUNE_k_eface], grid_kind(ctx, KIND_STAG), s, ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Eface"));
     // inner edges; ghost edges keep their zero of AssembleRHS_Induction_CT_
     // except where the Eedge sync writes them
     prof_begin(ctx, "k_eedge");
-    k_eedge<<<grid_kind(ctx, KIND_STAG), kThreads, 0, s>>>(ctx->dbv);
+    launch_k_eedge(ctx->tune[TUNE_k_eedge], grid_kind(ctx, KIND_STAG), s, ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Eedge"));
     prof_begin(ctx, "k_curl_e2f");
-    k_curl_e2f<<<grid_kind(ctx, KIND_STAG), kThreads, 0, s>>>(ctx->dbv, F_Exi, F_RBxi, update_b ? F_Bxi : -1, -1.0,
+    launch_k_curl_e2f(ctx->tune[TUNE_k_curl_e2f], grid_kind(ctx, KIND_STAG), s, ctx->dbv, F_Exi, F_RBxi, update_b ? F_Bxi : -1, -1.0,
                                                              ctx->dt, 1.0, 0, nullptr);
     return launched(ctx);
 }
@@ -561,7 +581,7 @@ int launch_curl_rng(mhd_ctx *ctx, int fE0, int fR0, int fB0, double mult, int mu
     if (R.nreg_max == 0)
         return MHD_OK;
     prof_begin(ctx, "k_curl_e2f");
-    k_curl_e2f<<<dim3(grid_for(R.nreg_max), ctx->nblocks), kThreads, 0, ctx->stream>>>(
+    launch_k_curl_e2f(ctx->tune[TUNE_k_curl_e2f], dim3(grid_for(R.nreg_max), ctx->nblocks), ctx->stream, 
         ctx->dbv, fE0, fR0, fB0, mult, ctx->dt, 1.0, mult_is_neg_dt, R.rng);
     return launched(ctx);
 }
@@ -943,7 +963,7 @@ int launch_resistive_explicit(mhd_ctx *ctx)
         RUN(launched(ctx));
         RUN(run_sync(ctx, "Eres"));
         prof_begin(ctx, "k_curl_e2f");
-        k_curl_e2f<<<dim3(gs, nb), kThreads, 0, s>>>(ctx->dbv, F_Eresxi, F_RBresxi, F_Bxi, -1.0, ctx->dt,
+        launch_k_curl_e2f(ctx->tune[TUNE_k_curl_e2f], dim3(gs, nb), s, ctx->dbv, F_Eresxi, F_RBresxi, F_Bxi, -1.0, ctx->dt,
                                                      double(ctx->res_nsub), 0, nullptr);
         RUN(launched(ctx));
         RUN(run_sync(ctx, "Bface"));
@@ -1018,7 +1038,7 @@ int hall_trial_b(mhd_ctx *ctx, const double *X)
         LAUNCHN(k_alias_copy, H.nalias, ctx->pool, H.alias, H.owner, H.sign, H.nalias);
     RUN(run_sync(ctx, "Ehall", true));
     prof_begin(ctx, "k_curl_e2f");
-    k_curl_e2f<<<dim3(grid_for(max_stagger(ctx)), ctx->nblocks), kThreads, 0, ctx->stream>>>(
+    launch_k_curl_e2f(ctx->tune[TUNE_k_curl_e2f], dim3(grid_for(max_stagger(ctx)), ctx->nblocks), ctx->stream, 
         ctx->dbv, F_Ehxi, F_RBxi, F_Bxi, -1.0, ctx->dt, 1.0, 0, nullptr);
     RUN(launched(ctx));
     return run_sync(ctx, "Bface");
@@ -1990,7 +2010,7 @@ static int materialise_pv(mhd_ctx *ctx)
     RUN(materialise_group(ctx, "Ucell"));
     RUN(ensure_geom(ctx));
     prof_begin(ctx, "k_pv_uplus_dt");
-    k_pv_uplus_dt<<<dim3(grid_for(max_box(ctx, LOC_CELL, ctx->G)), ctx->nblocks), kThreads, 0, ctx->stream>>>(
+    launch_k_pv_uplus_dt(ctx->tune[TUNE_k_pv_uplus_dt], dim3(grid_for(max_box(ctx, LOC_CELL, ctx->G)), ctx->nblocks), ctx->stream, 
         ctx->dbv, ctx->c, nullptr, ctx->G, 0);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Uplus", true));
@@ -2522,6 +2542,113 @@ int mhd_set_flux_reference(mhd_ctx *ctx, const double prim[5])
     return mhd_set_flux_reference_run(ctx, -1, prim);
 }
 
+int mhd_autotune(mhd_ctx *ctx, int32_t reps, int32_t *min_ctas, int32_t n)
+{
+    if (!ctx || reps < 1 || n < 0 || (n > 0 && !min_ctas))
+        return fail(ctx, MHD_EINVAL, "bad autotune arguments");
+    if (ctx->capturing)
+        return fail(ctx, MHD_ESTATE, "autotune during capture");
+    RUN(ensure_geom(ctx));
+    cudaStream_t s = ctx->stream;
+    // snapshot of the state (U_H and the face B of every block) and of the
+    // run clocks (dt keys, dt, time, step: one contiguous allocation)
+    const int sf[4] = {F_U, F_Bxi, F_Beta, F_Bzeta};
+    size_t tot = 0;
+    for (int f : sf)
+        for (int b = 0; b < ctx->nblocks; ++b)
+            tot += size_t(kFields[f].ncomp) * size_t(ctx->hbv[size_t(b)].vol);
+    const size_t clock_bytes = 32 * size_t(ctx->nruns);
+    double *snap = nullptr;
+    CK(ctx, cudaMalloc(&snap, tot * 8 + clock_bytes));
+    auto copy_state = [&](bool save) -> int {
+        size_t o = 0;
+        for (int f : sf)
+            for (int b = 0; b < ctx->nblocks; ++b)
+            {
+                const size_t cnt = size_t(kFields[f].ncomp) * size_t(ctx->hbv[size_t(b)].vol);
+                double *field = ctx->pool + ctx->base[size_t(f)][size_t(b)];
+                CK(ctx, cudaMemcpyAsync(save ? snap + o : field, save ? field : snap + o, cnt * 8,
+                                        cudaMemcpyDeviceToDevice, s));
+                o += cnt;
+            }
+        char *clk = reinterpret_cast<char *>(snap + tot);
+        CK(ctx, cudaMemcpyAsync(save ? static_cast<void *>(clk) : static_cast<void *>(ctx->dt_key),
+                                save ? static_cast<const void *>(ctx->dt_key) : static_cast<const void *>(clk),
+                                clock_bytes, cudaMemcpyDeviceToDevice, s));
+        if (!save)
+            RUN(launch_update_derived(ctx)); // derived fields of the restored state
+        return MHD_OK;
+    };
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(ctx, cudaEventCreate(&e0));
+    CK(ctx, cudaEventCreate(&e1));
+    // `reps` whole steps (the step graph) from the saved state, after one
+    // step that builds the graph
+    auto time_steps = [&](float &ms) -> int {
+        RUN(copy_state(false));
+        RUN(run_steps(ctx, 1));
+        RUN(copy_state(false));
+        CK(ctx, cudaEventRecord(e0, s));
+        RUN(run_steps(ctx, reps));
+        CK(ctx, cudaEventRecord(e1, s));
+        CK(ctx, cudaEventSynchronize(e1));
+        CK(ctx, cudaEventElapsedTime(&ms, e0, e1));
+        return check_err(ctx);
+    };
+    // the faster of two timings of kernel t in variant v (clock and cache noise)
+    auto trial = [&](int t, int v, float &ms) -> int {
+        ctx->tune[t] = v;
+        drop_graph(ctx);
+        float a = 0.0f, b = 0.0f;
+        RUN(time_steps(a));
+        RUN(time_steps(b));
+        ms = std::min(a, b);
+        return MHD_OK;
+    };
+    int rc = copy_state(true);
+    // bring the clocks up before anything is compared
+    for (int w = 0; w < 3 && rc == MHD_OK; ++w)
+    {
+        float ms = 0.0f;
+        rc = time_steps(ms);
+    }
+    for (int t = 0; t < NTUNE && rc == MHD_OK; ++t)
+    {
+        // the flux kernel of the precision in use only
+        if ((t == TUNE_k_fluid_mixed && !ctx->pool32) || (t == TUNE_k_fluid_ucontra && ctx->pool32))
+            continue;
+        int keep = ctx->tune[t];
+        for (int v = 0; v < 3 && kTuneMinCtas[t][v] > 0 && rc == MHD_OK; ++v)
+        {
+            if (v == keep)
+                continue;
+            // the candidate and the kept variant timed back to back; the
+            // candidate replaces it only when the step is clearly faster
+            float ms_v = 0.0f, ms_k = 0.0f;
+            rc = trial(t, v, ms_v);
+            if (rc == MHD_OK)
+                rc = trial(t, keep, ms_k);
+            if (rc == MHD_OK && ms_v < 0.97f * ms_k)
+                keep = v;
+        }
+        ctx->tune[t] = keep;
+        drop_graph(ctx);
+    }
+    if (rc == MHD_OK)
+        rc = copy_state(false);
+    cudaStreamSynchronize(s);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(snap);
+    drop_graph(ctx);
+    RUN(rc);
+    for (int i = 0; i < n && i < NTUNE; ++i)
+        min_ctas[i] = kTuneMinCtas[i][ctx->tune[i]];
+    return MHD_OK;
+}
+
+const char *mhd_tune_name(int32_t i) { return (i >= 0 && i < NTUNE) ? kTuneNames[i] : nullptr; }
+
 int mhd_resistive_stats(const mhd_ctx *ctx, int32_t *its, double *rnorm, double *bnorm, int32_t *reason)
 {
     if (!ctx)
@@ -2674,7 +2801,7 @@ int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
         RUN(launch_update_u(ctx));
         {
             prof_begin(ctx, "k_curl_e2f");
-            k_curl_e2f<<<grid_kind(ctx, KIND_STAG), kThreads, 0, ctx->stream>>>(ctx->dbv, F_Exi, -1, F_Bxi, -1.0,
+            launch_k_curl_e2f(ctx->tune[TUNE_k_curl_e2f], grid_kind(ctx, KIND_STAG), ctx->stream, ctx->dbv, F_Exi, -1, F_Bxi, -1.0,
                                                                                 ctx->dt, 1.0, 0, nullptr);
             RUN(launched(ctx));
         }

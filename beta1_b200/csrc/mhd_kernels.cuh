@@ -22,26 +22,19 @@ struct Consts
 __global__ void k_fluid_rhs(const BlockView *bvs, Consts c, int64_t maxpts);
 __global__ void k_ucontra(const BlockView *bvs);
 __global__ void k_face_normals(const BlockView *bvs);
-__global__ void k_eface(const BlockView *bvs);
-__global__ void k_eedge(const BlockView *bvs);
 // Face / edge kernels run one thread per staggered point (i, j, k) in
 // [0, n + 1)^3 and handle all three axes there.  rng (may be null): per
 // block a region box lo[3], hi[3]; only points inside it are processed.
-__global__ void k_curl_e2f(const BlockView *bvs, int fE0, int fR0, int fB0, double mult, const double *dtp,
-                           double dtdiv, int mult_is_neg_dt, const int *rng);
 __global__ void k_update_u(const BlockView *bvs, const double *dtp);
 __global__ void k_divb(const BlockView *bvs);
 // mixed precision (mhd_kernels_mixed.cu)
 __global__ void k_geom32(const BlockView *bvs);
-__global__ void k_fluid_mixed(const BlockView *bvs, Consts c);
 __global__ void k_hall_cell(const BlockView *bvs, Consts c, double hall_coef);
 __global__ void k_hall_edge(const BlockView *bvs, const int *zb, int nzb);
 __global__ void k_eres_explicit(const BlockView *bvs, double inver_Rem);
 __global__ void k_bcell(const BlockView *bvs);
 __global__ void k_jedge(const BlockView *bvs, int fB0, int fJ0, double mult, const int *rng);
 __global__ void k_jcell(const BlockView *bvs);
-__global__ void k_pv_uplus_dt(const BlockView *bvs, Consts c, unsigned long long *dt_key, int depth, int with_jcell);
-__global__ void k_bcell_jedge(const BlockView *bvs);
 __global__ void k_begin_step(const unsigned long long *dt_key, double *dt, int *err, double dt_abort, int nruns);
 __global__ void k_arm_dt(unsigned long long *dt_key, int nruns);
 __global__ void k_end_step(const double *dt, double *time, long long *step, int nruns);
@@ -49,7 +42,6 @@ __global__ void k_gather(double *pool, const uint64_t *dst, const uint64_t *src,
 __global__ void k_set_consts(double *pool, const uint64_t *dst, const double *val, int64_t n);
 __global__ void k_wall_u(const BlockView *bvs, int blk, int dir, double gamma);
 __global__ void k_wall_u_all(const BlockView *bvs, const int *walls, double gamma);
-__global__ void k_fluid_ucontra(const BlockView *bvs, Consts c);
 __global__ void k_gather_stage(double *tmp, const double *pool, const uint64_t *src, int64_t n);
 __global__ void k_scatter_stage(double *pool, const double *tmp, const uint64_t *dst, int64_t n);
 __global__ void k_aos_to_soa(const BlockView *bvs, int blk, int fid, int ncomp, int lo0, int lo1, int lo2, int n0,
@@ -156,5 +148,26 @@ __global__ void k_hall_residual(const double *pool, const uint64_t *e, const dou
 __global__ void k_axpy_to(double *out, const double *x, double a, const double *y, int64_t n);
 __global__ void k_fd_quotient(double *out, const double *a, const double *b, double h, int64_t n);
 __global__ void k_negate(double *out, const double *x, int64_t n);
+
+
+// Hot stencil kernels in register / occupancy variants (the same code under
+// different __launch_bounds__ minimum CTAs per SM); variant 0 is the default.
+// Returns -1 for an unknown variant.
+// k_pv_uplus_dt: minimum CTAs per SM 4, 1, 5
+int launch_k_pv_uplus_dt(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c,
+                         unsigned long long *dt_key, int depth, int with_jcell);
+// k_fluid_ucontra: minimum CTAs per SM 1, 3
+int launch_k_fluid_ucontra(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c);
+// k_bcell_jedge: minimum CTAs per SM 1, 6
+int launch_k_bcell_jedge(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs);
+// k_eface: minimum CTAs per SM 1, 6
+int launch_k_eface(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs);
+// k_curl_e2f: minimum CTAs per SM 1, 6
+int launch_k_curl_e2f(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, int fE0, int fR0, int fB0,
+                      double mult, const double *dtp, double dtdiv, int mult_is_neg_dt, const int *rng);
+// k_eedge: minimum CTAs per SM 1, 8
+int launch_k_eedge(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs);
+// k_fluid_mixed: minimum CTAs per SM 2, 1, 3
+int launch_k_fluid_mixed(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c);
 
 } // namespace mhd

@@ -254,7 +254,7 @@ __global__ void k_ucontra(const BlockView *__restrict__ bvs)
 // the fluid RHS of the inner cells and the contravariant velocities of the
 // cells within one ghost layer in one pass (both read JD and Jac around the
 // same cells; U_contra is read only by the EMF kernels that follow)
-__global__ void k_fluid_ucontra(const BlockView *__restrict__ bvs, Consts c)
+__device__ __forceinline__ void k_fluid_ucontra_body(const BlockView *__restrict__ bvs, Consts c)
 {
     int64_t t;
     const BlockView &b = bvs[cta_block(bvs, KIND_CELL1, t)];
@@ -271,6 +271,12 @@ __global__ void k_fluid_ucontra(const BlockView *__restrict__ bvs, Consts c)
     UC[b.vol + p] = u_contra(b, 1, i, j, k);
     UC[2 * b.vol + p] = u_contra(b, 2, i, j, k);
 }
+
+template <int MINB> __global__ void __launch_bounds__(256, MINB) k_fluid_ucontra_t(const BlockView *__restrict__ bvs, Consts c)
+{
+    k_fluid_ucontra_body(bvs, c);
+}
+
 
 // contravariant velocity of a cell, as stored by the fluid pass
 __device__ __forceinline__ double uc(const BlockView &b, int axis, int i, int j, int k)
@@ -360,7 +366,7 @@ __device__ __forceinline__ bool inner_of(const BlockView &b, int kind, int a, in
     return i < b.ni + pl[0] && j < b.nj + pl[1] && k < b.nk + pl[2];
 }
 
-__global__ void k_eface(const BlockView *__restrict__ bvs)
+__device__ __forceinline__ void k_eface_body(const BlockView *__restrict__ bvs)
 {
     int64_t t;
     const BlockView &b = bvs[cta_block(bvs, KIND_STAG, t)];
@@ -372,6 +378,12 @@ __global__ void k_eface(const BlockView *__restrict__ bvs)
         if (inner_of(b, 0, fa, i, j, k))
             eface_one(b, fa, i, j, k);
 }
+
+template <int MINB> __global__ void __launch_bounds__(256, MINB) k_eface_t(const BlockView *__restrict__ bvs)
+{
+    k_eface_body(bvs);
+}
+
 
 // ---------------------------------------------------------------------------
 // AssembleEdgeEMF_FromFaceE_Ideal_ (LunarSolver_MagExplicit_Ideal.cpp:53-287)
@@ -437,7 +449,7 @@ __device__ __forceinline__ double eedge_one(const BlockView &b, int ea, int i, i
 
 // inner edges of all three axes; ghost edges keep the zero of
 // AssembleRHS_Induction_CT_ except where the Eedge sync writes them
-__global__ void k_eedge(const BlockView *__restrict__ bvs)
+__device__ __forceinline__ void k_eedge_body(const BlockView *__restrict__ bvs)
 {
     int64_t t;
     const BlockView &b = bvs[cta_block(bvs, KIND_STAG, t)];
@@ -449,6 +461,12 @@ __global__ void k_eedge(const BlockView *__restrict__ bvs)
         if (inner_of(b, 1, ea, i, j, k))
             b.f[F_Exi + ea][pidx(b, i, j, k)] = eedge_one(b, ea, i, j, k);
 }
+
+template <int MINB> __global__ void __launch_bounds__(256, MINB) k_eedge_t(const BlockView *__restrict__ bvs)
+{
+    k_eedge_body(bvs);
+}
+
 
 // ---------------------------------------------------------------------------
 // CTOperators::CurlEdgeToFace (Z4_Lunar/src/operators/CTOperators.cpp:6-56)
@@ -482,7 +500,7 @@ __device__ __forceinline__ void curl_point(const BlockView &b, int fE0, int fR0,
     }
 }
 
-__global__ void k_curl_e2f(const BlockView *__restrict__ bvs, int fE0, int fR0, int fB0, double mult,
+__device__ __forceinline__ void k_curl_e2f_body(const BlockView *__restrict__ bvs, int fE0, int fR0, int fB0, double mult,
                            const double *__restrict__ dtp, double dtdiv, int mult_is_neg_dt, const int *__restrict__ rng)
 {
     int64_t t;
@@ -495,6 +513,13 @@ __global__ void k_curl_e2f(const BlockView *__restrict__ bvs, int fE0, int fR0, 
         return;
     curl_point(b, fE0, fR0, fB0, mult, fB0 >= 0 ? dtp[b.run] / dtdiv : 0.0, i, j, k);
 }
+
+template <int MINB> __global__ void __launch_bounds__(256, MINB) k_curl_e2f_t(const BlockView *__restrict__ bvs, int fE0, int fR0, int fB0, double mult,
+                           const double *__restrict__ dtp, double dtdiv, int mult_is_neg_dt, const int *__restrict__ rng)
+{
+    k_curl_e2f_body(bvs, fE0, fR0, fB0, mult, dtp, dtdiv, mult_is_neg_dt, rng);
+}
+
 
 // calc_divB on inner cells (Z4_Lunar/src/physics/LunarSolver_Tools.cpp:685-775;
 // layouts with Pole patches, whose first shell the reference zeroes, are not
@@ -805,7 +830,7 @@ __global__ void k_jedge(const BlockView *__restrict__ bvs, int fB0, int fJ0, dou
 // calc_Bcell and Calc_J_Edge in one pass over the staggered points: both
 // read the face B around the same points (the B_cell sync between them in
 // the reference touches neither input)
-__global__ void k_bcell_jedge(const BlockView *__restrict__ bvs)
+__device__ __forceinline__ void k_bcell_jedge_body(const BlockView *__restrict__ bvs)
 {
     int64_t t;
     const BlockView &b = bvs[cta_block(bvs, KIND_STAG, t)];
@@ -819,6 +844,12 @@ __global__ void k_bcell_jedge(const BlockView *__restrict__ bvs)
         if (inner_of(b, 1, ea, i, j, k))
             jedge_one(b, ea, i, j, k, F_Bxi, F_Jxi, 1.0);
 }
+
+template <int MINB> __global__ void __launch_bounds__(256, MINB) k_bcell_jedge_t(const BlockView *__restrict__ bvs)
+{
+    k_bcell_jedge_body(bvs);
+}
+
 
 // ---------------------------------------------------------------------------
 // calc_Jcell (LunarSolver_Tools.cpp:837-892)
@@ -900,10 +931,10 @@ __device__ __forceinline__ unsigned long long dbl_key(double x)
     return (unsigned long long)__double_as_longlong(x);
 }
 
-// 64 registers (4 CTAs per SM) instead of 80 (3): the extra warps hide more
-// of the weight-stream latency (0.216 -> 0.205 ms on the C2 step)
-__global__ void __launch_bounds__(256, 4)
-    k_pv_uplus_dt(const BlockView *__restrict__ bvs, Consts c, unsigned long long *dt_key, int depth,
+// variants: at least 4 CTAs per SM (64 registers; the default: the extra
+// warps hide more of the weight-stream latency, 0.216 -> 0.205 ms on the C2
+// step against the uncapped 80 registers), uncapped, at least 5
+__device__ __forceinline__ void k_pv_uplus_dt_body(const BlockView *__restrict__ bvs, Consts c, unsigned long long *dt_key, int depth,
                               int with_jcell)
 {
     int64_t t;
@@ -1026,6 +1057,13 @@ __global__ void __launch_bounds__(256, 4)
             atomicMin(dt_key + b.run, key);
     }
 }
+
+template <int MINB> __global__ void __launch_bounds__(256, MINB) k_pv_uplus_dt_t(const BlockView *__restrict__ bvs, Consts c, unsigned long long *dt_key, int depth,
+                              int with_jcell)
+{
+    k_pv_uplus_dt_body(bvs, c, dt_key, depth, with_jcell);
+}
+
 
 // Start of StepOnce: dt = global minimum of the CFL bounds, abort check
 // (dt < dt_abort or NaN sets the error word, LunarSolver_Timestep.cpp:128-139).
@@ -1576,6 +1614,108 @@ __global__ void __launch_bounds__(256) k_gmres_resist(ResistSolve a)
         st->total_its += S.its;
         st->total_cycles += S.cycles;
     }
+}
+
+// launchers of the register / occupancy variants (tuned by mhd_autotune)
+int launch_k_pv_uplus_dt(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c, unsigned long long *dt_key, int depth,
+                              int with_jcell)
+{
+    switch (variant)
+    {
+    case 0:
+        k_pv_uplus_dt_t<4><<<grid, 256, 0, st>>>(bvs, c, dt_key, depth, with_jcell);
+        break;
+    case 1:
+        k_pv_uplus_dt_t<1><<<grid, 256, 0, st>>>(bvs, c, dt_key, depth, with_jcell);
+        break;
+    case 2:
+        k_pv_uplus_dt_t<5><<<grid, 256, 0, st>>>(bvs, c, dt_key, depth, with_jcell);
+        break;
+    default:
+        return -1;
+    }
+    return 0;
+}
+
+int launch_k_fluid_ucontra(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c)
+{
+    switch (variant)
+    {
+    case 0:
+        k_fluid_ucontra_t<1><<<grid, 256, 0, st>>>(bvs, c);
+        break;
+    case 1:
+        k_fluid_ucontra_t<3><<<grid, 256, 0, st>>>(bvs, c);
+        break;
+    default:
+        return -1;
+    }
+    return 0;
+}
+
+int launch_k_bcell_jedge(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs)
+{
+    switch (variant)
+    {
+    case 0:
+        k_bcell_jedge_t<1><<<grid, 256, 0, st>>>(bvs);
+        break;
+    case 1:
+        k_bcell_jedge_t<6><<<grid, 256, 0, st>>>(bvs);
+        break;
+    default:
+        return -1;
+    }
+    return 0;
+}
+
+int launch_k_eface(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs)
+{
+    switch (variant)
+    {
+    case 0:
+        k_eface_t<1><<<grid, 256, 0, st>>>(bvs);
+        break;
+    case 1:
+        k_eface_t<6><<<grid, 256, 0, st>>>(bvs);
+        break;
+    default:
+        return -1;
+    }
+    return 0;
+}
+
+int launch_k_curl_e2f(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, int fE0, int fR0, int fB0, double mult,
+                           const double *dtp, double dtdiv, int mult_is_neg_dt, const int *rng)
+{
+    switch (variant)
+    {
+    case 0:
+        k_curl_e2f_t<1><<<grid, 256, 0, st>>>(bvs, fE0, fR0, fB0, mult, dtp, dtdiv, mult_is_neg_dt, rng);
+        break;
+    case 1:
+        k_curl_e2f_t<6><<<grid, 256, 0, st>>>(bvs, fE0, fR0, fB0, mult, dtp, dtdiv, mult_is_neg_dt, rng);
+        break;
+    default:
+        return -1;
+    }
+    return 0;
+}
+
+int launch_k_eedge(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs)
+{
+    switch (variant)
+    {
+    case 0:
+        k_eedge_t<1><<<grid, 256, 0, st>>>(bvs);
+        break;
+    case 1:
+        k_eedge_t<8><<<grid, 256, 0, st>>>(bvs);
+        break;
+    default:
+        return -1;
+    }
+    return 0;
 }
 
 } // namespace mhd

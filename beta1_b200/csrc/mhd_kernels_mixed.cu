@@ -86,9 +86,10 @@ __device__ __forceinline__ void rusanov_dev32(const BlockView &b, const Ref32 &r
 // Fluid RHS of the inner cells (FP32 flux divergence, FP64 J x B source) and
 // the FP64 contravariant velocities of the cells within one ghost layer; the
 // FP64 face metric read for the velocities is the one the fluxes round.
-// capped at 128 registers (2 CTAs per SM; uncapped it takes 168, one CTA):
-// 0.265 -> 0.171 ms on the C2 step
-__global__ void __launch_bounds__(256, 2) k_fluid_mixed(const BlockView *__restrict__ bvs, Consts c)
+// variants: at least 2 CTAs per SM (128 registers; the default: uncapped it
+// takes 168 registers and one CTA, 0.265 -> 0.171 ms on the C2 step),
+// uncapped, at least 3
+__device__ __forceinline__ void k_fluid_mixed_body(const BlockView *__restrict__ bvs, Consts c)
 {
     int64_t t;
     const BlockView &b = bvs[cta_block(bvs, KIND_CELL1, t)];
@@ -170,6 +171,32 @@ __global__ void __launch_bounds__(256, 2) k_fluid_mixed(const BlockView *__restr
     R[2 * v + p] = -(double(r[2]) + phi[2]) * invJ + fc * fy;
     R[3 * v + p] = -(double(r[3]) + phi[3]) * invJ + fc * fz;
     R[4 * v + p] = -(double(r[4]) + phi[4]) * invJ + fc * (fx * PV[p] + fy * PV[v + p] + fz * PV[2 * v + p]);
+}
+
+template <int MINB> __global__ void __launch_bounds__(256, MINB) k_fluid_mixed_t(const BlockView *__restrict__ bvs, Consts c)
+{
+    k_fluid_mixed_body(bvs, c);
+}
+
+
+// launchers of the register / occupancy variants (tuned by mhd_autotune)
+int launch_k_fluid_mixed(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c)
+{
+    switch (variant)
+    {
+    case 0:
+        k_fluid_mixed_t<2><<<grid, 256, 0, st>>>(bvs, c);
+        break;
+    case 1:
+        k_fluid_mixed_t<1><<<grid, 256, 0, st>>>(bvs, c);
+        break;
+    case 2:
+        k_fluid_mixed_t<3><<<grid, 256, 0, st>>>(bvs, c);
+        break;
+    default:
+        return -1;
+    }
+    return 0;
 }
 
 } // namespace mhd

@@ -49,6 +49,8 @@ _SIGS = {
     "mhd_run_time": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                C.POINTER(C.c_int64)]),
     "mhd_set_flux_reference_run": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
+    "mhd_autotune": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.c_int32]),
+    "mhd_tune_name": (C.c_char_p, [C.c_int32]),
     "mhd_ctx_destroy": (C.c_int, [C.c_void_p]),
     "mhd_last_error": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),
     "mhd_field_info": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
@@ -286,6 +288,15 @@ class Context:
             self._check(self.lib.mhd_set_flux_reference(self.h, a), "set_flux_reference")
         else:
             self._check(self.lib.mhd_set_flux_reference_run(self.h, int(run), a), "set_flux_reference_run")
+
+    def autotune(self, reps: int = 10) -> Dict[str, int]:
+        """times the register / occupancy variants of the hot kernels on the
+        current state and keeps the fastest; returns kernel -> chosen minimum
+        CTAs per SM"""
+        n = 7
+        out = (C.c_int32 * n)()
+        self._check(self.lib.mhd_autotune(self.h, int(reps), out, n), "autotune")
+        return {self.lib.mhd_tune_name(i).decode(): int(out[i]) for i in range(n)}
 
     def run_time(self, run: int):
         """(dt of the last step, time, step count) of one run"""

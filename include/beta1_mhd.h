@@ -243,6 +243,22 @@ int mhd_set_flux_reference(mhd_ctx *ctx, const double prim[5]);
 /* The same for one run of a batch (run -1: every run). */
 int mhd_set_flux_reference_run(mhd_ctx *ctx, int32_t run, const double prim[5]);
 
+/* Autotuner (no counterpart in the reference): the hot stencil kernels are
+   compiled in register / occupancy variants (the same code under different
+   minimum-CTAs-per-SM launch bounds, so every variant gives bit-identical
+   results).  mhd_autotune times whole steps (`reps` graph launches, after a
+   warm-up) with one kernel's variant changed at a time, the candidate and
+   the kept variant back to back and each the faster of two timings, and
+   keeps a candidate when the step gets at least 3 % faster; every trial
+   starts from a snapshot of the state taken
+   at entry, and the state and run clocks are restored at the end, so the
+   call does not advance the simulation.  Call it after the state is loaded.
+   min_ctas[i] (i < n, at most MHD_NTUNE) receives the chosen minimum CTAs
+   per SM of kernel mhd_tune_name(i). */
+#define MHD_NTUNE 7
+int mhd_autotune(mhd_ctx *ctx, int32_t reps, int32_t *min_ctas, int32_t n);
+const char *mhd_tune_name(int32_t i);
+
 /* Iterations, final residual norm, ||b|| and convergence reason (2 rtol,
    3 atol, -3 iteration limit, as KSPConvergedReason) of the last solve. */
 int mhd_resistive_stats(const mhd_ctx *ctx, int32_t *its, double *rnorm, double *bnorm, int32_t *reason);

@@ -1,0 +1,57 @@
+"""The autotuner (mhd_autotune): it picks one register / occupancy variant
+per hot kernel by timing them on the context's own state.  The variants are
+the same code under different launch bounds, so a tuned context must still
+reproduce the reference bit for bit: the 4-block slab (ideal MHD) and the
+implicit resistive slab against their reference fixtures after tuning."""
+import numpy as np
+import pytest
+
+from conftest import load_golden, rel_l2, slab_setup
+
+from beta1_b200 import mhd, solver
+
+pytestmark = pytest.mark.gpu
+
+STATE = ["U_H", "B_xi", "B_eta", "B_zeta"]
+DERIVED = ["PV_H", "U_plus", "B_cell", "J_cell", "E_xi", "E_eta", "E_zeta", "RHS_H"]
+
+
+@pytest.mark.parametrize("fname,tol", [("slab_6x5x6_t2x2_r00_steps.npz", 0.0), ("slab_6x5x6_t2x2_r11_steps.npz", 1e-10)])
+def test_tuned_context_matches_reference(fname, tol):
+    g = load_golden(fname)
+    spec, st = slab_setup(g)
+    s = solver.Solver(spec, topology="tiled")
+    s.load_state(st)
+    chosen = s.ctx.autotune(reps=3)
+    assert set(chosen) == {"k_pv_uplus_dt", "k_fluid_ucontra", "k_bcell_jedge", "k_eface", "k_curl_e2f", "k_eedge",
+                           "k_fluid_mixed"}
+    assert all(v >= 1 for v in chosen.values())
+    nb = len(spec.blocks)
+    for n in (1, 2):
+        s.step(1)
+        for b in range(nb):
+            for f in STATE + DERIVED:
+                ref = g["s%d/b%d/%s" % (n, b, f)]
+                got = s.field(f, b)
+                if tol == 0.0:
+                    assert np.array_equal(got, ref), (n, b, f)
+                else:
+                    assert rel_l2(got, ref) <= tol, (n, b, f)
+    s.ctx.close()
+
+
+def test_tuned_mixed_equals_default_mixed():
+    g = load_golden("slab_6x5x6_t2x2_r00_steps.npz")
+    spec, st = slab_setup(g)
+    a = solver.Solver(spec, topology="tiled", precision=mhd.PREC_MIXED)
+    a.load_state(st)
+    a.ctx.autotune(reps=3)
+    a.step(3)
+    b = solver.Solver(spec, topology="tiled", precision=mhd.PREC_MIXED)
+    b.load_state(st)
+    b.step(3)
+    for blk in range(len(spec.blocks)):
+        for f in STATE:
+            assert np.array_equal(a.field(f, blk), b.field(f, blk)), (blk, f)
+    a.ctx.close()
+    b.ctx.close()
