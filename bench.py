@@ -300,6 +300,7 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=None, help="StepOnce per reference CPU sample")
     ap.add_argument("--e2e-iters", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep every kernel's default variant")
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="fp64, or FP32 face fluxes with FP64 CT / state / residuals (default: fp64, mixed for c5)")
     args = ap.parse_args()
@@ -341,7 +342,7 @@ def main():
         nblocks = len(spec.blocks)
     ctx = s.ctx
     # register / occupancy variant of each hot kernel, timed on this state
-    tuned = ctx.autotune(reps=10)
+    tuned = ctx.autotune(reps=10) if not args.no_autotune else None
     stream = torch.cuda.ExternalStream(ctx.stream())
     ctx_bytes = sum(ctx.field_info(f, b)["ncomp"] * int(np.prod([h - l for l, h in zip(
         ctx.field_info(f, b)["lo"], ctx.field_info(f, b)["hi"])])) * 8 for f in ("U_H", "PV_H", "JDxi", "JDet",
