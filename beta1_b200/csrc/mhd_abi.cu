@@ -108,8 +108,10 @@ enum TuneId
 };
 const char *const kTuneNames[NTUNE] = {"k_pv_uplus_dt", "k_fluid_ucontra", "k_bcell_jedge", "k_eface",
                                        "k_curl_e2f",    "k_eedge",         "k_fluid_mixed"};
-// minimum CTAs per SM of each variant (variant 0 first)
-const int kTuneMinCtas[NTUNE][3] = {{4, 1, 5}, {1, 3, 0}, {1, 6, 0}, {1, 6, 0}, {1, 6, 0}, {1, 8, 0}, {2, 1, 3}};
+// minimum CTAs per SM of each variant (variant 0 first; 0: the compiler's
+// own allocation, no launch bounds) and the number of variants
+const int kTuneMinCtas[NTUNE][3] = {{4, 0, 5}, {0, 3, 0}, {0, 6, 0}, {0, 6, 0}, {0, 6, 0}, {0, 8, 0}, {2, 0, 3}};
+const int kTuneCount[NTUNE] = {3, 2, 2, 2, 2, 2, 3};
 
 struct mhd_ctx
 {
@@ -2618,7 +2620,7 @@ int mhd_autotune(mhd_ctx *ctx, int32_t reps, int32_t *min_ctas, int32_t n)
         if ((t == TUNE_k_fluid_mixed && !ctx->pool32) || (t == TUNE_k_fluid_ucontra && ctx->pool32))
             continue;
         int keep = ctx->tune[t];
-        for (int v = 0; v < 3 && kTuneMinCtas[t][v] > 0 && rc == MHD_OK; ++v)
+        for (int v = 0; v < kTuneCount[t] && rc == MHD_OK; ++v)
         {
             if (v == keep)
                 continue;

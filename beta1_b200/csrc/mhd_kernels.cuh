@@ -151,23 +151,24 @@ __global__ void k_negate(double *out, const double *x, int64_t n);
 
 
 // Hot stencil kernels in register / occupancy variants (the same code under
-// different __launch_bounds__ minimum CTAs per SM); variant 0 is the default.
-// Returns -1 for an unknown variant.
-// k_pv_uplus_dt: minimum CTAs per SM 4, 1, 5
+// different __launch_bounds__ minimum CTAs per SM; 0 = no launch bounds, the
+// compiler's own allocation); variant 0 is the default.  Returns -1 for an
+// unknown variant.
+// k_pv_uplus_dt: minimum CTAs per SM 4, 0, 5
 int launch_k_pv_uplus_dt(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c,
                          unsigned long long *dt_key, int depth, int with_jcell);
-// k_fluid_ucontra: minimum CTAs per SM 1, 3
+// k_fluid_ucontra: minimum CTAs per SM 0, 3
 int launch_k_fluid_ucontra(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c);
-// k_bcell_jedge: minimum CTAs per SM 1, 6
+// k_bcell_jedge: minimum CTAs per SM 0, 6
 int launch_k_bcell_jedge(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs);
-// k_eface: minimum CTAs per SM 1, 6
+// k_eface: minimum CTAs per SM 0, 6
 int launch_k_eface(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs);
-// k_curl_e2f: minimum CTAs per SM 1, 6
+// k_curl_e2f: minimum CTAs per SM 0, 6
 int launch_k_curl_e2f(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, int fE0, int fR0, int fB0,
                       double mult, const double *dtp, double dtdiv, int mult_is_neg_dt, const int *rng);
-// k_eedge: minimum CTAs per SM 1, 8
+// k_eedge: minimum CTAs per SM 0, 8
 int launch_k_eedge(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs);
-// k_fluid_mixed: minimum CTAs per SM 2, 1, 3
+// k_fluid_mixed: minimum CTAs per SM 2, 0, 3
 int launch_k_fluid_mixed(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c);
 
 } // namespace mhd

@@ -276,6 +276,11 @@ template <int MINB> __global__ void __launch_bounds__(256, MINB) k_fluid_ucontra
 {
     k_fluid_ucontra_body(bvs, c);
 }
+// the compiler's own register allocation (no launch bounds)
+__global__ void k_fluid_ucontra_free(const BlockView *__restrict__ bvs, Consts c)
+{
+    k_fluid_ucontra_body(bvs, c);
+}
 
 
 // contravariant velocity of a cell, as stored by the fluid pass
@@ -383,6 +388,11 @@ template <int MINB> __global__ void __launch_bounds__(256, MINB) k_eface_t(const
 {
     k_eface_body(bvs);
 }
+// the compiler's own register allocation (no launch bounds)
+__global__ void k_eface_free(const BlockView *__restrict__ bvs)
+{
+    k_eface_body(bvs);
+}
 
 
 // ---------------------------------------------------------------------------
@@ -466,6 +476,11 @@ template <int MINB> __global__ void __launch_bounds__(256, MINB) k_eedge_t(const
 {
     k_eedge_body(bvs);
 }
+// the compiler's own register allocation (no launch bounds)
+__global__ void k_eedge_free(const BlockView *__restrict__ bvs)
+{
+    k_eedge_body(bvs);
+}
 
 
 // ---------------------------------------------------------------------------
@@ -515,6 +530,12 @@ __device__ __forceinline__ void k_curl_e2f_body(const BlockView *__restrict__ bv
 }
 
 template <int MINB> __global__ void __launch_bounds__(256, MINB) k_curl_e2f_t(const BlockView *__restrict__ bvs, int fE0, int fR0, int fB0, double mult,
+                           const double *__restrict__ dtp, double dtdiv, int mult_is_neg_dt, const int *__restrict__ rng)
+{
+    k_curl_e2f_body(bvs, fE0, fR0, fB0, mult, dtp, dtdiv, mult_is_neg_dt, rng);
+}
+// the compiler's own register allocation (no launch bounds)
+__global__ void k_curl_e2f_free(const BlockView *__restrict__ bvs, int fE0, int fR0, int fB0, double mult,
                            const double *__restrict__ dtp, double dtdiv, int mult_is_neg_dt, const int *__restrict__ rng)
 {
     k_curl_e2f_body(bvs, fE0, fR0, fB0, mult, dtp, dtdiv, mult_is_neg_dt, rng);
@@ -849,6 +870,11 @@ template <int MINB> __global__ void __launch_bounds__(256, MINB) k_bcell_jedge_t
 {
     k_bcell_jedge_body(bvs);
 }
+// the compiler's own register allocation (no launch bounds)
+__global__ void k_bcell_jedge_free(const BlockView *__restrict__ bvs)
+{
+    k_bcell_jedge_body(bvs);
+}
 
 
 // ---------------------------------------------------------------------------
@@ -1059,6 +1085,12 @@ __device__ __forceinline__ void k_pv_uplus_dt_body(const BlockView *__restrict__
 }
 
 template <int MINB> __global__ void __launch_bounds__(256, MINB) k_pv_uplus_dt_t(const BlockView *__restrict__ bvs, Consts c, unsigned long long *dt_key, int depth,
+                              int with_jcell)
+{
+    k_pv_uplus_dt_body(bvs, c, dt_key, depth, with_jcell);
+}
+// the compiler's own register allocation (no launch bounds)
+__global__ void k_pv_uplus_dt_free(const BlockView *__restrict__ bvs, Consts c, unsigned long long *dt_key, int depth,
                               int with_jcell)
 {
     k_pv_uplus_dt_body(bvs, c, dt_key, depth, with_jcell);
@@ -1626,7 +1658,7 @@ int launch_k_pv_uplus_dt(int variant, dim3 grid, cudaStream_t st, const BlockVie
         k_pv_uplus_dt_t<4><<<grid, 256, 0, st>>>(bvs, c, dt_key, depth, with_jcell);
         break;
     case 1:
-        k_pv_uplus_dt_t<1><<<grid, 256, 0, st>>>(bvs, c, dt_key, depth, with_jcell);
+        k_pv_uplus_dt_free<<<grid, 256, 0, st>>>(bvs, c, dt_key, depth, with_jcell);
         break;
     case 2:
         k_pv_uplus_dt_t<5><<<grid, 256, 0, st>>>(bvs, c, dt_key, depth, with_jcell);
@@ -1642,7 +1674,7 @@ int launch_k_fluid_ucontra(int variant, dim3 grid, cudaStream_t st, const BlockV
     switch (variant)
     {
     case 0:
-        k_fluid_ucontra_t<1><<<grid, 256, 0, st>>>(bvs, c);
+        k_fluid_ucontra_free<<<grid, 256, 0, st>>>(bvs, c);
         break;
     case 1:
         k_fluid_ucontra_t<3><<<grid, 256, 0, st>>>(bvs, c);
@@ -1658,7 +1690,7 @@ int launch_k_bcell_jedge(int variant, dim3 grid, cudaStream_t st, const BlockVie
     switch (variant)
     {
     case 0:
-        k_bcell_jedge_t<1><<<grid, 256, 0, st>>>(bvs);
+        k_bcell_jedge_free<<<grid, 256, 0, st>>>(bvs);
         break;
     case 1:
         k_bcell_jedge_t<6><<<grid, 256, 0, st>>>(bvs);
@@ -1674,7 +1706,7 @@ int launch_k_eface(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs
     switch (variant)
     {
     case 0:
-        k_eface_t<1><<<grid, 256, 0, st>>>(bvs);
+        k_eface_free<<<grid, 256, 0, st>>>(bvs);
         break;
     case 1:
         k_eface_t<6><<<grid, 256, 0, st>>>(bvs);
@@ -1691,7 +1723,7 @@ int launch_k_curl_e2f(int variant, dim3 grid, cudaStream_t st, const BlockView *
     switch (variant)
     {
     case 0:
-        k_curl_e2f_t<1><<<grid, 256, 0, st>>>(bvs, fE0, fR0, fB0, mult, dtp, dtdiv, mult_is_neg_dt, rng);
+        k_curl_e2f_free<<<grid, 256, 0, st>>>(bvs, fE0, fR0, fB0, mult, dtp, dtdiv, mult_is_neg_dt, rng);
         break;
     case 1:
         k_curl_e2f_t<6><<<grid, 256, 0, st>>>(bvs, fE0, fR0, fB0, mult, dtp, dtdiv, mult_is_neg_dt, rng);
@@ -1707,7 +1739,7 @@ int launch_k_eedge(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs
     switch (variant)
     {
     case 0:
-        k_eedge_t<1><<<grid, 256, 0, st>>>(bvs);
+        k_eedge_free<<<grid, 256, 0, st>>>(bvs);
         break;
     case 1:
         k_eedge_t<8><<<grid, 256, 0, st>>>(bvs);

@@ -177,6 +177,11 @@ template <int MINB> __global__ void __launch_bounds__(256, MINB) k_fluid_mixed_t
 {
     k_fluid_mixed_body(bvs, c);
 }
+// the compiler's own register allocation (no launch bounds)
+__global__ void k_fluid_mixed_free(const BlockView *__restrict__ bvs, Consts c)
+{
+    k_fluid_mixed_body(bvs, c);
+}
 
 
 // launchers of the register / occupancy variants (tuned by mhd_autotune)
@@ -188,7 +193,7 @@ int launch_k_fluid_mixed(int variant, dim3 grid, cudaStream_t st, const BlockVie
         k_fluid_mixed_t<2><<<grid, 256, 0, st>>>(bvs, c);
         break;
     case 1:
-        k_fluid_mixed_t<1><<<grid, 256, 0, st>>>(bvs, c);
+        k_fluid_mixed_free<<<grid, 256, 0, st>>>(bvs, c);
         break;
     case 2:
         k_fluid_mixed_t<3><<<grid, 256, 0, st>>>(bvs, c);

@@ -254,7 +254,8 @@ int mhd_set_flux_reference_run(mhd_ctx *ctx, int32_t run, const double prim[5]);
    at entry, and the state and run clocks are restored at the end, so the
    call does not advance the simulation.  Call it after the state is loaded.
    min_ctas[i] (i < n, at most MHD_NTUNE) receives the chosen minimum CTAs
-   per SM of kernel mhd_tune_name(i). */
+   per SM of kernel mhd_tune_name(i) (0: no launch bounds, the compiler's own
+   register allocation). */
 #define MHD_NTUNE 7
 int mhd_autotune(mhd_ctx *ctx, int32_t reps, int32_t *min_ctas, int32_t n);
 const char *mhd_tune_name(int32_t i);
