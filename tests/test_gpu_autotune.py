@@ -25,7 +25,8 @@ def test_tuned_context_matches_reference(fname, tol):
     chosen = s.ctx.autotune(reps=3)
     assert set(chosen) == {"k_pv_uplus_dt", "k_fluid_ucontra", "k_bcell_jedge", "k_eface", "k_curl_e2f", "k_eedge",
                            "k_fluid_mixed"}
-    assert all(v >= 1 for v in chosen.values())
+    # minimum CTAs per SM of the chosen variant (0: no launch bounds)
+    assert all(v >= 0 for v in chosen.values())
     nb = len(spec.blocks)
     for n in (1, 2):
         s.step(1)
