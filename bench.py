@@ -11,6 +11,10 @@ Workloads (--workload):
   periodic across the tiles) because the reference's halo exchange cannot
   run a cubed-sphere layout.  FP64.
 * c1: the plain FP64 64^3 periodic curvilinear block (ideal MHD).
+* c3 / c4: Hall MHD: 6 blocks of 128 x 64 x 64 cells (3,145,728 cells) on
+  the C2 slab layout and inflow, ideal MHD plus the implicit Hall step
+  (Newton rtol 1e-10, GMRES to 1e-5 per Newton step) after the explicit
+  part of every step; FP64 (c3) or mixed precision (c4).
 * c5: a parameter sweep of 48 independent runs in one batch context, each
   one slab block of Nr x Nt x Nt cells (Nr in 32..128, Nt in 24..96),
   inflow speed 4..12 and IMF clock angle 0..180 degrees drawn from
@@ -70,6 +74,10 @@ ALGO_BYTES_PER_CELL = {
     # PV / U_plus / CFL with J_cell: U 5, Jac 1, B_cell 3, face area + normal 12, J 3, W_J 36 read;
     # PV 5, U_plus 3, Csound 1, RhoE 1, J_cell 3 written
     "k_pv_uplus_dt": 73 * 8,
+    # Hall EMF: B_cell 3, J_cell 3, rho 1 read; E_hall_cell 3, beta 1 written (per cell) / E_hall_cell 3,
+    # beta 1, B 3, face area 3, dl 3, dr 9 read; E_hall 3 written (per edge triple)
+    "k_hall_cell": 11 * 8,
+    "k_hall_edge": 25 * 8,
     # mixed form: FP32 face states rho, u, v, w, p, RhoE, c 7 and face area 3 read; FP64 JD 9, Jac 1,
     # U_plus 3, rho 1, u/v/w 3, B_cell 3, J_cell 3 read, RHS_H 5 and U_contra 3 written
     "k_fluid_mixed": 10 * 4 + 31 * 8,
@@ -132,8 +140,13 @@ WORKLOADS = {
     "c2": dict(name="c2_slab6x96x48x48_implicit_resistive_fp64", ref_steps=4, ref_rss_gb=12.0),
     "c1": dict(name="c1_periodic_64cubed_fp64", ref_steps=40, ref_rss_gb=1.0),
     "c5": dict(name="c5_sweep48_slab_runs_mixed", ref_steps=2, ref_rss_gb=4.0),
+    "c3": dict(name="c3_slab6x128x64x64_hall_implicit_fp64", ref_steps=1, ref_rss_gb=4.0),
+    "c4": dict(name="c4_slab6x128x64x64_hall_implicit_mixed", ref_steps=1, ref_rss_gb=4.0),
 }
 SWEEP_RUNS = 48
+HALL_SAMPLE = ("6 blocks of 64 x 32 x 32 cells (the same layout at half the cells per direction), StepOnce "
+               "followed by the reference's implicit Hall solve (SolveOneStep, Newton rtol 1e-10) and calc_Bcell")
+
 
 
 def workload_name(name, mixed):
@@ -148,6 +161,10 @@ def build_case(workload, n=64, size=(96, 48)):
     if workload == "c1":
         spec = case.periodic_box_case((n, n, n))
         return spec, case.initial_state(spec), "periodic", n ** 3
+    if workload in ("c3", "c4"):
+        spec = case.slab_case(128, (64, 64), (3, 2))
+        cells = sum(b.ncell[0] * b.ncell[1] * b.ncell[2] for b in spec.blocks)
+        return spec, case.inflow_state(spec), "tiled", cells
     sc = case.ref_scales()
     spec = case.slab_case(size[0], (size[1], size[1]), (3, 2), is_Lunar_resistance=1, use_implicit_lunar_resistance=1,
                           eta_max_lunar=1e-3 * case.MU0 * sc["U"] * sc["L_ref"], implicit_resistive_ksp_rtol=1e-10)
@@ -175,7 +192,15 @@ def cpu_reference(workload, n, steps, nproc):
     if not os.path.exists(REF_BIN):
         return None
     nproc = max(1, min(nproc, int(0.6 * mem_available_gb() / WORKLOADS[workload]["ref_rss_gb"])))
-    spec, st, _, _ = build_case(workload, n)
+    command = "time"
+    if workload in ("c3", "c4"):
+        # bounded sample: the same layout at half the cells per direction,
+        # the step with the implicit Hall solve
+        spec = case.slab_case(64, (32, 32), (3, 2))
+        st = case.inflow_state(spec)
+        command = "timehall"
+    else:
+        spec, st, _, _ = build_case(workload, n)
     d = tempfile.mkdtemp(prefix="b1ref_")
     try:
         case.write_case(d, spec)
@@ -187,7 +212,7 @@ def cpu_reference(workload, n, steps, nproc):
             for entry in os.listdir(d):
                 if entry not in ("init.rst",) and not entry.startswith("r"):
                     os.symlink(os.path.join(d, entry), os.path.join(wd, entry))
-            procs.append(subprocess.Popen([REF_BIN, "time", os.path.join(d, "init.rst"), str(steps)], cwd=wd,
+            procs.append(subprocess.Popen([REF_BIN, command, os.path.join(d, "init.rst"), str(steps)], cwd=wd,
                                           stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
         vals = []
         for pr in procs:
@@ -270,6 +295,9 @@ def run_reference_arm(args):
     if args.workload == "c5":
         sample = "%s: the first %d runs of the sweep, one single-threaded process each, %d StepOnce per " \
                  "process, concurrently (bounded by host cores and memory)" % (wl["name"], nproc, steps)
+    elif args.workload in ("c3", "c4"):
+        sample = "%s: %s; %d steps per process, %d concurrent single-threaded processes (bounded by host " \
+                 "cores and memory)" % (wl["name"], HALL_SAMPLE, steps, nproc)
     else:
         sample = "%s: %d StepOnce per process, %d concurrent single-threaded processes (bounded by host cores " \
                  "and memory)" % (wl["name"], steps, nproc)
@@ -307,9 +335,9 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     if args.steps is None:
-        args.steps = {"c2": 200, "c1": 4000, "c5": 100}[args.workload]
+        args.steps = {"c2": 200, "c1": 4000, "c5": 100, "c3": 10, "c4": 10}[args.workload]
     if args.precision is None:
-        args.precision = "mixed" if args.workload == "c5" else "fp64"
+        args.precision = "mixed" if args.workload in ("c5", "c4") else "fp64"
 
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -338,6 +366,9 @@ def main():
         c2size = tuple(int(v) for v in args.c2_size.split("x"))
         spec, st, topology, cells = build_case(args.workload, args.n, c2size)
         s = solver.Solver(spec, topology=topology, precision=prec)
+        if args.workload in ("c3", "c4"):
+            # bounded: at most 10 Newton steps of at most 200 GMRES iterations per time step
+            s.install_hall_implicit(topology, rtol=1e-10, atol=1e-50, maxit=10, ksp_rtol=1e-5, ksp_maxit=200)
         s.load_state(st)
         nblocks = len(spec.blocks)
     ctx = s.ctx
@@ -446,9 +477,10 @@ def main():
             res = cpu_reference(args.workload, args.n, ref_steps, 1)
             if res is not None:
                 agg, vals, _ = res
+                what = HALL_SAMPLE if args.workload in ("c3", "c4") else "StepOnce"
                 cpu = {"value": agg, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
-                       "sample": "%s, %d StepOnce of the reference solver built from its own sources, one "
-                                 "single-threaded process" % (wl["name"], ref_steps)}
+                       "sample": "%s, %d x %s of the reference solver built from its own sources, one "
+                                 "single-threaded process" % (wl["name"], ref_steps, what)}
 
     config_name = workload_name(wl["name"] if args.workload != "c2" or args.c2_size == "96x48" else
                                 "c2_slab6x%sx%s_implicit_resistive_fp64" % (args.c2_size, args.c2_size.split("x")[1]), mixed)

@@ -123,6 +123,20 @@ class Solver:
             else:
                 self.install_explicit_resistive()
 
+    def _edge_ids(self, rows, names):
+        """point ids of edge rows (block, axis 1..3, i, j, k) in the fields
+        names[axis]; one field lookup per (field, block), vectorised over rows"""
+        rows = np.asarray(rows, dtype=np.int64).reshape(-1, 5)
+        out = np.empty(len(rows), dtype=np.int64)
+        for d in np.unique(rows[:, 1]).tolist():
+            for b in np.unique(rows[rows[:, 1] == d, 0]).tolist():
+                sel = (rows[:, 1] == d) & (rows[:, 0] == b)
+                info = self.ctx.field_info(names[d], b)
+                r = rows[sel]
+                out[sel] = self.ctx.point_base(names[d], b) + syncmap.aos_index(info["lo"], info["hi"], 1, r[:, 2],
+                                                                                  r[:, 3], r[:, 4], 0)
+        return out
+
     def install_resistive(self, topology):
         """Unknowns, resistivity and edge aliases of the implicit resistive
         solve (LunarSolver::SetupImplicitResistiveDiffusion_)."""
@@ -135,11 +149,7 @@ class Solver:
         names = {1: "Eres_xi", 2: "Eres_eta", 3: "Eres_zeta"}
 
         def ids(rows):
-            out = np.empty(len(rows), dtype=np.int64)
-            for q, (b, d, i, j, k) in enumerate(rows.tolist()):
-                info = self.ctx.field_info(names[d], b)
-                out[q] = self.ctx.point_base(names[d], b) + syncmap.aos_index(info["lo"], info["hi"], 1, i, j, k, 0)
-            return out
+            return self._edge_ids(rows, names)
 
         p = spec.params
         self.ctx.set_resistive(ids(dofs), eta, ids(alias), ids(owner), np.ones(len(alias)),
@@ -167,11 +177,7 @@ class Solver:
         names = {1: "Ehall_xi", 2: "Ehall_eta", 3: "Ehall_zeta"}
 
         def ids(rows):
-            out = np.empty(len(rows), dtype=np.int64)
-            for q, (b, d, i, j, k) in enumerate(rows.tolist()):
-                info = self.ctx.field_info(names[d], b)
-                out[q] = self.ctx.point_base(names[d], b) + syncmap.aos_index(info["lo"], info["hi"], 1, i, j, k, 0)
-            return out
+            return self._edge_ids(rows, names)
 
         self.ctx.set_hall_implicit(ids(owners), ids(alias), ids(owner), np.ones(len(alias)), rtol, atol, maxit,
                                    ksp_rtol, ksp_maxit)

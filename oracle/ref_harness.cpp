@@ -530,6 +530,36 @@ int cmd_time(Harness &h, const std::string &state, int nsteps)
     return 0;
 }
 
+// StepOnce followed by the implicit Hall solve (SolveOneStep at the step's dt,
+// Newton rtol 1e-10) and calc_Bcell, `nsteps` times: the step with the Hall
+// solve that HALL_IMPLICIT enables, for timing
+int cmd_timehall(Harness &h, const std::string &state, int nsteps)
+{
+    h.load_state(state);
+    LunarSolver &s = *h.solver;
+    s.UpdateDerivedFields_();
+    SNESSetTolerances(s.hall_implicit_.snes_, 1e-50, 1e-10, 1e-30, 50, PETSC_DEFAULT);
+    int64_t cells = 0;
+    for (int ib = 0; ib < h.fld->num_blocks(); ++ib)
+    {
+        FieldBlock &U = h.fld->field(s.fid_.fid_U_H, ib);
+        const Int3 lo = U.inner_lo(), hi = U.inner_hi();
+        cells += int64_t(hi.i - lo.i) * (hi.j - lo.j) * (hi.k - lo.k);
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int n = 0; n < nsteps; ++n)
+    {
+        s.StepOnce();
+        s.hall_implicit_.SolveOneStep(s.dt, true);
+        s.calc_Bcell();
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    const double sec = std::chrono::duration<double>(t1 - t0).count();
+    std::printf("{\"cells\": %lld, \"steps\": %d, \"seconds\": %.9f, \"cell_updates_per_s\": %.6e}\n",
+                (long long)cells, nsteps, sec, double(cells) * nsteps / sec);
+    return 0;
+}
+
 } // namespace
 
 // On abort (e.g. a failed bounds assertion in a checked build) print the
@@ -577,6 +607,11 @@ int main(int argc, char **argv)
             rc = cmd_run(h, argv[2], std::atoi(argv[3]), argv[4]);
         else if (cmd == "probe" && argc >= 5)
             rc = cmd_probe(h, argv[2], argv[3], argv[4]);
+        else if (cmd == "timehall" && argc >= 4)
+        {
+            std::cout.rdbuf(sink.rdbuf());
+            rc = cmd_timehall(h, argv[2], std::atoi(argv[3]));
+        }
         else if (cmd == "time" && argc >= 4)
         {
             std::cout.rdbuf(saved);
