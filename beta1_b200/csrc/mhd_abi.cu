@@ -1437,7 +1437,7 @@ int create_ctx(const mhd_block_desc *blocks, int32_t nblocks, const int32_t *run
     {
         size_t n32 = 0;
         for (int b = 0; b < nblocks; ++b)
-            n32 += size_t(G32_N + Q32_N + W32_NB + W32_NJ) * size_t(ctx->hbv[size_t(b)].vol);
+            n32 += size_t(G32_N + Q32_N) * size_t(ctx->hbv[size_t(b)].vol);
         if (cudaMalloc(&ctx->pool32, n32 * sizeof(float)) != cudaSuccess)
             return bail(MHD_ENOMEM);
         if (cudaMemset(ctx->pool32, 0, n32 * sizeof(float)) != cudaSuccess)
@@ -1448,9 +1448,7 @@ int create_ctx(const mhd_block_desc *blocks, int32_t nblocks, const int32_t *run
             BlockView &v = ctx->hbv[size_t(b)];
             v.g32 = ctx->pool32 + o;
             v.q32 = v.g32 + size_t(G32_N) * size_t(v.vol);
-            v.wb32 = v.q32 + size_t(Q32_N) * size_t(v.vol);
-            v.wj32 = v.wb32 + size_t(W32_NB) * size_t(v.vol);
-            o += size_t(G32_N + Q32_N + W32_NB + W32_NJ) * size_t(v.vol);
+            o += size_t(G32_N + Q32_N) * size_t(v.vol);
         }
     }
     else if (params->precision != MHD_PREC_FP64)
@@ -1613,9 +1611,7 @@ static int transfer(mhd_ctx *ctx, const char *name, int32_t block, const double 
     const int nc = kFields[f].ncomp;
     if (hin)
     {
-        // geometry the derived copies are made from (face areas and normals;
-        // the FP32 planes of the mixed form)
-        if (f == F_JDxi || f == F_JDeta || f == F_JDzeta || f == F_WB || f == F_WJ)
+        if (f == F_JDxi || f == F_JDeta || f == F_JDzeta)
             ctx->geom_dirty = true;
         CK(ctx, cudaMemcpyAsync(ctx->staging, hin, size_t(n) * 8, cudaMemcpyHostToDevice, ctx->stream));
         prof_begin(ctx, "k_aos_to_soa");

@@ -773,10 +773,9 @@ __device__ __forceinline__ void bcell_one(const BlockView &b, int i, int j, int 
 #pragma unroll
     for (int q = 0; q < 6; ++q)
     {
-        // the mixed form reads FP32 copies of the weights (wb32 set)
-        const double wx = b.wb32 ? double(b.wb32[q * v + p]) : W[q * v + p];
-        const double wy = b.wb32 ? double(b.wb32[(6 + q) * v + p]) : W[(6 + q) * v + p];
-        const double wz = b.wb32 ? double(b.wb32[(12 + q) * v + p]) : W[(12 + q) * v + p];
+        const double wx = W[q * v + p];
+        const double wy = W[(6 + q) * v + p];
+        const double wz = W[(12 + q) * v + p];
         bxt += wx * phi_tot[q];
         byt += wy * phi_tot[q];
         bzt += wz * phi_tot[q];
@@ -895,11 +894,9 @@ __device__ __forceinline__ void jcell_one(const BlockView &b, int i, int j, int 
 #pragma unroll
     for (int q = 0; q < 12; ++q)
     {
-        // the mixed form reads FP32 copies of the weights (wj32 set)
-        const float *W32 = b.wj32;
-        jx += (W32 ? double(W32[q * v + p]) : W[q * v + p]) * s[q];
-        jy += (W32 ? double(W32[(12 + q) * v + p]) : W[(12 + q) * v + p]) * s[q];
-        jz += (W32 ? double(W32[(24 + q) * v + p]) : W[(24 + q) * v + p]) * s[q];
+        jx += W[q * v + p] * s[q];
+        jy += W[(12 + q) * v + p] * s[q];
+        jz += W[(24 + q) * v + p] * s[q];
     }
     double *Jc = b.f[F_Jcell];
     Jc[p] = jx;

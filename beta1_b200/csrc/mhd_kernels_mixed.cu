@@ -12,9 +12,7 @@
 // conserved update, the contravariant velocities of the CT EMF, the EMF
 // itself, its curl and the face-B update stay FP64 (the contravariant
 // velocities here, the rest in other translation units), so div B stays at
-// FP64 round-off.  The derived-field pass (B_cell, J_cell) reads FP32 copies
-// of its least-squares weights and accumulates in FP64.  Compiled with
-// contracted multiply-adds.
+// FP64 round-off.  Compiled with contracted multiply-adds.
 #include "mhd_kernels.cuh"
 
 namespace mhd
@@ -22,9 +20,7 @@ namespace mhd
 
 __device__ __forceinline__ float fmaxs(float a, float b) { return (a < b) ? b : a; }
 
-// FP32 copies of the face areas |JD| and of the B_cell / J_cell
-// least-squares weights on every point of the padded box (the derived-field
-// pass reads the weights in FP32 and accumulates in FP64)
+// FP32 copy of the face areas |JD| on every point of the padded box
 __global__ void k_geom32(const BlockView *__restrict__ bvs)
 {
     const BlockView &b = bvs[blockIdx.y];
@@ -35,11 +31,6 @@ __global__ void k_geom32(const BlockView *__restrict__ bvs)
 #pragma unroll
     for (int a = 0; a < 3; ++a)
         b.g32[(G32_AREA + a) * v + p] = float(b.f[F_NAxi + a][p]);
-    // the B_cell / J_cell least-squares weights
-    for (int q = 0; q < W32_NB; ++q)
-        b.wb32[q * v + p] = float(b.f[F_WB][q * v + p]);
-    for (int q = 0; q < W32_NJ; ++q)
-        b.wj32[q * v + p] = float(b.f[F_WJ][q * v + p]);
 }
 
 // reference-state constants of the deviation flux, FP32

@@ -128,8 +128,6 @@ struct BlockView
     // mixed precision only (null otherwise): FP32 planes on the same padded box
     float *g32;       // face area xi, eta, zeta
     float *q32;       // face-state quantities rho, u, v, w, p, rhoE, c
-    float *wb32;      // least-squares weights of B_cell (18) and J_cell (36)
-    float *wj32;
     // run (independent time line) the block belongs to, and that run's
     // reference state of the mixed-precision flux (rho, u, v, w, p, E)
     int run;
@@ -178,9 +176,7 @@ enum : int
     Q32_P = 4,
     Q32_RHOE = 5,
     Q32_C = 6,
-    Q32_N = 7,
-    W32_NB = 18,
-    W32_NJ = 36
+    Q32_N = 7
 };
 
 __host__ __device__ inline int64_t pidx(const BlockView &b, int i, int j, int k)
