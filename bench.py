@@ -151,6 +151,23 @@ HALL_SAMPLE = ("6 blocks of 64 x 32 x 32 cells (the same layout at half the cell
 
 
 
+def max_over_ranks(ms: float, device) -> float:
+    """The largest of every rank's time (the job's time), all-reduced over
+    the process group when there is one (NCCL on the GPUs, gloo in tests)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world: int, cells: int, steps: int, ms_max: float) -> float:
+    """Whole-job cell-updates/s of `world` replicas that each advanced
+    `cells` cells `steps` times, over the slowest rank's time."""
+    return world * cells * steps / (ms_max / 1000.0)
+
+
 def workload_name(name, mixed):
     base = name.rsplit("_", 1)[0]
     return base + ("_mixed" if mixed else "_fp64")
@@ -416,11 +433,8 @@ def main():
                      "reason": rs["reason"], "unknowns": int(len(s.resistive_dofs[0])), "rtol": float(spec.params["implicit_resistive_ksp_rtol"])}
     stop.set()
     th.join()
-    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = world * cells * args.steps / (ms_max / 1000.0)
+    ms_max = max_over_ranks(ms, "cuda")
+    value = replica_throughput(world, cells, args.steps, ms_max)
 
     # per-kernel durations: eager steps with an event pair around every launch
     prof = {}
@@ -461,10 +475,7 @@ def main():
     f1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = f0.elapsed_time(f1) / args.e2e_iters
-    e2e_t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = world * cells / (float(e2e_t.item()) / 1000.0)
+    e2e_value = replica_throughput(world, cells, 1, max_over_ranks(e2e_ms, "cuda"))
     hin.free()
     hout.free()
 
