@@ -2706,6 +2706,22 @@ int mhd_step(mhd_ctx *ctx, int32_t nsteps, double *dt_out, double *time_out)
     return MHD_OK;
 }
 
+int mhd_batch_step(mhd_ctx *ctx, int32_t nsteps, double *dt_out, double *time_out, int32_t nruns)
+{
+    if (!ctx || nsteps < 0 || (nruns > 0 && (!dt_out && !time_out)))
+        return fail(ctx, MHD_EINVAL, "bad batch step arguments");
+    if (nruns != 0 && nruns != ctx->nruns)
+        return fail(ctx, MHD_EINVAL, "the context holds %d runs, not %d", ctx->nruns, nruns);
+    RUN(run_steps(ctx, nsteps));
+    RUN(check_err(ctx));
+    const size_t nr = size_t(nruns);
+    if (dt_out && nr)
+        CK(ctx, cudaMemcpy(dt_out, ctx->dt, 8 * nr, cudaMemcpyDeviceToHost));
+    if (time_out && nr)
+        CK(ctx, cudaMemcpy(time_out, ctx->time, 8 * nr, cudaMemcpyDeviceToHost));
+    return MHD_OK;
+}
+
 int64_t mhd_state_count(const mhd_ctx *ctx)
 {
     if (!ctx)

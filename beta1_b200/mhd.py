@@ -48,6 +48,7 @@ _SIGS = {
                                    C.POINTER(C.c_void_p)]),
     "mhd_run_time": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                C.POINTER(C.c_int64)]),
+    "mhd_batch_step": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int32]),
     "mhd_set_flux_reference_run": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
     "mhd_autotune": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.c_int32]),
     "mhd_tune_name": (C.c_char_p, [C.c_int32]),
@@ -297,6 +298,13 @@ class Context:
         out = (C.c_int32 * n)()
         self._check(self.lib.mhd_autotune(self.h, int(reps), out, n), "autotune")
         return {self.lib.mhd_tune_name(i).decode(): int(out[i]) for i in range(n)}
+
+    def batch_step(self, nsteps: int):
+        """nsteps steps of every run; returns (dt of every run, time of every run)"""
+        dt = (C.c_double * self.nruns)()
+        t = (C.c_double * self.nruns)()
+        self._check(self.lib.mhd_batch_step(self.h, int(nsteps), dt, t, self.nruns), "batch_step")
+        return list(dt), list(t)
 
     def run_time(self, run: int):
         """(dt of the last step, time, step count) of one run"""

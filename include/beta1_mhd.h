@@ -96,6 +96,11 @@ int mhd_batch_create(const mhd_block_desc *blocks, int32_t nblocks, const int32_
 /* dt of the last step, simulated time and step count of one run. */
 int mhd_run_time(mhd_ctx *ctx, int32_t run, double *dt, double *time, int64_t *step);
 
+/* nsteps steps of every run of a batch (each run its own dt), then every
+   run's last dt and time into dt_out[nruns] and time_out[nruns] (either may
+   be null; nruns must be the batch's run count, or 0 for no read-back). */
+int mhd_batch_step(mhd_ctx *ctx, int32_t nsteps, double *dt_out, double *time_out, int32_t nruns);
+
 /* ~LunarSolver / delete fld (Z4_Lunar/main.cpp:216-222). */
 int mhd_ctx_destroy(mhd_ctx *ctx);
 

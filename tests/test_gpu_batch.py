@@ -103,6 +103,17 @@ def test_batch_dt_per_run(cases, batch_run):
     assert len({dts[1][r][0] for r in range(len(cases))}) > 1
 
 
+def test_batch_step_reports_every_run(cases):
+    bt = solver.Batch([(c[2], c[3]) for c in cases])
+    bt.load_states([c[4] for c in cases])
+    dts, times = bt.ctx.batch_step(2)
+    for r, (kind, g, spec, topo, st) in enumerate(cases):
+        assert dts[r] == float(g["s2/dt"]), (r, dts[r])
+        assert times[r] == float(g["s1/dt"]) + float(g["s2/dt"]), (r, times[r])
+        assert bt.ctx.run_time(r)[:2] == (dts[r], times[r])
+    bt.ctx.close()
+
+
 def test_mixed_batch_equals_runs_alone(cases):
     bt = solver.Batch([(c[2], c[3]) for c in cases], precision=mhd.PREC_MIXED)
     bt.load_states([c[4] for c in cases])
