@@ -2552,9 +2552,14 @@ int mhd_autotune(mhd_ctx *ctx, int32_t reps, int32_t *min_ctas, int32_t n)
         return fail(ctx, MHD_ESTATE, "autotune during capture");
     RUN(ensure_geom(ctx));
     cudaStream_t s = ctx->stream;
-    // snapshot of the state (U_H and the face B of every block) and of the
-    // run clocks (dt keys, dt, time, step: one contiguous allocation)
-    const int sf[4] = {F_U, F_Bxi, F_Beta, F_Bzeta};
+    // snapshot of the state (U_H and the face B of every block; with the
+    // implicit Hall solve also its edge EMF, which starts the next Newton
+    // solve) and of the run clocks (dt keys, dt, time, step: one contiguous
+    // allocation)
+    std::vector<int> sf = {F_U, F_Bxi, F_Beta, F_Bzeta};
+    if (ctx->hall.on)
+        for (int a = 0; a < 3; ++a)
+            sf.push_back(F_Ehxi + a);
     size_t tot = 0;
     for (int f : sf)
         for (int b = 0; b < ctx->nblocks; ++b)

@@ -56,3 +56,24 @@ def test_tuned_mixed_equals_default_mixed():
             assert np.array_equal(a.field(f, blk), b.field(f, blk)), (blk, f)
     a.ctx.close()
     b.ctx.close()
+
+
+def test_tuning_leaves_the_implicit_hall_start_untouched():
+    # the implicit Hall solve starts Newton from the edge EMF of the last
+    # step; tuning must restore it, so a tuned and an untuned context take
+    # bit-identical steps
+    g = load_golden("slab_6x5x6_t2x2_r00_steps.npz")
+    spec, st = slab_setup(g)
+    out = []
+    for tune in (True, False):
+        s = solver.Solver(spec, topology="tiled")
+        s.install_hall_implicit("tiled", rtol=1e-10)
+        s.load_state(st)
+        s.step(1)
+        if tune:
+            s.ctx.autotune(reps=2)
+        s.step(1)
+        out.append({(f, b): s.field(f, b) for f in ("B_xi", "B_eta", "B_zeta", "Ehall_xi") for b in range(4)})
+        s.ctx.close()
+    for key in out[0]:
+        assert np.array_equal(out[0][key], out[1][key]), key
