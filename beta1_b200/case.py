@@ -582,6 +582,43 @@ def slab_interfaces(nr: int, nt: Tuple[int, int], tiles: Tuple[int, int]) -> Lis
     return inner
 
 
+def shell_blocks(nr: int, nth: int, nph: int, r0: float = 1.0, r1: float = 8.0) -> List[BlockGrid]:
+    """One spherical-shell block: nr log-spaced radial cells over [r0, r1]
+    (index i), nth polar cells over theta in [0, pi] (index j) and nph
+    azimuthal cells over phi in [0, 2 pi) (index k, nph even), with
+    x = r sin(theta) cos(phi), y = r sin(theta) sin(phi), z = r cos(theta).
+    Physical patches: Solid_Surface at i = 0, Farfield at i = nr, Pole at
+    j = 0 and j = nth (the node rows on the z axis)."""
+    if nph % 2:
+        raise ValueError("a Pole patch needs an even number of azimuthal cells")
+    r = r0 * (r1 / r0) ** (np.arange(nr + 1) / nr)
+    th = np.pi * np.arange(nth + 1) / nth
+    ph = 2.0 * np.pi * np.arange(nph + 1) / nph
+    R, T, P = np.meshgrid(r, th, ph, indexing="ij")
+    x = R * np.sin(T) * np.cos(P)
+    y = R * np.sin(T) * np.sin(P)
+    z = R * np.cos(T)
+    # the pole rows lie exactly on the axis
+    x[:, 0, :] = 0.0
+    y[:, 0, :] = 0.0
+    x[:, nth, :] = 0.0
+    y[:, nth, :] = 0.0
+    blk = BlockGrid("Fluid", x, y, z)
+    blk.physical = [((0, 0, 0, nth, 0, nph), "Solid_Surface"), ((nr, nr, 0, nth, 0, nph), "Farfield"),
+                    ((0, nr, 0, 0, 0, nph), "Pole"), ((0, nr, nth, nth, 0, nph), "Pole")]
+    return [blk]
+
+
+def shell_case(nr=16, nth=8, nph=12, **over) -> CaseSpec:
+    """The single-block spherical shell with Pole patches and its azimuthal
+    direction periodic onto itself (inflow parameters as the slab's)."""
+    I, J, K = nr + 1, nth + 1, nph + 1
+    kmin = (1, I, -1, -J, 1, 1)
+    kmax = (1, I, -1, -J, K, K)
+    inner = [[InnerFace(kmin, -1, kmax, -1), InnerFace(kmax, -1, kmin, -1)]]
+    return CaseSpec(shell_blocks(nr, nth, nph), inner, inflow_params(**over))
+
+
 def slab_case(nr=96, nt=(48, 48), tiles=(3, 2), **over) -> CaseSpec:
     blocks = slab_blocks(nr, nt, tiles)
     spec = CaseSpec(blocks, slab_interfaces(nr, nt, tiles), inflow_params(**over))

@@ -91,6 +91,41 @@ def ghost_mesh(x: np.ndarray, y: np.ndarray, z: np.ndarray, ngg: int) -> Padded:
     return Padded(P, o)
 
 
+def pole_ghosts(X: Padded, ncell: Tuple[int, int, int], patches) -> Padded:
+    """Grid::MeshTrans_Inner_Pole (src/1_grid/1_MPCNS_Grid_GCL.cpp:564-616):
+    beyond a Pole patch (normal xi or eta, rotation direction zeta), the
+    ngg+1 ghost node layers over the patch's own tangential range repeat the
+    patch's node row, so the ghost cells past the axis collapse.  patches:
+    ((imin, imax, jmin, jmax, kmin, kmax), name) node ranges (0-based) of the
+    block's physical patches; only "Pole" ones are applied, after the
+    reflected ghost mesh and the interface copies."""
+    P = X.a
+    o = X.off
+    G = o
+    for rng, name in patches:
+        if name != "Pole":
+            continue
+        sub = [min(abs(rng[2 * a]), abs(rng[2 * a + 1])) for a in range(3)]
+        sup = [max(abs(rng[2 * a]), abs(rng[2 * a + 1])) for a in range(3)]
+        cyc = [0, 0, 0]
+        for a in range(3):
+            if sub[a] == sup[a]:
+                cyc[a] = -1 if sub[a] == 0 else 1
+        if cyc[2] != 0 or sub[2] != 0 or sup[2] != ncell[2] or ncell[2] % 2:
+            raise ValueError("a Pole patch needs zeta as its rotation direction, unsplit, with an even cell count")
+        for index in range(1, G + 1):
+            dst = tuple(slice(sub[a] + index * cyc[a] + o, sup[a] + index * cyc[a] + o + 1) for a in range(3))
+            src = tuple(slice(sub[a] + o, sup[a] + o + 1) for a in range(3))
+            P[dst] = P[src]
+    return X
+
+
+def block_ghost_mesh(b, ngg: int) -> Padded:
+    """Ghost node mesh of a case block (BlockGrid): reflection, then the Pole
+    collapse of its Pole patches."""
+    return pole_ghosts(ghost_mesh(b.x, b.y, b.z, ngg), b.ncell, b.physical)
+
+
 # ----------------------------------------------------------------------------
 # helpers with the reference's operation order
 # ----------------------------------------------------------------------------

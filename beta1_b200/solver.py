@@ -79,7 +79,7 @@ class Solver:
         if cache is None or cache["spec"] is not spec:
             cache = {"spec": spec, "geom": [], "nodes": []}
             for b in spec.blocks:
-                X = geometry.ghost_mesh(b.x, b.y, b.z, ngg)
+                X = geometry.block_ghost_mesh(b, ngg)
                 cache["nodes"].append(X)
                 cache["geom"].append(geometry.build(X, b.ncell, ngg))
             _HOST_CACHE.clear()
@@ -238,7 +238,7 @@ def host_setup(spec: case_mod.CaseSpec, topology: Optional[str] = None):
     ngg = int(spec.params["ngg"])
     nodes, geom = [], []
     for b in spec.blocks:
-        X = geometry.ghost_mesh(b.x, b.y, b.z, ngg)
+        X = geometry.block_ghost_mesh(b, ngg)
         nodes.append(X)
         geom.append(geometry.build(X, b.ncell, ngg))
     return nodes, geom, (run_tables(spec, topology, nodes) if topology else None)

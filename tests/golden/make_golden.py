@@ -157,6 +157,19 @@ def slab_long(nr=16, nt=(8, 8), tiles=(2, 2), steps=100, resistive=0, implicit=0
     print("wrote", tag)
 
 
+def shell_geom(nr=8, nth=6, nph=8):
+    """The reference's geometry of a single-block spherical shell with Pole
+    patches at both ends of the polar index (and its ghost node mesh)."""
+    tag = "shell_%dx%dx%d" % (nr, nth, nph)
+    with tempfile.TemporaryDirectory() as d:
+        spec = case.shell_case(nr, nth, nph)
+        case.write_case(d, spec)
+        run(["geom", "geom.bin"], d)
+        g = rst.read(os.path.join(d, "geom.bin"))
+        np.savez_compressed(os.path.join(OUT, tag + "_geom.npz"), **flatten(g, list(g.fields)))
+    print("wrote", tag)
+
+
 def hall(spec_kind, seed=20261205):
     """The reference's Hall edge EMF (BuildHallFaceEMF_Rusanov_diff_) of a
     seeded state: a periodic box (no walls) and a slab whose Solid_Surface
@@ -289,6 +302,7 @@ if __name__ == "__main__":
          * case.ref_scales()["L_ref"], n_resistive_subcycles=2)
     # one block periodic onto itself across the transverse directions
     slab(steps=2, tiles=(1, 1))
+    shell_geom()
     slab_probe(resistive=0)
     slab_probe(resistive=1)
     hall("periodic")

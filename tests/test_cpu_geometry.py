@@ -31,3 +31,21 @@ def test_geometry_fields_bitwise(golden_periodic):
         assert tuple(lo) == tuple(int(v) for v in geom[name + "__lo"]), name
         assert a.shape == geom[name].shape, name
         assert np.array_equal(a, geom[name]), (name, np.abs(a - geom[name]).max())
+
+
+def test_pole_shell_geometry_bitwise():
+    """A single-block spherical shell with Pole patches at both ends of the
+    polar index: the ghost node rows past each pole collapse onto the pole
+    row (Grid::MeshTrans_Inner_Pole), and every geometry field, degenerate
+    cells included, equals the reference's."""
+    from conftest import load_golden
+    geom = load_golden("shell_8x6x8_geom.npz")
+    b = case.shell_case(8, 6, 8).blocks[0]
+    X = geometry.block_ghost_mesh(b, 4)
+    assert np.array_equal(X.a, geom["X_node"])
+    with np.errstate(all="ignore"):
+        g = geometry.build(X, b.ncell, 4)
+    for name in FIELDS:
+        lo, hi, a = g[name]
+        assert tuple(lo) == tuple(int(v) for v in geom[name + "__lo"]), name
+        assert np.array_equal(a, geom[name]), (name, np.abs(a - geom[name]).max())
