@@ -170,6 +170,31 @@ def shell_geom(nr=8, nth=6, nph=8):
     print("wrote", tag)
 
 
+def shell_steps(nr=8, nth=6, nph=8, steps=2, seed=20261207):
+    """The reference's fields after 0..steps StepOnce on the Pole shell (the
+    target of a device Pole path; the initial state is regenerated from
+    (case, seed) and kept here too)."""
+    tag = "shell_%dx%dx%d" % (nr, nth, nph)
+    with tempfile.TemporaryDirectory() as d:
+        spec = case.shell_case(nr, nth, nph)
+        case.write_case(d, spec)
+        st = case.inflow_state(spec, seed=seed)
+        rst.write(os.path.join(d, "init.rst"), st)
+        run(["run", "init.rst", str(steps), "step"], d)
+        arr = {}
+        for k, v in flatten(st, ["U_H", "B_xi", "B_eta", "B_zeta"], 0).items():
+            arr["init/b0/%s" % k] = v
+        for s_ in range(steps + 1):
+            r = rst.read(os.path.join(d, "step_%04d.bin" % s_))
+            for k, v in flatten(r, STEP_FIELDS, 0).items():
+                arr["s%d/b0/%s" % (s_, k)] = v
+            arr["s%d/dt" % s_] = r.fields["dt"].blocks[0].data.reshape(())
+        arr["n"] = np.array([nr, nth, nph])
+        arr["seed"] = np.array(seed)
+        np.savez_compressed(os.path.join(OUT, tag + "_steps.npz"), **arr)
+    print("wrote", tag, "steps")
+
+
 def hall(spec_kind, seed=20261205):
     """The reference's Hall edge EMF (BuildHallFaceEMF_Rusanov_diff_) of a
     seeded state: a periodic box (no walls) and a slab whose Solid_Surface
@@ -303,6 +328,7 @@ if __name__ == "__main__":
     # one block periodic onto itself across the transverse directions
     slab(steps=2, tiles=(1, 1))
     shell_geom()
+    shell_steps()
     slab_probe(resistive=0)
     slab_probe(resistive=1)
     hall("periodic")

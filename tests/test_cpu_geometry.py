@@ -49,3 +49,16 @@ def test_pole_shell_geometry_bitwise():
         lo, hi, a = g[name]
         assert tuple(lo) == tuple(int(v) for v in geom[name + "__lo"]), name
         assert np.array_equal(a, geom[name]), (name, np.abs(a - geom[name]).max())
+
+
+def test_pole_shell_fixture_starts_from_the_seeded_state():
+    """The Pole shell's step fixture (the reference's StepOnce on Pole
+    patches) starts from the state regenerated from (case, seed)."""
+    from conftest import load_golden
+    g = load_golden("shell_8x6x8_steps.npz")
+    n = tuple(int(v) for v in g["n"])
+    spec = case.shell_case(*n)
+    st = case.inflow_state(spec, seed=int(g["seed"]))
+    for name in ("U_H", "B_xi", "B_eta", "B_zeta"):
+        assert np.array_equal(st.fields[name].blocks[0].data, g["init/b0/" + name]), name
+    assert float(g["s1/dt"]) > 0.0 and np.isfinite(g["s2/b0/U_H"]).all()
