@@ -62,3 +62,26 @@ def test_pole_shell_fixture_starts_from_the_seeded_state():
     for name in ("U_H", "B_xi", "B_eta", "B_zeta"):
         assert np.array_equal(st.fields[name].blocks[0].data, g["init/b0/" + name]), name
     assert float(g["s1/dt"]) > 0.0 and np.isfinite(g["s2/b0/U_H"]).all()
+
+
+def test_block_ghost_mesh_without_poles_is_the_reflected_mesh():
+    b = case.slab_case(6, (5, 6), (2, 2)).blocks[0]
+    assert np.array_equal(geometry.block_ghost_mesh(b, 4).a, geometry.ghost_mesh(b.x, b.y, b.z, 4).a)
+
+
+def test_pole_patch_rules():
+    import pytest
+    # the reference requires zeta as the rotation direction and an even,
+    # unsplit azimuthal cell count (Grid::MeshTrans_Inner_Pole)
+    with pytest.raises(ValueError):
+        case.shell_case(4, 4, 5)
+    b = case.shell_case(4, 4, 6).blocks[0]
+    X = geometry.ghost_mesh(b.x, b.y, b.z, 4)
+    with pytest.raises(ValueError):
+        geometry.pole_ghosts(X, b.ncell, [((0, 4, 0, 4, 0, 0), "Pole")])
+    Y = geometry.block_ghost_mesh(b, 4)
+    o = Y.off
+    # every ghost row past the low pole repeats the pole row over the inner i, k range
+    for g in range(1, o + 1):
+        assert np.array_equal(Y.a[o:o + 5, o - g, o:o + 7], Y.a[o:o + 5, o, o:o + 7])
+        assert np.array_equal(Y.a[o:o + 5, o + 4 + g, o:o + 7], Y.a[o:o + 5, o + 4, o:o + 7])
