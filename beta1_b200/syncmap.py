@@ -327,3 +327,129 @@ def compile_tiled(ctx, layout: TiledLayout, resistive: bool, farfield_consts, no
                           cval=np.concatenate(cval) if cval else np.zeros(0),
                           walls=sorted(set(walls)))
     return out
+
+
+# ---------------------------------------------------------------------------
+# The single-block spherical shell: Solid_Surface / Farfield in i, Pole at
+# both ends of j, k periodic onto itself
+# ---------------------------------------------------------------------------
+#
+# A Sync(group) there is (Z4_Lunar/src/boundary/Boundary_Sync_.cpp:4-65):
+#   the physical handlers of the i walls (as on the slab) and of the Poles
+#   (the default copy of the ghost slab from the first inner layer,
+#   src/6_boundary/Boundary.cpp:303-332, unless a field overrides it),
+#   the corner default where a wall meets a Pole: every ghost point of the
+#   corner takes the value of the nearest inner point
+#   (BoundaryCore::ApplyPhysicalCornerDefault, src/6_boundary/Boundary.cpp:178-260),
+#   then the periodic halo in k.
+# Fields whose Pole handler computes values (U_H's ring average, the B_cell
+# and face-B collapses, the edge EMF and J edge regulation) are not compiled
+# here: their groups are listed in SHELL_POLE_HANDLED.
+
+SHELL_POLE_HANDLED = ("Ucell", "Bface", "Eedge", "B_cell", "Jedge", "Eres", "Eres1form")
+
+
+def shell_pole_rule(field: str) -> str:
+    """What the Pole handler of the shipped Lunar set-up does to a field
+    (Z4_Lunar/src/boundary/Boundary_Build.cpp:27-40 and the overrides after)."""
+    if field == "U_plus":
+        return "nop"
+    if field in ("U_H", "B_cell", "Bind_cell", "B_xi", "B_eta", "E_xi", "E_eta", "E_zeta", "Eres_xi", "Eres_eta",
+                 "Eres_zeta", "J_xi", "J_eta", "J_zeta"):
+        return "handler"
+    return "copy"
+
+
+# groups whose Sync runs the halo exchange only (no physical handlers, no
+# corner default): Sync("Uplus") after calc_Uplus
+SHELL_HALO_ONLY = ("Uplus",)
+
+
+def compile_shell(ctx, ncell, resistive: bool):
+    """Tables of every Sync group of the shell whose Pole handling is a copy
+    (or nothing); groups in SHELL_POLE_HANDLED are left out.  ctx: a context
+    or HostLayout of the one block.
+
+    The Sync is replayed in the reference's order on a map that holds, per
+    point, either the pre-sync value of some point or a constant: the Pole
+    patches (j min, j max), the Farfield, the Solid_Surface (the topology's
+    patch order), the corner default, then the periodic halo in k.  Unlike
+    the tiled layout, a copy here can read a point before a later handler
+    sets it to a constant (the Pole ghost copy at i = 0 reads the wall slab
+    before the wall handler zeroes it), so the gather entries deliver
+    PRE-sync values: apply the gather before the fixed values.
+    Returns {group: dict(dst, src, cdst, cval, walls)}."""
+    n = tuple(ncell)
+    out = {}
+    for group, fields in GROUPS.items():
+        if group in SHELL_POLE_HANDLED:
+            continue
+        physical = group not in SHELL_HALO_ONLY
+        dsts, srcs, cdst, cval = [], [], [], []
+        for f in fields:
+            if shell_pole_rule(f) == "handler":
+                raise ValueError(f"field {f} has a computing Pole handler")
+            info = ctx.field_info(f, 0)
+            loc, nc = info["loc"], info["ncomp"]
+            lo, hi = info["lo"], info["hi"]
+            pl = PLUS[loc]
+            ih = (n[0] + pl[0], n[1] + pl[1], n[2] + pl[2])
+            shape = (hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2])
+            npt = shape[0] * shape[1] * shape[2]
+            I, J, K = _field_points(info)
+
+            def off(i, j, k):
+                return ((i - lo[0]) * shape[1] + (j - lo[1])) * shape[2] + (k - lo[2])
+
+            src = np.arange(npt)           # pre-sync point whose value a point holds
+            isc = np.zeros(npt, dtype=bool)  # ... or a constant (zero here)
+
+            def copy(sel, i, j, k):
+                idx = np.nonzero(sel)[0]
+                o = off(i(idx), j(idx), k(idx))
+                src[idx] = src[o]
+                isc[idx] = isc[o]
+
+            def zero(sel):
+                isc[np.nonzero(sel)[0]] = True
+
+            if physical:
+                pin = (I >= 0) & (I < ih[0]) & (K >= 0) & (K < ih[2])
+                tin = (J >= 0) & (J < ih[1]) & (K >= 0) & (K < ih[2])
+                # Poles (j min, then j max): the default copy of the ghost slab
+                if shell_pole_rule(f) == "copy":
+                    copy(pin & (J < 0), lambda x: I[x], lambda x: np.zeros_like(J[x]), lambda x: K[x])
+                    copy(pin & (J >= ih[1]), lambda x: I[x], lambda x: np.full_like(J[x], ih[1] - 1), lambda x: K[x])
+                solid, far = wall_rules(f, resistive)
+                # Farfield (i max)
+                if far == "copy":
+                    copy(tin & (I >= ih[0]), lambda x: np.full_like(I[x], ih[0] - 1), lambda x: J[x], lambda x: K[x])
+                elif far != "nop":
+                    raise ValueError(f"Farfield rule {far} of {f} is not compiled for the shell")
+                # Solid_Surface (i min)
+                g_lo = tin & (I < 0)
+                if solid == "copy":
+                    copy(g_lo, lambda x: np.zeros_like(I[x]), lambda x: J[x], lambda x: K[x])
+                elif solid in ("slab_zero_copy", "slab_zero2_copy"):
+                    zero(tin & ((I == 0) | ((I == 1) & (solid == "slab_zero2_copy"))))
+                    copy(g_lo, lambda x: np.zeros_like(I[x]), lambda x: J[x], lambda x: K[x])
+                elif solid == "eface_ghost_zero":
+                    zero(g_lo | ((tin & (I == 0)) if f == "Eface_xi" else np.zeros_like(g_lo)))
+                elif solid != "nop":
+                    raise ValueError(f"Solid_Surface rule {solid} of {f} is not compiled for the shell")
+                # corner default where a wall meets a Pole (along k)
+                cor = (K >= 0) & (K < ih[2]) & ((I < 0) | (I >= ih[0])) & ((J < 0) | (J >= ih[1]))
+                copy(cor, lambda x: np.clip(I[x], 0, ih[0] - 1), lambda x: np.clip(J[x], 0, ih[1] - 1), lambda x: K[x])
+            # the periodic halo in k (the plane k = n_k of k-staggered fields is inner)
+            copy((K < 0) | (K >= ih[2]), lambda x: I[x], lambda x: J[x], lambda x: np.mod(K[x], n[2]))
+            base = ctx.point_base(f, 0)
+            g = np.nonzero(~isc & (src != np.arange(npt)))[0]
+            c = np.nonzero(isc)[0]
+            for m in range(nc):
+                dsts.append(base + g * nc + m)
+                srcs.append(base + src[g] * nc + m)
+                cdst.append(base + c * nc + m)
+                cval.append(np.zeros(c.size))
+        out[group] = dict(dst=np.concatenate(dsts).astype(np.int64), src=np.concatenate(srcs).astype(np.int64),
+                          cdst=np.concatenate(cdst).astype(np.int64), cval=np.concatenate(cval), walls=[])
+    return out

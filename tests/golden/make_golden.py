@@ -195,6 +195,29 @@ def shell_steps(nr=8, nth=6, nph=8, steps=2, seed=20261207):
     print("wrote", tag, "steps")
 
 
+def shell_probe(nr=8, nth=6, nph=8, seed=20261207):
+    """Every Sync group of the Pole shell probed on the reference (as
+    slab_probe)."""
+    from beta1_b200 import syncmap
+    tag = "shell_%dx%dx%d" % (nr, nth, nph)
+    with tempfile.TemporaryDirectory() as d:
+        spec = case.shell_case(nr, nth, nph)
+        case.write_case(d, spec)
+        rst.write(os.path.join(d, "init.rst"), case.inflow_state(spec, seed=seed))
+        arr = {}
+        for grp in syncmap.GROUPS:
+            run(["probe", "init.rst", grp, "p.bin"], d)
+            p = rst.read(os.path.join(d, "p.bin"))
+            for fname, rec in p.fields.items():
+                v = rec.blocks[0].data.reshape(-1)
+                own = np.arange(v.size, dtype=np.float64) + 1.0
+                changed = np.nonzero(v != own)[0]
+                arr["%s/%s/0/dst" % (grp, fname)] = changed.astype(np.int32)
+                arr["%s/%s/0/val" % (grp, fname)] = v[changed]
+        np.savez_compressed(os.path.join(OUT, tag + "_probe.npz"), **arr)
+    print("wrote", tag + "_probe")
+
+
 def hall(spec_kind, seed=20261205):
     """The reference's Hall edge EMF (BuildHallFaceEMF_Rusanov_diff_) of a
     seeded state: a periodic box (no walls) and a slab whose Solid_Surface
@@ -329,6 +352,7 @@ if __name__ == "__main__":
     slab(steps=2, tiles=(1, 1))
     shell_geom()
     shell_steps()
+    shell_probe()
     slab_probe(resistive=0)
     slab_probe(resistive=1)
     hall("periodic")
