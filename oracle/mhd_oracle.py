@@ -208,6 +208,46 @@ class Oracle:
             U[3][G - ng, J, K] = rho_r * zero
             U[4][G - ng, J, K] = p_r / (g - 1.0) + ke_g
 
+    def shell_ucell_sync(self, b, qinf):
+        """Sync("Ucell") of the single-block spherical shell (Solid_Surface and
+        Farfield in i, Pole at both ends of j, k periodic onto itself), in the
+        reference's order (Z4_Lunar/src/boundary/Boundary_Sync_.cpp:4-65 with the
+        topology's patch order Pole j-min, Pole j-max, Farfield, Solid_Surface):
+        BC_Pole_Cell_ (Z4_Lunar/src/boundary/Boundary_Condition_Fluid.cpp:186-219:
+        the first cell layer at the pole replaced by its average over k, summed
+        in k order, then the default ghost copy of src/6_boundary/Boundary.cpp:303-332),
+        the far-field state, the solid wall, the corner default
+        (src/6_boundary/Boundary.cpp:178-260) and the periodic halo in k."""
+        blk = self.blocks[b]
+        U = blk.f["U_H"]
+        G = blk.G
+        ni, nj, nk = blk.n
+        I = slice(G, G + ni)
+        K = slice(G, G + nk)
+        for jref, ghosts in ((0, range(-G, 0)), (nj - 1, range(nj, nj + G))):
+            for m in range(5):
+                acc = np.zeros(ni)
+                for k in range(nk):
+                    acc = acc + U[m][I, G + jref, G + k]
+                avg = acc / float(nk)
+                U[m][I, G + jref, K] = avg[:, None]
+            for j in ghosts:
+                for m in range(5):
+                    U[m][I, G + j, K] = U[m][I, G + jref, K]
+        J = slice(G, G + nj)
+        for m in range(5):
+            U[m][G + ni:G + ni + G, J, K] = qinf[m]
+        self.wall_u(b, -1)
+        for ig in list(range(-G, 0)) + list(range(ni, ni + G)):
+            for jg in list(range(-G, 0)) + list(range(nj, nj + G)):
+                ic = min(max(ig, 0), ni - 1)
+                jc = min(max(jg, 0), nj - 1)
+                for m in range(5):
+                    U[m][G + ig, G + jg, K] = U[m][G + ic, G + jc, K]
+        for kg in list(range(-G, 0)) + list(range(nk, nk + G)):
+            for m in range(5):
+                U[m][:, :, G + kg] = U[m][:, :, G + (kg % nk)]
+
     # ------------------------------------------------------- derived fields
     def calc_bcell(self, blk):
         """calc_Bcell (Z4_Lunar/src/physics/LunarSolver_Tools.cpp:163-240)"""
