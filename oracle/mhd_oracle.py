@@ -8,9 +8,11 @@ It restates LunarSolver::StepOnce (Z4_Lunar/src/LunarSolver_Driver.cpp:21-92)
 stage by stage with whole-array numpy operations in the reference's floating
 point operation order, so on the reference's own inputs it reproduces the
 reference's outputs (pinned against the fixtures in tests/golden, which the
-reference solver itself produced).  Boundary synchronisations apply the same
-composed tables the device receives (their own equality with the reference's
-Sync is pinned separately against the reference's probe fixtures).
+reference solver itself produced).  Boundary synchronisations of the
+periodic box and the tiled slab apply the same composed tables the device
+receives (their own equality with the reference's Sync is pinned separately
+against the reference's probe fixtures); on the Pole shell (ShellOracle) the
+Sync runs the reference's handlers themselves, in the reference's order.
 
 Data layout: per block, a field is a float64 array (ncomp, NI, NJ, NK) over
 the padded logical box [-G, n + 1 + G) in each direction.
@@ -36,6 +38,7 @@ FIELDS = {
     "divB": (0, 1, 1), "dr_xi": (4, 3, 3), "dr_eta": (5, 3, 3), "dr_zeta": (6, 3, 3),
     "Area_xi": (1, 1, 3), "Area_eta": (2, 1, 3), "Area_zeta": (3, 1, 3), "dl_xi": (4, 1, 3), "dl_eta": (5, 1, 3),
     "dl_zeta": (6, 1, 3), "Ehall_xi": (4, 1, 4), "Ehall_eta": (5, 1, 4), "Ehall_zeta": (6, 1, 4),
+    "Astar_xi": (4, 1, 3), "Astar_eta": (5, 1, 3), "Astar_zeta": (6, 1, 3),
 }
 PLUS = {0: (0, 0, 0), 1: (1, 0, 0), 2: (0, 1, 0), 3: (0, 0, 1), 4: (0, 1, 1), 5: (1, 0, 1), 6: (1, 1, 0)}
 
@@ -207,46 +210,6 @@ class Oracle:
             U[2][G - ng, J, K] = rho_r * zero
             U[3][G - ng, J, K] = rho_r * zero
             U[4][G - ng, J, K] = p_r / (g - 1.0) + ke_g
-
-    def shell_ucell_sync(self, b, qinf):
-        """Sync("Ucell") of the single-block spherical shell (Solid_Surface and
-        Farfield in i, Pole at both ends of j, k periodic onto itself), in the
-        reference's order (Z4_Lunar/src/boundary/Boundary_Sync_.cpp:4-65 with the
-        topology's patch order Pole j-min, Pole j-max, Farfield, Solid_Surface):
-        BC_Pole_Cell_ (Z4_Lunar/src/boundary/Boundary_Condition_Fluid.cpp:186-219:
-        the first cell layer at the pole replaced by its average over k, summed
-        in k order, then the default ghost copy of src/6_boundary/Boundary.cpp:303-332),
-        the far-field state, the solid wall, the corner default
-        (src/6_boundary/Boundary.cpp:178-260) and the periodic halo in k."""
-        blk = self.blocks[b]
-        U = blk.f["U_H"]
-        G = blk.G
-        ni, nj, nk = blk.n
-        I = slice(G, G + ni)
-        K = slice(G, G + nk)
-        for jref, ghosts in ((0, range(-G, 0)), (nj - 1, range(nj, nj + G))):
-            for m in range(5):
-                acc = np.zeros(ni)
-                for k in range(nk):
-                    acc = acc + U[m][I, G + jref, G + k]
-                avg = acc / float(nk)
-                U[m][I, G + jref, K] = avg[:, None]
-            for j in ghosts:
-                for m in range(5):
-                    U[m][I, G + j, K] = U[m][I, G + jref, K]
-        J = slice(G, G + nj)
-        for m in range(5):
-            U[m][G + ni:G + ni + G, J, K] = qinf[m]
-        self.wall_u(b, -1)
-        for ig in list(range(-G, 0)) + list(range(ni, ni + G)):
-            for jg in list(range(-G, 0)) + list(range(nj, nj + G)):
-                ic = min(max(ig, 0), ni - 1)
-                jc = min(max(jg, 0), nj - 1)
-                for m in range(5):
-                    U[m][G + ig, G + jg, K] = U[m][G + ic, G + jc, K]
-        for kg in list(range(-G, 0)) + list(range(nk, nk + G)):
-            for m in range(5):
-                U[m][:, :, G + kg] = U[m][:, :, G + (kg % nk)]
 
     # ------------------------------------------------------- derived fields
     def calc_bcell(self, blk):
@@ -862,3 +825,473 @@ class Oracle:
             for (za, zlo, zhi) in zero_boxes:
                 if za == ea:
                     blk.f[name][0][blk.s(zlo, zhi)] = 0.0
+
+
+# ---------------------------------------------------------------------------
+# The single-block spherical shell: Solid_Surface (i min) and Farfield (i max)
+# in r, Pole patches at both ends of theta (j), phi (k) periodic onto itself
+# ---------------------------------------------------------------------------
+
+def _solve3_gj(A, b):
+    """Gauss-Jordan elimination with partial pivoting on [A | b], the 3x3 solve
+    of the reference's Pole handlers and repairs (Z4_Lunar/src/boundary/
+    Boundary_Condition.cpp:244-292, Boundary_Condition_EM.cpp:107-165,
+    Z4_Lunar/src/physics/LunarSolver_Tools.cpp:894-944); None when a pivot
+    falls below 1e-300."""
+    M = [[A[r][0], A[r][1], A[r][2], b[r]] for r in range(3)]
+    for c in range(3):
+        piv = c
+        amax = abs(M[c][c])
+        for r0 in range(c + 1, 3):
+            av = abs(M[r0][c])
+            if av > amax:
+                amax = av
+                piv = r0
+        if amax < 1.0e-300:
+            return None
+        if piv != c:
+            for q in range(c, 4):
+                M[c][q], M[piv][q] = M[piv][q], M[c][q]
+        inv = 1.0 / M[c][c]
+        for q in range(c, 4):
+            M[c][q] *= inv
+        for r0 in range(3):
+            if r0 == c:
+                continue
+            fac = M[r0][c]
+            for q in range(c, 4):
+                M[r0][q] -= fac * M[c][q]
+    return [M[0][3], M[1][3], M[2][3]]
+
+
+def _cmax(a, b):
+    """std::max(a, b) on scalars"""
+    return b if a < b else a
+
+
+class ShellOracle(Oracle):
+    """The oracle on one spherical-shell block.  Sync(group) runs the
+    reference's handlers in place, in the reference's order
+    (Z4_Lunar/src/boundary/Boundary_Sync_.cpp:4-65): per field the physical
+    handlers of the topology's patches (Pole j min, Pole j max, Farfield,
+    Solid_Surface; Z4_Lunar/src/boundary/Boundary_Build.cpp:5-271 names the
+    handler of every field and patch), the corner default where a wall meets
+    a Pole (src/6_boundary/Boundary.cpp:178-260), then the periodic halo in k.
+    The derived-field pass adds the reference's Pole repairs: the B_zeta flux
+    rewrite after Sync("B_cell"), the least-squares J_cell of the pole shell
+    and the divB zeroing next to the Poles."""
+
+    POLES = (-1, +1)  # j min (direction -2), j max (direction +2)
+
+    def __init__(self, ncell, consts, nodes, qinf, B_imf, resistive=False, G=4):
+        super().__init__([ncell], consts, G)
+        if resistive:
+            raise NotImplementedError("the resistive handlers of the shell are not restated")
+        self.nodes = nodes      # Padded ghost node mesh (..., 3) of the block
+        self.qinf = np.asarray(qinf, dtype=np.float64)
+        self.B_imf = np.asarray(B_imf, dtype=np.float64)
+        u = [qinf[1] / qinf[0], qinf[2] / qinf[0], qinf[3] / qinf[0]]
+        # BC_Farfield_Eedge_set_zerocurl (Boundary_Condition.cpp:559-600): E_inf = -u_inf x B_imf
+        self.E_inf = [B_imf[1] * u[2] - B_imf[2] * u[1], B_imf[2] * u[0] - B_imf[0] * u[2],
+                      B_imf[0] * u[1] - B_imf[1] * u[0]]
+
+    # ------------------------------------------------------------ helpers
+    def _ih(self, name):
+        p = PLUS[FIELDS[name][0]]
+        n = self.blocks[0].n
+        return (n[0] + p[0], n[1] + p[1], n[2] + p[2])
+
+    def _at(self, name, i, j, k, m=0):
+        blk = self.blocks[0]
+        G = blk.G
+        return float(blk.f[name][m][i + G, j + G, k + G])
+
+    def _put(self, name, i, j, k, m, v):
+        blk = self.blocks[0]
+        G = blk.G
+        blk.f[name][m][i + G, j + G, k + G] = v
+
+    def _slab(self, name, axis, side):
+        """(index of the inner slab along axis, slices of the tangential inner range)"""
+        ih = self._ih(name)
+        G = self.blocks[0].G
+        ref = 0 if side < 0 else ih[axis] - 1
+        tang = [slice(G, G + ih[a]) for a in range(3)]
+        return ref, tang
+
+    def _copy_ghosts(self, name, axis, side):
+        """DefaultPhysicalCopy (src/6_boundary/Boundary.cpp:303-332): every ghost
+        layer of the slab takes the first inner layer."""
+        blk = self.blocks[0]
+        G = blk.G
+        ng = FIELDS[name][2]
+        ref, t = self._slab(name, axis, side)
+        src = list(t)
+        src[axis] = ref + G
+        for g in range(1, ng + 1):
+            dst = list(t)
+            dst[axis] = ref + side * g + G
+            blk.f[name][(slice(None),) + tuple(dst)] = blk.f[name][(slice(None),) + tuple(src)]
+
+    def _set_ghosts(self, name, axis, side, vals):
+        blk = self.blocks[0]
+        G = blk.G
+        ng = FIELDS[name][2]
+        ref, t = self._slab(name, axis, side)
+        for g in range(1, ng + 1):
+            dst = list(t)
+            dst[axis] = ref + side * g + G
+            for m, v in enumerate(vals):
+                blk.f[name][(m,) + tuple(dst)] = v
+
+    def _zero_slab(self, name, axis, side, layers=1):
+        blk = self.blocks[0]
+        G = blk.G
+        ref, t = self._slab(name, axis, side)
+        for q in range(layers):
+            dst = list(t)
+            dst[axis] = ref - side * q + G
+            blk.f[name][(slice(None),) + tuple(dst)] = 0.0
+
+    # ------------------------------------------------------- Pole handlers
+    def _pole(self, name, side):
+        """The Pole handler of a field (Boundary_Build.cpp:27-269)."""
+        if name == "U_plus":
+            return
+        if name == "U_H":
+            self._pole_cell(side)
+        elif name in ("B_cell", "Bind_cell"):
+            self._pole_bcell(name, side)
+        elif name == "B_xi":
+            self._pole_ring_average("B_xi", side)
+        elif name == "B_eta":
+            self._zero_slab("B_eta", 1, side)
+        elif name == "E_xi":
+            self._pole_eedge_axis(side)
+        elif name == "E_eta":
+            self._pole_eedge_regulate(side)
+            return
+        elif name in ("E_zeta", "J_xi", "J_zeta"):
+            self._zero_slab(name, 1, side)
+        elif name == "J_eta":
+            self._pole_jedge_regulate(side)
+            return
+        elif name.startswith("Eres"):
+            raise NotImplementedError(name)
+        self._copy_ghosts(name, 1, side)
+
+    def _pole_cell(self, side):
+        """BC_Pole_Cell_ (Z4_Lunar/src/boundary/Boundary_Condition_Fluid.cpp:186-219):
+        the first cell layer at the pole becomes its average over k (summed in
+        k order, divided by the count)."""
+        self._pole_ring_average("U_H", side)
+
+    def _pole_ring_average(self, name, side):
+        """k-ring average of the inner slab (BC_Pole_Cell_ and the axis-face
+        branch of BC_Pole_Bface_Collapse_, Boundary_Condition_EM.cpp:620-670)"""
+        blk = self.blocks[0]
+        G = blk.G
+        ih = self._ih(name)
+        j = (0 if side < 0 else ih[1] - 1) + G
+        I = slice(G, G + ih[0])
+        for m in range(FIELDS[name][1]):
+            acc = np.zeros(ih[0])
+            for k in range(ih[2]):
+                acc = acc + blk.f[name][m][I, j, G + k]
+            avg = acc / float(ih[2])
+            blk.f[name][m][I, j, G:G + ih[2]] = avg[:, None]
+
+    def _pole_bcell(self, name, side):
+        """BC_Pole_Bcell_Collapse_ for an eta Pole (Boundary_Condition_EM.cpp:3-380):
+        per ring the cell vector that best reproduces, in least squares, the
+        fluxes of the outer eta face and the two xi faces of every cell of the
+        ring (the total fields add Badd), written to the whole ring."""
+        total = name == "B_cell"
+        n = self.blocks[0].n
+        j0 = 0 if side < 0 else n[1] - 1
+        jn = j0 + 1 if side < 0 else j0
+        sn = 1.0 if side < 0 else -1.0
+
+        def face(F, Fa, i, j, k):
+            v = self._at(F, i, j, k)
+            if total:
+                v += self._at(Fa, i, j, k)
+            return v
+
+        for i in range(n[0]):
+            M = [[0.0] * 3 for _ in range(3)]
+            b = [0.0, 0.0, 0.0]
+
+            def push(S, phi):
+                sn2 = S[0] * S[0] + S[1] * S[1] + S[2] * S[2]
+                if sn2 <= 1.0e-300:
+                    return
+                for a in range(3):
+                    b[a] += phi * S[a]
+                    for c in range(3):
+                        M[a][c] += S[a] * S[c]
+
+            for k in range(n[2]):
+                push([sn * self._at("JDet", i, jn, k, m) for m in range(3)], sn * face("B_eta", "Badd_eta", i, jn, k))
+                push([-self._at("JDxi", i, j0, k, m) for m in range(3)], -face("B_xi", "Badd_xi", i, j0, k))
+                push([self._at("JDxi", i + 1, j0, k, m) for m in range(3)], face("B_xi", "Badd_xi", i + 1, j0, k))
+            tr = abs(M[0][0]) + abs(M[1][1]) + abs(M[2][2])
+            reg = 1.0e-12 * _cmax(1.0, tr)
+            for a in range(3):
+                M[a][a] += reg
+            Bp = _solve3_gj(M, b)
+            if Bp is None:
+                continue
+            for k in range(n[2]):
+                for m in range(3):
+                    self._put(name, i, j0, k, m, Bp[m])
+
+    def _pole_eedge_axis(self, side):
+        """BC_Pole_Eedge_Axis for E_xi on an eta Pole (Boundary_Condition.cpp:27-164):
+        E = -u_plus x B_cell of the first cell layer, projected on dr_xi."""
+        ih = self._ih("E_xi")
+        j = 0 if side < 0 else ih[1] - 1
+        jc = j if side < 0 else j - 1
+        for i in range(ih[0]):
+            for k in range(ih[2]):
+                ux, uy, uz = (self._at("U_plus", i, jc, k, m) for m in range(3))
+                Bx, By, Bz = (self._at("B_cell", i, jc, k, m) for m in range(3))
+                E = [-(uy * Bz - uz * By), -(uz * Bx - ux * Bz), -(ux * By - uy * Bx)]
+                dl = [self._at("dr_xi", i, j, k, m) for m in range(3)]
+                self._put("E_xi", i, j, k, 0, E[0] * dl[0] + E[1] * dl[1] + E[2] * dl[2])
+
+    def _pole_eedge_regulate(self, side):
+        """BC_Pole_Eedge_RegulateK_Norm for E_eta on an eta Pole
+        (Boundary_Condition.cpp:179-477): per ring the Cartesian vector whose
+        projections best reproduce the edge values (k = n_k excluded: it is
+        k = 0), projected back onto every edge; then the ghost copy."""
+        ih = self._ih("E_eta")
+        j = 0 if side < 0 else ih[1] - 1
+        for i in range(ih[0]):
+            A = [[0.0] * 3 for _ in range(3)]
+            b = [0.0, 0.0, 0.0]
+            cnt = 0
+            for k in range(ih[2] - 1):
+                dl = [self._at("dr_eta", i, j, k, m) for m in range(3)]
+                L = np.sqrt(dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2])
+                if L < 1.0e-14:
+                    continue
+                invL = 1.0 / L
+                tau = [dl[0] * invL, dl[1] * invL, dl[2] * invL]
+                y = self._at("E_eta", i, j, k) * invL
+                for a in range(3):
+                    b[a] += y * tau[a]
+                    for c in range(3):
+                        A[a][c] += tau[a] * tau[c]
+                cnt += 1
+            if cnt <= 0:
+                for k in range(ih[2]):
+                    self._put("E_eta", i, j, k, 0, 0.0)
+                continue
+            trA = A[0][0] + A[1][1] + A[2][2]
+            reg = 1.0e-12 * _cmax(1.0, trA)
+            for a in range(3):
+                A[a][a] += reg
+            Ev = _solve3_gj(A, b)
+            if Ev is None:
+                avg = 0.0
+                for k in range(ih[2]):
+                    avg += self._at("E_eta", i, j, k)
+                avg /= float(ih[2])
+                for k in range(ih[2]):
+                    self._put("E_eta", i, j, k, 0, avg)
+                continue
+            for k in range(ih[2]):
+                dl = [self._at("dr_eta", i, j, k, m) for m in range(3)]
+                L = np.sqrt(dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2])
+                v = 0.0 if L < 1.0e-14 else Ev[0] * dl[0] + Ev[1] * dl[1] + Ev[2] * dl[2]
+                self._put("E_eta", i, j, k, 0, v)
+        self._copy_ghosts("E_eta", 1, side)
+
+    def _pole_jedge_regulate(self, side):
+        """BC_Pole_Jedge_RegulateK_Norm for J_eta on an eta Pole
+        (Boundary_Condition.cpp:478-548): the circulation of beta_zeta B_zeta
+        around the dual edge times dl_eta / Astar_eta; the ghost slab is zeroed."""
+        blk = self.blocks[0]
+        G = blk.G
+        ih = self._ih("J_eta")
+        j = 0 if side < 0 else ih[1] - 1
+        lo, hi = (0, j, 0), (ih[0], j + 1, ih[2])
+        bz = lambda d: blk.box("beta_zeta", 0, lo, hi, d) * blk.box("B_zeta", 0, lo, hi, d)
+        circ = bz((-1, 0, 0)) - bz((0, 0, 0))
+        Ast = blk.box("Astar_eta", 0, lo, hi)
+        dl = blk.box("dl_eta", 0, lo, hi)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            v = np.where(np.abs(Ast) <= 1.0e-300, 0.0, (dl / Ast) * circ)
+        blk.f["J_eta"][0][blk.s(lo, hi)] = v
+        self._set_ghosts("J_eta", 1, side, [0.0])
+
+    # -------------------------------------------- Farfield / Solid_Surface
+    def _farfield(self, name):
+        """Farfield handler (i max) of the non-resistive set-up (Boundary_Build.cpp:5-271)."""
+        if name in ("U_plus", "B_xi", "B_eta", "B_zeta", "Eface_xi", "Eface_eta", "Eface_zeta"):
+            return
+        if name == "U_H":
+            self._set_ghosts("U_H", 0, +1, self.qinf)       # BC_UH_Farfield_H_
+        elif name == "B_cell":
+            self._set_ghosts("B_cell", 0, +1, self.B_imf)   # BC_Farfield_Bface
+        elif name == "Bind_cell":
+            self._set_ghosts("Bind_cell", 0, +1, [0.0, 0.0, 0.0])
+        elif name in ("E_xi", "E_eta", "E_zeta"):
+            # BC_Farfield_Eedge_set_zerocurl: slab <- E_inf . (x(edge end) - x(edge start)), then copy
+            blk = self.blocks[0]
+            G = blk.G
+            ih = self._ih(name)
+            d = {"E_xi": (1, 0, 0), "E_eta": (0, 1, 0), "E_zeta": (0, 0, 1)}[name]
+            i = ih[0] - 1
+            X, o = self.nodes.a, self.nodes.off
+            p0 = X[i + o, o:o + ih[1], o:o + ih[2]]
+            p1 = X[i + d[0] + o, o + d[1]:o + d[1] + ih[1], o + d[2]:o + d[2] + ih[2]]
+            E = self.E_inf
+            blk.f[name][0][i + G, G:G + ih[1], G:G + ih[2]] = (E[0] * (p1[..., 0] - p0[..., 0])
+                                                               + E[1] * (p1[..., 1] - p0[..., 1])
+                                                               + E[2] * (p1[..., 2] - p0[..., 2]))
+            self._copy_ghosts(name, 0, +1)
+        else:
+            self._copy_ghosts(name, 0, +1)
+
+    def _solid(self, name):
+        """Solid_Surface handler (i min) of the non-resistive set-up."""
+        if name in ("U_plus", "E_xi", "E_eta", "E_zeta"):
+            return
+        if name == "U_H":
+            self.wall_u(0, -1)                  # BC_Solid_Surface_
+            return
+        if name == "J_cell":
+            self._zero_slab("J_cell", 0, -1, layers=2)   # BC_Solid_Surface_Jcell (EM.cpp:382-427)
+        elif name.startswith("Eface_"):
+            self._zero_slab(name, 0, -1)        # BC_Solid_Surface_Eface_ (EM.cpp:787-803)
+        self._copy_ghosts(name, 0, -1)
+
+    def _corner_default(self, name):
+        """ApplyPhysicalCornerDefault on the four wall/Pole edges along k."""
+        blk = self.blocks[0]
+        G = blk.G
+        ng = FIELDS[name][2]
+        ih = self._ih(name)
+        K = slice(G, G + ih[2])
+        for ig in list(range(-ng, 0)) + list(range(ih[0], ih[0] + ng)):
+            for jg in list(range(-ng, 0)) + list(range(ih[1], ih[1] + ng)):
+                ic = min(max(ig, 0), ih[0] - 1)
+                jc = min(max(jg, 0), ih[1] - 1)
+                blk.f[name][:, ig + G, jg + G, K] = blk.f[name][:, ic + G, jc + G, K]
+
+    def _halo_k(self, name):
+        """The block's periodic halo in k: a ghost plane takes plane k mod n_k."""
+        blk = self.blocks[0]
+        G = blk.G
+        ng = FIELDS[name][2]
+        ih = self._ih(name)
+        nk = blk.n[2]
+        for kg in list(range(-ng, 0)) + list(range(ih[2], ih[2] + ng)):
+            blk.f[name][:, :, :, kg + G] = blk.f[name][:, :, :, (kg % nk) + G]
+
+    HALO_ONLY = ("Uplus",)
+
+    def sync(self, group):
+        from_groups = {
+            "Ucell": ["U_H"], "Bface": ["B_xi", "B_eta", "B_zeta"], "Eface": ["Eface_xi", "Eface_eta", "Eface_zeta"],
+            "Eedge": ["E_xi", "E_eta", "E_zeta"], "B_cell": ["B_cell", "Bind_cell"], "Jedge": ["J_xi", "J_eta", "J_zeta"],
+            "J_cell": ["J_cell"], "Uplus": ["U_plus"], "dB": ["dB_xi", "dB_eta", "dB_zeta"],
+            "Badd": ["Badd_xi", "Badd_eta", "Badd_zeta"], "Ehall": ["Ehall_xi", "Ehall_eta", "Ehall_zeta"]}
+        fields = from_groups[group]
+        if group not in self.HALO_ONLY:
+            for f in fields:
+                for side in self.POLES:
+                    self._pole(f, side)
+                self._farfield(f)
+                self._solid(f)
+            for f in fields:
+                self._corner_default(f)
+        for f in fields:
+            self._halo_k(f)
+
+    # ------------------------------------------------ Pole repairs
+    def bzeta_pole_rewrite(self):
+        """calc_Bcell after Sync("B_cell") (Z4_Lunar/src/physics/LunarSolver_Tools.cpp:242-307):
+        on the first cell layer at each eta Pole, B_zeta becomes the flux of
+        Bind_cell through the zeta face, k = 0 .. n_k."""
+        blk = self.blocks[0]
+        n = blk.n
+        for side in self.POLES:
+            jc = 0 if side < 0 else n[1] - 1
+            lo, hi = (0, jc, 0), (n[0], jc + 1, n[2] + 1)
+            bi = [blk.box("Bind_cell", m, lo, hi) for m in range(3)]
+            A = [blk.box("JDze", m, lo, hi) for m in range(3)]
+            blk.f["B_zeta"][0][blk.s(lo, hi)] = bi[0] * A[0] + bi[1] * A[1] + bi[2] * A[2]
+
+    def jcell_pole_repair(self):
+        """The least-squares J_cell of the first cell layer at each eta Pole
+        (calc_Jcell, LunarSolver_Tools.cpp:945-1090): per ring the Cartesian
+        vector that best reproduces the J edge 1-forms of the ring's norm
+        edges on the Pole layer and its axis / rotate edges one node layer away."""
+        n = self.blocks[0].n
+        for side in self.POLES:
+            jc = 0 if side < 0 else n[1] - 1
+            jt = jc + 1 if side < 0 else jc
+            for i in range(n[0]):
+                A = [[0.0] * 3 for _ in range(3)]
+                b = [0.0, 0.0, 0.0]
+                cnt = 0
+
+                def push(Je, dr, ii, jj, kk):
+                    nonlocal cnt
+                    d = [self._at(dr, ii, jj, kk, m) for m in range(3)]
+                    L = np.sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2])
+                    if L < 1.0e-14:
+                        return
+                    tau = [d[0] / L, d[1] / L, d[2] / L]
+                    y = self._at(Je, ii, jj, kk) / L
+                    for a in range(3):
+                        b[a] += y * tau[a]
+                        for c in range(3):
+                            A[a][c] += tau[a] * tau[c]
+                    cnt += 1
+
+                for k in range(n[2]):
+                    push("J_eta", "dr_eta", i, jc, k)
+                    push("J_eta", "dr_eta", i + 1, jc, k)
+                    push("J_eta", "dr_eta", i, jc, k + 1)
+                    push("J_eta", "dr_eta", i + 1, jc, k + 1)
+                    push("J_xi", "dr_xi", i, jt, k)
+                    push("J_xi", "dr_xi", i, jt, k + 1)
+                    push("J_zeta", "dr_zeta", i, jt, k)
+                    push("J_zeta", "dr_zeta", i + 1, jt, k)
+                if cnt <= 0:
+                    continue
+                trA = A[0][0] + A[1][1] + A[2][2]
+                reg = 1.0e-12 * _cmax(1.0, trA)
+                for a in range(3):
+                    A[a][a] += reg
+                Jp = _solve3_gj(A, b)
+                if Jp is None:
+                    continue
+                for k in range(n[2]):
+                    for m in range(3):
+                        self._put("J_cell", i, jc, k, m, Jp[m])
+
+    def update_magnetic_derived(self):
+        blk = self.blocks[0]
+        self.calc_bcell(blk)
+        self.sync("B_cell")
+        self.bzeta_pole_rewrite()
+        self.curl_adj(blk, ("B_xi", "B_eta", "B_zeta"), ("J_xi", "J_eta", "J_zeta"))
+        self.sync("Jedge")
+        self.calc_jcell(blk)
+        self.jcell_pole_repair()
+        self.sync("J_cell")
+
+    def calc_divb(self):
+        """calc_divB with the Pole zeroing of the first cell layer at each
+        Pole (LunarSolver_Tools.cpp:685-775)."""
+        super().calc_divb()
+        blk = self.blocks[0]
+        n = blk.n
+        for side in self.POLES:
+            jc = 0 if side < 0 else n[1] - 1
+            blk.f["divB"][0][blk.s((0, jc, 0), (n[0], jc + 1, n[2]))] = 0.0

@@ -44,34 +44,3 @@ def test_shell_tables_equal_reference_sync():
             checked += dd.size
     assert checked > 10000
 
-
-def test_oracle_shell_ucell_sync_equals_reference_sync():
-    """The U_H Sync of the shell: the Pole ring average of the first cell layer
-    and its ghost copy, the far-field state, the solid wall, the corner default
-    and the periodic halo, restated in the oracle, equal at every point to what
-    the reference's Sync leaves in the index-filled field."""
-    import os
-    import sys
-
-    from conftest import ROOT
-    from beta1_b200 import physics
-
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import mhd_oracle
-    from test_cpu_oracle import oracle_consts
-
-    probe = load_golden("shell_8x6x8_probe.npz")
-    spec = case.shell_case(8, 6, 8)
-    n = spec.blocks[0].ncell
-    o = mhd_oracle.Oracle([n], oracle_consts(spec.params))
-    G = 4
-    shape = (n[0] + 2 * G, n[1] + 2 * G, n[2] + 2 * G, 5)
-    o.blocks[0].set_ref("U_H", (-G, -G, -G), (np.arange(np.prod(shape), dtype=np.float64) + 1.0).reshape(shape))
-    qinf, _ = physics.farfield_state(spec.params)
-    o.shell_ucell_sync(0, qinf)
-    got = o.blocks[0].get_ref("U_H").reshape(-1)
-    ref = np.arange(got.size, dtype=np.float64) + 1.0
-    ref[probe["Ucell/U_H/0/dst"]] = probe["Ucell/U_H/0/val"]
-    assert probe["Ucell/U_H/0/dst"].size > 10000
-    bad = np.nonzero(got != ref)[0]
-    assert bad.size == 0, bad[:10]
