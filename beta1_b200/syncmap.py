@@ -334,63 +334,80 @@ def compile_tiled(ctx, layout: TiledLayout, resistive: bool, farfield_consts, no
 # both ends of j, k periodic onto itself
 # ---------------------------------------------------------------------------
 #
-# A Sync(group) there is (Z4_Lunar/src/boundary/Boundary_Sync_.cpp:4-65):
-#   the physical handlers of the i walls (as on the slab) and of the Poles
-#   (the default copy of the ghost slab from the first inner layer,
-#   src/6_boundary/Boundary.cpp:303-332, unless a field overrides it),
-#   the corner default where a wall meets a Pole: every ghost point of the
-#   corner takes the value of the nearest inner point
-#   (BoundaryCore::ApplyPhysicalCornerDefault, src/6_boundary/Boundary.cpp:178-260),
-#   then the periodic halo in k.
-# Fields whose Pole handler computes values (U_H's ring average, the B_cell
-# and face-B collapses, the edge EMF and J edge regulation) are not compiled
-# here: their groups are listed in SHELL_POLE_HANDLED.
+# A Sync(group) there is (Z4_Lunar/src/boundary/Boundary_Sync_.cpp:4-65), per
+# field, the physical handlers in the topology's patch order -- Pole j min,
+# Pole j max, Farfield (i max), Solid_Surface (i min) -- then the corner
+# default where a wall meets a Pole (every ghost point of the corner takes the
+# value of the nearest inner point, BoundaryCore::ApplyPhysicalCornerDefault,
+# src/6_boundary/Boundary.cpp:178-260), then the periodic halo in k.
+#
+# What the Pole handler of the shipped set-up does to a field
+# (Z4_Lunar/src/boundary/Boundary_Build.cpp:27-269, eta Poles):
+#   copy   the ghost slab <- the first inner layer (DefaultPhysicalCopy)
+#   nop    nothing
+#   ring   the device computes the first inner layer (the pole ring): U_H's
+#          k average (BC_Pole_Cell_), the B_cell / Bind_cell collapse, B_xi's
+#          k average (BC_Pole_Bface_Collapse_), E_xi from -u x B
+#          (BC_Pole_Eedge_Axis), E_eta's regulation (BC_Pole_Eedge_RegulateK_Norm);
+#          then the ghost copy
+#   zero   the first inner layer <- 0, then the ghost copy (B_eta's norm face,
+#          BC_Pole_Eedge_Zero_Rotate of E_zeta, J_xi, J_zeta)
+#   ring_ghost_zero  the device computes the first inner layer (J_eta,
+#          BC_Pole_Jedge_RegulateK_Norm); the ghost slab <- 0
+SHELL_POLE_RULES = {"U_plus": "nop", "U_H": "ring", "B_cell": "ring", "Bind_cell": "ring", "B_xi": "ring",
+                    "E_xi": "ring", "E_eta": "ring", "B_eta": "zero", "E_zeta": "zero", "J_xi": "zero",
+                    "J_zeta": "zero", "J_eta": "ring_ghost_zero"}
 
-SHELL_POLE_HANDLED = ("Ucell", "Bface", "Eedge", "B_cell", "Jedge", "Eres", "Eres1form")
-
-
-def shell_pole_rule(field: str) -> str:
-    """What the Pole handler of the shipped Lunar set-up does to a field
-    (Z4_Lunar/src/boundary/Boundary_Build.cpp:27-40 and the overrides after)."""
-    if field == "U_plus":
-        return "nop"
-    if field in ("U_H", "B_cell", "Bind_cell", "B_xi", "B_eta", "E_xi", "E_eta", "E_zeta", "Eres_xi", "Eres_eta",
-                 "Eres_zeta", "J_xi", "J_eta", "J_zeta"):
-        return "handler"
-    return "copy"
-
+# groups with a computing Pole handler (the device runs their ring kernels
+# before the group's tables)
+SHELL_POLE_HANDLED = ("Ucell", "Bface", "Eedge", "B_cell", "Jedge")
 
 # groups whose Sync runs the halo exchange only (no physical handlers, no
 # corner default): Sync("Uplus") after calc_Uplus
 SHELL_HALO_ONLY = ("Uplus",)
 
+# resistive groups: their Pole handlers (the Eres regulation) are not compiled
+SHELL_SKIPPED = ("Eres", "Eres1form")
 
-def compile_shell(ctx, ncell, resistive: bool):
-    """Tables of every Sync group of the shell whose Pole handling is a copy
-    (or nothing); groups in SHELL_POLE_HANDLED are left out.  ctx: a context
-    or HostLayout of the one block.
+
+def shell_pole_rule(field: str) -> str:
+    """What the Pole handler of the shipped Lunar set-up does to a field."""
+    if field.startswith("Eres"):
+        raise ValueError(f"the Pole handler of {field} is not compiled")
+    return SHELL_POLE_RULES.get(field, "copy")
+
+
+def compile_shell(ctx, ncell, resistive: bool, farfield_consts=None, nodes=None):
+    """Tables of every Sync group of the shell (the resistive groups aside).
+    ctx: a context or HostLayout of the one block; farfield_consts: dict with
+    'qinf' (5), 'B_imf' (3), 'E_inf' (3); nodes: the block's Padded ghost node
+    mesh (both needed by the groups with Farfield values).
 
     The Sync is replayed in the reference's order on a map that holds, per
-    point, either the pre-sync value of some point or a constant: the Pole
-    patches (j min, j max), the Farfield, the Solid_Surface (the topology's
-    patch order), the corner default, then the periodic halo in k.  Unlike
-    the tiled layout, a copy here can read a point before a later handler
-    sets it to a constant (the Pole ghost copy at i = 0 reads the wall slab
-    before the wall handler zeroes it), so the gather entries deliver
-    PRE-sync values: apply the gather before the fixed values.
-    Returns {group: dict(dst, src, cdst, cval, walls)}."""
+    point, the point whose value it takes and when that value is read, or a
+    constant.  The device runs a shell Sync as
+      1. the Pole ring kernels (in place, on the first inner layer),
+      2. the gather `dst/src`: sources read after the rings, before the walls,
+      3. the Solid_Surface fluid handler (`walls`; in place, wall layer and ghosts),
+      4. the gather `dst2/src2`: sources the wall handler wrote,
+      5. the fixed values `cdst/cval`.
+    A copy here can read a point before a later handler overwrites it (the
+    Pole ghost copy at i = 0 reads the wall layer before the wall handler
+    zeroes or rewrites it), hence the copies before the fixed values, and the
+    two gathers around the wall.
+    Returns {group: dict(dst, src, dst2, src2, cdst, cval, walls)}."""
+    if resistive:
+        raise NotImplementedError("the resistive handlers of the shell are not compiled")
     n = tuple(ncell)
     out = {}
     for group, fields in GROUPS.items():
-        if group in SHELL_POLE_HANDLED:
+        if group in SHELL_SKIPPED:
             continue
         physical = group not in SHELL_HALO_ONLY
-        dsts, srcs, cdst, cval = [], [], [], []
+        dsts, srcs, dsts2, srcs2, cdst, cval, walls = [], [], [], [], [], [], []
         for f in fields:
-            if shell_pole_rule(f) == "handler":
-                raise ValueError(f"field {f} has a computing Pole handler")
             info = ctx.field_info(f, 0)
-            loc, nc = info["loc"], info["ncomp"]
+            loc, nc, ng = info["loc"], info["ncomp"], info["nghost"]
             lo, hi = info["lo"], info["hi"]
             pl = PLUS[loc]
             ih = (n[0] + pl[0], n[1] + pl[1], n[2] + pl[2])
@@ -401,29 +418,59 @@ def compile_shell(ctx, ncell, resistive: bool):
             def off(i, j, k):
                 return ((i - lo[0]) * shape[1] + (j - lo[1])) * shape[2] + (k - lo[2])
 
-            src = np.arange(npt)           # pre-sync point whose value a point holds
-            isc = np.zeros(npt, dtype=bool)  # ... or a constant (zero here)
+            src = np.arange(npt)               # point whose value a point ends up holding
+            ver = np.zeros(npt, dtype=np.int8)  # ... read before (0) or after (1) the wall handler
+            isc = np.zeros(npt, dtype=bool)     # ... or a constant
+            cv = np.zeros((npt, nc))
 
             def copy(sel, i, j, k):
                 idx = np.nonzero(sel)[0]
                 o = off(i(idx), j(idx), k(idx))
                 src[idx] = src[o]
+                ver[idx] = ver[o]
                 isc[idx] = isc[o]
+                cv[idx] = cv[o]
 
-            def zero(sel):
-                isc[np.nonzero(sel)[0]] = True
+            def const(sel, vals):
+                idx = np.nonzero(sel)[0]
+                isc[idx] = True
+                cv[idx] = np.asarray(vals, dtype=np.float64).reshape(-1, nc) if np.ndim(vals) == 2 else vals
 
             if physical:
                 pin = (I >= 0) & (I < ih[0]) & (K >= 0) & (K < ih[2])
                 tin = (J >= 0) & (J < ih[1]) & (K >= 0) & (K < ih[2])
-                # Poles (j min, then j max): the default copy of the ghost slab
-                if shell_pole_rule(f) == "copy":
-                    copy(pin & (J < 0), lambda x: I[x], lambda x: np.zeros_like(J[x]), lambda x: K[x])
-                    copy(pin & (J >= ih[1]), lambda x: I[x], lambda x: np.full_like(J[x], ih[1] - 1), lambda x: K[x])
-                solid, far = wall_rules(f, resistive)
+                rule = shell_pole_rule(f)
+                for side in (-1, +1):
+                    jr = 0 if side < 0 else ih[1] - 1
+                    ghost = pin & ((J < 0) if side < 0 else (J >= ih[1]))
+                    if rule == "nop":
+                        continue
+                    if rule == "zero":
+                        const(pin & (J == jr), 0.0)
+                    if rule == "ring_ghost_zero":
+                        const(ghost, 0.0)
+                        continue
+                    copy(ghost, lambda x: I[x], lambda x, jr=jr: np.full_like(J[x], jr), lambda x: K[x])
+                solid, far = wall_rules(f, False)
                 # Farfield (i max)
+                g_hi = tin & (I >= ih[0])
                 if far == "copy":
-                    copy(tin & (I >= ih[0]), lambda x: np.full_like(I[x], ih[0] - 1), lambda x: J[x], lambda x: K[x])
+                    copy(g_hi, lambda x: np.full_like(I[x], ih[0] - 1), lambda x: J[x], lambda x: K[x])
+                elif far == "ghost_const":
+                    vals = {"U_H": farfield_consts["qinf"], "B_cell": farfield_consts["B_imf"],
+                            "Bind_cell": [0.0, 0.0, 0.0]}[f]
+                    const(g_hi, [float(v) for v in vals])
+                elif far == "slab_const_copy":
+                    sl = tin & (I == ih[0] - 1)
+                    idx = np.nonzero(sl)[0]
+                    d = {"E_xi": (1, 0, 0), "E_eta": (0, 1, 0), "E_zeta": (0, 0, 1)}[f]
+                    o = nodes.off
+                    p0 = nodes.a[I[idx] + o, J[idx] + o, K[idx] + o]
+                    p1 = nodes.a[I[idx] + d[0] + o, J[idx] + d[1] + o, K[idx] + d[2] + o]
+                    E = farfield_consts["E_inf"]
+                    val = (E[0] * (p1[:, 0] - p0[:, 0]) + E[1] * (p1[:, 1] - p0[:, 1])) + E[2] * (p1[:, 2] - p0[:, 2])
+                    const(sl, val[:, None])
+                    copy(g_hi, lambda x: np.full_like(I[x], ih[0] - 1), lambda x: J[x], lambda x: K[x])
                 elif far != "nop":
                     raise ValueError(f"Farfield rule {far} of {f} is not compiled for the shell")
                 # Solid_Surface (i min)
@@ -431,10 +478,15 @@ def compile_shell(ctx, ncell, resistive: bool):
                 if solid == "copy":
                     copy(g_lo, lambda x: np.zeros_like(I[x]), lambda x: J[x], lambda x: K[x])
                 elif solid in ("slab_zero_copy", "slab_zero2_copy"):
-                    zero(tin & ((I == 0) | ((I == 1) & (solid == "slab_zero2_copy"))))
+                    const(tin & ((I == 0) | ((I == 1) & (solid == "slab_zero2_copy"))), 0.0)
                     copy(g_lo, lambda x: np.zeros_like(I[x]), lambda x: J[x], lambda x: K[x])
-                elif solid == "eface_ghost_zero":
-                    zero(g_lo | ((tin & (I == 0)) if f == "Eface_xi" else np.zeros_like(g_lo)))
+                elif solid == "wall_u":
+                    # the wall handler rewrites the wall layer and its ghosts in place
+                    w = np.nonzero(tin & (I <= 0))[0]
+                    src[w] = w
+                    ver[w] = 1
+                    isc[w] = False
+                    walls = [(0, -1)]
                 elif solid != "nop":
                     raise ValueError(f"Solid_Surface rule {solid} of {f} is not compiled for the shell")
                 # corner default where a wall meets a Pole (along k)
@@ -443,13 +495,18 @@ def compile_shell(ctx, ncell, resistive: bool):
             # the periodic halo in k (the plane k = n_k of k-staggered fields is inner)
             copy((K < 0) | (K >= ih[2]), lambda x: I[x], lambda x: J[x], lambda x: np.mod(K[x], n[2]))
             base = ctx.point_base(f, 0)
-            g = np.nonzero(~isc & (src != np.arange(npt)))[0]
+            moved = ~isc & (src != np.arange(npt))
+            g1 = np.nonzero(moved & (ver == 0))[0]
+            g2 = np.nonzero(moved & (ver == 1))[0]
             c = np.nonzero(isc)[0]
             for m in range(nc):
-                dsts.append(base + g * nc + m)
-                srcs.append(base + src[g] * nc + m)
+                dsts.append(base + g1 * nc + m)
+                srcs.append(base + src[g1] * nc + m)
+                dsts2.append(base + g2 * nc + m)
+                srcs2.append(base + src[g2] * nc + m)
                 cdst.append(base + c * nc + m)
-                cval.append(np.zeros(c.size))
+                cval.append(cv[c, m])
         out[group] = dict(dst=np.concatenate(dsts).astype(np.int64), src=np.concatenate(srcs).astype(np.int64),
-                          cdst=np.concatenate(cdst).astype(np.int64), cval=np.concatenate(cval), walls=[])
+                          dst2=np.concatenate(dsts2).astype(np.int64), src2=np.concatenate(srcs2).astype(np.int64),
+                          cdst=np.concatenate(cdst).astype(np.int64), cval=np.concatenate(cval), walls=walls)
     return out

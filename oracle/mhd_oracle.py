@@ -1060,7 +1060,7 @@ class ShellOracle(Oracle):
                 dl = [self._at("dr_xi", i, j, k, m) for m in range(3)]
                 self._put("E_xi", i, j, k, 0, E[0] * dl[0] + E[1] * dl[1] + E[2] * dl[2])
 
-    def _pole_eedge_regulate(self, side):
+    def _pole_eedge_regulate(self, side, ghosts=True):
         """BC_Pole_Eedge_RegulateK_Norm for E_eta on an eta Pole
         (Boundary_Condition.cpp:179-477): per ring the Cartesian vector whose
         projections best reproduce the edge values (k = n_k excluded: it is
@@ -1106,9 +1106,10 @@ class ShellOracle(Oracle):
                 L = np.sqrt(dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2])
                 v = 0.0 if L < 1.0e-14 else Ev[0] * dl[0] + Ev[1] * dl[1] + Ev[2] * dl[2]
                 self._put("E_eta", i, j, k, 0, v)
-        self._copy_ghosts("E_eta", 1, side)
+        if ghosts:
+            self._copy_ghosts("E_eta", 1, side)
 
-    def _pole_jedge_regulate(self, side):
+    def _pole_jedge_regulate(self, side, ghosts=True):
         """BC_Pole_Jedge_RegulateK_Norm for J_eta on an eta Pole
         (Boundary_Condition.cpp:478-548): the circulation of beta_zeta B_zeta
         around the dual edge times dl_eta / Astar_eta; the ghost slab is zeroed."""
@@ -1124,7 +1125,25 @@ class ShellOracle(Oracle):
         with np.errstate(divide="ignore", invalid="ignore"):
             v = np.where(np.abs(Ast) <= 1.0e-300, 0.0, (dl / Ast) * circ)
         blk.f["J_eta"][0][blk.s(lo, hi)] = v
-        self._set_ghosts("J_eta", 1, side, [0.0])
+        if ghosts:
+            self._set_ghosts("J_eta", 1, side, [0.0])
+
+    def pole_rings(self, group):
+        """Only the values the Pole handlers of a group compute on the first
+        inner layer (both Poles), none of their copies or zeros."""
+        for side in self.POLES:
+            if group == "Ucell":
+                self._pole_cell(side)
+            elif group == "Bface":
+                self._pole_ring_average("B_xi", side)
+            elif group == "B_cell":
+                self._pole_bcell("B_cell", side)
+                self._pole_bcell("Bind_cell", side)
+            elif group == "Eedge":
+                self._pole_eedge_axis(side)
+                self._pole_eedge_regulate(side, ghosts=False)
+            elif group == "Jedge":
+                self._pole_jedge_regulate(side, ghosts=False)
 
     # -------------------------------------------- Farfield / Solid_Surface
     def _farfield(self, name):

@@ -1,46 +1,123 @@
 """Compiled synchronisation of the single-block spherical shell (Solid_Surface
 and Farfield in r, Pole patches at both ends of theta, phi periodic onto
-itself) against the reference's own Sync, for every group whose Pole
-handling is a copy: U_plus, the face EMF, J_cell, dB, Badd and the Hall edge
-EMF.  The probe fixture (tests/golden/make_golden.py, shell_probe) holds what
-the reference's Sync leaves in every point after each point was pre-filled
-with its own index.  The shell's gather entries deliver pre-sync values (a
-Pole ghost copy reads the wall slab before the wall handler zeroes it), so a
-copied point must hold its source's index, a fixed point its constant, and
-every other point its own index."""
+itself), in the order the device runs it: the Pole ring kernels, the gather
+of values read before the wall handler, the wall handler, the gather of
+values it wrote, then the fixed values (syncmap.compile_shell).
+
+That order is emulated here on the oracle's arrays (the ring kernels are the
+oracle's restatement of the reference's Pole handlers) and compared, bitwise
+and for every Sync group,
+* with the reference's own Sync: the probe fixture (tests/golden/make_golden.py,
+  shell_probe) holds what it leaves in every point after the group's fields
+  were filled with their own point indices;
+* with the oracle's Sync in the reference's order on a state in mid-run."""
+import copy
+
 import numpy as np
+import pytest
 
 from conftest import load_golden
+from test_cpu_oracle_shell import build_shell_oracle, mhd_oracle
 
-from beta1_b200 import case, mhd, syncmap
+from beta1_b200 import case, mhd, physics, syncmap
+
+MASK = (1 << 40) - 1
 
 
-def test_shell_tables_equal_reference_sync():
+def shell_tables(n=(8, 6, 8)):
+    spec = case.shell_case(*n)
+    b = spec.blocks[0]
+    q, B = physics.farfield_state(spec.params)
+    u = [q[1] / q[0], q[2] / q[0], q[3] / q[0]]
+    E_inf = [B[1] * u[2] - B[2] * u[1], B[2] * u[0] - B[0] * u[2], B[0] * u[1] - B[1] * u[0]]
+    from beta1_b200 import geometry
+    lay = mhd.HostLayout([b.ncell])
+    maps = syncmap.compile_shell(lay, b.ncell, False, dict(qinf=q, B_imf=B, E_inf=E_inf),
+                                 geometry.block_ghost_mesh(b, 4))
+    return lay, maps
+
+
+@pytest.fixture(scope="module")
+def tables():
+    return shell_tables()
+
+
+def _points(o, names, ids):
+    ids = np.asarray(ids, dtype=np.int64)
+    fi = ids >> 56
+    for f in np.unique(fi):
+        sel = np.nonzero(fi == f)[0]
+        assert np.all(((ids[sel] >> 40) & 0xFFFF) == 0)
+        m, I, J, K = o.aos_points(names[f], 0, ids[sel] & MASK)
+        G = o.blocks[0].G
+        yield sel, o.blocks[0].f[names[f]], (m, I + G, J + G, K + G)
+
+
+def _read(o, names, ids):
+    v = np.empty(len(ids))
+    for sel, arr, idx in _points(o, names, ids):
+        v[sel] = arr[idx]
+    return v
+
+
+def _write(o, names, ids, v):
+    for sel, arr, idx in _points(o, names, ids):
+        arr[idx] = v[sel]
+
+
+def device_order_sync(o, names, group, t):
+    o.pole_rings(group)
+    _write(o, names, t["dst"], _read(o, names, t["src"]))
+    for (b, d) in t["walls"]:
+        o.wall_u(b, d)
+    _write(o, names, t["dst2"], _read(o, names, t["src2"]))
+    _write(o, names, t["cdst"], t["cval"])
+
+
+def test_table_structure(tables):
+    lay, maps = tables
+    assert set(maps) == set(syncmap.GROUPS) - set(syncmap.SHELL_SKIPPED)
+    for group, t in maps.items():
+        d1, s1, d2, s2 = t["dst"], t["src"], t["dst2"], t["src2"]
+        # every point is written once, and no source is written by a gather
+        allw = np.concatenate([d1, d2, t["cdst"]])
+        assert np.unique(allw).size == allw.size, group
+        assert np.intersect1d(np.concatenate([d1, d2]), np.concatenate([s1, s2])).size == 0, group
+        # only the wall handler's group has copies after it
+        assert (d2.size > 0) == bool(t["walls"]), group
+    assert maps["Ucell"]["walls"] == [(0, -1)]
+
+
+@pytest.fixture(scope="module")
+def shell_oracle_mid():
+    o = build_shell_oracle()
+    o.step()
+    return o
+
+
+@pytest.mark.parametrize("group", [g for g in syncmap.GROUPS if g not in syncmap.SHELL_SKIPPED])
+def test_device_order_equals_reference_sync(tables, shell_oracle_mid, group):
+    lay, maps = tables
+    names = [t[0] for t in lay.table]
     probe = load_golden("shell_8x6x8_probe.npz")
-    spec = case.shell_case(8, 6, 8)
-    lay = mhd.HostLayout([spec.blocks[0].ncell])
-    maps = syncmap.compile_shell(lay, spec.blocks[0].ncell, False)
-    assert set(maps) == set(syncmap.GROUPS) - set(syncmap.SHELL_POLE_HANDLED)
-    mask = (1 << 40) - 1
-    checked = 0
-    for group, m in maps.items():
-        for field in syncmap.GROUPS[group]:
-            fi = lay.index[field]
-            info = lay.field_info(field, 0)
-            size = int(np.prod([h - l for l, h in zip(info["lo"], info["hi"])])) * info["ncomp"]
-            ref = np.arange(size, dtype=np.float64) + 1.0
-            ref[probe["%s/%s/0/dst" % (group, field)]] = probe["%s/%s/0/val" % (group, field)]
-            pred = np.arange(size, dtype=np.float64) + 1.0
-            sel = (m["dst"] >> 56) == fi
-            dd, ss = m["dst"][sel] & mask, m["src"][sel] & mask
-            assert np.all((m["src"][sel] >> 56) == fi)
-            # sources are never destinations: one gather of pre-sync values
-            assert np.intersect1d(dd, ss).size == 0, (group, field)
-            pred[dd] = ss + 1.0
-            cs = (m["cdst"] >> 56) == fi
-            pred[m["cdst"][cs] & mask] = m["cval"][cs]
-            bad = np.nonzero(pred != ref)[0]
-            assert bad.size == 0, (group, field, bad.size)
-            checked += dd.size
-    assert checked > 10000
-
+    o = copy.deepcopy(build_shell_oracle())
+    blk = o.blocks[0]
+    for f in syncmap.GROUPS[group]:
+        loc, nc, ng = mhd_oracle.FIELDS[f]
+        p = mhd_oracle.PLUS[loc]
+        shape = tuple(blk.n[a] + p[a] + 2 * ng for a in range(3)) + (nc,)
+        blk.set_ref(f, (-ng, -ng, -ng), (np.arange(np.prod(shape), dtype=np.float64) + 1.0).reshape(shape))
+    device_order_sync(o, names, group, maps[group])
+    for f in syncmap.GROUPS[group]:
+        got = blk.get_ref(f).reshape(-1)
+        ref = np.arange(got.size, dtype=np.float64) + 1.0
+        ref[probe["%s/%s/0/dst" % (group, f)]] = probe["%s/%s/0/val" % (group, f)]
+        bad = np.nonzero(got != ref)[0]
+        assert bad.size == 0, (group, f, bad.size)
+    # in mid-run: the device order against the reference's order
+    a = copy.deepcopy(shell_oracle_mid)
+    b = copy.deepcopy(shell_oracle_mid)
+    a.sync(group)
+    device_order_sync(b, names, group, maps[group])
+    for f in syncmap.GROUPS[group]:
+        assert np.array_equal(a.blocks[0].get_ref(f), b.blocks[0].get_ref(f)), (group, f)
