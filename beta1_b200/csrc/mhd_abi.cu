@@ -70,9 +70,12 @@ struct SyncMap
     std::vector<uint64_t> hd, hs, hcd; // full tables (pool offsets) on the host
     std::vector<double> hcv;
     std::vector<std::pair<int, int>> walls; // (block, direction) of Solid_Surface fluid handlers
+    // Pole contexts: composed copies whose sources the wall handlers write
+    // (run after them)
+    std::vector<uint64_t> hd2, hs2;
     bool staged = false;
     bool built = false; // device lists match the host tables
-    CopyList full, hot;
+    CopyList full, hot, post;
     int *dwalls = nullptr;  // walls on the device (block, direction pairs)
     int64_t wall_cols = 0;  // boundary cell columns of the largest wall
 };
@@ -89,7 +92,7 @@ const char *const kKernelNames[] = {
     "k_zero",         "k_residual",    "k_ucontra",      "k_face_normals", "k_divb",          "k_eres_explicit",
     "k_bcell_jedge",  "k_fluid_ucontra", "k_wall_u_all",   "k_hall_cell",    "k_hall_edge",
     "k_pack_vec",     "k_hall_residual", "k_axpy_to",      "k_fd_quotient",  "k_negate",
-    "k_geom32",       "k_fluid_mixed",  "k_gmres_resist"};
+    "k_geom32",       "k_fluid_mixed",  "k_gmres_resist", "k_pole"};
 constexpr int kNumKernelNames = int(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
 
 } // namespace
@@ -143,6 +146,10 @@ struct mhd_ctx
     int *cta_tab = nullptr;
     int64_t cta_total[NKIND] = {0, 0, 0};
     std::map<std::string, SyncMap> syncs;
+    // eta Poles: (block, direction) pairs; a context with Poles runs every
+    // sync in the topology order of the Pole shell
+    std::vector<int> poles;
+    int *dpoles = nullptr;
     // materialisation state: groups whose last sync ran its hot list only,
     // and PV / U_plus computed on the first ghost layer only
     std::map<std::string, bool> dirty;
@@ -417,8 +424,49 @@ int apply_list(mhd_ctx *ctx, const CopyList &l)
     return gather_map(ctx, l);
 }
 
+// one Pole operation on every Pole of the context
+int launch_pole(mhd_ctx *ctx, int op)
+{
+    const int np = int(ctx->poles.size() / 2);
+    if (np == 0)
+        return MHD_OK;
+    int64_t w = 0;
+    for (int q = 0; q < np; ++q)
+    {
+        const BlockView &v = ctx->hbv[size_t(ctx->poles[size_t(2 * q)])];
+        w = std::max(w, pole_work(op, v.ni, v.nk));
+    }
+    prof_begin(ctx, "k_pole");
+    k_pole<<<dim3(grid_for(w), unsigned(np)), kThreads, 0, ctx->stream>>>(ctx->dbv, ctx->dpoles, op);
+    return launched(ctx);
+}
+
+// the values the Pole handlers of a group compute on the pole rings
+// (Z4_Lunar/src/boundary/Boundary_Build.cpp:61-269)
+int pole_rings(mhd_ctx *ctx, const std::string &group)
+{
+    if (group == "Ucell")
+        return launch_pole(ctx, POLE_RING_U);
+    if (group == "Bface")
+        return launch_pole(ctx, POLE_RING_BXI);
+    if (group == "B_cell")
+        return launch_pole(ctx, POLE_BCELL);
+    if (group == "Eedge")
+    {
+        RUN(launch_pole(ctx, POLE_EXI_AXIS));
+        return launch_pole(ctx, POLE_EETA_REG);
+    }
+    if (group == "Jedge")
+        return launch_pole(ctx, POLE_JETA);
+    return MHD_OK;
+}
+
 // LunarBoundary::Sync(group): phase A (fixed values, wall handlers), then
-// the composed copies; the hot lists unless `full`
+// the composed copies; the hot lists unless `full`.  In a context with
+// Poles: the topology order of the Pole shell -- the Pole rings, the copies
+// read before the wall handlers, the wall handlers, the copies of what they
+// wrote, then the fixed values -- always with the full lists (the Pole
+// repairs of the derived-field pass change sources of earlier syncs).
 int run_sync(mhd_ctx *ctx, const char *group, bool full = false)
 {
     auto it = ctx->syncs.find(group);
@@ -430,6 +478,28 @@ int run_sync(mhd_ctx *ctx, const char *group, bool full = false)
         if (ctx->capturing)
             return fail(ctx, MHD_ESTATE, "sync group %s changed during capture", group);
         RUN(build_sync(ctx, it->first, m));
+    }
+    if (!ctx->poles.empty())
+    {
+        RUN(pole_rings(ctx, it->first));
+        RUN(gather_map(ctx, m.full));
+        if (!m.walls.empty())
+        {
+            prof_begin(ctx, "k_wall_u_all");
+            k_wall_u_all<<<dim3(grid_for(m.wall_cols), unsigned(m.walls.size())), kThreads, 0, ctx->stream>>>(
+                ctx->dbv, m.dwalls, ctx->c.gamma);
+            RUN(launched(ctx));
+        }
+        RUN(gather_map(ctx, m.post));
+        if (m.full.nconst > 0)
+        {
+            prof_begin(ctx, "k_set_consts");
+            k_set_consts<<<grid_for(m.full.nconst), kThreads, 0, ctx->stream>>>(ctx->pool, m.full.cdst, m.full.cval,
+                                                                                 m.full.nconst);
+            RUN(launched(ctx));
+        }
+        ctx->dirty[it->first] = false;
+        return MHD_OK;
     }
     const CopyList &l = full ? m.full : m.hot;
     if (l.nconst > 0)
@@ -481,8 +551,12 @@ int ensure_geom(mhd_ctx *ctx)
 // stream beside PV's FP64 work).  Each sync runs after the pass that writes
 // its fields and before any pass that reads them; the reference's order
 // among these independent fields does not change any value.
+int launch_update_derived_pole(mhd_ctx *ctx);
+
 int launch_update_derived(mhd_ctx *ctx)
 {
+    if (!ctx->poles.empty())
+        return launch_update_derived_pole(ctx);
     cudaStream_t s = ctx->stream;
     prof_begin(ctx, "k_bcell_jedge");
     launch_k_bcell_jedge(ctx->tune[TUNE_k_bcell_jedge], grid_kind(ctx, KIND_STAG), s, ctx->dbv);
@@ -499,6 +573,35 @@ int launch_update_derived(mhd_ctx *ctx)
     launch_k_pv_uplus_dt(ctx->tune[TUNE_k_pv_uplus_dt], grid_kind(ctx, KIND_CELL1), s, ctx->dbv, ctx->c, ctx->dt_key, 1, 1);
     ctx->pv_dirty = true;
     RUN(launched(ctx));
+    RUN(run_sync(ctx, "J_cell"));
+    RUN(run_sync(ctx, "Uplus"));
+    return MHD_OK;
+}
+
+// UpdateDerivedFields_ with Poles, in the reference's order: calc_Bcell and
+// Sync("B_cell"), the B_zeta rewrite of the first cell layer at each Pole
+// (which the J edges then read), Calc_J_Edge and Sync("Jedge"), then J_cell
+// (with PV / U_plus / the CFL bound), its pole-shell repair, and the syncs
+int launch_update_derived_pole(mhd_ctx *ctx)
+{
+    cudaStream_t s = ctx->stream;
+    prof_begin(ctx, "k_bcell");
+    k_bcell<<<dim3(grid_for(max_box(ctx, LOC_CELL, 0)), unsigned(ctx->nblocks)), kThreads, 0, s>>>(ctx->dbv);
+    RUN(launched(ctx));
+    RUN(run_sync(ctx, "B_cell"));
+    RUN(launch_pole(ctx, POLE_BZETA));
+    prof_begin(ctx, "k_jedge");
+    k_jedge<<<grid_kind(ctx, KIND_STAG), kThreads, 0, s>>>(ctx->dbv, F_Bxi, F_Jxi, 1.0, nullptr);
+    RUN(launched(ctx));
+    RUN(run_sync(ctx, "Jedge"));
+    prof_begin(ctx, "k_arm_dt");
+    k_arm_dt<<<1, 128, 0, s>>>(ctx->dt_key, ctx->nruns);
+    RUN(launched(ctx));
+    prof_begin(ctx, "k_pv_uplus_dt");
+    launch_k_pv_uplus_dt(ctx->tune[TUNE_k_pv_uplus_dt], grid_kind(ctx, KIND_CELL1), s, ctx->dbv, ctx->c, ctx->dt_key, 1, 1);
+    ctx->pv_dirty = true;
+    RUN(launched(ctx));
+    RUN(launch_pole(ctx, POLE_JCELL));
     RUN(run_sync(ctx, "J_cell"));
     RUN(run_sync(ctx, "Uplus"));
     return MHD_OK;
@@ -1541,8 +1644,10 @@ int mhd_ctx_destroy(mhd_ctx *ctx)
     {
         free_list(kv.second.full);
         free_list(kv.second.hot);
+        free_list(kv.second.post);
         cudaFree(kv.second.dwalls);
     }
+    cudaFree(ctx->dpoles);
     free_resistive(ctx);
     cudaFree(ctx->hall_zb);
     mhd_set_hall_implicit(ctx, 0, nullptr, 0, nullptr, nullptr, nullptr, 0.0, 0.0, 0, 0.0, 1);
@@ -1947,6 +2052,7 @@ static bool hot_point(const mhd_ctx *ctx, const PoolDecoder &dec, uint64_t off)
 int build_sync(mhd_ctx *ctx, const std::string &group, SyncMap &m)
 {
     RUN(upload_list(ctx, m.full, m.hcd, m.hcv, m.hd, m.hs, m.staged));
+    RUN(upload_list(ctx, m.post, {}, {}, m.hd2, m.hs2, false));
     cudaFree(m.dwalls);
     m.dwalls = nullptr;
     m.wall_cols = 0;
@@ -2224,6 +2330,57 @@ int mhd_set_sync_consts(mhd_ctx *ctx, const char *group, const int64_t *dst, con
     return MHD_OK;
 }
 
+int mhd_set_sync_map_post(mhd_ctx *ctx, const char *group, const int64_t *dst, const int64_t *src, int64_t n)
+{
+    if (!ctx || !group || n < 0 || (n > 0 && (!dst || !src)))
+        return fail(ctx, MHD_EINVAL, "bad sync map arguments");
+    std::vector<uint64_t> d(static_cast<size_t>(n)), s(static_cast<size_t>(n));
+    for (int64_t t = 0; t < n; ++t)
+    {
+        const int64_t od = pool_offset(ctx, dst[t]);
+        const int64_t os = pool_offset(ctx, src[t]);
+        if (od < 0 || os < 0)
+            return fail(ctx, MHD_EINVAL, "sync map entry %lld has an invalid point id", (long long)t);
+        d[size_t(t)] = uint64_t(od);
+        s[size_t(t)] = uint64_t(os);
+    }
+    // one gather: no source may be a destination
+    std::vector<uint64_t> sorted_d(d);
+    std::sort(sorted_d.begin(), sorted_d.end());
+    for (int64_t t = 0; t < n; ++t)
+        if (std::binary_search(sorted_d.begin(), sorted_d.end(), s[size_t(t)]))
+            return fail(ctx, MHD_EINVAL, "post-wall copy %lld reads a point the same list writes", (long long)t);
+    SyncMap &m = ctx->syncs[group];
+    m.hd2.swap(d);
+    m.hs2.swap(s);
+    m.built = false;
+    drop_graph(ctx);
+    return MHD_OK;
+}
+
+int mhd_set_pole(mhd_ctx *ctx, int32_t block, int32_t direction)
+{
+    if (!ctx || block < 0 || block >= ctx->nblocks || (direction != -2 && direction != 2))
+        return fail(ctx, MHD_EINVAL, "bad Pole arguments (eta Poles: direction -2 or +2)");
+    const BlockView &v = ctx->hbv[size_t(block)];
+    if (v.nj < 2)
+        return fail(ctx, MHD_EINVAL, "a block with Poles needs at least two cells in j");
+    if (ctx->res.on || ctx->res_nsub > 0 || ctx->hall.n > 0)
+        return fail(ctx, MHD_ESTATE, "Poles are not available with the resistive or implicit Hall solves");
+    for (size_t q = 0; q < ctx->poles.size(); q += 2)
+        if (ctx->poles[q] == block && ctx->poles[q + 1] == direction)
+            return MHD_OK;
+    ctx->poles.push_back(block);
+    ctx->poles.push_back(direction);
+    cudaFree(ctx->dpoles);
+    ctx->dpoles = nullptr;
+    RUN(upload_vec(ctx, ctx->poles, &ctx->dpoles));
+    for (auto &kv : ctx->syncs)
+        kv.second.built = false;
+    drop_graph(ctx);
+    return MHD_OK;
+}
+
 int mhd_set_sync_wall(mhd_ctx *ctx, const char *group, int32_t block, int32_t direction)
 {
     if (!ctx || !group || block < 0 || block >= ctx->nblocks || direction == 0 || direction < -3 || direction > 3)
@@ -2241,6 +2398,8 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
         return fail(ctx, MHD_EINVAL, "bad resistive arguments");
     if (ctx->nruns > 1 && n > 0)
         return fail(ctx, MHD_ESTATE, "the implicit resistive solve is not available in a batch of runs (one shared dt per solve)");
+    if (!ctx->poles.empty() && n > 0)
+        return fail(ctx, MHD_ESTATE, "the resistive Pole handlers are not available");
     if (restart <= 0 || restart > kMaxRestart)
         return fail(ctx, MHD_EINVAL, "GMRES restart must be in [1, %d]", kMaxRestart);
     if (maxit < 0)
@@ -2432,6 +2591,8 @@ int mhd_set_hall_implicit(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, int6
         return fail(ctx, MHD_EINVAL, "bad implicit Hall arguments");
     if (ctx->nruns > 1 && n > 0)
         return fail(ctx, MHD_ESTATE, "the implicit Hall solve is not available in a batch of runs (one shared dt per solve)");
+    if (!ctx->poles.empty() && n > 0)
+        return fail(ctx, MHD_ESTATE, "the implicit Hall solve is not available with Poles");
     auto &H = ctx->hall;
     for (void *p : {(void *)H.e, (void *)H.alias, (void *)H.owner, (void *)H.sign, (void *)H.bstar, (void *)H.X,
                     (void *)H.F, (void *)H.Xt, (void *)H.Ft, (void *)H.dx, (void *)H.b, (void *)H.r, (void *)H.V,
@@ -2513,6 +2674,8 @@ int mhd_set_resistive_explicit(mhd_ctx *ctx, double inver_Rem, int32_t nsub)
         return fail(ctx, MHD_ESTATE, "the explicit resistive sub-cycling is not available in a batch of runs (one shared dt per solve)");
     if (nsub > 0 && ctx->res.on)
         return fail(ctx, MHD_ESTATE, "the implicit resistive solve is set up; the two are exclusive");
+    if (nsub > 0 && !ctx->poles.empty())
+        return fail(ctx, MHD_ESTATE, "the resistive Pole handlers are not available");
     ctx->res_nsub = nsub;
     ctx->res_inver_Rem = inver_Rem;
     // the hot sync lists depend on it (J_cell ghost depth)
@@ -2856,6 +3019,7 @@ int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
         prof_begin(ctx, "k_divb");
         k_divb<<<dim3(grid_for(max_box(ctx, LOC_CELL, 0)), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv);
         RUN(launched(ctx));
+        RUN(launch_pole(ctx, POLE_DIVB)); // the first cell layer next to a Pole: 0
         break;
     default:
         return fail(ctx, MHD_EINVAL, "unknown stage %d", stage_id);

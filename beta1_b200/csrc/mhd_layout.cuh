@@ -89,7 +89,10 @@ namespace mhd
     X(Eheta, "Ehall_eta", 5, 1, 4)                         \
     X(Ehzeta, "Ehall_zeta", 6, 1, 4)                       \
     X(Ehc, "Ehall_cell", 0, 3, 4)                          \
-    X(HallBeta, "hall_beta_cell", 0, 1, 4)
+    X(HallBeta, "hall_beta_cell", 0, 1, 4)                 \
+    X(Astarxi, "Astar_xi", 4, 1, 3)                        \
+    X(Astareta, "Astar_eta", 5, 1, 3)                      \
+    X(Astarzeta, "Astar_zeta", 6, 1, 3)
 
 enum FieldId : int
 {

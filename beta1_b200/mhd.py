@@ -64,6 +64,8 @@ _SIGS = {
     "mhd_sync": (C.c_int, [C.c_void_p, C.c_char_p]),
     "mhd_set_sync_consts": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64]),
     "mhd_set_sync_wall": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_int32]),
+    "mhd_set_sync_map_post": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64]),
+    "mhd_set_pole": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "mhd_set_resistive": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int32, C.c_int32]),
     "mhd_set_hall_implicit": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
@@ -247,6 +249,18 @@ class Context:
 
     def set_sync_wall(self, group: str, block: int, direction: int):
         self._check(self.lib.mhd_set_sync_wall(self.h, group.encode(), block, direction), f"set_sync_wall {group}")
+
+    def set_sync_map_post(self, group: str, dst: np.ndarray, src: np.ndarray):
+        """copies run after the group's wall handlers (contexts with Poles)"""
+        d = np.ascontiguousarray(dst, dtype=np.int64)
+        s = np.ascontiguousarray(src, dtype=np.int64)
+        assert d.shape == s.shape
+        self._check(self.lib.mhd_set_sync_map_post(self.h, group.encode(), d.ctypes.data, s.ctypes.data, d.size),
+                    f"set_sync_map_post {group}")
+
+    def set_pole(self, block: int, direction: int):
+        """an eta Pole (direction -2: j = 0, +2: j = n_j) of a block"""
+        self._check(self.lib.mhd_set_pole(self.h, block, direction), "set_pole")
 
     def set_resistive(self, unknowns, eta, alias, owner, sign, rtol, atol, maxit, restart=30):
         u = np.ascontiguousarray(unknowns, dtype=np.int64)

@@ -12,7 +12,7 @@ from . import edges, geometry, mhd, physics, rst, syncmap
 
 GEOM_FIELDS = ["Jac", "JDxi", "JDet", "JDze", "beta_xi", "beta_eta", "beta_zeta", "alpha_xi", "alpha_eta",
                "alpha_zeta", "dr_xi", "dr_eta", "dr_zeta", "Bcell_from_Bface_w", "Jcell_from_Jedge_w", "Area_xi",
-               "Area_eta", "Area_zeta", "dl_xi", "dl_eta", "dl_zeta"]
+               "Area_eta", "Area_zeta", "dl_xi", "dl_eta", "dl_zeta", "Astar_xi", "Astar_eta", "Astar_zeta"]
 
 _EDGE_PLUS = {0: (0, 1, 1), 1: (1, 0, 1), 2: (1, 1, 0)}
 
@@ -48,6 +48,34 @@ def hall_zero_boxes(ncell, patches):
                 out.append([ea] + lo + hi)
     return out
 STATE_FIELDS = ["U_H", "B_xi", "B_eta", "B_zeta"]
+
+
+def pole_directions(block) -> list:
+    """Directions of a block's eta Pole patches: -2 for the node plane j = 0,
+    +2 for j = n_j (the patch's node range is one plane in j)."""
+    out = []
+    for (ist, ied, jst, jed, kst, ked), name in block.physical:
+        if name != "Pole":
+            continue
+        if jst != jed or jst not in (0, block.ncell[1]):
+            raise ValueError("only Pole patches on a j face (eta Poles) are supported")
+        out.append(-2 if jst == 0 else 2)
+    return out
+
+
+def topology_patches(topology, ncell, block=None):
+    """(bc name, direction, node lo, node hi) of the physical patches the Hall
+    EMF zeroes next to: the Solid_Surface face i = 0 of the tiled slab and the
+    shell, and the shell's Poles."""
+    n = ncell
+    if topology not in ("tiled", "shell"):
+        return []
+    out = [("Solid_Surface", -1, (0, 0, 0), (1, n[1] + 1, n[2] + 1))]
+    if topology == "shell":
+        for d in pole_directions(block):
+            j = 0 if d < 0 else n[1]
+            out.append(("Pole", d, (0, j, 0), (n[0] + 1, j + 1, n[2] + 1)))
+    return out
 
 
 def make_params(p, precision=mhd.PREC_FP64) -> mhd.Params:
@@ -110,6 +138,8 @@ class Solver:
             self.sync_sizes = syncmap.install_periodic(self.ctx, spec.blocks[0].ncell)
         elif topology == "tiled":
             self.install_tiled()
+        elif topology == "shell":
+            self.install_shell()
         else:
             raise ValueError(f"unknown topology {topology}")
         self.ctx.sync("Badd")
@@ -163,9 +193,7 @@ class Solver:
         the periodic box has no physical patch."""
         rows = []
         for ib, b in enumerate(self.spec.blocks):
-            n = b.ncell
-            patches = [("Solid_Surface", -1, (0, 0, 0), (1, n[1] + 1, n[2] + 1))] if topology == "tiled" else []
-            rows += [[ib] + r for r in hall_zero_boxes(n, patches)]
+            rows += [[ib] + r for r in hall_zero_boxes(b.ncell, topology_patches(topology, b.ncell, b))]
         self.ctx.set_hall(physics.constants(self.spec.params)["hall_coef"], rows)
 
     def install_hall_implicit(self, topology, rtol=1e-8, atol=1e-50, maxit=50, ksp_rtol=1e-5, ksp_maxit=10000):
@@ -212,6 +240,22 @@ class Solver:
                 self.ctx.set_sync_wall(group, b, d)
             self.sync_sizes[group] = (int(m["dst"].size), int(m["cdst"].size), len(m["walls"]))
 
+    def install_shell(self):
+        """The single-block spherical shell: Solid_Surface and Farfield in i,
+        eta Poles at both ends of j, k periodic onto itself (ideal MHD)."""
+        spec = self.spec
+        if len(spec.blocks) != 1:
+            raise ValueError("a shell has one block")
+        p = spec.params
+        if p.get("is_Lunar_resistance", 0):
+            raise NotImplementedError("the resistive Pole handlers are not built")
+        key = ("shell_maps",)
+        if key not in self._cache:
+            self._cache[key] = shell_tables(spec, self.nodes[0], self.ctx)
+        self.sync_sizes = install_maps(self.ctx, self._cache[key])
+        for d in pole_directions(spec.blocks[0]):
+            self.ctx.set_pole(0, d)
+
     def load_state(self, state: rst.RestartFile):
         """Restart load + the syncs that make ghosts consistent, then
         UpdateDerivedFields_ (the state the first StepOnce starts from)."""
@@ -228,6 +272,36 @@ class Solver:
 
     def field(self, name, block=0) -> np.ndarray:
         return self.ctx.download(name, block)
+
+
+def farfield_consts(params):
+    """q_inf, B_imf and the zero-curl far-field EMF E_inf = -u_inf x B_imf"""
+    q, B = physics.farfield_state(params)
+    u = [q[1] / q[0], q[2] / q[0], q[3] / q[0]]
+    E_inf = [B[1] * u[2] - B[2] * u[1], B[2] * u[0] - B[0] * u[2], B[0] * u[1] - B[1] * u[0]]
+    return dict(qinf=q, B_imf=B, E_inf=E_inf)
+
+
+def shell_tables(spec: case_mod.CaseSpec, nodes, layout=None):
+    """Sync tables of a single-block shell (syncmap.compile_shell)."""
+    b = spec.blocks[0]
+    lay = layout if layout is not None else mhd.HostLayout([b.ncell])
+    return syncmap.compile_shell(lay, b.ncell, False, farfield_consts(spec.params), nodes)
+
+
+def install_maps(ctx, maps):
+    """Gives a context its compiled sync tables; returns the sizes per group."""
+    sizes = {}
+    for group, m in maps.items():
+        ctx.set_sync_map(group, m["dst"], m["src"])
+        if m.get("dst2") is not None and m["dst2"].size:
+            ctx.set_sync_map_post(group, m["dst2"], m["src2"])
+        if m["cdst"].size:
+            ctx.set_sync_consts(group, m["cdst"], m["cval"])
+        for (b, d) in m["walls"]:
+            ctx.set_sync_wall(group, b, d)
+        sizes[group] = (int(m["dst"].size), int(m["cdst"].size), len(m["walls"]))
+    return sizes
 
 
 def host_setup(spec: case_mod.CaseSpec, topology: Optional[str] = None):
@@ -254,6 +328,8 @@ def run_tables(spec: case_mod.CaseSpec, topology: str, nodes):
     lay = mhd.HostLayout([b.ncell for b in spec.blocks])
     if topology == "periodic":
         return syncmap.periodic_maps(lay, spec.blocks[0].ncell)
+    if topology == "shell":
+        return shell_tables(spec, nodes[0], lay)
     if topology != "tiled":
         raise ValueError(f"unknown topology {topology}")
     q, B = physics.farfield_state(spec.params)
@@ -274,7 +350,8 @@ class Batch:
     """Independent runs in one context (mhd_batch_create): a parameter sweep
     whose runs differ in grid size, inflow and IMF, each with its own time
     step, all advanced by one step graph.  runs: (case spec, topology) per
-    run, topology "periodic" (one block) or "tiled"; the runs must agree on
+    run, topology "periodic" (one block), "tiled" or "shell" (one block with
+    Poles; a batch with shells holds shells only); the runs must agree on
     the constants of the step (gamma, CFL, the J x B and state scales) and
     may not use the resistive or Hall solves.  host: optional iterable of
     the host_setup(spec, topology) results of the runs in order (e.g. from a
@@ -292,8 +369,12 @@ class Batch:
                 raise ValueError(f"runs of a batch must share the step constants; differing: {bad}")
             if spec.params.get("is_Lunar_resistance", 0):
                 raise ValueError("resistive runs cannot be batched")
-            if topo == "periodic" and len(spec.blocks) != 1:
-                raise ValueError("a periodic run has one block")
+            if topo in ("periodic", "shell") and len(spec.blocks) != 1:
+                raise ValueError(f"a {topo} run has one block")
+        shells = [topo == "shell" for _, topo in self.runs]
+        if any(shells) and not all(shells):
+            # a context with Poles runs every sync in the shell's order
+            raise ValueError("a batch with shells holds shells only")
         ncells, run_of, self.offset = [], [], []
         for r, (spec, _) in enumerate(self.runs):
             self.offset.append(len(ncells))
@@ -304,6 +385,7 @@ class Batch:
             host = (host_setup(spec, topo) for spec, topo in self.runs)
         per_run = []
         zero_rows = []
+        poles = []
         for r, ((spec, topo), (nodes, geom, maps)) in enumerate(zip(self.runs, host)):
             off = self.offset[r]
             q, B = physics.farfield_state(spec.params)
@@ -318,19 +400,15 @@ class Batch:
             per_run.append((maps, off))
             del nodes, geom
             for ib, b in enumerate(spec.blocks):
-                n = b.ncell
-                patches = [("Solid_Surface", -1, (0, 0, 0), (1, n[1] + 1, n[2] + 1))] if topo == "tiled" else []
-                zero_rows += [[off + ib] + row for row in hall_zero_boxes(n, patches)]
+                zero_rows += [[off + ib] + row for row in hall_zero_boxes(b.ncell, topology_patches(topo, b.ncell, b))]
+                if topo == "shell":
+                    for d in pole_directions(b):
+                        poles.append((off + ib, d))
             if precision == mhd.PREC_MIXED:
                 self.ctx.set_flux_reference(_farfield_prim(spec.params), run=r)
-        self.sync_sizes = {}
-        for group, m in syncmap.merge_runs(per_run).items():
-            self.ctx.set_sync_map(group, m["dst"], m["src"])
-            if m["cdst"].size:
-                self.ctx.set_sync_consts(group, m["cdst"], m["cval"])
-            for (b, d) in m["walls"]:
-                self.ctx.set_sync_wall(group, b, d)
-            self.sync_sizes[group] = (int(m["dst"].size), int(m["cdst"].size), len(m["walls"]))
+        self.sync_sizes = install_maps(self.ctx, syncmap.merge_runs(per_run))
+        for b, d in poles:
+            self.ctx.set_pole(b, d)
         self.ctx.sync("Badd")
         self.ctx.set_hall(c0["hall_coef"], zero_rows)
 

@@ -104,12 +104,12 @@ def merge_runs(per_run) -> Dict[str, dict]:
     out: Dict[str, dict] = {}
     for maps, off in per_run:
         for group, m in shift_blocks(maps, off).items():
-            o = out.setdefault(group, dict(dst=[], src=[], cdst=[], cval=[], walls=[]))
-            for k in ("dst", "src", "cdst", "cval"):
+            o = out.setdefault(group, dict(dst=[], src=[], dst2=[], src2=[], cdst=[], cval=[], walls=[]))
+            for k in ("dst", "src", "dst2", "src2", "cdst", "cval"):
                 o[k].append(m[k])
             o["walls"] += m["walls"]
     for o in out.values():
-        for k in ("dst", "src", "cdst"):
+        for k in ("dst", "src", "dst2", "src2", "cdst"):
             o[k] = np.concatenate(o[k]).astype(np.int64)
         o["cval"] = np.concatenate(o["cval"]).astype(np.float64)
     return out
@@ -119,7 +119,9 @@ def shift_blocks(maps: Dict[str, dict], off: int) -> Dict[str, dict]:
     """The tables of a layout whose blocks become blocks off, off + 1, ... of
     a larger context (point ids carry the block in bits 40-55)."""
     sh = np.int64(off) << np.int64(40)
-    return {g: dict(dst=m["dst"] + sh, src=m["src"] + sh, cdst=m["cdst"] + sh, cval=m["cval"],
+    none = np.zeros(0, dtype=np.int64)
+    return {g: dict(dst=m["dst"] + sh, src=m["src"] + sh, dst2=m.get("dst2", none) + sh,
+                    src2=m.get("src2", none) + sh, cdst=m["cdst"] + sh, cval=m["cval"],
                     walls=[(b + off, d) for (b, d) in m["walls"]]) for g, m in maps.items()}
 
 

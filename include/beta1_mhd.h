@@ -178,6 +178,25 @@ int mhd_set_sync_map(mhd_ctx *ctx, const char *group, const int64_t *dst, const 
 int mhd_set_sync_consts(mhd_ctx *ctx, const char *group, const int64_t *dst, const double *val, int64_t n);
 int mhd_set_sync_wall(mhd_ctx *ctx, const char *group, int32_t block, int32_t direction);
 
+/* Pole patches (the "Pole" boundary of Z4_Lunar/src/boundary/Boundary_Build.cpp:27-269)
+   on a block face j = 0 (direction -2) or j = n_j (direction +2) whose
+   ring runs around the k direction (k periodic onto itself).  From then on
+   every Sync of the context runs in the topology order of the Pole shell
+   (Pole, Pole, Farfield, Solid_Surface, Boundary_Sync_.cpp:4-65): the Pole
+   rings the handlers compute (BC_Pole_Cell_, BC_Pole_Bcell_Collapse_,
+   BC_Pole_Bface_Collapse_, BC_Pole_Eedge_Axis, BC_Pole_Eedge_RegulateK_Norm,
+   BC_Pole_Jedge_RegulateK_Norm), the composed copies of mhd_set_sync_map
+   (sources read after the rings, before the wall handlers), the wall
+   handlers, the copies of mhd_set_sync_map_post (sources the wall handlers
+   wrote), then the fixed values of mhd_set_sync_consts.  The derived-field
+   pass adds the Pole repairs of Z4_Lunar/src/physics/LunarSolver_Tools.cpp
+   (B_zeta of the first cell layer after Sync("B_cell"), :242-307; the
+   least-squares J_cell of the pole shell, :945-1090) and MHD_STAGE_DIVB
+   zeroes divB there (:729-772).  Needs the geometry field Astar_eta.  Not
+   available with the resistive or implicit Hall solves (MHD_ESTATE). */
+int mhd_set_pole(mhd_ctx *ctx, int32_t block, int32_t direction);
+int mhd_set_sync_map_post(mhd_ctx *ctx, const char *group, const int64_t *dst, const int64_t *src, int64_t n);
+
 /* Implicit resistive step (LunarSolver::SolveImplicitResistiveDiffusion_,
    Z4_Lunar/src/implicit/Lunar_ImplicitResistive.cpp:430-518, with the
    PETSc KSPSolve/MatShell of :95-124 replaced by a device GMRES): unknowns
@@ -304,7 +323,7 @@ int mhd_host_free(void *ptr);
 #define MHD_STAGE_FLUID_RHS 2  /* ZeroRHS_ + Scheme_U_ + AddSourceToRHS_Fluid -> RHS_H */
 #define MHD_STAGE_INDUCTION 3  /* AssembleRHS_Induction_CT_ -> Eface, E, RHS_B */
 #define MHD_STAGE_UPDATE 4     /* ApplyUpdate_Euler_ with the current dt */
-#define MHD_STAGE_DIVB 5       /* calc_divB -> divB (inner cells; no Pole patches) */
+#define MHD_STAGE_DIVB 5       /* calc_divB -> divB (inner cells; 0 next to a Pole) */
 #define MHD_STAGE_HALL_EMF 6   /* BuildHallFaceEMF_Rusanov_diff_ -> Ehall_xi/eta/zeta (see mhd_set_hall) */
 #define MHD_STAGE_HALL_SOLVE 7 /* ImplicitHallSolver::SolveOneStep at the current dt, then calc_Bcell */
 int mhd_stage(mhd_ctx *ctx, int32_t stage_id);

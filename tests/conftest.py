@@ -55,6 +55,21 @@ def slab_setup(g):
     return spec, st
 
 
+def shell_setup(g):
+    """(case spec, restart state) of the committed Pole-shell fixture."""
+    from beta1_b200 import case, rst
+    LOCS = {"U_H": rst.CELL, "B_xi": rst.FACE_XI, "B_eta": rst.FACE_ET, "B_zeta": rst.FACE_ZE}
+    spec = case.shell_case(*(int(v) for v in g["n"]))
+    st = rst.RestartFile(0, 0.0, 1, {})
+    for name, loc in LOCS.items():
+        rec = rst.FieldRecord(name, loc, 5 if name == "U_H" else 1, 4)
+        a = g["init/b0/%s" % name]
+        lo = tuple(int(v) for v in g["init/b0/%s__lo" % name])
+        rec.blocks.append(rst.FieldArray(lo, tuple(l + s for l, s in zip(lo, a.shape[:3])), a))
+        st.fields[name] = rec
+    return spec, st
+
+
 def periodic_setup(g):
     """(case spec, restart state) of the committed periodic fixture."""
     from beta1_b200 import case, rst

@@ -121,3 +121,33 @@ def test_device_order_equals_reference_sync(tables, shell_oracle_mid, group):
     device_order_sync(b, names, group, maps[group])
     for f in syncmap.GROUPS[group]:
         assert np.array_equal(a.blocks[0].get_ref(f), b.blocks[0].get_ref(f)), (group, f)
+
+
+def test_pole_directions_and_patches():
+    from beta1_b200 import solver
+    spec = case.shell_case(8, 6, 8)
+    b = spec.blocks[0]
+    assert solver.pole_directions(b) == [-2, 2]
+    pats = solver.topology_patches("shell", b.ncell, b)
+    assert [(p[0], p[1]) for p in pats] == [("Solid_Surface", -1), ("Pole", -2), ("Pole", 2)]
+    assert pats[2][2] == (0, 6, 0) and pats[2][3] == (9, 7, 9)
+    rows = solver.hall_zero_boxes(b.ncell, pats)
+    # the eta Poles zero the xi and zeta edges of their node planes
+    assert [0, 0, 0, 0, 8, 1, 9] in rows and [2, 0, 6, 0, 9, 7, 8] in rows
+    assert solver.topology_patches("periodic", b.ncell, b) == []
+
+
+def test_batch_of_shells_merges_every_list():
+    from beta1_b200 import geometry, solver
+    specs = [case.shell_case(6, 4, 6), case.shell_case(8, 6, 8)]
+    lays = [mhd.HostLayout([s.blocks[0].ncell]) for s in specs]
+    per_run = [(solver.shell_tables(s, geometry.block_ghost_mesh(s.blocks[0], 4), lay), r)
+               for r, (s, lay) in enumerate(zip(specs, lays))]
+    merged = syncmap.merge_runs(per_run)
+    for group in merged:
+        for key in ("dst", "src", "dst2", "src2", "cdst"):
+            assert merged[group][key].size == sum(m[group][key].size for m, _ in per_run), (group, key)
+        blocks = (merged[group]["dst2"] >> 40) & 0xFFFF
+        assert set(blocks.tolist()) <= {0, 1}
+    assert merged["Ucell"]["walls"] == [(0, -1), (1, -1)]
+    assert set(((merged["Ucell"]["dst2"] >> 40) & 0xFFFF).tolist()) == {0, 1}
