@@ -21,8 +21,11 @@ Workloads (--workload):
   MT19937_64(5) (beta1_b200.case.sweep_cases; 14.7 M cells in all), ideal
   MHD, each run with its own time step; mixed precision unless --precision
   fp64.  Host geometry is built by a spawned process pool.
+* c5s: the same sweep (same draws) with every run a single-block spherical
+  shell of Nr x Nt x Nph cells (Nph = Nt rounded up to even) with Pole
+  patches at both ends of theta (case.sweep_cases(grid="shell")).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload c2|c1|c5]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload c2|c1|c5|c5s|c3|c4]
                     [--precision fp64|mixed]
 
 Multi-GPU (torchrun): the path does not shard, so N ranks run N independent
@@ -142,10 +145,12 @@ WORKLOADS = {
     "c2": dict(name="c2_slab6x96x48x48_implicit_resistive_fp64", ref_steps=4, ref_rss_gb=12.0),
     "c1": dict(name="c1_periodic_64cubed_fp64", ref_steps=40, ref_rss_gb=1.0),
     "c5": dict(name="c5_sweep48_slab_runs_mixed", ref_steps=2, ref_rss_gb=4.0),
+    "c5s": dict(name="c5s_sweep48_shell_runs_mixed", ref_steps=2, ref_rss_gb=4.0),
     "c3": dict(name="c3_slab6x128x64x64_hall_implicit_fp64", ref_steps=1, ref_rss_gb=4.0),
     "c4": dict(name="c4_slab6x128x64x64_hall_implicit_mixed", ref_steps=1, ref_rss_gb=4.0),
 }
 SWEEP_RUNS = 48
+SWEEP_GRID = {"c5": ("slab", "tiled"), "c5s": ("shell", "shell")}  # sweep workload -> (grid, topology)
 HALL_SAMPLE = ("6 blocks of 64 x 32 x 32 cells (the same layout at half the cells per direction), StepOnce "
                "followed by the reference's implicit Hall solve (SolveOneStep, Newton rtol 1e-10) and calc_Bcell")
 
@@ -246,7 +251,7 @@ def cpu_reference(workload, n, steps, nproc):
         shutil.rmtree(d, ignore_errors=True)
 
 
-def cpu_reference_sweep(steps, nproc, nruns=SWEEP_RUNS):
+def cpu_reference_sweep(steps, nproc, nruns=SWEEP_RUNS, grid="slab"):
     """The reference's StepOnce loop on a sample of the sweep's runs: the
     first `nproc` runs (bounded by host cores and memory), one
     single-threaded process per run, concurrently; returns aggregate
@@ -254,7 +259,7 @@ def cpu_reference_sweep(steps, nproc, nruns=SWEEP_RUNS):
     from beta1_b200 import case, rst
     if not os.path.exists(REF_BIN):
         return None
-    runs = case.sweep_cases(nruns)
+    runs = case.sweep_cases(nruns, grid=grid)
     nproc = max(1, min(nproc, len(runs), int(0.6 * mem_available_gb() / WORKLOADS["c5"]["ref_rss_gb"])))
     d = tempfile.mkdtemp(prefix="b1sweep_")
     try:
@@ -282,16 +287,17 @@ def cpu_reference_sweep(steps, nproc, nruns=SWEEP_RUNS):
 SWEEP_SEED0 = 5000
 
 
-def build_sweep(precision, nruns=SWEEP_RUNS):
-    """The c5 batch: host geometry of every run from a spawned process pool
+def build_sweep(precision, nruns=SWEEP_RUNS, workload="c5"):
+    """The sweep batch: host geometry of every run from a spawned process pool
     (bounded by cores and memory), uploaded run by run as it arrives."""
     import multiprocessing as mp
     from beta1_b200 import case, solver
-    runs = case.sweep_cases(nruns)
+    grid, topo = SWEEP_GRID[workload]
+    runs = case.sweep_cases(nruns, grid=grid)
     nproc = max(1, min(len(runs), os.cpu_count() or 1, 16, int(mem_available_gb() / 8.0)))
     with mp.get_context("spawn").Pool(nproc) as pool:
-        host = pool.imap(solver.host_setup_run, [(spec, "tiled") for spec, _ in runs])
-        bt = solver.Batch([(spec, "tiled") for spec, _ in runs], precision=precision, host=host)
+        host = pool.imap(solver.host_setup_run, [(spec, topo) for spec, _ in runs])
+        bt = solver.Batch([(spec, topo) for spec, _ in runs], precision=precision, host=host)
     bt.load_states([case.inflow_state(spec, seed=SWEEP_SEED0 + r) for r, (spec, _) in enumerate(runs)])
     return bt, sum(bt.cells), runs
 
@@ -302,16 +308,16 @@ def run_reference_arm(args):
         return 0
     wl = WORKLOADS[args.workload]
     steps = min(args.steps, args.ref_steps or wl["ref_steps"])
-    if args.workload == "c5":
-        res = cpu_reference_sweep(steps, os.cpu_count() or 1)
+    if args.workload in SWEEP_GRID:
+        res = cpu_reference_sweep(steps, os.cpu_count() or 1, grid=SWEEP_GRID[args.workload][0])
     else:
         res = cpu_reference(args.workload, args.n, steps, os.cpu_count() or 1)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_lunar not built or failed"}))
         return 0
     agg, vals, nproc = res
-    cells = vals[0]["cells"] if args.workload != "c5" else sum(v["cells"] for v in vals)
-    if args.workload == "c5":
+    cells = vals[0]["cells"] if args.workload not in SWEEP_GRID else sum(v["cells"] for v in vals)
+    if args.workload in SWEEP_GRID:
         sample = "%s: the first %d runs of the sweep, one single-threaded process each, %d StepOnce per " \
                  "process, concurrently (bounded by host cores and memory)" % (wl["name"], nproc, steps)
     elif args.workload in ("c3", "c4"):
@@ -354,9 +360,9 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     if args.steps is None:
-        args.steps = {"c2": 200, "c1": 4000, "c5": 100, "c3": 10, "c4": 10}[args.workload]
+        args.steps = {"c2": 200, "c1": 4000, "c5": 100, "c5s": 100, "c3": 10, "c4": 10}[args.workload]
     if args.precision is None:
-        args.precision = "mixed" if args.workload in ("c5", "c4") else "fp64"
+        args.precision = "mixed" if args.workload in ("c5", "c5s", "c4") else "fp64"
 
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -377,8 +383,8 @@ def main():
     wl = WORKLOADS[args.workload]
     mixed = args.precision == "mixed"
     prec = mhd.PREC_MIXED if mixed else mhd.PREC_FP64
-    if args.workload == "c5":
-        s, cells, sweep = build_sweep(prec)
+    if args.workload in SWEEP_GRID:
+        s, cells, sweep = build_sweep(prec, workload=args.workload)
         spec = None
         nblocks = len(sweep)
     else:
@@ -482,8 +488,8 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ref_steps = args.ref_steps or wl["ref_steps"]
-        if args.workload == "c5":
-            res = cpu_reference_sweep(ref_steps, 1)
+        if args.workload in SWEEP_GRID:
+            res = cpu_reference_sweep(ref_steps, 1, grid=SWEEP_GRID[args.workload][0])
             if res is not None:
                 cpu = {"value": res[0], "unit": "cell-updates/s", "cores": 1, "kind": "reference",
                        "sample": "%s, run 0 of the sweep (%d cells), %d StepOnce of the reference solver built "

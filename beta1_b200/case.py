@@ -675,14 +675,19 @@ class MT19937_64:
         return lo + (hi - lo) * ((self.next() >> 11) * 2.0 ** -53)
 
 
-def sweep_cases(nruns: int = 48, seed: int = 5, nr=(32, 128), nt=(24, 96), mach=(4.0, 12.0), angle=(0.0, 180.0)):
+def sweep_cases(nruns: int = 48, seed: int = 5, nr=(32, 128), nt=(24, 96), mach=(4.0, 12.0), angle=(0.0, 180.0),
+                grid: str = "slab"):
     """Runs of a parameter sweep: per run (drawn in this order from
-    MT19937_64(seed)) radial cells Nr, transverse cells Nt (the block is
-    Nr x Nt x Nt), inflow speed `mach` (v = (-mach, 0, 0) in units of the
-    reference speed) and IMF clock angle theta in degrees, B = 0.5 (0,
-    cos theta, sin theta).  Each run is one slab block between a
-    Solid_Surface and a Farfield, periodic onto itself transversally.
-    Returns [(spec, dict of the drawn values)]."""
+    MT19937_64(seed)) radial cells Nr, transverse cells Nt, inflow speed
+    `mach` (v = (-mach, 0, 0) in units of the reference speed) and IMF clock
+    angle theta in degrees, B = 0.5 (0, cos theta, sin theta).  grid "slab":
+    each run is one Nr x Nt x Nt slab block between a Solid_Surface and a
+    Farfield, periodic onto itself transversally; grid "shell": one
+    spherical shell of Nr x Nt x Nph cells with Pole patches (shell_case),
+    Nph = Nt rounded up to even (the Pole's ghost rows pair phi with
+    phi + pi).  Returns [(spec, dict of the drawn values)]."""
+    if grid not in ("slab", "shell"):
+        raise ValueError(f"unknown sweep grid {grid}")
     g = MT19937_64(seed)
     out = []
     for _ in range(nruns):
@@ -691,6 +696,9 @@ def sweep_cases(nruns: int = 48, seed: int = 5, nr=(32, 128), nt=(24, 96), mach=
         m = g.real(*mach)
         th = g.real(*angle)
         B = (0.0, 0.5 * math.cos(math.radians(th)), 0.5 * math.sin(math.radians(th)))
-        spec = slab_case(n_r, (n_t, n_t), (1, 1), mach_u=m, B=B)
+        if grid == "shell":
+            spec = shell_case(n_r, n_t, n_t + (n_t & 1), mach_u=m, B=B)
+        else:
+            spec = slab_case(n_r, (n_t, n_t), (1, 1), mach_u=m, B=B)
         out.append((spec, dict(nr=n_r, nt=n_t, mach=m, angle=th)))
     return out

@@ -73,3 +73,17 @@ def test_merged_tables_address_each_runs_own_blocks():
     assert lay.point_base("U_H", 4) == syncmap.shift_blocks({"g": dict(
         dst=np.array([mhd.HostLayout([(1, 1, 1)]).point_base("U_H", 0)]), src=np.zeros(1, np.int64),
         cdst=np.zeros(0, np.int64), cval=np.zeros(0), walls=[])}, 4)["g"]["dst"][0]
+
+
+def test_shell_sweep_same_draws():
+    """grid="shell": the same draws, each run a spherical shell with Poles and
+    an even azimuthal cell count (Nt rounded up)."""
+    from beta1_b200 import case, solver
+    slab = case.sweep_cases(6)
+    shell = case.sweep_cases(6, grid="shell")
+    for (sp_a, va), (sp_b, vb) in zip(slab, shell):
+        assert va == vb
+        n = sp_b.blocks[0].ncell
+        assert n == (va["nr"], va["nt"], va["nt"] + (va["nt"] & 1))
+        assert solver.pole_directions(sp_b.blocks[0]) == [-2, 2]
+        assert sp_b.params["INITIAL"] == sp_a.params["INITIAL"]
