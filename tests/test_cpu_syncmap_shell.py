@@ -151,3 +151,51 @@ def test_batch_of_shells_merges_every_list():
         assert set(blocks.tolist()) <= {0, 1}
     assert merged["Ucell"]["walls"] == [(0, -1), (1, -1)]
     assert set(((merged["Ucell"]["dst2"] >> 40) & 0xFFFF).tolist()) == {0, 1}
+
+
+def test_device_order_steps_equal_reference(tables):
+    """Two StepOnce with every Sync in the device order (compiled tables) and
+    the device's derived-field order: the reference's fields bitwise."""
+    lay, maps = tables
+    names = [t[0] for t in lay.table]
+
+    class DeviceOrder(mhd_oracle.ShellOracle):
+        def sync(self, group):
+            device_order_sync(self, names, group, maps[group])
+
+        def update_magnetic_derived(self):
+            # k_bcell, Sync, B_zeta rewrite, k_jedge, Sync, J_cell, its ring, Sync
+            blk = self.blocks[0]
+            self.calc_bcell(blk)
+            self.sync("B_cell")
+            self.bzeta_pole_rewrite()
+            self.curl_adj(blk, ("B_xi", "B_eta", "B_zeta"), ("J_xi", "J_eta", "J_zeta"))
+            self.sync("Jedge")
+            self.calc_jcell(blk)
+            self.jcell_pole_repair()
+            self.sync("J_cell")
+
+    ref = build_shell_oracle()
+    o = DeviceOrder.__new__(DeviceOrder)
+    o.__dict__.update(copy.deepcopy(ref.__dict__))
+    # restart load through the device order
+    g = load_golden("shell_8x6x8_steps.npz")
+    from conftest import shell_setup
+    spec, st = shell_setup(g)
+    for name in ("U_H", "B_xi", "B_eta", "B_zeta"):
+        fa = st.fields[name].blocks[0]
+        o.blocks[0].set_ref(name, fa.lo, fa.data)
+    o.sync("Ucell")
+    o.sync("Bface")
+    o.update_derived()
+    for s in (0, 1, 2):
+        if s:
+            assert o.step() == float(g["s%d/dt" % s])
+        o.calc_divb()
+        for key in g.files:
+            if not key.startswith("s%d/b0/" % s) or key.endswith("__lo"):
+                continue
+            f = key.split("/")[-1]
+            if s == 0 and f.startswith(("E", "RHS")):
+                continue
+            assert np.array_equal(o.blocks[0].get_ref(f), g[key]), (s, f)
