@@ -2,6 +2,7 @@
 #pragma once
 
 #include "mhd_layout.cuh"
+#include "mhd_pole.cuh"
 #include "../../include/beta1_mhd.h"
 
 namespace mhd
@@ -36,48 +37,9 @@ __global__ void k_bcell(const BlockView *bvs);
 __global__ void k_jedge(const BlockView *bvs, int fB0, int fJ0, double mult, const int *rng);
 __global__ void k_jcell(const BlockView *bvs);
 
-// Pole handlers and repairs on eta Poles (block faces j = 0 or j = n_j whose
-// axis is the k direction): per Pole a (block, direction) pair in `poles`,
-// one grid row per Pole
-enum PoleOp : int
-{
-    POLE_RING_U = 0, // U_H: k average of the first cell layer
-    POLE_RING_BXI,   // B_xi: k average of the first layer
-    POLE_BCELL,      // B_cell and Bind_cell: least-squares collapse of the ring
-    POLE_EXI_AXIS,   // E_xi on the pole line: -u_plus x B_cell . dr_xi
-    POLE_EETA_REG,   // E_eta: regulation of the ring by one Cartesian vector
-    POLE_JETA,       // J_eta: (dl / A*) times the circulation of beta_zeta B_zeta
-    POLE_BZETA,      // B_zeta of the first cell layer: flux of Bind_cell
-    POLE_JCELL,      // J_cell of the first cell layer: least-squares ring vector
-    POLE_DIVB,       // divB of the first cell layer: 0
-    NPOLE_OP
-};
+// Pole handlers and repairs on eta Poles (mhd_pole.cuh): per Pole a
+// (block, direction) pair in `poles`, one grid row per Pole
 __global__ void k_pole(const BlockView *bvs, const int *poles, int op);
-// threads one Pole of a block with (ni, nj, nk) cells needs for an operation
-__host__ __device__ inline int64_t pole_work(int op, int ni, int nk)
-{
-    switch (op)
-    {
-    case POLE_RING_U:
-        return int64_t(ni) * 5;
-    case POLE_RING_BXI:
-    case POLE_EETA_REG:
-        return ni + 1;
-    case POLE_BCELL:
-        return int64_t(ni) * 2;
-    case POLE_EXI_AXIS:
-    case POLE_BZETA:
-        return int64_t(ni) * (nk + 1);
-    case POLE_JETA:
-        return int64_t(ni + 1) * (nk + 1);
-    case POLE_JCELL:
-        return ni;
-    case POLE_DIVB:
-        return int64_t(ni) * nk;
-    default:
-        return 0;
-    }
-}
 __global__ void k_begin_step(const unsigned long long *dt_key, double *dt, int *err, double dt_abort, int nruns);
 __global__ void k_arm_dt(unsigned long long *dt_key, int nruns);
 __global__ void k_end_step(const double *dt, double *time, long long *step, int nruns);
