@@ -92,7 +92,8 @@ const char *const kKernelNames[] = {
     "k_zero",         "k_residual",    "k_ucontra",      "k_face_normals", "k_divb",          "k_eres_explicit",
     "k_bcell_jedge",  "k_fluid_ucontra", "k_wall_u_all",   "k_hall_cell",    "k_hall_edge",
     "k_pack_vec",     "k_hall_residual", "k_axpy_to",      "k_fd_quotient",  "k_negate",
-    "k_geom32",       "k_fluid_mixed",  "k_gmres_resist", "k_pole"};
+    "k_geom32",       "k_fluid_mixed",  "k_gmres_resist", "k_pole",
+    "k_geometry"};
 constexpr int kNumKernelNames = int(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
 
 } // namespace
@@ -2354,6 +2355,39 @@ int mhd_set_sync_map_post(mhd_ctx *ctx, const char *group, const int64_t *dst, c
     m.hd2.swap(d);
     m.hs2.swap(s);
     m.built = false;
+    drop_graph(ctx);
+    return MHD_OK;
+}
+
+int mhd_build_geometry(mhd_ctx *ctx, int32_t block, const double *nodes, int64_t count, const double *B_imf)
+{
+    if (!ctx || block < 0 || block >= ctx->nblocks || !nodes)
+        return fail(ctx, MHD_EINVAL, "bad geometry arguments");
+    if (ctx->capturing)
+        return fail(ctx, MHD_ESTATE, "geometry changed during capture");
+    const BlockView &v = ctx->hbv[size_t(block)];
+    const int off = ctx->G + 1;
+    NodeMesh m{nullptr, off, v.nj + 1 + 2 * off, v.nk + 1 + 2 * off};
+    const int64_t want = int64_t(v.ni + 1 + 2 * off) * m.NJ * m.NK * 3;
+    if (count != want)
+        return fail(ctx, MHD_EINVAL, "node mesh of block %d: %lld values, expected %lld", block, (long long)count,
+                    (long long)want);
+    RUN(ensure_staging(ctx, size_t(count)));
+    CK(ctx, cudaMemcpyAsync(ctx->staging, nodes, size_t(count) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    m.a = ctx->staging;
+    prof_begin(ctx, "k_geometry");
+    k_geometry<<<dim3(grid_for(v.vol), GEOM_BADD), kThreads, 0, ctx->stream>>>(ctx->dbv, block, m, ctx->G, 0, 0.0,
+                                                                                  0.0, 0.0);
+    RUN(launched(ctx));
+    if (B_imf && (B_imf[0] != 0.0 || B_imf[1] != 0.0 || B_imf[2] != 0.0))
+    {
+        prof_begin(ctx, "k_geometry");
+        k_geometry<<<dim3(grid_for(v.vol), 1), kThreads, 0, ctx->stream>>>(ctx->dbv, block, m, ctx->G, GEOM_BADD,
+                                                                             B_imf[0], B_imf[1], B_imf[2]);
+        RUN(launched(ctx));
+    }
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->geom_dirty = true;
     drop_graph(ctx);
     return MHD_OK;
 }

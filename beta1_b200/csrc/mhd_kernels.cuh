@@ -3,6 +3,7 @@
 
 #include "mhd_layout.cuh"
 #include "mhd_pole.cuh"
+#include "mhd_geom.cuh"
 #include "../../include/beta1_mhd.h"
 
 namespace mhd
@@ -40,6 +41,8 @@ __global__ void k_jcell(const BlockView *bvs);
 // Pole handlers and repairs on eta Poles (mhd_pole.cuh): per Pole a
 // (block, direction) pair in `poles`, one grid row per Pole
 __global__ void k_pole(const BlockView *bvs, const int *poles, int op);
+__global__ void k_geometry(const BlockView *bvs, int blk, NodeMesh m, int G, int group0, double b0, double b1,
+                           double b2);
 __global__ void k_begin_step(const unsigned long long *dt_key, double *dt, int *err, double dt_abort, int nruns);
 __global__ void k_arm_dt(unsigned long long *dt_key, int nruns);
 __global__ void k_end_step(const double *dt, double *time, long long *step, int nruns);

@@ -1750,6 +1750,22 @@ int launch_k_eedge(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs
     return 0;
 }
 
+// Geometry of one block from its ghost node mesh (mhd_geom.cuh): one thread
+// per point of the padded box, one grid row per group (group0, group0 + 1, ...)
+__global__ void k_geometry(const BlockView *__restrict__ bvs, int blk, NodeMesh m, int G, int group0, double b0,
+                           double b1, double b2)
+{
+    const BlockView &b = bvs[blk];
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= b.vol)
+        return;
+    const int k = int(t % b.NK) - b.G;
+    const int j = int((t / b.NK) % b.NJ) - b.G;
+    const int i = int(t / (int64_t(b.NK) * b.NJ)) - b.G;
+    const double gb[3] = {b0, b1, b2};
+    geom_point(m, b, group0 + int(blockIdx.y), i, j, k, G, gb);
+}
+
 // Pole handlers and repairs: one thread per pole_one work item (mhd_pole.cuh)
 __global__ void k_pole(const BlockView *__restrict__ bvs, const int *__restrict__ poles, int op)
 {

@@ -66,6 +66,7 @@ _SIGS = {
     "mhd_set_sync_wall": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_int32]),
     "mhd_set_sync_map_post": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64]),
     "mhd_set_pole": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+    "mhd_build_geometry": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p]),
     "mhd_set_resistive": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int32, C.c_int32]),
     "mhd_set_hall_implicit": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
@@ -257,6 +258,17 @@ class Context:
         assert d.shape == s.shape
         self._check(self.lib.mhd_set_sync_map_post(self.h, group.encode(), d.ctypes.data, s.ctypes.data, d.size),
                     f"set_sync_map_post {group}")
+
+    def build_geometry(self, block: int, nodes: np.ndarray, B_imf=None):
+        """every geometry field of a block from its ghost node mesh, on the
+        device (nodes: the Padded array of geometry.block_ghost_mesh)"""
+        a = np.ascontiguousarray(nodes, dtype=np.float64)
+        bp = None
+        if B_imf is not None:
+            bv = np.ascontiguousarray(B_imf, dtype=np.float64)
+            assert bv.size == 3
+            bp = bv.ctypes.data
+        self._check(self.lib.mhd_build_geometry(self.h, block, a.ctypes.data, a.size, bp), "build_geometry")
 
     def set_pole(self, block: int, direction: int):
         """an eta Pole (direction -2: j = 0, +2: j = n_j) of a block"""

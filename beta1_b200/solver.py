@@ -99,19 +99,27 @@ _HOST_CACHE: dict = {}
 
 
 class Solver:
-    def __init__(self, spec: case_mod.CaseSpec, topology: str = "periodic", precision=mhd.PREC_FP64):
+    def __init__(self, spec: case_mod.CaseSpec, topology: str = "periodic", precision=mhd.PREC_FP64,
+                 geometry_on: str = "host"):
+        """geometry_on: "host" builds the geometry fields with beta1_b200.geometry
+        and uploads them; "device" sends only the ghost node meshes and builds
+        them with mhd_build_geometry (the same values)."""
+        if geometry_on not in ("host", "device"):
+            raise ValueError(f"unknown geometry builder {geometry_on}")
         self.spec = spec
         ngg = int(spec.params["ngg"])
         self.ctx = mhd.Context([b.ncell for b in spec.blocks], make_params(spec.params, precision))
         cache = _HOST_CACHE.get(id(spec))
         if cache is None or cache["spec"] is not spec:
-            cache = {"spec": spec, "geom": [], "nodes": []}
+            cache = {"spec": spec, "geom": [None] * len(spec.blocks), "nodes": []}
             for b in spec.blocks:
-                X = geometry.block_ghost_mesh(b, ngg)
-                cache["nodes"].append(X)
-                cache["geom"].append(geometry.build(X, b.ncell, ngg))
+                cache["nodes"].append(geometry.block_ghost_mesh(b, ngg))
             _HOST_CACHE.clear()
             _HOST_CACHE[id(spec)] = cache
+        if geometry_on == "host":
+            for ib, b in enumerate(spec.blocks):
+                if cache["geom"][ib] is None:
+                    cache["geom"][ib] = geometry.build(cache["nodes"][ib], b.ncell, ngg)
         self._cache = cache
         if precision == mhd.PREC_MIXED:
             q0, _ = physics.farfield_state(spec.params)
@@ -124,13 +132,16 @@ class Solver:
         _, B_imf = physics.farfield_state(spec.params)
         for ib, b in enumerate(spec.blocks):
             X = cache["nodes"][ib]
-            g = cache["geom"][ib]
-            for name in GEOM_FIELDS:
-                lo, hi, a = g[name]
-                self.ctx.upload(name, ib, a)
-            if any(v != 0.0 for v in B_imf):
-                for fname, jd in (("Badd_xi", "JDxi"), ("Badd_eta", "JDet"), ("Badd_zeta", "JDze")):
-                    self.ctx.upload(fname, ib, badd_faces(g[jd][2], B_imf))
+            g = cache["geom"][ib] if geometry_on == "host" else None
+            if g is None:
+                self.ctx.build_geometry(ib, X.a, B_imf)
+            else:
+                for name in GEOM_FIELDS:
+                    lo, hi, a = g[name]
+                    self.ctx.upload(name, ib, a)
+                if any(v != 0.0 for v in B_imf):
+                    for fname, jd in (("Badd_xi", "JDxi"), ("Badd_eta", "JDet"), ("Badd_zeta", "JDze")):
+                        self.ctx.upload(fname, ib, badd_faces(g[jd][2], B_imf))
             self.geom.append(g)
             self.nodes.append(X)
         if topology == "periodic":
@@ -304,22 +315,23 @@ def install_maps(ctx, maps):
     return sizes
 
 
-def host_setup(spec: case_mod.CaseSpec, topology: Optional[str] = None):
-    """Host-side set-up of a case: per block the ghost node mesh and the
-    geometry fields, and (given the topology) the run's sync tables compiled
-    on its own blocks 0, 1, ...  A pure function of the case, safe to run in
-    worker processes.  Returns (nodes, geom, tables or None)."""
+def host_setup(spec: case_mod.CaseSpec, topology: Optional[str] = None, geometry_on: str = "host"):
+    """Host-side set-up of a case: per block the ghost node mesh and (unless
+    the device builds it) the geometry fields, and (given the topology) the
+    run's sync tables compiled on its own blocks 0, 1, ...  A pure function
+    of the case, safe to run in worker processes.  Returns (nodes, geom, tables
+    or None); geom holds None per block when geometry_on is "device"."""
     ngg = int(spec.params["ngg"])
     nodes, geom = [], []
     for b in spec.blocks:
         X = geometry.block_ghost_mesh(b, ngg)
         nodes.append(X)
-        geom.append(geometry.build(X, b.ncell, ngg))
+        geom.append(geometry.build(X, b.ncell, ngg) if geometry_on == "host" else None)
     return nodes, geom, (run_tables(spec, topology, nodes) if topology else None)
 
 
 def host_setup_run(run):
-    """host_setup of a (spec, topology) pair (process-pool entry)"""
+    """host_setup of a (spec, topology[, geometry_on]) tuple (process-pool entry)"""
     return host_setup(*run)
 
 
@@ -355,11 +367,13 @@ class Batch:
     the constants of the step (gamma, CFL, the J x B and state scales) and
     may not use the resistive or Hall solves.  host: optional iterable of
     the host_setup(spec, topology) results of the runs in order (e.g. from a
-    process pool); each is uploaded and released as it arrives."""
+    process pool); each is uploaded and released as it arrives.  A run whose
+    host set-up holds no geometry (host_setup(..., geometry_on="device")) has
+    it built on the device from its node mesh."""
 
     CONSTS = ("gamma", "cfl", "inver_MA2", "momentum_hall_coeff", "state_coeff", "M_H", "M_ref", "ne_hall_floor")
 
-    def __init__(self, runs, precision=mhd.PREC_FP64, host=None):
+    def __init__(self, runs, precision=mhd.PREC_FP64, host=None, geometry_on: str = "host"):
         self.runs = [(spec, topo) for spec, topo in runs]
         c0 = physics.constants(self.runs[0][0].params)
         for spec, topo in self.runs:
@@ -382,7 +396,7 @@ class Batch:
             run_of += [r] * len(spec.blocks)
         self.ctx = mhd.Context(ncells, make_params(self.runs[0][0].params, precision), runs=run_of)
         if host is None:
-            host = (host_setup(spec, topo) for spec, topo in self.runs)
+            host = (host_setup(spec, topo, geometry_on) for spec, topo in self.runs)
         per_run = []
         zero_rows = []
         poles = []
@@ -390,6 +404,9 @@ class Batch:
             off = self.offset[r]
             q, B = physics.farfield_state(spec.params)
             for ib, g in enumerate(geom):
+                if g is None:
+                    self.ctx.build_geometry(off + ib, nodes[ib].a, B)
+                    continue
                 for name in GEOM_FIELDS:
                     self.ctx.upload(name, off + ib, g[name][2])
                 if any(v != 0.0 for v in B):

@@ -195,6 +195,17 @@ int mhd_set_sync_wall(mhd_ctx *ctx, const char *group, int32_t block, int32_t di
    zeroes divB there (:729-772).  Needs the geometry field Astar_eta.  Not
    available with the resistive or implicit Hall solves (MHD_ESTATE). */
 int mhd_set_pole(mhd_ctx *ctx, int32_t block, int32_t direction);
+
+/* Geometry of a block built on the device from its ghost node mesh
+   (Block::Add_ghostmesh and, with Poles, Grid::MeshTrans_Inner_Pole done by
+   the caller): JDxi/JDet/JDze, Jac, Area_*, beta_*, dl_*, Astar_*, alpha_*,
+   dr_*, Bcell_from_Bface_w and Jcell_from_Jedge_w on their reference extents
+   (src/3_field/4_MPCNS_Geometry.cpp:4-640, Z4_Lunar/src/LunarSolver.cpp:243-915),
+   in place of uploading each with mhd_upload_field; with B_imf (3 values, or
+   null) not zero also Badd_* = B_imf . JD.  nodes: (n_i + 1 + 2 (G + 1)) x
+   (n_j + ...) x (n_k + ...) x 3 doubles, G = mhd_params.ngg, logical node
+   (i, j, k) at ((i + G + 1) * NJ + j + G + 1) * NK + k + G + 1, x y z last. */
+int mhd_build_geometry(mhd_ctx *ctx, int32_t block, const double *nodes, int64_t count, const double *B_imf);
 int mhd_set_sync_map_post(mhd_ctx *ctx, const char *group, const int64_t *dst, const int64_t *src, int64_t n);
 
 /* Implicit resistive step (LunarSolver::SolveImplicitResistiveDiffusion_,
