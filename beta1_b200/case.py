@@ -131,7 +131,11 @@ def write_setup(case_dir: str, p: Dict[str, object]) -> None:
     g.append(f"int     corner_treat            {_num(p['corner_treat'])}")
     g.append(f"double  scale                   {_num(p['scale'])}")
     g.append(f"double  mole_mass1              {_num(p['mole_mass1'])}")
-    g.append(f"double  eta_max_lunar           {_num(p['eta_max_lunar'])}")
+    if p.get("solver") == "mercury":
+        g.append(f"double  mole_mass2              {_num(p['mole_mass2'])}")
+        g.append(f"double  eta_max_mercury         {_num(p['eta_max_mercury'])}")
+    else:
+        g.append(f"double  eta_max_lunar           {_num(p['eta_max_lunar'])}")
     g.append("")
     g.append("LIST==================================================================")
     g.append("constant        5")
@@ -171,8 +175,28 @@ def write_setup(case_dir: str, p: Dict[str, object]) -> None:
                 "LIST==================================================================\n\nEND_OF_FILE\n")
     m = []
     m.append(f"int     num_of_dipole                   {_num(p['num_of_dipole'])}")
-    m.append(f"bool    is_Lunar_resistance           {_num(p['is_Lunar_resistance'])}")
-    m.append(f"bool    use_implicit_lunar_resistance {_num(p['use_implicit_lunar_resistance'])}")
+    mercury = p.get("solver") == "mercury"
+    if mercury:
+        # DipoleField::load_from_param (Z5_Mercury/include/operators/Dipole.h:44-88)
+        for i, dp in enumerate(p.get("dipoles", [])[:int(p["num_of_dipole"])], start=1):
+            m.append("LIST==================================================================")
+            m.append(f"Dipole{i}         7")
+            m.append("(double)")
+            m.append("x0              y0              z0          mx          my          mz          a")
+            m.append(" ".join(_num(dp[k]) for k in ["x0", "y0", "z0", "mx", "my", "mz", "a"]))
+            m.append("LIST==================================================================")
+        m.append(f"bool    is_Mercury_resistance           {_num(p['is_Mercury_resistance'])}")
+        m.append(f"bool    use_implicit_mercury_resistance {_num(p['use_implicit_mercury_resistance'])}")
+        m.append(f"bool    is_Ambipolar_Efield             {_num(p['is_Ambipolar_Efield'])}")
+        m.append(f"double  r_min                           {_num(p['r_min'])}")
+        m.append(f"double  r_max                           {_num(p['r_max'])}")
+        m.append(f"bool    is_local_artificial_resistivity {_num(p['is_local_artificial_resistivity'])}")
+        for k in ("local_arti_eta_max", "local_arti_x0", "local_arti_y0", "local_arti_z0", "local_arti_r_decay",
+                  "local_arti_r_cutoff"):
+            m.append(f"double  {k:<31} {_num(p[k])}")
+    else:
+        m.append(f"bool    is_Lunar_resistance           {_num(p['is_Lunar_resistance'])}")
+        m.append(f"bool    use_implicit_lunar_resistance {_num(p['use_implicit_lunar_resistance'])}")
     m.append(f"int     n_resistive_subcycles           {_num(p['n_resistive_subcycles'])}")
     m.append(f"double  implicit_resistive_ksp_rtol     {_num(p['implicit_resistive_ksp_rtol'])}")
     m.append(f"double  implicit_resistive_ksp_atol     {_num(p['implicit_resistive_ksp_atol'])}")
@@ -516,6 +540,19 @@ def inflow_params(mach_u=8.0, B=(0.0, 0.5 / math.sqrt(2.0), 0.5 / math.sqrt(2.0)
     p["INITIAL"] = dict(U=mach_u * r["U"], T=T, n=r["n"], Molecular_mass=r["Molecular_mass"], c_y=0.0, c_z=0.0,
                         Bx=B[0] * r["B_ref"], By=B[1] * r["B_ref"], Bz=B[2] * r["B_ref"])
     return p
+
+
+def mercury_params(**over):
+    """Parameters of the reference's Mercury (two-fluid) solver: the inflow
+    parameters plus the keys MercurySolver reads (Z5_Mercury/9999setup/*,
+    MercurySolver.cpp, MercurySolver_Tools.cpp); every optional term off
+    unless set.  dipoles: [dict(x0, y0, z0, mx, my, mz, a)] in SI units."""
+    base = dict(solver="mercury", mole_mass2=0.023, eta_max_mercury=0.0, is_Mercury_resistance=0,
+                use_implicit_mercury_resistance=0, is_Ambipolar_Efield=0, r_min=1.1, r_max=1.2,
+                is_local_artificial_resistivity=0, local_arti_eta_max=0.0, local_arti_x0=0.0, local_arti_y0=0.0,
+                local_arti_z0=0.0, local_arti_r_decay=0.05, local_arti_r_cutoff=0.05, dipoles=[])
+    base.update(over)
+    return inflow_params(**base)
 
 
 def cubed_sphere_inflow_case(nr=96, na=48, **over) -> CaseSpec:

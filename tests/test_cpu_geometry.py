@@ -85,3 +85,32 @@ def test_pole_patch_rules():
     for g in range(1, o + 1):
         assert np.array_equal(Y.a[o:o + 5, o - g, o:o + 7], Y.a[o:o + 5, o, o:o + 7])
         assert np.array_equal(Y.a[o:o + 5, o + 4 + g, o:o + 7], Y.a[o:o + 5, o + 4, o:o + 7])
+
+
+def test_mercury_setup_has_every_key_the_solver_reads(tmp_path):
+    """The setup files of a Mercury case (case.mercury_params) hold every key
+    MercurySolver and the shared core read (Param::GetDou / GetInt / GetBoo
+    keys of Z5_Mercury and src/), and a dipole list in the reference's LIST
+    syntax."""
+    from beta1_b200 import case
+    keys = ["Archive_Output_Time", "CFL", "J_range_on", "J_range_start", "arti_eta_max", "continue_calc", "dimension",
+            "eta_max_mercury", "implicit_resistive_ksp_atol", "implicit_resistive_ksp_max_it",
+            "implicit_resistive_ksp_rtol", "is_Ambipolar_Efield", "is_Mercury_resistance",
+            "is_local_artificial_resistivity", "local_arti_eta_max", "local_arti_r_cutoff", "local_arti_r_decay",
+            "local_arti_x0", "local_arti_y0", "local_arti_z0", "max_Nstep", "max_Time", "mole_mass1", "mole_mass2",
+            "n_resistive_subcycles", "ngg", "num_of_dipole", "output_residual", "output_step", "r_max", "r_min",
+            "use_implicit_mercury_resistance"]
+    dip = dict(x0=0.0, y0=0.0, z0=4.88e5, mx=0.0, my=0.0, mz=-2.83e19, a=5.0e2)
+    p = case.mercury_params(num_of_dipole=1, dipoles=[dip])
+    spec = case.CaseSpec(case.slab_blocks(6, (4, 4), (1, 1)), case.slab_interfaces(6, (4, 4), (1, 1)), p)
+    case.write_case(str(tmp_path), spec)
+    d = tmp_path / "CASE" / "setup"
+    text = "".join((d / f).read_text() for f in ("0_General_Setting.txt", "1_Initial_condition.txt",
+                                                 "2_Boundary_Condition.txt", "3_MHD_Control.txt"))
+    words = set(text.split())
+    assert [k for k in keys if k not in words] == []
+    assert "eta_max_lunar" not in words and "is_Lunar_resistance" not in words
+    ctl = (d / "3_MHD_Control.txt").read_text().splitlines()
+    i = ctl.index("Dipole1         7")
+    assert ctl[i + 2].split() == ["x0", "y0", "z0", "mx", "my", "mz", "a"]
+    assert float(ctl[i + 3].split()[5]) == -2.83e19
