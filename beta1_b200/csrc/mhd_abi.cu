@@ -93,7 +93,7 @@ const char *const kKernelNames[] = {
     "k_bcell_jedge",  "k_fluid_ucontra", "k_wall_u_all",   "k_hall_cell",    "k_hall_edge",
     "k_pack_vec",     "k_hall_residual", "k_axpy_to",      "k_fd_quotient",  "k_negate",
     "k_geom32",       "k_fluid_mixed",  "k_gmres_resist", "k_pole",
-    "k_geometry"};
+    "k_geometry",     "k_diag_init",   "k_diag"};
 constexpr int kNumKernelNames = int(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
 
 } // namespace
@@ -151,6 +151,7 @@ struct mhd_ctx
     // sync in the topology order of the Pole shell
     std::vector<int> poles;
     int *dpoles = nullptr;
+    unsigned long long *diag_keys = nullptr; // output-step minima / maxima (mhd_diagnostics)
     // materialisation state: groups whose last sync ran its hot list only,
     // and PV / U_plus computed on the first ghost layer only
     std::map<std::string, bool> dirty;
@@ -1649,6 +1650,7 @@ int mhd_ctx_destroy(mhd_ctx *ctx)
         cudaFree(kv.second.dwalls);
     }
     cudaFree(ctx->dpoles);
+    cudaFree(ctx->diag_keys);
     free_resistive(ctx);
     cudaFree(ctx->hall_zb);
     mhd_set_hall_implicit(ctx, 0, nullptr, 0, nullptr, nullptr, nullptr, 0.0, 0.0, 0, 0.0, 1);
@@ -2389,6 +2391,31 @@ int mhd_build_geometry(mhd_ctx *ctx, int32_t block, const double *nodes, int64_t
     CK(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->geom_dirty = true;
     drop_graph(ctx);
+    return MHD_OK;
+}
+
+int mhd_diagnostics(mhd_ctx *ctx, int32_t run, double *mins, double *maxs)
+{
+    if (!ctx || !mins || !maxs || run >= ctx->nruns)
+        return fail(ctx, MHD_EINVAL, "bad diagnostics arguments");
+    if (ctx->capturing)
+        return fail(ctx, MHD_ESTATE, "diagnostics during capture");
+    if (!ctx->diag_keys)
+        CK(ctx, cudaMalloc(&ctx->diag_keys, (DIAG_NMIN + DIAG_NQ) * sizeof(unsigned long long)));
+    prof_begin(ctx, "k_diag_init");
+    k_diag_init<<<1, 32, 0, ctx->stream>>>(ctx->diag_keys);
+    RUN(launched(ctx));
+    prof_begin(ctx, "k_diag");
+    k_diag<<<dim3(grid_for(ctx->max_cells), unsigned(ctx->nblocks)), kThreads, 0, ctx->stream>>>(ctx->dbv, run,
+                                                                                                 ctx->diag_keys);
+    RUN(launched(ctx));
+    unsigned long long keys[DIAG_NMIN + DIAG_NQ];
+    CK(ctx, cudaMemcpyAsync(keys, ctx->diag_keys, sizeof keys, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int q = 0; q < DIAG_NMIN; ++q)
+        mins[q] = diag_unkey(keys[q]);
+    for (int q = 0; q < DIAG_NQ; ++q)
+        maxs[q] = diag_unkey(keys[DIAG_NMIN + q]);
     return MHD_OK;
 }
 

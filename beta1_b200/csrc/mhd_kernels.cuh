@@ -4,6 +4,7 @@
 #include "mhd_layout.cuh"
 #include "mhd_pole.cuh"
 #include "mhd_geom.cuh"
+#include "mhd_output.cuh"
 #include "../../include/beta1_mhd.h"
 
 namespace mhd
@@ -43,6 +44,10 @@ __global__ void k_jcell(const BlockView *bvs);
 __global__ void k_pole(const BlockView *bvs, const int *poles, int op);
 __global__ void k_geometry(const BlockView *bvs, int blk, NodeMesh m, int G, int group0, double b0, double b1,
                            double b2);
+// output-step minima / maxima over the inner cells of a run's blocks (run < 0:
+// every block); keys[0..DIAG_NMIN) minima, keys[DIAG_NMIN..DIAG_NMIN + DIAG_NQ) maxima
+__global__ void k_diag_init(unsigned long long *keys);
+__global__ void k_diag(const BlockView *bvs, int run, unsigned long long *keys);
 __global__ void k_begin_step(const unsigned long long *dt_key, double *dt, int *err, double dt_abort, int nruns);
 __global__ void k_arm_dt(unsigned long long *dt_key, int nruns);
 __global__ void k_end_step(const double *dt, double *time, long long *step, int nruns);

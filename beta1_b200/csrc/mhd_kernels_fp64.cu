@@ -1766,6 +1766,69 @@ __global__ void k_geometry(const BlockView *__restrict__ bvs, int blk, NodeMesh 
     geom_point(m, b, group0 + int(blockIdx.y), i, j, k, G, gb);
 }
 
+// output-step diagnostics: minima start at +inf, maxima at -inf, max |divB| at 0
+__global__ void k_diag_init(unsigned long long *keys)
+{
+    const int t = threadIdx.x;
+    if (t < DIAG_NMIN)
+        keys[t] = diag_key(INFINITY);
+    else if (t < DIAG_NMIN + DIAG_NQ - 1)
+        keys[t] = diag_key(-INFINITY);
+    else if (t == DIAG_NMIN + DIAG_NQ - 1)
+        keys[t] = diag_key(0.0);
+}
+
+// one inner cell per thread, one grid row per block; NaN values are skipped
+// (std::min / std::max keep the running value against a NaN)
+__global__ void k_diag(const BlockView *__restrict__ bvs, int run, unsigned long long *keys)
+{
+    const BlockView &b = bvs[blockIdx.y];
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    unsigned long long kmin[DIAG_NMIN], kmax[DIAG_NQ];
+#pragma unroll
+    for (int q = 0; q < DIAG_NQ; ++q)
+    {
+        if (q < DIAG_NMIN)
+            kmin[q] = ~0ull;
+        kmax[q] = 0ull;
+    }
+    if ((run < 0 || b.run == run) && t < int64_t(b.ni) * b.nj * b.nk)
+    {
+        const int k = int(t % b.nk), j = int((t / b.nk) % b.nj), i = int(t / (int64_t(b.nk) * b.nj));
+        double v[DIAG_NQ];
+        diag_cell(b, i, j, k, v);
+#pragma unroll
+        for (int q = 0; q < DIAG_NQ; ++q)
+            if (v[q] == v[q])
+            {
+                const unsigned long long key = diag_key(v[q]);
+                if (q < DIAG_NMIN)
+                    kmin[q] = key;
+                kmax[q] = key;
+            }
+    }
+#pragma unroll
+    for (int q = 0; q < DIAG_NQ; ++q)
+    {
+        unsigned long long lo = (q < DIAG_NMIN) ? kmin[q] : ~0ull, hi = kmax[q];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            const unsigned long long olo = __shfl_xor_sync(0xffffffffu, lo, off);
+            const unsigned long long ohi = __shfl_xor_sync(0xffffffffu, hi, off);
+            lo = (olo < lo) ? olo : lo;
+            hi = (ohi > hi) ? ohi : hi;
+        }
+        if ((threadIdx.x & 31) == 0)
+        {
+            if (q < DIAG_NMIN && lo != ~0ull)
+                atomicMin(&keys[q], lo);
+            if (hi != 0ull)
+                atomicMax(&keys[DIAG_NMIN + q], hi);
+        }
+    }
+}
+
 // Pole handlers and repairs: one thread per pole_one work item (mhd_pole.cuh)
 __global__ void k_pole(const BlockView *__restrict__ bvs, const int *__restrict__ poles, int op)
 {

@@ -67,6 +67,7 @@ _SIGS = {
     "mhd_set_sync_map_post": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64]),
     "mhd_set_pole": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "mhd_build_geometry": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p]),
+    "mhd_diagnostics": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "mhd_set_resistive": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int32, C.c_int32]),
     "mhd_set_hall_implicit": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
@@ -269,6 +270,14 @@ class Context:
             assert bv.size == 3
             bp = bv.ctypes.data
         self._check(self.lib.mhd_build_geometry(self.h, block, a.ctypes.data, a.size, bp), "build_geometry")
+
+    def diagnostics(self, run: int = -1):
+        """PrintMinMaxDiagnostics_ values: (mins of rho, p, Bx, By, Bz, |B|^2/2;
+        their maxima and max |divB|) over a run's inner cells (-1: all)"""
+        mins = (C.c_double * 6)()
+        maxs = (C.c_double * 7)()
+        self._check(self.lib.mhd_diagnostics(self.h, run, mins, maxs), "diagnostics")
+        return list(mins), list(maxs)
 
     def set_pole(self, block: int, direction: int):
         """an eta Pole (direction -2: j = 0, +2: j = n_j) of a block"""

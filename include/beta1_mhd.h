@@ -206,6 +206,14 @@ int mhd_set_pole(mhd_ctx *ctx, int32_t block, int32_t direction);
    (n_j + ...) x (n_k + ...) x 3 doubles, G = mhd_params.ngg, logical node
    (i, j, k) at ((i + G + 1) * NJ + j + G + 1) * NK + k + G + 1, x y z last. */
 int mhd_build_geometry(mhd_ctx *ctx, int32_t block, const double *nodes, int64_t count, const double *B_imf);
+
+/* Output-step diagnostics of LunarSolver::PrintMinMaxDiagnostics_
+   (Z4_Lunar/src/tools/LunarSolver_PrintDiag.cpp:7-85) over the inner cells of
+   a run's blocks (run -1: every block): mins[6] = the minima of rho, p, Bx,
+   By, Bz, |B|^2 / 2, maxs[7] = their maxima and max |divB| (NaN values are
+   skipped).  Reads U_H, PV_H, B_cell and divB: call MHD_STAGE_DIVB first, as
+   the reference calls calc_divB first. */
+int mhd_diagnostics(mhd_ctx *ctx, int32_t run, double *mins, double *maxs);
 int mhd_set_sync_map_post(mhd_ctx *ctx, const char *group, const int64_t *dst, const int64_t *src, int64_t n);
 
 /* Implicit resistive step (LunarSolver::SolveImplicitResistiveDiffusion_,

@@ -668,6 +668,39 @@ class Oracle:
             num = bx((1, 0, 0)) - bx(z) + be((0, 1, 0)) - be(z) + bz((0, 0, 1)) - bz(z)
             blk.f["divB"][0][blk.s(lo, hi)] = num / blk.box("Jac", 0, lo, hi)
 
+    # ------------------------------------------------------- diagnostics
+    def minmax_diagnostics(self):
+        """PrintMinMaxDiagnostics_ (Z4_Lunar/src/tools/LunarSolver_PrintDiag.cpp:7-85):
+        over the inner cells of every block the minima of rho, p, Bx, By, Bz,
+        |B|^2 / 2 and their maxima plus max |divB| (std::min / std::max skip
+        NaN).  Returns (mins[6], maxs[7])."""
+        mins = [np.inf] * 6
+        maxs = [-np.inf] * 6 + [0.0]
+        for blk in self.blocks:
+            lo, hi = blk.inner(0)
+            bx, by, bz = (blk.box("B_cell", c, lo, hi) for c in range(3))
+            vals = [blk.box("U_H", 0, lo, hi), blk.box("PV_H", 3, lo, hi), bx, by, bz,
+                    0.5 * (bx * bx + by * by + bz * bz)]
+            for q, v in enumerate(vals):
+                v = v[~np.isnan(v)]
+                if v.size:
+                    mins[q] = min(mins[q], float(v.min()))
+                    maxs[q] = max(maxs[q], float(v.max()))
+            d = np.abs(blk.box("divB", 0, lo, hi))
+            d = d[~np.isnan(d)]
+            if d.size:
+                maxs[6] = max(maxs[6], float(d.max()))
+        return mins, maxs
+
+    @staticmethod
+    def format_diagnostics(mins, maxs):
+        """the three lines PrintMinMaxDiagnostics_ prints"""
+        b_abs_max = np.sqrt(max(0.0, 2.0 * maxs[5]))
+        return ["           rho=[%.3e, %.3e]  p=[%.3e, %.3e]" % (mins[0], maxs[0], mins[1], maxs[1]),
+                "           Bx =[%.3e, %.3e]  By=[%.3e, %.3e]  Bz=[%.3e, %.3e]" % (mins[2], maxs[2], mins[3],
+                                                                                  maxs[3], mins[4], maxs[4]),
+                "           Pmag=[%.3e, %.3e]  |B|max=%.3e  divB_max=%.3e" % (mins[5], maxs[5], b_abs_max, maxs[6])]
+
     # ------------------------------------------------ explicit resistivity
     explicit = None
 

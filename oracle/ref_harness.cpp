@@ -360,6 +360,20 @@ void dump_state(Harness &h, const std::string &path)
     write_dump(path, s->run_data_->step, s->run_data_->time, h.fld->num_blocks(), items);
 }
 
+// The reference's output-step diagnostics after nsteps StepOnce: calc_divB,
+// then PrintMinMaxDiagnostics_ (its own printf lines on stdout)
+int cmd_diag(Harness &h, const std::string &state, int nsteps)
+{
+    h.load_state(state);
+    LunarSolver &s = *h.solver;
+    s.UpdateDerivedFields_();
+    for (int n = 0; n < nsteps; ++n)
+        s.StepOnce();
+    s.calc_divB();
+    s.PrintMinMaxDiagnostics_();
+    return 0;
+}
+
 int cmd_run(Harness &h, const std::string &state, int nsteps, const std::string &prefix)
 {
     h.load_state(state);
@@ -607,6 +621,11 @@ int main(int argc, char **argv)
             rc = cmd_run(h, argv[2], std::atoi(argv[3]), argv[4]);
         else if (cmd == "probe" && argc >= 5)
             rc = cmd_probe(h, argv[2], argv[3], argv[4]);
+        else if (cmd == "diag" && argc >= 4)
+        {
+            std::cout.rdbuf(saved);
+            rc = cmd_diag(h, argv[2], std::atoi(argv[3]));
+        }
         else if (cmd == "timehall" && argc >= 4)
         {
             std::cout.rdbuf(sink.rdbuf());

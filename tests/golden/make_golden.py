@@ -195,6 +195,23 @@ def shell_steps(nr=8, nth=6, nph=8, steps=2, seed=20261207):
     print("wrote", tag, "steps")
 
 
+def shell_diag(nr=8, nth=6, nph=8, seed=20261207, steps=2):
+    """The reference's output-step diagnostics (calc_divB, then
+    PrintMinMaxDiagnostics_) after `steps` StepOnce on the Pole shell: the
+    lines it prints."""
+    tag = "shell_%dx%dx%d" % (nr, nth, nph)
+    with tempfile.TemporaryDirectory() as d:
+        spec = case.shell_case(nr, nth, nph)
+        case.write_case(d, spec)
+        rst.write(os.path.join(d, "init.rst"), case.inflow_state(spec, seed=seed))
+        out = subprocess.run([REF_BIN, "diag", "init.rst", str(steps)], cwd=d, capture_output=True, text=True,
+                             check=True).stdout
+    lines = [ln.rstrip() for ln in out.splitlines() if ln.strip().startswith(("rho=", "Bx", "Pmag"))]
+    with open(os.path.join(OUT, tag + "_diag.txt"), "w") as f:
+        f.write("\n".join(lines) + "\n")
+    print("wrote", tag + "_diag")
+
+
 def shell_probe(nr=8, nth=6, nph=8, seed=20261207):
     """Every Sync group of the Pole shell probed on the reference (as
     slab_probe)."""
@@ -353,6 +370,7 @@ if __name__ == "__main__":
     shell_geom()
     shell_steps()
     shell_probe()
+    shell_diag()
     slab_probe(resistive=0)
     slab_probe(resistive=1)
     hall("periodic")

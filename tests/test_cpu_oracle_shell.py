@@ -121,3 +121,17 @@ def test_shell_oracle_steps_bitwise(shell_run, step):
     assert checked >= 13
     if step:
         assert dts[step] == float(g["s%d/dt" % step])
+
+
+def test_shell_oracle_diagnostics_equal_reference_print(shell_run):
+    """PrintMinMaxDiagnostics_ after two steps: the oracle's minima / maxima,
+    printed as the reference prints them, equal the reference's lines
+    (tests/golden/shell_8x6x8_diag.txt)."""
+    o = build_shell_oracle()
+    for _ in range(2):
+        o.step()
+    o.calc_divb()
+    mins, maxs = o.minmax_diagnostics()
+    with open(os.path.join(ROOT, "tests", "golden", "shell_8x6x8_diag.txt")) as f:
+        ref = [ln.rstrip() for ln in f if ln.strip()]
+    assert o.format_diagnostics(mins, maxs) == ref

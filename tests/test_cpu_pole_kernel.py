@@ -117,3 +117,42 @@ def test_pole_work_items_equal_oracle(host_lib, mid_run, op):
         assert np.array_equal(arr, other), (op, name, int(np.count_nonzero(arr != other)))
         changed += int(np.count_nonzero(arr != start.blocks[0].f[name]))
     assert changed > 0, op
+
+
+def test_diag_keys_order_and_round_trip(host_lib):
+    """diag_key orders doubles as their values (-0 just below +0) and
+    diag_unkey inverts it bit for bit."""
+    rng = np.random.default_rng(5)
+    x = np.concatenate([rng.standard_normal(2000) * 10.0 ** rng.integers(-300, 300, 2000),
+                        [0.0, -0.0, np.inf, -np.inf, 5e-324, -5e-324, 1.7976931348623157e308]])
+    k = np.zeros(x.size, dtype=np.uint64)
+    back = np.zeros(x.size)
+    host_lib.diag_keys.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+    host_lib.diag_keys(x.ctypes.data, k.ctypes.data, back.ctypes.data, x.size)
+    assert np.array_equal(back.view(np.uint64), x.view(np.uint64))
+    order = np.argsort(k, kind="stable")
+    xs = x[order]
+    assert np.all(xs[:-1] <= xs[1:])
+
+
+def test_diag_reduction_equals_oracle(host_lib, mid_run):
+    """k_diag's per-cell values and key reduction (host build) against the
+    oracle's PrintMinMaxDiagnostics_ restatement, on the shell in mid-run."""
+    o = copy.deepcopy(mid_run)
+    o.calc_divb()
+    names = [t[0] for t in mhd.field_table()]
+    blk = o.blocks[0]
+    spare = []
+    ptrs = (C.c_void_p * len(names))()
+    for f, name in enumerate(names):
+        a = blk.f.get(name)
+        if a is None:
+            a = np.zeros((mhd_oracle_ncomp(name),) + blk.f["U_H"].shape[1:])
+            spare.append(a)
+        ptrs[f] = a.ctypes.data
+    mins = (C.c_double * 6)()
+    maxs = (C.c_double * 7)()
+    host_lib.diag_host.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_void_p), C.c_int, C.c_void_p, C.c_void_p]
+    assert host_lib.diag_host(blk.n[0], blk.n[1], blk.n[2], blk.G, ptrs, len(names), mins, maxs) == 0
+    rmins, rmaxs = o.minmax_diagnostics()
+    assert list(mins) == rmins and list(maxs) == rmaxs
