@@ -287,8 +287,9 @@ def cpu_reference_sweep(steps, nproc, nruns=SWEEP_RUNS, grid="slab"):
 SWEEP_SEED0 = 5000
 
 
-def build_sweep(precision, nruns=SWEEP_RUNS, workload="c5"):
-    """The sweep batch: host geometry of every run from a spawned process pool
+def build_sweep(precision, nruns=SWEEP_RUNS, workload="c5", geometry_on="host"):
+    """The sweep batch: host set-up of every run (node mesh, sync tables and,
+    unless the device builds it, the geometry) from a spawned process pool
     (bounded by cores and memory), uploaded run by run as it arrives."""
     import multiprocessing as mp
     from beta1_b200 import case, solver
@@ -296,7 +297,7 @@ def build_sweep(precision, nruns=SWEEP_RUNS, workload="c5"):
     runs = case.sweep_cases(nruns, grid=grid)
     nproc = max(1, min(len(runs), os.cpu_count() or 1, 16, int(mem_available_gb() / 8.0)))
     with mp.get_context("spawn").Pool(nproc) as pool:
-        host = pool.imap(solver.host_setup_run, [(spec, topo) for spec, _ in runs])
+        host = pool.imap(solver.host_setup_run, [(spec, topo, geometry_on) for spec, _ in runs])
         bt = solver.Batch([(spec, topo) for spec, _ in runs], precision=precision, host=host)
     bt.load_states([case.inflow_state(spec, seed=SWEEP_SEED0 + r) for r, (spec, _) in enumerate(runs)])
     return bt, sum(bt.cells), runs
@@ -354,6 +355,9 @@ def main():
     ap.add_argument("--e2e-iters", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep every kernel's default variant")
+    ap.add_argument("--geometry", default="host", choices=["host", "device"],
+                    help="geometry fields built on the host and uploaded, or built on the device from the node "
+                         "meshes (mhd_build_geometry); same values")
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="fp64, or FP32 face fluxes with FP64 CT / state / residuals (default: fp64, mixed for c5)")
     args = ap.parse_args()
@@ -383,20 +387,22 @@ def main():
     wl = WORKLOADS[args.workload]
     mixed = args.precision == "mixed"
     prec = mhd.PREC_MIXED if mixed else mhd.PREC_FP64
+    t_setup = time.time()
     if args.workload in SWEEP_GRID:
-        s, cells, sweep = build_sweep(prec, workload=args.workload)
+        s, cells, sweep = build_sweep(prec, workload=args.workload, geometry_on=args.geometry)
         spec = None
         nblocks = len(sweep)
     else:
         c2size = tuple(int(v) for v in args.c2_size.split("x"))
         spec, st, topology, cells = build_case(args.workload, args.n, c2size)
-        s = solver.Solver(spec, topology=topology, precision=prec)
+        s = solver.Solver(spec, topology=topology, precision=prec, geometry_on=args.geometry)
         if args.workload in ("c3", "c4"):
             # bounded: at most 10 Newton steps of at most 200 GMRES iterations per time step
             s.install_hall_implicit(topology, rtol=1e-10, atol=1e-50, maxit=10, ksp_rtol=1e-5, ksp_maxit=200)
         s.load_state(st)
         nblocks = len(spec.blocks)
     ctx = s.ctx
+    setup_s = time.time() - t_setup
     # register / occupancy variant of each hot kernel, timed on this state
     tuned = ctx.autotune(reps=10) if not args.no_autotune else None
     stream = torch.cuda.ExternalStream(ctx.stream())
@@ -517,7 +523,8 @@ def main():
                        "cells_per_gpu": cells, "blocks": nblocks, "autotune_min_ctas_per_sm": tuned,
                        "integrator": "forward Euler StepOnce (reference parity mode)", "precision": args.precision,
                        "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "no flush: per-step working set %.2f GB > 126 MB L2" % (ctx_bytes / 1e9)},
+                       "l2": "no flush: per-step working set %.2f GB > 126 MB L2" % (ctx_bytes / 1e9),
+                       "geometry": args.geometry, "setup_s": round(setup_s, 2)},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": nstate * 8,
                     "d2h_bytes_per_step": nstate * 8},
             "gpu_launches": int(launches),
