@@ -2150,9 +2150,14 @@ static int materialise_all(mhd_ctx *ctx)
 // after graph replays: every group ran its hot list
 static void mark_dirty(mhd_ctx *ctx)
 {
+    // a context with Poles runs every sync with its full lists: nothing is
+    // left to write at read-out (and a second Sync there is not idempotent:
+    // the Pole repairs change sources after their syncs, and a ring average
+    // of a ring need not reproduce it)
     for (auto &kv : ctx->syncs)
         if (kv.second.built)
-            ctx->dirty[kv.first] = kv.second.hot.n != kv.second.full.n || kv.second.hot.nconst != kv.second.full.nconst;
+            ctx->dirty[kv.first] = ctx->poles.empty() && (kv.second.hot.n != kv.second.full.n ||
+                                                          kv.second.hot.nconst != kv.second.full.nconst);
     ctx->pv_dirty = true;
 }
 
