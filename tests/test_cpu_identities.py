@@ -88,3 +88,20 @@ def test_uniform_state_stays_uniform(golden_periodic):
     scale = np.abs(blk.f["Badd_xi"]).max()
     for nm in ("B_xi", "B_eta", "B_zeta"):
         assert np.abs(blk.f[nm]).max() <= 1e-13 * scale, nm
+
+
+def test_fast_cell_drives_dt_below_the_abort_threshold(golden_periodic):
+    """The premise of the device's dt-guard test: one cell moving at 1e9 (a
+    state injected on the host) bounds the CFL time step below dt_abort = 1e-7
+    (LunarSolver_Timestep.cpp:128-139), where StepOnce aborts and the device
+    step returns MHD_EDT instead."""
+    from test_cpu_oracle import build_periodic_oracle
+    o = build_periodic_oracle(golden_periodic)
+    blk = o.blocks[0]
+    G = blk.G
+    rho = blk.f["U_H"][0][G + 2, G + 3, G + 1]
+    blk.f["U_H"][1][G + 2, G + 3, G + 1] = 1e9 * rho
+    o.sync("Ucell")
+    o.sync("Bface")
+    o.update_derived()
+    assert o.compute_timestep() < 1e-7
