@@ -379,7 +379,7 @@ int cmd_run(Harness &h, const std::string &state, int nsteps, const std::string 
     h.load_state(state);
     LunarSolver &s = *h.solver;
     s.UpdateDerivedFields_();
-    // divB as the driver computes it at output steps (UpdateControlAndOutput)
+    // divB as the reference computes it at output steps (UpdateControlAndOutput)
     s.calc_divB();
     dump_state(h, prefix + "_0000.bin");
     for (int n = 1; n <= nsteps; ++n)
