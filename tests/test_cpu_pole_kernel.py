@@ -40,9 +40,9 @@ def host_lib(tmp_path_factory):
     return lib
 
 
-@pytest.fixture(scope="module")
-def mid_run():
-    o = build_shell_oracle()
+@pytest.fixture(scope="module", params=[(8, 6, 8), (6, 2, 4)], ids=["8x6x8", "6x2x4"])
+def mid_run(request):
+    o = build_shell_oracle(request.param, seed=31)
     o.step()
     return o
 

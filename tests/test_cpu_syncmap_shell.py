@@ -199,3 +199,23 @@ def test_device_order_steps_equal_reference(tables):
             if s == 0 and f.startswith(("E", "RHS")):
                 continue
             assert np.array_equal(o.blocks[0].get_ref(f), g[key]), (s, f)
+
+
+@pytest.mark.parametrize("n", [(10, 5, 12), (6, 2, 4)])
+def test_device_order_on_other_shells(n):
+    """Other shell sizes (an odd polar count; two polar cells, where the two
+    pole rings are neighbours): every group in the device order equals the
+    oracle's Sync in the reference's order, in mid-run."""
+    lay, maps = shell_tables(n)
+    names = [t[0] for t in lay.table]
+    spec = case.shell_case(*n)
+    mid = build_shell_oracle(n, seed=31)
+    mid.step()
+    for group in maps:
+        a = copy.deepcopy(mid)
+        b = copy.deepcopy(mid)
+        a.sync(group)
+        device_order_sync(b, names, group, maps[group])
+        for f in syncmap.GROUPS[group]:
+            assert np.array_equal(a.blocks[0].get_ref(f), b.blocks[0].get_ref(f)), (n, group, f)
+    assert spec.blocks[0].ncell == n
