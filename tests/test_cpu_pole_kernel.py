@@ -104,7 +104,7 @@ def test_pole_work_items_equal_oracle(host_lib, mid_run, op):
     rng = np.random.default_rng(OP[op])
     for name in OUTPUTS[op]:
         arr = start.blocks[0].f[name]
-        arr *= 1.0 + 0.25 * rng.standard_normal(arr.shape)
+        arr += 0.25 * (np.abs(arr).max() + 1.0) * rng.standard_normal(arr.shape)
     a = copy.deepcopy(start)
     b = copy.deepcopy(start)
     oracle_op(a, op)
