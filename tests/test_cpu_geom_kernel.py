@@ -35,7 +35,8 @@ def host_lib(tmp_path_factory):
 
 CASES = {"periodic": lambda: case.periodic_box_case((8, 6, 5)),
          "slab": lambda: case.slab_case(6, (5, 6), (1, 1)),
-         "shell": lambda: case.shell_case(8, 6, 8)}
+         "shell": lambda: case.shell_case(8, 6, 8),
+         "shell_two_polar_cells": lambda: case.shell_case(6, 2, 4)}
 
 
 @pytest.mark.parametrize("name", list(CASES))
