@@ -1,6 +1,7 @@
 // C-ABI of the B200 MHD hot path (see include/beta1_mhd.h): context and
 // field pool management, host<->device transfers, compiled boundary syncs,
 // and the per-step launch sequence replayed as a CUDA graph.
+#include "mhd_device_scope.h"
 #include "mhd_kernels.cuh"
 
 #include <cuda_runtime.h>
@@ -13,15 +14,33 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
-#include <mutex>
 #include <string>
 #include <unordered_set>
 #include <vector>
 
 using namespace mhd;
 
+// Staging array of the allocation-free read-out (mhd_download_field_noalloc):
+// every device that loads the library holds it until the process exits.  Its
+// name is a host-side stand-in in host code; the device address is looked up
+// with cudaGetSymbolAddress when a context is created on that device.
+static __device__ __align__(256) double g_noalloc_staging[MHD_NOALLOC_MAX_DOUBLES];
+
 namespace
 {
+
+struct CudaDeviceApi
+{
+    static int get(int *d) { return cudaGetDevice(d) == cudaSuccess ? 0 : 1; }
+    static int set(int d) { return cudaSetDevice(d) == cudaSuccess ? 0 : 1; }
+};
+
+// makes the context's device current for the rest of the entry point and
+// restores the caller's device on return
+#define BIND_DEVICE(ctx)                                                                        \
+    DeviceScope<CudaDeviceApi> dev_scope_((ctx) ? (ctx)->device : -1);                          \
+    if (!dev_scope_.ok())                                                                       \
+        return MHD_ECUDA
 
 struct FieldSpec
 {
@@ -119,6 +138,8 @@ const int kTuneCount[NTUNE] = {3, 2, 2, 2, 2, 2, 3};
 
 struct mhd_ctx
 {
+    int device = -1;               // CUDA device the context lives on
+    double *noalloc = nullptr;     // device address of g_noalloc_staging on it
     int nblocks = 0;
     mhd_params prm{};
     Consts c{};
@@ -1484,6 +1505,11 @@ int create_ctx(const mhd_block_desc *blocks, int32_t nblocks, const int32_t *run
     else if (nruns != 1)
         return MHD_EINVAL;
     mhd_ctx *ctx = new mhd_ctx;
+    if (cudaGetDevice(&ctx->device) != cudaSuccess)
+    {
+        delete ctx;
+        return MHD_ECUDA;
+    }
     ctx->nblocks = nblocks;
     ctx->nruns = nruns;
     ctx->prm = *params;
@@ -1531,6 +1557,12 @@ int create_ctx(const mhd_block_desc *blocks, int32_t nblocks, const int32_t *run
     };
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(MHD_ECUDA);
+    {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_staging) != cudaSuccess)
+            return bail(MHD_ECUDA);
+        ctx->noalloc = static_cast<double *>(p);
+    }
     if (cudaMalloc(&ctx->pool, off * sizeof(double)) != cudaSuccess)
         return bail(MHD_ENOMEM);
     if (cudaMemsetAsync(ctx->pool, 0, off * sizeof(double), ctx->stream) != cudaSuccess)
@@ -1639,6 +1671,7 @@ int mhd_batch_create(const mhd_block_desc *blocks, int32_t nblocks, const int32_
 
 int mhd_ctx_destroy(mhd_ctx *ctx)
 {
+    BIND_DEVICE(ctx);
     if (!ctx)
         return MHD_OK;
     drop_graph(ctx);
@@ -1743,6 +1776,7 @@ static int transfer(mhd_ctx *ctx, const char *name, int32_t block, const double 
 
 int mhd_upload_field(mhd_ctx *ctx, const char *name, int32_t block, const double *data, int64_t count)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || !data)
         return fail(ctx, MHD_EINVAL, "null data");
     // every field the device holds is brought to the reference's state first
@@ -1751,44 +1785,12 @@ int mhd_upload_field(mhd_ctx *ctx, const char *name, int32_t block, const double
 }
 
 // ---------------------------------------------------------------------------
-// Allocation-free read-out (no counterpart in the reference).  The staging
-// array is a fixed device array in this file; host code may not use its name
-// as a device address, so its address is looked up once per device.
+// Allocation-free read-out (no counterpart in the reference): stages through
+// g_noalloc_staging, whose device address the context looked up at creation.
 // ---------------------------------------------------------------------------
-} // extern "C"
-
-static __device__ __align__(256) double g_noalloc_staging[MHD_NOALLOC_MAX_DOUBLES];
-
-namespace
-{
-constexpr int kNoallocDevices = 64;
-std::mutex g_noalloc_mutex;
-double *g_noalloc_ptr[kNoallocDevices] = {};
-
-// device address of the staging array on the current device
-int noalloc_staging(mhd_ctx *ctx, double **out)
-{
-    int dev = -1;
-    CK(ctx, cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kNoallocDevices)
-        return fail(ctx, MHD_EINVAL, "device %d is beyond the %d devices of the read-out table", dev,
-                    kNoallocDevices);
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev])
-    {
-        void *p = nullptr;
-        CK(ctx, cudaGetSymbolAddress(&p, g_noalloc_staging));
-        g_noalloc_ptr[dev] = static_cast<double *>(p);
-    }
-    *out = g_noalloc_ptr[dev];
-    return MHD_OK;
-}
-} // namespace
-
-extern "C" {
-
 int mhd_download_field_noalloc(mhd_ctx *ctx, const char *name, int32_t block, double *data, int64_t count)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || !data)
         return fail(ctx, MHD_EINVAL, "null data");
     const int f = field_by_name(name);
@@ -1808,8 +1810,9 @@ int mhd_download_field_noalloc(mhd_ctx *ctx, const char *name, int32_t block, do
         if (!kv.second.built)
             return fail(ctx, MHD_ESTATE, "sync group %s is not on the device yet; step or update the derived "
                         "fields once before an allocation-free read-out", kv.first.c_str());
-    double *stage = nullptr;
-    RUN(noalloc_staging(ctx, &stage));
+    double *stage = ctx->noalloc;
+    if (!stage)
+        return fail(ctx, MHD_ESTATE, "the read-out array's device address is unknown");
     RUN(materialise_field(ctx, f));
     int lo[3], hi[3];
     field_box(ctx, f, block, lo, hi);
@@ -1824,6 +1827,7 @@ int mhd_download_field_noalloc(mhd_ctx *ctx, const char *name, int32_t block, do
 
 int mhd_download_field(mhd_ctx *ctx, const char *name, int32_t block, double *data, int64_t count)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || !data)
         return fail(ctx, MHD_EINVAL, "null data");
     const int f = field_by_name(name);
@@ -2278,6 +2282,7 @@ extern "C" {
 
 int mhd_set_sync_map(mhd_ctx *ctx, const char *group, const int64_t *dst, const int64_t *src, int64_t n)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || !group || n < 0 || (n > 0 && (!dst || !src)))
         return fail(ctx, MHD_EINVAL, "bad sync map arguments");
     std::vector<uint64_t> d(static_cast<size_t>(n)), s(static_cast<size_t>(n));
@@ -2314,6 +2319,7 @@ int mhd_set_sync_map(mhd_ctx *ctx, const char *group, const int64_t *dst, const 
 
 int mhd_set_sync_consts(mhd_ctx *ctx, const char *group, const int64_t *dst, const double *val, int64_t n)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || !group || n < 0 || (n > 0 && (!dst || !val)))
         return fail(ctx, MHD_EINVAL, "bad sync constant arguments");
     std::vector<uint64_t> d(static_cast<size_t>(n));
@@ -2340,6 +2346,7 @@ int mhd_set_sync_consts(mhd_ctx *ctx, const char *group, const int64_t *dst, con
 
 int mhd_set_sync_map_post(mhd_ctx *ctx, const char *group, const int64_t *dst, const int64_t *src, int64_t n)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || !group || n < 0 || (n > 0 && (!dst || !src)))
         return fail(ctx, MHD_EINVAL, "bad sync map arguments");
     std::vector<uint64_t> d(static_cast<size_t>(n)), s(static_cast<size_t>(n));
@@ -2368,6 +2375,7 @@ int mhd_set_sync_map_post(mhd_ctx *ctx, const char *group, const int64_t *dst, c
 
 int mhd_build_geometry(mhd_ctx *ctx, int32_t block, const double *nodes, int64_t count, const double *B_imf)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || block < 0 || block >= ctx->nblocks || !nodes)
         return fail(ctx, MHD_EINVAL, "bad geometry arguments");
     if (ctx->capturing)
@@ -2401,6 +2409,7 @@ int mhd_build_geometry(mhd_ctx *ctx, int32_t block, const double *nodes, int64_t
 
 int mhd_diagnostics(mhd_ctx *ctx, int32_t run, double *mins, double *maxs)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || !mins || !maxs || run >= ctx->nruns)
         return fail(ctx, MHD_EINVAL, "bad diagnostics arguments");
     if (ctx->capturing)
@@ -2426,6 +2435,7 @@ int mhd_diagnostics(mhd_ctx *ctx, int32_t run, double *mins, double *maxs)
 
 int mhd_set_pole(mhd_ctx *ctx, int32_t block, int32_t direction)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || block < 0 || block >= ctx->nblocks || (direction != -2 && direction != 2))
         return fail(ctx, MHD_EINVAL, "bad Pole arguments (eta Poles: direction -2 or +2)");
     const BlockView &v = ctx->hbv[size_t(block)];
@@ -2449,6 +2459,7 @@ int mhd_set_pole(mhd_ctx *ctx, int32_t block, int32_t direction)
 
 int mhd_set_sync_wall(mhd_ctx *ctx, const char *group, int32_t block, int32_t direction)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || !group || block < 0 || block >= ctx->nblocks || direction == 0 || direction < -3 || direction > 3)
         return fail(ctx, MHD_EINVAL, "bad wall handler arguments");
     ctx->syncs[group].walls.emplace_back(block, direction);
@@ -2460,6 +2471,7 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
                       const int64_t *alias, const int64_t *owner, const double *sign, double rtol, double atol,
                       int32_t maxit, int32_t restart)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || n < 0 || nalias < 0 || (n > 0 && (!unknowns || !eta)) || (nalias > 0 && (!alias || !owner || !sign)))
         return fail(ctx, MHD_EINVAL, "bad resistive arguments");
     if (ctx->nruns > 1 && n > 0)
@@ -2627,6 +2639,7 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
 
 int mhd_set_hall(mhd_ctx *ctx, double hall_coef, const int32_t *zero_boxes, int32_t nbox)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || nbox < 0 || (nbox > 0 && !zero_boxes))
         return fail(ctx, MHD_EINVAL, "bad Hall arguments");
     for (int q = 0; q < nbox; ++q)
@@ -2652,6 +2665,7 @@ int mhd_set_hall_implicit(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, int6
                           const int64_t *owner, const double *sign, double rtol, double atol, int32_t maxit,
                           double ksp_rtol, int32_t ksp_maxit)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || n < 0 || nalias < 0 || maxit < 0 || ksp_maxit < 1 || (n > 0 && !unknowns) ||
         (nalias > 0 && (!alias || !owner || !sign)))
         return fail(ctx, MHD_EINVAL, "bad implicit Hall arguments");
@@ -2716,6 +2730,7 @@ int mhd_set_hall_implicit(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, int6
 int mhd_hall_stats(const mhd_ctx *ctx, int32_t *newton_its, int32_t *linear_its, double *fnorm, double *fnorm0,
                    int32_t *reason)
 {
+    BIND_DEVICE(ctx);
     if (!ctx)
         return MHD_EINVAL;
     const auto &H = ctx->hall;
@@ -2734,6 +2749,7 @@ int mhd_hall_stats(const mhd_ctx *ctx, int32_t *newton_its, int32_t *linear_its,
 
 int mhd_set_resistive_explicit(mhd_ctx *ctx, double inver_Rem, int32_t nsub)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || nsub < 0)
         return fail(ctx, MHD_EINVAL, "bad explicit resistive arguments");
     if (ctx->nruns > 1 && nsub > 0)
@@ -2753,6 +2769,7 @@ int mhd_set_resistive_explicit(mhd_ctx *ctx, double inver_Rem, int32_t nsub)
 
 int mhd_set_flux_reference_run(mhd_ctx *ctx, int32_t run, const double prim[5])
 {
+    BIND_DEVICE(ctx);
     if (!ctx || !prim)
         return fail(ctx, MHD_EINVAL, "null flux reference");
     if (run < -1 || run >= ctx->nruns)
@@ -2775,6 +2792,7 @@ int mhd_set_flux_reference(mhd_ctx *ctx, const double prim[5])
 
 int mhd_autotune(mhd_ctx *ctx, int32_t reps, int32_t *min_ctas, int32_t n)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || reps < 1 || n < 0 || (n > 0 && !min_ctas))
         return fail(ctx, MHD_EINVAL, "bad autotune arguments");
     if (ctx->capturing)
@@ -2887,6 +2905,7 @@ const char *mhd_tune_name(int32_t i) { return (i >= 0 && i < NTUNE) ? kTuneNames
 
 int mhd_resistive_stats(const mhd_ctx *ctx, int32_t *its, double *rnorm, double *bnorm, int32_t *reason)
 {
+    BIND_DEVICE(ctx);
     if (!ctx)
         return MHD_EINVAL;
     GmresState h;
@@ -2908,8 +2927,25 @@ int mhd_resistive_stats(const mhd_ctx *ctx, int32_t *its, double *rnorm, double 
     return MHD_OK;
 }
 
+int mhd_test_stall_barrier(mhd_ctx *ctx, uint32_t spin_limit)
+{
+    BIND_DEVICE(ctx);
+    if (!ctx || spin_limit == 0)
+        return MHD_EINVAL;
+    auto &R = ctx->res;
+    if (!R.on || !R.bar)
+        return fail(ctx, MHD_ESTATE, "test_stall_barrier: no persistent implicit resistive solve is set up");
+    // arrival count one short of the grid for good (no CTA completes the
+    // barrier), and a short polling limit for every wait
+    const unsigned w[4] = {0xFFFFFFFFu, 0u, spin_limit, 0u};
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    CK(ctx, cudaMemcpy(R.bar, w, sizeof(w), cudaMemcpyHostToDevice));
+    return MHD_OK;
+}
+
 int mhd_sync(mhd_ctx *ctx, const char *group)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || !group)
         return MHD_EINVAL;
     RUN(run_sync(ctx, group, true));
@@ -2919,6 +2955,7 @@ int mhd_sync(mhd_ctx *ctx, const char *group)
 
 int mhd_update_derived(mhd_ctx *ctx)
 {
+    BIND_DEVICE(ctx);
     if (!ctx)
         return MHD_EINVAL;
     RUN(ensure_geom(ctx));
@@ -2929,6 +2966,7 @@ int mhd_update_derived(mhd_ctx *ctx)
 
 int mhd_step(mhd_ctx *ctx, int32_t nsteps, double *dt_out, double *time_out)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || nsteps < 0)
         return MHD_EINVAL;
     RUN(run_steps(ctx, nsteps));
@@ -2942,6 +2980,7 @@ int mhd_step(mhd_ctx *ctx, int32_t nsteps, double *dt_out, double *time_out)
 
 int mhd_batch_step(mhd_ctx *ctx, int32_t nsteps, double *dt_out, double *time_out, int32_t nruns)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || nsteps < 0 || (nruns > 0 && (!dt_out && !time_out)))
         return fail(ctx, MHD_EINVAL, "bad batch step arguments");
     if (nruns != 0 && nruns != ctx->nruns)
@@ -2970,6 +3009,7 @@ int64_t mhd_state_count(const mhd_ctx *ctx)
 int mhd_step_host(mhd_ctx *ctx, int32_t nsteps, const double *state_in, double *state_out, int64_t count,
                   double *dt_out)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || !state_in || !state_out || nsteps < 0)
         return MHD_EINVAL;
     if (count != mhd_state_count(ctx))
@@ -3033,6 +3073,7 @@ int mhd_host_free(void *ptr)
 
 int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
 {
+    BIND_DEVICE(ctx);
     if (!ctx)
         return MHD_EINVAL;
     RUN(ensure_geom(ctx));
@@ -3096,6 +3137,7 @@ int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
 
 int mhd_run_time(mhd_ctx *ctx, int32_t run, double *dt, double *time, int64_t *step)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || run < 0 || run >= ctx->nruns)
         return MHD_EINVAL;
     double d = 0.0, t = 0.0;
@@ -3115,11 +3157,13 @@ int mhd_run_time(mhd_ctx *ctx, int32_t run, double *dt, double *time, int64_t *s
 
 int mhd_get_time(mhd_ctx *ctx, double *dt, double *time, int64_t *step)
 {
+    BIND_DEVICE(ctx);
     return mhd_run_time(ctx, 0, dt, time, step);
 }
 
 int mhd_set_time(mhd_ctx *ctx, double dt, double time, int64_t step)
 {
+    BIND_DEVICE(ctx);
     if (!ctx)
         return MHD_EINVAL;
     const size_t nr = size_t(ctx->nruns);
@@ -3166,6 +3210,7 @@ int mhd_field_spec(int32_t index, const char **name, int32_t *loc, int32_t *ncom
 
 int mhd_profile_step(mhd_ctx *ctx, int32_t cap, int32_t *kernel_ids, float *ms, int32_t *count)
 {
+    BIND_DEVICE(ctx);
     if (!ctx || !count || cap < 0)
         return MHD_EINVAL;
     RUN(ensure_geom(ctx));

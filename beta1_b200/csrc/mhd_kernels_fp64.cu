@@ -1299,6 +1299,9 @@ __global__ void k_soa_to_aos(const BlockView *__restrict__ bvs, int blk, int fid
 
 constexpr long long kBarrierSpins = 1ll << 22; // about a second of polling
 
+// bar[0]: arrival count, bar[1]: generation, bar[2]: polling limit of every
+// wait (0: kBarrierSpins; a smaller limit is set only by the failure-
+// detection hook mhd_test_stall_barrier, and the host clears it after use)
 __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err)
 {
     __shared__ int ok; // one decision for the whole CTA
@@ -1307,6 +1310,8 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err)
     {
         volatile unsigned *gen = bar + 1;
         const unsigned g = *gen;
+        const unsigned lim = *(volatile unsigned *)(bar + 2);
+        const long long limit = lim ? (long long)lim : kBarrierSpins;
         __threadfence();
         if (atomicAdd(bar, 1u) + 1u == gridDim.x)
         {
@@ -1319,7 +1324,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err)
             long long spins = 0;
             while (*gen == g)
             {
-                if (++spins > kBarrierSpins)
+                if (++spins > limit)
                 {
                     atomicExch(err, MHD_EKRYLOV);
                     break;

@@ -62,6 +62,7 @@ _SIGS = {
     "mhd_point_id": (C.c_int64, [C.c_void_p, C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "mhd_set_sync_map": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64]),
     "mhd_sync": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "mhd_test_stall_barrier": (C.c_int, [C.c_void_p, C.c_uint32]),
     "mhd_set_sync_consts": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64]),
     "mhd_set_sync_wall": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_int32]),
     "mhd_set_sync_map_post": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64]),
@@ -352,6 +353,12 @@ class Context:
         self._check(self.lib.mhd_resistive_stats(self.h, C.byref(its), C.byref(rn), C.byref(bn), C.byref(rs)),
                     "resistive_stats")
         return dict(its=its.value, rnorm=rn.value, bnorm=bn.value, reason=rs.value)
+
+    def test_stall_barrier(self, spin_limit: int):
+        """failure-detection hook: the next persistent resistive solve waits
+        for a barrier arrival that never comes, each wait bounded at
+        spin_limit polls, and the step reports EKRYLOV"""
+        self._check(self.lib.mhd_test_stall_barrier(self.h, int(spin_limit)), "test_stall_barrier")
 
     def sync(self, group: str):
         self._check(self.lib.mhd_sync(self.h, group.encode()), f"sync {group}")

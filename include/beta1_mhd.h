@@ -5,7 +5,10 @@
  * one CUDA stream, the device copies of the solver's fields and the gather
  * tables of its boundary/halo synchronisations.  All entry points return 0 on
  * success and a positive MHD_E* code otherwise; nothing here exits or throws.
- * A context is not thread-safe; different contexts are independent.
+ * A context is not thread-safe; different contexts are independent.  A
+ * context lives on the CUDA device that was current when it was created;
+ * every entry point makes that device current for the duration of the call
+ * and restores the caller's current device before it returns.
  *
  * Field data cross this boundary in the reference's own host layout: a field
  * on block b is the half-open logical box [lo, hi) of its stagger location
@@ -32,7 +35,9 @@ extern "C" {
 #define MHD_ENOMEM 3      /* device or host allocation failed */
 #define MHD_EDT 4         /* time step underflow or NaN (dt < dt_abort) */
 #define MHD_ESTATE 5      /* call out of order (e.g. step before set-up) */
-#define MHD_EKRYLOV 6     /* implicit solve did not converge */
+#define MHD_EKRYLOV 6     /* a persistent Krylov solve gave up waiting at a grid barrier (a solve that
+                             does not converge is no error: it continues, as the reference does,
+                             with the reason in mhd_resistive_stats) */
 
 /* stagger locations, numbered as the reference's restart writer does
    (src/5_io/IOModule_Bin.cpp:62-85) */
@@ -138,12 +143,13 @@ int mhd_download_field(mhd_ctx *ctx, const char *name, int32_t block, double *da
    - The fields must have been synchronised on the device at least once (a
      step or mhd_update_derived) before the call, so that the read-out needs
      no new device tables.  Otherwise the call returns MHD_ESTATE.
-   - The first call on a device looks up the array's device address once for
-     that device, with the context's device current; make that first call
-     before any stream capture begins.
-   - All calls share the one array.  Each call overwrites the part it uses
-     and waits for its copy to finish before it returns.  Calls that overlap
-     on the same GPU (other host threads, other contexts) race. */
+   - The array's device address on the context's GPU is looked up when the
+     context is created (mhd_ctx_create / mhd_batch_create), so the read-out
+     itself does no set-up.
+   - All calls share the one array, whichever context makes them.  Each call
+     overwrites the part it uses and waits for its copy to finish before it
+     returns; the array keeps the last call's values.  Calls that overlap on
+     the same GPU (other host threads, other contexts) race. */
 #define MHD_NOALLOC_MAX_DOUBLES (1 << 21)
 int mhd_download_field_noalloc(mhd_ctx *ctx, const char *name, int32_t block, double *data, int64_t count);
 
@@ -306,6 +312,15 @@ const char *mhd_tune_name(int32_t i);
 /* Iterations, final residual norm, ||b|| and convergence reason (2 rtol,
    3 atol, -3 iteration limit, as KSPConvergedReason) of the last solve. */
 int mhd_resistive_stats(const mhd_ctx *ctx, int32_t *its, double *rnorm, double *bnorm, int32_t *reason);
+
+/* Failure-detection hook (no counterpart in the reference, whose solves
+   cannot stall): makes the grid barrier of the next persistent implicit
+   resistive solve wait for an arrival that never comes, and bounds every
+   wait of that solve at spin_limit polls (about 0.1 us each).  The solve
+   gives up, the step returns MHD_EKRYLOV, the barrier is reset, and the
+   context steps again once a good state is loaded.  Nothing faults or hangs:
+   every wait is bounded.  MHD_ESTATE without a persistent solve. */
+int mhd_test_stall_barrier(mhd_ctx *ctx, uint32_t spin_limit);
 
 /* LunarBoundary::Sync(group) on the device. */
 int mhd_sync(mhd_ctx *ctx, const char *group);

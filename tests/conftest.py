@@ -83,3 +83,24 @@ def periodic_setup(g):
         st.fields[name] = rst.FieldRecord(name, loc, a.shape[3], 4, [rst.FieldArray(lo, hi, a)])
     return spec, st
 
+
+
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "ref_lunar")
+
+
+def reference_run(spec, st, steps, workdir):
+    """The reference's own StepOnce (oracle/_ref/ref_lunar, built from the
+    reference's sources by __graft_entry__.build) on a case written in its
+    input formats: returns [RestartFile after the load, after step 1, ...]
+    with every state, derived and intermediate field and dt.  Skips the
+    calling test when the reference binary is not built."""
+    import subprocess
+
+    from beta1_b200 import case, rst
+    if not os.path.exists(REF_BIN):
+        pytest.skip("oracle/_ref/ref_lunar is not built (make -C oracle)")
+    case.write_case(workdir, spec)
+    rst.write(os.path.join(workdir, "init.rst"), st)
+    subprocess.run([REF_BIN, "run", "init.rst", str(steps), "step"], cwd=workdir, check=True,
+                   stdout=subprocess.DEVNULL)
+    return [rst.read(os.path.join(workdir, "step_%04d.bin" % s)) for s in range(steps + 1)]
