@@ -379,6 +379,10 @@ class Context:
         self._check(self.lib.mhd_get_time(self.h, C.byref(dt), C.byref(t), C.byref(s)), "get_time")
         return dt.value, t.value, s.value
 
+    def set_time(self, dt: float, time: float, step: int):
+        """dt, time and step count of every run"""
+        self._check(self.lib.mhd_set_time(self.h, float(dt), float(time), int(step)), "set_time")
+
     def state_count(self) -> int:
         return int(self.lib.mhd_state_count(self.h))
 

@@ -140,9 +140,10 @@ int mhd_download_field(mhd_ctx *ctx, const char *name, int32_t block, double *da
    Limits and rules:
    - A field of one block larger than MHD_NOALLOC_MAX_DOUBLES values is
      rejected with MHD_EINVAL.
-   - The fields must have been synchronised on the device at least once (a
-     step or mhd_update_derived) before the call, so that the read-out needs
-     no new device tables.  Otherwise the call returns MHD_ESTATE.
+   - The context must have taken at least one step (mhd_step or
+     mhd_batch_step) before the call, so that every sync table the read-out
+     may replay is already on the device.  Otherwise the call returns
+     MHD_ESTATE.
    - The array's device address on the context's GPU is looked up when the
      context is created (mhd_ctx_create / mhd_batch_create), so the read-out
      itself does no set-up.

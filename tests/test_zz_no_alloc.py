@@ -128,15 +128,16 @@ def test_noalloc_readout_rejects_fields_beyond_its_array():
 
 
 def test_noalloc_readout_refuses_before_the_sync_tables_are_built(golden_periodic):
-    """Before the first step or derived-field update the context's sync
-    tables are not on the device; building them would allocate, so the
-    read-out refuses with MHD_ESTATE."""
+    """Before the first step some of the context's sync tables are not on
+    the device; building them would allocate, so the read-out refuses with
+    MHD_ESTATE, and works after the first step."""
     spec, st = periodic_setup(golden_periodic["steps"])
     s = solver.Solver(spec)
     try:
         rc, _ = _raw_noalloc(s.ctx, "U_H")
         assert mhd.ERRORS.get(rc) == "ESTATE"
         s.load_state(st)
+        s.step(1)
         rc, u = _raw_noalloc(s.ctx, "U_H")
         assert rc == mhd.MHD_OK
         assert np.array_equal(u, s.field("U_H"))
