@@ -2,7 +2,7 @@
 
 Workloads (--workload):
 
-* c2 (default): 6 blocks of 96 x 48 x 48 cells (1,327,104 cells), radial
+* c2: 6 blocks of 96 x 48 x 48 cells (1,327,104 cells), radial
   cells log-spaced over r in [1, 8], a Solid_Surface inner wall and a
   Farfield outer boundary, inflow rho = 1, v = (-8, 0, 0),
   B = (0, 0.5, 0.5)/sqrt(2), p = 0.05 with seeded 1e-3 noise, and the
@@ -21,11 +21,16 @@ Workloads (--workload):
   MT19937_64(5) (beta1_b200.case.sweep_cases; 14.7 M cells in all), ideal
   MHD, each run with its own time step; mixed precision unless --precision
   fp64.  Host geometry is built by a spawned process pool.
-* c5s: the same sweep (same draws) with every run a single-block spherical
-  shell of Nr x Nt x Nph cells (Nph = Nt rounded up to even) with Pole
-  patches at both ends of theta (case.sweep_cases(grid="shell")).
+* c5s (default): the same sweep (same draws) with every run a single-block
+  spherical shell of Nr x Nt x Nph cells (Nph = Nt rounded up to even) with
+  Pole patches at both ends of theta (case.sweep_cases(grid="shell")),
+  15.3 M cells in all; geometry built on the device.  The line's value is
+  the mixed-precision form; the FP64 form is timed on the same runs in the
+  same job, and after the same steps every field of the mixed form is
+  compared with the FP64 form's (relative L2 over all runs) together with
+  max |div B| dx / |B|.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload c2|c1|c5|c5s|c3|c4]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload c5s|c2|c1|c5|c3|c4]
                     [--precision fp64|mixed]
 
 Multi-GPU (torchrun): the path does not shard, so N ranks run N independent
@@ -85,8 +90,21 @@ ALGO_BYTES_PER_CELL = {
     # U_plus 3, rho 1, u/v/w 3, B_cell 3, J_cell 3 read, RHS_H 5 and U_contra 3 written
     "k_fluid_mixed": 10 * 4 + 31 * 8,
 }
+ALGO_BYTES_PER_CELL.update({
+    # B_cell alone (the Pole path's unfused derived pass): B 3, Badd 3, W_B 18 read; B_cell 3, Bind_cell 3 written
+    "k_bcell": 30 * 8,
+    # J edges: B 3, beta 3, alpha 3 read; J 3 written
+    "k_jedge": 12 * 8,
+})
+# The flux + CT group (calc_PV, Scheme_U_ with its J x B source, the face and
+# edge EMF, the curl and both Euler updates): reads U 5, B_face 3, Badd 3,
+# JD 9, Jac 1, B_cell 3, J_cell 3; writes U 5, B_face 3.  FP64 35 x 8 =
+# 280 B per cell; mixed (JD, Jac, B_cell, J_cell as FP32 copies) 16 x 4 +
+# 19 x 8 = 216 B per cell.
+FLUX_CT_GROUP = ("k_fluid_ucontra", "k_fluid_mixed", "k_eface", "k_eedge", "k_curl_e2f", "k_update_u")
+FLUX_CT_BYTES = {False: 280, True: 216}
 WHOLE_GRID_KERNELS = {"k_pv_uplus_dt", "k_fluid_ucontra", "k_fluid_mixed", "k_bcell_jedge", "k_eface", "k_eedge",
-                      "k_update_u", "k_hall_cell", "k_hall_edge"}
+                      "k_update_u", "k_hall_cell", "k_hall_edge", "k_bcell", "k_jedge"}
 # the mixed form's PV pass also writes the 7 FP32 face states
 ALGO_BYTES_MIXED_EXTRA = {"k_pv_uplus_dt": 7 * 4}
 
@@ -94,7 +112,7 @@ ALGO_BYTES_MIXED_EXTRA = {"k_pv_uplus_dt": 7 * 4}
 # the dominant kernel, from one ncu capture of the C2 workload at half the
 # cells per direction (165,888 cells: 114.26 MB read + 10.32 MB written),
 # scaled by the cell count to a full C2 launch (1,327,104 cells; the kernel's
-# traffic grows with the cells it covers); profiles/k_pv_uplus_dt_c2small_fp64.md
+# traffic grows with the cells it covers)
 NCU_TRAFFIC_BYTES = {("k_pv_uplus_dt", "c2_slab6x96x48x48_implicit_resistive_fp64"): (114.25536e6 + 10.321408e6) * 8.0}
 
 
@@ -287,20 +305,96 @@ def cpu_reference_sweep(steps, nproc, nruns=SWEEP_RUNS, grid="slab"):
 SWEEP_SEED0 = 5000
 
 
-def build_sweep(precision, nruns=SWEEP_RUNS, workload="c5", geometry_on="host"):
-    """The sweep batch: host set-up of every run (node mesh, sync tables and,
+def sweep_host_setup(workload="c5", nruns=SWEEP_RUNS, geometry_on="host"):
+    """Host set-up of every run of the sweep (node mesh, sync tables and,
     unless the device builds it, the geometry) from a spawned process pool
-    (bounded by cores and memory), uploaded run by run as it arrives."""
+    bounded by cores and memory; returns (runs, [host set-up per run])."""
     import multiprocessing as mp
     from beta1_b200 import case, solver
     grid, topo = SWEEP_GRID[workload]
     runs = case.sweep_cases(nruns, grid=grid)
     nproc = max(1, min(len(runs), os.cpu_count() or 1, 16, int(mem_available_gb() / 8.0)))
     with mp.get_context("spawn").Pool(nproc) as pool:
-        host = pool.imap(solver.host_setup_run, [(spec, topo, geometry_on) for spec, _ in runs])
-        bt = solver.Batch([(spec, topo) for spec, _ in runs], precision=precision, host=host)
+        host = pool.map(solver.host_setup_run, [(spec, topo, geometry_on) for spec, _ in runs])
+    return runs, host
+
+
+def build_sweep(precision, runs, host, workload="c5"):
+    """The sweep batch from its host set-up, every run's seeded inflow state
+    loaded."""
+    from beta1_b200 import case, solver
+    topo = SWEEP_GRID[workload][1]
+    bt = solver.Batch([(spec, topo) for spec, _ in runs], precision=precision, host=iter(host))
     bt.load_states([case.inflow_state(spec, seed=SWEEP_SEED0 + r) for r, (spec, _) in enumerate(runs)])
-    return bt, sum(bt.cells), runs
+    return bt, sum(bt.cells)
+
+
+ERROR_FIELDS = ["U_H", "B_xi", "B_eta", "B_zeta", "PV_H", "B_cell", "J_cell"]
+
+
+def _inner(ctx, name, b, a):
+    """the inner points of a downloaded field (cells [0, n), faces [0, n])"""
+    inf = ctx.field_info(name, b)
+    blk = ctx.ncells[b]
+    hi = [n + (1 if name == "B_" + ax else 0) for n, ax in zip(blk, ("xi", "eta", "zeta"))]
+    return a[tuple(slice(-lo, -lo + h) for lo, h in zip(inf["lo"], hi))]
+
+
+def error_report(test, ref, nblocks):
+    """Relative L2 over every block's inner points of each field of `test`
+    against `ref` (two contexts advanced the same steps from the same state),
+    and max |div B| dx / |B| of `test` (dx the cube root of the cell
+    volume)."""
+    from beta1_b200 import mhd
+    test.stage(mhd.STAGE_DIVB)
+    num = {f: 0.0 for f in ERROR_FIELDS}
+    den = {f: 0.0 for f in ERROR_FIELDS}
+    divb = 0.0
+    for b in range(nblocks):
+        for f in ERROR_FIELDS:
+            a = _inner(test, f, b, test.download(f, b))
+            r = _inner(ref, f, b, ref.download(f, b))
+            num[f] += float(np.sum((a - r) ** 2))
+            den[f] += float(np.sum(r ** 2))
+        dx = np.cbrt(np.abs(_inner(test, "Jac", b, test.download("Jac", b))[..., 0]))
+        bmag = np.linalg.norm(_inner(test, "B_cell", b, test.download("B_cell", b)), axis=-1)
+        dv = np.abs(_inner(test, "divB", b, test.download("divB", b))[..., 0])
+        divb = max(divb, float(np.max(dv * dx / bmag)))
+    rel = {f: (float(np.sqrt(num[f] / den[f])) if den[f] > 0 else float(np.sqrt(num[f]))) for f in ERROR_FIELDS}
+    return rel, divb
+
+
+def timed_steps(ctx, steps, warmup, world, local, stream):
+    """W warm-up steps, then exactly `steps` steps between a barrier and a
+    device synchronisation on both sides, timed with CUDA events on the
+    context's stream while nvidia-smi samples the clocks.  Returns (ms,
+    kernel launches, clock samples)."""
+    import torch
+    import torch.distributed as dist
+    ctx.step(warmup)
+    clocks, stop = [], threading.Event()
+    try:
+        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        gpu_id = str(local)
+    th = threading.Thread(target=sample_clocks, args=(stop, clocks, gpu_id), daemon=True)
+    th.start()
+    time.sleep(0.25)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = ctx.launches()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    stop.set()
+    th.join()
+    return e0.elapsed_time(e1), ctx.launches() - l0, clocks
 
 
 def run_reference_arm(args):
@@ -347,7 +441,7 @@ def main():
     ap.add_argument("--steps", type=int, default=None, help="timed steps (default 200 for c2, 4000 for c1)")
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c2", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="c5s", choices=list(WORKLOADS))
     ap.add_argument("--n", type=int, default=64, help="cells per direction of the c1 periodic block")
     ap.add_argument("--c2-size", default="96x48", help="radial x transverse cells per c2 block (profiling runs "
                                                          "use a smaller case; the bench line is quoted on 96x48)")
@@ -355,11 +449,14 @@ def main():
     ap.add_argument("--e2e-iters", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep every kernel's default variant")
-    ap.add_argument("--geometry", default="host", choices=["host", "device"],
+    ap.add_argument("--geometry", default=None, choices=["host", "device"],
                     help="geometry fields built on the host and uploaded, or built on the device from the node "
-                         "meshes (mhd_build_geometry); same values")
+                         "meshes (mhd_build_geometry); same values (default: device for the sweeps, host otherwise)")
+    ap.add_argument("--no-fp64-compare", action="store_true",
+                    help="sweeps in mixed precision: skip timing the FP64 form on the same runs")
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
-                    help="fp64, or FP32 face fluxes with FP64 CT / state / residuals (default: fp64, mixed for c5)")
+                    help="fp64, or FP32 face fluxes with FP64 CT / state / residuals (default: mixed for c5, c5s "
+                         "and c4, fp64 otherwise)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -387,15 +484,22 @@ def main():
     wl = WORKLOADS[args.workload]
     mixed = args.precision == "mixed"
     prec = mhd.PREC_MIXED if mixed else mhd.PREC_FP64
+    sweep = args.workload in SWEEP_GRID
+    geometry_on = args.geometry or ("device" if sweep else "host")
     t_setup = time.time()
-    if args.workload in SWEEP_GRID:
-        s, cells, sweep = build_sweep(prec, workload=args.workload, geometry_on=args.geometry)
+    fp64_cmp = None
+    if sweep:
+        runs, host = sweep_host_setup(args.workload, geometry_on=geometry_on)
+        s, cells = build_sweep(prec, runs, host, args.workload)
         spec = None
-        nblocks = len(sweep)
+        nblocks = len(runs)
+        if mixed and not args.no_fp64_compare:
+            fp64_cmp, _ = build_sweep(mhd.PREC_FP64, runs, host, args.workload)
+        del host
     else:
         c2size = tuple(int(v) for v in args.c2_size.split("x"))
         spec, st, topology, cells = build_case(args.workload, args.n, c2size)
-        s = solver.Solver(spec, topology=topology, precision=prec, geometry_on=args.geometry)
+        s = solver.Solver(spec, topology=topology, precision=prec, geometry_on=geometry_on)
         if args.workload in ("c3", "c4"):
             # bounded: at most 10 Newton steps of at most 200 GMRES iterations per time step
             s.install_hall_implicit(topology, rtol=1e-10, atol=1e-50, maxit=10, ksp_rtol=1e-5, ksp_maxit=200)
@@ -413,40 +517,38 @@ def main():
         for b in range(nblocks))
     res_stats = None
 
-    # warm-up (also builds and instantiates the step graph)
-    ctx.step(args.warmup)
+    # the FP64 form on the same runs, same steps, for the speed ratio and the
+    # error report of the mixed form
+    fp64_line = None
+    if fp64_cmp is not None:
+        ctx64 = fp64_cmp.ctx
+        tuned64 = ctx64.autotune(reps=10) if not args.no_autotune else None
+        ms64, _, clocks64 = timed_steps(ctx64, args.steps, args.warmup, world, local,
+                                        torch.cuda.ExternalStream(ctx64.stream()))
+        ms64 = max_over_ranks(ms64, "cuda")
+        fp64_line = {"value": replica_throughput(world, cells, args.steps, ms64), "ms_per_step": ms64 / args.steps,
+                     "autotune_min_ctas_per_sm": tuned64, "clocks": summarize_clocks(clocks64)}
 
-    # timed region
-    clocks, stop = [], threading.Event()
-    try:
-        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
-    except Exception:
-        gpu_id = str(local)
-    th = threading.Thread(target=sample_clocks, args=(stop, clocks, gpu_id), daemon=True)
-    th.start()
-    time.sleep(0.25)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    l0 = ctx.launches()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    ctx.step(args.steps)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    ms = e0.elapsed_time(e1)
-    launches = ctx.launches() - l0
+    ms, launches, clocks = timed_steps(ctx, args.steps, args.warmup, world, local, stream)
     if spec is not None and spec.params.get("is_Lunar_resistance", 0):
         rs = ctx.resistive_stats()
         res_stats = {"krylov_its_last_step": rs["its"], "rnorm": rs["rnorm"], "bnorm": rs["bnorm"],
                      "reason": rs["reason"], "unknowns": int(len(s.resistive_dofs[0])), "rtol": float(spec.params["implicit_resistive_ksp_rtol"])}
-    stop.set()
-    th.join()
     ms_max = max_over_ranks(ms, "cuda")
     value = replica_throughput(world, cells, args.steps, ms_max)
+    if fp64_cmp is not None:
+        rel, divb = error_report(ctx, fp64_cmp.ctx, nblocks)
+        t_m = [ctx.run_time(r)[1] for r in range(ctx.nruns)]
+        t_d = [fp64_cmp.ctx.run_time(r)[1] for r in range(ctx.nruns)]
+        fp64_line.update({
+            "mixed_over_fp64": value / fp64_line["value"],
+            "steps_compared": args.warmup + args.steps,
+            "mixed_rel_l2_vs_fp64": {f: float("%.3e" % e) for f, e in rel.items()},
+            "mixed_max_rel_l2": max(rel.values()),
+            "mixed_max_divb_dx_over_b": divb,
+            "time_rel_diff": max(abs(a - b) / b for a, b in zip(t_m, t_d)),
+            "bounds": {"rel_l2": 1e-5, "divb_dx_over_b": 1e-12}})
+        fp64_cmp.ctx.close()
 
     # per-kernel durations: eager steps with an event pair around every launch
     prof = {}
@@ -455,16 +557,27 @@ def main():
             prof.setdefault(name, []).append(t)
     per_step = {k: sum(v) / 5.0 for k, v in prof.items()}
     total = sum(per_step.values())
-    dominant = max((k for k in per_step if k in ALGO_BYTES_PER_CELL), key=lambda k: per_step[k])
     launches_of = {k: len(v) / 5.0 for k, v in prof.items()}
+    # the dominant kernel by time over every kernel of the step
+    dominant = max(per_step, key=lambda k: per_step[k])
     avg_launch_ms = per_step[dominant] / launches_of[dominant]
-    algo = ALGO_BYTES_PER_CELL[dominant] + (ALGO_BYTES_MIXED_EXTRA.get(dominant, 0) if mixed else 0)
-    # kernels whose every launch covers the whole grid (the Hall EMF runs once
-    # per Newton / Krylov evaluation); other kernels' per-step bytes are
-    # shared by their launches (per-block or region launches)
-    bytes_per_launch = algo * cells if dominant in WHOLE_GRID_KERNELS else algo * cells / launches_of[dominant]
-    achieved = bytes_per_launch / (avg_launch_ms / 1000.0) / 1e9
+    if dominant == "k_gmres_resist" and res_stats is not None:
+        # per solve: 18 doubles per unknown triple per matvec (its + one per
+        # restart cycle) and (2k + 4) doubles per unknown in Arnoldi step k
+        n, its = res_stats["unknowns"], max(1, res_stats["krylov_its_last_step"])
+        bytes_per_launch = (its + 1) * 18 * 8 * (n / 3.0) + sum((2 * k + 4) * 8 * n for k in range(1, its + 1))
+    elif dominant in ALGO_BYTES_PER_CELL:
+        algo = ALGO_BYTES_PER_CELL[dominant] + (ALGO_BYTES_MIXED_EXTRA.get(dominant, 0) if mixed else 0)
+        # kernels whose every launch covers the whole grid (the Hall EMF runs
+        # once per Newton / Krylov evaluation); other kernels' per-step bytes
+        # are shared by their launches (per-block or region launches)
+        bytes_per_launch = algo * cells if dominant in WHOLE_GRID_KERNELS else algo * cells / launches_of[dominant]
+    else:
+        bytes_per_launch = None
+    achieved = bytes_per_launch / (avg_launch_ms / 1000.0) / 1e9 if bytes_per_launch else None
     peak, peak_kind = measured_peak()
+    group_ms = sum(per_step.get(k, 0.0) for k in FLUX_CT_GROUP)
+    group_gbs = FLUX_CT_BYTES[mixed] * cells / (group_ms / 1000.0) / 1e9 if group_ms > 0 else None
 
     # end to end through host buffers (pinned), H2D + D2H inside the region
     from beta1_b200.mhd import PinnedArray
@@ -524,15 +637,19 @@ def main():
                        "integrator": "forward Euler StepOnce (reference parity mode)", "precision": args.precision,
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "no flush: per-step working set %.2f GB > 126 MB L2" % (ctx_bytes / 1e9),
-                       "geometry": args.geometry, "setup_s": round(setup_s, 2)},
+                       "geometry": geometry_on, "setup_s": round(setup_s, 2)},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": nstate * 8,
                     "d2h_bytes_per_step": nstate * 8},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "frac": achieved / peak if achieved else None, "peak_kind": peak_kind,
                          "traffic": NCU_TRAFFIC_BYTES.get((dominant, config_name)),
                          "algo_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_launch_ms,
                          "kernel_share": per_step[dominant] / total},
+            "flux_ct_group": {"kernels": [k for k in FLUX_CT_GROUP if k in per_step], "ms_per_step": group_ms,
+                              "algo_bytes_per_cell": FLUX_CT_BYTES[mixed], "achieved": group_gbs, "unit": "GB/s",
+                              "frac": group_gbs / peak if group_gbs else None},
+            "fp64_same_runs": fp64_line,
             "kernels_ms_per_step": {k: round(v, 5) for k, v in sorted(per_step.items(), key=lambda kv: -kv[1])},
             "resistive_solve": res_stats,
             "cpu_baseline": cpu,

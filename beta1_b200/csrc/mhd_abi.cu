@@ -112,7 +112,7 @@ const char *const kKernelNames[] = {
     "k_bcell_jedge",  "k_fluid_ucontra", "k_wall_u_all",   "k_hall_cell",    "k_hall_edge",
     "k_pack_vec",     "k_hall_residual", "k_axpy_to",      "k_fd_quotient",  "k_negate",
     "k_geom32",       "k_fluid_mixed",  "k_gmres_resist", "k_pole",
-    "k_geometry",     "k_diag_init",   "k_diag"};
+    "k_geometry",     "k_diag_init",   "k_diag",        "k_rk2"};
 constexpr int kNumKernelNames = int(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
 
 } // namespace
@@ -249,6 +249,9 @@ struct mhd_ctx
     double hall_coef = 0.0;
     int *hall_zb = nullptr;
     int hall_nzb = 0;
+    // time integrator (MHD_INTEGRATOR_*) and the SSP-RK2 start-of-step state
+    int integrator = MHD_INTEGRATOR_EULER;
+    double *rk = nullptr;
     // explicit resistive sub-cycles (ResistiveDiffusionSubcycles_): 0 = off
     int res_nsub = 0;
     double res_inver_Rem = 0.0;
@@ -582,7 +585,7 @@ int launch_update_derived(mhd_ctx *ctx)
         return launch_update_derived_pole(ctx);
     cudaStream_t s = ctx->stream;
     prof_begin(ctx, "k_bcell_jedge");
-    launch_k_bcell_jedge(ctx->tune[TUNE_k_bcell_jedge], grid_kind(ctx, KIND_STAG), s, ctx->dbv);
+    launch_k_bcell_jedge(ctx->tune[TUNE_k_bcell_jedge], ctx->pool32 != nullptr, grid_kind(ctx, KIND_STAG), s, ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "B_cell"));
     RUN(run_sync(ctx, "Jedge"));
@@ -593,7 +596,8 @@ int launch_update_derived(mhd_ctx *ctx)
     // first ghost layer only: deeper PV / U_plus ghosts are read by no kernel
     // of the step and are filled when read out (materialise_pv)
     prof_begin(ctx, "k_pv_uplus_dt");
-    launch_k_pv_uplus_dt(ctx->tune[TUNE_k_pv_uplus_dt], grid_kind(ctx, KIND_CELL1), s, ctx->dbv, ctx->c, ctx->dt_key, 1, 1);
+    launch_k_pv_uplus_dt(ctx->tune[TUNE_k_pv_uplus_dt], ctx->pool32 != nullptr, grid_kind(ctx, KIND_CELL1), s, ctx->dbv,
+                         ctx->c, ctx->dt_key, 1, 1);
     ctx->pv_dirty = true;
     RUN(launched(ctx));
     RUN(run_sync(ctx, "J_cell"));
@@ -609,7 +613,8 @@ int launch_update_derived_pole(mhd_ctx *ctx)
 {
     cudaStream_t s = ctx->stream;
     prof_begin(ctx, "k_bcell");
-    k_bcell<<<dim3(grid_for(max_box(ctx, LOC_CELL, 0)), unsigned(ctx->nblocks)), kThreads, 0, s>>>(ctx->dbv);
+    launch_k_bcell(ctx->pool32 != nullptr, dim3(grid_for(max_box(ctx, LOC_CELL, 0)), unsigned(ctx->nblocks)), s,
+                   ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "B_cell"));
     RUN(launch_pole(ctx, POLE_BZETA));
@@ -621,7 +626,8 @@ int launch_update_derived_pole(mhd_ctx *ctx)
     k_arm_dt<<<1, 128, 0, s>>>(ctx->dt_key, ctx->nruns);
     RUN(launched(ctx));
     prof_begin(ctx, "k_pv_uplus_dt");
-    launch_k_pv_uplus_dt(ctx->tune[TUNE_k_pv_uplus_dt], grid_kind(ctx, KIND_CELL1), s, ctx->dbv, ctx->c, ctx->dt_key, 1, 1);
+    launch_k_pv_uplus_dt(ctx->tune[TUNE_k_pv_uplus_dt], ctx->pool32 != nullptr, grid_kind(ctx, KIND_CELL1), s, ctx->dbv,
+                         ctx->c, ctx->dt_key, 1, 1);
     ctx->pv_dirty = true;
     RUN(launched(ctx));
     RUN(launch_pole(ctx, POLE_JCELL));
@@ -1075,7 +1081,7 @@ int launch_resistive_explicit(mhd_ctx *ctx)
     {
         RUN(run_sync(ctx, "Bface"));
         prof_begin(ctx, "k_bcell");
-        k_bcell<<<dim3(grid_for(max_box(ctx, LOC_CELL, 0)), nb), kThreads, 0, s>>>(ctx->dbv);
+        launch_k_bcell(false, dim3(grid_for(max_box(ctx, LOC_CELL, 0)), nb), s, ctx->dbv);
         RUN(launched(ctx));
         RUN(run_sync(ctx, "B_cell"));
         prof_begin(ctx, "k_jedge");
@@ -1135,7 +1141,7 @@ int hall_emf_from_current_b(mhd_ctx *ctx)
     const int nb = ctx->nblocks;
     cudaStream_t s = ctx->stream;
     prof_begin(ctx, "k_bcell");
-    k_bcell<<<dim3(grid_for(max_box(ctx, LOC_CELL, 0)), nb), kThreads, 0, s>>>(ctx->dbv);
+    launch_k_bcell(false, dim3(grid_for(max_box(ctx, LOC_CELL, 0)), nb), s, ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "B_cell", true));
     prof_begin(ctx, "k_jedge");
@@ -1341,8 +1347,49 @@ int launch_step_a_mid(mhd_ctx *ctx)
     return MHD_OK;
 }
 
+// the resistive part of an Euler stage (implicit solve or explicit sub-cycles)
+int launch_resistive_part(mhd_ctx *ctx)
+{
+    if (ctx->res.on)
+        return launch_resistive(ctx);
+    if (ctx->res_nsub > 0)
+        return launch_resistive_explicit(ctx);
+    return MHD_OK;
+}
+
+int launch_rk2(mhd_ctx *ctx, int save)
+{
+    prof_begin(ctx, "k_rk2");
+    k_rk2<<<grid_kind(ctx, KIND_STAG), kThreads, 0, ctx->stream>>>(ctx->dbv, save);
+    return launched(ctx);
+}
+
+// One SSP-RK2 step (Shu and Osher, 1988) from two of StepOnce's Euler stages
+// at the dt of the step's start (the reference has only forward Euler,
+// Z4_Lunar/src/LunarSolver_Driver.cpp:21-92): U1 = U^n + dt L(U^n), with the
+// syncs and derived fields of the end of a step; U2 = U1 + dt L(U1); then
+// U^{n+1} = 0.5 (U^n + U2) on the points the Euler update writes, and the
+// step's closing syncs and derived fields.
+int launch_step_rk2(mhd_ctx *ctx)
+{
+    RUN(launch_rk2(ctx, 1));
+    RUN(launch_step_a(ctx));
+    RUN(launch_resistive_part(ctx));
+    RUN(run_sync(ctx, "Ucell"));
+    RUN(run_sync(ctx, "Bface"));
+    RUN(launch_update_derived(ctx));
+    RUN(launch_fluid_ucontra(ctx));
+    RUN(launch_induction(ctx, /*update_b=*/true, /*with_ucontra=*/false));
+    RUN(launch_update_u(ctx));
+    RUN(launch_resistive_part(ctx));
+    RUN(launch_rk2(ctx, 0));
+    return launch_step_c(ctx);
+}
+
 int launch_step(mhd_ctx *ctx)
 {
+    if (ctx->integrator == MHD_INTEGRATOR_SSPRK2)
+        return launch_step_rk2(ctx);
     RUN(launch_step_a(ctx));
     if (ctx->res.on)
         RUN(launch_resistive(ctx));
@@ -1427,6 +1474,12 @@ int build_graph(mhd_ctx *ctx)
     if (ctx->gexec || ctx->gexec_a)
         return MHD_OK;
     RUN(build_all_syncs(ctx));
+    if (ctx->integrator == MHD_INTEGRATOR_SSPRK2)
+    {
+        if (ctx->res.on && ctx->res.pgrid == 0)
+            return fail(ctx, MHD_ESTATE, "SSP-RK2 with the implicit resistive solve needs the persistent solve");
+        return capture(ctx, launch_step, &ctx->graph, &ctx->gexec, &ctx->graph_kernels);
+    }
     if (ctx->res.on && ctx->res.graph_loops && !ctx->hall.on)
     {
         const int rc = capture(ctx, launch_step, &ctx->graph, &ctx->gexec, &ctx->graph_kernels);
@@ -1574,7 +1627,7 @@ int create_ctx(const mhd_block_desc *blocks, int32_t nblocks, const int32_t *run
     {
         size_t n32 = 0;
         for (int b = 0; b < nblocks; ++b)
-            n32 += size_t(G32_N + Q32_N) * size_t(ctx->hbv[size_t(b)].vol);
+            n32 += size_t(G32_N + Q32_N + W32_N) * size_t(ctx->hbv[size_t(b)].vol);
         if (cudaMalloc(&ctx->pool32, n32 * sizeof(float)) != cudaSuccess)
             return bail(MHD_ENOMEM);
         if (cudaMemset(ctx->pool32, 0, n32 * sizeof(float)) != cudaSuccess)
@@ -1585,7 +1638,8 @@ int create_ctx(const mhd_block_desc *blocks, int32_t nblocks, const int32_t *run
             BlockView &v = ctx->hbv[size_t(b)];
             v.g32 = ctx->pool32 + o;
             v.q32 = v.g32 + size_t(G32_N) * size_t(v.vol);
-            o += size_t(G32_N + Q32_N) * size_t(v.vol);
+            v.w32 = v.q32 + size_t(Q32_N) * size_t(v.vol);
+            o += size_t(G32_N + Q32_N + W32_N) * size_t(v.vol);
         }
     }
     else if (params->precision != MHD_PREC_FP64)
@@ -1693,6 +1747,7 @@ int mhd_ctx_destroy(mhd_ctx *ctx)
     if (ctx->dt_key)
         cudaFree(ctx->dt_key);
     cudaFree(ctx->cta_tab);
+    cudaFree(ctx->rk);
     cudaFree(ctx->staging);
     cudaFree(ctx->dbv);
     cudaFree(ctx->pool);
@@ -1752,8 +1807,8 @@ static int transfer(mhd_ctx *ctx, const char *name, int32_t block, const double 
     const int nc = kFields[f].ncomp;
     if (hin)
     {
-        if (f == F_JDxi || f == F_JDeta || f == F_JDzeta)
-            ctx->geom_dirty = true;
+        if (f == F_JDxi || f == F_JDeta || f == F_JDzeta || f == F_WB || f == F_WJ)
+            ctx->geom_dirty = true; // face normals and the FP32 copies follow
         CK(ctx, cudaMemcpyAsync(ctx->staging, hin, size_t(n) * 8, cudaMemcpyHostToDevice, ctx->stream));
         prof_begin(ctx, "k_aos_to_soa");
         k_aos_to_soa<<<grid_for(n), kThreads, 0, ctx->stream>>>(ctx->dbv, block, f, nc, lo[0], lo[1], lo[2],
@@ -2125,8 +2180,8 @@ static int materialise_pv(mhd_ctx *ctx)
     RUN(materialise_group(ctx, "Ucell"));
     RUN(ensure_geom(ctx));
     prof_begin(ctx, "k_pv_uplus_dt");
-    launch_k_pv_uplus_dt(ctx->tune[TUNE_k_pv_uplus_dt], dim3(grid_for(max_box(ctx, LOC_CELL, ctx->G)), ctx->nblocks), ctx->stream, 
-        ctx->dbv, ctx->c, nullptr, ctx->G, 0);
+    launch_k_pv_uplus_dt(ctx->tune[TUNE_k_pv_uplus_dt], false, dim3(grid_for(max_box(ctx, LOC_CELL, ctx->G)), ctx->nblocks),
+                         ctx->stream, ctx->dbv, ctx->c, nullptr, ctx->G, 0);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "Uplus", true));
     ctx->pv_dirty = false;
@@ -2669,6 +2724,8 @@ int mhd_set_hall_implicit(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, int6
     if (!ctx || n < 0 || nalias < 0 || maxit < 0 || ksp_maxit < 1 || (n > 0 && !unknowns) ||
         (nalias > 0 && (!alias || !owner || !sign)))
         return fail(ctx, MHD_EINVAL, "bad implicit Hall arguments");
+    if (n > 0 && ctx->integrator != MHD_INTEGRATOR_EULER)
+        return fail(ctx, MHD_ESTATE, "the implicit Hall solve runs with the Euler integrator only");
     if (ctx->nruns > 1 && n > 0)
         return fail(ctx, MHD_ESTATE, "the implicit Hall solve is not available in a batch of runs (one shared dt per solve)");
     if (!ctx->poles.empty() && n > 0)
@@ -2927,6 +2984,45 @@ int mhd_resistive_stats(const mhd_ctx *ctx, int32_t *its, double *rnorm, double 
     return MHD_OK;
 }
 
+int mhd_set_integrator(mhd_ctx *ctx, int32_t integrator)
+{
+    BIND_DEVICE(ctx);
+    if (!ctx)
+        return MHD_EINVAL;
+    if (integrator != MHD_INTEGRATOR_EULER && integrator != MHD_INTEGRATOR_SSPRK2)
+        return fail(ctx, MHD_EINVAL, "unknown integrator %d", integrator);
+    if (ctx->capturing)
+        return fail(ctx, MHD_ESTATE, "integrator changed during capture");
+    if (integrator == MHD_INTEGRATOR_SSPRK2)
+    {
+        if (ctx->hall.on)
+            return fail(ctx, MHD_ESTATE, "SSP-RK2 is not available with the implicit Hall solve");
+        if (!ctx->rk)
+        {
+            size_t n = 0;
+            for (const auto &v : ctx->hbv)
+                n += 8 * size_t(v.vol);
+            CK(ctx, cudaMalloc(&ctx->rk, n * sizeof(double)));
+            CK(ctx, cudaMemsetAsync(ctx->rk, 0, n * sizeof(double), ctx->stream));
+            size_t o = 0;
+            for (auto &v : ctx->hbv)
+            {
+                v.rk = ctx->rk + o;
+                o += 8 * size_t(v.vol);
+            }
+            CK(ctx, cudaMemcpyAsync(ctx->dbv, ctx->hbv.data(), sizeof(BlockView) * ctx->hbv.size(),
+                                    cudaMemcpyHostToDevice, ctx->stream));
+            CK(ctx, cudaStreamSynchronize(ctx->stream));
+        }
+    }
+    if (integrator != ctx->integrator)
+    {
+        ctx->integrator = integrator;
+        drop_graph(ctx);
+    }
+    return MHD_OK;
+}
+
 int mhd_test_stall_barrier(mhd_ctx *ctx, uint32_t spin_limit)
 {
     BIND_DEVICE(ctx);
@@ -3118,7 +3214,7 @@ int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
             return fail(ctx, MHD_ESTATE, "the implicit Hall solve is not set up");
         RUN(launch_hall_implicit(ctx));
         prof_begin(ctx, "k_bcell");
-        k_bcell<<<dim3(grid_for(max_box(ctx, LOC_CELL, 0)), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv);
+        launch_k_bcell(false, dim3(grid_for(max_box(ctx, LOC_CELL, 0)), ctx->nblocks), ctx->stream, ctx->dbv);
         RUN(launched(ctx));
         RUN(run_sync(ctx, "B_cell"));
         break;

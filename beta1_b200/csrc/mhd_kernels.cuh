@@ -32,10 +32,13 @@ __global__ void k_update_u(const BlockView *bvs, const double *dtp);
 __global__ void k_divb(const BlockView *bvs);
 // mixed precision (mhd_kernels_mixed.cu)
 __global__ void k_geom32(const BlockView *bvs);
+__global__ void k_rk2(const BlockView *bvs, int save);
 __global__ void k_hall_cell(const BlockView *bvs, Consts c, double hall_coef);
 __global__ void k_hall_edge(const BlockView *bvs, const int *zb, int nzb);
 __global__ void k_eres_explicit(const BlockView *bvs, double inver_Rem);
-__global__ void k_bcell(const BlockView *bvs);
+// calc_Bcell on the inner cells (2-D launch, one grid row per block); w32:
+// from the FP32 weight copies (mixed form)
+void launch_k_bcell(bool w32, dim3 grid, cudaStream_t st, const BlockView *bvs);
 __global__ void k_jedge(const BlockView *bvs, int fB0, int fJ0, double mult, const int *rng);
 __global__ void k_jcell(const BlockView *bvs);
 
@@ -167,13 +170,14 @@ __global__ void k_negate(double *out, const double *x, int64_t n);
 // different __launch_bounds__ minimum CTAs per SM; 0 = no launch bounds, the
 // compiler's own allocation); variant 0 is the default.  Returns -1 for an
 // unknown variant.
-// k_pv_uplus_dt: minimum CTAs per SM 4, 0, 5
-int launch_k_pv_uplus_dt(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c,
+// k_pv_uplus_dt: minimum CTAs per SM 4, 0, 5; w32: J_cell from the FP32
+// weight copies (mixed form)
+int launch_k_pv_uplus_dt(int variant, bool w32, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c,
                          unsigned long long *dt_key, int depth, int with_jcell);
 // k_fluid_ucontra: minimum CTAs per SM 0, 3
 int launch_k_fluid_ucontra(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c);
-// k_bcell_jedge: minimum CTAs per SM 0, 6
-int launch_k_bcell_jedge(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs);
+// k_bcell_jedge: minimum CTAs per SM 0, 6; w32 as above
+int launch_k_bcell_jedge(int variant, bool w32, dim3 grid, cudaStream_t st, const BlockView *bvs);
 // k_eface: minimum CTAs per SM 0, 6
 int launch_k_eface(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs);
 // k_curl_e2f: minimum CTAs per SM 0, 6

@@ -755,9 +755,62 @@ __global__ void k_update_u(const BlockView *__restrict__ bvs, const double *__re
         b.f[F_U][m * b.vol + p] += dt * b.f[F_RHS][m * b.vol + p];
 }
 
+// SSP-RK2 (Shu and Osher, 1988) from two Euler stages at one dt: the state
+// of the step's start on the points the Euler update writes (inner cells,
+// inner faces), then U^{n+1} = 0.5 (U^n + U2) there.  save = 1 stores,
+// save = 0 averages.
+__global__ void k_rk2(const BlockView *__restrict__ bvs, int save)
+{
+    int64_t t;
+    const BlockView &b = bvs[cta_block(bvs, KIND_STAG, t)];
+    int i, j, k;
+    if (!stagger_point(b, nullptr, 0, t, i, j, k))
+        return;
+    const int64_t p = pidx(b, i, j, k);
+    const int64_t v = b.vol;
+    double *r = b.rk;
+    if (i < b.ni && j < b.nj && k < b.nk)
+    {
+        double *U = b.f[F_U];
+#pragma unroll
+        for (int m = 0; m < 5; ++m)
+        {
+            if (save)
+                r[m * v + p] = U[m * v + p];
+            else
+                U[m * v + p] = 0.5 * (r[m * v + p] + U[m * v + p]);
+        }
+    }
+#pragma unroll
+    for (int fa = 0; fa < 3; ++fa)
+        if (inner_of(b, 0, fa, i, j, k))
+        {
+            double *B = b.f[F_Bxi + fa];
+            double *R = r + (5 + fa) * v;
+            if (save)
+                R[p] = B[p];
+            else
+                B[p] = 0.5 * (R[p] + B[p]);
+        }
+}
+
+// least-squares weight planes of a block: the FP64 field, or its FP32 copy
+template <typename WT> __device__ __forceinline__ const WT *weights(const BlockView &b, int f, int plane32);
+template <> __device__ __forceinline__ const double *weights<double>(const BlockView &b, int f, int)
+{
+    return b.f[f];
+}
+template <> __device__ __forceinline__ const float *weights<float>(const BlockView &b, int, int plane32)
+{
+    return b.w32 + int64_t(plane32) * b.vol;
+}
+
 // ---------------------------------------------------------------------------
 // calc_Bcell (Z4_Lunar/src/physics/LunarSolver_Tools.cpp:163-241)
 // ---------------------------------------------------------------------------
+// WT: double (the reference's weights, FP64 form) or float (their FP32
+// copies, mixed form: the products and sums stay FP64)
+template <typename WT>
 __device__ __forceinline__ void bcell_one(const BlockView &b, int i, int j, int k)
 {
     const double *Bx = b.f[F_Bxi], *Be = b.f[F_Beta], *Bz = b.f[F_Bzeta];
@@ -767,15 +820,15 @@ __device__ __forceinline__ void bcell_one(const BlockView &b, int i, int j, int 
     const double phi_tot[6] = {-Bx[p] - Ax[p], Bx[pi1] + Ax[pi1], -Be[p] - Ae[p],
                                Be[pj1] + Ae[pj1], -Bz[p] - Az[p], Bz[pk1] + Az[pk1]};
     const double phi_ind[6] = {-Bx[p], Bx[pi1], -Be[p], Be[pj1], -Bz[p], Bz[pk1]};
-    const double *W = b.f[F_WB];
     const int64_t v = b.vol;
+    const WT *W = weights<WT>(b, F_WB, W32_B);
     double bxt = 0.0, byt = 0.0, bzt = 0.0, bxi = 0.0, byi = 0.0, bzi = 0.0;
 #pragma unroll
     for (int q = 0; q < 6; ++q)
     {
-        const double wx = W[q * v + p];
-        const double wy = W[(6 + q) * v + p];
-        const double wz = W[(12 + q) * v + p];
+        const double wx = double(W[q * v + p]);
+        const double wy = double(W[(6 + q) * v + p]);
+        const double wz = double(W[(12 + q) * v + p]);
         bxt += wx * phi_tot[q];
         byt += wy * phi_tot[q];
         bzt += wz * phi_tot[q];
@@ -792,7 +845,7 @@ __device__ __forceinline__ void bcell_one(const BlockView &b, int i, int j, int 
     Bi[2 * v + p] = bzi;
 }
 
-__global__ void k_bcell(const BlockView *__restrict__ bvs)
+template <typename WT> __global__ void k_bcell_w(const BlockView *__restrict__ bvs)
 {
     const BlockView &b = bvs[blockIdx.y];
     int lo[3], n[3];
@@ -800,7 +853,15 @@ __global__ void k_bcell(const BlockView *__restrict__ bvs)
     int i, j, k;
     if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
         return;
-    bcell_one(b, i, j, k);
+    bcell_one<WT>(b, i, j, k);
+}
+
+void launch_k_bcell(bool w32, dim3 grid, cudaStream_t st, const BlockView *bvs)
+{
+    if (w32)
+        k_bcell_w<float><<<grid, 256, 0, st>>>(bvs);
+    else
+        k_bcell_w<double><<<grid, 256, 0, st>>>(bvs);
 }
 
 // ---------------------------------------------------------------------------
@@ -851,7 +912,7 @@ __global__ void k_jedge(const BlockView *__restrict__ bvs, int fB0, int fJ0, dou
 // calc_Bcell and Calc_J_Edge in one pass over the staggered points: both
 // read the face B around the same points (the B_cell sync between them in
 // the reference touches neither input)
-__device__ __forceinline__ void k_bcell_jedge_body(const BlockView *__restrict__ bvs)
+template <typename WT> __device__ __forceinline__ void k_bcell_jedge_body(const BlockView *__restrict__ bvs)
 {
     int64_t t;
     const BlockView &b = bvs[cta_block(bvs, KIND_STAG, t)];
@@ -859,44 +920,45 @@ __device__ __forceinline__ void k_bcell_jedge_body(const BlockView *__restrict__
     if (!stagger_point(b, nullptr, 0, t, i, j, k))
         return;
     if (i < b.ni && j < b.nj && k < b.nk)
-        bcell_one(b, i, j, k);
+        bcell_one<WT>(b, i, j, k);
 #pragma unroll
     for (int ea = 0; ea < 3; ++ea)
         if (inner_of(b, 1, ea, i, j, k))
             jedge_one(b, ea, i, j, k, F_Bxi, F_Jxi, 1.0);
 }
 
-template <int MINB> __global__ void __launch_bounds__(256, MINB) k_bcell_jedge_t(const BlockView *__restrict__ bvs)
+template <typename WT, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_bcell_jedge_t(const BlockView *__restrict__ bvs)
 {
-    k_bcell_jedge_body(bvs);
+    k_bcell_jedge_body<WT>(bvs);
 }
 // the compiler's own register allocation (no launch bounds)
-__global__ void k_bcell_jedge_free(const BlockView *__restrict__ bvs)
+template <typename WT> __global__ void k_bcell_jedge_free(const BlockView *__restrict__ bvs)
 {
-    k_bcell_jedge_body(bvs);
+    k_bcell_jedge_body<WT>(bvs);
 }
 
 
 // ---------------------------------------------------------------------------
 // calc_Jcell (LunarSolver_Tools.cpp:837-892)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void jcell_one(const BlockView &b, int i, int j, int k)
+template <typename WT> __device__ __forceinline__ void jcell_one(const BlockView &b, int i, int j, int k)
 {
     const double *Jx = b.f[F_Jxi], *Je = b.f[F_Jeta], *Jz = b.f[F_Jzeta];
     const double s[12] = {Jx[pidx(b, i, j, k)],         Jx[pidx(b, i, j + 1, k)],     Jx[pidx(b, i, j, k + 1)],
                           Jx[pidx(b, i, j + 1, k + 1)], Je[pidx(b, i, j, k)],         Je[pidx(b, i + 1, j, k)],
                           Je[pidx(b, i, j, k + 1)],     Je[pidx(b, i + 1, j, k + 1)], Jz[pidx(b, i, j, k)],
                           Jz[pidx(b, i + 1, j, k)],     Jz[pidx(b, i, j + 1, k)],     Jz[pidx(b, i + 1, j + 1, k)]};
-    const double *W = b.f[F_WJ];
+    const WT *W = weights<WT>(b, F_WJ, W32_J);
     const int64_t p = pidx(b, i, j, k);
     const int64_t v = b.vol;
     double jx = 0.0, jy = 0.0, jz = 0.0;
 #pragma unroll
     for (int q = 0; q < 12; ++q)
     {
-        jx += W[q * v + p] * s[q];
-        jy += W[(12 + q) * v + p] * s[q];
-        jz += W[(24 + q) * v + p] * s[q];
+        jx += double(W[q * v + p]) * s[q];
+        jy += double(W[(12 + q) * v + p]) * s[q];
+        jz += double(W[(24 + q) * v + p]) * s[q];
     }
     double *Jc = b.f[F_Jcell];
     Jc[p] = jx;
@@ -912,7 +974,7 @@ __global__ void k_jcell(const BlockView *__restrict__ bvs)
     int i, j, k;
     if (!box_point(lo, n, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, i, j, k))
         return;
-    jcell_one(b, i, j, k);
+    jcell_one<double>(b, i, j, k);
 }
 
 // ---------------------------------------------------------------------------
@@ -960,6 +1022,7 @@ __device__ __forceinline__ unsigned long long dbl_key(double x)
 // variants: at least 4 CTAs per SM (64 registers; the default: the extra
 // warps hide more of the weight-stream latency, 0.216 -> 0.205 ms on the C2
 // step against the uncapped 80 registers), uncapped, at least 5
+template <typename WT>
 __device__ __forceinline__ void k_pv_uplus_dt_body(const BlockView *__restrict__ bvs, Consts c, unsigned long long *dt_key, int depth,
                               int with_jcell)
 {
@@ -974,7 +1037,7 @@ __device__ __forceinline__ void k_pv_uplus_dt_body(const BlockView *__restrict__
         // calc_Jcell on inner cells in the same pass: its weight stream
         // overlaps this kernel's FP64 work (J_cell is not read here)
         if (with_jcell && i >= 0 && j >= 0 && k >= 0 && i < b.ni && j < b.nj && k < b.nk)
-            jcell_one(b, i, j, k);
+            jcell_one<WT>(b, i, j, k);
         const int64_t p = pidx(b, i, j, k);
         const int64_t v = b.vol;
         const double *U = b.f[F_U];
@@ -1084,16 +1147,18 @@ __device__ __forceinline__ void k_pv_uplus_dt_body(const BlockView *__restrict__
     }
 }
 
-template <int MINB> __global__ void __launch_bounds__(256, MINB) k_pv_uplus_dt_t(const BlockView *__restrict__ bvs, Consts c, unsigned long long *dt_key, int depth,
+template <typename WT, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_pv_uplus_dt_t(const BlockView *__restrict__ bvs, Consts c, unsigned long long *dt_key, int depth,
                               int with_jcell)
 {
-    k_pv_uplus_dt_body(bvs, c, dt_key, depth, with_jcell);
+    k_pv_uplus_dt_body<WT>(bvs, c, dt_key, depth, with_jcell);
 }
 // the compiler's own register allocation (no launch bounds)
+template <typename WT>
 __global__ void k_pv_uplus_dt_free(const BlockView *__restrict__ bvs, Consts c, unsigned long long *dt_key, int depth,
                               int with_jcell)
 {
-    k_pv_uplus_dt_body(bvs, c, dt_key, depth, with_jcell);
+    k_pv_uplus_dt_body<WT>(bvs, c, dt_key, depth, with_jcell);
 }
 
 
@@ -1654,24 +1719,34 @@ __global__ void __launch_bounds__(256) k_gmres_resist(ResistSolve a)
 }
 
 // launchers of the register / occupancy variants (tuned by mhd_autotune)
-int launch_k_pv_uplus_dt(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c, unsigned long long *dt_key, int depth,
-                              int with_jcell)
+template <typename WT>
+int launch_pv_variant(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c, unsigned long long *dt_key,
+                      int depth, int with_jcell)
 {
     switch (variant)
     {
     case 0:
-        k_pv_uplus_dt_t<4><<<grid, 256, 0, st>>>(bvs, c, dt_key, depth, with_jcell);
+        k_pv_uplus_dt_t<WT, 4><<<grid, 256, 0, st>>>(bvs, c, dt_key, depth, with_jcell);
         break;
     case 1:
-        k_pv_uplus_dt_free<<<grid, 256, 0, st>>>(bvs, c, dt_key, depth, with_jcell);
+        k_pv_uplus_dt_free<WT><<<grid, 256, 0, st>>>(bvs, c, dt_key, depth, with_jcell);
         break;
     case 2:
-        k_pv_uplus_dt_t<5><<<grid, 256, 0, st>>>(bvs, c, dt_key, depth, with_jcell);
+        k_pv_uplus_dt_t<WT, 5><<<grid, 256, 0, st>>>(bvs, c, dt_key, depth, with_jcell);
         break;
     default:
         return -1;
     }
     return 0;
+}
+
+// w32: the mixed form's FP32 weight copies (a separate instantiation, so the
+// FP64 form's kernel is unchanged)
+int launch_k_pv_uplus_dt(int variant, bool w32, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c,
+                         unsigned long long *dt_key, int depth, int with_jcell)
+{
+    return w32 ? launch_pv_variant<float>(variant, grid, st, bvs, c, dt_key, depth, with_jcell)
+               : launch_pv_variant<double>(variant, grid, st, bvs, c, dt_key, depth, with_jcell);
 }
 
 int launch_k_fluid_ucontra(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c)
@@ -1690,20 +1765,26 @@ int launch_k_fluid_ucontra(int variant, dim3 grid, cudaStream_t st, const BlockV
     return 0;
 }
 
-int launch_k_bcell_jedge(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs)
+template <typename WT> int launch_bcell_jedge_variant(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs)
 {
     switch (variant)
     {
     case 0:
-        k_bcell_jedge_free<<<grid, 256, 0, st>>>(bvs);
+        k_bcell_jedge_free<WT><<<grid, 256, 0, st>>>(bvs);
         break;
     case 1:
-        k_bcell_jedge_t<6><<<grid, 256, 0, st>>>(bvs);
+        k_bcell_jedge_t<WT, 6><<<grid, 256, 0, st>>>(bvs);
         break;
     default:
         return -1;
     }
     return 0;
+}
+
+int launch_k_bcell_jedge(int variant, bool w32, dim3 grid, cudaStream_t st, const BlockView *bvs)
+{
+    return w32 ? launch_bcell_jedge_variant<float>(variant, grid, st, bvs)
+               : launch_bcell_jedge_variant<double>(variant, grid, st, bvs);
 }
 
 int launch_k_eface(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs)

@@ -20,7 +20,8 @@ namespace mhd
 
 __device__ __forceinline__ float fmaxs(float a, float b) { return (a < b) ? b : a; }
 
-// FP32 copy of the face areas |JD| on every point of the padded box
+// FP32 copies of the face areas |JD| and of the B_cell / J_cell
+// least-squares weights on every point of the padded box
 __global__ void k_geom32(const BlockView *__restrict__ bvs)
 {
     const BlockView &b = bvs[blockIdx.y];
@@ -31,6 +32,10 @@ __global__ void k_geom32(const BlockView *__restrict__ bvs)
 #pragma unroll
     for (int a = 0; a < 3; ++a)
         b.g32[(G32_AREA + a) * v + p] = float(b.f[F_NAxi + a][p]);
+    for (int q = 0; q < 18; ++q)
+        b.w32[(W32_B + q) * v + p] = float(b.f[F_WB][q * v + p]);
+    for (int q = 0; q < 36; ++q)
+        b.w32[(W32_J + q) * v + p] = float(b.f[F_WJ][q * v + p]);
 }
 
 // reference-state constants of the deviation flux, FP32

@@ -131,6 +131,10 @@ struct BlockView
     // mixed precision only (null otherwise): FP32 planes on the same padded box
     float *g32;       // face area xi, eta, zeta
     float *q32;       // face-state quantities rho, u, v, w, p, rhoE, c
+    float *w32;       // least-squares weights: Bcell_from_Bface_w (18 planes), Jcell_from_Jedge_w (36)
+    // SSP-RK2 only (null otherwise): the state at the step's start, U_H 5
+    // planes then B_xi, B_eta, B_zeta, on the same padded box
+    double *rk;
     // run (independent time line) the block belongs to, and that run's
     // reference state of the mixed-precision flux (rho, u, v, w, p, E)
     int run;
@@ -179,7 +183,10 @@ enum : int
     Q32_P = 4,
     Q32_RHOE = 5,
     Q32_C = 6,
-    Q32_N = 7
+    Q32_N = 7,
+    W32_B = 0,
+    W32_J = 18,
+    W32_N = 54
 };
 
 __host__ __device__ inline int64_t pidx(const BlockView &b, int i, int j, int k)

@@ -29,6 +29,8 @@ PREC_MIXED = 1
 STAGE_TIMESTEP, STAGE_FLUID_RHS, STAGE_INDUCTION, STAGE_UPDATE, STAGE_DIVB, STAGE_HALL_EMF = 1, 2, 3, 4, 5, 6
 STAGE_HALL_SOLVE = 7
 
+INTEGRATOR_EULER, INTEGRATOR_SSPRK2 = 0, 1
+
 
 class BlockDesc(C.Structure):
     _fields_ = [("ni", C.c_int32), ("nj", C.c_int32), ("nk", C.c_int32)]
@@ -63,6 +65,7 @@ _SIGS = {
     "mhd_set_sync_map": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64]),
     "mhd_sync": (C.c_int, [C.c_void_p, C.c_char_p]),
     "mhd_test_stall_barrier": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "mhd_set_integrator": (C.c_int, [C.c_void_p, C.c_int32]),
     "mhd_set_sync_consts": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64]),
     "mhd_set_sync_wall": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_int32]),
     "mhd_set_sync_map_post": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64]),
@@ -353,6 +356,11 @@ class Context:
         self._check(self.lib.mhd_resistive_stats(self.h, C.byref(its), C.byref(rn), C.byref(bn), C.byref(rs)),
                     "resistive_stats")
         return dict(its=its.value, rnorm=rn.value, bnorm=bn.value, reason=rs.value)
+
+    def set_integrator(self, integrator: int):
+        """INTEGRATOR_EULER (the reference's StepOnce) or INTEGRATOR_SSPRK2
+        (two Euler stages at one dt and their convex average)"""
+        self._check(self.lib.mhd_set_integrator(self.h, int(integrator)), "set_integrator")
 
     def test_stall_barrier(self, spin_limit: int):
         """failure-detection hook: the next persistent resistive solve waits

@@ -314,6 +314,20 @@ const char *mhd_tune_name(int32_t i);
    3 atol, -3 iteration limit, as KSPConvergedReason) of the last solve. */
 int mhd_resistive_stats(const mhd_ctx *ctx, int32_t *its, double *rnorm, double *bnorm, int32_t *reason);
 
+/* Time integrator of every following step.  The reference has one: a single
+   forward-Euler stage per StepOnce (Z4_Lunar/src/LunarSolver_Driver.cpp:21-92,
+   Z4_Lunar/src/physics/LunarSolver_Advance.cpp:61-122), MHD_INTEGRATOR_EULER,
+   the default.  MHD_INTEGRATOR_SSPRK2 composes two of those Euler stages at
+   the dt of the step's start (Shu-Osher SSP-RK2): U1 = U^n + dt L(U^n), with
+   Sync("Ucell"), Sync("Bface") and UpdateDerivedFields_ after it, then
+   U^{n+1} = 0.5 (U^n + (U1 + dt L(U1))) on the inner cells and faces, then
+   the step's closing syncs and derived fields.  Each stage includes the
+   resistive part.  Not available with the implicit Hall solve (MHD_ESTATE).
+   Allocates the start-of-step copy of U_H and face B on first use. */
+#define MHD_INTEGRATOR_EULER 0
+#define MHD_INTEGRATOR_SSPRK2 1
+int mhd_set_integrator(mhd_ctx *ctx, int32_t integrator);
+
 /* Failure-detection hook (no counterpart in the reference, whose solves
    cannot stall): makes the grid barrier of the next persistent implicit
    resistive solve wait for an arrival that never comes, and bounds every

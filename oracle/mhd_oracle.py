@@ -530,6 +530,50 @@ class Oracle:
         solve when it is set up, then the closing syncs and derived fields."""
         self.compute_timestep()
         dt = self.dt
+        self.euler_stage(dt)
+        self.time += dt
+        self.sync("Ucell")
+        self.sync("Bface")
+        self.update_derived()
+        return dt
+
+    STATE = (("U_H", 0, 5), ("B_xi", 1, 1), ("B_eta", 2, 1), ("B_zeta", 3, 1))
+
+    def rk2_step(self):
+        """SSP-RK2 (Shu and Osher, 1988) from two StepOnce Euler stages at the
+        dt of the step's start (the composition the reference harness's rk2
+        command runs with the reference's own stage functions): U1 = U^n +
+        dt L(U^n) with the closing syncs and derived fields, U2 = U1 + dt L(U1),
+        U^{n+1} = 0.5 (U^n + U2) on the inner cells and faces, then the closing
+        syncs and derived fields."""
+        self.compute_timestep()
+        dt = self.dt
+        saved = []
+        for blk in self.blocks:
+            keep = {}
+            for name, loc, nc in self.STATE:
+                lo, hi = blk.inner(loc)
+                keep[name] = [blk.box(name, m, lo, hi).copy() for m in range(nc)]
+            saved.append(keep)
+        self.euler_stage(dt)
+        self.sync("Ucell")
+        self.sync("Bface")
+        self.update_derived()
+        self.euler_stage(dt)
+        for blk, keep in zip(self.blocks, saved):
+            for name, loc, nc in self.STATE:
+                lo, hi = blk.inner(loc)
+                for m in range(nc):
+                    blk.f[name][m][blk.s(lo, hi)] = 0.5 * (keep[name][m] + blk.box(name, m, lo, hi))
+        self.time += dt
+        self.sync("Ucell")
+        self.sync("Bface")
+        self.update_derived()
+        return dt
+
+    def euler_stage(self, dt):
+        """The forward-Euler stage of StepOnce at a given dt (fluid RHS, CT
+        induction, update, resistive part), without the closing syncs."""
         self.fluid_rhs()
         for blk in self.blocks:
             self.eface(blk)
@@ -550,11 +594,6 @@ class Oracle:
             self.resistive_step()
         elif self.explicit is not None:
             self.resistive_subcycles()
-        self.time += dt
-        self.sync("Ucell")
-        self.sync("Bface")
-        self.update_derived()
-        return dt
 
     # ------------------------------------------------------ implicit resistivity
     def set_resistive(self, unknowns, eta, alias, owner, sign):

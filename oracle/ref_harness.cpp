@@ -10,6 +10,7 @@
 // Usage (run inside a case directory holding ./CASE):
 //   ref_lunar geom  <out.bin>                      geometry + node coordinates
 //   ref_lunar run   <state.rst> <nsteps> <prefix>  state after each StepOnce
+//   ref_lunar rk2   <state.rst> <nsteps> <prefix>  state after each SSP-RK2 step of two Euler stages
 //   ref_lunar probe <state.rst> <group> <out.bin>  index-encoded Sync(group)
 //   ref_lunar hall <state.rst> <out.bin>           Hall edge EMF of the state
 //   ref_lunar hallstep <state.rst> <out.bin>       one implicit Hall solve (tight tolerances)
@@ -393,6 +394,94 @@ int cmd_run(Harness &h, const std::string &state, int nsteps, const std::string 
     return 0;
 }
 
+// One forward-Euler stage of StepOnce at the solver's current dt
+// (Z4_Lunar/src/LunarSolver_Driver.cpp:21-48 without Compute_Timestep): the
+// reference's own RHS, CT induction, update and resistive part.
+void euler_stage(LunarSolver &s)
+{
+    s.ZeroRHS_();
+    s.Scheme_U_();
+    s.AddSourceToRHS_Fluid();
+    s.AssembleRHS_Induction_CT_();
+    s.ApplyUpdate_Euler_();
+    if (s.resist_control.use_implicit_lunar_resistance)
+    {
+        s.lunar_bound_.Sync("Bface");
+        s.SolveImplicitResistiveDiffusion_(s.dt);
+    }
+    else
+        s.ResistiveDiffusionSubcycles_();
+}
+
+// The state fields the Euler update writes, on the inner points it writes
+// (ApplyUpdate_Euler_, Z4_Lunar/src/physics/LunarSolver_Advance.cpp:61-122)
+std::vector<FieldBlock *> state_blocks(Harness &h, int ib)
+{
+    LunarSolver &s = *h.solver;
+    return {&h.fld->field(s.fid_.fid_U_H, ib), &h.fld->field(s.fid_.fid_B.xi, ib),
+            &h.fld->field(s.fid_.fid_B.eta, ib), &h.fld->field(s.fid_.fid_B.zeta, ib)};
+}
+
+template <class F> void for_inner(FieldBlock &f, F fn)
+{
+    const Int3 lo = f.inner_lo(), hi = f.inner_hi();
+    const int nc = f.descriptor().ncomp;
+    for (int i = lo.i; i < hi.i; ++i)
+        for (int j = lo.j; j < hi.j; ++j)
+            for (int k = lo.k; k < hi.k; ++k)
+                for (int m = 0; m < nc; ++m)
+                    fn(f(i, j, k, m));
+}
+
+// SSP-RK2 (Shu and Osher, 1988) composed from two of the reference's Euler
+// stages at the dt of the step's start: U1 = U^n + dt L(U^n), then
+// U^{n+1} = 0.5 (U^n + (U1 + dt L(U1))) on the inner points, with the
+// reference's syncs and derived fields after each stage.  The reference has
+// no multi-stage integrator; this is the composition the device's
+// mhd_set_integrator(MHD_INTEGRATOR_SSPRK2) follows.
+int cmd_rk2(Harness &h, const std::string &state, int nsteps, const std::string &prefix)
+{
+    h.load_state(state);
+    LunarSolver &s = *h.solver;
+    s.UpdateDerivedFields_();
+    s.calc_divB();
+    dump_state(h, prefix + "_0000.bin");
+    const int nb = h.fld->num_blocks();
+    for (int n = 1; n <= nsteps; ++n)
+    {
+        s.Compute_Timestep();
+        std::vector<std::vector<double>> u0(static_cast<size_t>(nb));
+        for (int ib = 0; ib < nb; ++ib)
+            for (FieldBlock *f : state_blocks(h, ib))
+                for_inner(*f, [&](double &x) { u0[size_t(ib)].push_back(x); });
+        euler_stage(s);
+        s.lunar_bound_.Sync("Ucell");
+        s.lunar_bound_.Sync("Bface");
+        s.UpdateDerivedFields_();
+        euler_stage(s);
+        for (int ib = 0; ib < nb; ++ib)
+        {
+            size_t q = 0;
+            for (FieldBlock *f : state_blocks(h, ib))
+                for_inner(*f, [&](double &x) {
+                    x = 0.5 * (u0[size_t(ib)][q] + x);
+                    ++q;
+                });
+        }
+        s.run_data_->dt = s.dt;
+        s.run_data_->time += s.dt;
+        s.run_data_->step += 1;
+        s.lunar_bound_.Sync("Ucell");
+        s.lunar_bound_.Sync("Bface");
+        s.UpdateDerivedFields_();
+        s.calc_divB();
+        char buf[32];
+        std::snprintf(buf, sizeof(buf), "_%04d.bin", n);
+        dump_state(h, prefix + buf);
+    }
+    return 0;
+}
+
 // Every field of the group is overwritten with value = block*2^32 + AoS
 // offset + 1 (exact in a double), then the reference Sync(group) runs; the
 // dump therefore records, for every point, which original point it was copied
@@ -619,6 +708,8 @@ int main(int argc, char **argv)
             rc = cmd_geom(h, argv[2]);
         else if (cmd == "run" && argc >= 5)
             rc = cmd_run(h, argv[2], std::atoi(argv[3]), argv[4]);
+        else if (cmd == "rk2" && argc >= 5)
+            rc = cmd_rk2(h, argv[2], std::atoi(argv[3]), argv[4]);
         else if (cmd == "probe" && argc >= 5)
             rc = cmd_probe(h, argv[2], argv[3], argv[4]);
         else if (cmd == "diag" && argc >= 4)

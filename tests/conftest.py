@@ -88,11 +88,12 @@ def periodic_setup(g):
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "ref_lunar")
 
 
-def reference_run(spec, st, steps, workdir):
+def reference_run(spec, st, steps, workdir, command="run"):
     """The reference's own StepOnce (oracle/_ref/ref_lunar, built from the
     reference's sources by __graft_entry__.build) on a case written in its
     input formats: returns [RestartFile after the load, after step 1, ...]
-    with every state, derived and intermediate field and dt.  Skips the
+    with every state, derived and intermediate field and dt.  command "rk2":
+    SSP-RK2 steps of two of the reference's Euler stages each.  Skips the
     calling test when the reference binary is not built."""
     import subprocess
 
@@ -101,6 +102,6 @@ def reference_run(spec, st, steps, workdir):
         pytest.skip("oracle/_ref/ref_lunar is not built (make -C oracle)")
     case.write_case(workdir, spec)
     rst.write(os.path.join(workdir, "init.rst"), st)
-    subprocess.run([REF_BIN, "run", "init.rst", str(steps), "step"], cwd=workdir, check=True,
+    subprocess.run([REF_BIN, command, "init.rst", str(steps), "step"], cwd=workdir, check=True,
                    stdout=subprocess.DEVNULL)
     return [rst.read(os.path.join(workdir, "step_%04d.bin" % s)) for s in range(steps + 1)]

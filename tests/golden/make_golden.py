@@ -86,6 +86,31 @@ def periodic(n=(8, 6, 5), steps=2, seed=20261203):
     print("wrote", tag)
 
 
+def periodic_rk2(n=(8, 6, 5), steps=2, seed=20261203):
+    """SSP-RK2 steps of the periodic box, each two of the reference's Euler
+    stages at one dt and their convex average (harness command rk2)."""
+    tag = "periodic_%dx%dx%d_rk2" % n
+    with tempfile.TemporaryDirectory() as d:
+        spec = case.periodic_box_case(n)
+        case.write_case(d, spec)
+        st = case.initial_state(spec, seed=seed)
+        rst.write(os.path.join(d, "init.rst"), st)
+        run(["rk2", "init.rst", str(steps), "step"], d)
+        arr = {}
+        for k, v in flatten(st, ["U_H", "B_xi", "B_eta", "B_zeta"]).items():
+            arr["init/" + k] = v
+        for s_ in range(steps + 1):
+            r = rst.read(os.path.join(d, "step_%04d.bin" % s_))
+            for k, v in flatten(r, STEP_FIELDS).items():
+                arr["s%d/%s" % (s_, k)] = v
+            arr["s%d/dt" % s_] = r.fields["dt"].blocks[0].data.reshape(())
+            arr["s%d/time" % s_] = np.array(r.time)
+        arr["n"] = np.array(n)
+        arr["seed"] = np.array(seed)
+        np.savez_compressed(os.path.join(OUT, tag + ".npz"), **arr)
+    print("wrote", tag)
+
+
 def slab(nr=6, nt=(5, 6), tiles=(2, 2), steps=2, resistive=0, implicit=0, seed=20261204, **over):
     tag = "slab_%dx%dx%d_t%dx%d_r%d%d" % ((nr,) + tuple(nt) + tuple(tiles) + (resistive, implicit))
     with tempfile.TemporaryDirectory() as d:
@@ -356,6 +381,12 @@ def slab_owners(nr=6, nt=(5, 6), tiles=(2, 2), seed=20261204, **over):
 if __name__ == "__main__":
     if not os.path.exists(REF_BIN):
         sys.exit("build the oracle first: make -C oracle -j8")
+    if len(sys.argv) > 1:
+        # named generators only, with their default arguments
+        for name in sys.argv[1:]:
+            globals()[name]()
+        sys.exit(0)
+    periodic_rk2()
     periodic((8, 6, 5), steps=2)
     slab(steps=2)
     # implicit resistive shell with peak resistivity 1 (inver_Rem = 1), solved to rtol 1e-13
