@@ -221,6 +221,16 @@ struct mhd_ctx
         double *ppartial = nullptr;              // per-CTA partial dot products, double-buffered
         unsigned *bar = nullptr;                 // grid barrier: arrival count, generation
         int pgrid = 0;                           // CTAs of the persistent kernel (0: unavailable)
+        // fused operator phases of the persistent solve (n < 0: the copy-list phases)
+        struct Fused
+        {
+            uint64_t *dst = nullptr;
+            int *kind = nullptr;
+            int64_t *idx = nullptr;
+            double *val = nullptr;
+            int *blk = nullptr;
+            int64_t n = -1;
+        } fa, fb;
     } res;
     // implicit Hall solve (ImplicitHallSolver::SolveOneStep): Newton on
     // F(X) = X - Ehall(B* - theta dt curl X) over the inner Hall edges of
@@ -636,25 +646,27 @@ int launch_update_derived_pole(mhd_ctx *ctx)
     return MHD_OK;
 }
 
-int launch_fluid_ucontra(mhd_ctx *ctx);
+int launch_fluid_ucontra(mhd_ctx *ctx, bool with_update);
 
 int launch_fluid_rhs(mhd_ctx *ctx)
 {
     if (ctx->pool32) // the mixed form's flux pass (its FP32 U_contra are a by-product)
-        return launch_fluid_ucontra(ctx);
+        return launch_fluid_ucontra(ctx, false);
     const int64_t nc = max_box(ctx, LOC_CELL, 0);
     prof_begin(ctx, "k_fluid_rhs");
     k_fluid_rhs<<<dim3(grid_for(nc), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv, ctx->c, nc);
     return launched(ctx);
 }
 
-// fluid RHS together with the contravariant velocities of the EMF stencils
-int launch_fluid_ucontra(mhd_ctx *ctx)
+// fluid RHS together with the contravariant velocities of the EMF stencils;
+// with_update (mixed form only): the cell update U += dt RHS_H in the same pass
+int launch_fluid_ucontra(mhd_ctx *ctx, bool with_update)
 {
     if (ctx->pool32)
     {
         prof_begin(ctx, "k_fluid_mixed");
-        launch_k_fluid_mixed(ctx->tune[TUNE_k_fluid_mixed], grid_kind(ctx, KIND_CELL1), ctx->stream, ctx->dbv, ctx->c);
+        launch_k_fluid_mixed(ctx->tune[TUNE_k_fluid_mixed], grid_kind(ctx, KIND_CELL1), ctx->stream, ctx->dbv, ctx->c,
+                             with_update ? ctx->dt : nullptr);
         return launched(ctx);
     }
     prof_begin(ctx, "k_fluid_ucontra");
@@ -1012,6 +1024,8 @@ int launch_gmres_persistent(mhd_ctx *ctx)
     a.atol = R.atol;
     a.bar = R.bar;
     a.err = ctx->err;
+    a.fa = FusedList{R.fa.dst, R.fa.kind, R.fa.idx, R.fa.val, R.fa.blk, R.fa.n};
+    a.fb = FusedList{R.fb.dst, R.fb.kind, R.fb.idx, R.fb.val, R.fb.blk, R.fb.n};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(unsigned(R.pgrid));
     cfg.blockDim = dim3(256);
@@ -1046,15 +1060,23 @@ int launch_resistive(mhd_ctx *ctx)
     return launch_curl_rng(ctx, F_Eresxi, F_RBresxi, F_Bxi, -1.0, 0);
 }
 
+// the Euler stage at the current dt: fluid RHS, CT induction with the face-B
+// update, cell update (in the mixed form done by the flux pass itself)
+int launch_euler_core(mhd_ctx *ctx)
+{
+    const bool fused = ctx->pool32 != nullptr;
+    RUN(launch_fluid_ucontra(ctx, fused));
+    RUN(launch_induction(ctx, /*update_b=*/true, /*with_ucontra=*/false));
+    return fused ? MHD_OK : launch_update_u(ctx);
+}
+
 // one LunarSolver::StepOnce, explicit part: dt, fluid RHS, CT induction, update
 int launch_step_a(mhd_ctx *ctx)
 {
     prof_begin(ctx, "k_begin_step");
     k_begin_step<<<1, 128, 0, ctx->stream>>>(ctx->dt_key, ctx->dt, ctx->err, ctx->prm.dt_abort, ctx->nruns);
     RUN(launched(ctx));
-    RUN(launch_fluid_ucontra(ctx));
-    RUN(launch_induction(ctx, /*update_b=*/true, /*with_ucontra=*/false));
-    return launch_update_u(ctx);
+    return launch_euler_core(ctx);
 }
 
 // ... and its closing part: run data, Sync("Ucell"), Sync("Bface"), derived fields
@@ -1378,9 +1400,7 @@ int launch_step_rk2(mhd_ctx *ctx)
     RUN(run_sync(ctx, "Ucell"));
     RUN(run_sync(ctx, "Bface"));
     RUN(launch_update_derived(ctx));
-    RUN(launch_fluid_ucontra(ctx));
-    RUN(launch_induction(ctx, /*update_b=*/true, /*with_ucontra=*/false));
-    RUN(launch_update_u(ctx));
+    RUN(launch_euler_core(ctx));
     RUN(launch_resistive_part(ctx));
     RUN(launch_rk2(ctx, 0));
     return launch_step_c(ctx);
@@ -1961,6 +1981,9 @@ static void free_resistive(mhd_ctx *ctx)
                     (void *)R.b, (void *)R.r, (void *)R.partial, (void *)R.dots, (void *)R.st,
                     (void *)R.alias_of, (void *)R.ppartial, (void *)R.bar, (void *)R.uloc})
         cudaFree(p);
+    for (auto *fl : {&R.fa, &R.fb})
+        for (void *p : {(void *)fl->dst, (void *)fl->kind, (void *)fl->idx, (void *)fl->val, (void *)fl->blk})
+            cudaFree(p);
     free_list(R.eres1form);
     free_list(R.db);
     const bool loops = R.graph_loops;
@@ -2333,6 +2356,161 @@ static int resistive_region(mhd_ctx *ctx, const std::vector<uint64_t> &seed)
     return MHD_OK;
 }
 
+// The persistent solve's operator in fewer grid-wide phases.  Phase A: the
+// unknowns, their aliases, Sync("Eres1form")'s fixed values and copies,
+// written in that order by the reference, become one list with a single
+// writer per point, each copy taking the expression of the value its source
+// holds after the writes before it.  Phase B: Sync("dB")'s copies are
+// written with the curl, each destination computing the curl at its source,
+// when no copy lands on a point the curl or a fixed value writes.  Neither
+// fusion applies when a copy's source is another copy's destination (the
+// chained case keeps the staged copy lists).  The values are the same bits
+// as the phase-by-phase operator's.
+static int build_fused_operator(mhd_ctx *ctx, const std::vector<uint64_t> &he, const std::vector<uint64_t> &ae,
+                                const std::vector<int64_t> &aidx, const std::vector<double> &asign)
+{
+    auto &R = ctx->res;
+    R.fa.n = R.fb.n = -1;
+    struct E
+    {
+        int kind;
+        int64_t idx;
+        double val;
+        int blk;
+    };
+    auto fetch = [&](const CopyList &l, std::vector<uint64_t> &d, std::vector<uint64_t> &sr, std::vector<uint64_t> &cd,
+                     std::vector<double> &cv) -> int {
+        d.resize(size_t(l.n));
+        sr.resize(size_t(l.n));
+        cd.resize(size_t(l.nconst));
+        cv.resize(size_t(l.nconst));
+        if (l.n > 0)
+        {
+            CK(ctx, cudaMemcpy(d.data(), l.dst, size_t(l.n) * 8, cudaMemcpyDeviceToHost));
+            CK(ctx, cudaMemcpy(sr.data(), l.src, size_t(l.n) * 8, cudaMemcpyDeviceToHost));
+        }
+        if (l.nconst > 0)
+        {
+            CK(ctx, cudaMemcpy(cd.data(), l.cdst, size_t(l.nconst) * 8, cudaMemcpyDeviceToHost));
+            CK(ctx, cudaMemcpy(cv.data(), l.cval, size_t(l.nconst) * 8, cudaMemcpyDeviceToHost));
+        }
+        return MHD_OK;
+    };
+    auto chained = [](const std::vector<uint64_t> &d, const std::vector<uint64_t> &sr) {
+        std::unordered_set<uint64_t> ds(d.begin(), d.end());
+        for (uint64_t x : sr)
+            if (ds.count(x))
+                return true;
+        return false;
+    };
+    auto upload = [&](mhd_ctx::Resistive::Fused &out, const std::vector<uint64_t> &order,
+                      const std::map<uint64_t, E> &m) -> int {
+        std::vector<uint64_t> d;
+        std::vector<int> kd, bl;
+        std::vector<int64_t> ix;
+        std::vector<double> vl;
+        for (uint64_t o : order)
+        {
+            const E &e = m.at(o);
+            d.push_back(o);
+            kd.push_back(e.kind);
+            ix.push_back(e.idx);
+            vl.push_back(e.val);
+            bl.push_back(e.blk);
+        }
+        RUN(upload_vec(ctx, d, &out.dst));
+        RUN(upload_vec(ctx, kd, &out.kind));
+        RUN(upload_vec(ctx, ix, &out.idx));
+        RUN(upload_vec(ctx, vl, &out.val));
+        RUN(upload_vec(ctx, bl, &out.blk));
+        out.n = int64_t(order.size());
+        return MHD_OK;
+    };
+    std::vector<uint64_t> d1, s1, cd1, d2, s2, cd2;
+    std::vector<double> cv1, cv2;
+    RUN(fetch(R.eres1form, d1, s1, cd1, cv1));
+    RUN(fetch(R.db, d2, s2, cd2, cv2));
+    // phase A
+    if (!chained(d1, s1))
+    {
+        std::map<uint64_t, E> m;
+        std::vector<uint64_t> order;
+        auto put = [&](uint64_t dst, const E &e) {
+            auto it = m.find(dst);
+            if (it == m.end())
+            {
+                m.emplace(dst, e);
+                order.push_back(dst);
+            }
+            else
+                it->second = e;
+        };
+        for (size_t t = 0; t < he.size(); ++t)
+            put(he[t], E{FUSE_UNKNOWN, int64_t(t), 0.0, 0});
+        for (size_t q = 0; q < ae.size(); ++q)
+            put(ae[q], E{FUSE_ALIAS, aidx[q], asign[q], 0});
+        for (size_t c = 0; c < cd1.size(); ++c)
+            put(cd1[c], E{FUSE_CONST, 0, cv1[c], 0});
+        std::vector<std::pair<uint64_t, E>> cps;
+        for (size_t c = 0; c < d1.size(); ++c)
+        {
+            auto it = m.find(s1[c]);
+            cps.push_back({d1[c], it != m.end() ? it->second : E{FUSE_POOL, int64_t(s1[c]), 0.0, 0}});
+        }
+        for (const auto &pr : cps)
+            put(pr.first, pr.second);
+        RUN(upload(R.fa, order, m));
+    }
+    // phase B
+    if (R.merge2 && !chained(d2, s2))
+    {
+        std::vector<int> rg(size_t(ctx->nblocks) * 6);
+        CK(ctx, cudaMemcpy(rg.data(), R.rng, rg.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        const PoolDecoder dec(ctx);
+        // is the dB point `off` a face the curl writes (inner face in the region)?
+        auto curl_face = [&](uint64_t off, int &b, int &fa, int &i, int &j, int &k) {
+            int f;
+            if (!dec.decode(off, f, b, i, j, k) || f < F_dBxi || f > F_dBxi + 2)
+                return false;
+            fa = f - F_dBxi;
+            const BlockView &v = ctx->hbv[size_t(b)];
+            const int *r = rg.data() + 6 * b;
+            const int p[3] = {i, j, k};
+            for (int a = 0; a < 3; ++a)
+                if (p[a] < r[a] || p[a] >= r[3 + a])
+                    return false;
+            return i >= 0 && j >= 0 && k >= 0 && i < v.ni + (fa == 0) && j < v.nj + (fa == 1) && k < v.nk + (fa == 2);
+        };
+        std::unordered_set<uint64_t> consts(cd2.begin(), cd2.end());
+        std::map<uint64_t, E> m;
+        std::vector<uint64_t> order;
+        bool ok = true;
+        int b, fa, i, j, k;
+        for (size_t c = 0; c < d2.size() && ok; ++c)
+        {
+            if (consts.count(d2[c]) || curl_face(d2[c], b, fa, i, j, k) || m.count(d2[c]))
+            {
+                ok = false; // a copy onto a written point: keep the phase-by-phase operator
+                break;
+            }
+            E e{FUSE_POOL, int64_t(s2[c]), 0.0, 0};
+            if (consts.count(s2[c]))
+            {
+                for (size_t q = 0; q < cd2.size(); ++q)
+                    if (cd2[q] == s2[c])
+                        e = E{FUSE_CONST, 0, cv2[q], 0};
+            }
+            else if (curl_face(s2[c], b, fa, i, j, k))
+                e = E{FUSE_CURL, fuse_pack(fa, i, j, k), 0.0, b};
+            m.emplace(d2[c], e);
+            order.push_back(d2[c]);
+        }
+        if (ok)
+            RUN(upload(R.fb, order, m));
+    }
+    return MHD_OK;
+}
+
 extern "C" {
 
 int mhd_set_sync_map(mhd_ctx *ctx, const char *group, const int64_t *dst, const int64_t *src, int64_t n)
@@ -2641,6 +2819,7 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
             if (i >= 0 && j >= 0 && k >= 0 && i < v.ni + (a == 0) && j < v.nj + (a == 1) && k < v.nk + (a == 2))
                 R.merge2 = 0;
         }
+        RUN(build_fused_operator(ctx, he, fa, fidx, fs));
     }
     // every point of the solve's fields starts at zero
     for (int f0 : {int(F_Eresxi), int(F_dBxi), int(F_dJxi), int(F_RBresxi)})

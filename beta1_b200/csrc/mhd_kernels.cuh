@@ -103,6 +103,33 @@ struct DevCopy // fixed values then copies of a point list (apply_list)
     double *tmp; // staging when a source is also a destination
     int64_t n;
 };
+// One point-wise write list of the fused resistive operator: pool[dst[q]] =
+// kind 0: x[idx] / div (an unknown), 1: val * (x[idx] / div) (an alias),
+// 2: val (a fixed value), 3: pool[idx] (a point no phase writes),
+// 4: -dt * (discrete curl of Eres at the face packed in idx, block blk)
+struct FusedList
+{
+    const uint64_t *dst;
+    const int *kind;
+    const int64_t *idx;
+    const double *val;
+    const int *blk;
+    int64_t n;
+};
+enum : int
+{
+    FUSE_UNKNOWN = 0,
+    FUSE_ALIAS = 1,
+    FUSE_CONST = 2,
+    FUSE_POOL = 3,
+    FUSE_CURL = 4
+};
+// face packed as ((fa * 4096 + i + 64) * 4096 + j + 64) * 4096 + k + 64
+__host__ __device__ inline int64_t fuse_pack(int fa, int i, int j, int k)
+{
+    return ((int64_t(fa) * 4096 + (i + 64)) * 4096 + (j + 64)) * 4096 + (k + 64);
+}
+
 struct ResistSolve
 {
     const BlockView *bvs;
@@ -129,6 +156,11 @@ struct ResistSolve
     double rtol, atol;
     unsigned *bar; // arrival count, generation
     int *err;      // set to MHD_EKRYLOV when a barrier wait gives up
+    // fused operator phases (n < 0: not fused, the copy-list phases run):
+    // A: every Eres point the unknowns' writes and Sync("Eres1form") set,
+    // each as one expression of the basis vector; B: the Sync("dB") copies,
+    // each as the curl at its source (or a fixed or unchanged value)
+    FusedList fa, fb;
 };
 __global__ void k_gmres_resist(ResistSolve a);
 
@@ -186,6 +218,7 @@ int launch_k_curl_e2f(int variant, dim3 grid, cudaStream_t st, const BlockView *
 // k_eedge: minimum CTAs per SM 0, 8
 int launch_k_eedge(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs);
 // k_fluid_mixed: minimum CTAs per SM 2, 0, 3
-int launch_k_fluid_mixed(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c);
+// dtp non-null: also U += dt RHS_H on the inner cells (the step's update)
+int launch_k_fluid_mixed(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c, const double *dtp);
 
 } // namespace mhd

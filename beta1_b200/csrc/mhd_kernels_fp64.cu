@@ -515,6 +515,18 @@ __device__ __forceinline__ void curl_point(const BlockView &b, int fE0, int fR0,
     }
 }
 
+// the discrete curl curl_point forms on face axis fa at (i, j, k)
+__device__ __forceinline__ double face_curl(const BlockView &b, int fE0, int fa, int i, int j, int k)
+{
+    const double *Ex = b.f[fE0], *Ee = b.f[fE0 + 1], *Ez = b.f[fE0 + 2];
+    const int64_t p = pidx(b, i, j, k);
+    if (fa == 0)
+        return (Ee[p] - Ee[pidx(b, i, j, k + 1)]) + (Ez[pidx(b, i, j + 1, k)] - Ez[p]);
+    if (fa == 1)
+        return (Ex[pidx(b, i, j, k + 1)] - Ex[p]) + (Ez[p] - Ez[pidx(b, i + 1, j, k)]);
+    return (Ex[p] - Ex[pidx(b, i, j + 1, k)]) + (Ee[pidx(b, i + 1, j, k)] - Ee[p]);
+}
+
 __device__ __forceinline__ void k_curl_e2f_body(const BlockView *__restrict__ bvs, int fE0, int fR0, int fB0, double mult,
                            const double *__restrict__ dtp, double dtdiv, int mult_is_neg_dt, const int *__restrict__ rng)
 {
@@ -1068,8 +1080,13 @@ __device__ __forceinline__ void k_pv_uplus_dt_body(const BlockView *__restrict__
             // (Reconstruction_Rusanov, LunarSolver_FluidRHS.cpp:34-111)
             const double cs = sqrt(smax(0.0, c.gamma * pr / smax(U0, 1e-30)));
             const double rhoe = pr / (c.gamma - 1.0) + 0.5 * U0 * (u * u + vv * vv + w * w);
-            b.f[F_Cs][p] = cs;
-            b.f[F_RhoE][p] = rhoe;
+            if (sizeof(WT) == sizeof(double))
+            {
+                // FP64 face states of the FP64 flux (the mixed form's flux
+                // reads the FP32 copies below instead)
+                b.f[F_Cs][p] = cs;
+                b.f[F_RhoE][p] = rhoe;
+            }
             if (b.q32)
             {
                 // FP32 face states of the mixed-precision flux: deviations
@@ -1411,15 +1428,18 @@ struct GmresScalars
     int j, its, reason, breakdown, inner, outer, cycles;
 };
 
-// out[c] = V_c . w for c < nv, or out[0] = w . w (V null); every CTA ends
-// with the same values in out (shared memory)
-__device__ bool grid_dots(const ResistSolve &a, const double *V, int nv, const double *w, double *out, int &pbuf)
+// out[c] = V_c . w for c < nv, or out[0] = w . w (V null); with_self also
+// out[nv] = w . w in the same reduction; every CTA ends with the same values
+// in out (shared memory)
+__device__ bool grid_dots(const ResistSolve &a, const double *V, int nv, const double *w, double *out, int &pbuf,
+                          bool with_self = false)
 {
     __shared__ double wred[8][8];
     const int G = gridDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     double *part = a.partial + int64_t(pbuf) * 32 * G;
     pbuf ^= 1;
-    for (int c0 = 0; c0 < nv; c0 += 8)
+    const int nd = nv + (with_self ? 1 : 0);
+    for (int c0 = 0; c0 < nd; c0 += 8)
     {
         double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         for (int64_t t = int64_t(blockIdx.x) * blockDim.x + tid; t < a.n; t += int64_t(G) * blockDim.x)
@@ -1427,8 +1447,8 @@ __device__ bool grid_dots(const ResistSolve &a, const double *V, int nv, const d
             const double wt = w[t];
 #pragma unroll
             for (int q = 0; q < 8; ++q)
-                if (c0 + q < nv)
-                    acc[q] += (V ? V[int64_t(c0 + q) * a.n + t] : wt) * wt;
+                if (c0 + q < nd)
+                    acc[q] += ((V && c0 + q < nv) ? V[int64_t(c0 + q) * a.n + t] : wt) * wt;
         }
 #pragma unroll
         for (int q = 0; q < 8; ++q)
@@ -1438,7 +1458,7 @@ __device__ bool grid_dots(const ResistSolve &a, const double *V, int nv, const d
             for (int q = 0; q < 8; ++q)
                 wred[warp][q] = acc[q];
         __syncthreads();
-        if (tid < 8 && c0 + tid < nv)
+        if (tid < 8 && c0 + tid < nd)
         {
             double sum = 0.0;
             for (int wp = 0; wp < int(blockDim.x >> 5); ++wp)
@@ -1449,7 +1469,7 @@ __device__ bool grid_dots(const ResistSolve &a, const double *V, int nv, const d
     }
     if (!grid_barrier(a.bar, a.err))
         return false;
-    for (int c = warp; c < nv; c += int(blockDim.x >> 5))
+    for (int c = warp; c < nd; c += int(blockDim.x >> 5))
     {
         double sum = 0.0;
         for (int g = lane; g < G; g += 32)
@@ -1503,18 +1523,42 @@ __device__ bool grid_matvec(const ResistSolve &a, const double *src, double div,
     const int64_t t0 = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, ts = int64_t(gridDim.x) * blockDim.x;
     if (first_barrier && !grid_barrier(a.bar, a.err))
         return false;
-    for (int64_t t = t0; t < a.n; t += ts)
-        a.pool[a.e[t]] = src[t] / div;
-    for (int64_t q = t0; q < a.nalias; q += ts)
-        a.pool[a.alias[q]] = a.sign[q] * (src[a.alias_of[q]] / div);
-    if (a.merge1)
-        for (int64_t t = t0; t < a.eres1form.nconst; t += ts)
-            a.pool[a.eres1form.cdst[t]] = a.eres1form.cval[t];
-    if (!grid_barrier(a.bar, a.err))
-        return false;
-    if (!grid_apply(a, a.eres1form, a.merge1 != 0))
-        return false;
     const double mdt = -a.dtp[0];
+    if (a.fa.n >= 0)
+    {
+        // one phase: every Eres point the unknowns, aliases and Sync("Eres1form") set
+        for (int64_t q = t0; q < a.fa.n; q += ts)
+        {
+            const int kd = a.fa.kind[q];
+            const int64_t ix = a.fa.idx[q];
+            double v;
+            if (kd == FUSE_UNKNOWN)
+                v = src[ix] / div;
+            else if (kd == FUSE_ALIAS)
+                v = a.fa.val[q] * (src[ix] / div);
+            else if (kd == FUSE_CONST)
+                v = a.fa.val[q];
+            else
+                v = a.pool[ix];
+            a.pool[a.fa.dst[q]] = v;
+        }
+        if (!grid_barrier(a.bar, a.err))
+            return false;
+    }
+    else
+    {
+        for (int64_t t = t0; t < a.n; t += ts)
+            a.pool[a.e[t]] = src[t] / div;
+        for (int64_t q = t0; q < a.nalias; q += ts)
+            a.pool[a.alias[q]] = a.sign[q] * (src[a.alias_of[q]] / div);
+        if (a.merge1)
+            for (int64_t t = t0; t < a.eres1form.nconst; t += ts)
+                a.pool[a.eres1form.cdst[t]] = a.eres1form.cval[t];
+        if (!grid_barrier(a.bar, a.err))
+            return false;
+        if (!grid_apply(a, a.eres1form, a.merge1 != 0))
+            return false;
+    }
     const int64_t np = int64_t(a.nblocks) * a.nreg;
     for (int64_t q = t0; q < np; q += ts)
     {
@@ -1527,10 +1571,37 @@ __device__ bool grid_matvec(const ResistSolve &a, const double *src, double div,
     if (a.merge2)
         for (int64_t t = t0; t < a.db.nconst; t += ts)
             a.pool[a.db.cdst[t]] = a.db.cval[t];
-    if (!grid_barrier(a.bar, a.err))
-        return false;
-    if (!grid_apply(a, a.db, a.merge2 != 0))
-        return false;
+    if (a.fb.n >= 0)
+    {
+        // the Sync("dB") copies in the same phase: each destination takes
+        // the curl at its source directly (fixed values were written above)
+        for (int64_t q = t0; q < a.fb.n; q += ts)
+        {
+            const int kd = a.fb.kind[q];
+            const int64_t ix = a.fb.idx[q];
+            double v;
+            if (kd == FUSE_CURL)
+            {
+                const int k = int(ix % 4096) - 64, j = int((ix / 4096) % 4096) - 64;
+                const int i = int((ix / (int64_t(4096) * 4096)) % 4096) - 64, fa = int(ix / (int64_t(4096) * 4096 * 4096));
+                v = mdt * face_curl(a.bvs[a.fb.blk[q]], F_Eresxi, fa, i, j, k);
+            }
+            else if (kd == FUSE_CONST)
+                v = a.fb.val[q];
+            else
+                v = a.pool[ix];
+            a.pool[a.fb.dst[q]] = v;
+        }
+        if (!grid_barrier(a.bar, a.err))
+            return false;
+    }
+    else
+    {
+        if (!grid_barrier(a.bar, a.err))
+            return false;
+        if (!grid_apply(a, a.db, a.merge2 != 0))
+            return false;
+    }
     for (int64_t t = t0; t < a.n; t += ts)
     {
         const int *u = a.uloc + 5 * t;
@@ -1617,7 +1688,9 @@ __global__ void __launch_bounds__(256) k_gmres_resist(ResistSolve a)
                     s -= S.hcol[c] * a.V[int64_t(c) * n + t];
                 a.w[t] = s;
             }
-            if (!grid_dots(a, a.V, j + 1, a.w, S.d, pbuf))
+            // second pass, its dots and ||w'||^2 in one reduction: with V
+            // orthonormal, ||w' - V d||^2 = ||w'||^2 - ||d||^2
+            if (!grid_dots(a, a.V, j + 1, a.w, S.d, pbuf, true))
                 return;
             for (int64_t t = t0; t < n; t += ts)
             {
@@ -1629,12 +1702,14 @@ __global__ void __launch_bounds__(256) k_gmres_resist(ResistSolve a)
             if (tid <= j)
                 S.hcol[tid] += S.d[tid];
             __syncthreads();
-            if (!grid_dots(a, nullptr, 1, a.w, dv, pbuf))
-                return;
             if (tid == 0)
             {
                 // new column: rotations, residual estimate
-                S.hcol[j + 1] = sqrt(dv[0]);
+                double dd = 0.0;
+                for (int c = 0; c <= j; ++c)
+                    dd += S.d[c] * S.d[c];
+                const double nw2 = S.d[j + 1] - dd;
+                S.hcol[j + 1] = sqrt(nw2 > 0.0 ? nw2 : 0.0);
                 for (int i = 0; i <= j + 1; ++i)
                     S.H[i * 31 + j] = S.hcol[i];
                 for (int i = 0; i < j; ++i)

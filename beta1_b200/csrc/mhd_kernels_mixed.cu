@@ -94,7 +94,14 @@ __device__ __forceinline__ void rusanov_dev32(const BlockView &b, const Ref32 &r
 // variants: at least 2 CTAs per SM (128 registers; the default: uncapped it
 // takes 168 registers and one CTA, 0.265 -> 0.171 ms on the C2 step),
 // uncapped, at least 3
-__device__ __forceinline__ void k_fluid_mixed_body(const BlockView *__restrict__ bvs, Consts c)
+// dtp (may be null): the step's dt per run; when given, the cell part of
+// ApplyUpdate_Euler_ (U += dt RHS_H, LunarSolver_Advance.cpp:82-93) is done
+// here too, with the same unfused multiply and add as the update kernel.
+// Safe in this pass: it reads U only at its own cell (the neighbours' face
+// states come from the FP32 copies), and no kernel between the flux pass and
+// the update reads U.
+__device__ __forceinline__ void k_fluid_mixed_body(const BlockView *__restrict__ bvs, Consts c,
+                                                   const double *__restrict__ dtp)
 {
     int64_t t;
     const BlockView &b = bvs[cta_block(bvs, KIND_CELL1, t)];
@@ -170,38 +177,52 @@ __device__ __forceinline__ void k_fluid_mixed_body(const BlockView *__restrict__
     const double bx = B[p], by = B[v + p], bz = B[2 * v + p];
     const double fx = jy * bz - jz * by, fy = jz * bx - jx * bz, fz = jx * by - jy * bx;
     const double invJ = 1.0 / jac;
+    double rhs[5];
+    rhs[0] = -(double(r[0]) + phi[0]) * invJ;
+    rhs[1] = -(double(r[1]) + phi[1]) * invJ + fc * fx;
+    rhs[2] = -(double(r[2]) + phi[2]) * invJ + fc * fy;
+    rhs[3] = -(double(r[3]) + phi[3]) * invJ + fc * fz;
+    rhs[4] = -(double(r[4]) + phi[4]) * invJ + fc * (fx * PV[p] + fy * PV[v + p] + fz * PV[2 * v + p]);
     double *R = b.f[F_RHS];
-    R[p] = -(double(r[0]) + phi[0]) * invJ;
-    R[v + p] = -(double(r[1]) + phi[1]) * invJ + fc * fx;
-    R[2 * v + p] = -(double(r[2]) + phi[2]) * invJ + fc * fy;
-    R[3 * v + p] = -(double(r[3]) + phi[3]) * invJ + fc * fz;
-    R[4 * v + p] = -(double(r[4]) + phi[4]) * invJ + fc * (fx * PV[p] + fy * PV[v + p] + fz * PV[2 * v + p]);
+#pragma unroll
+    for (int m = 0; m < 5; ++m)
+        R[m * v + p] = rhs[m];
+    if (dtp)
+    {
+        const double dt = dtp[b.run];
+        double *U = b.f[F_U];
+#pragma unroll
+        for (int m = 0; m < 5; ++m)
+            U[m * v + p] = __dadd_rn(U[m * v + p], __dmul_rn(dt, rhs[m]));
+    }
 }
 
-template <int MINB> __global__ void __launch_bounds__(256, MINB) k_fluid_mixed_t(const BlockView *__restrict__ bvs, Consts c)
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_fluid_mixed_t(const BlockView *__restrict__ bvs, Consts c,
+                                                             const double *__restrict__ dtp)
 {
-    k_fluid_mixed_body(bvs, c);
+    k_fluid_mixed_body(bvs, c, dtp);
 }
 // the compiler's own register allocation (no launch bounds)
-__global__ void k_fluid_mixed_free(const BlockView *__restrict__ bvs, Consts c)
+__global__ void k_fluid_mixed_free(const BlockView *__restrict__ bvs, Consts c, const double *__restrict__ dtp)
 {
-    k_fluid_mixed_body(bvs, c);
+    k_fluid_mixed_body(bvs, c, dtp);
 }
 
 
 // launchers of the register / occupancy variants (tuned by mhd_autotune)
-int launch_k_fluid_mixed(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c)
+int launch_k_fluid_mixed(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c, const double *dtp)
 {
     switch (variant)
     {
     case 0:
-        k_fluid_mixed_t<2><<<grid, 256, 0, st>>>(bvs, c);
+        k_fluid_mixed_t<2><<<grid, 256, 0, st>>>(bvs, c, dtp);
         break;
     case 1:
-        k_fluid_mixed_free<<<grid, 256, 0, st>>>(bvs, c);
+        k_fluid_mixed_free<<<grid, 256, 0, st>>>(bvs, c, dtp);
         break;
     case 2:
-        k_fluid_mixed_t<3><<<grid, 256, 0, st>>>(bvs, c);
+        k_fluid_mixed_t<3><<<grid, 256, 0, st>>>(bvs, c, dtp);
         break;
     default:
         return -1;
