@@ -224,7 +224,7 @@ def mem_available_gb():
     return 16.0
 
 
-def cpu_reference(workload, n, steps, nproc):
+def cpu_reference(workload, n, steps, nproc, integrator="euler"):
     """Times the reference's own StepOnce loop (oracle/_ref/ref_lunar, built
     from the reference sources) on `nproc` concurrent single-threaded
     processes (bounded by host memory), each on the same bounded sample;
@@ -234,7 +234,7 @@ def cpu_reference(workload, n, steps, nproc):
     if not os.path.exists(REF_BIN):
         return None
     nproc = max(1, min(nproc, int(0.6 * mem_available_gb() / WORKLOADS[workload]["ref_rss_gb"])))
-    command = "time"
+    command = "timerk2" if integrator == "rk2" else "time"
     if workload in ("c3", "c4"):
         # bounded sample: the same layout at half the cells per direction,
         # the step with the implicit Hall solve
@@ -305,14 +305,14 @@ def cpu_reference_sweep(steps, nproc, nruns=SWEEP_RUNS, grid="slab"):
 SWEEP_SEED0 = 5000
 
 
-def sweep_host_setup(workload="c5", nruns=SWEEP_RUNS, geometry_on="host"):
+def sweep_host_setup(workload="c5", nruns=SWEEP_RUNS, geometry_on="host", use_runs=None):
     """Host set-up of every run of the sweep (node mesh, sync tables and,
     unless the device builds it, the geometry) from a spawned process pool
     bounded by cores and memory; returns (runs, [host set-up per run])."""
     import multiprocessing as mp
     from beta1_b200 import case, solver
     grid, topo = SWEEP_GRID[workload]
-    runs = case.sweep_cases(nruns, grid=grid)
+    runs = case.sweep_cases(nruns, grid=grid)[:use_runs]
     nproc = max(1, min(len(runs), os.cpu_count() or 1, 16, int(mem_available_gb() / 8.0)))
     with mp.get_context("spawn").Pool(nproc) as pool:
         host = pool.map(solver.host_setup_run, [(spec, topo, geometry_on) for spec, _ in runs])
@@ -406,7 +406,7 @@ def run_reference_arm(args):
     if args.workload in SWEEP_GRID:
         res = cpu_reference_sweep(steps, os.cpu_count() or 1, grid=SWEEP_GRID[args.workload][0])
     else:
-        res = cpu_reference(args.workload, args.n, steps, os.cpu_count() or 1)
+        res = cpu_reference(args.workload, args.n, steps, os.cpu_count() or 1, args.integrator)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_lunar not built or failed"}))
         return 0
@@ -419,8 +419,9 @@ def run_reference_arm(args):
         sample = "%s: %s; %d steps per process, %d concurrent single-threaded processes (bounded by host " \
                  "cores and memory)" % (wl["name"], HALL_SAMPLE, steps, nproc)
     else:
-        sample = "%s: %d StepOnce per process, %d concurrent single-threaded processes (bounded by host cores " \
-                 "and memory)" % (wl["name"], steps, nproc)
+        sample = "%s: %d %s per process, %d concurrent single-threaded processes (bounded by host cores " \
+                 "and memory)" % (wl["name"], steps, "SSP-RK2 steps" if args.integrator == "rk2" else "StepOnce",
+                                  nproc)
     line = {
         "impl": "reference", "metric": "cell-updates/s", "value": agg, "unit": "cell-updates/s",
         "n_gpus": args.gpus, "steps": steps, "warmup": 0,
@@ -452,6 +453,12 @@ def main():
     ap.add_argument("--geometry", default=None, choices=["host", "device"],
                     help="geometry fields built on the host and uploaded, or built on the device from the node "
                          "meshes (mhd_build_geometry); same values (default: device for the sweeps, host otherwise)")
+    ap.add_argument("--integrator", default=None, choices=["euler", "rk2"],
+                    help="euler: the reference's StepOnce; rk2: SSP-RK2 of two of its Euler stages at one dt "
+                         "(default: rk2 for c1, euler otherwise)")
+    ap.add_argument("--sweep-runs", type=int, default=SWEEP_RUNS,
+                    help="sweeps: the first N runs of the 48 (profiling captures use a few; the bench line is "
+                         "quoted on all 48)")
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="sweeps in mixed precision: skip timing the FP64 form on the same runs")
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
@@ -464,6 +471,8 @@ def main():
         args.steps = {"c2": 200, "c1": 4000, "c5": 100, "c5s": 100, "c3": 10, "c4": 10}[args.workload]
     if args.precision is None:
         args.precision = "mixed" if args.workload in ("c5", "c5s", "c4") else "fp64"
+    if args.integrator is None:
+        args.integrator = "rk2" if args.workload == "c1" else "euler"
 
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -489,7 +498,7 @@ def main():
     t_setup = time.time()
     fp64_cmp = None
     if sweep:
-        runs, host = sweep_host_setup(args.workload, geometry_on=geometry_on)
+        runs, host = sweep_host_setup(args.workload, geometry_on=geometry_on, use_runs=args.sweep_runs)
         s, cells = build_sweep(prec, runs, host, args.workload)
         spec = None
         nblocks = len(runs)
@@ -506,6 +515,9 @@ def main():
         s.load_state(st)
         nblocks = len(spec.blocks)
     ctx = s.ctx
+    if args.integrator == "rk2":
+        for c in ([ctx] + ([fp64_cmp.ctx] if fp64_cmp is not None else [])):
+            c.set_integrator(mhd.INTEGRATOR_SSPRK2)
     setup_s = time.time() - t_setup
     # register / occupancy variant of each hot kernel, timed on this state
     tuned = ctx.autotune(reps=10) if not args.no_autotune else None
@@ -615,16 +627,19 @@ def main():
                                  "from its own sources, one single-threaded process"
                                  % (wl["name"], res[1][0]["cells"], ref_steps)}
         else:
-            res = cpu_reference(args.workload, args.n, ref_steps, 1)
+            res = cpu_reference(args.workload, args.n, ref_steps, 1, args.integrator)
             if res is not None:
                 agg, vals, _ = res
-                what = HALL_SAMPLE if args.workload in ("c3", "c4") else "StepOnce"
+                what = HALL_SAMPLE if args.workload in ("c3", "c4") else (
+                    "SSP-RK2 step" if args.integrator == "rk2" else "StepOnce")
                 cpu = {"value": agg, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
                        "sample": "%s, %d x %s of the reference solver built from its own sources, one "
                                  "single-threaded process" % (wl["name"], ref_steps, what)}
 
     config_name = workload_name(wl["name"] if args.workload != "c2" or args.c2_size == "96x48" else
                                 "c2_slab6x%sx%s_implicit_resistive_fp64" % (args.c2_size, args.c2_size.split("x")[1]), mixed)
+    if sweep and len(runs) != SWEEP_RUNS:
+        config_name = config_name.replace("sweep48", "sweep%d" % len(runs))
     if rank == 0:
         line = {
             "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
@@ -634,7 +649,10 @@ def main():
             "data": "synthetic (seeded 1e-3 noise on rho, v and div-free B; reference restart format)",
             "config": {"workload": config_name,
                        "cells_per_gpu": cells, "blocks": nblocks, "autotune_min_ctas_per_sm": tuned,
-                       "integrator": "forward Euler StepOnce (reference parity mode)", "precision": args.precision,
+                       "integrator": ("SSP-RK2: two of StepOnce's forward-Euler stages at one dt and their "
+                                      "convex average" if args.integrator == "rk2" else
+                                      "forward Euler StepOnce (the reference's integrator)"),
+                       "precision": args.precision,
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "no flush: per-step working set %.2f GB > 126 MB L2" % (ctx_bytes / 1e9),
                        "geometry": geometry_on, "setup_s": round(setup_s, 2)},

@@ -473,7 +473,7 @@ int launch_pole(mhd_ctx *ctx, int op)
         w = std::max(w, pole_work(op, v.ni, v.nk));
     }
     prof_begin(ctx, "k_pole");
-    k_pole<<<dim3(grid_for(w), unsigned(np)), kThreads, 0, ctx->stream>>>(ctx->dbv, ctx->dpoles, op);
+    launch_pole_op(op, w, np, ctx->stream, ctx->dbv, ctx->dpoles);
     return launched(ctx);
 }
 

@@ -45,6 +45,9 @@ __global__ void k_jcell(const BlockView *bvs);
 // Pole handlers and repairs on eta Poles (mhd_pole.cuh): per Pole a
 // (block, direction) pair in `poles`, one grid row per Pole
 __global__ void k_pole(const BlockView *bvs, const int *poles, int op);
+// one Pole operation over every Pole (work items per Pole: pole_work); the
+// ring least squares run one warp per ring
+void launch_pole_op(int op, int64_t work, int npoles, cudaStream_t st, const BlockView *bvs, const int *poles);
 __global__ void k_geometry(const BlockView *bvs, int blk, NodeMesh m, int G, int group0, double b0, double b1,
                            double b2);
 // output-step minima / maxima over the inner cells of a run's blocks (run < 0:

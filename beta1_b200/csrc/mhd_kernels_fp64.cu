@@ -1998,4 +1998,273 @@ __global__ void k_pole(const BlockView *__restrict__ bvs, const int *__restrict_
     pole_one(b, side, op, int64_t(blockIdx.x) * blockDim.x + threadIdx.x);
 }
 
+// ---------------------------------------------------------------------------
+// The ring least squares of POLE_BCELL, POLE_EETA_REG and POLE_JCELL with one
+// warp per ring.  The lanes form the pushed vectors and values of 32 k at a
+// time (square roots and divisions in parallel, the same operations as
+// pole_one); lane 0 then pushes them in the reference's order -- k, then the
+// handler's order within k -- so A and the right-hand side are summed exactly
+// as the one-thread ring sums them, and solves; the lanes write the ring.
+// ---------------------------------------------------------------------------
+constexpr int kPoleWarps = 4; // warps (rings) per CTA
+constexpr int kPoleTerms = 8; // at most 8 pushes per k (J_cell)
+
+struct PoleTerm
+{
+    double s[3], phi;
+    int ok;
+};
+
+__device__ __forceinline__ void pole_push_chunk(const PoleTerm *sh, int nterm, double A[3][3], double rhs[3], int &cnt)
+{
+    for (int q = 0; q < nterm; ++q)
+        if (sh[q].ok)
+        {
+            pole_push(A, rhs, sh[q].s, sh[q].phi);
+            ++cnt;
+        }
+}
+
+// regularised 3x3 solve of lane 0, broadcast to the warp; false when the
+// ring has no usable term (cnt <= 0) or the solve fails
+__device__ __forceinline__ bool pole_solve_bcast(double A[3][3], double rhs[3], int cnt, double x[3], bool trace_abs,
+                                                 int &status)
+{
+    const int lane = threadIdx.x & 31;
+    int st = 0;
+    if (lane == 0)
+    {
+        if (cnt <= 0)
+            st = 1;
+        else
+        {
+            const double tr = trace_abs ? fabs(A[0][0]) + fabs(A[1][1]) + fabs(A[2][2]) : A[0][0] + A[1][1] + A[2][2];
+            const double reg = 1.0e-12 * pole_max1(tr);
+            A[0][0] += reg;
+            A[1][1] += reg;
+            A[2][2] += reg;
+            st = pole_solve3(A, rhs, x) ? 0 : 2;
+        }
+    }
+    status = __shfl_sync(0xffffffffu, st, 0);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        x[c] = __shfl_sync(0xffffffffu, lane == 0 ? x[c] : 0.0, 0);
+    return status == 0;
+}
+
+__device__ void pole_bcell_warp(const BlockView &b, int side, int64_t t, PoleTerm *sh)
+{
+    const int lane = threadIdx.x & 31;
+    const int nj = b.nj, nk = b.nk;
+    const int64_t v = b.vol;
+    const int i = int(t >> 1);
+    const bool total = (t & 1) == 0;
+    const int jc = side < 0 ? 0 : nj - 1;
+    const int jn = side < 0 ? jc + 1 : jc;
+    const double sn = side < 0 ? 1.0 : -1.0;
+    const double *Aet = b.f[F_JDeta], *Axi = b.f[F_JDxi];
+    const double *Bet = b.f[F_Beta], *Bxi = b.f[F_Bxi], *Aadd = b.f[F_Baddeta], *Xadd = b.f[F_Baddxi];
+    double A[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    double rhs[3] = {0.0, 0.0, 0.0};
+    int cnt = 0;
+    for (int k0 = 0; k0 < nk; k0 += 32)
+    {
+        const int k = k0 + lane;
+        if (k < nk)
+        {
+            const int64_t pn = pidx(b, i, jn, k), p0 = pidx(b, i, jc, k), p1 = pidx(b, i + 1, jc, k);
+            PoleTerm *o = sh + 3 * lane;
+            double f = Bet[pn];
+            if (total)
+                f += Aadd[pn];
+            o[0] = PoleTerm{{sn * Aet[pn], sn * Aet[v + pn], sn * Aet[2 * v + pn]}, sn * f, 0};
+            f = Bxi[p0];
+            if (total)
+                f += Xadd[p0];
+            o[1] = PoleTerm{{-Axi[p0], -Axi[v + p0], -Axi[2 * v + p0]}, -f, 0};
+            f = Bxi[p1];
+            if (total)
+                f += Xadd[p1];
+            o[2] = PoleTerm{{Axi[p1], Axi[v + p1], Axi[2 * v + p1]}, f, 0};
+            for (int q = 0; q < 3; ++q)
+            {
+                const double *S = o[q].s;
+                o[q].ok = !((S[0] * S[0] + S[1] * S[1] + S[2] * S[2]) <= 1.0e-300);
+            }
+        }
+        __syncwarp();
+        if (lane == 0)
+            pole_push_chunk(sh, 3 * min(32, nk - k0), A, rhs, cnt);
+        __syncwarp();
+    }
+    // BC_Pole_Bcell_Collapse_ pushes no count: the system is solved whenever
+    // it is regular (cnt is only the "any term" guard here)
+    double Bp[3];
+    int st;
+    if (!pole_solve_bcast(A, rhs, 1, Bp, true, st))
+        return;
+    double *Out = b.f[total ? F_Bcell : F_Bind];
+    for (int k = lane; k < nk; k += 32)
+    {
+        const int64_t p = pidx(b, i, jc, k);
+        Out[p] = Bp[0];
+        Out[v + p] = Bp[1];
+        Out[2 * v + p] = Bp[2];
+    }
+}
+
+__device__ void pole_eeta_warp(const BlockView &b, int side, int64_t t, PoleTerm *sh)
+{
+    const int lane = threadIdx.x & 31;
+    const int nj = b.nj, nk = b.nk;
+    const int64_t v = b.vol;
+    const int i = int(t);
+    const int jc = side < 0 ? 0 : nj - 1;
+    double *E = b.f[F_Eeta];
+    const double *dr = b.f[F_dreta];
+    double A[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    double rhs[3] = {0.0, 0.0, 0.0};
+    int cnt = 0;
+    for (int k0 = 0; k0 < nk; k0 += 32) // k = n_k is the same edge as k = 0
+    {
+        const int k = k0 + lane;
+        if (k < nk)
+        {
+            const int64_t p = pidx(b, i, jc, k);
+            const double d0 = dr[p], d1 = dr[v + p], d2 = dr[2 * v + p];
+            const double L = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+            PoleTerm &o = sh[lane];
+            o.ok = !(L < 1.0e-14);
+            if (o.ok)
+            {
+                const double invL = 1.0 / L;
+                o.s[0] = d0 * invL;
+                o.s[1] = d1 * invL;
+                o.s[2] = d2 * invL;
+                o.phi = E[p] * invL;
+            }
+        }
+        __syncwarp();
+        if (lane == 0)
+            pole_push_chunk(sh, min(32, nk - k0), A, rhs, cnt);
+        __syncwarp();
+    }
+    double Ev[3];
+    int st;
+    if (pole_solve_bcast(A, rhs, __shfl_sync(0xffffffffu, cnt, 0), Ev, false, st))
+    {
+        for (int k = lane; k <= nk; k += 32)
+        {
+            const int64_t p = pidx(b, i, jc, k);
+            const double d0 = dr[p], d1 = dr[v + p], d2 = dr[2 * v + p];
+            const double L = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+            E[p] = (L < 1.0e-14) ? 0.0 : Ev[0] * d0 + Ev[1] * d1 + Ev[2] * d2;
+        }
+        return;
+    }
+    if (st == 1) // no usable edge
+    {
+        for (int k = lane; k <= nk; k += 32)
+            E[pidx(b, i, jc, k)] = 0.0;
+        return;
+    }
+    // singular system: the ring average, summed in k order by lane 0
+    double avg = 0.0;
+    if (lane == 0)
+    {
+        for (int k = 0; k <= nk; ++k)
+            avg += E[pidx(b, i, jc, k)];
+        avg /= double(nk + 1);
+    }
+    avg = __shfl_sync(0xffffffffu, avg, 0);
+    for (int k = lane; k <= nk; k += 32)
+        E[pidx(b, i, jc, k)] = avg;
+}
+
+__device__ void pole_jcell_warp(const BlockView &b, int side, int64_t t, PoleTerm *sh)
+{
+    const int lane = threadIdx.x & 31;
+    const int nj = b.nj, nk = b.nk;
+    const int64_t v = b.vol;
+    const int i = int(t);
+    const int jc = side < 0 ? 0 : nj - 1;
+    const int jt = side < 0 ? jc + 1 : jc; // node plane one layer away from the Pole
+    // the 8 pushes of each k, in the order of the reference's loop
+    const int di[8] = {0, 1, 0, 1, 0, 0, 0, 1};
+    const int dk[8] = {0, 0, 1, 1, 0, 1, 0, 0};
+    const int fj[8] = {F_Jeta, F_Jeta, F_Jeta, F_Jeta, F_Jxi, F_Jxi, F_Jzeta, F_Jzeta};
+    const int fd[8] = {F_dreta, F_dreta, F_dreta, F_dreta, F_drxi, F_drxi, F_drzeta, F_drzeta};
+    double A[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    double rhs[3] = {0.0, 0.0, 0.0};
+    int cnt = 0;
+    for (int k0 = 0; k0 < nk; k0 += 32)
+    {
+        const int k = k0 + lane;
+        if (k < nk)
+        {
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+            {
+                const int64_t p = pidx(b, i + di[q], q < 4 ? jc : jt, k + dk[q]);
+                const double *dr = b.f[fd[q]];
+                const double dx = dr[p], dy = dr[v + p], dz = dr[2 * v + p];
+                const double L = sqrt(dx * dx + dy * dy + dz * dz);
+                PoleTerm &o = sh[8 * lane + q];
+                o.ok = !(L < 1.0e-14);
+                if (o.ok)
+                {
+                    o.s[0] = dx / L;
+                    o.s[1] = dy / L;
+                    o.s[2] = dz / L;
+                    o.phi = b.f[fj[q]][p] / L;
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0)
+            pole_push_chunk(sh, 8 * min(32, nk - k0), A, rhs, cnt);
+        __syncwarp();
+    }
+    double Jp[3];
+    int st;
+    if (!pole_solve_bcast(A, rhs, __shfl_sync(0xffffffffu, cnt, 0), Jp, false, st))
+        return;
+    double *Jc = b.f[F_Jcell];
+    for (int k = lane; k < nk; k += 32)
+    {
+        const int64_t p = pidx(b, i, jc, k);
+        Jc[p] = Jp[0];
+        Jc[v + p] = Jp[1];
+        Jc[2 * v + p] = Jp[2];
+    }
+}
+
+__global__ void __launch_bounds__(32 * kPoleWarps) k_pole_warp(const BlockView *__restrict__ bvs,
+                                                               const int *__restrict__ poles, int op)
+{
+    __shared__ PoleTerm sh[kPoleWarps][32 * kPoleTerms];
+    const BlockView &b = bvs[poles[2 * blockIdx.y]];
+    const int side = poles[2 * blockIdx.y + 1] > 0 ? 1 : -1;
+    const int warp = threadIdx.x >> 5;
+    const int64_t t = int64_t(blockIdx.x) * kPoleWarps + warp;
+    if (t >= pole_work(op, b.ni, b.nk))
+        return; // the whole warp leaves together
+    if (op == POLE_BCELL)
+        pole_bcell_warp(b, side, t, sh[warp]);
+    else if (op == POLE_EETA_REG)
+        pole_eeta_warp(b, side, t, sh[warp]);
+    else
+        pole_jcell_warp(b, side, t, sh[warp]);
+}
+
+void launch_pole_op(int op, int64_t work, int npoles, cudaStream_t st, const BlockView *bvs, const int *poles)
+{
+    if (op == POLE_BCELL || op == POLE_EETA_REG || op == POLE_JCELL)
+        k_pole_warp<<<dim3(unsigned((work + kPoleWarps - 1) / kPoleWarps), unsigned(npoles)), 32 * kPoleWarps, 0,
+                      st>>>(bvs, poles, op);
+    else
+        k_pole<<<dim3(unsigned((work + 255) / 256), unsigned(npoles)), 256, 0, st>>>(bvs, poles, op);
+}
+
 } // namespace mhd

@@ -15,6 +15,7 @@
 //   ref_lunar hall <state.rst> <out.bin>           Hall edge EMF of the state
 //   ref_lunar hallstep <state.rst> <out.bin>       one implicit Hall solve (tight tolerances)
 //   ref_lunar time  <state.rst> <nsteps>           wall time of the step loop
+//   ref_lunar timerk2 <state.rst> <nsteps>         wall time of SSP-RK2 steps
 //
 // The member functions are private in the reference; this translation unit
 // alone widens access to call them (the class layout is unchanged).
@@ -439,6 +440,37 @@ template <class F> void for_inner(FieldBlock &f, F fn)
 // reference's syncs and derived fields after each stage.  The reference has
 // no multi-stage integrator; this is the composition the device's
 // mhd_set_integrator(MHD_INTEGRATOR_SSPRK2) follows.
+void rk2_step(Harness &h)
+{
+    LunarSolver &s = *h.solver;
+    const int nb = h.fld->num_blocks();
+    s.Compute_Timestep();
+    std::vector<std::vector<double>> u0(static_cast<size_t>(nb));
+    for (int ib = 0; ib < nb; ++ib)
+        for (FieldBlock *f : state_blocks(h, ib))
+            for_inner(*f, [&](double &x) { u0[size_t(ib)].push_back(x); });
+    euler_stage(s);
+    s.lunar_bound_.Sync("Ucell");
+    s.lunar_bound_.Sync("Bface");
+    s.UpdateDerivedFields_();
+    euler_stage(s);
+    for (int ib = 0; ib < nb; ++ib)
+    {
+        size_t q = 0;
+        for (FieldBlock *f : state_blocks(h, ib))
+            for_inner(*f, [&](double &x) {
+                x = 0.5 * (u0[size_t(ib)][q] + x);
+                ++q;
+            });
+    }
+    s.run_data_->dt = s.dt;
+    s.run_data_->time += s.dt;
+    s.run_data_->step += 1;
+    s.lunar_bound_.Sync("Ucell");
+    s.lunar_bound_.Sync("Bface");
+    s.UpdateDerivedFields_();
+}
+
 int cmd_rk2(Harness &h, const std::string &state, int nsteps, const std::string &prefix)
 {
     h.load_state(state);
@@ -446,34 +478,9 @@ int cmd_rk2(Harness &h, const std::string &state, int nsteps, const std::string 
     s.UpdateDerivedFields_();
     s.calc_divB();
     dump_state(h, prefix + "_0000.bin");
-    const int nb = h.fld->num_blocks();
     for (int n = 1; n <= nsteps; ++n)
     {
-        s.Compute_Timestep();
-        std::vector<std::vector<double>> u0(static_cast<size_t>(nb));
-        for (int ib = 0; ib < nb; ++ib)
-            for (FieldBlock *f : state_blocks(h, ib))
-                for_inner(*f, [&](double &x) { u0[size_t(ib)].push_back(x); });
-        euler_stage(s);
-        s.lunar_bound_.Sync("Ucell");
-        s.lunar_bound_.Sync("Bface");
-        s.UpdateDerivedFields_();
-        euler_stage(s);
-        for (int ib = 0; ib < nb; ++ib)
-        {
-            size_t q = 0;
-            for (FieldBlock *f : state_blocks(h, ib))
-                for_inner(*f, [&](double &x) {
-                    x = 0.5 * (u0[size_t(ib)][q] + x);
-                    ++q;
-                });
-        }
-        s.run_data_->dt = s.dt;
-        s.run_data_->time += s.dt;
-        s.run_data_->step += 1;
-        s.lunar_bound_.Sync("Ucell");
-        s.lunar_bound_.Sync("Bface");
-        s.UpdateDerivedFields_();
+        rk2_step(h);
         s.calc_divB();
         char buf[32];
         std::snprintf(buf, sizeof(buf), "_%04d.bin", n);
@@ -633,6 +640,29 @@ int cmd_time(Harness &h, const std::string &state, int nsteps)
     return 0;
 }
 
+// wall time of `nsteps` SSP-RK2 steps (rk2_step), for timing
+int cmd_timerk2(Harness &h, const std::string &state, int nsteps)
+{
+    h.load_state(state);
+    LunarSolver &s = *h.solver;
+    s.UpdateDerivedFields_();
+    int64_t cells = 0;
+    for (int ib = 0; ib < h.fld->num_blocks(); ++ib)
+    {
+        FieldBlock &U = h.fld->field(s.fid_.fid_U_H, ib);
+        const Int3 lo = U.inner_lo(), hi = U.inner_hi();
+        cells += int64_t(hi.i - lo.i) * (hi.j - lo.j) * (hi.k - lo.k);
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int n = 0; n < nsteps; ++n)
+        rk2_step(h);
+    const auto t1 = std::chrono::steady_clock::now();
+    const double sec = std::chrono::duration<double>(t1 - t0).count();
+    std::printf("{\"cells\": %lld, \"steps\": %d, \"seconds\": %.9f, \"cell_updates_per_s\": %.6e}\n",
+                (long long)cells, nsteps, sec, double(cells) * nsteps / sec);
+    return 0;
+}
+
 // StepOnce followed by the implicit Hall solve (SolveOneStep at the step's dt,
 // Newton rtol 1e-10) and calc_Bcell, `nsteps` times: the step with the Hall
 // solve that HALL_IMPLICIT enables, for timing
@@ -721,6 +751,12 @@ int main(int argc, char **argv)
         {
             std::cout.rdbuf(sink.rdbuf());
             rc = cmd_timehall(h, argv[2], std::atoi(argv[3]));
+        }
+        else if (cmd == "timerk2" && argc >= 4)
+        {
+            std::cout.rdbuf(saved);
+            std::cout.rdbuf(sink.rdbuf());
+            rc = cmd_timerk2(h, argv[2], std::atoi(argv[3]));
         }
         else if (cmd == "time" && argc >= 4)
         {
