@@ -95,6 +95,9 @@ struct SyncMap
     bool staged = false;
     bool built = false; // device lists match the host tables
     CopyList full, hot, post;
+    // Pole contexts: the copies and fixed values a step leaves for read-out
+    // (cold), written then without the rings, walls and post-wall copies
+    CopyList cold;
     int *dwalls = nullptr;  // walls on the device (block, direction pairs)
     int64_t wall_cols = 0;  // boundary cell columns of the largest wall
 };
@@ -517,8 +520,10 @@ int run_sync(mhd_ctx *ctx, const char *group, bool full = false)
     }
     if (!ctx->poles.empty())
     {
+        // the hot lists in a step: the cold rest is written at read-out
+        const CopyList &l = full ? m.full : m.hot;
         RUN(pole_rings(ctx, it->first));
-        RUN(gather_map(ctx, m.full));
+        RUN(gather_map(ctx, l));
         if (!m.walls.empty())
         {
             prof_begin(ctx, "k_wall_u_all");
@@ -527,14 +532,13 @@ int run_sync(mhd_ctx *ctx, const char *group, bool full = false)
             RUN(launched(ctx));
         }
         RUN(gather_map(ctx, m.post));
-        if (m.full.nconst > 0)
+        if (l.nconst > 0)
         {
             prof_begin(ctx, "k_set_consts");
-            k_set_consts<<<grid_for(m.full.nconst), kThreads, 0, ctx->stream>>>(ctx->pool, m.full.cdst, m.full.cval,
-                                                                                 m.full.nconst);
+            k_set_consts<<<grid_for(l.nconst), kThreads, 0, ctx->stream>>>(ctx->pool, l.cdst, l.cval, l.nconst);
             RUN(launched(ctx));
         }
-        ctx->dirty[it->first] = false;
+        ctx->dirty[it->first] = !full && (m.cold.n > 0 || m.cold.nconst > 0);
         return MHD_OK;
     }
     const CopyList &l = full ? m.full : m.hot;
@@ -1754,6 +1758,7 @@ int mhd_ctx_destroy(mhd_ctx *ctx)
         free_list(kv.second.full);
         free_list(kv.second.hot);
         free_list(kv.second.post);
+        free_list(kv.second.cold);
         cudaFree(kv.second.dwalls);
     }
     cudaFree(ctx->dpoles);
@@ -2090,6 +2095,10 @@ static int hot_depth(const mhd_ctx *ctx, int f)
     // an edge, one ghost layer deep
     if (f == F_Jcell && ctx->res_nsub > 0)
         return 1;
+    // the Pole work items read B_cell / Bind_cell at k = n_k, the ring's
+    // periodic ghost (E_xi on the pole line, the B_zeta rewrite)
+    if ((f == F_Bcell || f == F_Bind) && !ctx->poles.empty())
+        return 1;
     switch (f)
     {
     case F_U:
@@ -2131,6 +2140,71 @@ static bool hot_point(const mhd_ctx *ctx, const PoolDecoder &dec, uint64_t off)
     return i >= -d && j >= -d && k >= -d && i < v.ni + pl[0] + d && j < v.nj + pl[1] + d && k < v.nk + pl[2] + d;
 }
 
+// Hot and cold lists of a Pole context's group.  Its Sync runs the rings,
+// the copies, the wall handlers, the post-wall copies, then the fixed values;
+// a step runs the hot part and read-out the cold part (copies, then fixed
+// values).  A copy may wait for read-out only when its destination is read
+// by no kernel of the step (not a hot point) and its source holds at read-out
+// what it held when the copies ran: not a point the wall handlers, the
+// post-wall copies or the fixed values of the same Sync write, and not in a
+// group whose sources a later Pole repair rewrites (Bface: the B_zeta rewrite
+// of the derived-field pass); nor may the wall handlers or the post-wall
+// copies overwrite its destination.  A fixed value is hot at a hot point or at the
+// destination of a hot copy (it overwrites the copy), cold otherwise.
+static int build_sync_pole(mhd_ctx *ctx, const std::string &group, SyncMap &m, const PoolDecoder &dec)
+{
+    std::vector<uint64_t> d, s2, cd, dc, sc, cdc;
+    std::vector<double> cv, cvc;
+    const bool all_hot = (group == "Bface");
+    std::unordered_set<uint64_t> later(m.hcd.begin(), m.hcd.end());
+    later.insert(m.hd2.begin(), m.hd2.end());
+    // points the wall handlers write: the boundary cell layer and the ghost
+    // layers beyond it on the wall's face
+    auto wall_point = [&](uint64_t off) {
+        int f, b, i, j, k;
+        if (m.walls.empty() || !dec.decode(off, f, b, i, j, k))
+            return false;
+        for (const auto &w : m.walls)
+        {
+            if (w.first != b)
+                continue;
+            const BlockView &v = ctx->hbv[size_t(b)];
+            const int ax = std::abs(w.second) - 1;
+            const int p[3] = {i, j, k}, n[3] = {v.ni, v.nj, v.nk};
+            if ((w.second < 0 && p[ax] <= 0) || (w.second > 0 && p[ax] >= n[ax] - 1))
+                return true;
+        }
+        return false;
+    };
+    std::unordered_set<uint64_t> hot_dst, post_dst(m.hd2.begin(), m.hd2.end());
+    for (size_t t = 0; t < m.hd.size(); ++t)
+    {
+        // a copy the wall handlers or the post-wall copies overwrite in the
+        // same Sync must run before them, in the step
+        const bool hot = all_hot || hot_point(ctx, dec, m.hd[t]) || later.count(m.hs[t]) || wall_point(m.hs[t]) ||
+                         wall_point(m.hd[t]) || post_dst.count(m.hd[t]);
+        (hot ? d : dc).push_back(m.hd[t]);
+        (hot ? s2 : sc).push_back(m.hs[t]);
+        if (hot)
+            hot_dst.insert(m.hd[t]);
+    }
+    for (size_t t = 0; t < m.hcd.size(); ++t)
+    {
+        const bool hot = all_hot || hot_point(ctx, dec, m.hcd[t]) || hot_dst.count(m.hcd[t]);
+        (hot ? cd : cdc).push_back(m.hcd[t]);
+        (hot ? cv : cvc).push_back(m.hcv[t]);
+    }
+    RUN(upload_list(ctx, m.hot, cd, cv, d, s2, m.staged));
+    RUN(upload_list(ctx, m.cold, cdc, cvc, dc, sc, m.staged));
+    int f, b, i, j, k;
+    for (const auto *tab : {&m.hd, &m.hcd})
+        for (uint64_t off : *tab)
+            if (dec.decode(off, f, b, i, j, k))
+                ctx->field_group[size_t(f)] = group;
+    m.built = true;
+    return MHD_OK;
+}
+
 // device lists of a group from its host tables: the full lists, and the hot
 // ones (copies to hot points; fixed values at hot points or at sources of
 // hot copies)
@@ -2155,6 +2229,8 @@ int build_sync(mhd_ctx *ctx, const std::string &group, SyncMap &m)
     const PoolDecoder dec(ctx);
     std::vector<uint64_t> d, s2, cd;
     std::vector<double> cv;
+    if (!ctx->poles.empty())
+        return build_sync_pole(ctx, group, m, dec);
     for (size_t t = 0; t < m.hd.size(); ++t)
         if (hot_point(ctx, dec, m.hd[t]))
         {
@@ -2187,11 +2263,32 @@ static int build_all_syncs(mhd_ctx *ctx)
 }
 
 // read-out of fields whose last sync ran its hot list only
+// cold copies then cold fixed values of a Pole context's group (the order
+// of the full Sync: its fixed values come last)
+static int run_cold(mhd_ctx *ctx, const std::string &group)
+{
+    auto it = ctx->syncs.find(group);
+    if (it == ctx->syncs.end())
+        return MHD_OK;
+    const CopyList &c = it->second.cold;
+    RUN(gather_map(ctx, c));
+    if (c.nconst > 0)
+    {
+        prof_begin(ctx, "k_set_consts");
+        k_set_consts<<<grid_for(c.nconst), kThreads, 0, ctx->stream>>>(ctx->pool, c.cdst, c.cval, c.nconst);
+        RUN(launched(ctx));
+    }
+    ctx->dirty[group] = false;
+    return MHD_OK;
+}
+
 static int materialise_group(mhd_ctx *ctx, const std::string &group)
 {
     auto it = ctx->dirty.find(group);
     if (it == ctx->dirty.end() || !it->second)
         return MHD_OK;
+    if (!ctx->poles.empty())
+        return run_cold(ctx, group);
     return run_sync(ctx, group.c_str(), true);
 }
 
@@ -2223,23 +2320,27 @@ static int materialise_field(mhd_ctx *ctx, int f)
 static int materialise_all(mhd_ctx *ctx)
 {
     RUN(materialise_pv(ctx));
+    std::vector<std::string> dirty;
     for (auto &kv : ctx->dirty)
         if (kv.second)
-            RUN(run_sync(ctx, kv.first.c_str(), true));
+            dirty.push_back(kv.first);
+    for (const auto &g : dirty)
+        RUN(materialise_group(ctx, g));
     return MHD_OK;
 }
 
 // after graph replays: every group ran its hot list
 static void mark_dirty(mhd_ctx *ctx)
 {
-    // a context with Poles runs every sync with its full lists: nothing is
-    // left to write at read-out (and a second Sync there is not idempotent:
-    // the Pole repairs change sources after their syncs, and a ring average
-    // of a ring need not reproduce it)
+    // a context with Poles leaves its cold lists (copies whose sources the
+    // step no longer changes) for read-out; the whole Sync is not run again
+    // there (it is not idempotent: the ring averages need not reproduce a
+    // ring, and the Pole repairs change sources after their syncs)
     for (auto &kv : ctx->syncs)
         if (kv.second.built)
-            ctx->dirty[kv.first] = ctx->poles.empty() && (kv.second.hot.n != kv.second.full.n ||
-                                                          kv.second.hot.nconst != kv.second.full.nconst);
+            ctx->dirty[kv.first] = ctx->poles.empty() ? (kv.second.hot.n != kv.second.full.n ||
+                                                         kv.second.hot.nconst != kv.second.full.nconst)
+                                                      : (kv.second.cold.n > 0 || kv.second.cold.nconst > 0);
     ctx->pv_dirty = true;
 }
 
