@@ -117,7 +117,10 @@ __device__ __forceinline__ void k_fluid_mixed_body(const BlockView *__restrict__
     const int64_t p = pidx(b, i, j, k);
     const int64_t pp[3] = {pidx(b, i + 1, j, k), pidx(b, i, j + 1, k), pidx(b, i, j, k + 1)};
     const double jac = b.f[F_Jac][p];
-    double km[3][3], kp[3][3]; // face metric at the low (p) and high (pp) face of each axis
+    // face metric at the low (p) and high (pp) face of each axis: FP32 copies
+    // for the fluxes, and the FP64 sum of the cell's signed face vectors
+    float km[3][3], kp[3][3];
+    double S[3] = {0.0, 0.0, 0.0};
     {
         // contravariant velocities (cell_u_contra): (k-bar . U_plus) / (|Jac| + 1e-30)
         const double *Up = b.f[F_Uplus];
@@ -128,15 +131,19 @@ __device__ __forceinline__ void k_fluid_mixed_body(const BlockView *__restrict__
         for (int a = 0; a < 3; ++a)
         {
             const double *M = b.f[F_JDxi + a];
+            double m_[3], p_[3];
 #pragma unroll
             for (int d = 0; d < 3; ++d)
             {
-                km[a][d] = M[d * v + p];
-                kp[a][d] = M[d * v + pp[a]];
+                m_[d] = M[d * v + p];
+                p_[d] = M[d * v + pp[a]];
+                km[a][d] = float(m_[d]);
+                kp[a][d] = float(p_[d]);
+                S[d] += p_[d] - m_[d];
             }
-            const double kx = 0.5 * (km[a][0] + kp[a][0]);
-            const double ky = 0.5 * (km[a][1] + kp[a][1]);
-            const double kz = 0.5 * (km[a][2] + kp[a][2]);
+            const double kx = 0.5 * (m_[0] + p_[0]);
+            const double ky = 0.5 * (m_[1] + p_[1]);
+            const double kz = 0.5 * (m_[2] + p_[2]);
             UC[a * v + p] = (kx * ux + ky * uy + kz * uz) * inv_jac;
         }
     }
@@ -147,21 +154,15 @@ __device__ __forceinline__ void k_fluid_mixed_body(const BlockView *__restrict__
     const double *q0 = b.qref;
     const Ref32 r0 = {float(q0[0]), {float(q0[1]), float(q0[2]), float(q0[3])}, float(q0[5] + q0[4])};
     float r[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-    double S[3] = {0.0, 0.0, 0.0}; // sum of the signed face vectors of the cell
 #pragma unroll
     for (int dir = 0; dir < 3; ++dir)
     {
         float Fm[5], Fp[5];
-        rusanov_dev32(b, r0, float(km[dir][0]), float(km[dir][1]), float(km[dir][2]), g[(G32_AREA + dir) * v + p], p,
-                      pm[dir], Fm);
-        rusanov_dev32(b, r0, float(kp[dir][0]), float(kp[dir][1]), float(kp[dir][2]),
-                      g[(G32_AREA + dir) * v + pp[dir]], pp[dir], p, Fp);
+        rusanov_dev32(b, r0, km[dir][0], km[dir][1], km[dir][2], g[(G32_AREA + dir) * v + p], p, pm[dir], Fm);
+        rusanov_dev32(b, r0, kp[dir][0], kp[dir][1], kp[dir][2], g[(G32_AREA + dir) * v + pp[dir]], pp[dir], p, Fp);
 #pragma unroll
         for (int m = 0; m < 5; ++m)
             r[m] += Fp[m] - Fm[m];
-#pragma unroll
-        for (int d = 0; d < 3; ++d)
-            S[d] += kp[dir][d] - km[dir][d];
     }
     // divergence of the reference-state flux, FP64: Phi0(S)
     const double US = S[0] * q0[1] + S[1] * q0[2] + S[2] * q0[3];
