@@ -2750,6 +2750,7 @@ int mhd_diagnostics(mhd_ctx *ctx, int32_t run, double *mins, double *maxs)
         return fail(ctx, MHD_ESTATE, "diagnostics during capture");
     if (!ctx->diag_keys)
         CK(ctx, cudaMalloc(&ctx->diag_keys, (DIAG_NMIN + DIAG_NQ) * sizeof(unsigned long long)));
+    RUN(materialise_field(ctx, F_PV)); // the pressure of PV_H
     prof_begin(ctx, "k_diag_init");
     k_diag_init<<<1, 32, 0, ctx->stream>>>(ctx->diag_keys);
     RUN(launched(ctx));

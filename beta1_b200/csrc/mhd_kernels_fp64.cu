@@ -1064,13 +1064,19 @@ __device__ __forceinline__ void k_pv_uplus_dt_body(const BlockView *__restrict__
                 eint = 0.0;
             double pr = (c.gamma - 1.0) * eint;
             pr = smax(pr, 1e-12);
-            const double T = pr / (rho * c.state_coeff);
-            double *PV = b.f[F_PV];
-            PV[p] = u;
-            PV[v + p] = vv;
-            PV[2 * v + p] = w;
-            PV[3 * v + p] = pr;
-            PV[4 * v + p] = T;
+            if (sizeof(WT) == sizeof(double))
+            {
+                // PV_H (the mixed form's pass leaves it to read-out: its flux
+                // reads the FP32 face states, its J x B source the velocities
+                // from U)
+                const double T = pr / (rho * c.state_coeff);
+                double *PV = b.f[F_PV];
+                PV[p] = u;
+                PV[v + p] = vv;
+                PV[2 * v + p] = w;
+                PV[3 * v + p] = pr;
+                PV[4 * v + p] = T;
+            }
             const bool has_plasma = U0 > 1e-20;
             double *Up = b.f[F_Uplus];
             Up[p] = has_plasma ? u : 0.0;

@@ -173,7 +173,7 @@ __device__ __forceinline__ void k_fluid_mixed_body(const BlockView *__restrict__
     const double rho = b.f[F_U][p];
     const double n_true = ((rho < 0.0) ? 0.0 : rho) / c.M_H * c.M_ref;
     const double fc = c.mom_hall * (n_true / sqrt(n_true * n_true + c.ne_floor * c.ne_floor));
-    const double *J = b.f[F_Jcell], *B = b.f[F_Bcell], *PV = b.f[F_PV];
+    const double *J = b.f[F_Jcell], *B = b.f[F_Bcell], *Uc = b.f[F_U];
     const double jx = J[p], jy = J[v + p], jz = J[2 * v + p];
     const double bx = B[p], by = B[v + p], bz = B[2 * v + p];
     const double fx = jy * bz - jz * by, fy = jz * bx - jx * bz, fz = jx * by - jy * bx;
@@ -183,7 +183,11 @@ __device__ __forceinline__ void k_fluid_mixed_body(const BlockView *__restrict__
     rhs[1] = -(double(r[1]) + phi[1]) * invJ + fc * fx;
     rhs[2] = -(double(r[2]) + phi[2]) * invJ + fc * fy;
     rhs[3] = -(double(r[3]) + phi[3]) * invJ + fc * fz;
-    rhs[4] = -(double(r[4]) + phi[4]) * invJ + fc * (fx * PV[p] + fy * PV[v + p] + fz * PV[2 * v + p]);
+    // the primitive velocities of calc_PV (the mixed form's derived pass
+    // leaves PV_H to read-out): U_m / max(rho, 1e-12)
+    const double rho_pv = (rho < 1e-12) ? 1e-12 : rho;
+    const double pu = Uc[v + p] / rho_pv, pv = Uc[2 * v + p] / rho_pv, pw = Uc[3 * v + p] / rho_pv;
+    rhs[4] = -(double(r[4]) + phi[4]) * invJ + fc * (fx * pu + fy * pv + fz * pw);
     double *R = b.f[F_RHS];
 #pragma unroll
     for (int m = 0; m < 5; ++m)
