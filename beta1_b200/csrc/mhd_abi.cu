@@ -175,6 +175,8 @@ struct mhd_ctx
     // sync in the topology order of the Pole shell
     std::vector<int> poles;
     int *dpoles = nullptr;
+    double *pole_cache = nullptr; // normal matrices of the Pole rings' least squares
+    int pole_stride = 0;          // rings per Pole and operation in pole_cache
     unsigned long long *diag_keys = nullptr; // output-step minima / maxima (mhd_diagnostics)
     // materialisation state: groups whose last sync ran its hot list only,
     // and PV / U_plus computed on the first ghost layer only
@@ -476,7 +478,7 @@ int launch_pole(mhd_ctx *ctx, int op)
         w = std::max(w, pole_work(op, v.ni, v.nk));
     }
     prof_begin(ctx, "k_pole");
-    launch_pole_op(op, w, np, ctx->stream, ctx->dbv, ctx->dpoles);
+    launch_pole_op(op, w, np, ctx->stream, ctx->dbv, ctx->dpoles, ctx->pole_cache, ctx->pole_stride, 0);
     return launched(ctx);
 }
 
@@ -582,6 +584,33 @@ int ensure_geom(mhd_ctx *ctx)
         k_geom32<<<dim3(grid_for(vmax), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv);
         RUN(launched(ctx));
     }
+    const int np = int(ctx->poles.size() / 2);
+    if (np > 0)
+    {
+        // the Pole rings' normal matrices, from the geometry
+        int stride = 0;
+        for (int q = 0; q < np; ++q)
+            stride = std::max(stride, ctx->hbv[size_t(ctx->poles[size_t(2 * q)])].ni + 1);
+        if (stride != ctx->pole_stride || !ctx->pole_cache)
+        {
+            cudaFree(ctx->pole_cache);
+            ctx->pole_cache = nullptr;
+            CK(ctx, cudaMalloc(&ctx->pole_cache, size_t(np) * 3 * size_t(stride) * 10 * sizeof(double)));
+            ctx->pole_stride = stride;
+        }
+        for (int op : {int(POLE_BCELL), int(POLE_EETA_REG), int(POLE_JCELL)})
+        {
+            int64_t w = 0;
+            for (int q = 0; q < np; ++q)
+            {
+                const BlockView &v = ctx->hbv[size_t(ctx->poles[size_t(2 * q)])];
+                w = std::max(w, pole_work(op, v.ni, v.nk));
+            }
+            prof_begin(ctx, "k_pole");
+            launch_pole_op(op, w, np, ctx->stream, ctx->dbv, ctx->dpoles, ctx->pole_cache, ctx->pole_stride, 1);
+            RUN(launched(ctx));
+        }
+    }
     ctx->geom_dirty = false;
     return MHD_OK;
 }
@@ -650,27 +679,25 @@ int launch_update_derived_pole(mhd_ctx *ctx)
     return MHD_OK;
 }
 
-int launch_fluid_ucontra(mhd_ctx *ctx, bool with_update);
+int launch_fluid_ucontra(mhd_ctx *ctx);
 
 int launch_fluid_rhs(mhd_ctx *ctx)
 {
     if (ctx->pool32) // the mixed form's flux pass (its FP32 U_contra are a by-product)
-        return launch_fluid_ucontra(ctx, false);
+        return launch_fluid_ucontra(ctx);
     const int64_t nc = max_box(ctx, LOC_CELL, 0);
     prof_begin(ctx, "k_fluid_rhs");
     k_fluid_rhs<<<dim3(grid_for(nc), ctx->nblocks), kThreads, 0, ctx->stream>>>(ctx->dbv, ctx->c, nc);
     return launched(ctx);
 }
 
-// fluid RHS together with the contravariant velocities of the EMF stencils;
-// with_update (mixed form only): the cell update U += dt RHS_H in the same pass
-int launch_fluid_ucontra(mhd_ctx *ctx, bool with_update)
+// fluid RHS together with the contravariant velocities of the EMF stencils
+int launch_fluid_ucontra(mhd_ctx *ctx)
 {
     if (ctx->pool32)
     {
         prof_begin(ctx, "k_fluid_mixed");
-        launch_k_fluid_mixed(ctx->tune[TUNE_k_fluid_mixed], grid_kind(ctx, KIND_CELL1), ctx->stream, ctx->dbv, ctx->c,
-                             with_update ? ctx->dt : nullptr);
+        launch_k_fluid_mixed(ctx->tune[TUNE_k_fluid_mixed], grid_kind(ctx, KIND_CELL1), ctx->stream, ctx->dbv, ctx->c);
         return launched(ctx);
     }
     prof_begin(ctx, "k_fluid_ucontra");
@@ -1064,14 +1091,14 @@ int launch_resistive(mhd_ctx *ctx)
     return launch_curl_rng(ctx, F_Eresxi, F_RBresxi, F_Bxi, -1.0, 0);
 }
 
-// the Euler stage at the current dt: fluid RHS, CT induction with the face-B
-// update, cell update (in the mixed form done by the flux pass itself)
+// the Euler stage at the current dt: fluid RHS, CT induction with the
+// face-B update, cell update.  (The cell update stays a pass of its own: in
+// the latency-bound mixed flux pass it ran slower than alone.)
 int launch_euler_core(mhd_ctx *ctx)
 {
-    const bool fused = ctx->pool32 != nullptr;
-    RUN(launch_fluid_ucontra(ctx, fused));
+    RUN(launch_fluid_ucontra(ctx));
     RUN(launch_induction(ctx, /*update_b=*/true, /*with_ucontra=*/false));
-    return fused ? MHD_OK : launch_update_u(ctx);
+    return launch_update_u(ctx);
 }
 
 // one LunarSolver::StepOnce, explicit part: dt, fluid RHS, CT induction, update
@@ -1762,6 +1789,7 @@ int mhd_ctx_destroy(mhd_ctx *ctx)
         cudaFree(kv.second.dwalls);
     }
     cudaFree(ctx->dpoles);
+    cudaFree(ctx->pole_cache);
     cudaFree(ctx->diag_keys);
     free_resistive(ctx);
     cudaFree(ctx->hall_zb);
@@ -1832,8 +1860,9 @@ static int transfer(mhd_ctx *ctx, const char *name, int32_t block, const double 
     const int nc = kFields[f].ncomp;
     if (hin)
     {
-        if (f == F_JDxi || f == F_JDeta || f == F_JDzeta || f == F_WB || f == F_WJ)
-            ctx->geom_dirty = true; // face normals and the FP32 copies follow
+        if (f == F_JDxi || f == F_JDeta || f == F_JDzeta || f == F_WB || f == F_WJ || f == F_drxi || f == F_dreta ||
+            f == F_drzeta)
+            ctx->geom_dirty = true; // face normals, FP32 copies and Pole matrices follow
         CK(ctx, cudaMemcpyAsync(ctx->staging, hin, size_t(n) * 8, cudaMemcpyHostToDevice, ctx->stream));
         prof_begin(ctx, "k_aos_to_soa");
         k_aos_to_soa<<<grid_for(n), kThreads, 0, ctx->stream>>>(ctx->dbv, block, f, nc, lo[0], lo[1], lo[2],
@@ -2788,6 +2817,7 @@ int mhd_set_pole(mhd_ctx *ctx, int32_t block, int32_t direction)
     RUN(upload_vec(ctx, ctx->poles, &ctx->dpoles));
     for (auto &kv : ctx->syncs)
         kv.second.built = false;
+    ctx->geom_dirty = true; // the rings' normal matrices
     drop_graph(ctx);
     return MHD_OK;
 }
@@ -3325,6 +3355,7 @@ int mhd_sync(mhd_ctx *ctx, const char *group)
     BIND_DEVICE(ctx);
     if (!ctx || !group)
         return MHD_EINVAL;
+    RUN(ensure_geom(ctx));
     RUN(run_sync(ctx, group, true));
     CK(ctx, cudaStreamSynchronize(ctx->stream));
     return MHD_OK;

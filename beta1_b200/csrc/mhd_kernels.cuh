@@ -46,8 +46,11 @@ __global__ void k_jcell(const BlockView *bvs);
 // (block, direction) pair in `poles`, one grid row per Pole
 __global__ void k_pole(const BlockView *bvs, const int *poles, int op);
 // one Pole operation over every Pole (work items per Pole: pole_work); the
-// ring least squares run one warp per ring
-void launch_pole_op(int op, int64_t work, int npoles, cudaStream_t st, const BlockView *bvs, const int *poles);
+// ring least squares run one warp per ring, with their geometry-only normal
+// matrices in `cache` (per Pole, per least-squares operation, `stride`
+// rings, 10 values each), which build = 1 fills (after every geometry change)
+void launch_pole_op(int op, int64_t work, int npoles, cudaStream_t st, const BlockView *bvs, const int *poles,
+                    double *cache, int stride, int build);
 __global__ void k_geometry(const BlockView *bvs, int blk, NodeMesh m, int G, int group0, double b0, double b1,
                            double b2);
 // output-step minima / maxima over the inner cells of a run's blocks (run < 0:
@@ -221,7 +224,6 @@ int launch_k_curl_e2f(int variant, dim3 grid, cudaStream_t st, const BlockView *
 // k_eedge: minimum CTAs per SM 0, 8
 int launch_k_eedge(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs);
 // k_fluid_mixed: minimum CTAs per SM 2, 0, 3
-// dtp non-null: also U += dt RHS_H on the inner cells (the step's update)
-int launch_k_fluid_mixed(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c, const double *dtp);
+int launch_k_fluid_mixed(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c);
 
 } // namespace mhd

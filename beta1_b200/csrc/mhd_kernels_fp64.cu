@@ -2008,9 +2008,12 @@ __global__ void k_pole(const BlockView *__restrict__ bvs, const int *__restrict_
 // The ring least squares of POLE_BCELL, POLE_EETA_REG and POLE_JCELL with one
 // warp per ring.  The lanes form the pushed vectors and values of 32 k at a
 // time (square roots and divisions in parallel, the same operations as
-// pole_one); lane 0 then pushes them in the reference's order -- k, then the
-// handler's order within k -- so A and the right-hand side are summed exactly
-// as the one-thread ring sums them, and solves; the lanes write the ring.
+// pole_one).  Each sum then runs in one lane over the pushes in the
+// reference's order (k, then the handler's order within k), so it equals the
+// one-thread ring sum bit for bit: the normal matrix A and the count depend
+// on the geometry only and are summed once per geometry (build), nine lanes
+// one entry each; every application sums the right-hand side, three lanes
+// one component each, and lane 0 regularises, solves and broadcasts.
 // ---------------------------------------------------------------------------
 constexpr int kPoleWarps = 4; // warps (rings) per CTA
 constexpr int kPoleTerms = 8; // at most 8 pushes per k (J_cell)
@@ -2021,58 +2024,88 @@ struct PoleTerm
     int ok;
 };
 
-__device__ __forceinline__ void pole_push_chunk(const PoleTerm *sh, int nterm, double A[3][3], double rhs[3], int &cnt)
-{
-    for (int q = 0; q < nterm; ++q)
-        if (sh[q].ok)
-        {
-            pole_push(A, rhs, sh[q].s, sh[q].phi);
-            ++cnt;
-        }
-}
-
-// regularised 3x3 solve of lane 0, broadcast to the warp; false when the
-// ring has no usable term (cnt <= 0) or the solve fails
-__device__ __forceinline__ bool pole_solve_bcast(double A[3][3], double rhs[3], int cnt, double x[3], bool trace_abs,
-                                                 int &status)
+// one chunk of pushes: build: lane q < 9 sums s[q / 3] s[q % 3] (A), lane 9
+// counts; apply: lane a < 3 sums phi s[a]
+__device__ __forceinline__ void pole_accumulate(const PoleTerm *sh, int nterm, bool build, double &acc, int &cnt)
 {
     const int lane = threadIdx.x & 31;
+    if (build)
+    {
+        if (lane < 9)
+        {
+            const int a = lane / 3, c = lane % 3;
+            for (int q = 0; q < nterm; ++q)
+                if (sh[q].ok)
+                    acc += sh[q].s[a] * sh[q].s[c];
+        }
+        else if (lane == 9)
+            for (int q = 0; q < nterm; ++q)
+                cnt += sh[q].ok ? 1 : 0;
+    }
+    else if (lane < 3)
+        for (int q = 0; q < nterm; ++q)
+            if (sh[q].ok)
+                acc += sh[q].phi * sh[q].s[lane];
+}
+
+// build: store the ring's A and count (cache[0..8], cache[9]); apply: lane 0
+// loads them, regularises (trace of |A_aa| or of A_aa), solves and
+// broadcasts x.  status: 0 solved, 1 no usable push (count_guard), 2 singular
+__device__ bool pole_finish(double acc, int cnt, bool build, double *cache, bool trace_abs, bool count_guard,
+                            double x[3], int &status)
+{
+    const int lane = threadIdx.x & 31;
+    if (build)
+    {
+        if (lane < 9)
+            cache[lane] = acc;
+        else if (lane == 9)
+            cache[9] = double(cnt);
+        status = 3;
+        return false;
+    }
+    const double r0 = __shfl_sync(0xffffffffu, acc, 0), r1 = __shfl_sync(0xffffffffu, acc, 1),
+                 r2 = __shfl_sync(0xffffffffu, acc, 2);
     int st = 0;
+    double xs[3] = {0.0, 0.0, 0.0};
     if (lane == 0)
     {
-        if (cnt <= 0)
+        if (count_guard && int(cache[9]) <= 0)
             st = 1;
         else
         {
+            double A[3][3] = {{cache[0], cache[1], cache[2]}, {cache[3], cache[4], cache[5]}, {cache[6], cache[7], cache[8]}};
+            const double rhs[3] = {r0, r1, r2};
             const double tr = trace_abs ? fabs(A[0][0]) + fabs(A[1][1]) + fabs(A[2][2]) : A[0][0] + A[1][1] + A[2][2];
             const double reg = 1.0e-12 * pole_max1(tr);
             A[0][0] += reg;
             A[1][1] += reg;
             A[2][2] += reg;
-            st = pole_solve3(A, rhs, x) ? 0 : 2;
+            st = pole_solve3(A, rhs, xs) ? 0 : 2;
         }
     }
     status = __shfl_sync(0xffffffffu, st, 0);
 #pragma unroll
     for (int c = 0; c < 3; ++c)
-        x[c] = __shfl_sync(0xffffffffu, lane == 0 ? x[c] : 0.0, 0);
+        x[c] = __shfl_sync(0xffffffffu, xs[c], 0);
     return status == 0;
 }
 
-__device__ void pole_bcell_warp(const BlockView &b, int side, int64_t t, PoleTerm *sh)
+__device__ void pole_bcell_warp(const BlockView &b, int side, int64_t t, PoleTerm *sh, double *cache, bool build)
 {
     const int lane = threadIdx.x & 31;
     const int nj = b.nj, nk = b.nk;
     const int64_t v = b.vol;
     const int i = int(t >> 1);
     const bool total = (t & 1) == 0;
+    if (build && !total)
+        return; // one A per ring, shared by the total and the induced field
     const int jc = side < 0 ? 0 : nj - 1;
     const int jn = side < 0 ? jc + 1 : jc;
     const double sn = side < 0 ? 1.0 : -1.0;
     const double *Aet = b.f[F_JDeta], *Axi = b.f[F_JDxi];
     const double *Bet = b.f[F_Beta], *Bxi = b.f[F_Bxi], *Aadd = b.f[F_Baddeta], *Xadd = b.f[F_Baddxi];
-    double A[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
-    double rhs[3] = {0.0, 0.0, 0.0};
+    double acc = 0.0;
     int cnt = 0;
     for (int k0 = 0; k0 < nk; k0 += 32)
     {
@@ -2100,15 +2133,13 @@ __device__ void pole_bcell_warp(const BlockView &b, int side, int64_t t, PoleTer
             }
         }
         __syncwarp();
-        if (lane == 0)
-            pole_push_chunk(sh, 3 * min(32, nk - k0), A, rhs, cnt);
+        pole_accumulate(sh, 3 * min(32, nk - k0), build, acc, cnt);
         __syncwarp();
     }
-    // BC_Pole_Bcell_Collapse_ pushes no count: the system is solved whenever
-    // it is regular (cnt is only the "any term" guard here)
+    // BC_Pole_Bcell_Collapse_ solves whenever the regularised system is regular
     double Bp[3];
     int st;
-    if (!pole_solve_bcast(A, rhs, 1, Bp, true, st))
+    if (!pole_finish(acc, cnt, build, cache, true, false, Bp, st))
         return;
     double *Out = b.f[total ? F_Bcell : F_Bind];
     for (int k = lane; k < nk; k += 32)
@@ -2120,7 +2151,7 @@ __device__ void pole_bcell_warp(const BlockView &b, int side, int64_t t, PoleTer
     }
 }
 
-__device__ void pole_eeta_warp(const BlockView &b, int side, int64_t t, PoleTerm *sh)
+__device__ void pole_eeta_warp(const BlockView &b, int side, int64_t t, PoleTerm *sh, double *cache, bool build)
 {
     const int lane = threadIdx.x & 31;
     const int nj = b.nj, nk = b.nk;
@@ -2129,8 +2160,7 @@ __device__ void pole_eeta_warp(const BlockView &b, int side, int64_t t, PoleTerm
     const int jc = side < 0 ? 0 : nj - 1;
     double *E = b.f[F_Eeta];
     const double *dr = b.f[F_dreta];
-    double A[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
-    double rhs[3] = {0.0, 0.0, 0.0};
+    double acc = 0.0;
     int cnt = 0;
     for (int k0 = 0; k0 < nk; k0 += 32) // k = n_k is the same edge as k = 0
     {
@@ -2148,17 +2178,16 @@ __device__ void pole_eeta_warp(const BlockView &b, int side, int64_t t, PoleTerm
                 o.s[0] = d0 * invL;
                 o.s[1] = d1 * invL;
                 o.s[2] = d2 * invL;
-                o.phi = E[p] * invL;
+                o.phi = build ? 0.0 : E[p] * invL;
             }
         }
         __syncwarp();
-        if (lane == 0)
-            pole_push_chunk(sh, min(32, nk - k0), A, rhs, cnt);
+        pole_accumulate(sh, min(32, nk - k0), build, acc, cnt);
         __syncwarp();
     }
     double Ev[3];
     int st;
-    if (pole_solve_bcast(A, rhs, __shfl_sync(0xffffffffu, cnt, 0), Ev, false, st))
+    if (pole_finish(acc, cnt, build, cache, false, true, Ev, st))
     {
         for (int k = lane; k <= nk; k += 32)
         {
@@ -2175,6 +2204,8 @@ __device__ void pole_eeta_warp(const BlockView &b, int side, int64_t t, PoleTerm
             E[pidx(b, i, jc, k)] = 0.0;
         return;
     }
+    if (st != 2)
+        return; // build
     // singular system: the ring average, summed in k order by lane 0
     double avg = 0.0;
     if (lane == 0)
@@ -2188,7 +2219,7 @@ __device__ void pole_eeta_warp(const BlockView &b, int side, int64_t t, PoleTerm
         E[pidx(b, i, jc, k)] = avg;
 }
 
-__device__ void pole_jcell_warp(const BlockView &b, int side, int64_t t, PoleTerm *sh)
+__device__ void pole_jcell_warp(const BlockView &b, int side, int64_t t, PoleTerm *sh, double *cache, bool build)
 {
     const int lane = threadIdx.x & 31;
     const int nj = b.nj, nk = b.nk;
@@ -2201,8 +2232,7 @@ __device__ void pole_jcell_warp(const BlockView &b, int side, int64_t t, PoleTer
     const int dk[8] = {0, 0, 1, 1, 0, 1, 0, 0};
     const int fj[8] = {F_Jeta, F_Jeta, F_Jeta, F_Jeta, F_Jxi, F_Jxi, F_Jzeta, F_Jzeta};
     const int fd[8] = {F_dreta, F_dreta, F_dreta, F_dreta, F_drxi, F_drxi, F_drzeta, F_drzeta};
-    double A[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
-    double rhs[3] = {0.0, 0.0, 0.0};
+    double acc = 0.0;
     int cnt = 0;
     for (int k0 = 0; k0 < nk; k0 += 32)
     {
@@ -2223,18 +2253,17 @@ __device__ void pole_jcell_warp(const BlockView &b, int side, int64_t t, PoleTer
                     o.s[0] = dx / L;
                     o.s[1] = dy / L;
                     o.s[2] = dz / L;
-                    o.phi = b.f[fj[q]][p] / L;
+                    o.phi = build ? 0.0 : b.f[fj[q]][p] / L;
                 }
             }
         }
         __syncwarp();
-        if (lane == 0)
-            pole_push_chunk(sh, 8 * min(32, nk - k0), A, rhs, cnt);
+        pole_accumulate(sh, 8 * min(32, nk - k0), build, acc, cnt);
         __syncwarp();
     }
     double Jp[3];
     int st;
-    if (!pole_solve_bcast(A, rhs, __shfl_sync(0xffffffffu, cnt, 0), Jp, false, st))
+    if (!pole_finish(acc, cnt, build, cache, false, true, Jp, st))
         return;
     double *Jc = b.f[F_Jcell];
     for (int k = lane; k < nk; k += 32)
@@ -2246,8 +2275,17 @@ __device__ void pole_jcell_warp(const BlockView &b, int side, int64_t t, PoleTer
     }
 }
 
+// which of the three least-squares operations (cache slot), -1 otherwise
+__host__ __device__ inline int pole_lsq_slot(int op)
+{
+    return op == POLE_BCELL ? 0 : op == POLE_EETA_REG ? 1 : op == POLE_JCELL ? 2 : -1;
+}
+
+// cache: per Pole, per least-squares operation, per ring i (stride rings):
+// A (9 values) and the push count
 __global__ void __launch_bounds__(32 * kPoleWarps) k_pole_warp(const BlockView *__restrict__ bvs,
-                                                               const int *__restrict__ poles, int op)
+                                                               const int *__restrict__ poles, int op,
+                                                               double *__restrict__ cache, int stride, int build)
 {
     __shared__ PoleTerm sh[kPoleWarps][32 * kPoleTerms];
     const BlockView &b = bvs[poles[2 * blockIdx.y]];
@@ -2256,20 +2294,23 @@ __global__ void __launch_bounds__(32 * kPoleWarps) k_pole_warp(const BlockView *
     const int64_t t = int64_t(blockIdx.x) * kPoleWarps + warp;
     if (t >= pole_work(op, b.ni, b.nk))
         return; // the whole warp leaves together
+    const int ring = (op == POLE_BCELL) ? int(t >> 1) : int(t);
+    double *c = cache + ((int64_t(blockIdx.y) * 3 + pole_lsq_slot(op)) * stride + ring) * 10;
     if (op == POLE_BCELL)
-        pole_bcell_warp(b, side, t, sh[warp]);
+        pole_bcell_warp(b, side, t, sh[warp], c, build != 0);
     else if (op == POLE_EETA_REG)
-        pole_eeta_warp(b, side, t, sh[warp]);
+        pole_eeta_warp(b, side, t, sh[warp], c, build != 0);
     else
-        pole_jcell_warp(b, side, t, sh[warp]);
+        pole_jcell_warp(b, side, t, sh[warp], c, build != 0);
 }
 
-void launch_pole_op(int op, int64_t work, int npoles, cudaStream_t st, const BlockView *bvs, const int *poles)
+void launch_pole_op(int op, int64_t work, int npoles, cudaStream_t st, const BlockView *bvs, const int *poles,
+                    double *cache, int stride, int build)
 {
-    if (op == POLE_BCELL || op == POLE_EETA_REG || op == POLE_JCELL)
+    if (pole_lsq_slot(op) >= 0)
         k_pole_warp<<<dim3(unsigned((work + kPoleWarps - 1) / kPoleWarps), unsigned(npoles)), 32 * kPoleWarps, 0,
-                      st>>>(bvs, poles, op);
-    else
+                      st>>>(bvs, poles, op, cache, stride, build);
+    else if (!build)
         k_pole<<<dim3(unsigned((work + 255) / 256), unsigned(npoles)), 256, 0, st>>>(bvs, poles, op);
 }
 

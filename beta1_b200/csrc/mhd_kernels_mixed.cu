@@ -94,14 +94,7 @@ __device__ __forceinline__ void rusanov_dev32(const BlockView &b, const Ref32 &r
 // variants: at least 2 CTAs per SM (128 registers; the default: uncapped it
 // takes 168 registers and one CTA, 0.265 -> 0.171 ms on the C2 step),
 // uncapped, at least 3
-// dtp (may be null): the step's dt per run; when given, the cell part of
-// ApplyUpdate_Euler_ (U += dt RHS_H, LunarSolver_Advance.cpp:82-93) is done
-// here too, with the same unfused multiply and add as the update kernel.
-// Safe in this pass: it reads U only at its own cell (the neighbours' face
-// states come from the FP32 copies), and no kernel between the flux pass and
-// the update reads U.
-__device__ __forceinline__ void k_fluid_mixed_body(const BlockView *__restrict__ bvs, Consts c,
-                                                   const double *__restrict__ dtp)
+__device__ __forceinline__ void k_fluid_mixed_body(const BlockView *__restrict__ bvs, Consts c)
 {
     int64_t t;
     const BlockView &b = bvs[cta_block(bvs, KIND_CELL1, t)];
@@ -192,42 +185,33 @@ __device__ __forceinline__ void k_fluid_mixed_body(const BlockView *__restrict__
 #pragma unroll
     for (int m = 0; m < 5; ++m)
         R[m * v + p] = rhs[m];
-    if (dtp)
-    {
-        const double dt = dtp[b.run];
-        double *U = b.f[F_U];
-#pragma unroll
-        for (int m = 0; m < 5; ++m)
-            U[m * v + p] = __dadd_rn(U[m * v + p], __dmul_rn(dt, rhs[m]));
-    }
 }
 
 template <int MINB>
-__global__ void __launch_bounds__(256, MINB) k_fluid_mixed_t(const BlockView *__restrict__ bvs, Consts c,
-                                                             const double *__restrict__ dtp)
+__global__ void __launch_bounds__(256, MINB) k_fluid_mixed_t(const BlockView *__restrict__ bvs, Consts c)
 {
-    k_fluid_mixed_body(bvs, c, dtp);
+    k_fluid_mixed_body(bvs, c);
 }
 // the compiler's own register allocation (no launch bounds)
-__global__ void k_fluid_mixed_free(const BlockView *__restrict__ bvs, Consts c, const double *__restrict__ dtp)
+__global__ void k_fluid_mixed_free(const BlockView *__restrict__ bvs, Consts c)
 {
-    k_fluid_mixed_body(bvs, c, dtp);
+    k_fluid_mixed_body(bvs, c);
 }
 
 
 // launchers of the register / occupancy variants (tuned by mhd_autotune)
-int launch_k_fluid_mixed(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c, const double *dtp)
+int launch_k_fluid_mixed(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c)
 {
     switch (variant)
     {
     case 0:
-        k_fluid_mixed_t<2><<<grid, 256, 0, st>>>(bvs, c, dtp);
+        k_fluid_mixed_t<2><<<grid, 256, 0, st>>>(bvs, c);
         break;
     case 1:
-        k_fluid_mixed_free<<<grid, 256, 0, st>>>(bvs, c, dtp);
+        k_fluid_mixed_free<<<grid, 256, 0, st>>>(bvs, c);
         break;
     case 2:
-        k_fluid_mixed_t<3><<<grid, 256, 0, st>>>(bvs, c, dtp);
+        k_fluid_mixed_t<3><<<grid, 256, 0, st>>>(bvs, c);
         break;
     default:
         return -1;
