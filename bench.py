@@ -105,8 +105,14 @@ FLUX_CT_GROUP = ("k_fluid_ucontra", "k_fluid_mixed", "k_eface", "k_eedge", "k_cu
 FLUX_CT_BYTES = {False: 280, True: 216}
 WHOLE_GRID_KERNELS = {"k_pv_uplus_dt", "k_fluid_ucontra", "k_fluid_mixed", "k_bcell_jedge", "k_eface", "k_eedge",
                       "k_update_u", "k_hall_cell", "k_hall_edge", "k_bcell", "k_jedge"}
-# the mixed form's PV pass also writes the 7 FP32 face states
-ALGO_BYTES_MIXED_EXTRA = {"k_pv_uplus_dt": 7 * 4}
+# The mixed form's kernels where they differ: the PV pass reads the 36 J_cell
+# weights as FP32 copies and writes U_plus 3, J_cell 3 and the 7 FP32 face
+# states (PV_H and the FP64 face states are left to read-out): U 5, Jac 1,
+# B_cell 3, face area + normal 12, J 3 read as FP64 plus 36 FP32 weights;
+# 6 FP64 and 7 FP32 written.  The B_cell passes read their 18 weights as FP32.
+ALGO_BYTES_MIXED = {"k_pv_uplus_dt": 24 * 8 + 36 * 4 + 6 * 8 + 7 * 4,
+                    "k_bcell": 12 * 8 + 18 * 4,
+                    "k_bcell_jedge": 21 * 8 + 18 * 4}
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of
 # the dominant kernel, from one ncu capture of the C2 workload at half the
@@ -579,7 +585,7 @@ def main():
         n, its = res_stats["unknowns"], max(1, res_stats["krylov_its_last_step"])
         bytes_per_launch = (its + 1) * 18 * 8 * (n / 3.0) + sum((2 * k + 4) * 8 * n for k in range(1, its + 1))
     elif dominant in ALGO_BYTES_PER_CELL:
-        algo = ALGO_BYTES_PER_CELL[dominant] + (ALGO_BYTES_MIXED_EXTRA.get(dominant, 0) if mixed else 0)
+        algo = ALGO_BYTES_MIXED.get(dominant, ALGO_BYTES_PER_CELL[dominant]) if mixed else ALGO_BYTES_PER_CELL[dominant]
         # kernels whose every launch covers the whole grid (the Hall EMF runs
         # once per Newton / Krylov evaluation); other kernels' per-step bytes
         # are shared by their launches (per-block or region launches)
