@@ -1,7 +1,8 @@
 """Builds the in-tree CUDA library libbeta1_mhd.so for sm_100a with nvcc.
 
 The FP64 kernels are compiled with -fmad=false (no contracted multiply-adds)
-so that they reproduce the reference's CPU arithmetic bit for bit; the rest
+so that they reproduce the reference's CPU arithmetic bit for bit; the mixed
+form's kernels too, so that its kernel variants agree bit for bit; the rest
 is compiled normally.
 """
 from __future__ import annotations
@@ -20,7 +21,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 # (source, extra flags)
 UNITS = [
     ("mhd_kernels_fp64.cu", ["-fmad=false"]),
-    ("mhd_kernels_mixed.cu", []),
+    ("mhd_kernels_mixed.cu", ["-fmad=false"]),
     ("mhd_krylov.cu", []),
     ("mhd_abi.cu", []),
 ]

@@ -136,8 +136,11 @@ const char *const kTuneNames[NTUNE] = {"k_pv_uplus_dt", "k_fluid_ucontra", "k_bc
                                        "k_curl_e2f",    "k_eedge",         "k_fluid_mixed"};
 // minimum CTAs per SM of each variant (variant 0 first; 0: the compiler's
 // own allocation, no launch bounds) and the number of variants
-const int kTuneMinCtas[NTUNE][3] = {{4, 0, 5}, {0, 3, 0}, {0, 6, 0}, {0, 6, 0}, {0, 6, 0}, {0, 8, 0}, {2, 0, 3}};
-const int kTuneCount[NTUNE] = {3, 2, 2, 2, 2, 2, 3};
+// per variant the reported value: the minimum CTAs per SM of its launch
+// bounds (0: none); 12 for the face-tiled k_fluid_mixed (2 CTAs per SM)
+const int kTuneMinCtas[NTUNE][4] = {{4, 0, 5, 0}, {0, 3, 0, 0}, {0, 6, 0, 0}, {0, 6, 0, 0},
+                                    {0, 6, 0, 0}, {0, 8, 0, 0}, {2, 0, 3, 12}};
+const int kTuneCount[NTUNE] = {3, 2, 2, 2, 2, 2, 4};
 
 struct mhd_ctx
 {
@@ -169,7 +172,7 @@ struct mhd_ctx
     // flattened launches (batches): block of every CTA per launch kind
     bool flat = false;
     int *cta_tab = nullptr;
-    int64_t cta_total[NKIND] = {0, 0, 0};
+    int64_t cta_total[NKIND] = {};
     std::map<std::string, SyncMap> syncs;
     // eta Poles: (block, direction) pairs; a context with Poles runs every
     // sync in the topology order of the Pole shell
@@ -368,6 +371,9 @@ int64_t kind_points(const BlockView &v, int kind)
         return int64_t(v.ni) * v.nj * v.nk;
     if (kind == KIND_CELL1)
         return int64_t(v.ni + 2) * (v.nj + 2) * (v.nk + 2);
+    if (kind == KIND_TILE1) // one CTA of kThreads per tile
+        return int64_t((v.ni + 2 + TILE_I - 1) / TILE_I) * ((v.nj + 2 + TILE_J - 1) / TILE_J) *
+               ((v.nk + 2 + TILE_K - 1) / TILE_K) * kThreads;
     return int64_t(v.ni + 1) * (v.nj + 1) * (v.nk + 1);
 }
 
@@ -697,7 +703,8 @@ int launch_fluid_ucontra(mhd_ctx *ctx)
     if (ctx->pool32)
     {
         prof_begin(ctx, "k_fluid_mixed");
-        launch_k_fluid_mixed(ctx->tune[TUNE_k_fluid_mixed], grid_kind(ctx, KIND_CELL1), ctx->stream, ctx->dbv, ctx->c);
+        const int var = ctx->tune[TUNE_k_fluid_mixed];
+        launch_k_fluid_mixed(var, grid_kind(ctx, var == 3 ? KIND_TILE1 : KIND_CELL1), ctx->stream, ctx->dbv, ctx->c);
         return launched(ctx);
     }
     prof_begin(ctx, "k_fluid_ucontra");
@@ -1725,7 +1732,7 @@ int create_ctx(const mhd_block_desc *blocks, int32_t nblocks, const int32_t *run
     if (nruns > 1)
     {
         std::vector<int> tab;
-        int64_t first[NKIND] = {0, 0, 0};
+        int64_t first[NKIND] = {};
         for (int kind = 0; kind < NKIND; ++kind)
         {
             first[kind] = int64_t(tab.size());
@@ -3270,6 +3277,32 @@ int mhd_autotune(mhd_ctx *ctx, int32_t reps, int32_t *min_ctas, int32_t n)
 }
 
 const char *mhd_tune_name(int32_t i) { return (i >= 0 && i < NTUNE) ? kTuneNames[i] : nullptr; }
+
+int mhd_set_tune(mhd_ctx *ctx, const int32_t *min_ctas, int32_t n)
+{
+    BIND_DEVICE(ctx);
+    if (!ctx || n < 0 || n > NTUNE || (n > 0 && !min_ctas))
+        return fail(ctx, MHD_EINVAL, "bad variant list");
+    if (ctx->capturing)
+        return fail(ctx, MHD_ESTATE, "variants changed during capture");
+    int chosen[NTUNE];
+    for (int t = 0; t < NTUNE; ++t)
+    {
+        chosen[t] = ctx->tune[t];
+        if (t >= n)
+            continue;
+        chosen[t] = -1;
+        for (int v = 0; v < kTuneCount[t]; ++v)
+            if (kTuneMinCtas[t][v] == min_ctas[t])
+                chosen[t] = v;
+        if (chosen[t] < 0)
+            return fail(ctx, MHD_EINVAL, "kernel %s has no variant %d", kTuneNames[t], min_ctas[t]);
+    }
+    for (int t = 0; t < NTUNE; ++t)
+        ctx->tune[t] = chosen[t];
+    drop_graph(ctx);
+    return MHD_OK;
+}
 
 int mhd_resistive_stats(const mhd_ctx *ctx, int32_t *its, double *rnorm, double *bnorm, int32_t *reason)
 {

@@ -12,7 +12,8 @@
 // conserved update, the contravariant velocities of the CT EMF, the EMF
 // itself, its curl and the face-B update stay FP64 (the contravariant
 // velocities here, the rest in other translation units), so div B stays at
-// FP64 round-off.  Compiled with contracted multiply-adds.
+// FP64 round-off.  Compiled without contracted multiply-adds, so that the
+// per-cell and the face-tiled flux kernels give the same bits.
 #include "mhd_kernels.cuh"
 
 namespace mhd
@@ -88,6 +89,39 @@ __device__ __forceinline__ void rusanov_dev32(const BlockView &b, const Ref32 &r
         out[m] = 0.5f * (dF[0][m] + dF[1][m]) - 0.5f * rad * (dC[1][m] - dC[0][m]);
 }
 
+// RHS_H of one inner cell from its FP32 flux-deviation sum r: the FP64
+// divergence of the reference-state flux Phi0(S) (S the sum of the cell's
+// signed face vectors), the FP64 J x B force with the Hall_Num_Limiter weight
+// and its work, over the FP64 cell volume
+__device__ __forceinline__ void mixed_rhs(const BlockView &b, const Consts &c, int64_t p, double jac,
+                                          const double S[3], const float r[5])
+{
+    const int64_t v = b.vol;
+    const double *q0 = b.qref;
+    const double US = S[0] * q0[1] + S[1] * q0[2] + S[2] * q0[3];
+    const double mS = q0[0] * US;
+    const double phi[5] = {mS, mS * q0[1] + S[0] * q0[4], mS * q0[2] + S[1] * q0[4], mS * q0[3] + S[2] * q0[4],
+                           US * (q0[5] + q0[4])};
+    const double rho = b.f[F_U][p];
+    const double n_true = ((rho < 0.0) ? 0.0 : rho) / c.M_H * c.M_ref;
+    const double fc = c.mom_hall * (n_true / sqrt(n_true * n_true + c.ne_floor * c.ne_floor));
+    const double *J = b.f[F_Jcell], *B = b.f[F_Bcell], *U = b.f[F_U];
+    const double jx = J[p], jy = J[v + p], jz = J[2 * v + p];
+    const double bx = B[p], by = B[v + p], bz = B[2 * v + p];
+    const double fx = jy * bz - jz * by, fy = jz * bx - jx * bz, fz = jx * by - jy * bx;
+    const double invJ = 1.0 / jac;
+    // the work uses calc_PV's velocities U_m / max(rho, 1e-12) (the mixed
+    // form's derived pass leaves PV_H to read-out), as one quotient
+    const double rho_pv = (rho < 1e-12) ? 1e-12 : rho;
+    const double fU = fx * U[v + p] + fy * U[2 * v + p] + fz * U[3 * v + p];
+    double *R = b.f[F_RHS];
+    R[p] = -(double(r[0]) + phi[0]) * invJ;
+    R[v + p] = -(double(r[1]) + phi[1]) * invJ + fc * fx;
+    R[2 * v + p] = -(double(r[2]) + phi[2]) * invJ + fc * fy;
+    R[3 * v + p] = -(double(r[3]) + phi[3]) * invJ + fc * fz;
+    R[4 * v + p] = -(double(r[4]) + phi[4]) * invJ + fc * (fU / rho_pv);
+}
+
 // Fluid RHS of the inner cells (FP32 flux divergence, FP64 J x B source) and
 // the FP64 contravariant velocities of the cells within one ghost layer; the
 // FP64 face metric read for the velocities is the one the fluxes round.
@@ -157,34 +191,7 @@ __device__ __forceinline__ void k_fluid_mixed_body(const BlockView *__restrict__
         for (int m = 0; m < 5; ++m)
             r[m] += Fp[m] - Fm[m];
     }
-    // divergence of the reference-state flux, FP64: Phi0(S)
-    const double US = S[0] * q0[1] + S[1] * q0[2] + S[2] * q0[3];
-    const double mS = q0[0] * US;
-    const double phi[5] = {mS, mS * q0[1] + S[0] * q0[4], mS * q0[2] + S[1] * q0[4], mS * q0[3] + S[2] * q0[4],
-                           US * (q0[5] + q0[4])};
-    // J x B force with the Hall_Num_Limiter weight, FP64
-    const double rho = b.f[F_U][p];
-    const double n_true = ((rho < 0.0) ? 0.0 : rho) / c.M_H * c.M_ref;
-    const double fc = c.mom_hall * (n_true / sqrt(n_true * n_true + c.ne_floor * c.ne_floor));
-    const double *J = b.f[F_Jcell], *B = b.f[F_Bcell], *Uc = b.f[F_U];
-    const double jx = J[p], jy = J[v + p], jz = J[2 * v + p];
-    const double bx = B[p], by = B[v + p], bz = B[2 * v + p];
-    const double fx = jy * bz - jz * by, fy = jz * bx - jx * bz, fz = jx * by - jy * bx;
-    const double invJ = 1.0 / jac;
-    double rhs[5];
-    rhs[0] = -(double(r[0]) + phi[0]) * invJ;
-    rhs[1] = -(double(r[1]) + phi[1]) * invJ + fc * fx;
-    rhs[2] = -(double(r[2]) + phi[2]) * invJ + fc * fy;
-    rhs[3] = -(double(r[3]) + phi[3]) * invJ + fc * fz;
-    // the primitive velocities of calc_PV (the mixed form's derived pass
-    // leaves PV_H to read-out): U_m / max(rho, 1e-12)
-    const double rho_pv = (rho < 1e-12) ? 1e-12 : rho;
-    const double pu = Uc[v + p] / rho_pv, pv = Uc[2 * v + p] / rho_pv, pw = Uc[3 * v + p] / rho_pv;
-    rhs[4] = -(double(r[4]) + phi[4]) * invJ + fc * (fx * pu + fy * pv + fz * pw);
-    double *R = b.f[F_RHS];
-#pragma unroll
-    for (int m = 0; m < 5; ++m)
-        R[m * v + p] = rhs[m];
+    mixed_rhs(b, c, p, jac, S, r);
 }
 
 template <int MINB>
@@ -199,11 +206,143 @@ __global__ void k_fluid_mixed_free(const BlockView *__restrict__ bvs, Consts c)
 }
 
 
-// launchers of the register / occupancy variants (tuned by mhd_autotune)
+// ---------------------------------------------------------------------------
+// Face-tiled variant: a CTA covers TILE_I x TILE_J x TILE_K cells of the
+// depth-1 box (k fastest, one warp per (i, j) row of 32 k).  Every thread
+// forms its cell's contravariant velocities as above; then each face flux
+// needed by an inner cell is evaluated once -- a cell's three low faces by its
+// own thread, the high faces of the tile's last layer in each direction by the
+// threads of that layer -- into shared memory, and after one barrier each
+// inner cell sums its six faces.  The two cells of a face call rusanov_dev32
+// with the same arguments (face metric and area of the face, the two cells'
+// states), so the fluxes and the RHS are bit for bit those of the per-cell
+// variant (the file is compiled without contracted multiply-adds).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256, 2) k_fluid_mixed_tile(const BlockView *__restrict__ bvs, Consts c)
+{
+    __shared__ float Fx[TILE_I + 1][TILE_J][TILE_K][5];
+    __shared__ float Fy[TILE_I][TILE_J + 1][TILE_K][5];
+    __shared__ float Fz[TILE_I][TILE_J][TILE_K + 1][5];
+    int64_t t;
+    const BlockView &b = bvs[cta_block(bvs, KIND_TILE1, t)];
+    const int ntj = (b.nj + 2 + TILE_J - 1) / TILE_J, ntk = (b.nk + 2 + TILE_K - 1) / TILE_K;
+    const int64_t tile = t / 256;
+    if (tile >= int64_t((b.ni + 2 + TILE_I - 1) / TILE_I) * ntj * ntk)
+        return; // the whole CTA
+    const int tk = threadIdx.x & 31, tj = (threadIdx.x >> 5) % TILE_J, ti = (threadIdx.x >> 5) / TILE_J;
+    const int i = -1 + int(tile / (int64_t(ntj) * ntk)) * TILE_I + ti;
+    const int j = -1 + int((tile / ntk) % ntj) * TILE_J + tj;
+    const int k = -1 + int(tile % ntk) * TILE_K + tk;
+    const bool valid = i <= b.ni && j <= b.nj && k <= b.nk;
+    const bool inner = i >= 0 && j >= 0 && k >= 0 && i < b.ni && j < b.nj && k < b.nk;
+    const int64_t v = b.vol;
+    const int64_t p = pidx(b, i, j, k);
+    const int64_t pp[3] = {pidx(b, i + 1, j, k), pidx(b, i, j + 1, k), pidx(b, i, j, k + 1)};
+    const int64_t pm[3] = {pidx(b, i - 1, j, k), pidx(b, i, j - 1, k), pidx(b, i, j, k - 1)};
+    float km[3][3], kp[3][3];
+    double S[3] = {0.0, 0.0, 0.0};
+    double jac = 0.0;
+    if (valid)
+    {
+        jac = b.f[F_Jac][p];
+        const double *Up = b.f[F_Uplus];
+        const double ux = Up[p], uy = Up[v + p], uz = Up[2 * v + p];
+        const double inv_jac = 1.0 / (fabs(jac) + 1.0e-30);
+        double *UC = b.f[F_UC];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+        {
+            const double *M = b.f[F_JDxi + a];
+            double m_[3], p_[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+            {
+                m_[d] = M[d * v + p];
+                p_[d] = M[d * v + pp[a]];
+                km[a][d] = float(m_[d]);
+                kp[a][d] = float(p_[d]);
+                S[d] += p_[d] - m_[d];
+            }
+            const double kx = 0.5 * (m_[0] + p_[0]);
+            const double ky = 0.5 * (m_[1] + p_[1]);
+            const double kz = 0.5 * (m_[2] + p_[2]);
+            UC[a * v + p] = (kx * ux + ky * uy + kz * uz) * inv_jac;
+        }
+    }
+    const double *q0 = b.qref;
+    const Ref32 r0 = {float(q0[0]), {float(q0[1]), float(q0[2]), float(q0[3])}, float(q0[5] + q0[4])};
+    const float *g = b.g32;
+    // the low face of axis a of this cell joins cells -1 and 0 along a: needed
+    // by an inner cell when the cell's own index along a is in [0, n_a] and
+    // the other two are inner
+    const int idx[3] = {i, j, k}, n[3] = {b.ni, b.nj, b.nk};
+    const int last[3] = {ti == TILE_I - 1, tj == TILE_J - 1, tk == TILE_K - 1};
+    if (valid)
+    {
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+        {
+            bool others = true;
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                if (d != a && (idx[d] < 0 || idx[d] >= n[d]))
+                    others = false;
+            if (!others)
+                continue;
+            float F[5];
+            if (idx[a] >= 0 && idx[a] <= n[a])
+            {
+                rusanov_dev32(b, r0, km[a][0], km[a][1], km[a][2], g[(G32_AREA + a) * v + p], p, pm[a], F);
+                float *dst = a == 0 ? Fx[ti][tj][tk] : a == 1 ? Fy[ti][tj][tk] : Fz[ti][tj][tk];
+#pragma unroll
+                for (int m = 0; m < 5; ++m)
+                    dst[m] = F[m];
+            }
+            // the high face of the tile's last layer (the next tile's low face)
+            if (last[a] && idx[a] + 1 >= 0 && idx[a] + 1 <= n[a])
+            {
+                rusanov_dev32(b, r0, kp[a][0], kp[a][1], kp[a][2], g[(G32_AREA + a) * v + pp[a]], pp[a], p, F);
+                float *dst = a == 0 ? Fx[TILE_I][tj][tk] : a == 1 ? Fy[ti][TILE_J][tk] : Fz[ti][tj][TILE_K];
+#pragma unroll
+                for (int m = 0; m < 5; ++m)
+                    dst[m] = F[m];
+            }
+        }
+    }
+    __syncthreads();
+    if (!inner)
+        return;
+    float r[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    {
+        const float *Fm = Fx[ti][tj][tk], *Fp = Fx[ti + 1][tj][tk];
+#pragma unroll
+        for (int m = 0; m < 5; ++m)
+            r[m] += Fp[m] - Fm[m];
+    }
+    {
+        const float *Fm = Fy[ti][tj][tk], *Fp = Fy[ti][tj + 1][tk];
+#pragma unroll
+        for (int m = 0; m < 5; ++m)
+            r[m] += Fp[m] - Fm[m];
+    }
+    {
+        const float *Fm = Fz[ti][tj][tk], *Fp = Fz[ti][tj][tk + 1];
+#pragma unroll
+        for (int m = 0; m < 5; ++m)
+            r[m] += Fp[m] - Fm[m];
+    }
+    mixed_rhs(b, c, p, jac, S, r);
+}
+
+// launchers of the register / occupancy variants (tuned by mhd_autotune);
+// variant 3 is the face-tiled kernel (KIND_TILE1 grid)
 int launch_k_fluid_mixed(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c)
 {
     switch (variant)
     {
+    case 3:
+        k_fluid_mixed_tile<<<grid, 256, 0, st>>>(bvs, c);
+        break;
     case 0:
         k_fluid_mixed_t<2><<<grid, 256, 0, st>>>(bvs, c);
         break;

@@ -142,19 +142,22 @@ struct BlockView
     // flattened launches over blocks of uneven sizes: per launch kind the
     // block of every CTA (same table in every view; null = 2-D launches with
     // one grid row per block) and this block's first CTA
-    const int *cta_blk[3];
-    int cta0[3];
+    const int *cta_blk[4];
+    int cta0[4];
 };
 
 // launch kinds of the flattened grids: cells with depth 0, cells with depth
-// 1, and the staggered box [0, n + 1)^3 of the face / edge kernels
+// 1, the staggered box [0, n + 1)^3 of the face / edge kernels, and tiles of
+// TILE_I x TILE_J x TILE_K cells over the depth-1 box (one CTA each)
 enum : int
 {
     KIND_CELL0 = 0,
     KIND_CELL1 = 1,
     KIND_STAG = 2,
-    NKIND = 3
+    KIND_TILE1 = 3,
+    NKIND = 4
 };
+constexpr int TILE_I = 2, TILE_J = 4, TILE_K = 32; // TILE_I * TILE_J * TILE_K = 256 threads
 
 #ifdef __CUDACC__
 // Block and thread-in-block of the calling thread: flattened launches (one

@@ -26,6 +26,12 @@ NOALLOC_MAX_DOUBLES = 1 << 21
 PREC_FP64 = 0
 PREC_MIXED = 1
 
+# the default variant of each tunable kernel, in the values mhd_autotune
+# reports (minimum CTAs per SM of its launch bounds, 0: none; 12: the
+# face-tiled k_fluid_mixed)
+DEFAULT_TUNE = {"k_pv_uplus_dt": 4, "k_fluid_ucontra": 0, "k_bcell_jedge": 0, "k_eface": 0, "k_curl_e2f": 0,
+                "k_eedge": 0, "k_fluid_mixed": 2}
+
 STAGE_TIMESTEP, STAGE_FLUID_RHS, STAGE_INDUCTION, STAGE_UPDATE, STAGE_DIVB, STAGE_HALL_EMF = 1, 2, 3, 4, 5, 6
 STAGE_HALL_SOLVE = 7
 
@@ -54,6 +60,7 @@ _SIGS = {
     "mhd_set_flux_reference_run": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
     "mhd_autotune": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.c_int32]),
     "mhd_tune_name": (C.c_char_p, [C.c_int32]),
+    "mhd_set_tune": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.c_int32]),
     "mhd_ctx_destroy": (C.c_int, [C.c_void_p]),
     "mhd_last_error": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),
     "mhd_field_info": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
@@ -337,6 +344,14 @@ class Context:
         out = (C.c_int32 * n)()
         self._check(self.lib.mhd_autotune(self.h, int(reps), out, n), "autotune")
         return {self.lib.mhd_tune_name(i).decode(): int(out[i]) for i in range(n)}
+
+    def set_tune(self, chosen: Dict[str, int]):
+        """applies a variant choice in autotune()'s values (kernel -> value);
+        kernels not named get their default variant (DEFAULT_TUNE)"""
+        n = len(DEFAULT_TUNE)
+        names = [self.lib.mhd_tune_name(i).decode() for i in range(n)]
+        vals = (C.c_int32 * n)(*[int(chosen.get(nm, DEFAULT_TUNE[nm])) for nm in names])
+        self._check(self.lib.mhd_set_tune(self.h, vals, n), "set_tune")
 
     def batch_step(self, nsteps: int):
         """nsteps steps of every run; returns (dt of every run, time of every run)"""

@@ -305,10 +305,18 @@ int mhd_set_flux_reference_run(mhd_ctx *ctx, int32_t run, const double prim[5]);
    call does not advance the simulation.  Call it after the state is loaded.
    min_ctas[i] (i < n, at most MHD_NTUNE) receives the chosen minimum CTAs
    per SM of kernel mhd_tune_name(i) (0: no launch bounds, the compiler's own
-   register allocation). */
+   register allocation; 12: the face-tiled k_fluid_mixed). */
 #define MHD_NTUNE 7
 int mhd_autotune(mhd_ctx *ctx, int32_t reps, int32_t *min_ctas, int32_t n);
 const char *mhd_tune_name(int32_t i);
+
+/* Applies a variant choice (no counterpart in the reference): min_ctas[i]
+   (i < n) in the values mhd_autotune reports, e.g. one it returned in an
+   earlier run.  For k_fluid_mixed the value 12 selects the face-tiled kernel
+   (each face flux evaluated once per 2 x 4 x 32-cell tile and shared
+   through shared memory; the same bits as the per-cell variants).
+   MHD_EINVAL for a value that names no variant. */
+int mhd_set_tune(mhd_ctx *ctx, const int32_t *min_ctas, int32_t n);
 
 /* Iterations, final residual norm, ||b|| and convergence reason (2 rtol,
    3 atol, -3 iteration limit, as KSPConvergedReason) of the last solve. */

@@ -77,3 +77,52 @@ def test_tuning_leaves_the_implicit_hall_start_untouched():
         s.ctx.close()
     for key in out[0]:
         assert np.array_equal(out[0][key], out[1][key]), key
+
+
+@pytest.mark.parametrize("variant", [12, 0, 3])
+def test_flux_variants_give_the_same_bits(variant):
+    """The mixed flux pass in each of its variants -- the face-tiled kernel
+    (12: every face flux evaluated once per tile, shared through shared
+    memory) and the per-cell kernel under other launch bounds -- against the
+    default per-cell variant, bit for bit, on a batch of uneven shells and a
+    slab (tiles cut the blocks at every alignment)."""
+    from beta1_b200 import case
+    from conftest import shell_setup
+    g = load_golden("shell_8x6x8_steps.npz")
+    spec0, st0 = shell_setup(g)
+    spec1 = case.shell_case(10, 8, 12, mach_u=6.0)
+    st1 = case.inflow_state(spec1, seed=77)
+    runs = [(spec0, "shell", st0), (spec1, "shell", st1)]
+    out = []
+    for v in (2, variant):
+        bt = solver.Batch([(sp, topo) for sp, topo, _ in runs], precision=mhd.PREC_MIXED)
+        bt.ctx.set_tune({"k_fluid_mixed": v})
+        bt.load_states([st for _, _, st in runs])
+        bt.step(3)
+        out.append({(r, f): bt.field(r, f) for r in range(2) for f in STATE + ["RHS_H", "B_cell", "J_cell"]})
+        bt.ctx.close()
+    for key in out[0]:
+        assert np.array_equal(out[0][key], out[1][key]), (variant, key)
+    gs = load_golden("slab_6x5x6_t2x2_r00_steps.npz")
+    spec, st = slab_setup(gs)
+    res = []
+    for v in (2, variant):
+        s = solver.Solver(spec, topology="tiled", precision=mhd.PREC_MIXED)
+        s.ctx.set_tune({"k_fluid_mixed": v})
+        s.load_state(st)
+        s.step(2)
+        res.append({(f, b): s.field(f, b) for f in STATE + ["RHS_H"] for b in range(len(spec.blocks))})
+        s.ctx.close()
+    for key in res[0]:
+        assert np.array_equal(res[0][key], res[1][key]), (variant, key)
+
+
+def test_set_tune_rejects_unknown_variants(golden_periodic):
+    from conftest import periodic_setup
+    spec, st = periodic_setup(golden_periodic["steps"])
+    s = solver.Solver(spec)
+    try:
+        with pytest.raises(mhd.MHDError, match="EINVAL"):
+            s.ctx.set_tune({"k_fluid_mixed": 7})
+    finally:
+        s.ctx.close()
