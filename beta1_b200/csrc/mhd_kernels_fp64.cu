@@ -817,6 +817,18 @@ template <> __device__ __forceinline__ const float *weights<float>(const BlockVi
     return b.w32 + int64_t(plane32) * b.vol;
 }
 
+// plane q of axis a's face data: q = 0 the area, 1..3 the unit normal (the
+// FP64 field Anorm_*, or its FP32 copies)
+template <typename WT> __device__ __forceinline__ const WT *face_planes(const BlockView &b, int a, int q);
+template <> __device__ __forceinline__ const double *face_planes<double>(const BlockView &b, int a, int q)
+{
+    return b.f[F_NAxi + a] + int64_t(q) * b.vol;
+}
+template <> __device__ __forceinline__ const float *face_planes<float>(const BlockView &b, int a, int q)
+{
+    return b.g32 + int64_t(q == 0 ? G32_AREA + a : G32_NRM + 3 * a + q - 1) * b.vol;
+}
+
 // ---------------------------------------------------------------------------
 // calc_Bcell (Z4_Lunar/src/physics/LunarSolver_Tools.cpp:163-241)
 // ---------------------------------------------------------------------------
@@ -998,15 +1010,19 @@ __global__ void k_jcell(const BlockView *__restrict__ bvs)
 // ---------------------------------------------------------------------------
 
 // one face of the CFL bound: (|u . n| + c_f) A with n the outward unit
-// normal (A and JD / A precomputed per face, k_face_normals)
-__device__ __forceinline__ double cfl_face_term(const double *N, int64_t v, int64_t p, bool outward_plus, double ux,
-                                                double uy, double uz, double Bx, double By, double Bz, double B2,
-                                                double rho, double cs2, double inver_MA2)
+// normal (A and JD / A precomputed per face, k_face_normals); the face's area
+// and normal planes as FP64 (the reference's values) or as their FP32 copies
+// (the mixed form)
+template <typename T>
+__device__ __forceinline__ double cfl_face_term(const T *Ap, const T *N0, const T *N1, const T *N2, int64_t p,
+                                                bool outward_plus, double ux, double uy, double uz, double Bx,
+                                                double By, double Bz, double B2, double rho, double cs2,
+                                                double inver_MA2)
 {
-    const double A = N[p];
+    const double A = double(Ap[p]);
     if (A <= 0.0)
         return 0.0;
-    double nx = N[v + p], ny = N[2 * v + p], nz = N[3 * v + p];
+    double nx = double(N0[p]), ny = double(N1[p]), nz = double(N2[p]);
     if (!outward_plus)
     {
         nx = -nx;
@@ -1125,15 +1141,23 @@ __device__ __forceinline__ void k_pv_uplus_dt_body(const BlockView *__restrict__
                 const double *Bc = b.f[F_Bcell];
                 const double Bx = Bc[p], By = Bc[v + p], Bz = Bc[2 * v + p];
                 const double B2 = Bx * Bx + By * By + Bz * Bz;
-                const double *X = b.f[F_NAxi], *Y = b.f[F_NAeta], *Z = b.f[F_NAzeta];
-                const int64_t pi1 = pidx(b, i + 1, j, k), pj1 = pidx(b, i, j + 1, k), pk1 = pidx(b, i, j, k + 1);
+                // the mixed form reads the FP32 copies of the face areas and normals
+                const WT *P[3][4];
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        P[a][q] = face_planes<WT>(b, a, q);
+                const int64_t pa1[3] = {pidx(b, i + 1, j, k), pidx(b, i, j + 1, k), pidx(b, i, j, k + 1)};
                 double denom = 0.0;
-                denom += cfl_face_term(X, v, p, false, ux, uy, uz, Bx, By, Bz, B2, rho, cs2, c.inver_MA2);
-                denom += cfl_face_term(X, v, pi1, true, ux, uy, uz, Bx, By, Bz, B2, rho, cs2, c.inver_MA2);
-                denom += cfl_face_term(Y, v, p, false, ux, uy, uz, Bx, By, Bz, B2, rho, cs2, c.inver_MA2);
-                denom += cfl_face_term(Y, v, pj1, true, ux, uy, uz, Bx, By, Bz, B2, rho, cs2, c.inver_MA2);
-                denom += cfl_face_term(Z, v, p, false, ux, uy, uz, Bx, By, Bz, B2, rho, cs2, c.inver_MA2);
-                denom += cfl_face_term(Z, v, pk1, true, ux, uy, uz, Bx, By, Bz, B2, rho, cs2, c.inver_MA2);
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                {
+                    denom += cfl_face_term(P[a][0], P[a][1], P[a][2], P[a][3], p, false, ux, uy, uz, Bx, By, Bz, B2,
+                                           rho, cs2, c.inver_MA2);
+                    denom += cfl_face_term(P[a][0], P[a][1], P[a][2], P[a][3], pa1[a], true, ux, uy, uz, Bx, By, Bz,
+                                           B2, rho, cs2, c.inver_MA2);
+                }
                 // cells with denom <= 0 (or NaN) do not bound dt, as in the reference
                 if (denom > 0.0)
                     dtc = c.cfl * V / denom;

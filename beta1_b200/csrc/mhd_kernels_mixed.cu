@@ -21,8 +21,8 @@ namespace mhd
 
 __device__ __forceinline__ float fmaxs(float a, float b) { return (a < b) ? b : a; }
 
-// FP32 copies of the face areas |JD| and of the B_cell / J_cell
-// least-squares weights on every point of the padded box
+// FP32 copies of the face areas |JD|, the unit face normals and the
+// B_cell / J_cell least-squares weights on every point of the padded box
 __global__ void k_geom32(const BlockView *__restrict__ bvs)
 {
     const BlockView &b = bvs[blockIdx.y];
@@ -32,7 +32,12 @@ __global__ void k_geom32(const BlockView *__restrict__ bvs)
         return;
 #pragma unroll
     for (int a = 0; a < 3; ++a)
+    {
         b.g32[(G32_AREA + a) * v + p] = float(b.f[F_NAxi + a][p]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            b.g32[(G32_NRM + 3 * a + c) * v + p] = float(b.f[F_NAxi + a][(1 + c) * v + p]);
+    }
     for (int q = 0; q < 18; ++q)
         b.w32[(W32_B + q) * v + p] = float(b.f[F_WB][q * v + p]);
     for (int q = 0; q < 36; ++q)

@@ -129,7 +129,7 @@ struct BlockView
     int NJ, NK;       // padded extents (j, k)
     int64_t vol;      // doubles per component plane
     // mixed precision only (null otherwise): FP32 planes on the same padded box
-    float *g32;       // face area xi, eta, zeta
+    float *g32;       // face area xi, eta, zeta, then their unit normals
     float *q32;       // face-state quantities rho, u, v, w, p, rhoE, c
     float *w32;       // least-squares weights: Bcell_from_Bface_w (18 planes), Jcell_from_Jedge_w (36)
     // SSP-RK2 only (null otherwise): the state at the step's start, U_H 5
@@ -179,8 +179,9 @@ __device__ __forceinline__ int cta_block(const BlockView *bvs, int kind, int64_t
 // plane indices of BlockView::g32 / q32
 enum : int
 {
-    G32_AREA = 0,
-    G32_N = 3,
+    G32_AREA = 0, // face area of axis a: plane a
+    G32_NRM = 3,  // unit normal of axis a, component c: plane 3 + 3 a + c
+    G32_N = 12,
     Q32_RHO = 0,
     Q32_U = 1,
     Q32_P = 4,
