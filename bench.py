@@ -106,11 +106,12 @@ FLUX_CT_BYTES = {False: 280, True: 216}
 WHOLE_GRID_KERNELS = {"k_pv_uplus_dt", "k_fluid_ucontra", "k_fluid_mixed", "k_bcell_jedge", "k_eface", "k_eedge",
                       "k_update_u", "k_hall_cell", "k_hall_edge", "k_bcell", "k_jedge"}
 # The mixed form's kernels where they differ: the PV pass reads the 36 J_cell
-# weights as FP32 copies and writes U_plus 3, J_cell 3 and the 7 FP32 face
-# states (PV_H and the FP64 face states are left to read-out): U 5, Jac 1,
-# B_cell 3, face area + normal 12, J 3 read as FP64 plus 36 FP32 weights;
-# 6 FP64 and 7 FP32 written.  The B_cell passes read their 18 weights as FP32.
-ALGO_BYTES_MIXED = {"k_pv_uplus_dt": 24 * 8 + 36 * 4 + 6 * 8 + 7 * 4,
+# weights and the face areas + normals (12) as FP32 copies and writes U_plus
+# 3, J_cell 3 and the 7 FP32 face states (PV_H and the FP64 face states are
+# left to read-out): U 5, Jac 1, B_cell 3, J 3 read as FP64 plus 48 FP32
+# values; 6 FP64 and 7 FP32 written.  The B_cell passes read their 18 weights
+# as FP32.
+ALGO_BYTES_MIXED = {"k_pv_uplus_dt": 12 * 8 + 48 * 4 + 6 * 8 + 7 * 4,
                     "k_bcell": 12 * 8 + 18 * 4,
                     "k_bcell_jedge": 21 * 8 + 18 * 4}
 
