@@ -457,6 +457,8 @@ def main():
     ap.add_argument("--e2e-iters", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep every kernel's default variant")
+    ap.add_argument("--tune", default=None,
+                    help="kernel=value,... variants applied with mhd_set_tune instead of autotuning (profiling)")
     ap.add_argument("--geometry", default=None, choices=["host", "device"],
                     help="geometry fields built on the host and uploaded, or built on the device from the node "
                          "meshes (mhd_build_geometry); same values (default: device for the sweeps, host otherwise)")
@@ -527,7 +529,11 @@ def main():
             c.set_integrator(mhd.INTEGRATOR_SSPRK2)
     setup_s = time.time() - t_setup
     # register / occupancy variant of each hot kernel, timed on this state
-    tuned = ctx.autotune(reps=10) if not args.no_autotune else None
+    if args.tune:
+        tuned = {kv.split("=")[0]: int(kv.split("=")[1]) for kv in args.tune.split(",")}
+        ctx.set_tune(tuned)
+    else:
+        tuned = ctx.autotune(reps=10) if not args.no_autotune else None
     stream = torch.cuda.ExternalStream(ctx.stream())
     ctx_bytes = sum(ctx.field_info(f, b)["ncomp"] * int(np.prod([h - l for l, h in zip(
         ctx.field_info(f, b)["lo"], ctx.field_info(f, b)["hi"])])) * 8 for f in ("U_H", "PV_H", "JDxi", "JDet",
@@ -541,7 +547,7 @@ def main():
     fp64_line = None
     if fp64_cmp is not None:
         ctx64 = fp64_cmp.ctx
-        tuned64 = ctx64.autotune(reps=10) if not args.no_autotune else None
+        tuned64 = ctx64.autotune(reps=10) if not (args.no_autotune or args.tune) else None
         ms64, _, clocks64 = timed_steps(ctx64, args.steps, args.warmup, world, local,
                                         torch.cuda.ExternalStream(ctx64.stream()))
         ms64 = max_over_ranks(ms64, "cuda")
