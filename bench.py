@@ -171,13 +171,14 @@ WORKLOADS = {
     "c1": dict(name="c1_periodic_64cubed_fp64", ref_steps=40, ref_rss_gb=1.0),
     "c5": dict(name="c5_sweep48_slab_runs_mixed", ref_steps=2, ref_rss_gb=4.0),
     "c5s": dict(name="c5s_sweep48_shell_runs_mixed", ref_steps=2, ref_rss_gb=4.0),
-    "c3": dict(name="c3_slab6x128x64x64_hall_implicit_fp64", ref_steps=1, ref_rss_gb=4.0),
-    "c4": dict(name="c4_slab6x128x64x64_hall_implicit_mixed", ref_steps=1, ref_rss_gb=4.0),
+    "c3": dict(name="c3_slab6x128x64x64_hall_implicit_fp64", ref_steps=1, ref_rss_gb=28.0),
+    "c4": dict(name="c4_slab6x128x64x64_hall_implicit_mixed", ref_steps=1, ref_rss_gb=28.0),
 }
 SWEEP_RUNS = 48
 SWEEP_GRID = {"c5": ("slab", "tiled"), "c5s": ("shell", "shell")}  # sweep workload -> (grid, topology)
-HALL_SAMPLE = ("6 blocks of 64 x 32 x 32 cells (the same layout at half the cells per direction), StepOnce "
-               "followed by the reference's implicit Hall solve (SolveOneStep, Newton rtol 1e-10) and calc_Bcell")
+HALL_SAMPLE = ("the full workload (6 blocks of 128 x 64 x 64 cells), StepOnce as compiled with the implicit Hall "
+               "solve (SolveOneStep at the step's dt, Newton rtol 1e-10, then calc_Bcell, before the closing syncs "
+               "and derived fields)")
 
 
 
@@ -242,14 +243,10 @@ def cpu_reference(workload, n, steps, nproc, integrator="euler"):
         return None
     nproc = max(1, min(nproc, int(0.6 * mem_available_gb() / WORKLOADS[workload]["ref_rss_gb"])))
     command = "timerk2" if integrator == "rk2" else "time"
+    spec, st, _, _ = build_case(workload, n)
     if workload in ("c3", "c4"):
-        # bounded sample: the same layout at half the cells per direction,
-        # the step with the implicit Hall solve
-        spec = case.slab_case(64, (32, 32), (3, 2))
-        st = case.inflow_state(spec)
+        # the step with the implicit Hall solve, at the workload's full size
         command = "timehall"
-    else:
-        spec, st, _, _ = build_case(workload, n)
     d = tempfile.mkdtemp(prefix="b1ref_")
     try:
         case.write_case(d, spec)

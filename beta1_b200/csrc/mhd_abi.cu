@@ -113,9 +113,11 @@ const char *const kKernelNames[] = {
     "k_cycle_start",  "k_gmres_column", "k_inner_check", "k_gmres_solve_y", "k_add_basis",    "k_outer_check",
     "k_zero",         "k_residual",    "k_ucontra",      "k_face_normals", "k_divb",          "k_eres_explicit",
     "k_bcell_jedge",  "k_fluid_ucontra", "k_wall_u_all",   "k_hall_cell",    "k_hall_edge",
-    "k_pack_vec",     "k_hall_residual", "k_axpy_to",      "k_fd_quotient",  "k_negate",
-    "k_geom32",       "k_fluid_mixed",  "k_gmres_resist", "k_pole",
-    "k_geometry",     "k_diag_init",   "k_diag",        "k_rk2"};
+    "k_pack_vec",     "k_geom32",       "k_fluid_mixed",  "k_gmres_resist", "k_pole",
+    "k_geometry",     "k_diag_init",   "k_diag",        "k_rk2",          "k_hall_begin",    "k_hall_step_begin",
+    "k_hall_gmres_init", "k_hall_cycle_prep", "k_hall_ls_begin", "k_hall_ls_check", "k_hall_accept", "k_hall_column",
+    "k_hall_trial",   "k_hall_jv_dots", "k_hall_proj_dots", "k_hall_next",  "k_hall_res_dots", "k_hall_restart_r",
+    "k_hall_gmres_prologue", "k_norm2", "k_hall_take",    "k_copy_segments"};
 constexpr int kNumKernelNames = int(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
 
 } // namespace
@@ -141,6 +143,17 @@ const char *const kTuneNames[NTUNE] = {"k_pv_uplus_dt", "k_fluid_ucontra", "k_bc
 const int kTuneMinCtas[NTUNE][4] = {{4, 0, 5, 0}, {0, 3, 0, 0}, {0, 6, 0, 0}, {0, 6, 0, 0},
                                     {0, 6, 0, 0}, {0, 8, 0, 0}, {2, 0, 3, 12}};
 const int kTuneCount[NTUNE] = {3, 2, 2, 2, 2, 2, 4};
+
+// loop bodies of the device-steered implicit Hall solve
+enum
+{
+    HALL_KB_NEWTON,
+    HALL_KB_CYCLE,
+    HALL_KB_INNER,
+    HALL_KB_RESTART,
+    HALL_KB_LS,
+    HALL_KB_N
+};
 
 struct mhd_ctx
 {
@@ -255,13 +268,20 @@ struct mhd_ctx
         int maxit = 50;
         double ksp_rtol = 1e-5;                    // linear solves (PETSc KSP default)
         int ksp_maxit = 10000, restart = 30;
-        double *bstar = nullptr;                   // snapshot of the face B arrays
+        double *bstar = nullptr;                   // snapshot of the face B arrays (one range per block)
+        int64_t *seg_snap = nullptr, *seg_restore = nullptr; // per block: dst offset, src offset, length
+        int copy_ctas = 1;
         double *X = nullptr, *F = nullptr, *Xt = nullptr, *Ft = nullptr, *dx = nullptr, *b = nullptr, *r = nullptr;
         double *V = nullptr, *w = nullptr, *partial = nullptr, *dots = nullptr;
+        unsigned *done = nullptr;                  // CTAs finished in a reduction pass
         GmresState *st = nullptr;
+        HallCtl *ctl = nullptr;                    // Newton / line-search control and statistics
         int ngroups = 1;
-        int its = 0, lin_its = 0, reason = 0;      // statistics of the last solve
-        double fnorm = 0.0, fnorm0 = 0.0;
+        // launch accounting: kernels per pass of each loop body (captured),
+        // passes run eagerly
+        int64_t kb[HALL_KB_N] = {0, 0, 0, 0, 0};
+        int64_t kb_nested = 0;                     // kernels of one captured Newton pass, nested bodies included
+        long long eager[HALL_KB_N] = {0, 0, 0, 0, 0};
     } hall;
     // Hall edge EMF: coefficient and zero boxes (block, axis, lo[3], hi[3])
     double hall_coef = 0.0;
@@ -273,7 +293,7 @@ struct mhd_ctx
     // explicit resistive sub-cycles (ResistiveDiffusionSubcycles_): 0 = off
     int res_nsub = 0;
     double res_inver_Rem = 0.0;
-    cudaStream_t spare[2] = {nullptr, nullptr}; // capture streams of conditional bodies
+    cudaStream_t spare[4] = {nullptr, nullptr, nullptr, nullptr}; // capture streams of conditional bodies
     int spare_depth = 0;
 
     // register / occupancy variant of each tunable kernel (mhd_autotune)
@@ -895,13 +915,6 @@ int gmres_cycle_end(mhd_ctx *ctx, cudaGraphConditionalHandle h, int use)
     return MHD_OK;
 }
 
-int read_scalar(mhd_ctx *ctx, const double *dev, double *host)
-{
-    CK(ctx, cudaMemcpyAsync(host, dev, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(ctx, cudaStreamSynchronize(ctx->stream));
-    return MHD_OK;
-}
-
 int read_flag(mhd_ctx *ctx, const int *dev, int *host)
 {
     CK(ctx, cudaMemcpyAsync(host, dev, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -941,13 +954,14 @@ int capture_graph_of(mhd_ctx *ctx, cudaGraph_t *g)
     return MHD_OK;
 }
 
-// Appends a conditional while node (handle h) at the capture position of
-// ctx->stream and captures body(ctx, h) into it on a spare stream; *kernels
-// receives the kernels one pass of the body launches.
-int capture_while(mhd_ctx *ctx, cudaGraphConditionalHandle h, int (*body)(mhd_ctx *, cudaGraphConditionalHandle),
-                  int64_t *kernels)
+// Appends a conditional node of the given type (while or if; handle h) at
+// the capture position of ctx->stream and captures body(ctx, h) into it on a
+// spare stream; *kernels receives the kernels one pass of the body launches
+// (the bodies nested in it included).
+int capture_cond(mhd_ctx *ctx, cudaGraphConditionalNodeType type, cudaGraphConditionalHandle h,
+                 int (*body)(mhd_ctx *, cudaGraphConditionalHandle), int64_t *kernels)
 {
-    if (ctx->spare_depth >= 2)
+    if (ctx->spare_depth >= int(sizeof ctx->spare / sizeof ctx->spare[0]))
         return fail(ctx, MHD_ESTATE, "conditional nodes nested too deep");
     cudaStreamCaptureStatus st;
     cudaGraph_t g = nullptr;
@@ -956,7 +970,7 @@ int capture_while(mhd_ctx *ctx, cudaGraphConditionalHandle h, int (*body)(mhd_ct
     CK(ctx, cudaStreamGetCaptureInfo(ctx->stream, &st, nullptr, &g, &deps, &ndeps));
     cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
     p.conditional.handle = h;
-    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.type = type;
     p.conditional.size = 1;
     cudaGraphNode_t node;
     CK(ctx, cudaGraphAddNode(&node, g, deps, ndeps, &p));
@@ -981,6 +995,12 @@ int capture_while(mhd_ctx *ctx, cudaGraphConditionalHandle h, int (*body)(mhd_ct
     if (e != cudaSuccess)
         return fail(ctx, MHD_ECUDA, "conditional body capture failed: %s", cudaGetErrorString(e));
     return MHD_OK;
+}
+
+int capture_while(mhd_ctx *ctx, cudaGraphConditionalHandle h, int (*body)(mhd_ctx *, cudaGraphConditionalHandle),
+                  int64_t *kernels)
+{
+    return capture_cond(ctx, cudaGraphCondTypeWhile, h, body, kernels);
 }
 
 int gmres_step_graph(mhd_ctx *ctx, cudaGraphConditionalHandle h) { return gmres_step(ctx, h, 1); }
@@ -1171,42 +1191,90 @@ int launch_resistive_explicit(mhd_ctx *ctx)
 // Hall_Implicit_Formfunction.cpp:7-106).  Newton with a backtracking line
 // search; each Newton system J dx = -F solved by restarted GMRES whose
 // products J v are finite differences of F (the reference uses an
-// approximate whistler Jacobian; both converge to the root of F).  Driven
-// from the host: one scalar read per Krylov iteration.
+// approximate whistler Jacobian; both converge to the root of F).
+//
+// Steered on the device: the control state (HallCtl, GmresState) lives in
+// device memory and one-thread kernels take every decision.  Inside the
+// step graph the four loops (Newton steps, GMRES cycles, Arnoldi steps,
+// line-search trials) and the restart product are conditional nodes whose
+// handles those kernels set, so a step runs with no host round trip; run
+// eagerly (a stage, or where conditional nodes cannot be built) the host
+// reads the same kernels' mirror flags.  Every loop is bounded: Newton by
+// maxit, GMRES by its iteration limit, the line search by 12 trials.
 // ---------------------------------------------------------------------------
 
-// B <- B* (restore) or B* <- B (snapshot), the whole face B arrays
-int hall_snapshot(mhd_ctx *ctx, bool restore)
+int hall_use(const mhd_ctx *ctx) { return ctx->capturing ? 1 : 0; }
+
+// a conditional handle of the graph being captured (0 when eager)
+int new_handle(mhd_ctx *ctx, cudaGraphConditionalHandle *h)
 {
-    auto &H = ctx->hall;
-    size_t off = 0;
-    for (int f = F_Bxi; f <= F_Bzeta; ++f)
-        for (int b = 0; b < ctx->nblocks; ++b)
-        {
-            const size_t n = size_t(ctx->hbv[size_t(b)].vol);
-            double *field = ctx->pool + ctx->base[size_t(f)][size_t(b)];
-            if (restore)
-                CK(ctx, cudaMemcpyAsync(field, H.bstar + off, n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
-            else
-                CK(ctx, cudaMemcpyAsync(H.bstar + off, field, n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
-            off += n;
-        }
+    *h = 0;
+    if (!ctx->capturing)
+        return MHD_OK;
+    cudaGraph_t g = nullptr;
+    RUN(capture_graph_of(ctx, &g));
+    CK(ctx, cudaGraphConditionalHandleCreate(h, g, 0, 0));
     return MHD_OK;
 }
 
+// A loop (while) or branch (if) of the solve: captured as a conditional node
+// whose body the device steers through h, or run eagerly with the host
+// reading the flag the same kernels write.  *kernels receives the kernels
+// of one captured pass; *eager counts the passes run eagerly.
+int hall_cond(mhd_ctx *ctx, cudaGraphConditionalNodeType type, cudaGraphConditionalHandle h, const int *flag,
+              int (*body)(mhd_ctx *, cudaGraphConditionalHandle), int64_t *kernels, long long *eager)
+{
+    if (ctx->capturing)
+        return capture_cond(ctx, type, h, body, kernels);
+    int go = 0;
+    RUN(read_flag(ctx, flag, &go));
+    while (go)
+    {
+        RUN(body(ctx, 0));
+        *eager += 1;
+        if (type == cudaGraphCondTypeIf)
+            break;
+        RUN(read_flag(ctx, flag, &go));
+    }
+    return MHD_OK;
+}
+
+// one pass of a vector reduction kernel over the solve's unknowns
+#define HALL_RED(name, ...)                                                  \
+    do                                                                       \
+    {                                                                        \
+        prof_begin(ctx, #name);                                              \
+        name<<<ctx->hall.ngroups, 256, 0, ctx->stream>>>(__VA_ARGS__);       \
+        RUN(launched(ctx));                                                  \
+    } while (0)
+
+// B <- B* (snapshot = false) or B* <- B (snapshot = true): the face B
+// arrays of every block, one contiguous range per block
+int hall_copy_b(mhd_ctx *ctx, bool snapshot)
+{
+    auto &H = ctx->hall;
+    prof_begin(ctx, "k_copy_segments");
+    if (snapshot)
+        k_copy_segments<<<dim3(unsigned(H.copy_ctas), unsigned(ctx->nblocks)), kThreads, 0, ctx->stream>>>(
+            H.bstar, ctx->pool, H.seg_snap, ctx->nblocks);
+    else
+        k_copy_segments<<<dim3(unsigned(H.copy_ctas), unsigned(ctx->nblocks)), kThreads, 0, ctx->stream>>>(
+            ctx->pool, H.bstar, H.seg_restore, ctx->nblocks);
+    return launched(ctx);
+}
+
 // UpdateMagneticDerivedFields_ with the B_cell / J_cell ghosts the Hall
-// stencils read, then the Hall edge EMF
+// stencils read, then the Hall edge EMF.  B_cell and the J edges in one pass
+// (both read only the face B; the B_cell sync between them in the reference
+// touches neither input).
 int hall_emf_from_current_b(mhd_ctx *ctx)
 {
     const int nb = ctx->nblocks;
     cudaStream_t s = ctx->stream;
-    prof_begin(ctx, "k_bcell");
-    launch_k_bcell(false, dim3(grid_for(max_box(ctx, LOC_CELL, 0)), nb), s, ctx->dbv);
+    prof_begin(ctx, "k_bcell_jedge");
+    launch_k_bcell_jedge(ctx->tune[TUNE_k_bcell_jedge], false, grid_kind(ctx, KIND_STAG), s, ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "B_cell", true));
-    prof_begin(ctx, "k_jedge");
-    k_jedge<<<dim3(grid_for(max_stagger(ctx)), nb), kThreads, 0, s>>>(ctx->dbv, F_Bxi, F_Jxi, 1.0, nullptr);
-    RUN(launched(ctx));
     RUN(run_sync(ctx, "Jedge"));
     prof_begin(ctx, "k_jcell");
     k_jcell<<<dim3(grid_for(max_box(ctx, LOC_CELL, 0)), nb), kThreads, 0, s>>>(ctx->dbv);
@@ -1221,122 +1289,113 @@ int hall_emf_from_current_b(mhd_ctx *ctx)
     return launched(ctx);
 }
 
-// Ehall <- X, Sync("Ehall"), B = B* + dt (-curl Ehall) on inner faces (theta = 1), Sync("Bface")
-int hall_trial_b(mhd_ctx *ctx, const double *X)
+// the trial B of the Ehall unknowns in the pool (UnpackVecToEhallField_:
+// owners already written, then their aliases), Sync("Ehall"), B = B* + dt
+// (-curl Ehall) on inner faces (theta = 1), Sync("Bface")
+int hall_trial_b(mhd_ctx *ctx)
 {
     auto &H = ctx->hall;
-    RUN(hall_snapshot(ctx, true));
-    // UnpackVecToEhallField_: owners, then their aliases
-    LAUNCHN(k_scatter_vec, H.n, ctx->pool, H.e, X, H.n, nullptr, H.n);
+    RUN(hall_copy_b(ctx, false));
     if (H.nalias > 0)
         LAUNCHN(k_alias_copy, H.nalias, ctx->pool, H.alias, H.owner, H.sign, H.nalias);
     RUN(run_sync(ctx, "Ehall", true));
     prof_begin(ctx, "k_curl_e2f");
-    launch_k_curl_e2f(ctx->tune[TUNE_k_curl_e2f], dim3(grid_for(max_stagger(ctx)), ctx->nblocks), ctx->stream, 
-        ctx->dbv, F_Ehxi, F_RBxi, F_Bxi, -1.0, ctx->dt, 1.0, 0, nullptr);
+    launch_k_curl_e2f(ctx->tune[TUNE_k_curl_e2f], dim3(grid_for(max_stagger(ctx)), ctx->nblocks), ctx->stream,
+                      ctx->dbv, F_Ehxi, F_RBxi, F_Bxi, -1.0, ctx->dt, 1.0, 0, nullptr);
     RUN(launched(ctx));
     return run_sync(ctx, "Bface");
 }
 
-// F = X - Ehall(trial B of X)   (FormFunction_)
-int hall_residual(mhd_ctx *ctx, const double *X, double *F)
+// FormFunction_ up to the predicted Hall EMF of the trial in the pool
+int hall_chain(mhd_ctx *ctx)
+{
+    RUN(hall_trial_b(ctx));
+    return hall_emf_from_current_b(ctx);
+}
+
+// one Arnoldi step: w = J V_j as (F(X + h V_j) - F(X)) / h, classical
+// Gram-Schmidt twice against V_0..V_j (the second pass's norm by Pythagoras),
+// the new Hessenberg column and V_{j+1}
+int hall_arnoldi(mhd_ctx *ctx, cudaGraphConditionalHandle hin)
 {
     auto &H = ctx->hall;
-    RUN(hall_trial_b(ctx, X));
-    RUN(hall_emf_from_current_b(ctx));
-    LAUNCHN(k_hall_residual, H.n, ctx->pool, H.e, X, F, H.n);
+    const int *jd = &H.st->j;
+    LAUNCHN(k_hall_trial, H.n, ctx->pool, H.e, H.X, &H.ctl->h, H.V, H.n, jd, H.Xt, H.n);
+    RUN(hall_chain(ctx));
+    HALL_RED(k_hall_jv_dots, ctx->pool, H.e, H.Xt, H.F, &H.ctl->h, H.w, H.V, H.n, H.st, H.n, H.partial, H.st->hcol,
+             H.done);
+    HALL_RED(k_hall_proj_dots, H.V, H.n, H.st, H.w, H.n, H.partial, H.dots, H.done);
+    LAUNCH1(k_hall_column, H.st, H.dots);
+    LAUNCHN(k_hall_next, H.n, H.V, H.n, H.w, H.st, H.dots, H.n);
+    LAUNCH1(k_inner_check, H.st, hin, hall_use(ctx));
     return MHD_OK;
 }
 
-int hall_dots(mhd_ctx *ctx, const double *V, int nvec, const int *jdev, const double *w, double *out)
+// r = b - J dx at a GMRES restart
+int hall_restart_product(mhd_ctx *ctx, cudaGraphConditionalHandle)
 {
     auto &H = ctx->hall;
-    const int ny = jdev ? H.restart + 1 : nvec;
-    prof_begin(ctx, "k_dots");
-    k_dots<<<dim3(H.ngroups, ny), 256, 0, ctx->stream>>>(V, H.n, nvec, w, H.n, H.partial, jdev, out, H.st->dot_done);
-    return launched(ctx);
-}
-
-int hall_norm(mhd_ctx *ctx, const double *x, double *out)
-{
-    auto &H = ctx->hall;
-    RUN(hall_dots(ctx, nullptr, 1, nullptr, x, H.dots + 48));
-    double v = 0.0;
-    RUN(read_scalar(ctx, H.dots + 48, &v));
-    *out = std::sqrt(v);
+    LAUNCHN(k_hall_trial, H.n, ctx->pool, H.e, H.X, &H.ctl->hdx, H.dx, 0, nullptr, H.Xt, H.n);
+    RUN(hall_chain(ctx));
+    LAUNCHN(k_hall_restart_r, H.n, ctx->pool, H.e, H.Xt, H.F, &H.ctl->hdx, H.b, H.r, H.n);
     return MHD_OK;
 }
 
-// w = J v by a forward difference around X (F = F(X) given)
-int hall_jv(mhd_ctx *ctx, const double *v, double vnorm, double xnorm, double *w)
+// one GMRES(m) cycle for J dx = -F (x0 = 0, PETSc's default test)
+int hall_cycle(mhd_ctx *ctx, cudaGraphConditionalHandle hout)
 {
     auto &H = ctx->hall;
-    if (vnorm <= 0.0)
-    {
-        LAUNCHN(k_zero, H.n, w, H.n);
-        return MHD_OK;
-    }
-    const double h = std::sqrt(2.220446049250313e-16) * (1.0 + xnorm) / vnorm;
-    LAUNCHN(k_axpy_to, H.n, H.Xt, H.X, h, v, H.n);
-    RUN(hall_residual(ctx, H.Xt, H.Ft));
-    LAUNCHN(k_fd_quotient, H.n, w, H.Ft, H.F, h, H.n);
+    const int use = hall_use(ctx);
+    HALL_RED(k_norm2, H.dx, H.n, H.partial, H.dots + 40, H.done);
+    cudaGraphConditionalHandle hr;
+    RUN(new_handle(ctx, &hr));
+    LAUNCH1(k_hall_cycle_prep, H.ctl, H.dots + 40, hr, use);
+    RUN(hall_cond(ctx, cudaGraphCondTypeIf, hr, &H.ctl->restart, hall_restart_product, &H.kb[HALL_KB_RESTART],
+                  &H.eager[HALL_KB_RESTART]));
+    HALL_RED(k_norm2, H.r, H.n, H.partial, H.dots + 44, H.done);
+    cudaGraphConditionalHandle hin;
+    RUN(new_handle(ctx, &hin));
+    LAUNCH1(k_cycle_start, H.st, H.dots + 44, hin, use);
+    LAUNCHN(k_div_guard, H.n, H.V, H.r, &H.st->beta, H.n, &H.st->inner);
+    RUN(hall_cond(ctx, cudaGraphCondTypeWhile, hin, &H.st->inner, hall_arnoldi, &H.kb[HALL_KB_INNER],
+                  &H.eager[HALL_KB_INNER]));
+    LAUNCH1(k_gmres_solve_y, H.st);
+    LAUNCHN(k_add_basis, H.n, H.V, H.n, H.st, H.dx, H.n);
+    LAUNCH1(k_outer_check, H.st, hout, use);
     return MHD_OK;
 }
 
-// restarted GMRES for J dx = -F (x0 = 0), the kernels of the resistive solve
-int hall_gmres(mhd_ctx *ctx, double xnorm)
+// one line-search trial X + lambda dx
+int hall_ls_trial(mhd_ctx *ctx, cudaGraphConditionalHandle hls)
 {
     auto &H = ctx->hall;
-    LAUNCHN(k_negate, H.n, H.b, H.F, H.n);
-    RUN(hall_dots(ctx, nullptr, 1, nullptr, H.b, H.dots + 40));
-    LAUNCH1(k_gmres_init, H.st, H.dots + 40, H.ksp_rtol, 0.0, H.ksp_maxit, H.restart);
-    LAUNCHN(k_zero, H.n, H.dx, H.n);
-    bool first = true;
-    int outer = 1;
-    while (outer)
-    {
-        if (first)
-            CK(ctx, cudaMemcpyAsync(H.r, H.b, size_t(H.n) * 8, cudaMemcpyDeviceToDevice, ctx->stream));
-        else
-        {
-            double dn = 0.0;
-            RUN(hall_norm(ctx, H.dx, &dn));
-            RUN(hall_jv(ctx, H.dx, dn, xnorm, H.w));
-            LAUNCHN(k_residual, H.n, H.b, H.w, H.r, H.n);
-        }
-        first = false;
-        RUN(hall_dots(ctx, nullptr, 1, nullptr, H.r, H.dots));
-        LAUNCH1(k_cycle_start, H.st, H.dots, 0, 0);
-        LAUNCHN(k_div_guard, H.n, H.V, H.r, &H.st->beta, H.n, &H.st->inner);
-        int inner = 0;
-        RUN(read_flag(ctx, &H.st->inner, &inner));
-        int j = 0;
-        while (inner)
-        {
-            // basis vectors have unit norm
-            RUN(hall_jv(ctx, H.V + int64_t(j) * H.n, 1.0, xnorm, H.w));
-            const int *jd = &H.st->j;
-            double *hcol = H.st->hcol;
-            RUN(hall_dots(ctx, H.V, 0, jd, H.w, hcol));
-            LAUNCHN(k_sub_proj, H.n, H.V, H.n, 0, hcol, H.w, H.n, jd);
-            RUN(hall_dots(ctx, H.V, 0, jd, H.w, H.dots));
-            LAUNCHN(k_sub_proj, H.n, H.V, H.n, 0, H.dots, H.w, H.n, jd);
-            prof_begin(ctx, "k_add_small");
-            k_add_small<<<1, 32, 0, ctx->stream>>>(hcol, H.dots, jd);
-            RUN(launched(ctx));
-            RUN(hall_dots(ctx, nullptr, 1, nullptr, H.w, H.dots + 32));
-            LAUNCH1(k_gmres_column, H.st, H.dots + 32);
-            LAUNCHN(k_div_next, H.n, H.V, H.n, H.w, H.st, H.n);
-            LAUNCH1(k_inner_check, H.st, 0, 0);
-            ++j;
-            ++H.lin_its;
-            RUN(read_flag(ctx, &H.st->inner, &inner));
-        }
-        LAUNCH1(k_gmres_solve_y, H.st);
-        LAUNCHN(k_add_basis, H.n, H.V, H.n, H.st, H.dx, H.n);
-        LAUNCH1(k_outer_check, H.st, 0, 0);
-        RUN(read_flag(ctx, &H.st->outer, &outer));
-    }
+    LAUNCHN(k_hall_trial, H.n, ctx->pool, H.e, H.X, &H.ctl->lambda, H.dx, 0, nullptr, H.Xt, H.n);
+    RUN(hall_chain(ctx));
+    HALL_RED(k_hall_res_dots, ctx->pool, H.e, H.Xt, H.Ft, H.n, H.partial, H.dots + 48, H.done);
+    LAUNCH1(k_hall_ls_check, H.ctl, H.dots + 48, hls, hall_use(ctx));
+    return MHD_OK;
+}
+
+// one Newton step: ||X||, GMRES for the correction, the line search, the new iterate
+int hall_newton_step(mhd_ctx *ctx, cudaGraphConditionalHandle hn)
+{
+    auto &H = ctx->hall;
+    const int use = hall_use(ctx);
+    HALL_RED(k_norm2, H.X, H.n, H.partial, H.dots + 52, H.done);
+    LAUNCH1(k_hall_step_begin, H.ctl, H.dots + 52);
+    HALL_RED(k_hall_gmres_prologue, H.F, H.b, H.r, H.dx, H.n, H.partial, H.dots + 56, H.done);
+    cudaGraphConditionalHandle hout;
+    RUN(new_handle(ctx, &hout));
+    LAUNCH1(k_hall_gmres_init, H.st, H.dots + 56, H.ksp_rtol, 0.0, H.ksp_maxit, H.restart, hout, use);
+    RUN(hall_cond(ctx, cudaGraphCondTypeWhile, hout, &H.st->outer, hall_cycle, &H.kb[HALL_KB_CYCLE],
+                  &H.eager[HALL_KB_CYCLE]));
+    cudaGraphConditionalHandle hls;
+    RUN(new_handle(ctx, &hls));
+    LAUNCH1(k_hall_ls_begin, H.ctl, hls, use);
+    RUN(hall_cond(ctx, cudaGraphCondTypeWhile, hls, &H.ctl->ls, hall_ls_trial, &H.kb[HALL_KB_LS],
+                  &H.eager[HALL_KB_LS]));
+    LAUNCHN(k_hall_take, H.n, H.X, H.Xt, H.F, H.Ft, H.n);
+    LAUNCH1(k_hall_accept, H.ctl, hn, use);
     return MHD_OK;
 }
 
@@ -1349,52 +1408,26 @@ int launch_hall_implicit(mhd_ctx *ctx)
     if (!H.on || H.n == 0)
         return MHD_OK;
     RUN(build_all_syncs(ctx));
-    RUN(hall_snapshot(ctx, false));
+    RUN(hall_copy_b(ctx, true));
     LAUNCHN(k_pack_vec, H.n, ctx->pool, H.e, H.X, H.n);
-    RUN(hall_residual(ctx, H.X, H.F));
-    double f = 0.0;
-    RUN(hall_norm(ctx, H.F, &f));
-    H.fnorm0 = f;
-    H.its = 0;
-    H.lin_its = 0;
-    H.reason = -5; // iteration limit
-    for (int it = 0; it <= H.maxit; ++it)
+    // F of the initial guess (the unknowns in the pool are X already)
+    RUN(hall_chain(ctx));
+    HALL_RED(k_hall_res_dots, ctx->pool, H.e, H.X, H.F, H.n, H.partial, H.dots + 60, H.done);
+    cudaGraphConditionalHandle hn;
+    RUN(new_handle(ctx, &hn));
+    LAUNCH1(k_hall_begin, H.ctl, H.dots + 60, H.st, H.rtol, H.atol, H.maxit, hn, hall_use(ctx));
+    RUN(hall_cond(ctx, cudaGraphCondTypeWhile, hn, &H.ctl->newton, hall_newton_step, &H.kb[HALL_KB_NEWTON],
+                  &H.eager[HALL_KB_NEWTON]));
+    if (ctx->capturing)
     {
-        if (f <= H.atol)
-        {
-            H.reason = 2; // SNES_CONVERGED_FNORM_ABS
-            break;
-        }
-        if (f <= H.rtol * H.fnorm0)
-        {
-            H.reason = 3; // SNES_CONVERGED_FNORM_RELATIVE
-            break;
-        }
-        if (it == H.maxit)
-            break;
-        double xnorm = 0.0;
-        RUN(hall_norm(ctx, H.X, &xnorm));
-        RUN(hall_gmres(ctx, xnorm));
-        // backtracking: halve the step until ||F|| decreases sufficiently
-        double lambda = 1.0, ft = 0.0;
-        for (int ls = 0; ls < 12; ++ls)
-        {
-            LAUNCHN(k_axpy_to, H.n, H.Xt, H.X, lambda, H.dx, H.n);
-            RUN(hall_residual(ctx, H.Xt, H.Ft));
-            RUN(hall_norm(ctx, H.Ft, &ft));
-            if (ft <= (1.0 - 1e-4 * lambda) * f)
-                break;
-            lambda *= 0.5;
-        }
-        std::swap(H.X, H.Xt);
-        std::swap(H.F, H.Ft);
-        f = ft;
-        H.its = it + 1;
+        // kernels per pass of each body, without the bodies nested in it
+        H.kb[HALL_KB_CYCLE] -= H.kb[HALL_KB_INNER] + H.kb[HALL_KB_RESTART];
+        H.kb_nested = H.kb[HALL_KB_NEWTON];
+        H.kb[HALL_KB_NEWTON] -= (H.kb[HALL_KB_CYCLE] + H.kb[HALL_KB_INNER] + H.kb[HALL_KB_RESTART]) + H.kb[HALL_KB_LS];
     }
-    H.fnorm = f;
-    // final update with the converged Hall EMF
-    RUN(hall_trial_b(ctx, H.X));
-    return MHD_OK;
+    // the final update with the converged Hall EMF
+    LAUNCHN(k_hall_trial, H.n, ctx->pool, H.e, H.X, nullptr, nullptr, 0, nullptr, nullptr, H.n);
+    return hall_trial_b(ctx);
 }
 
 // the part of a step before the eagerly driven solves: the explicit step,
@@ -1538,19 +1571,23 @@ int build_graph(mhd_ctx *ctx)
             return fail(ctx, MHD_ESTATE, "SSP-RK2 with the implicit resistive solve needs the persistent solve");
         return capture(ctx, launch_step, &ctx->graph, &ctx->gexec, &ctx->graph_kernels);
     }
-    if (ctx->res.on && ctx->res.graph_loops && !ctx->hall.on)
+    if ((ctx->res.on || ctx->hall.on) && ctx->res.graph_loops)
     {
+        ctx->hall.kb_nested = 0;
         const int rc = capture(ctx, launch_step, &ctx->graph, &ctx->gexec, &ctx->graph_kernels);
         if (rc == MHD_OK)
         {
             // the loop bodies were captured once; their launches are counted per pass
-            ctx->graph_kernels -= ctx->res.k_cycle + ctx->res.k_inner;
+            ctx->graph_kernels -= ctx->res.k_cycle + ctx->res.k_inner + ctx->hall.kb_nested;
             return MHD_OK;
         }
         // conditional nodes unavailable: clear the error state of the stream and fall back
         cudaGetLastError();
         drop_graph(ctx);
         ctx->res.graph_loops = false;
+        ctx->hall.kb_nested = 0;
+        for (auto &k : ctx->hall.kb)
+            k = 0;
     }
     if (ctx->res.on || ctx->hall.on)
     {
@@ -3051,7 +3088,8 @@ int mhd_set_hall_implicit(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, int6
     auto &H = ctx->hall;
     for (void *p : {(void *)H.e, (void *)H.alias, (void *)H.owner, (void *)H.sign, (void *)H.bstar, (void *)H.X,
                     (void *)H.F, (void *)H.Xt, (void *)H.Ft, (void *)H.dx, (void *)H.b, (void *)H.r, (void *)H.V,
-                    (void *)H.w, (void *)H.partial, (void *)H.dots, (void *)H.st})
+                    (void *)H.w, (void *)H.partial, (void *)H.dots, (void *)H.st, (void *)H.ctl, (void *)H.done,
+                    (void *)H.seg_snap, (void *)H.seg_restore})
         cudaFree(p);
     H = mhd_ctx::HallImplicit();
     drop_graph(ctx);
@@ -3086,18 +3124,39 @@ int mhd_set_hall_implicit(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, int6
     H.ksp_rtol = ksp_rtol;
     H.ksp_maxit = ksp_maxit;
     H.ngroups = int(std::min<int64_t>(std::max<int64_t>((H.n + 255) / 256, 1), 592));
+    // the face B arrays of a block are one range of the pool (B_xi, B_eta,
+    // B_zeta consecutive, with the alignment gaps between them)
+    std::vector<int64_t> snap, restore;
     size_t nbs = 0;
+    int64_t seg_max = 0;
     for (int b = 0; b < ctx->nblocks; ++b)
-        nbs += 3 * size_t(ctx->hbv[size_t(b)].vol);
+    {
+        const int64_t lo = int64_t(ctx->base[F_Bxi][size_t(b)]);
+        const int64_t len = int64_t(ctx->base[F_Bzeta][size_t(b)]) + ctx->hbv[size_t(b)].vol - lo;
+        snap.insert(snap.end(), {int64_t(nbs), lo, len});
+        restore.insert(restore.end(), {lo, int64_t(nbs), len});
+        nbs += size_t(len);
+        seg_max = std::max(seg_max, len);
+    }
+    H.copy_ctas = int(std::min<int64_t>(std::max<int64_t>((seg_max + kThreads - 1) / kThreads, 1), 1184));
+    RUN(upload_vec(ctx, snap, &H.seg_snap));
+    RUN(upload_vec(ctx, restore, &H.seg_restore));
     CK(ctx, cudaMalloc(&H.bstar, nbs * 8));
     const size_t nn = size_t(H.n);
     for (double **p : {&H.X, &H.F, &H.Xt, &H.Ft, &H.dx, &H.b, &H.r, &H.w})
         CK(ctx, cudaMalloc(p, nn * 8));
     CK(ctx, cudaMalloc(&H.V, nn * size_t(H.restart + 1) * 8));
-    CK(ctx, cudaMalloc(&H.partial, size_t(H.ngroups) * size_t(H.restart + 2) * 8));
+    CK(ctx, cudaMalloc(&H.partial, size_t(H.ngroups) * size_t(kMdMax) * 8));
     CK(ctx, cudaMalloc(&H.dots, 64 * 8));
     CK(ctx, cudaMalloc(&H.st, sizeof(GmresState)));
     CK(ctx, cudaMemset(H.st, 0, sizeof(GmresState)));
+    CK(ctx, cudaMalloc(&H.ctl, sizeof(HallCtl)));
+    CK(ctx, cudaMemset(H.ctl, 0, sizeof(HallCtl)));
+    CK(ctx, cudaMalloc(&H.done, sizeof(unsigned)));
+    CK(ctx, cudaMemset(H.done, 0, sizeof(unsigned)));
+    for (auto &sp : ctx->spare)
+        if (!sp)
+            CK(ctx, cudaStreamCreateWithFlags(&sp, cudaStreamNonBlocking));
     H.on = true;
     return MHD_OK;
 }
@@ -3109,16 +3168,26 @@ int mhd_hall_stats(const mhd_ctx *ctx, int32_t *newton_its, int32_t *linear_its,
     if (!ctx)
         return MHD_EINVAL;
     const auto &H = ctx->hall;
+    HallCtl c{};
+    GmresState g{};
+    if (H.ctl)
+    {
+        // the statistics live in the solve's device state
+        if (cudaMemcpyAsync(&c, H.ctl, sizeof c, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+            cudaMemcpyAsync(&g, H.st, sizeof g, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+            cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+            return MHD_ECUDA;
+    }
     if (newton_its)
-        *newton_its = H.its;
+        *newton_its = c.it;
     if (linear_its)
-        *linear_its = H.lin_its;
+        *linear_its = int32_t(g.total_its - c.lin0);
     if (fnorm)
-        *fnorm = H.fnorm;
+        *fnorm = c.f;
     if (fnorm0)
-        *fnorm0 = H.fnorm0;
+        *fnorm0 = c.f0;
     if (reason)
-        *reason = H.reason;
+        *reason = c.reason;
     return MHD_OK;
 }
 
@@ -3630,6 +3699,21 @@ int64_t mhd_kernel_launches(const mhd_ctx *ctx)
         if (cudaMemcpyAsync(&h, R.st, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream) == cudaSuccess &&
             cudaStreamSynchronize(ctx->stream) == cudaSuccess)
             n += R.k_cycle * (h.total_cycles - R.cycles_eager) + R.k_inner * (h.total_its - R.its_eager);
+    }
+    const auto &H = ctx->hall;
+    if (H.ctl && H.kb_nested > 0)
+    {
+        // passes of the graph-resident Hall loops, counted on the device
+        HallCtl c;
+        GmresState g;
+        if (cudaMemcpyAsync(&c, H.ctl, sizeof c, cudaMemcpyDeviceToHost, ctx->stream) == cudaSuccess &&
+            cudaMemcpyAsync(&g, H.st, sizeof g, cudaMemcpyDeviceToHost, ctx->stream) == cudaSuccess &&
+            cudaStreamSynchronize(ctx->stream) == cudaSuccess)
+        {
+            const long long pass[HALL_KB_N] = {c.pass[0], g.total_cycles, g.total_its, c.pass[1], c.pass[2]};
+            for (int q = 0; q < HALL_KB_N; ++q)
+                n += H.kb[q] * (pass[q] - H.eager[q]);
+        }
     }
     return n;
 }

@@ -198,10 +198,68 @@ __global__ void k_resist_rhs(const double *pool, const uint64_t *j, const double
 __global__ void k_alias_copy(double *pool, const uint64_t *alias, const uint64_t *owner, const double *sign,
                              int64_t n);
 __global__ void k_pack_vec(const double *pool, const uint64_t *src, double *x, int64_t n);
-__global__ void k_hall_residual(const double *pool, const uint64_t *e, const double *x, double *F, int64_t n);
-__global__ void k_axpy_to(double *out, const double *x, double a, const double *y, int64_t n);
-__global__ void k_fd_quotient(double *out, const double *a, const double *b, double h, int64_t n);
-__global__ void k_negate(double *out, const double *x, int64_t n);
+
+// Control state of the implicit Hall solve on the device: Newton with a
+// backtracking line search around GMRES on finite-difference products.
+// One-thread kernels update it and set the loop conditions (the graph's
+// conditional handles inside a graph; the mirror flags, read by the host,
+// when run eagerly).
+struct HallCtl
+{
+    double f, f0, ft; // ||F|| of the iterate, of the initial guess, of the line-search trial
+    double xnorm;     // ||X|| at the start of the Newton step
+    double h;         // difference step of a product with a unit basis vector
+    double hdx;       // ... with the correction dx (restart residual)
+    double lambda;    // line-search step
+    double rtol, atol;
+    int it, maxit;    // Newton steps taken / allowed
+    int cut;          // line-search halvings in this step
+    int reason;       // 2 ||F|| <= atol, 3 ||F|| <= rtol ||F0||, -5 step limit
+    int first;        // the first GMRES cycle of the Newton step (r = b, no product)
+    int newton, ls, restart; // loop conditions
+    long long lin0;          // cumulative GMRES iterations before this solve
+    long long pass[3];       // cumulative: Newton steps, restart products, line-search trials
+};
+// products per multi-dot pass: up to kMaxRestart + 1 basis vectors and one norm
+constexpr int kMdMax = 32;
+__global__ void k_hall_begin(HallCtl *c, const double *f2, const GmresState *st, double rtol, double atol, int maxit,
+                             cudaGraphConditionalHandle h, int use);
+__global__ void k_hall_step_begin(HallCtl *c, const double *x2);
+__global__ void k_hall_gmres_init(GmresState *st, const double *b2, double rtol, double atol, int maxit, int m,
+                                  cudaGraphConditionalHandle hout, int use);
+__global__ void k_hall_cycle_prep(HallCtl *c, const double *dx2, cudaGraphConditionalHandle h, int use);
+__global__ void k_hall_ls_begin(HallCtl *c, cudaGraphConditionalHandle h, int use);
+__global__ void k_hall_ls_check(HallCtl *c, const double *ft2, cudaGraphConditionalHandle h, int use);
+__global__ void k_hall_accept(HallCtl *c, cudaGraphConditionalHandle h, int use);
+__global__ void k_hall_column(GmresState *st, const double *d);
+// Xt = X + (*a) v (v = v0 + (*jdev) ldv; Xt = X when a is null), written into the pool's unknowns
+__global__ void k_hall_trial(double *pool, const uint64_t *e, const double *X, const double *a, const double *v0,
+                             int64_t ldv, const int *jdev, double *Xt, int64_t n);
+// w = ((Xt - pool[e]) - F) / *h and out[c] = V_c . w for c <= j
+__global__ void k_hall_jv_dots(const double *pool, const uint64_t *e, const double *Xt, const double *F,
+                               const double *h, double *w, const double *V, int64_t ldv, const GmresState *st,
+                               int64_t n, double *partial, double *out, unsigned *done);
+// w -= sum_c hcol[c] V_c; out[c] = V_c . w (c <= j), out[j + 1] = w . w
+__global__ void k_hall_proj_dots(const double *V, int64_t ldv, const GmresState *st, double *w, int64_t n,
+                                 double *partial, double *out, unsigned *done);
+// V_{j+1} = (w - sum_c d[c] V_c) / hcol[j + 1]
+__global__ void k_hall_next(double *V, int64_t ldv, const double *w, const GmresState *st, const double *d,
+                            int64_t n);
+// Ft = Xt - pool[e]; out[0] = Ft . Ft
+__global__ void k_hall_res_dots(const double *pool, const uint64_t *e, const double *Xt, double *Ft, int64_t n,
+                                double *partial, double *out, unsigned *done);
+// r = b - ((Xt - pool[e]) - F) / *h
+__global__ void k_hall_restart_r(const double *pool, const uint64_t *e, const double *Xt, const double *F,
+                                 const double *h, const double *b, double *r, int64_t n);
+// b = -F, r = b, dx = 0; out[0] = b . b
+__global__ void k_hall_gmres_prologue(const double *F, double *b, double *r, double *dx, int64_t n, double *partial,
+                                      double *out, unsigned *done);
+// out[0] = x . x
+__global__ void k_norm2(const double *x, int64_t n, double *partial, double *out, unsigned *done);
+// X = Xt, F = Ft
+__global__ void k_hall_take(double *X, const double *Xt, double *F, const double *Ft, int64_t n);
+// dst = src over nseg segments (seg: dst offset, src offset, length)
+__global__ void k_copy_segments(double *dst, const double *src, const int64_t *seg, int nseg);
 
 
 // Hot stencil kernels in register / occupancy variants (the same code under

@@ -119,7 +119,8 @@ __global__ void k_div_next(double *__restrict__ V, int64_t ldv, const double *__
 }
 
 // start of a solve: ||b||, the stopping threshold, counters
-__global__ void k_gmres_init(GmresState *st, const double *__restrict__ b2, double rtol, double atol, int maxit, int m)
+__device__ __forceinline__ void gmres_init_state(GmresState *st, const double *__restrict__ b2, double rtol,
+                                                 double atol, int maxit, int m)
 {
     const double bnorm = sqrt(b2[0]);
     st->bnorm = bnorm;
@@ -132,6 +133,11 @@ __global__ void k_gmres_init(GmresState *st, const double *__restrict__ b2, doub
     st->j = 0;
     st->inner = 0;
     st->outer = 1;
+}
+
+__global__ void k_gmres_init(GmresState *st, const double *__restrict__ b2, double rtol, double atol, int maxit, int m)
+{
+    gmres_init_state(st, b2, rtol, atol, maxit, m);
 }
 
 // start of a cycle: beta = ||r||, g = beta e1; decides whether the cycle runs
@@ -164,10 +170,9 @@ __global__ void k_cycle_start(GmresState *st, const double *__restrict__ beta2, 
 
 // new column j: hcol[j + 1] = ||w||, H[0..j+1, j] = hcol; apply the
 // previous rotations, form a new one, update g and the residual estimate
-__global__ void k_gmres_column(GmresState *st, const double *__restrict__ wnorm2)
+__device__ __forceinline__ void gmres_rotate_column(GmresState *st)
 {
     const int j = st->j;
-    st->hcol[j + 1] = sqrt(wnorm2[0]);
     double *H = st->H;
     for (int i = 0; i <= j + 1; ++i)
         H[i * 31 + j] = st->hcol[i];
@@ -187,6 +192,12 @@ __global__ void k_gmres_column(GmresState *st, const double *__restrict__ wnorm2
     st->g[j] = st->cs[j] * st->g[j];
     st->resid = fabs(st->g[j + 1]);
     st->breakdown = (st->hcol[j + 1] == 0.0) ? 1 : 0;
+}
+
+__global__ void k_gmres_column(GmresState *st, const double *__restrict__ wnorm2)
+{
+    st->hcol[st->j + 1] = sqrt(wnorm2[0]);
+    gmres_rotate_column(st);
 }
 
 // end of an Arnoldi step: counters and the inner loop condition
@@ -321,39 +332,364 @@ __global__ void k_pack_vec(const double *__restrict__ pool, const uint64_t *__re
         x[t] = pool[src[t]];
 }
 
-// F[t] = x[t] - pool[e[t]]   (WriteResidual_: unknown minus predicted Hall EMF)
-__global__ void k_hall_residual(const double *__restrict__ pool, const uint64_t *__restrict__ e,
-                                const double *__restrict__ x, double *__restrict__ F, int64_t n)
+
+// ---------------------------------------------------------------------------
+// The implicit Hall solve steered on the device (ImplicitHallSolver::
+// SolveOneStep, Z4_Lunar/src/implicit/Hall_Implicit_Solver.cpp:268-391):
+// one-thread control kernels over HallCtl, and vector passes that fuse the
+// finite-difference product, the Gram-Schmidt projections and the dot
+// products a GMRES step needs (three passes over the basis per step).
+// ---------------------------------------------------------------------------
+
+namespace
+{
+__device__ __forceinline__ void set_cond(cudaGraphConditionalHandle h, int use, int v)
+{
+    if (use)
+        cudaGraphSetConditional(h, unsigned(v));
+}
+
+// sqrt of the FP64 unit roundoff: the relative difference step
+__device__ __forceinline__ double fd_scale() { return sqrt(2.220446049250313e-16); }
+
+// the Newton loop test of SNESSolve's default convergence test
+__device__ void hall_newton_test(HallCtl *c, cudaGraphConditionalHandle h, int use)
+{
+    int go = 0;
+    if (c->f <= c->atol)
+        c->reason = 2;
+    else if (c->f <= c->rtol * c->f0)
+        c->reason = 3;
+    else if (c->it >= c->maxit)
+        c->reason = -5;
+    else
+        go = 1;
+    c->newton = go;
+    set_cond(h, use, go);
+}
+
+// Adds acc[c], c < nv, over the grid in a fixed order (warp shuffles, the
+// CTA's warps in order, then the last CTA adds the CTAs' partials in order),
+// so every pass is reproducible.  nv is uniform over the grid.
+__device__ void mdot_finish(double (&acc)[kMdMax], int nv, double *__restrict__ partial, double *__restrict__ out,
+                            unsigned *__restrict__ done)
+{
+    constexpr int kWarps = kRedThreads / 32;
+    __shared__ double red[kMdMax][kWarps];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < kMdMax; ++c)
+        if (c < nv)
+        {
+            double v = acc[c];
+            for (int o = 16; o > 0; o >>= 1)
+                v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0)
+                red[c][wid] = v;
+        }
+    __syncthreads();
+    if (int(threadIdx.x) < nv)
+    {
+        double s = 0.0;
+        for (int w = 0; w < kWarps; ++w)
+            s += red[threadIdx.x][w];
+        partial[int64_t(threadIdx.x) * gridDim.x + blockIdx.x] = s;
+        __threadfence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        last = (atomicAdd(done, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!last)
+        return;
+    __threadfence();
+    for (int c = wid; c < nv; c += kWarps)
+    {
+        double s = 0.0;
+        for (int b = lane; b < int(gridDim.x); b += 32)
+            s += __ldcg(&partial[int64_t(c) * gridDim.x + b]);
+        for (int o = 16; o > 0; o >>= 1)
+            s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0)
+            out[c] = s;
+    }
+    if (threadIdx.x == 0)
+        *done = 0u;
+}
+} // namespace
+
+__global__ void k_hall_begin(HallCtl *c, const double *__restrict__ f2, const GmresState *__restrict__ st, double rtol,
+                             double atol, int maxit, cudaGraphConditionalHandle h, int use)
+{
+    c->f = sqrt(f2[0]);
+    c->f0 = c->f;
+    c->rtol = rtol;
+    c->atol = atol;
+    c->maxit = maxit;
+    c->it = 0;
+    c->reason = -5;
+    c->lin0 = st->total_its;
+    hall_newton_test(c, h, use);
+}
+
+// start of a Newton step: ||X|| and the difference step of unit vectors
+__global__ void k_hall_step_begin(HallCtl *c, const double *__restrict__ x2)
+{
+    c->xnorm = sqrt(x2[0]);
+    c->h = fd_scale() * (1.0 + c->xnorm) / 1.0;
+    c->first = 1;
+}
+
+__global__ void k_hall_gmres_init(GmresState *st, const double *__restrict__ b2, double rtol, double atol, int maxit,
+                                  int m, cudaGraphConditionalHandle hout, int use)
+{
+    gmres_init_state(st, b2, rtol, atol, maxit, m);
+    set_cond(hout, use, 1);
+}
+
+// top of a GMRES cycle: a restart needs r = b - J dx, one product with dx
+// (none on the first cycle, where r = b, nor when dx = 0)
+__global__ void k_hall_cycle_prep(HallCtl *c, const double *__restrict__ dx2, cudaGraphConditionalHandle h, int use)
+{
+    const double dn = sqrt(dx2[0]);
+    const int go = !c->first && dn > 0.0;
+    if (go)
+    {
+        c->hdx = fd_scale() * (1.0 + c->xnorm) / dn;
+        c->pass[1] += 1;
+    }
+    c->first = 0;
+    c->restart = go;
+    set_cond(h, use, go);
+}
+
+__global__ void k_hall_ls_begin(HallCtl *c, cudaGraphConditionalHandle h, int use)
+{
+    c->lambda = 1.0;
+    c->cut = 0;
+    c->ls = 1;
+    set_cond(h, use, 1);
+}
+
+// backtracking: accept when ||F(X + lambda dx)|| <= (1 - 1e-4 lambda) ||F(X)||,
+// else halve lambda, at most 12 trials (the last one is taken regardless)
+__global__ void k_hall_ls_check(HallCtl *c, const double *__restrict__ ft2, cudaGraphConditionalHandle h, int use)
+{
+    const double ft = sqrt(ft2[0]);
+    c->ft = ft;
+    c->pass[2] += 1;
+    int go = 0;
+    if (!(ft <= (1.0 - 1e-4 * c->lambda) * c->f) && c->cut < 11)
+    {
+        c->lambda *= 0.5;
+        c->cut += 1;
+        go = 1;
+    }
+    c->ls = go;
+    set_cond(h, use, go);
+}
+
+__global__ void k_hall_accept(HallCtl *c, cudaGraphConditionalHandle h, int use)
+{
+    c->f = c->ft;
+    c->it += 1;
+    c->pass[0] += 1;
+    hall_newton_test(c, h, use);
+}
+
+// the column of a CGS2 step whose second pass gave d: h += d, and
+// ||w''||^2 = ||w'||^2 - ||d||^2 (w'' = w' - V d with V orthonormal)
+__global__ void k_hall_column(GmresState *st, const double *__restrict__ d)
+{
+    const int j = st->j;
+    double s2 = d[j + 1];
+    for (int c = 0; c <= j; ++c)
+    {
+        st->hcol[c] += d[c];
+        s2 -= d[c] * d[c];
+    }
+    st->hcol[j + 1] = sqrt(fmax(s2, 0.0));
+    gmres_rotate_column(st);
+}
+
+__global__ void k_hall_trial(double *__restrict__ pool, const uint64_t *__restrict__ e, const double *__restrict__ X,
+                             const double *__restrict__ a, const double *__restrict__ v0, int64_t ldv,
+                             const int *__restrict__ jdev, double *__restrict__ Xt, int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n)
+        return;
+    double x = X[t];
+    if (a)
+    {
+        const double *v = jdev ? v0 + int64_t(jdev[0]) * ldv : v0;
+        x = x + a[0] * v[t];
+    }
+    if (Xt)
+        Xt[t] = x;
+    pool[e[t]] = x;
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_hall_jv_dots(const double *__restrict__ pool,
+                                                              const uint64_t *__restrict__ e,
+                                                              const double *__restrict__ Xt,
+                                                              const double *__restrict__ F,
+                                                              const double *__restrict__ h, double *__restrict__ w,
+                                                              const double *__restrict__ V, int64_t ldv,
+                                                              const GmresState *__restrict__ st, int64_t n,
+                                                              double *__restrict__ partial, double *__restrict__ out,
+                                                              unsigned *__restrict__ done)
+{
+    const int nv = st->j + 1;
+    const double hh = h[0];
+    double acc[kMdMax];
+#pragma unroll
+    for (int c = 0; c < kMdMax; ++c)
+        acc[c] = 0.0;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x)
+    {
+        const double wt = ((Xt[t] - pool[e[t]]) - F[t]) / hh;
+        w[t] = wt;
+#pragma unroll
+        for (int c = 0; c < kMdMax; ++c)
+            if (c < nv)
+                acc[c] += V[int64_t(c) * ldv + t] * wt;
+    }
+    mdot_finish(acc, nv, partial, out, done);
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_hall_proj_dots(const double *__restrict__ V, int64_t ldv,
+                                                                const GmresState *__restrict__ st,
+                                                                double *__restrict__ w, int64_t n,
+                                                                double *__restrict__ partial,
+                                                                double *__restrict__ out, unsigned *__restrict__ done)
+{
+    __shared__ double hs[kMdMax];
+    const int nv = st->j + 1;
+    if (int(threadIdx.x) < nv)
+        hs[threadIdx.x] = st->hcol[threadIdx.x];
+    __syncthreads();
+    double acc[kMdMax];
+#pragma unroll
+    for (int c = 0; c < kMdMax; ++c)
+        acc[c] = 0.0;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x)
+    {
+        double wt = w[t];
+#pragma unroll
+        for (int c = 0; c < kMdMax; ++c)
+            if (c < nv)
+                wt -= hs[c] * V[int64_t(c) * ldv + t];
+        w[t] = wt;
+#pragma unroll
+        for (int c = 0; c < kMdMax; ++c)
+            if (c < nv)
+                acc[c] += V[int64_t(c) * ldv + t] * wt;
+            else if (c == nv)
+                acc[c] += wt * wt;
+    }
+    mdot_finish(acc, nv + 1, partial, out, done);
+}
+
+__global__ void k_hall_next(double *__restrict__ V, int64_t ldv, const double *__restrict__ w,
+                            const GmresState *__restrict__ st, const double *__restrict__ d, int64_t n)
+{
+    if (st->breakdown)
+        return;
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n)
+        return;
+    const int j = st->j;
+    double s = w[t];
+    for (int c = 0; c <= j; ++c)
+        s -= d[c] * V[int64_t(c) * ldv + t];
+    V[int64_t(j + 1) * ldv + t] = s / st->hcol[j + 1];
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_hall_res_dots(const double *__restrict__ pool,
+                                                               const uint64_t *__restrict__ e,
+                                                               const double *__restrict__ Xt, double *__restrict__ Ft,
+                                                               int64_t n, double *__restrict__ partial,
+                                                               double *__restrict__ out, unsigned *__restrict__ done)
+{
+    double acc[kMdMax];
+#pragma unroll
+    for (int c = 0; c < kMdMax; ++c)
+        acc[c] = 0.0;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x)
+    {
+        const double f = Xt[t] - pool[e[t]];
+        Ft[t] = f;
+        acc[0] += f * f;
+    }
+    mdot_finish(acc, 1, partial, out, done);
+}
+
+__global__ void k_hall_restart_r(const double *__restrict__ pool, const uint64_t *__restrict__ e,
+                                 const double *__restrict__ Xt, const double *__restrict__ F,
+                                 const double *__restrict__ h, const double *__restrict__ b, double *__restrict__ r,
+                                 int64_t n)
 {
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t < n)
-        F[t] = x[t] - pool[e[t]];
+        r[t] = b[t] - ((Xt[t] - pool[e[t]]) - F[t]) / h[0];
 }
 
-// out = x + a y
-__global__ void k_axpy_to(double *__restrict__ out, const double *__restrict__ x, double a, const double *__restrict__ y,
-                          int64_t n)
+__global__ void __launch_bounds__(kRedThreads) k_hall_gmres_prologue(const double *__restrict__ F,
+                                                                     double *__restrict__ b, double *__restrict__ r,
+                                                                     double *__restrict__ dx, int64_t n,
+                                                                     double *__restrict__ partial,
+                                                                     double *__restrict__ out,
+                                                                     unsigned *__restrict__ done)
+{
+    double acc[kMdMax];
+#pragma unroll
+    for (int c = 0; c < kMdMax; ++c)
+        acc[c] = 0.0;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x)
+    {
+        const double v = -F[t];
+        b[t] = v;
+        r[t] = v;
+        dx[t] = 0.0;
+        acc[0] += v * v;
+    }
+    mdot_finish(acc, 1, partial, out, done);
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_norm2(const double *__restrict__ x, int64_t n,
+                                                       double *__restrict__ partial, double *__restrict__ out,
+                                                       unsigned *__restrict__ done)
+{
+    double acc[kMdMax];
+#pragma unroll
+    for (int c = 0; c < kMdMax; ++c)
+        acc[c] = 0.0;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x)
+        acc[0] += x[t] * x[t];
+    mdot_finish(acc, 1, partial, out, done);
+}
+
+__global__ void k_hall_take(double *__restrict__ X, const double *__restrict__ Xt, double *__restrict__ F,
+                            const double *__restrict__ Ft, int64_t n)
 {
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t < n)
-        out[t] = x[t] + a * y[t];
+    {
+        X[t] = Xt[t];
+        F[t] = Ft[t];
+    }
 }
 
-// out = (a - b) / h   (finite-difference Jacobian-vector product)
-__global__ void k_fd_quotient(double *__restrict__ out, const double *__restrict__ a, const double *__restrict__ b,
-                              double h, int64_t n)
+__global__ void k_copy_segments(double *__restrict__ dst, const double *__restrict__ src,
+                                const int64_t *__restrict__ seg, int nseg)
 {
-    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t < n)
-        out[t] = (a[t] - b[t]) / h;
+    const int s = blockIdx.y;
+    if (s >= nseg)
+        return;
+    const int64_t d0 = seg[3 * s], s0 = seg[3 * s + 1], len = seg[3 * s + 2];
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < len; t += int64_t(gridDim.x) * blockDim.x)
+        dst[d0 + t] = src[s0 + t];
 }
-
-// out = -x
-__global__ void k_negate(double *__restrict__ out, const double *__restrict__ x, int64_t n)
-{
-    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t < n)
-        out[t] = -x[t];
-}
-
 } // namespace mhd

@@ -14,6 +14,7 @@
 //   ref_lunar probe <state.rst> <group> <out.bin>  index-encoded Sync(group)
 //   ref_lunar hall <state.rst> <out.bin>           Hall edge EMF of the state
 //   ref_lunar hallstep <state.rst> <out.bin>       one implicit Hall solve (tight tolerances)
+//   ref_lunar hallrun <state.rst> <n> <prefix>     n StepOnce with the implicit Hall solve (HALL_IMPLICIT == 1)
 //   ref_lunar time  <state.rst> <nsteps>           wall time of the step loop
 //   ref_lunar timerk2 <state.rst> <nsteps>         wall time of SSP-RK2 steps
 //
@@ -339,10 +340,12 @@ int cmd_geom(Harness &h, const std::string &out)
     return 0;
 }
 
-void dump_state(Harness &h, const std::string &path)
+void dump_state(Harness &h, const std::string &path, const std::vector<std::string> &extra = {})
 {
     std::vector<DumpItem> items;
     for (const auto &n : state_fields())
+        items.push_back(field_item(h.fld, n));
+    for (const auto &n : extra)
         items.push_back(field_item(h.fld, n));
     // dt of the step just taken, as a 1x1x1 pseudo-field
     DumpItem dti;
@@ -485,6 +488,45 @@ int cmd_rk2(Harness &h, const std::string &state, int nsteps, const std::string 
         char buf[32];
         std::snprintf(buf, sizeof(buf), "_%04d.bin", n);
         dump_state(h, prefix + buf);
+    }
+    return 0;
+}
+
+// StepOnce as the reference compiles it with HALL_IMPLICIT == 1
+// (Z4_Lunar/src/LunarSolver_Driver.cpp:21-92): the Euler stage, then the
+// implicit Hall solve at the step's dt (SolveOneStep) and calc_Bcell, then
+// the step's closing syncs and derived fields.  The nonlinear solve is
+// tightened to ||F|| <= 1e-12 ||F0|| so that its root is pinned closely.
+void hall_step(LunarSolver &s)
+{
+    s.Compute_Timestep();
+    euler_stage(s);
+    s.hall_implicit_.SolveOneStep(s.dt, false);
+    s.calc_Bcell();
+    s.run_data_->dt = s.dt;
+    s.run_data_->time += s.dt;
+    s.run_data_->step += 1;
+    s.lunar_bound_.Sync("Ucell");
+    s.lunar_bound_.Sync("Bface");
+    s.UpdateDerivedFields_();
+}
+
+int cmd_hallrun(Harness &h, const std::string &state, int nsteps, const std::string &prefix)
+{
+    h.load_state(state);
+    LunarSolver &s = *h.solver;
+    s.UpdateDerivedFields_();
+    SNESSetTolerances(s.hall_implicit_.snes_, 1e-30, 1e-12, 1e-30, 200, PETSC_DEFAULT);
+    s.calc_divB();
+    const std::vector<std::string> ehall = {"Ehall_xi", "Ehall_eta", "Ehall_zeta"};
+    dump_state(h, prefix + "_0000.bin", ehall);
+    for (int n = 1; n <= nsteps; ++n)
+    {
+        hall_step(s);
+        s.calc_divB();
+        char buf[32];
+        std::snprintf(buf, sizeof(buf), "_%04d.bin", n);
+        dump_state(h, prefix + buf, ehall);
     }
     return 0;
 }
@@ -663,9 +705,9 @@ int cmd_timerk2(Harness &h, const std::string &state, int nsteps)
     return 0;
 }
 
-// StepOnce followed by the implicit Hall solve (SolveOneStep at the step's dt,
-// Newton rtol 1e-10) and calc_Bcell, `nsteps` times: the step with the Hall
-// solve that HALL_IMPLICIT enables, for timing
+// `nsteps` StepOnce as compiled with HALL_IMPLICIT == 1 (hall_step: the
+// implicit Hall solve at the step's dt, Newton rtol 1e-10, then calc_Bcell,
+// before the closing syncs and derived fields), for timing
 int cmd_timehall(Harness &h, const std::string &state, int nsteps)
 {
     h.load_state(state);
@@ -681,11 +723,7 @@ int cmd_timehall(Harness &h, const std::string &state, int nsteps)
     }
     const auto t0 = std::chrono::steady_clock::now();
     for (int n = 0; n < nsteps; ++n)
-    {
-        s.StepOnce();
-        s.hall_implicit_.SolveOneStep(s.dt, true);
-        s.calc_Bcell();
-    }
+        hall_step(s);
     const auto t1 = std::chrono::steady_clock::now();
     const double sec = std::chrono::duration<double>(t1 - t0).count();
     std::printf("{\"cells\": %lld, \"steps\": %d, \"seconds\": %.9f, \"cell_updates_per_s\": %.6e}\n",
@@ -740,6 +778,8 @@ int main(int argc, char **argv)
             rc = cmd_run(h, argv[2], std::atoi(argv[3]), argv[4]);
         else if (cmd == "rk2" && argc >= 5)
             rc = cmd_rk2(h, argv[2], std::atoi(argv[3]), argv[4]);
+        else if (cmd == "hallrun" && argc >= 5)
+            rc = cmd_hallrun(h, argv[2], std::atoi(argv[3]), argv[4]);
         else if (cmd == "probe" && argc >= 5)
             rc = cmd_probe(h, argv[2], argv[3], argv[4]);
         else if (cmd == "diag" && argc >= 4)
