@@ -556,6 +556,12 @@ def main():
         rs = ctx.resistive_stats()
         res_stats = {"krylov_its_last_step": rs["its"], "rnorm": rs["rnorm"], "bnorm": rs["bnorm"],
                      "reason": rs["reason"], "unknowns": int(len(s.resistive_dofs[0])), "rtol": float(spec.params["implicit_resistive_ksp_rtol"])}
+    hall_stats = None
+    if args.workload in ("c3", "c4"):
+        hs = ctx.hall_stats()
+        hall_stats = {"newton_its_last_step": hs["its"], "gmres_its_last_step": hs["linear_its"],
+                      "fnorm": hs["fnorm"], "fnorm0": hs["fnorm0"], "reason": hs["reason"],
+                      "residual_evaluations_at_least": 1 + hs["its"] + hs["linear_its"]}
     ms_max = max_over_ranks(ms, "cuda")
     value = replica_throughput(world, cells, args.steps, ms_max)
     if fp64_cmp is not None:
@@ -680,6 +686,7 @@ def main():
             "fp64_same_runs": fp64_line,
             "kernels_ms_per_step": {k: round(v, 5) for k, v in sorted(per_step.items(), key=lambda kv: -kv[1])},
             "resistive_solve": res_stats,
+            "hall_solve": hall_stats,
             "cpu_baseline": cpu,
             "clocks": summarize_clocks(clocks),
         }

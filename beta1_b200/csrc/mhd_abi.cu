@@ -139,10 +139,12 @@ const char *const kTuneNames[NTUNE] = {"k_pv_uplus_dt", "k_fluid_ucontra", "k_bc
 // minimum CTAs per SM of each variant (variant 0 first; 0: the compiler's
 // own allocation, no launch bounds) and the number of variants
 // per variant the reported value: the minimum CTAs per SM of its launch
-// bounds (0: none); 12 for the face-tiled k_fluid_mixed (2 CTAs per SM)
-const int kTuneMinCtas[NTUNE][4] = {{4, 0, 5, 0}, {0, 3, 0, 0}, {0, 6, 0, 0}, {0, 6, 0, 0},
+// bounds (0: none); 12 for the face-tiled k_fluid_mixed (2 CTAs per SM), 14
+// for k_pv_uplus_dt with J_cell in a pass of its own (the PV pass at 4)
+const int kTuneMinCtas[NTUNE][4] = {{4, 0, 5, 14}, {0, 3, 0, 0}, {0, 6, 0, 0}, {0, 6, 0, 0},
                                     {0, 6, 0, 0}, {0, 8, 0, 0}, {2, 0, 3, 12}};
-const int kTuneCount[NTUNE] = {3, 2, 2, 2, 2, 2, 4};
+const int kTuneCount[NTUNE] = {4, 2, 2, 2, 2, 2, 4};
+constexpr int kPvSplit = 3; // variant index of k_pv_uplus_dt's split form
 
 // loop bodies of the device-steered implicit Hall solve
 enum
@@ -648,6 +650,16 @@ int ensure_geom(mhd_ctx *ctx)
 // among these independent fields does not change any value.
 int launch_update_derived_pole(mhd_ctx *ctx);
 
+// J_cell's own pass when the derived-field pass runs split (k_pv_uplus_dt variant kPvSplit)
+int launch_jcell_split(mhd_ctx *ctx)
+{
+    if (ctx->tune[TUNE_k_pv_uplus_dt] != kPvSplit)
+        return MHD_OK;
+    prof_begin(ctx, "k_jcell");
+    launch_k_jcell(ctx->pool32 != nullptr, grid_kind(ctx, KIND_CELL0), ctx->stream, ctx->dbv);
+    return launched(ctx);
+}
+
 int launch_update_derived(mhd_ctx *ctx)
 {
     if (!ctx->poles.empty())
@@ -664,6 +676,7 @@ int launch_update_derived(mhd_ctx *ctx)
     RUN(launched(ctx));
     // first ghost layer only: deeper PV / U_plus ghosts are read by no kernel
     // of the step and are filled when read out (materialise_pv)
+    RUN(launch_jcell_split(ctx));
     prof_begin(ctx, "k_pv_uplus_dt");
     launch_k_pv_uplus_dt(ctx->tune[TUNE_k_pv_uplus_dt], ctx->pool32 != nullptr, grid_kind(ctx, KIND_CELL1), s, ctx->dbv,
                          ctx->c, ctx->dt_key, 1, 1);
@@ -694,6 +707,7 @@ int launch_update_derived_pole(mhd_ctx *ctx)
     prof_begin(ctx, "k_arm_dt");
     k_arm_dt<<<1, 128, 0, s>>>(ctx->dt_key, ctx->nruns);
     RUN(launched(ctx));
+    RUN(launch_jcell_split(ctx));
     prof_begin(ctx, "k_pv_uplus_dt");
     launch_k_pv_uplus_dt(ctx->tune[TUNE_k_pv_uplus_dt], ctx->pool32 != nullptr, grid_kind(ctx, KIND_CELL1), s, ctx->dbv,
                          ctx->c, ctx->dt_key, 1, 1);

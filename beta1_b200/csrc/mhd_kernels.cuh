@@ -41,6 +41,8 @@ __global__ void k_eres_explicit(const BlockView *bvs, double inver_Rem);
 void launch_k_bcell(bool w32, dim3 grid, cudaStream_t st, const BlockView *bvs);
 __global__ void k_jedge(const BlockView *bvs, int fB0, int fJ0, double mult, const int *rng);
 __global__ void k_jcell(const BlockView *bvs);
+// J_cell on the inner cells over the flattened KIND_CELL0 grid (w32: FP32 weights)
+void launch_k_jcell(bool w32, dim3 grid, cudaStream_t st, const BlockView *bvs);
 
 // Pole handlers and repairs on eta Poles (mhd_pole.cuh): per Pole a
 // (block, direction) pair in `poles`, one grid row per Pole
@@ -266,8 +268,9 @@ __global__ void k_copy_segments(double *dst, const double *src, const int64_t *s
 // different __launch_bounds__ minimum CTAs per SM; 0 = no launch bounds, the
 // compiler's own allocation); variant 0 is the default.  Returns -1 for an
 // unknown variant.
-// k_pv_uplus_dt: minimum CTAs per SM 4, 0, 5; w32: J_cell from the FP32
-// weight copies (mixed form)
+// k_pv_uplus_dt: minimum CTAs per SM 4, 0, 5, and variant 3: at 4 without
+// J_cell, which launch_k_jcell computes in a pass of its own before it; w32:
+// J_cell from the FP32 weight copies (mixed form)
 int launch_k_pv_uplus_dt(int variant, bool w32, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c,
                          unsigned long long *dt_key, int depth, int with_jcell);
 // k_fluid_ucontra: minimum CTAs per SM 0, 3

@@ -1001,6 +1001,29 @@ __global__ void k_jcell(const BlockView *__restrict__ bvs)
     jcell_one<double>(b, i, j, k);
 }
 
+// J_cell in a pass of its own over the flattened inner-cell grid (the split
+// variant of the derived-field pass: the weight stream with the compiler's
+// own register budget, the PV / CFL pass without it)
+template <typename WT> __global__ void k_jcell_w(const BlockView *__restrict__ bvs)
+{
+    int64_t t;
+    const BlockView &b = bvs[cta_block(bvs, KIND_CELL0, t)];
+    int lo[3], n[3];
+    loc_box(b, LOC_CELL, 0, lo, n);
+    int i, j, k;
+    if (!box_point(lo, n, t, i, j, k))
+        return;
+    jcell_one<WT>(b, i, j, k);
+}
+
+void launch_k_jcell(bool w32, dim3 grid, cudaStream_t st, const BlockView *bvs)
+{
+    if (w32)
+        k_jcell_w<float><<<grid, 256, 0, st>>>(bvs);
+    else
+        k_jcell_w<double><<<grid, 256, 0, st>>>(bvs);
+}
+
 // ---------------------------------------------------------------------------
 // calc_PV + calc_Uplus (LunarSolver_Tools.cpp:58-141) on the inner cells
 // and `depth` ghost layers (the reference covers the whole array) and, on
@@ -1838,6 +1861,10 @@ int launch_pv_variant(int variant, dim3 grid, cudaStream_t st, const BlockView *
         break;
     case 2:
         k_pv_uplus_dt_t<WT, 5><<<grid, 256, 0, st>>>(bvs, c, dt_key, depth, with_jcell);
+        break;
+    case 3:
+        // split: J_cell runs in its own pass (launch_k_jcell) before this one
+        k_pv_uplus_dt_t<WT, 4><<<grid, 256, 0, st>>>(bvs, c, dt_key, depth, 0);
         break;
     default:
         return -1;

@@ -258,14 +258,16 @@ int mhd_set_hall(mhd_ctx *ctx, double hall_coef, const int32_t *zero_boxes, int3
    GMRES(30) with finite-difference Jacobian-vector products.  Stops at
    ||F|| <= max(rtol ||F0||, atol) or after maxit Newton steps (PETSc SNES
    defaults: 1e-8, 1e-50, 50); ksp_rtol / ksp_maxit bound the linear
-   solves.  Needs mhd_set_hall and the "Ehall" sync group.  n = 0 switches
-   it off. */
+   solves.  The solve is steered on the device: in mhd_step its loops are
+   conditional nodes of the step's CUDA graph, with no host round trip.
+   Needs mhd_set_hall and the "Ehall" sync group.  n = 0 switches it off. */
 int mhd_set_hall_implicit(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, int64_t nalias, const int64_t *alias,
                           const int64_t *owner, const double *sign, double rtol, double atol, int32_t maxit,
                           double ksp_rtol, int32_t ksp_maxit);
 
 /* Newton steps, GMRES iterations, final and initial ||F|| and reason
-   (2 atol, 3 rtol, -5 Newton iteration limit) of the last implicit Hall solve. */
+   (2 atol, 3 rtol, -5 Newton iteration limit) of the last implicit Hall solve
+   (read from the device; waits for the context's stream). */
 int mhd_hall_stats(const mhd_ctx *ctx, int32_t *newton_its, int32_t *linear_its, double *fnorm, double *fnorm0,
                    int32_t *reason);
 

@@ -117,6 +117,44 @@ def test_flux_variants_give_the_same_bits(variant):
         assert np.array_equal(res[0][key], res[1][key]), (variant, key)
 
 
+@pytest.mark.parametrize("precision", [mhd.PREC_FP64, mhd.PREC_MIXED])
+def test_split_derived_pass_gives_the_same_bits(precision):
+    """k_pv_uplus_dt variant 14 -- J_cell in a pass of its own before the PV /
+    U_plus / CFL pass -- against the fused default (4), bit for bit, on a
+    batch of uneven shells (the Pole path, whose J_cell ring repair follows
+    the pass) and the tiled slab, in both precisions."""
+    from beta1_b200 import case
+    from conftest import shell_setup
+    g = load_golden("shell_8x6x8_steps.npz")
+    spec0, st0 = shell_setup(g)
+    spec1 = case.shell_case(10, 8, 12, mach_u=6.0)
+    st1 = case.inflow_state(spec1, seed=77)
+    runs = [(spec0, "shell", st0), (spec1, "shell", st1)]
+    out = []
+    for v in (4, 14):
+        bt = solver.Batch([(sp, topo) for sp, topo, _ in runs], precision=precision)
+        bt.ctx.set_tune({"k_pv_uplus_dt": v})
+        bt.load_states([st for _, _, st in runs])
+        bt.step(3)
+        out.append({(r, f): bt.field(r, f) for r in range(2) for f in STATE + ["U_plus", "B_cell", "J_cell"]})
+        out[-1]["dt"] = bt.ctx.get_time()
+        bt.ctx.close()
+    for key in out[0]:
+        assert np.array_equal(np.asarray(out[0][key]), np.asarray(out[1][key])), (precision, key)
+    gs = load_golden("slab_6x5x6_t2x2_r00_steps.npz")
+    spec, st = slab_setup(gs)
+    res = []
+    for v in (4, 14):
+        s = solver.Solver(spec, topology="tiled", precision=precision)
+        s.ctx.set_tune({"k_pv_uplus_dt": v})
+        s.load_state(st)
+        s.step(2)
+        res.append({(f, b): s.field(f, b) for f in STATE + ["J_cell", "PV_H"] for b in range(len(spec.blocks))})
+        s.ctx.close()
+    for key in res[0]:
+        assert np.array_equal(res[0][key], res[1][key]), (precision, key)
+
+
 def test_set_tune_rejects_unknown_variants(golden_periodic):
     from conftest import periodic_setup
     spec, st = periodic_setup(golden_periodic["steps"])

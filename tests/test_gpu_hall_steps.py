@@ -10,7 +10,12 @@ solve tightened to ||F|| <= 1e-12 ||F0||, calc_Bcell, the closing syncs and
 derived fields) on the same restart file.
 
 Every state, derived and intermediate field, the converged Hall EMF and dt
-are compared after each step.  Bound: 1e-10 relative L2 per field (the two
+are compared after each step, except the face EMF Eface_*: the reference's
+Jacobian (its linearised whistler operator, BuildLinearHallFaceEMF_,
+Z4_Lunar/src/implicit/Hall_Implicit_Solver.cpp:964-1080) uses those fields
+as scratch, so after its solve they hold the last linearised Hall face EMF,
+not the step's ideal face EMF; the device, whose products are differences
+of the residual, leaves them as the explicit part wrote them.  Bound: 1e-10 relative L2 per field (the two
 Newton iterations stop at 1e-12 of ||F0|| with different Jacobians, so they
 agree on the root to about that; the rest of the step is the FP64 path of
 the parity tests).  The first step's dt, computed before any solve, is
@@ -26,7 +31,7 @@ pytestmark = pytest.mark.gpu
 
 TOL = 1e-10
 FIELDS = ["U_H", "B_xi", "B_eta", "B_zeta", "PV_H", "U_plus", "B_cell", "Bind_cell", "J_xi", "J_eta", "J_zeta",
-          "J_cell", "E_xi", "E_eta", "E_zeta", "Eface_xi", "Eface_eta", "Eface_zeta", "RHS_H", "RHS_B_xi",
+          "J_cell", "E_xi", "E_eta", "E_zeta", "RHS_H", "RHS_B_xi",
           "RHS_B_eta", "RHS_B_zeta", "Ehall_xi", "Ehall_eta", "Ehall_zeta", "divB"]
 
 
