@@ -132,18 +132,23 @@ enum TuneId
     TUNE_k_curl_e2f,
     TUNE_k_eedge,
     TUNE_k_fluid_mixed,
+    TUNE_k_gmres_resist,
     NTUNE
 };
 const char *const kTuneNames[NTUNE] = {"k_pv_uplus_dt", "k_fluid_ucontra", "k_bcell_jedge", "k_eface",
-                                       "k_curl_e2f",    "k_eedge",         "k_fluid_mixed"};
+                                       "k_curl_e2f",    "k_eedge",         "k_fluid_mixed", "k_gmres_resist"};
 // minimum CTAs per SM of each variant (variant 0 first; 0: the compiler's
 // own allocation, no launch bounds) and the number of variants
 // per variant the reported value: the minimum CTAs per SM of its launch
-// bounds (0: none); 12 for the face-tiled k_fluid_mixed (2 CTAs per SM), 14
-// for k_pv_uplus_dt with J_cell in a pass of its own (the PV pass at 4)
-const int kTuneMinCtas[NTUNE][4] = {{4, 0, 5, 14}, {0, 3, 0, 0}, {0, 6, 0, 0}, {0, 6, 0, 0},
-                                    {0, 6, 0, 0}, {0, 8, 0, 0}, {2, 0, 3, 12}};
-const int kTuneCount[NTUNE] = {4, 2, 2, 2, 2, 2, 4};
+// bounds (0: none); 12 for the face-tiled k_fluid_mixed (2 CTAs per SM), 16
+// for the same with its face states staged in shared memory, 14
+// for k_pv_uplus_dt with J_cell in a pass of its own (the PV pass at 4); for
+// the persistent k_gmres_resist the CTAs of its grid (0: two per SM; fewer
+// CTAs meet at its grid barriers sooner, and a small system needs few)
+const int kTuneMinCtas[NTUNE][5] = {{4, 0, 5, 14, 0}, {0, 3, 0, 0, 0},        {0, 6, 0, 0, 0},
+                                    {0, 6, 0, 0, 0},  {0, 6, 0, 0, 0},        {0, 8, 0, 0, 0},
+                                    {2, 0, 3, 12, 16}, {0, 148, 64, 32, 0}};
+const int kTuneCount[NTUNE] = {4, 2, 2, 2, 2, 2, 5, 4};
 constexpr int kPvSplit = 3; // variant index of k_pv_uplus_dt's split form
 
 // loop bodies of the device-steered implicit Hall solve
@@ -299,7 +304,7 @@ struct mhd_ctx
     int spare_depth = 0;
 
     // register / occupancy variant of each tunable kernel (mhd_autotune)
-    int tune[NTUNE] = {0, 0, 0, 0, 0, 0, 0};
+    int tune[NTUNE] = {0, 0, 0, 0, 0, 0, 0, 0};
 
     // eager profiling: one event pair per launch
     bool profiling = false;
@@ -738,7 +743,7 @@ int launch_fluid_ucontra(mhd_ctx *ctx)
     {
         prof_begin(ctx, "k_fluid_mixed");
         const int var = ctx->tune[TUNE_k_fluid_mixed];
-        launch_k_fluid_mixed(var, grid_kind(ctx, var == 3 ? KIND_TILE1 : KIND_CELL1), ctx->stream, ctx->dbv, ctx->c);
+        launch_k_fluid_mixed(var, grid_kind(ctx, var >= 3 ? KIND_TILE1 : KIND_CELL1), ctx->stream, ctx->dbv, ctx->c);
         return launched(ctx);
     }
     prof_begin(ctx, "k_fluid_ucontra");
@@ -1099,7 +1104,8 @@ int launch_gmres_persistent(mhd_ctx *ctx)
     a.fa = FusedList{R.fa.dst, R.fa.kind, R.fa.idx, R.fa.val, R.fa.blk, R.fa.n};
     a.fb = FusedList{R.fb.dst, R.fb.kind, R.fb.idx, R.fb.val, R.fb.blk, R.fb.n};
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(unsigned(R.pgrid));
+    const int want = kTuneMinCtas[TUNE_k_gmres_resist][ctx->tune[TUNE_k_gmres_resist]];
+    cfg.gridDim = dim3(unsigned(want > 0 ? std::min(want, R.pgrid) : R.pgrid));
     cfg.blockDim = dim3(256);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = ctx->stream;
@@ -3328,6 +3334,9 @@ int mhd_autotune(mhd_ctx *ctx, int32_t reps, int32_t *min_ctas, int32_t n)
     {
         // the flux kernel of the precision in use only
         if ((t == TUNE_k_fluid_mixed && !ctx->pool32) || (t == TUNE_k_fluid_ucontra && ctx->pool32))
+            continue;
+        // the persistent resistive solve's grid, where it runs
+        if (t == TUNE_k_gmres_resist && !(ctx->res.on && ctx->res.pgrid > 0))
             continue;
         int keep = ctx->tune[t];
         for (int v = 0; v < kTuneCount[t] && rc == MHD_OK; ++v)

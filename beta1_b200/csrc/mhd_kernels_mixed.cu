@@ -58,20 +58,35 @@ struct Ref32
 //   energy  U (E + p) - U0 (E0 + p0)      = dU (E + p) + U0 (dE + dp)
 // and the dissipation uses conserved differences of the deviations
 // (rho u - rho0 u0 = drho u + rho0 du).
-__device__ __forceinline__ void rusanov_dev32(const BlockView &b, const Ref32 &r0, float k1, float k2, float k3,
-                                              float area, int64_t p, int64_t pL, float out[5])
+// the FP32 face states of a cell: its planes in the pool (index: the cell's
+// pool offset) or in a tile staged in shared memory (index: its place there)
+struct QPool
 {
-    const int64_t v = b.vol;
-    const float *q = b.q32;
+    const float *q;
+    int64_t v;
+    __device__ __forceinline__ float operator()(int plane, int64_t c) const { return q[plane * v + c]; }
+};
+constexpr int QS_I = TILE_I + 2, QS_J = TILE_J + 2, QS_K = TILE_K + 2; // a tile and one halo cell each side
+constexpr int QS_N = QS_I * QS_J * QS_K;
+struct QTile
+{
+    const float *q;
+    __device__ __forceinline__ float operator()(int plane, int64_t c) const { return q[plane * QS_N + c]; }
+};
+
+template <class Q>
+__device__ __forceinline__ void rusanov_dev32q(const Q &q, const Ref32 &r0, float k1, float k2, float k3, float area,
+                                               int64_t p, int64_t pL, float out[5])
+{
     const float U0 = k1 * r0.u[0] + k2 * r0.u[1] + k3 * r0.u[2];
     float dF[2][5], dC[2][5], rad = 0.0f;
 #pragma unroll
     for (int s = 0; s < 2; ++s)
     {
         const int64_t c = s ? p : pL;
-        const float dr = q[Q32_RHO * v + c];
-        const float du = q[Q32_U * v + c], dv = q[(Q32_U + 1) * v + c], dw = q[(Q32_U + 2) * v + c];
-        const float dp = q[Q32_P * v + c], dE = q[Q32_RHOE * v + c], cs = q[Q32_C * v + c];
+        const float dr = q(Q32_RHO, c);
+        const float du = q(Q32_U, c), dv = q(Q32_U + 1, c), dw = q(Q32_U + 2, c);
+        const float dp = q(Q32_P, c), dE = q(Q32_RHOE, c), cs = q(Q32_C, c);
         const float u = r0.u[0] + du, vv = r0.u[1] + dv, w = r0.u[2] + dw;
         const float dU = k1 * du + k2 * dv + k3 * dw;
         const float U = U0 + dU;
@@ -92,6 +107,12 @@ __device__ __forceinline__ void rusanov_dev32(const BlockView &b, const Ref32 &r
 #pragma unroll
     for (int m = 0; m < 5; ++m)
         out[m] = 0.5f * (dF[0][m] + dF[1][m]) - 0.5f * rad * (dC[1][m] - dC[0][m]);
+}
+
+__device__ __forceinline__ void rusanov_dev32(const BlockView &b, const Ref32 &r0, float k1, float k2, float k3,
+                                              float area, int64_t p, int64_t pL, float out[5])
+{
+    rusanov_dev32q(QPool{b.q32, b.vol}, r0, k1, k2, k3, area, p, pL, out);
 }
 
 // RHS_H of one inner cell from its FP32 flux-deviation sum r: the FP64
@@ -212,38 +233,75 @@ __global__ void k_fluid_mixed_free(const BlockView *__restrict__ bvs, Consts c)
 
 
 // ---------------------------------------------------------------------------
-// Face-tiled variant: a CTA covers TILE_I x TILE_J x TILE_K cells of the
+// Face-tiled variants: a CTA covers TILE_I x TILE_J x TILE_K cells of the
 // depth-1 box (k fastest, one warp per (i, j) row of 32 k).  Every thread
 // forms its cell's contravariant velocities as above; then each face flux
 // needed by an inner cell is evaluated once -- a cell's three low faces by its
 // own thread, the high faces of the tile's last layer in each direction by the
 // threads of that layer -- into shared memory, and after one barrier each
-// inner cell sums its six faces.  The two cells of a face call rusanov_dev32
+// inner cell sums its six faces.  The two cells of a face call the same flux
 // with the same arguments (face metric and area of the face, the two cells'
 // states), so the fluxes and the RHS are bit for bit those of the per-cell
 // variant (the file is compiled without contracted multiply-adds).
+//
+// STAGED: the FP32 face states of the tile and a one-cell halo are copied
+// into shared memory with asynchronous copies issued first thing, which run
+// while the threads form the FP64 contravariant velocities; the fluxes then
+// read them there.  The loads are in flight without holding registers.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, 2) k_fluid_mixed_tile(const BlockView *__restrict__ bvs, Consts c)
+__device__ __forceinline__ void cp_async4(float *dst, const float *src)
+{
+    const unsigned d = unsigned(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;\n" ::: "memory");
+}
+
+template <bool STAGED> __device__ __forceinline__ void k_fluid_mixed_tile_body(const BlockView *__restrict__ bvs, Consts c)
 {
     __shared__ float Fx[TILE_I + 1][TILE_J][TILE_K][5];
     __shared__ float Fy[TILE_I][TILE_J + 1][TILE_K][5];
     __shared__ float Fz[TILE_I][TILE_J][TILE_K + 1][5];
+    __shared__ float qs[STAGED ? 7 * QS_N : 1];
     int64_t t;
     const BlockView &b = bvs[cta_block(bvs, KIND_TILE1, t)];
     const int ntj = (b.nj + 2 + TILE_J - 1) / TILE_J, ntk = (b.nk + 2 + TILE_K - 1) / TILE_K;
     const int64_t tile = t / 256;
     if (tile >= int64_t((b.ni + 2 + TILE_I - 1) / TILE_I) * ntj * ntk)
         return; // the whole CTA
+    const int i0 = -1 + int(tile / (int64_t(ntj) * ntk)) * TILE_I;
+    const int j0 = -1 + int((tile / ntk) % ntj) * TILE_J;
+    const int k0 = -1 + int(tile % ntk) * TILE_K;
+    const int64_t v = b.vol;
+    if (STAGED)
+    {
+        // the tile's cells and one halo cell each side, where the padded
+        // array has them (the halo beyond the box's last cell is never read)
+        const int G = b.G;
+        for (int e = threadIdx.x; e < QS_N; e += blockDim.x)
+        {
+            const int gk = k0 - 1 + e % QS_K, gj = j0 - 1 + (e / QS_K) % QS_J, gi = i0 - 1 + e / (QS_K * QS_J);
+            if (gi < -G || gj < -G || gk < -G || gi > b.ni + G || gj > b.nj + G || gk > b.nk + G)
+                continue;
+            const int64_t gp = pidx(b, gi, gj, gk);
+#pragma unroll
+            for (int m = 0; m < 7; ++m)
+                cp_async4(&qs[m * QS_N + e], &b.q32[m * v + gp]);
+        }
+    }
     const int tk = threadIdx.x & 31, tj = (threadIdx.x >> 5) % TILE_J, ti = (threadIdx.x >> 5) / TILE_J;
-    const int i = -1 + int(tile / (int64_t(ntj) * ntk)) * TILE_I + ti;
-    const int j = -1 + int((tile / ntk) % ntj) * TILE_J + tj;
-    const int k = -1 + int(tile % ntk) * TILE_K + tk;
+    const int i = i0 + ti, j = j0 + tj, k = k0 + tk;
     const bool valid = i <= b.ni && j <= b.nj && k <= b.nk;
     const bool inner = i >= 0 && j >= 0 && k >= 0 && i < b.ni && j < b.nj && k < b.nk;
-    const int64_t v = b.vol;
     const int64_t p = pidx(b, i, j, k);
     const int64_t pp[3] = {pidx(b, i + 1, j, k), pidx(b, i, j + 1, k), pidx(b, i, j, k + 1)};
     const int64_t pm[3] = {pidx(b, i - 1, j, k), pidx(b, i, j - 1, k), pidx(b, i, j, k - 1)};
+    // the same cells in the staged tile
+    const int64_t sp = (int64_t(ti + 1) * QS_J + (tj + 1)) * QS_K + (tk + 1);
+    const int64_t sd[3] = {int64_t(QS_J) * QS_K, QS_K, 1};
     float km[3][3], kp[3][3];
     double S[3] = {0.0, 0.0, 0.0};
     double jac = 0.0;
@@ -274,6 +332,11 @@ __global__ void __launch_bounds__(256, 2) k_fluid_mixed_tile(const BlockView *__
             UC[a * v + p] = (kx * ux + ky * uy + kz * uz) * inv_jac;
         }
     }
+    if (STAGED)
+    {
+        cp_async_wait_all();
+        __syncthreads();
+    }
     const double *q0 = b.qref;
     const Ref32 r0 = {float(q0[0]), {float(q0[1]), float(q0[2]), float(q0[3])}, float(q0[5] + q0[4])};
     const float *g = b.g32;
@@ -297,7 +360,11 @@ __global__ void __launch_bounds__(256, 2) k_fluid_mixed_tile(const BlockView *__
             float F[5];
             if (idx[a] >= 0 && idx[a] <= n[a])
             {
-                rusanov_dev32(b, r0, km[a][0], km[a][1], km[a][2], g[(G32_AREA + a) * v + p], p, pm[a], F);
+                if (STAGED)
+                    rusanov_dev32q(QTile{qs}, r0, km[a][0], km[a][1], km[a][2], g[(G32_AREA + a) * v + p], sp,
+                                   sp - sd[a], F);
+                else
+                    rusanov_dev32(b, r0, km[a][0], km[a][1], km[a][2], g[(G32_AREA + a) * v + p], p, pm[a], F);
                 float *dst = a == 0 ? Fx[ti][tj][tk] : a == 1 ? Fy[ti][tj][tk] : Fz[ti][tj][tk];
 #pragma unroll
                 for (int m = 0; m < 5; ++m)
@@ -306,7 +373,11 @@ __global__ void __launch_bounds__(256, 2) k_fluid_mixed_tile(const BlockView *__
             // the high face of the tile's last layer (the next tile's low face)
             if (last[a] && idx[a] + 1 >= 0 && idx[a] + 1 <= n[a])
             {
-                rusanov_dev32(b, r0, kp[a][0], kp[a][1], kp[a][2], g[(G32_AREA + a) * v + pp[a]], pp[a], p, F);
+                if (STAGED)
+                    rusanov_dev32q(QTile{qs}, r0, kp[a][0], kp[a][1], kp[a][2], g[(G32_AREA + a) * v + pp[a]],
+                                   sp + sd[a], sp, F);
+                else
+                    rusanov_dev32(b, r0, kp[a][0], kp[a][1], kp[a][2], g[(G32_AREA + a) * v + pp[a]], pp[a], p, F);
                 float *dst = a == 0 ? Fx[TILE_I][tj][tk] : a == 1 ? Fy[ti][TILE_J][tk] : Fz[ti][tj][TILE_K];
 #pragma unroll
                 for (int m = 0; m < 5; ++m)
@@ -339,14 +410,28 @@ __global__ void __launch_bounds__(256, 2) k_fluid_mixed_tile(const BlockView *__
     mixed_rhs(b, c, p, jac, S, r);
 }
 
+__global__ void __launch_bounds__(256, 2) k_fluid_mixed_tile(const BlockView *__restrict__ bvs, Consts c)
+{
+    k_fluid_mixed_tile_body<false>(bvs, c);
+}
+
+__global__ void __launch_bounds__(256, 2) k_fluid_mixed_staged(const BlockView *__restrict__ bvs, Consts c)
+{
+    k_fluid_mixed_tile_body<true>(bvs, c);
+}
+
 // launchers of the register / occupancy variants (tuned by mhd_autotune);
-// variant 3 is the face-tiled kernel (KIND_TILE1 grid)
+// variant 3 is the face-tiled kernel, 4 the same with the staged face states
+// (both on the KIND_TILE1 grid)
 int launch_k_fluid_mixed(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c)
 {
     switch (variant)
     {
     case 3:
         k_fluid_mixed_tile<<<grid, 256, 0, st>>>(bvs, c);
+        break;
+    case 4:
+        k_fluid_mixed_staged<<<grid, 256, 0, st>>>(bvs, c);
         break;
     case 0:
         k_fluid_mixed_t<2><<<grid, 256, 0, st>>>(bvs, c);

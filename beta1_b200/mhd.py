@@ -28,9 +28,11 @@ PREC_MIXED = 1
 
 # the default variant of each tunable kernel, in the values mhd_autotune
 # reports (minimum CTAs per SM of its launch bounds, 0: none; 12: the
-# face-tiled k_fluid_mixed)
+# face-tiled k_fluid_mixed, 16: the same with staged face states; 14:
+# k_pv_uplus_dt with J_cell in its own pass;
+# k_gmres_resist: the CTAs of the persistent grid, 0: two per SM)
 DEFAULT_TUNE = {"k_pv_uplus_dt": 4, "k_fluid_ucontra": 0, "k_bcell_jedge": 0, "k_eface": 0, "k_curl_e2f": 0,
-                "k_eedge": 0, "k_fluid_mixed": 2}
+                "k_eedge": 0, "k_fluid_mixed": 2, "k_gmres_resist": 0}
 
 STAGE_TIMESTEP, STAGE_FLUID_RHS, STAGE_INDUCTION, STAGE_UPDATE, STAGE_DIVB, STAGE_HALL_EMF = 1, 2, 3, 4, 5, 6
 STAGE_HALL_SOLVE = 7

@@ -307,8 +307,12 @@ int mhd_set_flux_reference_run(mhd_ctx *ctx, int32_t run, const double prim[5]);
    call does not advance the simulation.  Call it after the state is loaded.
    min_ctas[i] (i < n, at most MHD_NTUNE) receives the chosen minimum CTAs
    per SM of kernel mhd_tune_name(i) (0: no launch bounds, the compiler's own
-   register allocation; 12: the face-tiled k_fluid_mixed). */
-#define MHD_NTUNE 7
+   register allocation; 12: the face-tiled k_fluid_mixed, 16: the same with
+   its FP32 face states staged in shared memory; 14: k_pv_uplus_dt
+   with J_cell in a pass of its own).  For the persistent k_gmres_resist the
+   value is the CTAs of its grid (0: two per SM); its partial sums group
+   differently per grid, so its results agree to round-off, not bitwise. */
+#define MHD_NTUNE 8
 int mhd_autotune(mhd_ctx *ctx, int32_t reps, int32_t *min_ctas, int32_t n);
 const char *mhd_tune_name(int32_t i);
 
@@ -316,7 +320,9 @@ const char *mhd_tune_name(int32_t i);
    (i < n) in the values mhd_autotune reports, e.g. one it returned in an
    earlier run.  For k_fluid_mixed the value 12 selects the face-tiled kernel
    (each face flux evaluated once per 2 x 4 x 32-cell tile and shared
-   through shared memory; the same bits as the per-cell variants).
+   through shared memory; the same bits as the per-cell variants), 16 the
+   same with the tile's FP32 face states copied into shared memory by
+   asynchronous copies first.
    MHD_EINVAL for a value that names no variant. */
 int mhd_set_tune(mhd_ctx *ctx, const int32_t *min_ctas, int32_t n);
 

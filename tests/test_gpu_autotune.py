@@ -24,7 +24,7 @@ def test_tuned_context_matches_reference(fname, tol):
     s.load_state(st)
     chosen = s.ctx.autotune(reps=3)
     assert set(chosen) == {"k_pv_uplus_dt", "k_fluid_ucontra", "k_bcell_jedge", "k_eface", "k_curl_e2f", "k_eedge",
-                           "k_fluid_mixed"}
+                           "k_fluid_mixed", "k_gmres_resist"}
     # minimum CTAs per SM of the chosen variant (0: no launch bounds)
     assert all(v >= 0 for v in chosen.values())
     nb = len(spec.blocks)
@@ -79,11 +79,13 @@ def test_tuning_leaves_the_implicit_hall_start_untouched():
         assert np.array_equal(out[0][key], out[1][key]), key
 
 
-@pytest.mark.parametrize("variant", [12, 0, 3])
+@pytest.mark.parametrize("variant", [12, 16, 0, 3])
 def test_flux_variants_give_the_same_bits(variant):
     """The mixed flux pass in each of its variants -- the face-tiled kernel
     (12: every face flux evaluated once per tile, shared through shared
-    memory) and the per-cell kernel under other launch bounds -- against the
+    memory; 16: the same with the tile's face states staged in shared memory
+    by asynchronous copies) and the per-cell kernel under other launch
+    bounds -- against the
     default per-cell variant, bit for bit, on a batch of uneven shells and a
     slab (tiles cut the blocks at every alignment)."""
     from beta1_b200 import case
