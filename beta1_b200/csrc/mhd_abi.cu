@@ -695,19 +695,29 @@ int launch_update_derived(mhd_ctx *ctx)
 // UpdateDerivedFields_ with Poles, in the reference's order: calc_Bcell and
 // Sync("B_cell"), the B_zeta rewrite of the first cell layer at each Pole
 // (which the J edges then read), Calc_J_Edge and Sync("Jedge"), then J_cell
-// (with PV / U_plus / the CFL bound), its pole-shell repair, and the syncs
+// (with PV / U_plus / the CFL bound), its pole-shell repair, and the syncs.
+// B_cell and the J edges run as one pass before the rewrite; the few J edges
+// that read a rewritten face are formed again after it (k_pole_jedge).
 int launch_update_derived_pole(mhd_ctx *ctx)
 {
     cudaStream_t s = ctx->stream;
-    prof_begin(ctx, "k_bcell");
-    launch_k_bcell(ctx->pool32 != nullptr, dim3(grid_for(max_box(ctx, LOC_CELL, 0)), unsigned(ctx->nblocks)), s,
-                   ctx->dbv);
+    prof_begin(ctx, "k_bcell_jedge");
+    launch_k_bcell_jedge(ctx->tune[TUNE_k_bcell_jedge], ctx->pool32 != nullptr, grid_kind(ctx, KIND_STAG), s, ctx->dbv);
     RUN(launched(ctx));
     RUN(run_sync(ctx, "B_cell"));
     RUN(launch_pole(ctx, POLE_BZETA));
-    prof_begin(ctx, "k_jedge");
-    k_jedge<<<grid_kind(ctx, KIND_STAG), kThreads, 0, s>>>(ctx->dbv, F_Bxi, F_Jxi, 1.0, nullptr);
-    RUN(launched(ctx));
+    {
+        const int np = int(ctx->poles.size() / 2);
+        int64_t w = 0;
+        for (int q = 0; q < np; ++q)
+        {
+            const BlockView &v = ctx->hbv[size_t(ctx->poles[size_t(2 * q)])];
+            w = std::max<int64_t>(w, int64_t(v.ni + 1) * 2 * (v.nk + 1));
+        }
+        prof_begin(ctx, "k_jedge");
+        k_pole_jedge<<<dim3(grid_for(w), unsigned(np)), kThreads, 0, s>>>(ctx->dbv, ctx->dpoles);
+        RUN(launched(ctx));
+    }
     RUN(run_sync(ctx, "Jedge"));
     prof_begin(ctx, "k_arm_dt");
     k_arm_dt<<<1, 128, 0, s>>>(ctx->dt_key, ctx->nruns);

@@ -47,6 +47,9 @@ void launch_k_jcell(bool w32, dim3 grid, cudaStream_t st, const BlockView *bvs);
 // Pole handlers and repairs on eta Poles (mhd_pole.cuh): per Pole a
 // (block, direction) pair in `poles`, one grid row per Pole
 __global__ void k_pole(const BlockView *bvs, const int *poles, int op);
+// Calc_J_Edge again on the J_xi / J_eta edges that read the B_zeta faces
+// POLE_BZETA rewrote (staggered layers jc, jc + 1 of each Pole; grid.y: Poles)
+__global__ void k_pole_jedge(const BlockView *bvs, const int *poles);
 // one Pole operation over every Pole (work items per Pole: pole_work); the
 // ring least squares run one warp per ring, with their geometry-only normal
 // matrices in `cache` (per Pole, per least-squares operation, `stride`

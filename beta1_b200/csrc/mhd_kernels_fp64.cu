@@ -2055,6 +2055,29 @@ __global__ void k_pole(const BlockView *__restrict__ bvs, const int *__restrict_
     pole_one(b, side, op, int64_t(blockIdx.x) * blockDim.x + threadIdx.x);
 }
 
+// The J edges that read a B_zeta face the Pole rewrite changed (POLE_BZETA
+// writes the first cell layer jc at each Pole: J_xi at j = jc, jc + 1 and
+// J_eta at j = jc read it): Calc_J_Edge again on the staggered points
+// j = jc, jc + 1 of each Pole, after the rewrite.  Every other J edge was
+// formed before the rewrite, in the fused B_cell / J-edge pass, from the
+// same faces, so the J edges are those of the reference's order (calc_Bcell
+// with the rewrite, then Calc_J_Edge) bit for bit.  Work items per Pole:
+// (ni + 1) x 2 x (nk + 1).
+__global__ void k_pole_jedge(const BlockView *__restrict__ bvs, const int *__restrict__ poles)
+{
+    const BlockView &b = bvs[poles[2 * blockIdx.y]];
+    const int side = poles[2 * blockIdx.y + 1] > 0 ? 1 : -1;
+    const int jc = side < 0 ? 0 : b.nj - 1;
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= int64_t(b.ni + 1) * 2 * (b.nk + 1))
+        return;
+    const int k = int(t % (b.nk + 1)), j = jc + int((t / (b.nk + 1)) % 2), i = int(t / (2 * int64_t(b.nk + 1)));
+#pragma unroll
+    for (int ea = 0; ea < 2; ++ea)
+        if (inner_of(b, 1, ea, i, j, k))
+            jedge_one(b, ea, i, j, k, F_Bxi, F_Jxi, 1.0);
+}
+
 // ---------------------------------------------------------------------------
 // The ring least squares of POLE_BCELL, POLE_EETA_REG and POLE_JCELL with one
 // warp per ring.  The lanes form the pushed vectors and values of 32 k at a
