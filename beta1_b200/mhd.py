@@ -342,7 +342,7 @@ class Context:
         """times the register / occupancy variants of the hot kernels on the
         current state and keeps the fastest; returns kernel -> chosen minimum
         CTAs per SM"""
-        n = 7
+        n = len(DEFAULT_TUNE)
         out = (C.c_int32 * n)()
         self._check(self.lib.mhd_autotune(self.h, int(reps), out, n), "autotune")
         return {self.lib.mhd_tune_name(i).decode(): int(out[i]) for i in range(n)}

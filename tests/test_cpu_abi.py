@@ -55,6 +55,14 @@ def test_kernel_names_and_errors_without_gpu(lib):
     assert lib.mhd_update_derived(None) == 1
 
 
+def test_tunable_kernels_match_the_python_defaults(lib):
+    # every tunable kernel of the library has a default variant on the Python
+    # side, in the library's order, and no more
+    names = [lib.mhd_tune_name(i) for i in range(len(mhd.DEFAULT_TUNE) + 1)]
+    assert [n.decode() for n in names[:-1]] == list(mhd.DEFAULT_TUNE)
+    assert names[-1] is None
+
+
 def test_host_layout_point_ids(lib):
     lay = mhd.HostLayout([(8, 6, 5), (4, 4, 4)])
     info = lay.field_info("B_eta", 1)
