@@ -204,15 +204,16 @@ def workload_name(name, mixed):
     return base + ("_mixed" if mixed else "_fp64")
 
 
-def build_case(workload, n=64, size=(96, 48)):
+def build_case(workload, n=64, size=(96, 48), hall_size=(128, 64)):
     """(spec, restart state, topology, interior cells) of a workload; size:
-    (radial, transverse) cells per block of the c2 slab."""
+    (radial, transverse) cells per block of the c2 slab, hall_size the same
+    for c3 / c4."""
     from beta1_b200 import case
     if workload == "c1":
         spec = case.periodic_box_case((n, n, n))
         return spec, case.initial_state(spec), "periodic", n ** 3
     if workload in ("c3", "c4"):
-        spec = case.slab_case(128, (64, 64), (3, 2))
+        spec = case.slab_case(hall_size[0], (hall_size[1], hall_size[1]), (3, 2))
         cells = sum(b.ncell[0] * b.ncell[1] * b.ncell[2] for b in spec.blocks)
         return spec, case.inflow_state(spec), "tiled", cells
     sc = case.ref_scales()
@@ -450,6 +451,9 @@ def main():
     ap.add_argument("--n", type=int, default=64, help="cells per direction of the c1 periodic block")
     ap.add_argument("--c2-size", default="96x48", help="radial x transverse cells per c2 block (profiling runs "
                                                          "use a smaller case; the bench line is quoted on 96x48)")
+    ap.add_argument("--hall-size", default="128x64", help="radial x transverse cells per c3 / c4 block (profiling "
+                                                            "runs use a smaller case; the bench line is quoted on "
+                                                            "128x64)")
     ap.add_argument("--ref-steps", type=int, default=None, help="StepOnce per reference CPU sample")
     ap.add_argument("--e2e-iters", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -513,7 +517,8 @@ def main():
         del host
     else:
         c2size = tuple(int(v) for v in args.c2_size.split("x"))
-        spec, st, topology, cells = build_case(args.workload, args.n, c2size)
+        hallsize = tuple(int(v) for v in args.hall_size.split("x"))
+        spec, st, topology, cells = build_case(args.workload, args.n, c2size, hallsize)
         s = solver.Solver(spec, topology=topology, precision=prec, geometry_on=geometry_on)
         if args.workload in ("c3", "c4"):
             # bounded: at most 10 Newton steps of at most 200 GMRES iterations per time step
@@ -654,6 +659,8 @@ def main():
 
     config_name = workload_name(wl["name"] if args.workload != "c2" or args.c2_size == "96x48" else
                                 "c2_slab6x%sx%s_implicit_resistive_fp64" % (args.c2_size, args.c2_size.split("x")[1]), mixed)
+    if args.workload in ("c3", "c4") and args.hall_size != "128x64":
+        config_name = config_name.replace("128x64x64", "%sx%s" % (args.hall_size, args.hall_size.split("x")[1]))
     if sweep and len(runs) != SWEEP_RUNS:
         config_name = config_name.replace("sweep48", "sweep%d" % len(runs))
     if rank == 0:

@@ -368,35 +368,49 @@ __device__ void hall_newton_test(HallCtl *c, cudaGraphConditionalHandle h, int u
     set_cond(h, use, go);
 }
 
-// Adds acc[c], c < nv, over the grid in a fixed order (warp shuffles, the
-// CTA's warps in order, then the last CTA adds the CTAs' partials in order),
-// so every pass is reproducible.  nv is uniform over the grid.
-__device__ void mdot_finish(double (&acc)[kMdMax], int nv, double *__restrict__ partial, double *__restrict__ out,
-                            unsigned *__restrict__ done)
+// Grid reductions in a fixed order, so every pass is reproducible: each CTA
+// adds its threads' sums (warp shuffles, then the warps in order) into one
+// partial per product; the last CTA to finish adds the partials in CTA
+// order.  Products are taken in chunks of at most kChunk per pass over the
+// vectors (registers per thread stay bounded whatever the basis size).
+constexpr int kChunk = 8;
+
+// the CTA's partial sums of products c0 + q (q < N, c0 + q < nd)
+template <int N>
+__device__ __forceinline__ void block_partials(const double (&acc)[N], int c0, int nd, double *__restrict__ partial)
 {
     constexpr int kWarps = kRedThreads / 32;
-    __shared__ double red[kMdMax][kWarps];
-    __shared__ bool last;
+    __shared__ double red[N][kWarps];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-    for (int c = 0; c < kMdMax; ++c)
-        if (c < nv)
+    for (int q = 0; q < N; ++q)
+        if (c0 + q < nd)
         {
-            double v = acc[c];
+            double v = acc[q];
             for (int o = 16; o > 0; o >>= 1)
                 v += __shfl_down_sync(0xffffffffu, v, o);
             if (lane == 0)
-                red[c][wid] = v;
+                red[q][wid] = v;
         }
     __syncthreads();
-    if (int(threadIdx.x) < nv)
+    if (int(threadIdx.x) < N && c0 + int(threadIdx.x) < nd)
     {
         double s = 0.0;
         for (int w = 0; w < kWarps; ++w)
             s += red[threadIdx.x][w];
-        partial[int64_t(threadIdx.x) * gridDim.x + blockIdx.x] = s;
-        __threadfence();
+        partial[int64_t(c0 + int(threadIdx.x)) * gridDim.x + blockIdx.x] = s;
     }
+    __syncthreads();
+}
+
+// out[c] for c < nd from the CTAs' partials, by the last CTA to arrive
+__device__ void grid_finish(int nd, const double *__restrict__ partial, double *__restrict__ out,
+                            unsigned *__restrict__ done)
+{
+    constexpr int kWarps = kRedThreads / 32;
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __threadfence();
     __syncthreads();
     if (threadIdx.x == 0)
         last = (atomicAdd(done, 1u) == gridDim.x - 1);
@@ -404,7 +418,7 @@ __device__ void mdot_finish(double (&acc)[kMdMax], int nv, double *__restrict__ 
     if (!last)
         return;
     __threadfence();
-    for (int c = wid; c < nv; c += kWarps)
+    for (int c = wid; c < nd; c += kWarps)
     {
         double s = 0.0;
         for (int b = lane; b < int(gridDim.x); b += 32)
@@ -543,20 +557,31 @@ __global__ void __launch_bounds__(kRedThreads) k_hall_jv_dots(const double *__re
 {
     const int nv = st->j + 1;
     const double hh = h[0];
-    double acc[kMdMax];
-#pragma unroll
-    for (int c = 0; c < kMdMax; ++c)
-        acc[c] = 0.0;
-    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x)
+    const int64_t t0 = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, ts = int64_t(gridDim.x) * blockDim.x;
+    for (int c0 = 0; c0 < nv; c0 += kChunk)
     {
-        const double wt = ((Xt[t] - pool[e[t]]) - F[t]) / hh;
-        w[t] = wt;
+        double acc[kChunk];
 #pragma unroll
-        for (int c = 0; c < kMdMax; ++c)
-            if (c < nv)
-                acc[c] += V[int64_t(c) * ldv + t] * wt;
+        for (int q = 0; q < kChunk; ++q)
+            acc[q] = 0.0;
+        for (int64_t t = t0; t < n; t += ts)
+        {
+            double wt;
+            if (c0 == 0)
+            {
+                wt = ((Xt[t] - pool[e[t]]) - F[t]) / hh;
+                w[t] = wt;
+            }
+            else
+                wt = w[t];
+#pragma unroll
+            for (int q = 0; q < kChunk; ++q)
+                if (c0 + q < nv)
+                    acc[q] += V[int64_t(c0 + q) * ldv + t] * wt;
+        }
+        block_partials(acc, c0, nv, partial);
     }
-    mdot_finish(acc, nv, partial, out, done);
+    grid_finish(nv, partial, out, done);
 }
 
 __global__ void __launch_bounds__(kRedThreads) k_hall_proj_dots(const double *__restrict__ V, int64_t ldv,
@@ -570,26 +595,46 @@ __global__ void __launch_bounds__(kRedThreads) k_hall_proj_dots(const double *__
     if (int(threadIdx.x) < nv)
         hs[threadIdx.x] = st->hcol[threadIdx.x];
     __syncthreads();
-    double acc[kMdMax];
-#pragma unroll
-    for (int c = 0; c < kMdMax; ++c)
-        acc[c] = 0.0;
-    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x)
+    const int64_t t0 = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, ts = int64_t(gridDim.x) * blockDim.x;
+    // the subtraction, the first chunk of products and w . w in one pass
     {
-        double wt = w[t];
+        double acc[kChunk], self[1] = {0.0};
 #pragma unroll
-        for (int c = 0; c < kMdMax; ++c)
-            if (c < nv)
+        for (int q = 0; q < kChunk; ++q)
+            acc[q] = 0.0;
+        for (int64_t t = t0; t < n; t += ts)
+        {
+            double wt = w[t];
+#pragma unroll 4
+            for (int c = 0; c < nv; ++c)
                 wt -= hs[c] * V[int64_t(c) * ldv + t];
-        w[t] = wt;
+            w[t] = wt;
+            self[0] += wt * wt;
 #pragma unroll
-        for (int c = 0; c < kMdMax; ++c)
-            if (c < nv)
-                acc[c] += V[int64_t(c) * ldv + t] * wt;
-            else if (c == nv)
-                acc[c] += wt * wt;
+            for (int q = 0; q < kChunk; ++q)
+                if (q < nv)
+                    acc[q] += V[int64_t(q) * ldv + t] * wt;
+        }
+        block_partials(acc, 0, nv, partial);
+        block_partials(self, nv, nv + 1, partial);
     }
-    mdot_finish(acc, nv + 1, partial, out, done);
+    for (int c0 = kChunk; c0 < nv; c0 += kChunk)
+    {
+        double acc[kChunk];
+#pragma unroll
+        for (int q = 0; q < kChunk; ++q)
+            acc[q] = 0.0;
+        for (int64_t t = t0; t < n; t += ts)
+        {
+            const double wt = w[t];
+#pragma unroll
+            for (int q = 0; q < kChunk; ++q)
+                if (c0 + q < nv)
+                    acc[q] += V[int64_t(c0 + q) * ldv + t] * wt;
+        }
+        block_partials(acc, c0, nv, partial);
+    }
+    grid_finish(nv + 1, partial, out, done);
 }
 
 __global__ void k_hall_next(double *__restrict__ V, int64_t ldv, const double *__restrict__ w,
@@ -613,17 +658,15 @@ __global__ void __launch_bounds__(kRedThreads) k_hall_res_dots(const double *__r
                                                                int64_t n, double *__restrict__ partial,
                                                                double *__restrict__ out, unsigned *__restrict__ done)
 {
-    double acc[kMdMax];
-#pragma unroll
-    for (int c = 0; c < kMdMax; ++c)
-        acc[c] = 0.0;
+    double acc[1] = {0.0};
     for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x)
     {
         const double f = Xt[t] - pool[e[t]];
         Ft[t] = f;
         acc[0] += f * f;
     }
-    mdot_finish(acc, 1, partial, out, done);
+    block_partials(acc, 0, 1, partial);
+    grid_finish(1, partial, out, done);
 }
 
 __global__ void k_hall_restart_r(const double *__restrict__ pool, const uint64_t *__restrict__ e,
@@ -643,10 +686,7 @@ __global__ void __launch_bounds__(kRedThreads) k_hall_gmres_prologue(const doubl
                                                                      double *__restrict__ out,
                                                                      unsigned *__restrict__ done)
 {
-    double acc[kMdMax];
-#pragma unroll
-    for (int c = 0; c < kMdMax; ++c)
-        acc[c] = 0.0;
+    double acc[1] = {0.0};
     for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x)
     {
         const double v = -F[t];
@@ -655,20 +695,19 @@ __global__ void __launch_bounds__(kRedThreads) k_hall_gmres_prologue(const doubl
         dx[t] = 0.0;
         acc[0] += v * v;
     }
-    mdot_finish(acc, 1, partial, out, done);
+    block_partials(acc, 0, 1, partial);
+    grid_finish(1, partial, out, done);
 }
 
 __global__ void __launch_bounds__(kRedThreads) k_norm2(const double *__restrict__ x, int64_t n,
                                                        double *__restrict__ partial, double *__restrict__ out,
                                                        unsigned *__restrict__ done)
 {
-    double acc[kMdMax];
-#pragma unroll
-    for (int c = 0; c < kMdMax; ++c)
-        acc[c] = 0.0;
+    double acc[1] = {0.0};
     for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x)
         acc[0] += x[t] * x[t];
-    mdot_finish(acc, 1, partial, out, done);
+    block_partials(acc, 0, 1, partial);
+    grid_finish(1, partial, out, done);
 }
 
 __global__ void k_hall_take(double *__restrict__ X, const double *__restrict__ Xt, double *__restrict__ F,
