@@ -278,6 +278,12 @@ struct mhd_ctx
         double *bstar = nullptr;                   // snapshot of the face B arrays (one range per block)
         int64_t *seg_snap = nullptr, *seg_restore = nullptr; // per block: dst offset, src offset, length
         int copy_ctas = 1;
+        const double **bs = nullptr;               // per block: the snapshot's B_xi, B_eta, B_zeta
+        // trials read B* from the snapshot instead of restoring it: exact when
+        // Sync("Bface") writes every destination from points no trial writes
+        // (no staged copies, no wall handler), so the points neither the curl
+        // nor the sync writes keep B*
+        bool from_snapshot = false;
         double *X = nullptr, *F = nullptr, *Xt = nullptr, *Ft = nullptr, *dx = nullptr, *b = nullptr, *r = nullptr;
         double *V = nullptr, *w = nullptr, *partial = nullptr, *dots = nullptr;
         unsigned *done = nullptr;                  // CTAs finished in a reduction pass
@@ -1325,13 +1331,18 @@ int hall_emf_from_current_b(mhd_ctx *ctx)
 int hall_trial_b(mhd_ctx *ctx)
 {
     auto &H = ctx->hall;
-    RUN(hall_copy_b(ctx, false));
+    if (!H.from_snapshot)
+        RUN(hall_copy_b(ctx, false));
     if (H.nalias > 0)
         LAUNCHN(k_alias_copy, H.nalias, ctx->pool, H.alias, H.owner, H.sign, H.nalias);
     RUN(run_sync(ctx, "Ehall", true));
     prof_begin(ctx, "k_curl_e2f");
-    launch_k_curl_e2f(ctx->tune[TUNE_k_curl_e2f], dim3(grid_for(max_stagger(ctx)), ctx->nblocks), ctx->stream,
-                      ctx->dbv, F_Ehxi, F_RBxi, F_Bxi, -1.0, ctx->dt, 1.0, 0, nullptr);
+    if (H.from_snapshot)
+        k_curl_from_snapshot<<<grid_kind(ctx, KIND_STAG), kThreads, 0, ctx->stream>>>(ctx->dbv, F_Ehxi, F_RBxi, F_Bxi,
+                                                                                      -1.0, ctx->dt, H.bs);
+    else
+        launch_k_curl_e2f(ctx->tune[TUNE_k_curl_e2f], dim3(grid_for(max_stagger(ctx)), ctx->nblocks), ctx->stream,
+                          ctx->dbv, F_Ehxi, F_RBxi, F_Bxi, -1.0, ctx->dt, 1.0, 0, nullptr);
     RUN(launched(ctx));
     return run_sync(ctx, "Bface");
 }
@@ -1438,6 +1449,11 @@ int launch_hall_implicit(mhd_ctx *ctx)
     if (!H.on || H.n == 0)
         return MHD_OK;
     RUN(build_all_syncs(ctx));
+    {
+        const auto it = ctx->syncs.find("Bface");
+        H.from_snapshot = it != ctx->syncs.end() && it->second.built && it->second.full.tmp == nullptr &&
+                          it->second.walls.empty() && ctx->poles.empty();
+    }
     RUN(hall_copy_b(ctx, true));
     LAUNCHN(k_pack_vec, H.n, ctx->pool, H.e, H.X, H.n);
     // F of the initial guess (the unknowns in the pool are X already)
@@ -3119,7 +3135,7 @@ int mhd_set_hall_implicit(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, int6
     for (void *p : {(void *)H.e, (void *)H.alias, (void *)H.owner, (void *)H.sign, (void *)H.bstar, (void *)H.X,
                     (void *)H.F, (void *)H.Xt, (void *)H.Ft, (void *)H.dx, (void *)H.b, (void *)H.r, (void *)H.V,
                     (void *)H.w, (void *)H.partial, (void *)H.dots, (void *)H.st, (void *)H.ctl, (void *)H.done,
-                    (void *)H.seg_snap, (void *)H.seg_restore})
+                    (void *)H.seg_snap, (void *)H.seg_restore, (void *)H.bs})
         cudaFree(p);
     H = mhd_ctx::HallImplicit();
     drop_graph(ctx);
@@ -3172,6 +3188,15 @@ int mhd_set_hall_implicit(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, int6
     RUN(upload_vec(ctx, snap, &H.seg_snap));
     RUN(upload_vec(ctx, restore, &H.seg_restore));
     CK(ctx, cudaMalloc(&H.bstar, nbs * 8));
+    {
+        std::vector<const double *> bsp;
+        for (int b = 0; b < ctx->nblocks; ++b)
+            for (int f = F_Bxi; f <= F_Bzeta; ++f)
+                bsp.push_back(H.bstar + snap[size_t(3 * b)] +
+                              (int64_t(ctx->base[size_t(f)][size_t(b)]) - int64_t(ctx->base[F_Bxi][size_t(b)])));
+        CK(ctx, cudaMalloc(&H.bs, bsp.size() * sizeof(double *)));
+        CK(ctx, cudaMemcpy(H.bs, bsp.data(), bsp.size() * sizeof(double *), cudaMemcpyHostToDevice));
+    }
     const size_t nn = size_t(H.n);
     for (double **p : {&H.X, &H.F, &H.Xt, &H.Ft, &H.dx, &H.b, &H.r, &H.w})
         CK(ctx, cudaMalloc(p, nn * 8));

@@ -41,6 +41,10 @@ __global__ void k_eres_explicit(const BlockView *bvs, double inver_Rem);
 void launch_k_bcell(bool w32, dim3 grid, cudaStream_t st, const BlockView *bvs);
 __global__ void k_jedge(const BlockView *bvs, int fB0, int fJ0, double mult, const int *rng);
 __global__ void k_jcell(const BlockView *bvs);
+// RHS = mult curl E and B = B* + dt RHS on the inner faces, B* from a snapshot
+// (bs[3 * block + axis]: the snapshot's B arrays of each block, pool layout)
+__global__ void k_curl_from_snapshot(const BlockView *bvs, int fE0, int fR0, int fB0, double mult, const double *dtp,
+                                     const double *const *bs);
 // J_cell on the inner cells over the flattened KIND_CELL0 grid (w32: FP32 weights)
 void launch_k_jcell(bool w32, dim3 grid, cudaStream_t st, const BlockView *bvs);
 

@@ -515,6 +515,41 @@ __device__ __forceinline__ void curl_point(const BlockView &b, int fE0, int fR0,
     }
 }
 
+// The implicit Hall trial's face update from the snapshot B*: on the inner
+// faces RHS = mult curl E and B = B* + dt RHS, B* read from its snapshot (bs:
+// per block the B*_xi, B*_eta, B*_zeta arrays, in the pool's point layout).
+// The same operands and operations as restoring B = B* and then B += dt RHS,
+// so the same bits, without the copy.
+__global__ void k_curl_from_snapshot(const BlockView *__restrict__ bvs, int fE0, int fR0, int fB0, double mult,
+                                     const double *__restrict__ dtp, const double *const *__restrict__ bs)
+{
+    int64_t t;
+    const int bi = cta_block(bvs, KIND_STAG, t);
+    const BlockView &b = bvs[bi];
+    int i, j, k;
+    if (!stagger_point(b, nullptr, 0, t, i, j, k))
+        return;
+    const double dtB = dtp[b.run] / 1.0;
+    const double *Ex = b.f[fE0], *Ee = b.f[fE0 + 1], *Ez = b.f[fE0 + 2];
+    const int64_t p = pidx(b, i, j, k);
+#pragma unroll
+    for (int fa = 0; fa < 3; ++fa)
+    {
+        if (!inner_of(b, 0, fa, i, j, k))
+            continue;
+        double curl;
+        if (fa == 0)
+            curl = (Ee[p] - Ee[pidx(b, i, j, k + 1)]) + (Ez[pidx(b, i, j + 1, k)] - Ez[p]);
+        else if (fa == 1)
+            curl = (Ex[pidx(b, i, j, k + 1)] - Ex[p]) + (Ez[p] - Ez[pidx(b, i + 1, j, k)]);
+        else
+            curl = (Ex[p] - Ex[pidx(b, i, j + 1, k)]) + (Ee[pidx(b, i + 1, j, k)] - Ee[p]);
+        const double rhs = mult * curl;
+        b.f[fR0 + fa][p] = rhs;
+        b.f[fB0 + fa][p] = bs[3 * bi + fa][p] + dtB * rhs;
+    }
+}
+
 // the discrete curl curl_point forms on face axis fa at (i, j, k)
 __device__ __forceinline__ double face_curl(const BlockView &b, int fE0, int fa, int i, int j, int k)
 {
