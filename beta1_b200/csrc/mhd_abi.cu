@@ -133,22 +133,25 @@ enum TuneId
     TUNE_k_eedge,
     TUNE_k_fluid_mixed,
     TUNE_k_gmres_resist,
+    TUNE_k_hall_edge,
     NTUNE
 };
-const char *const kTuneNames[NTUNE] = {"k_pv_uplus_dt", "k_fluid_ucontra", "k_bcell_jedge", "k_eface",
-                                       "k_curl_e2f",    "k_eedge",         "k_fluid_mixed", "k_gmres_resist"};
+const char *const kTuneNames[NTUNE] = {"k_pv_uplus_dt", "k_fluid_ucontra", "k_bcell_jedge",  "k_eface",
+                                       "k_curl_e2f",    "k_eedge",         "k_fluid_mixed",  "k_gmres_resist",
+                                       "k_hall_edge"};
 // minimum CTAs per SM of each variant (variant 0 first; 0: the compiler's
 // own allocation, no launch bounds) and the number of variants
 // per variant the reported value: the minimum CTAs per SM of its launch
 // bounds (0: none); 12 for the face-tiled k_fluid_mixed (2 CTAs per SM), 16
 // for the same with its face states staged in shared memory, 14
 // for k_pv_uplus_dt with J_cell in a pass of its own (the PV pass at 4); for
-// the persistent k_gmres_resist the CTAs of its grid (0: two per SM; fewer
-// CTAs meet at its grid barriers sooner, and a small system needs few)
+// the persistent k_gmres_resist the CTAs of its grid (0: two per SM); for
+// k_hall_edge 2 selects the form that reads the seven cells of a staggered
+// point once
 const int kTuneMinCtas[NTUNE][5] = {{4, 0, 5, 14, 0}, {0, 3, 0, 0, 0},        {0, 6, 0, 0, 0},
                                     {0, 6, 0, 0, 0},  {0, 6, 0, 0, 0},        {0, 8, 0, 0, 0},
-                                    {2, 0, 3, 12, 16}, {0, 148, 64, 32, 0}};
-const int kTuneCount[NTUNE] = {4, 2, 2, 2, 2, 2, 5, 4};
+                                    {2, 0, 3, 12, 16}, {0, 148, 64, 32, 0},   {0, 2, 0, 0, 0}};
+const int kTuneCount[NTUNE] = {4, 2, 2, 2, 2, 2, 5, 4, 2};
 constexpr int kPvSplit = 3; // variant index of k_pv_uplus_dt's split form
 
 // loop bodies of the device-steered implicit Hall solve
@@ -310,7 +313,7 @@ struct mhd_ctx
     int spare_depth = 0;
 
     // register / occupancy variant of each tunable kernel (mhd_autotune)
-    int tune[NTUNE] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int tune[NTUNE] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 
     // eager profiling: one event pair per launch
     bool profiling = false;
@@ -1321,7 +1324,7 @@ int hall_emf_from_current_b(mhd_ctx *ctx)
                                                                                         ctx->hall_coef);
     RUN(launched(ctx));
     prof_begin(ctx, "k_hall_edge");
-    k_hall_edge<<<dim3(grid_for(max_stagger(ctx)), nb), kThreads, 0, s>>>(ctx->dbv, ctx->hall_zb, ctx->hall_nzb);
+    launch_k_hall_edge(ctx->tune[TUNE_k_hall_edge], grid_kind(ctx, KIND_STAG), s, ctx->dbv, ctx->hall_zb, ctx->hall_nzb);
     return launched(ctx);
 }
 
@@ -3373,6 +3376,9 @@ int mhd_autotune(mhd_ctx *ctx, int32_t reps, int32_t *min_ctas, int32_t n)
         // the persistent resistive solve's grid, where it runs
         if (t == TUNE_k_gmres_resist && !(ctx->res.on && ctx->res.pgrid > 0))
             continue;
+        // the Hall edge EMF, where the implicit Hall solve runs it
+        if (t == TUNE_k_hall_edge && !ctx->hall.on)
+            continue;
         int keep = ctx->tune[t];
         for (int v = 0; v < kTuneCount[t] && rc == MHD_OK; ++v)
         {
@@ -3676,8 +3682,8 @@ int mhd_stage(mhd_ctx *ctx, int32_t stage_id)
             ctx->dbv, ctx->c, ctx->hall_coef);
         RUN(launched(ctx));
         prof_begin(ctx, "k_hall_edge");
-        k_hall_edge<<<dim3(grid_for(max_stagger(ctx)), ctx->nblocks), kThreads, 0, ctx->stream>>>(
-            ctx->dbv, ctx->hall_zb, ctx->hall_nzb);
+        launch_k_hall_edge(ctx->tune[TUNE_k_hall_edge], grid_kind(ctx, KIND_STAG), ctx->stream, ctx->dbv,
+                           ctx->hall_zb, ctx->hall_nzb);
         RUN(launched(ctx));
         break;
     case MHD_STAGE_HALL_SOLVE:

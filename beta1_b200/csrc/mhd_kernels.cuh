@@ -34,7 +34,10 @@ __global__ void k_divb(const BlockView *bvs);
 __global__ void k_geom32(const BlockView *bvs);
 __global__ void k_rk2(const BlockView *bvs, int save);
 __global__ void k_hall_cell(const BlockView *bvs, Consts c, double hall_coef);
-__global__ void k_hall_edge(const BlockView *bvs, const int *zb, int nzb);
+// the Hall edge EMF, variant 0: per-edge cell reads (no launch bounds), 1: the
+// seven cells of a staggered point read once (at least 2 CTAs per SM); the
+// same bits
+int launch_k_hall_edge(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, const int *zb, int nzb);
 __global__ void k_eres_explicit(const BlockView *bvs, double inver_Rem);
 // calc_Bcell on the inner cells (2-D launch, one grid row per block); w32:
 // from the FP32 weight copies (mixed form)

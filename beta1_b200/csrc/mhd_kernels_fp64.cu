@@ -703,49 +703,38 @@ __global__ void k_hall_cell(const BlockView *__restrict__ bvs, Consts c, double 
 }
 
 // one inner edge of axis ea: 4-cell mean of Ehc along dr, minus the
-// whistler diffusion of the two face-B jumps across the edge
-__device__ __forceinline__ double hall_edge_one(const BlockView &b, int ea, int i, int j, int k)
+// whistler diffusion of the two face-B jumps across the edge.  E[q][c] and
+// be[q] are the Ehc components and beta of the edge's four cells, in the
+// order the reference sums them.
+__device__ __forceinline__ double hall_edge_one(const BlockView &b, int ea, int i, int j, int k, const double (&E)[4][3],
+                                                const double (&be)[4])
 {
     const double eps = 1e-14, Cwh = 0.1;
     const int64_t v = b.vol;
     const int64_t p = pidx(b, i, j, k);
-    int64_t c[4];
     int Fm, Fp, Am, Ap;
     int64_t qm, qp, am, ap;
     if (ea == 0)
     {
-        c[0] = pidx(b, i, j - 1, k - 1);
-        c[1] = pidx(b, i, j - 1, k);
-        c[2] = pidx(b, i, j, k - 1);
-        c[3] = p;
         Fm = F_Bzeta, qm = pidx(b, i, j - 1, k), Fp = F_Beta, qp = pidx(b, i, j, k - 1);
         Am = F_Areazeta, am = pidx(b, i, j - 1, k), Ap = F_Areaeta, ap = pidx(b, i, j, k - 1);
     }
     else if (ea == 1)
     {
-        c[0] = pidx(b, i - 1, j, k - 1);
-        c[1] = pidx(b, i - 1, j, k);
-        c[2] = pidx(b, i, j, k - 1);
-        c[3] = p;
         Fm = F_Bxi, qm = pidx(b, i, j, k - 1), Fp = F_Bzeta, qp = pidx(b, i - 1, j, k);
         Am = F_Areaxi, am = pidx(b, i, j, k - 1), Ap = F_Areazeta, ap = pidx(b, i - 1, j, k);
     }
     else
     {
-        c[0] = pidx(b, i - 1, j - 1, k);
-        c[1] = pidx(b, i - 1, j, k);
-        c[2] = pidx(b, i, j - 1, k);
-        c[3] = p;
         Fm = F_Beta, qm = pidx(b, i - 1, j, k), Fp = F_Bxi, qp = pidx(b, i, j - 1, k);
         Am = F_Areaeta, am = pidx(b, i - 1, j, k), Ap = F_Areaxi, ap = pidx(b, i, j - 1, k);
     }
-    const double *E = b.f[F_Ehc], *be = b.f[F_HallBeta];
-    const double Ecx = 0.25 * (E[c[0]] + E[c[1]] + E[c[2]] + E[c[3]]);
-    const double Ecy = 0.25 * (E[v + c[0]] + E[v + c[1]] + E[v + c[2]] + E[v + c[3]]);
-    const double Ecz = 0.25 * (E[2 * v + c[0]] + E[2 * v + c[1]] + E[2 * v + c[2]] + E[2 * v + c[3]]);
+    const double Ecx = 0.25 * (E[0][0] + E[1][0] + E[2][0] + E[3][0]);
+    const double Ecy = 0.25 * (E[0][1] + E[1][1] + E[2][1] + E[3][1]);
+    const double Ecz = 0.25 * (E[0][2] + E[1][2] + E[2][2] + E[3][2]);
     const double *dr = b.f[F_drxi + ea];
     const double Ecen = Ecx * dr[p] + Ecy * dr[v + p] + Ecz * dr[2 * v + p];
-    const double beta_e = smax(smax(be[c[0]], be[c[1]]), smax(be[c[2]], be[c[3]]));
+    const double beta_e = smax(smax(be[0], be[1]), smax(be[2], be[3]));
     const double L = smax(b.f[F_dlxi + ea][p], eps);
     const double Abar_m = 0.5 * (b.f[Am][p] + b.f[Am][am]);
     const double inv_m = L / smax(Abar_m, eps);
@@ -758,9 +747,35 @@ __device__ __forceinline__ double hall_edge_one(const BlockView &b, int ea, int 
     return Ecen - 0.5 * mu_m * dB_m + 0.5 * mu_p * dB_p;
 }
 
+// zero box test of the Hall edge EMF (Solid_Surface layers and Pole edges)
+__device__ __forceinline__ bool hall_zeroed(const int *__restrict__ zb, int nzb, int bi, int ea, int i, int j, int k)
+{
+    bool zero = false;
+    for (int q = 0; q < nzb && !zero; ++q)
+    {
+        const int *z = zb + 8 * q;
+        zero = (z[0] == bi && z[1] == ea && i >= z[2] && j >= z[3] && k >= z[4] && i < z[5] && j < z[6] && k < z[7]);
+    }
+    return zero;
+}
+
+// the four cells of each edge axis, in the reference's order, as offsets
+// into the seven cells around a staggered point: 0 (0,0,0), 1 (0,-1,0),
+// 2 (0,0,-1), 3 (0,-1,-1), 4 (-1,0,0), 5 (-1,0,-1), 6 (-1,-1,0)
+__constant__ int kHallCells[3][4] = {{3, 1, 2, 0}, {5, 4, 2, 0}, {6, 4, 1, 0}};
+
+__device__ __forceinline__ int64_t hall_cell_of(const BlockView &b, int q, int i, int j, int k)
+{
+    const int di = (q >= 4) ? -1 : 0;
+    const int dj = (q == 1 || q == 3 || q == 6) ? -1 : 0;
+    const int dk = (q == 2 || q == 3 || q == 5) ? -1 : 0;
+    return pidx(b, i + di, j + dj, k + dk);
+}
+
 // inner Hall edge EMF of all three axes; zero inside the boxes zb[8 q ..]:
-// block, edge axis, lo[3], hi[3] (Solid_Surface layers and Pole edges)
-__global__ void k_hall_edge(const BlockView *__restrict__ bvs, const int *__restrict__ zb, int nzb)
+// block, edge axis, lo[3], hi[3].  Per-edge form: each edge reads its four
+// cells (the compiler's own register allocation).
+__global__ void k_hall_edge_percell(const BlockView *__restrict__ bvs, const int *__restrict__ zb, int nzb)
 {
     int64_t t;
     const int bi = cta_block(bvs, KIND_STAG, t);
@@ -768,21 +783,97 @@ __global__ void k_hall_edge(const BlockView *__restrict__ bvs, const int *__rest
     int i, j, k;
     if (!stagger_point(b, nullptr, 0, t, i, j, k))
         return;
+    const int64_t v = b.vol;
+    const double *Ec = b.f[F_Ehc], *bec = b.f[F_HallBeta];
     const int64_t p = pidx(b, i, j, k);
 #pragma unroll
     for (int ea = 0; ea < 3; ++ea)
     {
         if (!inner_of(b, 1, ea, i, j, k))
             continue;
-        bool zero = false;
-        for (int q = 0; q < nzb && !zero; ++q)
+        double r = 0.0;
+        if (!hall_zeroed(zb, nzb, bi, ea, i, j, k))
         {
-            const int *z = zb + 8 * q;
-            zero = (z[0] == bi && z[1] == ea && i >= z[2] && j >= z[3] && k >= z[4] && i < z[5] &&
-                    j < z[6] && k < z[7]);
+            double E[4][3], be[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+            {
+                const int64_t c = hall_cell_of(b, kHallCells[ea][q], i, j, k);
+                E[q][0] = Ec[c];
+                E[q][1] = Ec[v + c];
+                E[q][2] = Ec[2 * v + c];
+                be[q] = bec[c];
+            }
+            r = hall_edge_one(b, ea, i, j, k, E, be);
         }
-        b.f[F_Ehxi + ea][p] = zero ? 0.0 : hall_edge_one(b, ea, i, j, k);
+        b.f[F_Ehxi + ea][p] = r;
     }
+}
+
+// Shared-cell form: the seven cells the three edges of a staggered point
+// share are read once, and every edge is formed before any is stored (at
+// least 2 CTAs per SM).
+__global__ void __launch_bounds__(256, 2) k_hall_edge_shared(const BlockView *__restrict__ bvs,
+                                                             const int *__restrict__ zb, int nzb)
+{
+    int64_t t;
+    const int bi = cta_block(bvs, KIND_STAG, t);
+    const BlockView &b = bvs[bi];
+    int i, j, k;
+    if (!stagger_point(b, nullptr, 0, t, i, j, k))
+        return;
+    const int64_t v = b.vol;
+    const double *Ec = b.f[F_Ehc], *bec = b.f[F_HallBeta];
+    double E7[7][3], be7[7];
+#pragma unroll
+    for (int q = 0; q < 7; ++q)
+    {
+        const int64_t c = hall_cell_of(b, q, i, j, k);
+        E7[q][0] = Ec[c];
+        E7[q][1] = Ec[v + c];
+        E7[q][2] = Ec[2 * v + c];
+        be7[q] = bec[c];
+    }
+    double out[3] = {0.0, 0.0, 0.0};
+    bool inner[3];
+#pragma unroll
+    for (int ea = 0; ea < 3; ++ea)
+    {
+        inner[ea] = inner_of(b, 1, ea, i, j, k);
+        if (!inner[ea] || hall_zeroed(zb, nzb, bi, ea, i, j, k))
+            continue;
+        double E[4][3], be[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+        {
+            E[q][0] = E7[kHallCells[ea][q]][0];
+            E[q][1] = E7[kHallCells[ea][q]][1];
+            E[q][2] = E7[kHallCells[ea][q]][2];
+            be[q] = be7[kHallCells[ea][q]];
+        }
+        out[ea] = hall_edge_one(b, ea, i, j, k, E, be);
+    }
+    const int64_t p = pidx(b, i, j, k);
+#pragma unroll
+    for (int ea = 0; ea < 3; ++ea)
+        if (inner[ea])
+            b.f[F_Ehxi + ea][p] = out[ea];
+}
+
+int launch_k_hall_edge(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, const int *zb, int nzb)
+{
+    switch (variant)
+    {
+    case 0:
+        k_hall_edge_percell<<<grid, 256, 0, st>>>(bvs, zb, nzb);
+        break;
+    case 1:
+        k_hall_edge_shared<<<grid, 256, 0, st>>>(bvs, zb, nzb);
+        break;
+    default:
+        return -1;
+    }
+    return 0;
 }
 
 // cell part of ApplyUpdate_Euler_ (LunarSolver_Advance.cpp:82-93): U += dt*RHS_H

@@ -311,8 +311,9 @@ int mhd_set_flux_reference_run(mhd_ctx *ctx, int32_t run, const double prim[5]);
    its FP32 face states staged in shared memory; 14: k_pv_uplus_dt
    with J_cell in a pass of its own).  For the persistent k_gmres_resist the
    value is the CTAs of its grid (0: two per SM); its partial sums group
-   differently per grid, so its results agree to round-off, not bitwise. */
-#define MHD_NTUNE 8
+   differently per grid, so its results agree to round-off, not bitwise.
+   k_hall_edge 2: the seven cells of a staggered point read once. */
+#define MHD_NTUNE 9
 int mhd_autotune(mhd_ctx *ctx, int32_t reps, int32_t *min_ctas, int32_t n);
 const char *mhd_tune_name(int32_t i);
 

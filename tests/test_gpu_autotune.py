@@ -24,7 +24,7 @@ def test_tuned_context_matches_reference(fname, tol):
     s.load_state(st)
     chosen = s.ctx.autotune(reps=3)
     assert set(chosen) == {"k_pv_uplus_dt", "k_fluid_ucontra", "k_bcell_jedge", "k_eface", "k_curl_e2f", "k_eedge",
-                           "k_fluid_mixed", "k_gmres_resist"}
+                           "k_fluid_mixed", "k_gmres_resist", "k_hall_edge"}
     # minimum CTAs per SM of the chosen variant (0: no launch bounds)
     assert all(v >= 0 for v in chosen.values())
     nb = len(spec.blocks)

@@ -29,14 +29,18 @@ def state_of(g, spec):
     return st
 
 
+# k_hall_edge variants: 0 reads each edge's four cells, 2 the seven cells of
+# a staggered point once; both give the reference's bits
+@pytest.mark.parametrize("variant", [0, 2])
 @pytest.mark.parametrize("kind", ["periodic", "slab"])
-def test_hall_emf_matches_reference(kind):
+def test_hall_emf_matches_reference(kind, variant):
     if kind == "periodic":
         spec, g, topo = case.periodic_box_case((8, 6, 5)), load_golden("hall_periodic_8x6x5.npz"), "periodic"
     else:
         spec, g, topo = case.slab_case(24, (5, 6), (2, 2)), load_golden("hall_slab_24x5x6_t2x2.npz"), "tiled"
     s = solver.Solver(spec, topology=topo)
     try:
+        s.ctx.set_tune({"k_hall_edge": variant})
         s.load_state(state_of(g, spec))
         s.ctx.stage(mhd.STAGE_HALL_EMF)
         worst = 0.0
