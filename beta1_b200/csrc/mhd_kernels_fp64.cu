@@ -761,8 +761,13 @@ __device__ __forceinline__ bool hall_zeroed(const int *__restrict__ zb, int nzb,
 
 // the four cells of each edge axis, in the reference's order, as offsets
 // into the seven cells around a staggered point: 0 (0,0,0), 1 (0,-1,0),
-// 2 (0,0,-1), 3 (0,-1,-1), 4 (-1,0,0), 5 (-1,0,-1), 6 (-1,-1,0)
-__constant__ int kHallCells[3][4] = {{3, 1, 2, 0}, {5, 4, 2, 0}, {6, 4, 1, 0}};
+// 2 (0,0,-1), 3 (0,-1,-1), 4 (-1,0,0), 5 (-1,0,-1), 6 (-1,-1,0) (a
+// compile-time table: every use sits in a fully unrolled loop)
+__device__ __forceinline__ constexpr int hall_cells(int ea, int q)
+{
+    return ea == 0 ? (q == 0 ? 3 : q == 1 ? 1 : q == 2 ? 2 : 0)
+                   : ea == 1 ? (q == 0 ? 5 : q == 1 ? 4 : q == 2 ? 2 : 0) : (q == 0 ? 6 : q == 1 ? 4 : q == 2 ? 1 : 0);
+}
 
 __device__ __forceinline__ int64_t hall_cell_of(const BlockView &b, int q, int i, int j, int k)
 {
@@ -798,7 +803,7 @@ __global__ void k_hall_edge_percell(const BlockView *__restrict__ bvs, const int
 #pragma unroll
             for (int q = 0; q < 4; ++q)
             {
-                const int64_t c = hall_cell_of(b, kHallCells[ea][q], i, j, k);
+                const int64_t c = hall_cell_of(b, hall_cells(ea, q), i, j, k);
                 E[q][0] = Ec[c];
                 E[q][1] = Ec[v + c];
                 E[q][2] = Ec[2 * v + c];
@@ -846,10 +851,10 @@ __global__ void __launch_bounds__(256, 2) k_hall_edge_shared(const BlockView *__
 #pragma unroll
         for (int q = 0; q < 4; ++q)
         {
-            E[q][0] = E7[kHallCells[ea][q]][0];
-            E[q][1] = E7[kHallCells[ea][q]][1];
-            E[q][2] = E7[kHallCells[ea][q]][2];
-            be[q] = be7[kHallCells[ea][q]];
+            E[q][0] = E7[hall_cells(ea, q)][0];
+            E[q][1] = E7[hall_cells(ea, q)][1];
+            E[q][2] = E7[hall_cells(ea, q)][2];
+            be[q] = be7[hall_cells(ea, q)];
         }
         out[ea] = hall_edge_one(b, ea, i, j, k, E, be);
     }
