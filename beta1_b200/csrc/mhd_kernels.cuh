@@ -73,6 +73,8 @@ __global__ void k_begin_step(const unsigned long long *dt_key, double *dt, int *
 __global__ void k_arm_dt(unsigned long long *dt_key, int nruns);
 __global__ void k_end_step(const double *dt, double *time, long long *step, int nruns);
 __global__ void k_gather(double *pool, const uint64_t *dst, const uint64_t *src, int64_t n);
+// the same with 32-bit pool offsets (pools of fewer than 2^32 points)
+__global__ void k_gather32(double *pool, const uint32_t *dst, const uint32_t *src, int64_t n);
 __global__ void k_set_consts(double *pool, const uint64_t *dst, const double *val, int64_t n);
 __global__ void k_wall_u(const BlockView *bvs, int blk, int dir, double gamma);
 __global__ void k_wall_u_all(const BlockView *bvs, const int *walls, double gamma);

@@ -1404,6 +1404,14 @@ __global__ void k_gather(double *__restrict__ pool, const uint64_t *__restrict__
         pool[dst[t]] = pool[src[t]];
 }
 
+__global__ void k_gather32(double *__restrict__ pool, const uint32_t *__restrict__ dst,
+                           const uint32_t *__restrict__ src, int64_t n)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n)
+        pool[dst[t]] = pool[src[t]];
+}
+
 // phase A of a Sync: points set to fixed values by physical handlers
 // (Farfield states, zero-curl edge EMF, zeroed wall layers)
 __global__ void k_set_consts(double *__restrict__ pool, const uint64_t *__restrict__ dst,
