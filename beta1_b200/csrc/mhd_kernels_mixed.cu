@@ -168,56 +168,56 @@ __device__ __forceinline__ void k_fluid_mixed_body(const BlockView *__restrict__
     const int i = lo + int(t / n1);
     const int64_t v = b.vol;
     const int64_t p = pidx(b, i, j, k);
-    const int64_t pp[3] = {pidx(b, i + 1, j, k), pidx(b, i, j + 1, k), pidx(b, i, j, k + 1)};
     const double jac = b.f[F_Jac][p];
-    // face metric at the low (p) and high (pp) face of each axis: FP32 copies
-    // for the fluxes, and the FP64 sum of the cell's signed face vectors
-    float km[3][3], kp[3][3];
-    double S[3] = {0.0, 0.0, 0.0};
-    {
-        // contravariant velocities (cell_u_contra): (k-bar . U_plus) / (|Jac| + 1e-30)
-        const double *Up = b.f[F_Uplus];
-        const double ux = Up[p], uy = Up[v + p], uz = Up[2 * v + p];
-        const double inv_jac = 1.0 / (fabs(jac) + 1.0e-30);
-        double *UC = b.f[F_UC];
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-        {
-            const double *M = b.f[F_JDxi + a];
-            double m_[3], p_[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d)
-            {
-                m_[d] = M[d * v + p];
-                p_[d] = M[d * v + pp[a]];
-                km[a][d] = float(m_[d]);
-                kp[a][d] = float(p_[d]);
-                S[d] += p_[d] - m_[d];
-            }
-            const double kx = 0.5 * (m_[0] + p_[0]);
-            const double ky = 0.5 * (m_[1] + p_[1]);
-            const double kz = 0.5 * (m_[2] + p_[2]);
-            UC[a * v + p] = (kx * ux + ky * uy + kz * uz) * inv_jac;
-        }
-    }
-    if (i < 0 || j < 0 || k < 0 || i >= b.ni || j >= b.nj || k >= b.nk)
-        return;
+    const bool inner = i >= 0 && j >= 0 && k >= 0 && i < b.ni && j < b.nj && k < b.nk;
+    // contravariant velocities (cell_u_contra): (k-bar . U_plus) / (|Jac| + 1e-30)
+    const double *Up = b.f[F_Uplus];
+    const double ux = Up[p], uy = Up[v + p], uz = Up[2 * v + p];
+    const double inv_jac = 1.0 / (fabs(jac) + 1.0e-30);
+    double *UC = b.f[F_UC];
     const float *g = b.g32;
-    const int64_t pm[3] = {pidx(b, i - 1, j, k), pidx(b, i, j - 1, k), pidx(b, i, j, k - 1)};
     const double *q0 = b.qref;
     const Ref32 r0 = {float(q0[0]), {float(q0[1]), float(q0[2]), float(q0[3])}, float(q0[5] + q0[4])};
+    // one axis at a time: its face metric at the low (p) and high (pp) face,
+    // the cell's velocity along it, its share of the FP64 sum of signed face
+    // vectors, and (inner cells) its two FP32 face fluxes -- the same
+    // operations in the same order as forming all three axes first, with a
+    // third of the metric live at once
+    double S[3] = {0.0, 0.0, 0.0};
     float r[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-    for (int dir = 0; dir < 3; ++dir)
+    for (int a = 0; a < 3; ++a)
     {
-        float Fm[5], Fp[5];
-        rusanov_dev32(b, r0, km[dir][0], km[dir][1], km[dir][2], g[(G32_AREA + dir) * v + p], p, pm[dir], Fm);
-        rusanov_dev32(b, r0, kp[dir][0], kp[dir][1], kp[dir][2], g[(G32_AREA + dir) * v + pp[dir]], pp[dir], p, Fp);
+        const int64_t pp = a == 0 ? pidx(b, i + 1, j, k) : a == 1 ? pidx(b, i, j + 1, k) : pidx(b, i, j, k + 1);
+        const double *M = b.f[F_JDxi + a];
+        double m_[3], p_[3];
+        float km[3], kp[3];
 #pragma unroll
-        for (int m = 0; m < 5; ++m)
-            r[m] += Fp[m] - Fm[m];
+        for (int d = 0; d < 3; ++d)
+        {
+            m_[d] = M[d * v + p];
+            p_[d] = M[d * v + pp];
+            km[d] = float(m_[d]);
+            kp[d] = float(p_[d]);
+            S[d] += p_[d] - m_[d];
+        }
+        const double kx = 0.5 * (m_[0] + p_[0]);
+        const double ky = 0.5 * (m_[1] + p_[1]);
+        const double kz = 0.5 * (m_[2] + p_[2]);
+        UC[a * v + p] = (kx * ux + ky * uy + kz * uz) * inv_jac;
+        if (inner)
+        {
+            const int64_t pm = a == 0 ? pidx(b, i - 1, j, k) : a == 1 ? pidx(b, i, j - 1, k) : pidx(b, i, j, k - 1);
+            float Fm[5], Fp[5];
+            rusanov_dev32(b, r0, km[0], km[1], km[2], g[(G32_AREA + a) * v + p], p, pm, Fm);
+            rusanov_dev32(b, r0, kp[0], kp[1], kp[2], g[(G32_AREA + a) * v + pp], pp, p, Fp);
+#pragma unroll
+            for (int m = 0; m < 5; ++m)
+                r[m] += Fp[m] - Fm[m];
+        }
     }
-    mixed_rhs(b, c, p, jac, S, r);
+    if (inner)
+        mixed_rhs(b, c, p, jac, S, r);
 }
 
 template <int MINB>
