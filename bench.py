@@ -116,11 +116,20 @@ ALGO_BYTES_MIXED = {"k_pv_uplus_dt": 12 * 8 + 48 * 4 + 6 * 8 + 7 * 4,
                     "k_bcell_jedge": 21 * 8 + 18 * 4}
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of
-# the dominant kernel, from one ncu capture of the C2 workload at half the
-# cells per direction (165,888 cells: 114.26 MB read + 10.32 MB written),
-# scaled by the cell count to a full C2 launch (1,327,104 cells; the kernel's
-# traffic grows with the cells it covers)
-NCU_TRAFFIC_BYTES = {("k_pv_uplus_dt", "c2_slab6x96x48x48_implicit_resistive_fp64"): (114.25536e6 + 10.321408e6) * 8.0}
+# the dominant kernel, from one ncu capture of a smaller case of the same
+# workload, scaled by the cell count to a full launch (the kernels' traffic
+# grows with the cells they cover):
+# * C2 at half the cells per direction (165,888 cells: 114.26 MB read +
+#   10.32 MB written) to the full C2 slab (1,327,104 cells);
+# * the shell sweep's first 6 runs (2,269,318 cells; k_fluid_mixed 602.42 MB
+#   read + 141.94 MB written, k_pv_uplus_dt 763.50 + 185.09 MB) to all 48
+#   runs (14,879,028 cells)
+_SWEEP_SCALE = 14879028.0 / 2269318.0
+NCU_TRAFFIC_BYTES = {
+    ("k_pv_uplus_dt", "c2_slab6x96x48x48_implicit_resistive_fp64"): (114.25536e6 + 10.321408e6) * 8.0,
+    ("k_fluid_mixed", "c5s_sweep48_shell_runs_mixed"): (602.41792e6 + 141.940224e6) * _SWEEP_SCALE,
+    ("k_pv_uplus_dt", "c5s_sweep48_shell_runs_mixed"): (763.501568e6 + 185.093888e6) * _SWEEP_SCALE,
+}
 
 
 def sample_clocks(stop: threading.Event, out: list, gpu_id: str):

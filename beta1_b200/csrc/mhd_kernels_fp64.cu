@@ -777,9 +777,66 @@ __device__ __forceinline__ int64_t hall_cell_of(const BlockView &b, int q, int i
     return pidx(b, i + di, j + dj, k + dk);
 }
 
+// one inner edge of axis ea, its cells read here: 4-cell mean of Ehc along
+// dr, minus the whistler diffusion of the two face-B jumps across the edge
+__device__ __forceinline__ double hall_edge_direct(const BlockView &b, int ea, int i, int j, int k)
+{
+    const double eps = 1e-14, Cwh = 0.1;
+    const int64_t v = b.vol;
+    const int64_t p = pidx(b, i, j, k);
+    int64_t c[4];
+    int Fm, Fp, Am, Ap;
+    int64_t qm, qp, am, ap;
+    if (ea == 0)
+    {
+        c[0] = pidx(b, i, j - 1, k - 1);
+        c[1] = pidx(b, i, j - 1, k);
+        c[2] = pidx(b, i, j, k - 1);
+        c[3] = p;
+        Fm = F_Bzeta, qm = pidx(b, i, j - 1, k), Fp = F_Beta, qp = pidx(b, i, j, k - 1);
+        Am = F_Areazeta, am = pidx(b, i, j - 1, k), Ap = F_Areaeta, ap = pidx(b, i, j, k - 1);
+    }
+    else if (ea == 1)
+    {
+        c[0] = pidx(b, i - 1, j, k - 1);
+        c[1] = pidx(b, i - 1, j, k);
+        c[2] = pidx(b, i, j, k - 1);
+        c[3] = p;
+        Fm = F_Bxi, qm = pidx(b, i, j, k - 1), Fp = F_Bzeta, qp = pidx(b, i - 1, j, k);
+        Am = F_Areaxi, am = pidx(b, i, j, k - 1), Ap = F_Areazeta, ap = pidx(b, i - 1, j, k);
+    }
+    else
+    {
+        c[0] = pidx(b, i - 1, j - 1, k);
+        c[1] = pidx(b, i - 1, j, k);
+        c[2] = pidx(b, i, j - 1, k);
+        c[3] = p;
+        Fm = F_Beta, qm = pidx(b, i - 1, j, k), Fp = F_Bxi, qp = pidx(b, i, j - 1, k);
+        Am = F_Areaeta, am = pidx(b, i - 1, j, k), Ap = F_Areaxi, ap = pidx(b, i, j - 1, k);
+    }
+    const double *E = b.f[F_Ehc], *be = b.f[F_HallBeta];
+    const double Ecx = 0.25 * (E[c[0]] + E[c[1]] + E[c[2]] + E[c[3]]);
+    const double Ecy = 0.25 * (E[v + c[0]] + E[v + c[1]] + E[v + c[2]] + E[v + c[3]]);
+    const double Ecz = 0.25 * (E[2 * v + c[0]] + E[2 * v + c[1]] + E[2 * v + c[2]] + E[2 * v + c[3]]);
+    const double *dr = b.f[F_drxi + ea];
+    const double Ecen = Ecx * dr[p] + Ecy * dr[v + p] + Ecz * dr[2 * v + p];
+    const double beta_e = smax(smax(be[c[0]], be[c[1]]), smax(be[c[2]], be[c[3]]));
+    const double L = smax(b.f[F_dlxi + ea][p], eps);
+    const double Abar_m = 0.5 * (b.f[Am][p] + b.f[Am][am]);
+    const double inv_m = L / smax(Abar_m, eps);
+    const double mu_m = Cwh * beta_e * inv_m * inv_m;
+    const double Abar_p = 0.5 * (b.f[Ap][p] + b.f[Ap][ap]);
+    const double inv_p = L / smax(Abar_p, eps);
+    const double mu_p = Cwh * beta_e * inv_p * inv_p;
+    const double dB_m = b.f[Fm][p] - b.f[Fm][qm];
+    const double dB_p = b.f[Fp][p] - b.f[Fp][qp];
+    return Ecen - 0.5 * mu_m * dB_m + 0.5 * mu_p * dB_p;
+}
+
 // inner Hall edge EMF of all three axes; zero inside the boxes zb[8 q ..]:
-// block, edge axis, lo[3], hi[3].  Per-edge form: each edge reads its four
-// cells (the compiler's own register allocation).
+// block, edge axis, lo[3], hi[3] (Solid_Surface layers and Pole edges).
+// Per-edge form: each edge reads its four cells (the compiler's own
+// register allocation).
 __global__ void k_hall_edge_percell(const BlockView *__restrict__ bvs, const int *__restrict__ zb, int nzb)
 {
     int64_t t;
@@ -788,30 +845,20 @@ __global__ void k_hall_edge_percell(const BlockView *__restrict__ bvs, const int
     int i, j, k;
     if (!stagger_point(b, nullptr, 0, t, i, j, k))
         return;
-    const int64_t v = b.vol;
-    const double *Ec = b.f[F_Ehc], *bec = b.f[F_HallBeta];
     const int64_t p = pidx(b, i, j, k);
 #pragma unroll
     for (int ea = 0; ea < 3; ++ea)
     {
         if (!inner_of(b, 1, ea, i, j, k))
             continue;
-        double r = 0.0;
-        if (!hall_zeroed(zb, nzb, bi, ea, i, j, k))
+        bool zero = false;
+        for (int q = 0; q < nzb && !zero; ++q)
         {
-            double E[4][3], be[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-            {
-                const int64_t c = hall_cell_of(b, hall_cells(ea, q), i, j, k);
-                E[q][0] = Ec[c];
-                E[q][1] = Ec[v + c];
-                E[q][2] = Ec[2 * v + c];
-                be[q] = bec[c];
-            }
-            r = hall_edge_one(b, ea, i, j, k, E, be);
+            const int *z = zb + 8 * q;
+            zero = (z[0] == bi && z[1] == ea && i >= z[2] && j >= z[3] && k >= z[4] && i < z[5] &&
+                    j < z[6] && k < z[7]);
         }
-        b.f[F_Ehxi + ea][p] = r;
+        b.f[F_Ehxi + ea][p] = zero ? 0.0 : hall_edge_direct(b, ea, i, j, k);
     }
 }
 
