@@ -590,6 +590,12 @@ def main():
             "mixed_max_divb_dx_over_b": divb,
             "time_rel_diff": max(abs(a - b) / b for a, b in zip(t_m, t_d)),
             "bounds": {"rel_l2": 1e-5, "divb_dx_over_b": 1e-12}})
+        # the FP64 form's per-kernel durations (after the comparison: these steps advance it)
+        prof64 = {}
+        for _ in range(3):
+            for name, t in fp64_cmp.ctx.profile_step():
+                prof64[name] = prof64.get(name, 0.0) + t / 3.0
+        fp64_line["kernels_ms_per_step"] = {k: round(v, 5) for k, v in sorted(prof64.items(), key=lambda kv: -kv[1])}
         fp64_cmp.ctx.close()
 
     # per-kernel durations: eager steps with an event pair around every launch
