@@ -142,27 +142,25 @@ __device__ __forceinline__ void fluid_one(const BlockView &b, const Consts &c, i
     double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     const double invJ = 1.0 / b.f[F_Jac][p];
 
+    // each component takes its three flux differences in the reference's
+    // order, r -= dx / J, r -= dy / J, r -= dz / J; they are applied as each
+    // direction completes (the same operations per component), so no
+    // direction's differences stay live
     rusanov_face(b, c, 0, i, j, k, Fm);
     rusanov_face(b, c, 0, i + 1, j, k, Fp);
-    double dx[5];
 #pragma unroll
     for (int m = 0; m < 5; ++m)
-        dx[m] = Fp[m] - Fm[m];
+        r[m] -= (Fp[m] - Fm[m]) * invJ;
     rusanov_face(b, c, 1, i, j, k, Fm);
     rusanov_face(b, c, 1, i, j + 1, k, Fp);
-    double dy[5];
 #pragma unroll
     for (int m = 0; m < 5; ++m)
-        dy[m] = Fp[m] - Fm[m];
+        r[m] -= (Fp[m] - Fm[m]) * invJ;
     rusanov_face(b, c, 2, i, j, k, Fm);
     rusanov_face(b, c, 2, i, j, k + 1, Fp);
 #pragma unroll
     for (int m = 0; m < 5; ++m)
-    {
-        r[m] -= dx[m] * invJ;
-        r[m] -= dy[m] * invJ;
         r[m] -= (Fp[m] - Fm[m]) * invJ;
-    }
 
     // J x B force with the Hall_Num_Limiter weight (LunarSolver_Tools.cpp:47-56)
     const double rho = b.f[F_U][p];
