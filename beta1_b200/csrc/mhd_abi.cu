@@ -153,7 +153,7 @@ const char *const kTuneNames[NTUNE] = {"k_pv_uplus_dt", "k_fluid_ucontra", "k_bc
 // point once
 const int kTuneMinCtas[NTUNE][5] = {{4, 0, 5, 14, 0}, {0, 3, 0, 0, 0},        {0, 6, 0, 0, 0},
                                     {0, 6, 0, 0, 0},  {0, 6, 0, 0, 0},        {0, 8, 0, 0, 0},
-                                    {2, 0, 3, 12, 16}, {0, 148, 64, 32, 0},   {0, 2, 0, 0, 0}};
+                                    {3, 0, 2, 12, 16}, {0, 148, 64, 32, 0},   {0, 2, 0, 0, 0}};
 const int kTuneCount[NTUNE] = {4, 2, 2, 2, 2, 2, 5, 4, 2};
 constexpr int kPvSplit = 3; // variant index of k_pv_uplus_dt's split form
 

@@ -296,7 +296,7 @@ int launch_k_curl_e2f(int variant, dim3 grid, cudaStream_t st, const BlockView *
                       double mult, const double *dtp, double dtdiv, int mult_is_neg_dt, const int *rng);
 // k_eedge: minimum CTAs per SM 0, 8
 int launch_k_eedge(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs);
-// k_fluid_mixed: minimum CTAs per SM 2, 0, 3
+// k_fluid_mixed: minimum CTAs per SM 3, 0, 2
 int launch_k_fluid_mixed(int variant, dim3 grid, cudaStream_t st, const BlockView *bvs, Consts c);
 
 } // namespace mhd

@@ -151,9 +151,9 @@ __device__ __forceinline__ void mixed_rhs(const BlockView &b, const Consts &c, i
 // Fluid RHS of the inner cells (FP32 flux divergence, FP64 J x B source) and
 // the FP64 contravariant velocities of the cells within one ghost layer; the
 // FP64 face metric read for the velocities is the one the fluxes round.
-// variants: at least 2 CTAs per SM (128 registers; the default: uncapped it
-// takes 168 registers and one CTA, 0.265 -> 0.171 ms on the C2 step),
-// uncapped, at least 3
+// variants: at least 3 CTAs per SM (80 registers; the default: 1.73 -> 1.52 ms
+// per step on the shell sweep against 2 CTAs per SM), uncapped (96
+// registers), at least 2
 __device__ __forceinline__ void k_fluid_mixed_body(const BlockView *__restrict__ bvs, Consts c)
 {
     int64_t t;
@@ -434,13 +434,13 @@ int launch_k_fluid_mixed(int variant, dim3 grid, cudaStream_t st, const BlockVie
         k_fluid_mixed_staged<<<grid, 256, 0, st>>>(bvs, c);
         break;
     case 0:
-        k_fluid_mixed_t<2><<<grid, 256, 0, st>>>(bvs, c);
+        k_fluid_mixed_t<3><<<grid, 256, 0, st>>>(bvs, c);
         break;
     case 1:
         k_fluid_mixed_free<<<grid, 256, 0, st>>>(bvs, c);
         break;
     case 2:
-        k_fluid_mixed_t<3><<<grid, 256, 0, st>>>(bvs, c);
+        k_fluid_mixed_t<2><<<grid, 256, 0, st>>>(bvs, c);
         break;
     default:
         return -1;

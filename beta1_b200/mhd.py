@@ -32,7 +32,7 @@ PREC_MIXED = 1
 # k_pv_uplus_dt with J_cell in its own pass;
 # k_gmres_resist: the CTAs of the persistent grid, 0: two per SM)
 DEFAULT_TUNE = {"k_pv_uplus_dt": 4, "k_fluid_ucontra": 0, "k_bcell_jedge": 0, "k_eface": 0, "k_curl_e2f": 0,
-                "k_eedge": 0, "k_fluid_mixed": 2, "k_gmres_resist": 0, "k_hall_edge": 0}
+                "k_eedge": 0, "k_fluid_mixed": 3, "k_gmres_resist": 0, "k_hall_edge": 0}
 
 STAGE_TIMESTEP, STAGE_FLUID_RHS, STAGE_INDUCTION, STAGE_UPDATE, STAGE_DIVB, STAGE_HALL_EMF = 1, 2, 3, 4, 5, 6
 STAGE_HALL_SOLVE = 7

@@ -79,7 +79,7 @@ def test_tuning_leaves_the_implicit_hall_start_untouched():
         assert np.array_equal(out[0][key], out[1][key]), key
 
 
-@pytest.mark.parametrize("variant", [12, 16, 0, 3])
+@pytest.mark.parametrize("variant", [12, 16, 0, 2])
 def test_flux_variants_give_the_same_bits(variant):
     """The mixed flux pass in each of its variants -- the face-tiled kernel
     (12: every face flux evaluated once per tile, shared through shared
@@ -96,7 +96,7 @@ def test_flux_variants_give_the_same_bits(variant):
     st1 = case.inflow_state(spec1, seed=77)
     runs = [(spec0, "shell", st0), (spec1, "shell", st1)]
     out = []
-    for v in (2, variant):
+    for v in (3, variant):
         bt = solver.Batch([(sp, topo) for sp, topo, _ in runs], precision=mhd.PREC_MIXED)
         bt.ctx.set_tune({"k_fluid_mixed": v})
         bt.load_states([st for _, _, st in runs])
@@ -108,7 +108,7 @@ def test_flux_variants_give_the_same_bits(variant):
     gs = load_golden("slab_6x5x6_t2x2_r00_steps.npz")
     spec, st = slab_setup(gs)
     res = []
-    for v in (2, variant):
+    for v in (3, variant):
         s = solver.Solver(spec, topology="tiled", precision=mhd.PREC_MIXED)
         s.ctx.set_tune({"k_fluid_mixed": v})
         s.load_state(st)
