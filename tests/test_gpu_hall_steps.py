@@ -82,3 +82,25 @@ def test_steps_with_implicit_hall_match_reference(kind, tmp_path):
         print("Hall steps %s: max rel L2 %.3e, solver %s" % (kind, worst, stats))
     finally:
         s.ctx.close()
+
+
+def test_newton_step_limit_ends_the_solve_on_the_device():
+    """A Newton step limit of one with an unreachable tolerance: the
+    device-steered loop stops after one step with the iteration-limit reason
+    (-5, as SNES_DIVERGED_MAX_IT), and the step completes with finite fields;
+    the GMRES iteration limit bounds each linear solve the same way."""
+    spec = case.slab_case(24, (5, 6), (2, 2))
+    st = case.inflow_state(spec, seed=20261205)
+    s = solver.Solver(spec, topology="tiled")
+    try:
+        s.load_state(st)
+        s.install_hall_implicit("tiled", rtol=1e-300, atol=1e-300, maxit=1, ksp_rtol=1e-300, ksp_maxit=3)
+        s.step(2)
+        stats = s.ctx.hall_stats()
+        assert stats["reason"] == -5 and stats["its"] == 1, stats
+        assert 1 <= stats["linear_its"] <= 3, stats
+        assert stats["fnorm"] < stats["fnorm0"], stats
+        for name in ("U_H", "B_xi", "Ehall_xi"):
+            assert np.all(np.isfinite(s.field(name, 1))), name
+    finally:
+        s.ctx.close()
