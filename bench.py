@@ -121,13 +121,13 @@ ALGO_BYTES_MIXED = {"k_pv_uplus_dt": 12 * 8 + 48 * 4 + 6 * 8 + 7 * 4,
 # grows with the cells they cover):
 # * C2 at half the cells per direction (165,888 cells: 114.26 MB read +
 #   10.32 MB written) to the full C2 slab (1,327,104 cells);
-# * the shell sweep's first 6 runs (2,269,318 cells; k_fluid_mixed 602.42 MB
-#   read + 141.94 MB written, k_pv_uplus_dt 763.50 + 185.09 MB) to all 48
-#   runs (14,879,028 cells)
+# * the shell sweep's first 6 runs (2,269,318 cells; k_fluid_mixed at 3 CTAs
+#   per SM 602.60 MB read + 145.68 MB written, k_pv_uplus_dt 763.50 + 185.09
+#   MB) to all 48 runs (14,879,028 cells)
 _SWEEP_SCALE = 14879028.0 / 2269318.0
 NCU_TRAFFIC_BYTES = {
     ("k_pv_uplus_dt", "c2_slab6x96x48x48_implicit_resistive_fp64"): (114.25536e6 + 10.321408e6) * 8.0,
-    ("k_fluid_mixed", "c5s_sweep48_shell_runs_mixed"): (602.41792e6 + 141.940224e6) * _SWEEP_SCALE,
+    ("k_fluid_mixed", "c5s_sweep48_shell_runs_mixed"): (602.596096e6 + 145.683968e6) * _SWEEP_SCALE,
     ("k_pv_uplus_dt", "c5s_sweep48_shell_runs_mixed"): (763.501568e6 + 185.093888e6) * _SWEEP_SCALE,
 }
 
