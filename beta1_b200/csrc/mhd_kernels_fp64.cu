@@ -1209,34 +1209,34 @@ void launch_k_jcell(bool w32, dim3 grid, cudaStream_t st, const BlockView *bvs)
 // ---------------------------------------------------------------------------
 
 // one face of the CFL bound: (|u . n| + c_f) A with n the outward unit
-// normal (A and JD / A precomputed per face, k_face_normals); the face's area
-// and normal planes as FP64 (the reference's values) or as their FP32 copies
-// (the mixed form)
+// normal (A and JD / A precomputed per face, k_face_normals), in the
+// arithmetic of the face planes: FP64 with the FP64 planes (the reference's
+// values and operations), FP32 with their FP32 copies (the mixed form: the
+// speeds in FP32, summed over the faces in FP64)
 template <typename T>
-__device__ __forceinline__ double cfl_face_term(const T *Ap, const T *N0, const T *N1, const T *N2, int64_t p,
-                                                bool outward_plus, double ux, double uy, double uz, double Bx,
-                                                double By, double Bz, double B2, double rho, double cs2,
-                                                double inver_MA2)
+__device__ __forceinline__ T cfl_face_term(const T *Ap, const T *N0, const T *N1, const T *N2, int64_t p,
+                                           bool outward_plus, T ux, T uy, T uz, T Bx, T By, T Bz, T B2, T rho, T cs2,
+                                           T inver_MA2)
 {
-    const double A = double(Ap[p]);
-    if (A <= 0.0)
-        return 0.0;
-    double nx = double(N0[p]), ny = double(N1[p]), nz = double(N2[p]);
+    const T A = Ap[p];
+    if (A <= T(0))
+        return T(0);
+    T nx = N0[p], ny = N1[p], nz = N2[p];
     if (!outward_plus)
     {
         nx = -nx;
         ny = -ny;
         nz = -nz;
     }
-    const double un = ux * nx + uy * ny + uz * nz;
-    const double Bn = Bx * nx + By * ny + Bz * nz;
-    const double vA2 = inver_MA2 * B2 / rho;
-    const double vAn2 = inver_MA2 * (Bn * Bn) / rho;
-    const double term = cs2 + vA2;
-    double disc = term * term - 4.0 * cs2 * vAn2;
-    if (disc < 0.0)
-        disc = 0.0;
-    const double cf = sqrt(0.5 * (term + sqrt(disc)));
+    const T un = ux * nx + uy * ny + uz * nz;
+    const T Bn = Bx * nx + By * ny + Bz * nz;
+    const T vA2 = inver_MA2 * B2 / rho;
+    const T vAn2 = inver_MA2 * (Bn * Bn) / rho;
+    const T term = cs2 + vA2;
+    T disc = term * term - T(4) * cs2 * vAn2;
+    if (disc < T(0))
+        disc = T(0);
+    const T cf = sqrt(T(0.5) * (term + sqrt(disc)));
     return (fabs(un) + cf) * A;
 }
 
@@ -1348,14 +1348,17 @@ __device__ __forceinline__ void k_pv_uplus_dt_body(const BlockView *__restrict__
                     for (int q = 0; q < 4; ++q)
                         P[a][q] = face_planes<WT>(b, a, q);
                 const int64_t pa1[3] = {pidx(b, i + 1, j, k), pidx(b, i, j + 1, k), pidx(b, i, j, k + 1)};
+                // the face speeds in the planes' arithmetic (identity casts in FP64)
+                const WT uxw = WT(ux), uyw = WT(uy), uzw = WT(uz), Bxw = WT(Bx), Byw = WT(By), Bzw = WT(Bz);
+                const WT B2w = WT(B2), rhow = WT(rho), cs2w = WT(cs2), iMA2 = WT(c.inver_MA2);
                 double denom = 0.0;
 #pragma unroll
                 for (int a = 0; a < 3; ++a)
                 {
-                    denom += cfl_face_term(P[a][0], P[a][1], P[a][2], P[a][3], p, false, ux, uy, uz, Bx, By, Bz, B2,
-                                           rho, cs2, c.inver_MA2);
-                    denom += cfl_face_term(P[a][0], P[a][1], P[a][2], P[a][3], pa1[a], true, ux, uy, uz, Bx, By, Bz,
-                                           B2, rho, cs2, c.inver_MA2);
+                    denom += double(cfl_face_term<WT>(P[a][0], P[a][1], P[a][2], P[a][3], p, false, uxw, uyw, uzw, Bxw,
+                                                      Byw, Bzw, B2w, rhow, cs2w, iMA2));
+                    denom += double(cfl_face_term<WT>(P[a][0], P[a][1], P[a][2], P[a][3], pa1[a], true, uxw, uyw, uzw,
+                                                      Bxw, Byw, Bzw, B2w, rhow, cs2w, iMA2));
                 }
                 // cells with denom <= 0 (or NaN) do not bound dt, as in the reference
                 if (denom > 0.0)
