@@ -627,24 +627,29 @@ def main():
     group_ms = sum(per_step.get(k, 0.0) for k in FLUX_CT_GROUP)
     group_gbs = FLUX_CT_BYTES[mixed] * cells / (group_ms / 1000.0) / 1e9 if group_ms > 0 else None
 
-    # end to end through host buffers (pinned), H2D + D2H inside the region
+    # end to end through host buffers (pinned), H2D + D2H inside the region:
+    # the state's inner points (mhd_step_host_inner; the ghost points the
+    # step reads are formed on the device by the Syncs)
     from beta1_b200.mhd import PinnedArray
-    nstate = ctx.state_count()
+    nstate = ctx.state_count_inner()
     hin, hout = PinnedArray(nstate), PinnedArray(nstate)
     # the state after the timed steps, as the caller would hold it
     off = 0
     for b in range(nblocks):
         for name in ("U_H", "B_xi", "B_eta", "B_zeta"):
-            a = ctx.download(name, b).ravel()
+            inf = ctx.field_info(name, b)
+            a = ctx.download(name, b)
+            a = np.ascontiguousarray(a[tuple(slice(-l, h) for l, h in zip(inf["lo"], inf["hi"]))]).ravel()
             hin.a[off:off + a.size] = a
             off += a.size
-    ctx.step_host(1, hin.a, hout.a)
+    assert off == nstate
+    ctx.step_host_inner(1, hin.a, hout.a)
     torch.cuda.synchronize()
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     for _ in range(args.e2e_iters):
-        ctx.step_host(1, hin.a, hout.a)
+        ctx.step_host_inner(1, hin.a, hout.a)
     f1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = f0.elapsed_time(f1) / args.e2e_iters

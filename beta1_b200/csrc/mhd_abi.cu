@@ -3583,26 +3583,46 @@ int mhd_batch_step(mhd_ctx *ctx, int32_t nsteps, double *dt_out, double *time_ou
     return MHD_OK;
 }
 
-int64_t mhd_state_count(const mhd_ctx *ctx)
+namespace
 {
-    if (!ctx)
-        return -1;
+// the host state's box of field f in block b: the whole array (ghosts
+// included) or its inner points only (cells [0, n), faces [0, n] along
+// their own axis)
+void state_box(const mhd_ctx *ctx, int f, int b, bool inner, int lo[3], int hi[3])
+{
+    field_box(ctx, f, b, lo, hi);
+    if (!inner)
+        return;
+    const int g = kFields[f].nghost;
+    for (int a = 0; a < 3; ++a)
+    {
+        lo[a] = 0;
+        hi[a] -= g;
+    }
+}
+
+int64_t state_count(const mhd_ctx *ctx, bool inner)
+{
     int64_t n = 0;
     for (int b = 0; b < ctx->nblocks; ++b)
         for (int f : {int(F_U), int(F_Bxi), int(F_Beta), int(F_Bzeta)})
-            n += field_count(ctx, f, b);
+        {
+            int lo[3], hi[3];
+            state_box(ctx, f, b, inner, lo, hi);
+            n += int64_t(hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]) * kFields[f].ncomp;
+        }
     return n;
 }
 
-int mhd_step_host(mhd_ctx *ctx, int32_t nsteps, const double *state_in, double *state_out, int64_t count,
-                  double *dt_out)
+// upload, syncs, derived fields, steps, download of the state's boxes
+int step_host(mhd_ctx *ctx, int32_t nsteps, const double *state_in, double *state_out, int64_t count, double *dt_out,
+              bool inner)
 {
-    BIND_DEVICE(ctx);
-    if (!ctx || !state_in || !state_out || nsteps < 0)
+    if (!state_in || !state_out || nsteps < 0)
         return MHD_EINVAL;
-    if (count != mhd_state_count(ctx))
+    if (count != state_count(ctx, inner))
         return fail(ctx, MHD_EINVAL, "state holds %lld values, expected %lld", (long long)count,
-                    (long long)mhd_state_count(ctx));
+                    (long long)state_count(ctx, inner));
     RUN(ensure_staging(ctx, size_t(count)));
     CK(ctx, cudaMemcpyAsync(ctx->staging, state_in, size_t(count) * 8, cudaMemcpyHostToDevice, ctx->stream));
     int64_t off = 0;
@@ -3610,8 +3630,8 @@ int mhd_step_host(mhd_ctx *ctx, int32_t nsteps, const double *state_in, double *
         for (int f : {int(F_U), int(F_Bxi), int(F_Beta), int(F_Bzeta)})
         {
             int lo[3], hi[3];
-            field_box(ctx, f, b, lo, hi);
-            const int64_t n = field_count(ctx, f, b);
+            state_box(ctx, f, b, inner, lo, hi);
+            const int64_t n = int64_t(hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]) * kFields[f].ncomp;
             prof_begin(ctx, "k_aos_to_soa");
             k_aos_to_soa<<<grid_for(n), kThreads, 0, ctx->stream>>>(ctx->dbv, b, f, kFields[f].ncomp, lo[0], lo[1],
                                                                     lo[2], hi[0] - lo[0], hi[1] - lo[1],
@@ -3631,8 +3651,8 @@ int mhd_step_host(mhd_ctx *ctx, int32_t nsteps, const double *state_in, double *
         for (int f : {int(F_U), int(F_Bxi), int(F_Beta), int(F_Bzeta)})
         {
             int lo[3], hi[3];
-            field_box(ctx, f, b, lo, hi);
-            const int64_t n = field_count(ctx, f, b);
+            state_box(ctx, f, b, inner, lo, hi);
+            const int64_t n = int64_t(hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]) * kFields[f].ncomp;
             prof_begin(ctx, "k_soa_to_aos");
             k_soa_to_aos<<<grid_for(n), kThreads, 0, ctx->stream>>>(ctx->dbv, b, f, kFields[f].ncomp, lo[0], lo[1],
                                                                     lo[2], hi[0] - lo[0], hi[1] - lo[1],
@@ -3645,6 +3665,35 @@ int mhd_step_host(mhd_ctx *ctx, int32_t nsteps, const double *state_in, double *
     if (dt_out)
         CK(ctx, cudaMemcpy(dt_out, ctx->dt, 8, cudaMemcpyDeviceToHost));
     return MHD_OK;
+}
+} // namespace
+
+int64_t mhd_state_count(const mhd_ctx *ctx)
+{
+    return ctx ? state_count(ctx, false) : -1;
+}
+
+int64_t mhd_state_count_inner(const mhd_ctx *ctx)
+{
+    return ctx ? state_count(ctx, true) : -1;
+}
+
+int mhd_step_host(mhd_ctx *ctx, int32_t nsteps, const double *state_in, double *state_out, int64_t count,
+                  double *dt_out)
+{
+    BIND_DEVICE(ctx);
+    if (!ctx)
+        return MHD_EINVAL;
+    return step_host(ctx, nsteps, state_in, state_out, count, dt_out, false);
+}
+
+int mhd_step_host_inner(mhd_ctx *ctx, int32_t nsteps, const double *state_in, double *state_out, int64_t count,
+                        double *dt_out)
+{
+    BIND_DEVICE(ctx);
+    if (!ctx)
+        return MHD_EINVAL;
+    return step_host(ctx, nsteps, state_in, state_out, count, dt_out, true);
 }
 
 int mhd_host_alloc(int64_t bytes, void **ptr)

@@ -96,6 +96,9 @@ _SIGS = {
     "mhd_step": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "mhd_step_host": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_double)]),
     "mhd_state_count": (C.c_int64, [C.c_void_p]),
+    "mhd_step_host_inner": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64,
+                                      C.POINTER(C.c_double)]),
+    "mhd_state_count_inner": (C.c_int64, [C.c_void_p]),
     "mhd_host_alloc": (C.c_int, [C.c_int64, C.POINTER(C.c_void_p)]),
     "mhd_host_free": (C.c_int, [C.c_void_p]),
     "mhd_stage": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -415,6 +418,16 @@ class Context:
         dt = C.c_double()
         self._check(self.lib.mhd_step_host(self.h, nsteps, state_in.ctypes.data, state_out.ctypes.data,
                                            state_in.size, C.byref(dt)), "step_host")
+        return dt.value
+
+    def state_count_inner(self) -> int:
+        return int(self.lib.mhd_state_count_inner(self.h))
+
+    def step_host_inner(self, nsteps: int, state_in: np.ndarray, state_out: np.ndarray) -> float:
+        """mhd_step_host with the state's inner points only"""
+        dt = C.c_double()
+        self._check(self.lib.mhd_step_host_inner(self.h, nsteps, state_in.ctypes.data, state_out.ctypes.data,
+                                                 state_in.size, C.byref(dt)), "step_host_inner")
         return dt.value
 
     def launches(self) -> int:

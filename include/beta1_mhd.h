@@ -379,6 +379,17 @@ int mhd_step_host(mhd_ctx *ctx, int32_t nsteps, const double *state_in, double *
 /* Size in doubles of the concatenated host state used by mhd_step_host. */
 int64_t mhd_state_count(const mhd_ctx *ctx);
 
+/* The same end-to-end step with the state's inner points only (no
+   counterpart in the reference, whose arrays carry their ghost layers):
+   cells [0, n) and faces [0, n] along their own axis, AoS, block after
+   block, U_H then B_xi / B_eta / B_zeta.  The ghost points the step reads
+   are formed on the device by the Syncs, as in mhd_step_host; ghost points
+   no Sync writes keep their device values and are not read by the step.
+   mhd_state_count_inner gives the size in doubles. */
+int mhd_step_host_inner(mhd_ctx *ctx, int32_t nsteps, const double *state_in, double *state_out, int64_t count,
+                        double *dt_out);
+int64_t mhd_state_count_inner(const mhd_ctx *ctx);
+
 /* Page-locked host memory for the state buffers (cudaHostAlloc). */
 int mhd_host_alloc(int64_t bytes, void **ptr);
 int mhd_host_free(void *ptr);
