@@ -372,7 +372,10 @@ int mhd_step(mhd_ctx *ctx, int32_t nsteps, double *dt_out, double *time_out);
    every block from host AoS arrays (concatenated block after block), runs
    Sync("Ucell"), Sync("Bface"), UpdateDerivedFields_ and `nsteps` StepOnce,
    downloads the same fields back.  The host arrays may be pinned (see
-   mhd_host_alloc) for full copy bandwidth. */
+   mhd_host_alloc) for full copy bandwidth.  Each call starts as a restart
+   does: the state is taken as read from a restart file, before
+   UpdateDerivedFields_ (on a grid with Poles that pass rewrites B_zeta on the
+   first cell layer, so feeding a call's output back in applies it twice). */
 int mhd_step_host(mhd_ctx *ctx, int32_t nsteps, const double *state_in, double *state_out, int64_t count,
                   double *dt_out);
 
