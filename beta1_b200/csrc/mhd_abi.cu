@@ -547,6 +547,8 @@ int pole_rings(mhd_ctx *ctx, const std::string &group)
     }
     if (group == "Jedge")
         return launch_pole(ctx, POLE_JETA);
+    if (group == "Eres" || group == "Eres1form")
+        return launch_pole(ctx, POLE_ERES_REG);
     return MHD_OK;
 }
 
@@ -1196,7 +1198,10 @@ int launch_step_c(mhd_ctx *ctx)
 // ResistiveDiffusionSubcycles_ (Z4_Lunar/src/physics/LunarSolver_MagneticRHS.cpp:53-115):
 // per sub-cycle Sync("Bface"), B_cell / J edge / J_cell with their syncs,
 // the resistive edge EMF, Sync("Eres"), then B += (dt / nsub) (-curl Eres)
-// and Sync("Bface")
+// and Sync("Bface").  With Poles, UpdateMagneticDerivedFields_ in the
+// reference's order: the B_zeta rewrite after Sync("B_cell") (which the J
+// edges read) and the pole-shell J_cell before Sync("J_cell"); Sync("Eres")
+// regulates Eres_eta on the pole rings.
 int launch_resistive_explicit(mhd_ctx *ctx)
 {
     const int nb = ctx->nblocks;
@@ -1209,6 +1214,7 @@ int launch_resistive_explicit(mhd_ctx *ctx)
         launch_k_bcell(false, dim3(grid_for(max_box(ctx, LOC_CELL, 0)), nb), s, ctx->dbv);
         RUN(launched(ctx));
         RUN(run_sync(ctx, "B_cell"));
+        RUN(launch_pole(ctx, POLE_BZETA));
         prof_begin(ctx, "k_jedge");
         k_jedge<<<dim3(gs, nb), kThreads, 0, s>>>(ctx->dbv, F_Bxi, F_Jxi, 1.0, nullptr);
         RUN(launched(ctx));
@@ -1216,6 +1222,7 @@ int launch_resistive_explicit(mhd_ctx *ctx)
         prof_begin(ctx, "k_jcell");
         k_jcell<<<dim3(grid_for(max_box(ctx, LOC_CELL, 0)), nb), kThreads, 0, s>>>(ctx->dbv);
         RUN(launched(ctx));
+        RUN(launch_pole(ctx, POLE_JCELL));
         RUN(run_sync(ctx, "J_cell"));
         prof_begin(ctx, "k_eres_explicit");
         k_eres_explicit<<<dim3(gs, nb), kThreads, 0, s>>>(ctx->dbv, ctx->res_inver_Rem);
@@ -2912,8 +2919,8 @@ int mhd_set_pole(mhd_ctx *ctx, int32_t block, int32_t direction)
     const BlockView &v = ctx->hbv[size_t(block)];
     if (v.nj < 2)
         return fail(ctx, MHD_EINVAL, "a block with Poles needs at least two cells in j");
-    if (ctx->res.on || ctx->res_nsub > 0 || ctx->hall.n > 0)
-        return fail(ctx, MHD_ESTATE, "Poles are not available with the resistive or implicit Hall solves");
+    if (ctx->res.on || ctx->hall.n > 0)
+        return fail(ctx, MHD_ESTATE, "Poles are not available with the implicit resistive or Hall solves");
     for (size_t q = 0; q < ctx->poles.size(); q += 2)
         if (ctx->poles[q] == block && ctx->poles[q + 1] == direction)
             return MHD_OK;
@@ -2949,7 +2956,7 @@ int mhd_set_resistive(mhd_ctx *ctx, int64_t n, const int64_t *unknowns, const do
     if (ctx->nruns > 1 && n > 0)
         return fail(ctx, MHD_ESTATE, "the implicit resistive solve is not available in a batch of runs (one shared dt per solve)");
     if (!ctx->poles.empty() && n > 0)
-        return fail(ctx, MHD_ESTATE, "the resistive Pole handlers are not available");
+        return fail(ctx, MHD_ESTATE, "the implicit resistive solve is not available with Poles");
     if (restart <= 0 || restart > kMaxRestart)
         return fail(ctx, MHD_EINVAL, "GMRES restart must be in [1, %d]", kMaxRestart);
     if (maxit < 0)
@@ -3272,8 +3279,6 @@ int mhd_set_resistive_explicit(mhd_ctx *ctx, double inver_Rem, int32_t nsub)
         return fail(ctx, MHD_ESTATE, "the explicit resistive sub-cycling is not available in a batch of runs (one shared dt per solve)");
     if (nsub > 0 && ctx->res.on)
         return fail(ctx, MHD_ESTATE, "the implicit resistive solve is set up; the two are exclusive");
-    if (nsub > 0 && !ctx->poles.empty())
-        return fail(ctx, MHD_ESTATE, "the resistive Pole handlers are not available");
     ctx->res_nsub = nsub;
     ctx->res_inver_Rem = inver_Rem;
     // the hot sync lists depend on it (J_cell ghost depth)

@@ -2412,14 +2412,17 @@ __device__ void pole_bcell_warp(const BlockView &b, int side, int64_t t, PoleTer
     }
 }
 
-__device__ void pole_eeta_warp(const BlockView &b, int side, int64_t t, PoleTerm *sh, double *cache, bool build)
+// the regulation of E_eta (field F_Eeta) or Eres_eta (F_Ereseta): both are
+// eta edges of the same ring, so their normal matrices (from dr_eta) are one
+__device__ void pole_eeta_warp(const BlockView &b, int side, int64_t t, PoleTerm *sh, double *cache, bool build,
+                               int field)
 {
     const int lane = threadIdx.x & 31;
     const int nj = b.nj, nk = b.nk;
     const int64_t v = b.vol;
     const int i = int(t);
     const int jc = side < 0 ? 0 : nj - 1;
-    double *E = b.f[F_Eeta];
+    double *E = b.f[field];
     const double *dr = b.f[F_dreta];
     double acc = 0.0;
     int cnt = 0;
@@ -2539,7 +2542,7 @@ __device__ void pole_jcell_warp(const BlockView &b, int side, int64_t t, PoleTer
 // which of the three least-squares operations (cache slot), -1 otherwise
 __host__ __device__ inline int pole_lsq_slot(int op)
 {
-    return op == POLE_BCELL ? 0 : op == POLE_EETA_REG ? 1 : op == POLE_JCELL ? 2 : -1;
+    return op == POLE_BCELL ? 0 : (op == POLE_EETA_REG || op == POLE_ERES_REG) ? 1 : op == POLE_JCELL ? 2 : -1;
 }
 
 // cache: per Pole, per least-squares operation, per ring i (stride rings):
@@ -2559,8 +2562,8 @@ __global__ void __launch_bounds__(32 * kPoleWarps) k_pole_warp(const BlockView *
     double *c = cache + ((int64_t(blockIdx.y) * 3 + pole_lsq_slot(op)) * stride + ring) * 10;
     if (op == POLE_BCELL)
         pole_bcell_warp(b, side, t, sh[warp], c, build != 0);
-    else if (op == POLE_EETA_REG)
-        pole_eeta_warp(b, side, t, sh[warp], c, build != 0);
+    else if (op == POLE_EETA_REG || op == POLE_ERES_REG)
+        pole_eeta_warp(b, side, t, sh[warp], c, build != 0, op == POLE_ERES_REG ? F_Ereseta : F_Eeta);
     else
         pole_jcell_warp(b, side, t, sh[warp], c, build != 0);
 }

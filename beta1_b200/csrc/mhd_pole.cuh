@@ -24,6 +24,7 @@ enum PoleOp : int
     POLE_BZETA,      // B_zeta of the first cell layer: flux of Bind_cell
     POLE_JCELL,      // J_cell of the first cell layer: least-squares ring vector
     POLE_DIVB,       // divB of the first cell layer: 0
+    POLE_ERES_REG,   // Eres_eta: the regulation of POLE_EETA_REG on the resistive edge EMF
     NPOLE_OP
 };
 
@@ -36,6 +37,7 @@ __host__ __device__ inline int64_t pole_work(int op, int ni, int nk)
         return int64_t(ni) * 5;
     case POLE_RING_BXI:
     case POLE_EETA_REG:
+    case POLE_ERES_REG:
         return ni + 1;
     case POLE_BCELL:
         return int64_t(ni) * 2;
@@ -224,9 +226,10 @@ __host__ __device__ inline void pole_one(const BlockView &b, int side, int op, i
         break;
     }
     case POLE_EETA_REG: // BC_Pole_Eedge_RegulateK_Norm, E_eta on an eta Pole (Boundary_Condition.cpp:179-477)
+    case POLE_ERES_REG: // ... and Eres_eta (Boundary_Build.cpp:218-226)
     {
         const int i = int(t);
-        double *E = b.f[F_Eeta];
+        double *E = b.f[op == POLE_ERES_REG ? F_Ereseta : F_Eeta];
         const double *dr = b.f[F_dreta];
         double A[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
         double rhs[3] = {0.0, 0.0, 0.0};

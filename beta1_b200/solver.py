@@ -253,14 +253,15 @@ class Solver:
 
     def install_shell(self):
         """The single-block spherical shell: Solid_Surface and Farfield in i,
-        eta Poles at both ends of j, k periodic onto itself (ideal MHD)."""
+        eta Poles at both ends of j, k periodic onto itself (ideal MHD, or
+        the explicit resistive sub-cycles)."""
         spec = self.spec
         if len(spec.blocks) != 1:
             raise ValueError("a shell has one block")
         p = spec.params
-        if p.get("is_Lunar_resistance", 0):
-            raise NotImplementedError("the resistive Pole handlers are not built")
-        key = ("shell_maps",)
+        if p.get("is_Lunar_resistance", 0) and p.get("use_implicit_lunar_resistance", 0):
+            raise NotImplementedError("the implicit resistive solve is not built for a shell")
+        key = ("shell_maps", bool(p.get("is_Lunar_resistance", 0)))
         if key not in self._cache:
             self._cache[key] = shell_tables(spec, self.nodes[0], self.ctx)
         self.sync_sizes = install_maps(self.ctx, self._cache[key])
@@ -294,10 +295,12 @@ def farfield_consts(params):
 
 
 def shell_tables(spec: case_mod.CaseSpec, nodes, layout=None):
-    """Sync tables of a single-block shell (syncmap.compile_shell)."""
+    """Sync tables of a single-block shell (syncmap.compile_shell), with the
+    resistive handlers when the case sets is_Lunar_resistance."""
     b = spec.blocks[0]
     lay = layout if layout is not None else mhd.HostLayout([b.ncell])
-    return syncmap.compile_shell(lay, b.ncell, False, farfield_consts(spec.params), nodes)
+    return syncmap.compile_shell(lay, b.ncell, bool(spec.params.get("is_Lunar_resistance", 0)),
+                                 farfield_consts(spec.params), nodes)
 
 
 def install_maps(ctx, maps):

@@ -350,37 +350,40 @@ def compile_tiled(ctx, layout: TiledLayout, resistive: bool, farfield_consts, no
 #   ring   the device computes the first inner layer (the pole ring): U_H's
 #          k average (BC_Pole_Cell_), the B_cell / Bind_cell collapse, B_xi's
 #          k average (BC_Pole_Bface_Collapse_), E_xi from -u x B
-#          (BC_Pole_Eedge_Axis), E_eta's regulation (BC_Pole_Eedge_RegulateK_Norm);
-#          then the ghost copy
+#          (BC_Pole_Eedge_Axis), E_eta's and Eres_eta's regulation
+#          (BC_Pole_Eedge_RegulateK_Norm); then the ghost copy
 #   zero   the first inner layer <- 0, then the ghost copy (B_eta's norm face,
-#          BC_Pole_Eedge_Zero_Rotate of E_zeta, J_xi, J_zeta)
+#          BC_Pole_Eedge_Zero_Rotate of E_zeta, J_xi, J_zeta, Eres_xi, Eres_zeta)
 #   ring_ghost_zero  the device computes the first inner layer (J_eta,
 #          BC_Pole_Jedge_RegulateK_Norm); the ghost slab <- 0
 SHELL_POLE_RULES = {"U_plus": "nop", "U_H": "ring", "B_cell": "ring", "Bind_cell": "ring", "B_xi": "ring",
                     "E_xi": "ring", "E_eta": "ring", "B_eta": "zero", "E_zeta": "zero", "J_xi": "zero",
-                    "J_zeta": "zero", "J_eta": "ring_ghost_zero"}
+                    "J_zeta": "zero", "J_eta": "ring_ghost_zero", "Eres_xi": "zero", "Eres_eta": "ring",
+                    "Eres_zeta": "zero"}
 
 # groups with a computing Pole handler (the device runs their ring kernels
 # before the group's tables)
-SHELL_POLE_HANDLED = ("Ucell", "Bface", "Eedge", "B_cell", "Jedge")
+SHELL_POLE_HANDLED = ("Ucell", "Bface", "Eedge", "B_cell", "Jedge", "Eres", "Eres1form")
 
 # groups whose Sync runs the halo exchange only (no physical handlers, no
 # corner default): Sync("Uplus") after calc_Uplus
 SHELL_HALO_ONLY = ("Uplus",)
 
-# resistive groups: their Pole handlers (the Eres regulation) are not compiled
+# resistive groups: compiled only for a resistive set-up
 SHELL_SKIPPED = ("Eres", "Eres1form")
 
 
 def shell_pole_rule(field: str) -> str:
-    """What the Pole handler of the shipped Lunar set-up does to a field."""
-    if field.startswith("Eres"):
-        raise ValueError(f"the Pole handler of {field} is not compiled")
+    """What the Pole handler of the shipped Lunar set-up does to a field
+    (eta Poles: Eres_xi and Eres_zeta Zero_Rotate, Eres_eta regulated,
+    Z4_Lunar/src/boundary/Boundary_Build.cpp:208-239)."""
     return SHELL_POLE_RULES.get(field, "copy")
 
 
 def compile_shell(ctx, ncell, resistive: bool, farfield_consts=None, nodes=None):
-    """Tables of every Sync group of the shell (the resistive groups aside).
+    """Tables of every Sync group of the shell; the resistive groups and
+    handlers with `resistive` (is_Lunar_resistance: the Solid_Surface
+    handlers of J_cell, Eface and the edge EMF of Boundary_Build.cpp:93-163).
     ctx: a context or HostLayout of the one block; farfield_consts: dict with
     'qinf' (5), 'B_imf' (3), 'E_inf' (3); nodes: the block's Padded ghost node
     mesh (both needed by the groups with Farfield values).
@@ -398,12 +401,10 @@ def compile_shell(ctx, ncell, resistive: bool, farfield_consts=None, nodes=None)
     zeroes or rewrites it), hence the copies before the fixed values, and the
     two gathers around the wall.
     Returns {group: dict(dst, src, dst2, src2, cdst, cval, walls)}."""
-    if resistive:
-        raise NotImplementedError("the resistive handlers of the shell are not compiled")
     n = tuple(ncell)
     out = {}
     for group, fields in GROUPS.items():
-        if group in SHELL_SKIPPED:
+        if group in SHELL_SKIPPED and not resistive:
             continue
         physical = group not in SHELL_HALO_ONLY
         dsts, srcs, dsts2, srcs2, cdst, cval, walls = [], [], [], [], [], [], []
@@ -453,7 +454,7 @@ def compile_shell(ctx, ncell, resistive: bool, farfield_consts=None, nodes=None)
                         const(ghost, 0.0)
                         continue
                     copy(ghost, lambda x: I[x], lambda x, jr=jr: np.full_like(J[x], jr), lambda x: K[x])
-                solid, far = wall_rules(f, False)
+                solid, far = wall_rules(f, resistive)
                 # Farfield (i max)
                 g_hi = tin & (I >= ih[0])
                 if far == "copy":
@@ -482,6 +483,10 @@ def compile_shell(ctx, ncell, resistive: bool, farfield_consts=None, nodes=None)
                 elif solid in ("slab_zero_copy", "slab_zero2_copy"):
                     const(tin & ((I == 0) | ((I == 1) & (solid == "slab_zero2_copy"))), 0.0)
                     copy(g_lo, lambda x: np.zeros_like(I[x]), lambda x: J[x], lambda x: K[x])
+                elif solid == "eface_ghost_zero":
+                    # BC_Solid_Surface_Eface_ghots_zero: the normal field's wall
+                    # layer and every field's ghost slab <- 0
+                    const(g_lo | (tin & (I == 0) & (f == "Eface_xi")), 0.0)
                 elif solid == "wall_u":
                     # the wall handler rewrites the wall layer and its ghosts in place
                     w = np.nonzero(tin & (I <= 0))[0]

@@ -192,15 +192,18 @@ int mhd_set_sync_wall(mhd_ctx *ctx, const char *group, int32_t block, int32_t di
    (Pole, Pole, Farfield, Solid_Surface, Boundary_Sync_.cpp:4-65): the Pole
    rings the handlers compute (BC_Pole_Cell_, BC_Pole_Bcell_Collapse_,
    BC_Pole_Bface_Collapse_, BC_Pole_Eedge_Axis, BC_Pole_Eedge_RegulateK_Norm,
-   BC_Pole_Jedge_RegulateK_Norm), the composed copies of mhd_set_sync_map
+   BC_Pole_Jedge_RegulateK_Norm, and in the resistive groups Eres / Eres1form
+   the regulation of Eres_eta), the composed copies of mhd_set_sync_map
    (sources read after the rings, before the wall handlers), the wall
    handlers, the copies of mhd_set_sync_map_post (sources the wall handlers
    wrote), then the fixed values of mhd_set_sync_consts.  The derived-field
    pass adds the Pole repairs of Z4_Lunar/src/physics/LunarSolver_Tools.cpp
    (B_zeta of the first cell layer after Sync("B_cell"), :242-307; the
    least-squares J_cell of the pole shell, :945-1090) and MHD_STAGE_DIVB
-   zeroes divB there (:729-772).  Needs the geometry field Astar_eta.  Not
-   available with the resistive or implicit Hall solves (MHD_ESTATE). */
+   zeroes divB there (:729-772); the explicit resistive sub-cycles
+   (mhd_set_resistive_explicit) run the same repairs in each sub-cycle's
+   UpdateMagneticDerivedFields_.  Needs the geometry field Astar_eta.  Not
+   available with the implicit resistive or implicit Hall solves (MHD_ESTATE). */
 int mhd_set_pole(mhd_ctx *ctx, int32_t block, int32_t direction);
 
 /* Geometry of a block built on the device from its ghost node mesh

@@ -951,14 +951,16 @@ class ShellOracle(Oracle):
     a Pole (src/6_boundary/Boundary.cpp:178-260), then the periodic halo in k.
     The derived-field pass adds the reference's Pole repairs: the B_zeta flux
     rewrite after Sync("B_cell"), the least-squares J_cell of the pole shell
-    and the divB zeroing next to the Poles."""
+    and the divB zeroing next to the Poles.  resistive: the handlers the
+    reference registers when is_Lunar_resistance is set (the Solid_Surface
+    handlers of J_cell, Eface and the edge EMF, Boundary_Build.cpp:93-163)
+    and the Eres groups with their Pole handlers (Boundary_Build.cpp:208-239)."""
 
     POLES = (-1, +1)  # j min (direction -2), j max (direction +2)
 
     def __init__(self, ncell, consts, nodes, qinf, B_imf, resistive=False, G=4):
         super().__init__([ncell], consts, G)
-        if resistive:
-            raise NotImplementedError("the resistive handlers of the shell are not restated")
+        self.resistive = bool(resistive)
         self.nodes = nodes      # Padded ghost node mesh (..., 3) of the block
         self.qinf = np.asarray(qinf, dtype=np.float64)
         self.B_imf = np.asarray(B_imf, dtype=np.float64)
@@ -1040,16 +1042,16 @@ class ShellOracle(Oracle):
             self._zero_slab("B_eta", 1, side)
         elif name == "E_xi":
             self._pole_eedge_axis(side)
-        elif name == "E_eta":
-            self._pole_eedge_regulate(side)
+        elif name in ("E_eta", "Eres_eta"):
+            self._pole_eedge_regulate(side, name=name)
             return
-        elif name in ("E_zeta", "J_xi", "J_zeta"):
+        elif name in ("E_zeta", "J_xi", "J_zeta", "Eres_xi", "Eres_zeta"):
+            # BC_Pole_Eedge_Zero_Rotate (Boundary_Condition.cpp:165-177); on an
+            # eta Pole Eres_xi takes it too (Boundary_Build.cpp:208-216)
             self._zero_slab(name, 1, side)
         elif name == "J_eta":
             self._pole_jedge_regulate(side)
             return
-        elif name.startswith("Eres"):
-            raise NotImplementedError(name)
         self._copy_ghosts(name, 1, side)
 
     def _pole_cell(self, side):
@@ -1132,12 +1134,12 @@ class ShellOracle(Oracle):
                 dl = [self._at("dr_xi", i, j, k, m) for m in range(3)]
                 self._put("E_xi", i, j, k, 0, E[0] * dl[0] + E[1] * dl[1] + E[2] * dl[2])
 
-    def _pole_eedge_regulate(self, side, ghosts=True):
-        """BC_Pole_Eedge_RegulateK_Norm for E_eta on an eta Pole
+    def _pole_eedge_regulate(self, side, ghosts=True, name="E_eta"):
+        """BC_Pole_Eedge_RegulateK_Norm for E_eta (or Eres_eta) on an eta Pole
         (Boundary_Condition.cpp:179-477): per ring the Cartesian vector whose
         projections best reproduce the edge values (k = n_k excluded: it is
         k = 0), projected back onto every edge; then the ghost copy."""
-        ih = self._ih("E_eta")
+        ih = self._ih(name)
         j = 0 if side < 0 else ih[1] - 1
         for i in range(ih[0]):
             A = [[0.0] * 3 for _ in range(3)]
@@ -1150,7 +1152,7 @@ class ShellOracle(Oracle):
                     continue
                 invL = 1.0 / L
                 tau = [dl[0] * invL, dl[1] * invL, dl[2] * invL]
-                y = self._at("E_eta", i, j, k) * invL
+                y = self._at(name, i, j, k) * invL
                 for a in range(3):
                     b[a] += y * tau[a]
                     for c in range(3):
@@ -1158,7 +1160,7 @@ class ShellOracle(Oracle):
                 cnt += 1
             if cnt <= 0:
                 for k in range(ih[2]):
-                    self._put("E_eta", i, j, k, 0, 0.0)
+                    self._put(name, i, j, k, 0, 0.0)
                 continue
             trA = A[0][0] + A[1][1] + A[2][2]
             reg = 1.0e-12 * _cmax(1.0, trA)
@@ -1168,18 +1170,18 @@ class ShellOracle(Oracle):
             if Ev is None:
                 avg = 0.0
                 for k in range(ih[2]):
-                    avg += self._at("E_eta", i, j, k)
+                    avg += self._at(name, i, j, k)
                 avg /= float(ih[2])
                 for k in range(ih[2]):
-                    self._put("E_eta", i, j, k, 0, avg)
+                    self._put(name, i, j, k, 0, avg)
                 continue
             for k in range(ih[2]):
                 dl = [self._at("dr_eta", i, j, k, m) for m in range(3)]
                 L = np.sqrt(dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2])
                 v = 0.0 if L < 1.0e-14 else Ev[0] * dl[0] + Ev[1] * dl[1] + Ev[2] * dl[2]
-                self._put("E_eta", i, j, k, 0, v)
+                self._put(name, i, j, k, 0, v)
         if ghosts:
-            self._copy_ghosts("E_eta", 1, side)
+            self._copy_ghosts(name, 1, side)
 
     def _pole_jedge_regulate(self, side, ghosts=True):
         """BC_Pole_Jedge_RegulateK_Norm for J_eta on an eta Pole
@@ -1216,6 +1218,8 @@ class ShellOracle(Oracle):
                 self._pole_eedge_regulate(side, ghosts=False)
             elif group == "Jedge":
                 self._pole_jedge_regulate(side, ghosts=False)
+            elif group in ("Eres", "Eres1form"):
+                self._pole_eedge_regulate(side, ghosts=False, name="Eres_eta")
 
     # -------------------------------------------- Farfield / Solid_Surface
     def _farfield(self, name):
@@ -1247,13 +1251,21 @@ class ShellOracle(Oracle):
             self._copy_ghosts(name, 0, +1)
 
     def _solid(self, name):
-        """Solid_Surface handler (i min) of the non-resistive set-up."""
-        if name in ("U_plus", "E_xi", "E_eta", "E_zeta"):
+        """Solid_Surface handler (i min).  With resistivity the reference
+        registers no J_cell or edge-EMF handler there (the default copy runs)
+        and zeroes only the Eface ghosts (with the normal field's wall layer)."""
+        if name == "U_plus" or (name in ("E_xi", "E_eta", "E_zeta") and not self.resistive):
             return
         if name == "U_H":
             self.wall_u(0, -1)                  # BC_Solid_Surface_
             return
-        if name == "J_cell":
+        if name.startswith("Eface_") and self.resistive:
+            # BC_Solid_Surface_Eface_ghots_zero (Boundary_Condition_EM.cpp)
+            if name == "Eface_xi":
+                self._zero_slab(name, 0, -1)
+            self._set_ghosts(name, 0, -1, [0.0, 0.0, 0.0])
+            return
+        if name == "J_cell" and not self.resistive:
             self._zero_slab("J_cell", 0, -1, layers=2)   # BC_Solid_Surface_Jcell (EM.cpp:382-427)
         elif name.startswith("Eface_"):
             self._zero_slab(name, 0, -1)        # BC_Solid_Surface_Eface_ (EM.cpp:787-803)
@@ -1289,7 +1301,8 @@ class ShellOracle(Oracle):
             "Ucell": ["U_H"], "Bface": ["B_xi", "B_eta", "B_zeta"], "Eface": ["Eface_xi", "Eface_eta", "Eface_zeta"],
             "Eedge": ["E_xi", "E_eta", "E_zeta"], "B_cell": ["B_cell", "Bind_cell"], "Jedge": ["J_xi", "J_eta", "J_zeta"],
             "J_cell": ["J_cell"], "Uplus": ["U_plus"], "dB": ["dB_xi", "dB_eta", "dB_zeta"],
-            "Badd": ["Badd_xi", "Badd_eta", "Badd_zeta"], "Ehall": ["Ehall_xi", "Ehall_eta", "Ehall_zeta"]}
+            "Badd": ["Badd_xi", "Badd_eta", "Badd_zeta"], "Ehall": ["Ehall_xi", "Ehall_eta", "Ehall_zeta"],
+            "Eres": ["Eres_xi", "Eres_eta", "Eres_zeta"], "Eres1form": ["Eres_xi", "Eres_eta", "Eres_zeta"]}
         fields = from_groups[group]
         if group not in self.HALO_ONLY:
             for f in fields:

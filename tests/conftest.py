@@ -56,10 +56,15 @@ def slab_setup(g):
 
 
 def shell_setup(g):
-    """(case spec, restart state) of the committed Pole-shell fixture."""
+    """(case spec, restart state) of a committed Pole-shell fixture (with the
+    explicit resistive sub-cycles when the fixture's flag says so)."""
     from beta1_b200 import case, rst
     LOCS = {"U_H": rst.CELL, "B_xi": rst.FACE_XI, "B_eta": rst.FACE_ET, "B_zeta": rst.FACE_ZE}
-    spec = case.shell_case(*(int(v) for v in g["n"]))
+    over = {}
+    if "resistive" in g.files and int(g["resistive"][0]):
+        over = {k[len("param/"):]: g[k].item() for k in g.files if k.startswith("param/")}
+        over.update(is_Lunar_resistance=1, use_implicit_lunar_resistance=0)
+    spec = case.shell_case(*(int(v) for v in g["n"]), **over)
     st = rst.RestartFile(0, 0.0, 1, {})
     for name, loc in LOCS.items():
         rec = rst.FieldRecord(name, loc, 5 if name == "U_H" else 1, 4)

@@ -195,13 +195,19 @@ def shell_geom(nr=8, nth=6, nph=8):
     print("wrote", tag)
 
 
-def shell_steps(nr=8, nth=6, nph=8, steps=2, seed=20261207):
+def shell_tag(nr, nth, nph, resistive):
+    """fixture name of a shell; resistive shells (explicit sub-cycles) add _r10"""
+    return "shell_%dx%dx%d" % (nr, nth, nph) + ("_r10" if resistive else "")
+
+
+def shell_steps(nr=8, nth=6, nph=8, steps=2, seed=20261207, resistive=0, **over):
     """The reference's fields after 0..steps StepOnce on the Pole shell (the
     target of a device Pole path; the initial state is regenerated from
-    (case, seed) and kept here too)."""
-    tag = "shell_%dx%dx%d" % (nr, nth, nph)
+    (case, seed) and kept here too).  resistive: the explicit resistive
+    sub-cycles (is_Lunar_resistance with use_implicit_lunar_resistance 0)."""
+    tag = shell_tag(nr, nth, nph, resistive)
     with tempfile.TemporaryDirectory() as d:
-        spec = case.shell_case(nr, nth, nph)
+        spec = case.shell_case(nr, nth, nph, is_Lunar_resistance=resistive, use_implicit_lunar_resistance=0, **over)
         case.write_case(d, spec)
         st = case.inflow_state(spec, seed=seed)
         rst.write(os.path.join(d, "init.rst"), st)
@@ -209,13 +215,17 @@ def shell_steps(nr=8, nth=6, nph=8, steps=2, seed=20261207):
         arr = {}
         for k, v in flatten(st, ["U_H", "B_xi", "B_eta", "B_zeta"], 0).items():
             arr["init/b0/%s" % k] = v
+        names = STEP_FIELDS + (["Eres_xi", "Eres_eta", "Eres_zeta"] if resistive else [])
         for s_ in range(steps + 1):
             r = rst.read(os.path.join(d, "step_%04d.bin" % s_))
-            for k, v in flatten(r, STEP_FIELDS, 0).items():
+            for k, v in flatten(r, names, 0).items():
                 arr["s%d/b0/%s" % (s_, k)] = v
             arr["s%d/dt" % s_] = r.fields["dt"].blocks[0].data.reshape(())
         arr["n"] = np.array([nr, nth, nph])
         arr["seed"] = np.array(seed)
+        arr["resistive"] = np.array([resistive, 0])
+        for k, v in over.items():
+            arr["param/" + k] = np.array(v)
         np.savez_compressed(os.path.join(OUT, tag + "_steps.npz"), **arr)
     print("wrote", tag, "steps")
 
@@ -237,13 +247,13 @@ def shell_diag(nr=8, nth=6, nph=8, seed=20261207, steps=2):
     print("wrote", tag + "_diag")
 
 
-def shell_probe(nr=8, nth=6, nph=8, seed=20261207):
+def shell_probe(nr=8, nth=6, nph=8, seed=20261207, resistive=0):
     """Every Sync group of the Pole shell probed on the reference (as
-    slab_probe)."""
+    slab_probe); resistive: the handlers of a resistive set-up."""
     from beta1_b200 import syncmap
-    tag = "shell_%dx%dx%d" % (nr, nth, nph)
+    tag = shell_tag(nr, nth, nph, resistive)
     with tempfile.TemporaryDirectory() as d:
-        spec = case.shell_case(nr, nth, nph)
+        spec = case.shell_case(nr, nth, nph, is_Lunar_resistance=resistive, use_implicit_lunar_resistance=0)
         case.write_case(d, spec)
         rst.write(os.path.join(d, "init.rst"), case.inflow_state(spec, seed=seed))
         arr = {}
@@ -258,6 +268,15 @@ def shell_probe(nr=8, nth=6, nph=8, seed=20261207):
                 arr["%s/%s/0/val" % (grp, fname)] = v[changed]
         np.savez_compressed(os.path.join(OUT, tag + "_probe.npz"), **arr)
     print("wrote", tag + "_probe")
+
+
+def shell_resistive():
+    """The explicit resistive sub-cycles on the Pole shell: the reference's
+    steps and Sync probe with the resistive handlers (peak resistivity 1,
+    two sub-cycles per step)."""
+    eta = 1.0 * case.MU0 * case.ref_scales()["U"] * case.ref_scales()["L_ref"]
+    shell_steps(resistive=1, eta_max_lunar=eta, n_resistive_subcycles=2)
+    shell_probe(resistive=1)
 
 
 def hall(spec_kind, seed=20261205):
@@ -402,6 +421,8 @@ if __name__ == "__main__":
     shell_steps()
     shell_probe()
     shell_diag()
+    # the shell with the explicit resistive sub-cycles (two per step) at peak resistivity 1
+    shell_resistive()
     slab_probe(resistive=0)
     slab_probe(resistive=1)
     hall("periodic")

@@ -18,13 +18,13 @@ from test_cpu_oracle_shell import build_shell_oracle, mhd_oracle
 from beta1_b200 import mhd
 
 OPS = ["POLE_RING_U", "POLE_RING_BXI", "POLE_BCELL", "POLE_EXI_AXIS", "POLE_EETA_REG", "POLE_JETA", "POLE_BZETA",
-       "POLE_JCELL", "POLE_DIVB"]
+       "POLE_JCELL", "POLE_DIVB", "POLE_ERES_REG"]
 OP = {name: i for i, name in enumerate(OPS)}
 # fields each operation writes: overwritten with noise first, so that the
 # operation has to produce them (the mid-run state already holds its results)
 OUTPUTS = {"POLE_RING_U": ["U_H"], "POLE_RING_BXI": ["B_xi"], "POLE_BCELL": ["B_cell", "Bind_cell"],
            "POLE_EXI_AXIS": ["E_xi"], "POLE_EETA_REG": ["E_eta"], "POLE_JETA": ["J_eta"], "POLE_BZETA": ["B_zeta"],
-           "POLE_JCELL": ["J_cell"], "POLE_DIVB": ["divB"]}
+           "POLE_JCELL": ["J_cell"], "POLE_DIVB": ["divB"], "POLE_ERES_REG": ["Eres_eta"]}
 
 
 @pytest.fixture(scope="module")
@@ -87,6 +87,9 @@ def oracle_op(o, op):
     elif op == "POLE_EETA_REG":
         for s in S:
             o._pole_eedge_regulate(s, ghosts=False)
+    elif op == "POLE_ERES_REG":
+        for s in S:
+            o._pole_eedge_regulate(s, ghosts=False, name="Eres_eta")
     elif op == "POLE_JETA":
         for s in S:
             o._pole_jedge_regulate(s, ghosts=False)

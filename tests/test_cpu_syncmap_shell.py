@@ -17,14 +17,14 @@ import numpy as np
 import pytest
 
 from conftest import load_golden
-from test_cpu_oracle_shell import build_shell_oracle, mhd_oracle
+from test_cpu_oracle_shell import build_shell_oracle, mhd_oracle, resistive_shell_params
 
 from beta1_b200 import case, mhd, physics, syncmap
 
 MASK = (1 << 40) - 1
 
 
-def shell_tables(n=(8, 6, 8)):
+def shell_tables(n=(8, 6, 8), resistive=False):
     spec = case.shell_case(*n)
     b = spec.blocks[0]
     q, B = physics.farfield_state(spec.params)
@@ -32,7 +32,7 @@ def shell_tables(n=(8, 6, 8)):
     E_inf = [B[1] * u[2] - B[2] * u[1], B[2] * u[0] - B[0] * u[2], B[0] * u[1] - B[1] * u[0]]
     from beta1_b200 import geometry
     lay = mhd.HostLayout([b.ncell])
-    maps = syncmap.compile_shell(lay, b.ncell, False, dict(qinf=q, B_imf=B, E_inf=E_inf),
+    maps = syncmap.compile_shell(lay, b.ncell, resistive, dict(qinf=q, B_imf=B, E_inf=E_inf),
                                  geometry.block_ghost_mesh(b, 4))
     return lay, maps
 
@@ -219,3 +219,73 @@ def test_device_order_on_other_shells(n):
         for f in syncmap.GROUPS[group]:
             assert np.array_equal(a.blocks[0].get_ref(f), b.blocks[0].get_ref(f)), (n, group, f)
     assert spec.blocks[0].ncell == n
+
+
+@pytest.fixture(scope="module")
+def resistive_tables():
+    return shell_tables(resistive=True)
+
+
+def test_resistive_tables_hold_every_group(resistive_tables):
+    lay, maps = resistive_tables
+    assert set(maps) == set(syncmap.GROUPS)
+    for group, t in maps.items():
+        allw = np.concatenate([t["dst"], t["dst2"], t["cdst"]])
+        assert np.unique(allw).size == allw.size, group
+
+
+@pytest.mark.parametrize("group", ["Eres", "Eres1form", "J_cell", "Eface", "Eedge", "Jedge", "B_cell", "Ucell"])
+def test_resistive_device_order_equals_reference_sync(resistive_tables, group):
+    """With is_Lunar_resistance: the compiled tables (after the Eres_eta
+    regulation on the pole rings) equal the reference's Sync on the probe
+    fixture, and the oracle's Sync in the reference's order in mid-run."""
+    lay, maps = resistive_tables
+    names = [t[0] for t in lay.table]
+    probe = load_golden("shell_8x6x8_r10_probe.npz")
+    over = resistive_shell_params()
+    o = build_shell_oracle(**over)
+    blk = o.blocks[0]
+    for f in syncmap.GROUPS[group]:
+        loc, nc, ng = mhd_oracle.FIELDS[f]
+        p = mhd_oracle.PLUS[loc]
+        shape = tuple(blk.n[a] + p[a] + 2 * ng for a in range(3)) + (nc,)
+        blk.set_ref(f, (-ng, -ng, -ng), (np.arange(np.prod(shape), dtype=np.float64) + 1.0).reshape(shape))
+    device_order_sync(o, names, group, maps[group])
+    for f in syncmap.GROUPS[group]:
+        got = blk.get_ref(f).reshape(-1)
+        ref = np.arange(got.size, dtype=np.float64) + 1.0
+        ref[probe["%s/%s/0/dst" % (group, f)]] = probe["%s/%s/0/val" % (group, f)]
+        assert np.count_nonzero(got != ref) == 0, (group, f)
+    mid = build_shell_oracle(**over)
+    mid.step()
+    a = copy.deepcopy(mid)
+    b = copy.deepcopy(mid)
+    a.sync(group)
+    device_order_sync(b, names, group, maps[group])
+    for f in syncmap.GROUPS[group]:
+        assert np.array_equal(a.blocks[0].get_ref(f), b.blocks[0].get_ref(f)), (group, f)
+
+
+def test_resistive_device_order_steps_equal_reference(resistive_tables):
+    """Two StepOnce with the explicit resistive sub-cycles, every Sync in the
+    device order (compiled resistive tables) and the device's derived-field
+    order in each sub-cycle: the reference's fields bitwise, Eres included."""
+    lay, maps = resistive_tables
+    names = [t[0] for t in lay.table]
+
+    class DeviceOrder(mhd_oracle.ShellOracle):
+        def sync(self, group):
+            device_order_sync(self, names, group, maps[group])
+
+    ref = build_shell_oracle(**resistive_shell_params())
+    o = DeviceOrder.__new__(DeviceOrder)
+    o.__dict__.update(copy.deepcopy(ref.__dict__))
+    g = load_golden("shell_8x6x8_r10_steps.npz")
+    for s in (1, 2):
+        assert o.step() == float(g["s%d/dt" % s])
+        o.calc_divb()
+        for key in g.files:
+            if not key.startswith("s%d/b0/" % s) or key.endswith("__lo"):
+                continue
+            f = key.split("/")[-1]
+            assert np.array_equal(o.blocks[0].get_ref(f), g[key]), (s, f)

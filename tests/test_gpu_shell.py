@@ -125,3 +125,47 @@ def test_shell_first_step_matches_reference_in_batch():
         assert np.array_equal(bt.field(0, f), g["s1/b0/" + f]), f
     assert bt.ctx.run_time(0)[0] == float(g["s1/dt"])
     bt.ctx.close()
+
+
+def test_resistive_shell_steps_match_reference():
+    """Two StepOnce with the explicit resistive sub-cycles (two per step, peak
+    resistivity 1) on the Pole shell: each sub-cycle's B_cell / J pass with
+    the B_zeta rewrite and the pole-shell J_cell, Sync("Eres") with the
+    Eres_eta regulation on the pole rings (Z4_Lunar/src/boundary/Boundary_Build.cpp:208-239)
+    and the resistive Solid_Surface handlers, against the reference's own
+    fields (tests/golden/shell_8x6x8_r10_steps.npz): every field, Eres
+    included, bit for bit, dt included (the 1e-12 relative L2 bound of the
+    FP64 path is asserted first, so that a failure reports its size)."""
+    g = load_golden("shell_8x6x8_r10_steps.npz")
+    spec, st = shell_setup(g)
+    assert spec.params["is_Lunar_resistance"] and int(spec.params["n_resistive_subcycles"]) == 2
+    s = solver.Solver(spec, topology="shell")
+    names = FIELDS + ["Eres_xi", "Eres_eta", "Eres_zeta"]
+    try:
+        s.load_state(st)
+        exact = total = 0
+        worst = 0.0
+        for n in (1, 2):
+            dt, _ = s.step(1)
+            ref_dt = float(g["s%d/dt" % n])
+            assert abs(dt - ref_dt) <= TOL * abs(ref_dt), (n, dt, ref_dt)
+            assert dt == ref_dt, (n, dt, ref_dt)
+            s.ctx.stage(mhd.STAGE_DIVB)
+            for f in names:
+                ref = g["s%d/b0/%s" % (n, f)]
+                got = s.field(f)
+                assert got.shape == ref.shape, (n, f)
+                if f == "divB":
+                    assert np.abs(got - ref).max() <= TOL, (n, f)
+                else:
+                    e = rel_l2(got, ref)
+                    worst = max(worst, e)
+                    assert e <= TOL, (n, f, e)
+                exact += int(np.array_equal(got, ref))
+                total += 1
+        # the resistive EMF reaches the pole rings: the regulated Eres_eta is not zero there
+        assert np.abs(g["s2/b0/Eres_eta"]).max() > 0.0
+        print("resistive shell: %d of %d fields bitwise, max rel L2 %.3e" % (exact, total, worst))
+        assert exact == total
+    finally:
+        s.ctx.close()
