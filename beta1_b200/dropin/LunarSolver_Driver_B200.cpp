@@ -23,11 +23,14 @@
 //
 // Errors follow the reference's convention: a message on stderr, then abort.
 // The implicit Hall solve (HALL_IMPLICIT 1) is not routed through the device
-// by this driver.
+// by this driver.  The explicit resistive sub-cycles are: their edge profile
+// is formed here from the solver's own node coordinates.
 #include "LunarSolver.h"
 
 #include "beta1_mhd.h"
 
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -211,6 +214,36 @@ const char *const kGeometry[] = {"Jac",      "JDxi",     "JDet",      "JDze",   
                                  "dl_zeta",  "Astar_xi", "Astar_eta", "Astar_zeta", "Bcell_from_Bface_w",
                                  "Jcell_from_Jedge_w", "Badd_xi", "Badd_eta", "Badd_zeta"};
 const char *const kState[] = {"U_H", "B_xi", "B_eta", "B_zeta"};
+
+// The resistivity profile of LunarSolver::AddResistiveEdgeEMF_To_
+// (Z4_Lunar/src/physics/LunarSolver_MagExplicit_Resis.cpp:72-88, 160-167) at
+// every inner edge of a block: yita0 of the radius of the edge's midpoint,
+// as the eta_edge_xi / eta_edge_eta / eta_edge_zeta fields the device's
+// resistive edge EMF reads (no ghost layers; edge box n + 1 across the edge).
+void upload_resistive_profile(mhd_ctx *ctx, Block &blk, int ib, int ni, int nj, int nk)
+{
+    const char *const names[3] = {"eta_edge_xi", "eta_edge_eta", "eta_edge_zeta"};
+    for (int ea = 0; ea < 3; ++ea)
+    {
+        const int di = ea == 0, dj = ea == 1, dk = ea == 2;
+        const int n0 = ni + (ea != 0), n1 = nj + (ea != 1), n2 = nk + (ea != 2);
+        std::vector<double> y(size_t(n0) * size_t(n1) * size_t(n2), 0.0);
+        for (int i = 0; i < n0; ++i)
+            for (int j = 0; j < n1; ++j)
+                for (int k = 0; k < n2; ++k)
+                {
+                    const double xm = 0.5 * (blk.x(i, j, k) + blk.x(i + di, j + dj, k + dk));
+                    const double ym = 0.5 * (blk.y(i, j, k) + blk.y(i + di, j + dj, k + dk));
+                    const double zm = 0.5 * (blk.z(i, j, k) + blk.z(i + di, j + dj, k + dk));
+                    const double r = std::sqrt(xm * xm + ym * ym + zm * zm);
+                    double v = 0.0;
+                    if (!(r <= 0.84 || r >= 1.04))
+                        v = 0.5 * (std::tanh((r - 0.84) / 0.02) - std::tanh((r - 1.04) / 0.02));
+                    y[(size_t(i) * size_t(n1) + size_t(j)) * size_t(n2) + size_t(k)] = v;
+                }
+        check(ctx, mhd_upload_field(ctx, names[ea], ib, y.data(), int64_t(y.size())), names[ea]);
+    }
+}
 // what the reference's diagnostics and writers read at output steps
 const char *const kOutput[] = {"U_H",   "B_xi",   "B_eta",  "B_zeta",    "PV_H",    "U_plus",
                                "B_cell", "Bind_cell", "J_xi", "J_eta",   "J_zeta",  "J_cell",
@@ -297,8 +330,12 @@ bool LunarSolver::StepOnce()
         }
         else if (resist_control.is_Lunar_resistance)
         {
-            std::fprintf(stderr, "[beta1_mhd] the explicit resistive sub-cycles are not routed by this driver\n");
-            std::abort();
+            // ResistiveDiffusionSubcycles_ (Z4_Lunar/src/physics/LunarSolver_MagneticRHS.cpp:53-115)
+            for (int ib = 0; ib < nb; ++ib)
+                upload_resistive_profile(d.ctx, fld_->grd->grids(ib), ib, blocks[size_t(ib)].ni,
+                                         blocks[size_t(ib)].nj, blocks[size_t(ib)].nk);
+            check(d.ctx, mhd_set_resistive_explicit(d.ctx, inver_Rem, std::max(1, resist_control.n_subcycles)),
+                  "mhd_set_resistive_explicit");
         }
         check(d.ctx, mhd_set_time(d.ctx, run_data_->dt, run_data_->time, run_data_->step), "mhd_set_time");
         // the host state's derived fields were computed by Advance(); the

@@ -36,14 +36,16 @@ def compile_case(spec, topology: str) -> dict:
     lay = mhd.HostLayout([b.ncell for b in spec.blocks])
     resistive = bool(spec.params.get("is_Lunar_resistance", 0))
     implicit = resistive and bool(spec.params.get("use_implicit_lunar_resistance", 0))
-    if resistive and not implicit:
-        raise NotImplementedError("the explicit resistive sub-cycles need the eta_edge fields; not exported")
+    # the explicit resistive sub-cycles need only the resistive sync groups:
+    # the driver forms their edge profile from its own node coordinates
     if topology == "tiled":
         consts = solver.farfield_consts(spec.params)
         groups = syncmap.compile_tiled(lay, syncmap.TiledLayout(spec.blocks[0].ncell, spec.tiles), resistive, consts,
                                        nodes)
-    elif resistive:
+    elif implicit:
         raise NotImplementedError("the implicit resistive solve is exported for the tiled layout only")
+    elif resistive and topology != "shell":
+        raise NotImplementedError("the resistive handlers are compiled for the tiled layout and the shell")
     else:
         groups = solver.run_tables(spec, topology, nodes)
     poles = []
