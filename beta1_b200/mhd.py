@@ -176,6 +176,20 @@ class HostLayout:
         return (self.index[name] << 56) | (int(block) << 40)
 
 
+
+def check_state_buffers(state_in: np.ndarray, state_out: np.ndarray, count: int) -> None:
+    """The host buffers of a host-buffer step: C-contiguous float64 arrays of
+    exactly `count` values each, the output writable (the library reads
+    `count` values from one and writes as many to the other; the input is
+    read in full before the output is written, so both may be one array)."""
+    for name, a in (("state_in", state_in), ("state_out", state_out)):
+        if not isinstance(a, np.ndarray) or a.dtype != np.float64 or not a.flags.c_contiguous:
+            raise TypeError(f"{name} must be a C-contiguous float64 numpy array")
+        if a.size != count:
+            raise ValueError(f"{name} holds {a.size} values, the state {count}")
+    if not state_out.flags.writeable:
+        raise ValueError("state_out is read-only")
+
 class Context:
     """One device context (all blocks of one grid on the current GPU)."""
 
@@ -415,6 +429,8 @@ class Context:
         return int(self.lib.mhd_state_count(self.h))
 
     def step_host(self, nsteps: int, state_in: np.ndarray, state_out: np.ndarray) -> float:
+        """mhd_step_host: the whole state arrays (ghost layers included)"""
+        check_state_buffers(state_in, state_out, self.state_count())
         dt = C.c_double()
         self._check(self.lib.mhd_step_host(self.h, nsteps, state_in.ctypes.data, state_out.ctypes.data,
                                            state_in.size, C.byref(dt)), "step_host")
@@ -425,6 +441,7 @@ class Context:
 
     def step_host_inner(self, nsteps: int, state_in: np.ndarray, state_out: np.ndarray) -> float:
         """mhd_step_host with the state's inner points only"""
+        check_state_buffers(state_in, state_out, self.state_count_inner())
         dt = C.c_double()
         self._check(self.lib.mhd_step_host_inner(self.h, nsteps, state_in.ctypes.data, state_out.ctypes.data,
                                                  state_in.size, C.byref(dt)), "step_host_inner")

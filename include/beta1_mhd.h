@@ -374,7 +374,9 @@ int mhd_step(mhd_ctx *ctx, int32_t nsteps, double *dt_out, double *time_out);
 /* End-to-end step through host buffers: uploads U_H and B_xi/B_eta/B_zeta of
    every block from host AoS arrays (concatenated block after block), runs
    Sync("Ucell"), Sync("Bface"), UpdateDerivedFields_ and `nsteps` StepOnce,
-   downloads the same fields back.  The host arrays may be pinned (see
+   downloads the same fields back.  state_in and state_out each hold `count`
+   values (mhd_state_count); the input is read in full before the output is
+   written, so they may be the same array.  The host arrays may be pinned (see
    mhd_host_alloc) for full copy bandwidth.  Each call starts as a restart
    does: the state is taken as read from a restart file, before
    UpdateDerivedFields_ (on a grid with Poles that pass rewrites B_zeta on the

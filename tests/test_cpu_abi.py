@@ -69,3 +69,25 @@ def test_host_layout_point_ids(lib):
     assert info["lo"] == (-4, -4, -4) and info["hi"] == (8, 9, 8)
     pid = lay.point_base("B_eta", 1)
     assert pid >> 56 == lay.index["B_eta"] and (pid >> 40) & 0xFFFF == 1
+
+
+def test_host_state_buffers_are_checked_before_the_call():
+    """The host-buffer step's wrapper refuses buffers the library would read
+    or write past: wrong size, dtype or layout, or a read-only output."""
+    import numpy as np
+    n = 12
+    good = np.zeros(n)
+    mhd.check_state_buffers(good, np.zeros(n), n)
+    mhd.check_state_buffers(good, good, n)  # in place
+    with pytest.raises(ValueError):
+        mhd.check_state_buffers(good, np.zeros(n - 1), n)
+    with pytest.raises(ValueError):
+        mhd.check_state_buffers(np.zeros(n + 1), np.zeros(n + 1), n)
+    with pytest.raises(TypeError):
+        mhd.check_state_buffers(np.zeros(n, dtype=np.float32), good, n)
+    with pytest.raises(TypeError):
+        mhd.check_state_buffers(good, np.zeros(2 * n)[::2], n)
+    ro = np.zeros(n)
+    ro.flags.writeable = False
+    with pytest.raises(ValueError):
+        mhd.check_state_buffers(good, ro, n)
