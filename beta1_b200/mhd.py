@@ -177,6 +177,14 @@ class HostLayout:
 
 
 
+def _same_size(*named):
+    """the arrays a call passes with one count hold that many values each"""
+    n = named[0][1].size
+    for name, a in named:
+        if a.size != n:
+            raise ValueError(f"{name} holds {a.size} values, {named[0][0]} {n}")
+
+
 def check_state_buffers(state_in: np.ndarray, state_out: np.ndarray, count: int) -> None:
     """The host buffers of a host-buffer step: C-contiguous float64 arrays of
     exactly `count` values each, the output writable (the library reads
@@ -268,14 +276,14 @@ class Context:
     def set_sync_map(self, group: str, dst: np.ndarray, src: np.ndarray):
         d = np.ascontiguousarray(dst, dtype=np.int64)
         s = np.ascontiguousarray(src, dtype=np.int64)
-        assert d.shape == s.shape
+        _same_size(("dst", d), ("src", s))
         self._check(self.lib.mhd_set_sync_map(self.h, group.encode(), d.ctypes.data, s.ctypes.data, d.size),
                     f"set_sync_map {group}")
 
     def set_sync_consts(self, group: str, dst: np.ndarray, val: np.ndarray):
         d = np.ascontiguousarray(dst, dtype=np.int64)
         v = np.ascontiguousarray(val, dtype=np.float64)
-        assert d.shape == v.shape
+        _same_size(("dst", d), ("val", v))
         self._check(self.lib.mhd_set_sync_consts(self.h, group.encode(), d.ctypes.data, v.ctypes.data, d.size),
                     f"set_sync_consts {group}")
 
@@ -286,7 +294,7 @@ class Context:
         """copies run after the group's wall handlers (contexts with Poles)"""
         d = np.ascontiguousarray(dst, dtype=np.int64)
         s = np.ascontiguousarray(src, dtype=np.int64)
-        assert d.shape == s.shape
+        _same_size(("dst", d), ("src", s))
         self._check(self.lib.mhd_set_sync_map_post(self.h, group.encode(), d.ctypes.data, s.ctypes.data, d.size),
                     f"set_sync_map_post {group}")
 
@@ -297,7 +305,8 @@ class Context:
         bp = None
         if B_imf is not None:
             bv = np.ascontiguousarray(B_imf, dtype=np.float64)
-            assert bv.size == 3
+            if bv.size != 3:
+                raise ValueError("B_imf holds three values")
             bp = bv.ctypes.data
         self._check(self.lib.mhd_build_geometry(self.h, block, a.ctypes.data, a.size, bp), "build_geometry")
 
@@ -319,6 +328,8 @@ class Context:
         a = np.ascontiguousarray(alias, dtype=np.int64)
         o = np.ascontiguousarray(owner, dtype=np.int64)
         sg = np.ascontiguousarray(sign, dtype=np.float64)
+        _same_size(("unknowns", u), ("eta", e))
+        _same_size(("alias", a), ("owner", o), ("sign", sg))
         self._check(self.lib.mhd_set_resistive(self.h, u.size, u.ctypes.data, e.ctypes.data, a.size, a.ctypes.data,
                                                o.ctypes.data, sg.ctypes.data, rtol, atol, maxit, restart),
                     "set_resistive")
@@ -333,6 +344,7 @@ class Context:
         a = np.ascontiguousarray(alias, dtype=np.int64)
         o = np.ascontiguousarray(owner, dtype=np.int64)
         sg = np.ascontiguousarray(sign, dtype=np.float64)
+        _same_size(("alias", a), ("owner", o), ("sign", sg))
         self._check(self.lib.mhd_set_hall_implicit(self.h, u.size, u.ctypes.data, a.size, a.ctypes.data,
                                                    o.ctypes.data, sg.ctypes.data, float(rtol), float(atol), int(maxit),
                                                    float(ksp_rtol), int(ksp_maxit)), "set_hall_implicit")

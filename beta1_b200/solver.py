@@ -145,7 +145,8 @@ class Solver:
             self.geom.append(g)
             self.nodes.append(X)
         if topology == "periodic":
-            assert len(spec.blocks) == 1
+            if len(spec.blocks) != 1:
+                raise ValueError("a periodic box has one block")
             self.sync_sizes = syncmap.install_periodic(self.ctx, spec.blocks[0].ncell)
         elif topology == "tiled":
             self.install_tiled()

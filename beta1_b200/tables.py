@@ -133,10 +133,12 @@ def read(path: str) -> dict:
         pos[0] += n * np.dtype(dtype).itemsize
         return a
 
-    assert buf[:4] == b"B1TB"
+    if buf[:4] != b"B1TB":
+        raise ValueError("not a set-up file (no B1TB tag)")
     pos[0] = 4
     ver, ng = take("<ii")
-    assert ver == 1
+    if ver != 1:
+        raise ValueError(f"set-up file version {ver}, expected 1")
     groups = {}
     for _ in range(ng):
         (ln,) = take("<i")
