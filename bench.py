@@ -242,12 +242,19 @@ def mem_available_gb():
     return 16.0
 
 
-def cpu_reference(workload, n, steps, nproc, integrator="euler"):
+def ref_warmup(workload, warmup):
+    """untimed reference steps before the timed ones: the bench's warm-up,
+    at most 3, none for the Hall workloads (one step of the reference takes
+    minutes there)"""
+    return 0 if workload in ("c3", "c4") else max(0, min(int(warmup), 3))
+
+
+def cpu_reference(workload, n, steps, nproc, integrator="euler", warmup=0):
     """Times the reference's own StepOnce loop (oracle/_ref/ref_lunar, built
     from the reference sources) on `nproc` concurrent single-threaded
-    processes (bounded by host memory), each on the same bounded sample;
-    returns aggregate cell-updates/s, the per-process figures and the
-    process count."""
+    processes (bounded by host memory), each on the same bounded sample,
+    after `warmup` untimed steps; returns aggregate cell-updates/s, the
+    per-process figures and the process count."""
     from beta1_b200 import case, rst
     if not os.path.exists(REF_BIN):
         return None
@@ -268,7 +275,8 @@ def cpu_reference(workload, n, steps, nproc, integrator="euler"):
             for entry in os.listdir(d):
                 if entry not in ("init.rst",) and not entry.startswith("r"):
                     os.symlink(os.path.join(d, entry), os.path.join(wd, entry))
-            procs.append(subprocess.Popen([REF_BIN, command, os.path.join(d, "init.rst"), str(steps)], cwd=wd,
+            procs.append(subprocess.Popen([REF_BIN, command, os.path.join(d, "init.rst"), str(steps), str(warmup)],
+                                          cwd=wd,
                                           stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
         vals = []
         for pr in procs:
@@ -283,11 +291,12 @@ def cpu_reference(workload, n, steps, nproc, integrator="euler"):
         shutil.rmtree(d, ignore_errors=True)
 
 
-def cpu_reference_sweep(steps, nproc, nruns=SWEEP_RUNS, grid="slab"):
+def cpu_reference_sweep(steps, nproc, nruns=SWEEP_RUNS, grid="slab", warmup=0):
     """The reference's StepOnce loop on a sample of the sweep's runs: the
     first `nproc` runs (bounded by host cores and memory), one
-    single-threaded process per run, concurrently; returns aggregate
-    cell-updates/s, the per-process figures and the process count."""
+    single-threaded process per run, concurrently, each after `warmup`
+    untimed steps; returns aggregate cell-updates/s, the per-process figures
+    and the process count."""
     from beta1_b200 import case, rst
     if not os.path.exists(REF_BIN):
         return None
@@ -302,7 +311,8 @@ def cpu_reference_sweep(steps, nproc, nruns=SWEEP_RUNS, grid="slab"):
             os.makedirs(wd)
             case.write_case(wd, spec)
             rst.write(os.path.join(wd, "init.rst"), case.inflow_state(spec, seed=SWEEP_SEED0 + r))
-            procs.append(subprocess.Popen([REF_BIN, "time", os.path.join(wd, "init.rst"), str(steps)], cwd=wd,
+            procs.append(subprocess.Popen([REF_BIN, "time", os.path.join(wd, "init.rst"), str(steps), str(warmup)],
+                                          cwd=wd,
                                           stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
         vals = []
         for pr in procs:
@@ -417,10 +427,11 @@ def run_reference_arm(args):
         return 0
     wl = WORKLOADS[args.workload]
     steps = min(args.steps, args.ref_steps or wl["ref_steps"])
+    warm = ref_warmup(args.workload, args.warmup)
     if args.workload in SWEEP_GRID:
-        res = cpu_reference_sweep(steps, os.cpu_count() or 1, grid=SWEEP_GRID[args.workload][0])
+        res = cpu_reference_sweep(steps, os.cpu_count() or 1, grid=SWEEP_GRID[args.workload][0], warmup=warm)
     else:
-        res = cpu_reference(args.workload, args.n, steps, os.cpu_count() or 1, args.integrator)
+        res = cpu_reference(args.workload, args.n, steps, os.cpu_count() or 1, args.integrator, warmup=warm)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_lunar not built or failed"}))
         return 0
@@ -428,17 +439,19 @@ def run_reference_arm(args):
     cells = vals[0]["cells"] if args.workload not in SWEEP_GRID else sum(v["cells"] for v in vals)
     if args.workload in SWEEP_GRID:
         sample = "%s: the first %d runs of the sweep, one single-threaded process each, %d StepOnce per " \
-                 "process, concurrently (bounded by host cores and memory)" % (wl["name"], nproc, steps)
+                 "process after %d untimed, concurrently (bounded by host cores and memory)" \
+                 % (wl["name"], nproc, steps, warm)
     elif args.workload in ("c3", "c4"):
-        sample = "%s: %s; %d steps per process, %d concurrent single-threaded processes (bounded by host " \
-                 "cores and memory)" % (wl["name"], HALL_SAMPLE, steps, nproc)
+        sample = "%s: %s; %d steps per process (no untimed step: one takes minutes), %d concurrent " \
+                 "single-threaded processes (bounded by host cores and memory)" % (wl["name"], HALL_SAMPLE, steps,
+                                                                                    nproc)
     else:
-        sample = "%s: %d %s per process, %d concurrent single-threaded processes (bounded by host cores " \
-                 "and memory)" % (wl["name"], steps, "SSP-RK2 steps" if args.integrator == "rk2" else "StepOnce",
-                                  nproc)
+        sample = "%s: %d %s per process after %d untimed, %d concurrent single-threaded processes (bounded by " \
+                 "host cores and memory)" % (wl["name"], steps,
+                                             "SSP-RK2 steps" if args.integrator == "rk2" else "StepOnce", warm, nproc)
     line = {
         "impl": "reference", "metric": "cell-updates/s", "value": agg, "unit": "cell-updates/s",
-        "n_gpus": args.gpus, "steps": steps, "warmup": 0,
+        "n_gpus": args.gpus, "steps": steps, "warmup": warm,
         "ms_per_step": 1000.0 * max(v["seconds"] / v["steps"] for v in vals), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": wl["name"], "cells": cells},
@@ -660,22 +673,23 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ref_steps = args.ref_steps or wl["ref_steps"]
+        warm = ref_warmup(args.workload, args.warmup)
         if args.workload in SWEEP_GRID:
-            res = cpu_reference_sweep(ref_steps, 1, grid=SWEEP_GRID[args.workload][0])
+            res = cpu_reference_sweep(ref_steps, 1, grid=SWEEP_GRID[args.workload][0], warmup=warm)
             if res is not None:
                 cpu = {"value": res[0], "unit": "cell-updates/s", "cores": 1, "kind": "reference",
                        "sample": "%s, run 0 of the sweep (%d cells), %d StepOnce of the reference solver built "
-                                 "from its own sources, one single-threaded process"
-                                 % (wl["name"], res[1][0]["cells"], ref_steps)}
+                                 "from its own sources after %d untimed, one single-threaded process"
+                                 % (wl["name"], res[1][0]["cells"], ref_steps, warm)}
         else:
-            res = cpu_reference(args.workload, args.n, ref_steps, 1, args.integrator)
+            res = cpu_reference(args.workload, args.n, ref_steps, 1, args.integrator, warmup=warm)
             if res is not None:
                 agg, vals, _ = res
                 what = HALL_SAMPLE if args.workload in ("c3", "c4") else (
                     "SSP-RK2 step" if args.integrator == "rk2" else "StepOnce")
                 cpu = {"value": agg, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
-                       "sample": "%s, %d x %s of the reference solver built from its own sources, one "
-                                 "single-threaded process" % (wl["name"], ref_steps, what)}
+                       "sample": "%s, %d x %s of the reference solver built from its own sources after %d "
+                                 "untimed, one single-threaded process" % (wl["name"], ref_steps, what, warm)}
 
     config_name = workload_name(wl["name"] if args.workload != "c2" or args.c2_size == "96x48" else
                                 "c2_slab6x%sx%s_implicit_resistive_fp64" % (args.c2_size, args.c2_size.split("x")[1]), mixed)

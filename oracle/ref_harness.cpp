@@ -15,8 +15,9 @@
 //   ref_lunar hall <state.rst> <out.bin>           Hall edge EMF of the state
 //   ref_lunar hallstep <state.rst> <out.bin>       one implicit Hall solve (tight tolerances)
 //   ref_lunar hallrun <state.rst> <n> <prefix>     n StepOnce with the implicit Hall solve (HALL_IMPLICIT == 1)
-//   ref_lunar time  <state.rst> <nsteps>           wall time of the step loop
-//   ref_lunar timerk2 <state.rst> <nsteps>         wall time of SSP-RK2 steps
+//   ref_lunar time  <state.rst> <nsteps> [w]       wall time of the step loop (after w untimed steps)
+//   ref_lunar timerk2 <state.rst> <nsteps> [w]     wall time of SSP-RK2 steps (after w untimed ones)
+//   ref_lunar timehall <state.rst> <nsteps> [w]    wall time of steps with the implicit Hall solve
 //
 // The member functions are private in the reference; this translation unit
 // alone widens access to call them (the class layout is unchanged).
@@ -660,11 +661,14 @@ int cmd_hallstep(Harness &h, const std::string &state, const std::string &out)
     return 0;
 }
 
-int cmd_time(Harness &h, const std::string &state, int nsteps)
+// wall time of `nsteps` StepOnce after `warmup` untimed ones, for timing
+int cmd_time(Harness &h, const std::string &state, int nsteps, int warmup)
 {
     h.load_state(state);
     LunarSolver &s = *h.solver;
     s.UpdateDerivedFields_();
+    for (int n = 0; n < warmup; ++n) // untimed
+        s.StepOnce();
     int64_t cells = 0;
     for (int ib = 0; ib < h.fld->num_blocks(); ++ib)
     {
@@ -683,11 +687,13 @@ int cmd_time(Harness &h, const std::string &state, int nsteps)
 }
 
 // wall time of `nsteps` SSP-RK2 steps (rk2_step), for timing
-int cmd_timerk2(Harness &h, const std::string &state, int nsteps)
+int cmd_timerk2(Harness &h, const std::string &state, int nsteps, int warmup)
 {
     h.load_state(state);
     LunarSolver &s = *h.solver;
     s.UpdateDerivedFields_();
+    for (int n = 0; n < warmup; ++n) // untimed
+        rk2_step(h);
     int64_t cells = 0;
     for (int ib = 0; ib < h.fld->num_blocks(); ++ib)
     {
@@ -708,12 +714,14 @@ int cmd_timerk2(Harness &h, const std::string &state, int nsteps)
 // `nsteps` StepOnce as compiled with HALL_IMPLICIT == 1 (hall_step: the
 // implicit Hall solve at the step's dt, Newton rtol 1e-10, then calc_Bcell,
 // before the closing syncs and derived fields), for timing
-int cmd_timehall(Harness &h, const std::string &state, int nsteps)
+int cmd_timehall(Harness &h, const std::string &state, int nsteps, int warmup)
 {
     h.load_state(state);
     LunarSolver &s = *h.solver;
     s.UpdateDerivedFields_();
     SNESSetTolerances(s.hall_implicit_.snes_, 1e-50, 1e-10, 1e-30, 50, PETSC_DEFAULT);
+    for (int n = 0; n < warmup; ++n) // untimed
+        hall_step(s);
     int64_t cells = 0;
     for (int ib = 0; ib < h.fld->num_blocks(); ++ib)
     {
@@ -790,13 +798,13 @@ int main(int argc, char **argv)
         else if (cmd == "timehall" && argc >= 4)
         {
             std::cout.rdbuf(sink.rdbuf());
-            rc = cmd_timehall(h, argv[2], std::atoi(argv[3]));
+            rc = cmd_timehall(h, argv[2], std::atoi(argv[3]), argc >= 5 ? std::atoi(argv[4]) : 0);
         }
         else if (cmd == "timerk2" && argc >= 4)
         {
             std::cout.rdbuf(saved);
             std::cout.rdbuf(sink.rdbuf());
-            rc = cmd_timerk2(h, argv[2], std::atoi(argv[3]));
+            rc = cmd_timerk2(h, argv[2], std::atoi(argv[3]), argc >= 5 ? std::atoi(argv[4]) : 0);
         }
         else if (cmd == "time" && argc >= 4)
         {
@@ -804,7 +812,7 @@ int main(int argc, char **argv)
             std::streambuf *s2 = std::cout.rdbuf();
             // timing result goes to stdout via printf; solver chatter to the log
             std::cout.rdbuf(sink.rdbuf());
-            rc = cmd_time(h, argv[2], std::atoi(argv[3]));
+            rc = cmd_time(h, argv[2], std::atoi(argv[3]), argc >= 5 ? std::atoi(argv[4]) : 0);
             (void)s2;
         }
         else
