@@ -289,3 +289,23 @@ def test_resistive_device_order_steps_equal_reference(resistive_tables):
                 continue
             f = key.split("/")[-1]
             assert np.array_equal(o.blocks[0].get_ref(f), g[key]), (s, f)
+
+
+@pytest.mark.parametrize("n", [(10, 5, 12), (6, 2, 4)])
+def test_resistive_device_order_on_other_shells(n):
+    """The resistive tables on other shell sizes (an odd polar count; two
+    polar cells): every group, the Eres groups included, in the device order
+    equals the oracle's Sync in the reference's order after a step with the
+    explicit resistive sub-cycles."""
+    lay, maps = shell_tables(n, resistive=True)
+    names = [t[0] for t in lay.table]
+    mid = build_shell_oracle(n, seed=33, **resistive_shell_params())
+    mid.step()
+    assert np.abs(mid.blocks[0].get_ref("Eres_eta")).max() > 0.0
+    for group in maps:
+        a = copy.deepcopy(mid)
+        b = copy.deepcopy(mid)
+        a.sync(group)
+        device_order_sync(b, names, group, maps[group])
+        for f in syncmap.GROUPS[group]:
+            assert np.array_equal(a.blocks[0].get_ref(f), b.blocks[0].get_ref(f)), (n, group, f)
